@@ -1,0 +1,137 @@
+// Internal declarations shared by the diablo_b200 CUDA sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/diablo_b200.h"
+
+#define DG_MAX_PASSES 12
+
+// ------------------------------------------------------------ error plumbing
+void dg_set_error(const char *msg);
+void dg_count_launch(int n = 1);
+
+#define DG_CUDA(call)                                                              \
+  do {                                                                             \
+    cudaError_t _e = (call);                                                       \
+    if (_e != cudaSuccess) {                                                       \
+      dg_set_error((std::string(#call) + ": " + cudaGetErrorString(_e)).c_str());  \
+      return (_e == cudaErrorMemoryAllocation) ? DG_ERR_OOM : DG_ERR_CUDA;         \
+    }                                                                              \
+  } while (0)
+
+#define DG_LAUNCHED()                                                              \
+  do {                                                                             \
+    dg_count_launch();                                                             \
+    cudaError_t _e = cudaGetLastError();                                           \
+    if (_e != cudaSuccess) {                                                       \
+      dg_set_error((std::string("kernel launch: ") + cudaGetErrorString(_e)).c_str()); \
+      return DG_ERR_CUDA;                                                          \
+    }                                                                              \
+  } while (0)
+
+#define DG_TRY(call)                  \
+  do {                                \
+    int _s = (call);                  \
+    if (_s != DG_OK) return _s;       \
+  } while (0)
+
+// ------------------------------------------------------------------- FFT plan
+struct FftPlan {
+  int n;                       // transform length
+  int np;                      // number of Stockham passes
+  int r[DG_MAX_PASSES];        // radix of each pass (2, 3, 4, 8)
+};
+
+bool dg_make_plan(int n, FftPlan *pl);
+
+// up to 3 + DG_MAX_TH field pointers passed by value to kernels
+struct FieldPtrs {
+  double2 *p[3 + DG_MAX_TH + 1];
+};
+struct CFieldPtrs {
+  const double2 *p[3 + DG_MAX_TH + 1];
+};
+
+// ---------------------------------------------------------- CN system tables
+// Per field type, the mode-independent tridiagonal system of one RK substep
+// after elimination (rows 0..NY+1): multiplier a'(j), reciprocal pivot 1/b'(j),
+// upper diagonal c(j), and what feeds row j's right-hand side.
+enum { ROW_ZERO = 0, ROW_RHS = 1, ROW_BC = 2 };
+
+// field slots in the solver (velocity then scalars)
+enum { F_U1 = 0, F_U2 = 1, F_U3 = 2, F_TH0 = 3 };
+
+struct dg_handle {
+  dg_params p;
+  int NX, NY, NZ, NTH, NKX, NKZ, TNKZ, NKY, TNKY;
+  int nkxp, nkzt, nkyt;
+  int nplanes;                  // NY+2 (channel) or TNKY+1 (periodic)
+  long ss;                      // retained modes per plane
+  long nspec;                   // complex values per spectral field
+  int periodic;
+  int nf;                       // 3 + N_TH prognostic fields
+  int jstart, jend, jstart_th[DG_MAX_TH], jend_th[DG_MAX_TH];
+  double pi, eps;
+
+  cudaStream_t st;
+  bool own_stream;
+
+  // host copies of the tables
+  double *h_gy, *h_gyf, *h_dy, *h_dyf, *h_kx, *h_kz, *h_ky;
+
+  // device tables
+  double *gyf, *dy, *dyf, *kx, *kz, *ky, *kx2, *kz2, *ky2;
+  double2 *twx, *twz, *twy;     // exp(-2 pi i m / N) for the x, z, y lengths
+  FftPlan plx, plz, ply;
+
+  // device scalars: [0]=time [1]=delta_t [2..4]=h_bar(1..3) [5]=cfl min
+  double *dscal;
+
+  // spectral state (compact layout), double2 = (re, im)
+  double2 *cu[3 + DG_MAX_TH];   // CU1, CU2, CU3, CTH(n)
+  double2 *cf[3 + DG_MAX_TH];   // CF1..3, CFTH(n)
+  double2 *cp;
+  double2 *cr1;                 // phi from REM_DIV
+  double2 *rhs[3 + DG_MAX_TH];  // CN right-hand sides
+  double2 *gphi;                // REM_DIV forward-sweep scratch
+  double *rem_a, *rem_rb;       // REM_DIV multipliers and reciprocal pivots [NY+2][ss]
+  double *cn_tab;               // CN tables [field][4][NY+2]
+  int *cn_kind;                 // row kinds [field][NY+2]
+  double *cn_bc;                // BC row values [field][NY+2]
+
+  // work arrays
+  double2 *H;                   // half-physical [nf][planes][NZ][nkxp]
+  double2 *G;                   // product half-spectra [2nf][planes][NZ][nkxp]
+  double2 *work;                // general scratch
+  size_t work_bytes;
+  unsigned long long *dmin_bits;// CFL min as ordered bits
+  int *dflag;                   // non-finite flag
+
+  // periodic extras
+  double2 *Hy;                  // y-inverse output [nf][NY][nkzt][nkxp]
+  double2 *P;                   // products [9][NY][NZ][nkxp] then [9][NY][nkzt][nkxp]
+  double2 *Q;                   // z-forward products [9][NY][nkzt][nkxp]
+};
+
+// common kernel-launch helpers (defined in fft_kernels.cu)
+int dg_zinv(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax,
+            double2 *H, int field_stride_planes);
+int dg_xc2r_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax, double *phys,
+                   long phys_plane_stride, long phys_row_stride, long field_stride);
+int dg_xr2c_planes(dg_handle *h, const double *phys, int nf, int jmin, int jmax,
+                   long phys_plane_stride, long phys_row_stride, long field_stride, double2 *H);
+int dg_zfwd_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax,
+                   double2 *const *fields, double2 *raw_ref, long raw_ld);
+
+// channel / periodic internals
+int dg_chan_init(dg_handle *h);
+int dg_per_init(dg_handle *h);
+int dg_apply_bc_vel_dev(dg_handle *h);
+int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step);
+int dg_courant_dev(dg_handle *h, const double2 *const *u);
+int dg_stats_dev(dg_handle *h, dg_stats *s);
+
+static inline int dg_cdiv(long a, long b) { return (int)((a + b - 1) / b); }

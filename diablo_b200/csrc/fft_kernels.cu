@@ -1,0 +1,252 @@
+// Plane transforms between the retained-mode spectral layout and physical
+// space, built from the shared-memory Stockham FFT in fft.cuh.
+//
+//   zinv : spectral [j][kz][kx] -> half-physical H [j][z][kx]   (c2c along z, +1)
+//   xc2r : H [j][z][kx]         -> physical rows                  (c2r along x)
+//   xr2c : physical rows        -> H [j][z][kx] / NX              (r2c along x)
+//   zfwd : H [j][z][kx]         -> spectral [j][kz][kx] / NZ      (c2c along z, -1)
+//
+// Packing follows FFT_XZ_TO_FOURIER / FFT_XZ_TO_PHYSICAL (for/mpi.f:1530-1674):
+// kz = 0..NKZ at 0..NKZ, kz = -NKZ..-1 at NKZ+1..TNKZ; |kz| > NKZ, kx > NKX
+// and the x-Nyquist bin are zero on the way to physical space.  Real
+// transforms use the two-real-rows-per-complex-transform identity; the
+// imaginary parts of the x-DC and x-Nyquist bins are ignored by the c2r, as in
+// FFTW's complex-to-real.
+#include "dg_internal.cuh"
+#include "fft.cuh"
+
+using namespace dgfft;
+
+namespace {
+
+constexpr int KXG = 8;     // kx columns per CTA in the z transforms
+constexpr int RPAIR = 4;   // row pairs per CTA in the x transforms
+
+__device__ __forceinline__ int packed_index(int z, int NZ, int NKZ) {
+  // physical-order z bin -> packed kz slot, or -1 if not retained
+  if (z <= NKZ) return z;
+  if (z >= NZ - NKZ) return z - NZ + 1 + 2 * NKZ;
+  return -1;
+}
+
+__global__ void k_zinv(CFieldPtrs fields, int jmin, long ss, int nkxp,
+                       int NZ, int NKZ, FftPlan pl, const double2 *__restrict__ tw,
+                       double2 *__restrict__ H, long Hfield) {
+  extern __shared__ double2 sm[];
+  const int sstr = NZ + 1;
+  double2 *stw = sm;
+  double2 *b0 = stw + NZ;
+  double2 *b1 = b0 + KXG * sstr;
+  const int kx0 = blockIdx.x * KXG;
+  const int j = jmin + blockIdx.y;
+  const int f = blockIdx.z;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const double2 *in = fields.p[f] + (long)j * ss;
+  for (int i = tid; i < NZ; i += nthr) stw[i] = tw[i];
+  for (int idx = tid; idx < KXG * NZ; idx += nthr) {
+    const int c = idx % KXG, z = idx / KXG;
+    double2 v = make_double2(0.0, 0.0);
+    const int kp = packed_index(z, NZ, NKZ);
+    if (kp >= 0 && kx0 + c < nkxp) v = in[(long)kp * nkxp + kx0 + c];
+    b0[c * sstr + z] = v;
+  }
+  __syncthreads();
+  double2 *res = run(b0, b1, pl, KXG, sstr, stw, +1);
+  double2 *out = H + f * Hfield + (long)j * NZ * nkxp;
+  for (int idx = tid; idx < KXG * NZ; idx += nthr) {
+    const int c = idx % KXG, z = idx / KXG;
+    if (kx0 + c < nkxp) out[(long)z * nkxp + kx0 + c] = res[c * sstr + z];
+  }
+}
+
+__global__ void k_zfwd(const double2 *__restrict__ H, long Hfield, int jmin, int nkxp, int nkzt,
+                       int NZ, int NKZ, FftPlan pl, const double2 *__restrict__ tw,
+                       FieldPtrs fields, long ss) {
+  extern __shared__ double2 sm[];
+  const int sstr = NZ + 1;
+  double2 *stw = sm;
+  double2 *b0 = stw + NZ;
+  double2 *b1 = b0 + KXG * sstr;
+  const int kx0 = blockIdx.x * KXG;
+  const int j = jmin + blockIdx.y;
+  const int f = blockIdx.z;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const double2 *in = H + f * Hfield + (long)j * NZ * nkxp;
+  for (int i = tid; i < NZ; i += nthr) stw[i] = tw[i];
+  for (int idx = tid; idx < KXG * NZ; idx += nthr) {
+    const int c = idx % KXG, z = idx / KXG;
+    double2 v = make_double2(0.0, 0.0);
+    if (kx0 + c < nkxp) v = in[(long)z * nkxp + kx0 + c];
+    b0[c * sstr + z] = v;
+  }
+  __syncthreads();
+  double2 *res = run(b0, b1, pl, KXG, sstr, stw, -1);
+  double2 *out = fields.p[f] + (long)j * ss;
+  const double rnz = (double)NZ;
+  for (int idx = tid; idx < KXG * nkzt; idx += nthr) {
+    const int c = idx % KXG, kp = idx / KXG;
+    if (kx0 + c >= nkxp) continue;
+    const int z = (kp <= NKZ) ? kp : (NZ - 1 + (kp - NKZ) - NKZ);
+    const double2 v = res[c * sstr + z];
+    out[(long)kp * nkxp + kx0 + c] = make_double2(v.x / rnz, v.y / rnz);
+  }
+}
+
+// c2r of RPAIR row pairs of one plane of one field.
+__global__ void k_xc2r(const double2 *__restrict__ H, long Hfield, int jmin, int nkxp, int NX,
+                       int NZ, FftPlan pl, const double2 *__restrict__ tw, double *__restrict__ phys,
+                       long pplane, long prow, long pfield) {
+  extern __shared__ double2 sm[];
+  const int sstr = NX + 1;
+  double2 *stw = sm;
+  double2 *b0 = stw + NX;
+  double2 *b1 = b0 + RPAIR * sstr;
+  const int z0 = blockIdx.x * 2 * RPAIR;
+  const int j = jmin + blockIdx.y;
+  const int f = blockIdx.z;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const double2 *in = H + f * Hfield + (long)j * NZ * nkxp;
+  const int NKX = nkxp - 1;
+  for (int i = tid; i < NX; i += nthr) stw[i] = tw[i];
+  for (int idx = tid; idx < RPAIR * NX; idx += nthr) {
+    const int q = idx / NX, k = idx % NX;
+    const int za = z0 + 2 * q, zb = za + 1;
+    double2 v = make_double2(0.0, 0.0);
+    if (za < NZ) {
+      // bin k of Z = A + iB with Hermitian extension of A and B
+      const int kk = (k <= NX / 2) ? k : NX - k;
+      if (kk <= NKX && kk < NX / 2) {
+        double2 a = in[(long)za * nkxp + kk];
+        double2 b = (zb < NZ) ? in[(long)zb * nkxp + kk] : make_double2(0.0, 0.0);
+        if (kk == 0) {
+          a.y = 0.0;
+          b.y = 0.0;
+        }
+        if (k == kk)  // A_k + i B_k
+          v = make_double2(a.x - b.y, a.y + b.x);
+        else          // conj(A_k) + i conj(B_k)
+          v = make_double2(a.x + b.y, -a.y + b.x);
+      }
+    }
+    b0[q * sstr + k] = v;
+  }
+  __syncthreads();
+  double2 *res = run(b0, b1, pl, RPAIR, sstr, stw, +1);
+  double *out = phys + f * pfield + (long)j * pplane;
+  for (int idx = tid; idx < RPAIR * NX; idx += nthr) {
+    const int q = idx / NX, x = idx % NX;
+    const int za = z0 + 2 * q, zb = za + 1;
+    const double2 v = res[q * sstr + x];
+    if (za < NZ) out[(long)za * prow + x] = v.x;
+    if (zb < NZ) out[(long)zb * prow + x] = v.y;
+  }
+}
+
+// r2c of RPAIR row pairs of one plane of one field; keeps kx = 0..NKX, / NX.
+__global__ void k_xr2c(const double *__restrict__ phys, long pplane, long prow, long pfield,
+                       int jmin, int nkxp, int NX, int NZ, FftPlan pl,
+                       const double2 *__restrict__ tw, double2 *__restrict__ H, long Hfield) {
+  extern __shared__ double2 sm[];
+  const int sstr = NX + 1;
+  double2 *stw = sm;
+  double2 *b0 = stw + NX;
+  double2 *b1 = b0 + RPAIR * sstr;
+  const int z0 = blockIdx.x * 2 * RPAIR;
+  const int j = jmin + blockIdx.y;
+  const int f = blockIdx.z;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const double *in = phys + f * pfield + (long)j * pplane;
+  for (int i = tid; i < NX; i += nthr) stw[i] = tw[i];
+  for (int idx = tid; idx < RPAIR * NX; idx += nthr) {
+    const int q = idx / NX, x = idx % NX;
+    const int za = z0 + 2 * q, zb = za + 1;
+    double a = (za < NZ) ? in[(long)za * prow + x] : 0.0;
+    double b = (zb < NZ) ? in[(long)zb * prow + x] : 0.0;
+    b0[q * sstr + x] = make_double2(a, b);
+  }
+  __syncthreads();
+  double2 *res = run(b0, b1, pl, RPAIR, sstr, stw, -1);
+  double2 *out = H + f * Hfield + (long)j * NZ * nkxp;
+  const double rnx = (double)NX;
+  for (int idx = tid; idx < RPAIR * nkxp; idx += nthr) {
+    const int q = idx / nkxp, k = idx % nkxp;
+    const int za = z0 + 2 * q, zb = za + 1;
+    const double2 zk = res[q * sstr + k];
+    const double2 zm = res[q * sstr + ((NX - k) % NX)];
+    // A = (Z_k + conj Z_{N-k})/2, B = -i/2 (Z_k - conj Z_{N-k})
+    const double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+    const double2 B = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
+    if (za < NZ) out[(long)za * nkxp + k] = make_double2(A.x / rnx, A.y / rnx);
+    if (zb < NZ) out[(long)zb * nkxp + k] = make_double2(B.x / rnx, B.y / rnx);
+  }
+}
+
+size_t zsmem(int NZ) { return sizeof(double2) * (NZ + 2 * KXG * (NZ + 1)); }
+size_t xsmem(int NX) { return sizeof(double2) * (NX + 2 * RPAIR * (NX + 1)); }
+
+}  // namespace
+
+// ------------------------------------------------------------- host wrappers
+int dg_zinv(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax, double2 *H,
+            int) {
+  if (jmax < jmin || nf <= 0) return DG_OK;
+  CFieldPtrs fp;
+  for (int f = 0; f < nf; f++) fp.p[f] = fields[f];
+  dim3 grid(dg_cdiv(h->nkxp, KXG), jmax - jmin + 1, nf);
+  k_zinv<<<grid, 256, zsmem(h->NZ), h->st>>>(fp, jmin, h->ss, h->nkxp, h->NZ, h->NKZ, h->plz,
+                                             h->twz, H, (long)h->nplanes * h->NZ * h->nkxp);
+  DG_LAUNCHED();
+  return DG_OK;
+}
+
+int dg_zfwd_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax,
+                   double2 *const *fields, double2 *, long) {
+  if (jmax < jmin || nf <= 0) return DG_OK;
+  FieldPtrs fp;
+  for (int f = 0; f < nf; f++) fp.p[f] = fields[f];
+  dim3 grid(dg_cdiv(h->nkxp, KXG), jmax - jmin + 1, nf);
+  k_zfwd<<<grid, 256, zsmem(h->NZ), h->st>>>(H, (long)h->nplanes * h->NZ * h->nkxp, jmin, h->nkxp,
+                                             h->nkzt, h->NZ, h->NKZ, h->plz, h->twz, fp, h->ss);
+  DG_LAUNCHED();
+  return DG_OK;
+}
+
+int dg_xc2r_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax, double *phys,
+                   long pplane, long prow, long pfield) {
+  if (jmax < jmin || nf <= 0) return DG_OK;
+  dim3 grid(dg_cdiv(h->NZ, 2 * RPAIR), jmax - jmin + 1, nf);
+  k_xc2r<<<grid, 256, xsmem(h->NX), h->st>>>(H, (long)h->nplanes * h->NZ * h->nkxp, jmin, h->nkxp,
+                                             h->NX, h->NZ, h->plx, h->twx, phys, pplane, prow,
+                                             pfield);
+  DG_LAUNCHED();
+  return DG_OK;
+}
+
+int dg_xr2c_planes(dg_handle *h, const double *phys, int nf, int jmin, int jmax, long pplane,
+                   long prow, long pfield, double2 *H) {
+  if (jmax < jmin || nf <= 0) return DG_OK;
+  dim3 grid(dg_cdiv(h->NZ, 2 * RPAIR), jmax - jmin + 1, nf);
+  k_xr2c<<<grid, 256, xsmem(h->NX), h->st>>>(phys, pplane, prow, pfield, jmin, h->nkxp, h->NX,
+                                             h->NZ, h->plx, h->twx, H,
+                                             (long)h->nplanes * h->NZ * h->nkxp);
+  DG_LAUNCHED();
+  return DG_OK;
+}
+
+bool dg_make_plan(int n, FftPlan *pl) {
+  pl->n = n;
+  pl->np = 0;
+  int m = n;
+  while (m > 1) {
+    int r;
+    if (m % 8 == 0) r = 8;
+    else if (m % 4 == 0) r = 4;
+    else if (m % 2 == 0) r = 2;
+    else if (m % 3 == 0) r = 3;
+    else return false;
+    if (pl->np >= DG_MAX_PASSES) return false;
+    pl->r[pl->np++] = r;
+    m /= r;
+  }
+  return true;
+}

@@ -1,0 +1,411 @@
+// Handle lifecycle, device-resident state, tables and field I/O.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <atomic>
+#include <mutex>
+#include <string>
+
+#include "dg_internal.cuh"
+
+namespace {
+thread_local std::string g_err;
+std::atomic<long long> g_launches{0};
+
+// exp(-2 pi i m / n) for m = 0..n-1, evaluated in long double
+void twiddles(int n, double2 *out) {
+  const long double tp = 6.283185307179586476925286766559005768L;
+  for (int m = 0; m < n; m++) {
+    long double a = tp * (long double)m / (long double)n;
+    out[m] = make_double2((double)cosl(a), -(double)sinl(a));
+  }
+}
+
+template <typename T>
+int dalloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    dg_set_error((std::string("cudaMalloc: ") + cudaGetErrorString(e)).c_str());
+    return e == cudaErrorMemoryAllocation ? DG_ERR_OOM : DG_ERR_CUDA;
+  }
+  return DG_OK;
+}
+
+__global__ void k_ref_to_compact(const double2 *__restrict__ ref, double2 *__restrict__ cmp,
+                                 int nplanes, int nzt, int nkxp, int nxp1, int nz2) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long tot = (long)nplanes * nzt * nkxp;
+  if (q >= tot) return;
+  const int i = (int)(q % nkxp);
+  const int k = (int)((q / nkxp) % nzt);
+  const int j = (int)(q / ((long)nkxp * nzt));
+  cmp[q] = ref[((long)j * nz2 + k) * nxp1 + i];
+}
+
+__global__ void k_compact_to_ref(const double2 *__restrict__ cmp, double2 *__restrict__ ref,
+                                 int nplanes, int nzt, int nkxp, int nxp1, int nz2) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long tot = (long)nplanes * nz2 * nxp1;
+  if (q >= tot) return;
+  const int i = (int)(q % nxp1);
+  const int k = (int)((q / nxp1) % nz2);
+  const int j = (int)(q / ((long)nxp1 * nz2));
+  double2 v = make_double2(0.0, 0.0);
+  if (i < nkxp && k < nzt) v = cmp[((long)j * nzt + k) * nkxp + i];
+  ref[q] = v;
+}
+
+__global__ void k_advance_time(double *dscal) { dscal[0] = dscal[0] + dscal[1]; }
+}  // namespace
+
+void dg_set_error(const char *msg) { g_err = msg ? msg : ""; }
+void dg_count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+extern "C" int dg_version(void) { return 100; }
+extern "C" const char *dg_last_error(void) { return g_err.c_str(); }
+extern "C" int64_t dg_kernel_launches(void) { return (int64_t)g_launches.load(); }
+
+static int validate(const dg_params *p, const double *gy) {
+  if (!p) return DG_ERR_ARG;
+  if (p->num_per_dir != 2 && p->num_per_dir != 3) {
+    dg_set_error("num_per_dir must be 2 (channel) or 3 (periodic)");
+    return DG_ERR_ARG;
+  }
+  if (p->n_th < 0 || p->n_th > DG_MAX_TH) {
+    dg_set_error("n_th out of range");
+    return DG_ERR_ARG;
+  }
+  if (p->nx < 8 || p->nz < 8 || (p->nx & 1) || (p->nz & 1) || p->nx > 4096 || p->nz > 4096) {
+    dg_set_error("NX and NZ must be even, 8..4096");
+    return DG_ERR_DIMS;
+  }
+  FftPlan t;
+  if (!dg_make_plan(p->nx, &t) || !dg_make_plan(p->nz, &t)) {
+    dg_set_error("NX and NZ must factor into 2 and 3");
+    return DG_ERR_DIMS;
+  }
+  if (p->num_per_dir == 2) {
+    if (p->ny < 4 || !gy) {
+      dg_set_error("channel needs NY >= 4 and a GY grid");
+      return DG_ERR_DIMS;
+    }
+    int bcs[6] = {p->u_bc_ymin, p->w_bc_ymin, p->u_bc_ymax, p->w_bc_ymax, p->v_bc_ymin, p->v_bc_ymax};
+    for (int i = 0; i < 4; i++)
+      if (bcs[i] != 0 && bcs[i] != 1) {
+        dg_set_error("Error: U/W_BC_Y* must be 0, or 1");
+        return DG_ERR_ARG;
+      }
+    for (int i = 4; i < 6; i++)
+      if (bcs[i] < 0 || bcs[i] > 2) {
+        dg_set_error("Error: V_BC_Y* must be 0, 1, or 2");
+        return DG_ERR_ARG;
+      }
+    if (p->precision != 0) {
+      dg_set_error("channel mixed precision is not available");
+      return DG_ERR_ARG;
+    }
+  } else {
+    if (!dg_make_plan(p->ny, &t) || p->ny < 8) {
+      dg_set_error("periodic NY must be >= 8 and factor into 2 and 3");
+      return DG_ERR_DIMS;
+    }
+  }
+  return DG_OK;
+}
+
+extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *stream,
+                               dg_handle **out) {
+  if (!out) return DG_ERR_ARG;
+  *out = nullptr;
+  DG_TRY(validate(p, gy));
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    dg_set_error("no CUDA device");
+    return DG_ERR_NODEV;
+  }
+  int dev = 0, major = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  if (major != 10) {
+    dg_set_error("this build targets sm_100a (B200)");
+    return DG_ERR_NODEV;
+  }
+  dg_handle *h = (dg_handle *)calloc(1, sizeof(dg_handle));
+  h->p = *p;
+  h->NX = p->nx; h->NY = p->ny; h->NZ = p->nz; h->NTH = p->n_th;
+  h->NKX = p->nx / 3; h->NKZ = p->nz / 3; h->TNKZ = 2 * h->NKZ;
+  h->NKY = p->ny / 3; h->TNKY = 2 * h->NKY;
+  h->nkxp = h->NKX + 1; h->nkzt = h->TNKZ + 1; h->nkyt = h->TNKY + 1;
+  h->periodic = (p->num_per_dir == 3);
+  h->nplanes = h->periodic ? h->nkyt : h->NY + 2;
+  h->ss = (long)h->nkxp * h->nkzt;
+  h->nspec = h->ss * h->nplanes;
+  h->nf = 3 + h->NTH;
+  h->pi = 4.0 * atan(1.0);
+  h->eps = (double)(float)0.000000001;  // default-real literal, for/fft.f:74
+  // INIT_CHAN_MPI with NPROCY = 1 (for/mpi.f:1080-1100)
+  h->jstart = 2;
+  h->jend = h->NY;
+  for (int n = 0; n < DG_MAX_TH; n++) {
+    h->jend_th[n] = h->NY;
+    h->jstart_th[n] = (n < h->NTH && p->th_bc_ymin[n] == 1) ? 1 : 2;
+  }
+  if (stream) {
+    h->st = (cudaStream_t)stream;
+    h->own_stream = false;
+  } else {
+    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+      free(h);
+      dg_set_error("stream creation failed");
+      return DG_ERR_CUDA;
+    }
+    h->own_stream = true;
+  }
+  *out = h;
+  const int NY = h->NY, L = NY + 2;
+
+  // ---- host tables
+  h->h_gy = (double *)calloc(L, sizeof(double));
+  h->h_gyf = (double *)calloc(L, sizeof(double));
+  h->h_dy = (double *)calloc(L, sizeof(double));
+  h->h_dyf = (double *)calloc(L, sizeof(double));
+  h->h_kx = (double *)calloc(h->nkxp, sizeof(double));
+  h->h_kz = (double *)calloc(h->nkzt, sizeof(double));
+  h->h_ky = (double *)calloc(h->nkyt, sizeof(double));
+  const double pi = h->pi;
+  for (int i = 0; i <= h->NKX; i++) h->h_kx[i] = (double)i * (2.0 * pi) / p->lx;
+  for (int k = 0; k <= h->NKZ; k++) h->h_kz[k] = (double)k * (2.0 * pi) / p->lz;
+  for (int k = 1; k <= h->NKZ; k++) h->h_kz[h->TNKZ + 1 - k] = -((double)k * (2.0 * pi) / p->lz);
+  if (h->periodic) {
+    for (int j = 1; j <= h->NKY; j++) h->h_ky[j] = (double)j * (2.0 * pi) / p->ly;
+    for (int j = 1; j <= h->NKY; j++) h->h_ky[h->TNKY + 1 - j] = -((double)j * (2.0 * pi) / p->ly);
+    for (int j = 0; j <= NY && j < L; j++) h->h_dy[j] = p->ly / NY;
+  } else {
+    // ReadGridHDF5 (for/hdf5.f:676-703) and metrics (for/channel.f:1646-1652)
+    for (int j = 1; j <= NY + 1; j++) h->h_gy[j] = gy[j - 1];
+    for (int j = 1; j <= NY; j++) h->h_gyf[j] = 0.5 * (h->h_gy[j] + h->h_gy[j + 1]);
+    h->h_gyf[0] = 2.0 * h->h_gyf[1] - h->h_gyf[2];
+    h->h_gyf[NY + 1] = 2.0 * h->h_gyf[NY] - h->h_gyf[NY - 1];
+    for (int j = 1; j <= NY + 1; j++) h->h_dy[j] = h->h_gyf[j] - h->h_gyf[j - 1];
+    for (int j = 1; j <= NY; j++) h->h_dyf[j] = h->h_gy[j + 1] - h->h_gy[j];
+    h->h_dyf[NY + 1] = h->h_dyf[NY];
+  }
+
+  // ---- device allocations
+  DG_TRY(dalloc(&h->gyf, L));
+  DG_TRY(dalloc(&h->dy, L));
+  DG_TRY(dalloc(&h->dyf, L));
+  DG_TRY(dalloc(&h->kx, h->nkxp));
+  DG_TRY(dalloc(&h->kz, h->nkzt));
+  DG_TRY(dalloc(&h->ky, h->nkyt));
+  DG_CUDA(cudaMemcpy(h->gyf, h->h_gyf, sizeof(double) * L, cudaMemcpyHostToDevice));
+  DG_CUDA(cudaMemcpy(h->dy, h->h_dy, sizeof(double) * L, cudaMemcpyHostToDevice));
+  DG_CUDA(cudaMemcpy(h->dyf, h->h_dyf, sizeof(double) * L, cudaMemcpyHostToDevice));
+  DG_CUDA(cudaMemcpy(h->kx, h->h_kx, sizeof(double) * h->nkxp, cudaMemcpyHostToDevice));
+  DG_CUDA(cudaMemcpy(h->kz, h->h_kz, sizeof(double) * h->nkzt, cudaMemcpyHostToDevice));
+  DG_CUDA(cudaMemcpy(h->ky, h->h_ky, sizeof(double) * h->nkyt, cudaMemcpyHostToDevice));
+
+  dg_make_plan(h->NX, &h->plx);
+  dg_make_plan(h->NZ, &h->plz);
+  if (h->periodic) dg_make_plan(h->NY, &h->ply);
+  {
+    int nmax = h->NX > h->NZ ? h->NX : h->NZ;
+    if (h->NY > nmax) nmax = h->NY;
+    double2 *tmp = (double2 *)malloc(sizeof(double2) * nmax);
+    DG_TRY(dalloc(&h->twx, h->NX));
+    twiddles(h->NX, tmp);
+    DG_CUDA(cudaMemcpy(h->twx, tmp, sizeof(double2) * h->NX, cudaMemcpyHostToDevice));
+    DG_TRY(dalloc(&h->twz, h->NZ));
+    twiddles(h->NZ, tmp);
+    DG_CUDA(cudaMemcpy(h->twz, tmp, sizeof(double2) * h->NZ, cudaMemcpyHostToDevice));
+    if (h->periodic) {
+      DG_TRY(dalloc(&h->twy, h->NY));
+      twiddles(h->NY, tmp);
+      DG_CUDA(cudaMemcpy(h->twy, tmp, sizeof(double2) * h->NY, cudaMemcpyHostToDevice));
+    }
+    free(tmp);
+  }
+
+  DG_TRY(dalloc(&h->dscal, 16));
+  DG_TRY(dalloc(&h->dmin_bits, 32));
+  DG_TRY(dalloc(&h->dflag, 4));
+  const size_t ns = (size_t)h->nspec;
+  for (int f = 0; f < h->nf; f++) {
+    DG_TRY(dalloc(&h->cu[f], ns));
+    DG_TRY(dalloc(&h->cf[f], ns));
+    DG_TRY(dalloc(&h->rhs[f], ns));
+    DG_CUDA(cudaMemset(h->cu[f], 0, ns * sizeof(double2)));
+    DG_CUDA(cudaMemset(h->cf[f], 0, ns * sizeof(double2)));
+    DG_CUDA(cudaMemset(h->rhs[f], 0, ns * sizeof(double2)));
+  }
+  DG_TRY(dalloc(&h->cp, ns));
+  DG_TRY(dalloc(&h->cr1, ns));
+  DG_CUDA(cudaMemset(h->cp, 0, ns * sizeof(double2)));
+  DG_CUDA(cudaMemset(h->cr1, 0, ns * sizeof(double2)));
+
+  if (!h->periodic) {
+    DG_TRY(dalloc(&h->gphi, ns));
+    DG_TRY(dalloc(&h->rem_a, ns));
+    DG_TRY(dalloc(&h->rem_rb, ns));
+    DG_TRY(dalloc(&h->cn_tab, (size_t)(3 + DG_MAX_TH) * 4 * L));
+    DG_TRY(dalloc(&h->cn_kind, (size_t)(3 + DG_MAX_TH) * L));
+    DG_TRY(dalloc(&h->cn_bc, (size_t)(3 + DG_MAX_TH) * L));
+    const size_t hsz = (size_t)h->nplanes * h->NZ * h->nkxp;
+    DG_TRY(dalloc(&h->H, hsz * h->nf));
+    DG_TRY(dalloc(&h->G, hsz * 2 * h->nf));
+    const size_t phys = (size_t)(NY + 2) * h->NZ * h->NX;
+    h->work_bytes = sizeof(double) * phys * (h->nf > 3 ? h->nf : 3);
+    if (h->work_bytes < sizeof(double) * 8 * L) h->work_bytes = sizeof(double) * 8 * L;
+    DG_TRY(dalloc((double **)&h->work, h->work_bytes / sizeof(double)));
+  } else {
+    DG_TRY(dg_per_init(h));
+  }
+  DG_TRY(diablo_set_time(h, 0.0, p->delta_t));
+  if (!h->periodic) DG_TRY(dg_chan_init(h));
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  return DG_OK;
+}
+
+extern "C" int diablo_gpu_finalize(dg_handle *h) {
+  if (!h) return DG_OK;
+  cudaStreamSynchronize(h->st);
+  void *dp[] = {h->gyf, h->dy, h->dyf, h->kx, h->kz, h->ky, h->kx2, h->kz2, h->ky2, h->twx, h->twz,
+                h->twy, h->dscal, h->cp, h->cr1, h->gphi, h->rem_a, h->rem_rb, h->cn_tab,
+                h->cn_kind, h->cn_bc, h->H, h->G, h->work, h->dmin_bits, h->dflag, h->Hy, h->P,
+                h->Q};
+  for (void *q : dp)
+    if (q) cudaFree(q);
+  for (int f = 0; f < 3 + DG_MAX_TH; f++) {
+    if (h->cu[f]) cudaFree(h->cu[f]);
+    if (h->cf[f]) cudaFree(h->cf[f]);
+    if (h->rhs[f]) cudaFree(h->rhs[f]);
+  }
+  if (h->own_stream) cudaStreamDestroy(h->st);
+  free(h->h_gy); free(h->h_gyf); free(h->h_dy); free(h->h_dyf);
+  free(h->h_kx); free(h->h_kz); free(h->h_ky);
+  free(h);
+  return DG_OK;
+}
+
+extern "C" int diablo_synchronize(dg_handle *h) {
+  if (!h) return DG_ERR_ARG;
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  return DG_OK;
+}
+
+extern "C" int diablo_set_time(dg_handle *h, double time, double delta_t) {
+  if (!h) return DG_ERR_ARG;
+  double s[5] = {time, delta_t, delta_t * (8.0 / 15.0), delta_t * (2.0 / 15.0),
+                 delta_t * (5.0 / 15.0)};
+  DG_CUDA(cudaMemcpyAsync(h->dscal, s, sizeof(s), cudaMemcpyHostToDevice, h->st));
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  return DG_OK;
+}
+
+extern "C" int diablo_get_time(dg_handle *h, double *time, double *delta_t) {
+  if (!h) return DG_ERR_ARG;
+  double s[2];
+  DG_CUDA(cudaMemcpyAsync(s, h->dscal, sizeof(s), cudaMemcpyDeviceToHost, h->st));
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  if (time) *time = s[0];
+  if (delta_t) *delta_t = s[1];
+  return DG_OK;
+}
+
+extern "C" int diablo_advance_time(dg_handle *h) {
+  if (!h) return DG_ERR_ARG;
+  k_advance_time<<<1, 1, 0, h->st>>>(h->dscal);
+  DG_LAUNCHED();
+  return DG_OK;
+}
+
+static double2 *field_ptr(dg_handle *h, int id) {
+  if (id >= DG_CFTH && id < DG_CFTH + h->NTH) return h->cf[3 + id - DG_CFTH];
+  if (id >= DG_CTH && id < DG_CTH + h->NTH) return h->cu[3 + id - DG_CTH];
+  switch (id) {
+    case DG_CU1: return h->cu[0];
+    case DG_CU2: return h->cu[1];
+    case DG_CU3: return h->cu[2];
+    case DG_CP: return h->cp;
+    case DG_CF1: return h->cf[0];
+    case DG_CF2: return h->cf[1];
+    case DG_CF3: return h->cf[2];
+    case DG_CR1: return h->cr1;
+    default: return nullptr;
+  }
+}
+
+// reference layout sizes: (NX/2+1) x (NZ+2) x planes complex
+static void ref_dims(const dg_handle *h, int *nxp1, int *nz2) {
+  *nxp1 = h->NX / 2 + 1;
+  *nz2 = h->NZ + 2;
+}
+
+extern "C" int diablo_set_field(dg_handle *h, int field, const double *src, int layout, int where) {
+  if (!h || !src) return DG_ERR_ARG;
+  double2 *dst = field_ptr(h, field);
+  if (!dst) return DG_ERR_ARG;
+  const size_t nc = (size_t)h->nspec;
+  if (layout == DG_LAYOUT_COMPACT) {
+    DG_CUDA(cudaMemcpyAsync(dst, src, nc * sizeof(double2),
+                            where == DG_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                            h->st));
+  } else {
+    int nxp1, nz2;
+    ref_dims(h, &nxp1, &nz2);
+    const size_t nr = (size_t)h->nplanes * nz2 * nxp1;
+    const double2 *dref = (const double2 *)src;
+    double2 *tmp = nullptr;
+    if (where == DG_HOST) {
+      DG_CUDA(cudaMallocAsync((void **)&tmp, nr * sizeof(double2), h->st));
+      DG_CUDA(cudaMemcpyAsync(tmp, src, nr * sizeof(double2), cudaMemcpyHostToDevice, h->st));
+      dref = tmp;
+    }
+    k_ref_to_compact<<<dg_cdiv(nc, 256), 256, 0, h->st>>>(dref, dst, h->nplanes, h->nkzt, h->nkxp,
+                                                         nxp1, nz2);
+    DG_LAUNCHED();
+    if (tmp) DG_CUDA(cudaFreeAsync(tmp, h->st));
+  }
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  return DG_OK;
+}
+
+extern "C" int diablo_get_field(dg_handle *h, int field, double *dst, int layout, int where) {
+  if (!h || !dst) return DG_ERR_ARG;
+  double2 *src = field_ptr(h, field);
+  if (!src) return DG_ERR_ARG;
+  const size_t nc = (size_t)h->nspec;
+  if (layout == DG_LAYOUT_COMPACT) {
+    DG_CUDA(cudaMemcpyAsync(dst, src, nc * sizeof(double2),
+                            where == DG_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                            h->st));
+  } else {
+    int nxp1, nz2;
+    ref_dims(h, &nxp1, &nz2);
+    const size_t nr = (size_t)h->nplanes * nz2 * nxp1;
+    double2 *dref = (double2 *)dst;
+    double2 *tmp = nullptr;
+    if (where == DG_HOST) {
+      DG_CUDA(cudaMallocAsync((void **)&tmp, nr * sizeof(double2), h->st));
+      dref = tmp;
+    }
+    k_compact_to_ref<<<dg_cdiv(nr, 256), 256, 0, h->st>>>(src, dref, h->nplanes, h->nkzt, h->nkxp,
+                                                         nxp1, nz2);
+    DG_LAUNCHED();
+    if (tmp) {
+      DG_CUDA(cudaMemcpyAsync(dst, tmp, nr * sizeof(double2), cudaMemcpyDeviceToHost, h->st));
+      DG_CUDA(cudaFreeAsync(tmp, h->st));
+    }
+  }
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  return DG_OK;
+}
+
+extern "C" int diablo_stats(dg_handle *h, dg_stats *s) {
+  if (!h || !s) return DG_ERR_ARG;
+  return dg_stats_dev(h, s);
+}

@@ -1,0 +1,257 @@
+"""Host-side mirror of the reference's stepper interface.
+
+``Channel`` and ``Periodic`` wrap one device handle and expose the
+reference's subroutines under their own names (``rk_chan_1``,
+``rem_div_chan``, ``fft_xz_to_fourier`` ...), with the same argument meaning,
+so a driver loop reads like ``for/diablo.f:66-120``::
+
+    for time_step in range(1, n + 1):
+        for rk_step in (1, 2, 3):
+            ch.rk_chan_1(time_step, rk_step)
+        ch.advance_time()          # TIME = TIME + DELTA_T
+
+Errors raise ``DiabloError`` (the reference would ``STOP``).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .grid import grid_metrics
+from .params import DgParams, Params
+
+__all__ = ["Channel", "Periodic", "DiabloError"]
+
+DiabloError = _lib.DiabloError
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class _Solver:
+    def __init__(self, p: Params, gy=None, stream=None):
+        self.L = _lib.load()
+        self.p = p
+        self._dp = p.to_struct(DgParams)
+        self._gy = None if gy is None else np.ascontiguousarray(gy, dtype=np.float64)
+        h = ctypes.c_void_p()
+        code = self.L.diablo_gpu_init(ctypes.byref(self._dp),
+                                      None if self._gy is None else _ptr(self._gy),
+                                      None if stream is None else ctypes.c_void_p(stream),
+                                      ctypes.byref(h))
+        _lib.check("diablo_gpu_init", code)
+        self.h = h
+        self.spec_shape = p.spec_shape()
+        self.phys_shape = p.phys_shape()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.diablo_gpu_finalize(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _call(self, name, *args):
+        _lib.check(name, getattr(self.L, name)(self.h, *args))
+
+    # ---- state I/O
+    def set_field(self, name: str, arr: np.ndarray, layout: str = "compact"):
+        a = np.ascontiguousarray(arr, dtype=np.complex128)
+        lay = _lib.DG_LAYOUT_REFERENCE if layout == "reference" else _lib.DG_LAYOUT_COMPACT
+        if lay == _lib.DG_LAYOUT_COMPACT and a.size != int(np.prod(self.spec_shape)):
+            raise ValueError(f"{name}: expected {self.spec_shape}, got {a.shape}")
+        self._call("diablo_set_field", _lib.field_id(name), _ptr(a), lay, _lib.DG_HOST)
+
+    def get_field(self, name: str, layout: str = "compact") -> np.ndarray:
+        if layout == "reference":
+            shp = (self.spec_shape[0], self.p.nz + 2, self.p.nx // 2 + 1)
+            lay = _lib.DG_LAYOUT_REFERENCE
+        else:
+            shp = self.spec_shape
+            lay = _lib.DG_LAYOUT_COMPACT
+        out = np.zeros(shp, dtype=np.complex128)
+        self._call("diablo_get_field", _lib.field_id(name), _ptr(out), lay, _lib.DG_HOST)
+        return out
+
+    def set_field_device(self, name: str, dev_ptr: int):
+        """Copy a compact-layout complex128 field from device memory."""
+        self._call("diablo_set_field", _lib.field_id(name), ctypes.c_void_p(dev_ptr),
+                   _lib.DG_LAYOUT_COMPACT, _lib.DG_DEVICE)
+
+    def get_field_device(self, name: str, dev_ptr: int):
+        self._call("diablo_get_field", _lib.field_id(name), ctypes.c_void_p(dev_ptr),
+                   _lib.DG_LAYOUT_COMPACT, _lib.DG_DEVICE)
+
+    def state_names(self):
+        n = ["CU1", "CU2", "CU3", "CP", "CF1", "CF2", "CF3"]
+        n += [f"CTH{k}" for k in range(self.p.n_th)] + [f"CFTH{k}" for k in range(self.p.n_th)]
+        return n
+
+    def get_state(self) -> dict:
+        return {k: self.get_field(k) for k in self.state_names()}
+
+    def set_state(self, st: dict):
+        for k, v in st.items():
+            self.set_field(k, v)
+
+    def set_time(self, time: float, delta_t: float):
+        self._call("diablo_set_time", ctypes.c_double(time), ctypes.c_double(delta_t))
+
+    def get_time(self):
+        t, d = ctypes.c_double(), ctypes.c_double()
+        self._call("diablo_get_time", ctypes.byref(t), ctypes.byref(d))
+        return t.value, d.value
+
+    def advance_time(self):
+        self._call("diablo_advance_time")
+
+    def synchronize(self):
+        self._call("diablo_synchronize")
+
+    def stats(self) -> dict:
+        s = _lib.DgStats()
+        self._call("diablo_stats", ctypes.byref(s))
+        d = {k: getattr(s, k) for k in ("ubulk", "urms_b", "vrms_b", "wrms_b", "ke", "div_max")}
+        d["thrms_b"] = list(s.thrms_b)[: self.p.n_th]
+        d["th_var"] = list(s.th_var)[: self.p.n_th]
+        return d
+
+
+class Channel(_Solver):
+    """Device-resident channel state driven through RK_CHAN_1 and helpers."""
+
+    def __init__(self, p: Params, gy, stream=None):
+        if p.num_per_dir != 2:
+            raise ValueError("Channel needs num_per_dir = 2")
+        super().__init__(p, gy, stream)
+        self.GY, self.GYF, self.DY, self.DYF = grid_metrics(gy)
+
+    # ---- the reference's subroutines
+    def rk_chan_1(self, time_step: int, rk_step: int):
+        self._call("diablo_rk_chan_1", time_step, rk_step)
+
+    def rem_div_chan(self):
+        self._call("diablo_rem_div_chan")
+
+    def poisson_p_chan(self):
+        self._call("diablo_poisson_p_chan")
+
+    def apply_bc_vel(self):
+        self._call("diablo_apply_bc_vel")
+
+    def courant(self):
+        self._call("diablo_courant")
+
+    def step(self, time_step: int):
+        for rk in (1, 2, 3):
+            self.rk_chan_1(time_step, rk)
+        self.advance_time()
+
+    # ---- transforms on reference-layout host arrays
+    def _ref_phys(self, v):
+        shp = (self.p.ny + 2, self.p.nz + 2, self.p.nx + 2)
+        return np.ascontiguousarray(v, dtype=np.float64).reshape(shp)
+
+    def fft_xz_to_fourier(self, V: np.ndarray, VV: np.ndarray | None = None, jmin=0, jmax=None):
+        """FFT_XZ_TO_FOURIER(V, VV, JMIN, JMAX) on reference-layout host arrays.
+        V: (NY+2, NZ+2, NX+2) float64; returns VV (NY+2, NZ+2, NX/2+1) complex128."""
+        jmax = self.p.ny + 1 if jmax is None else jmax
+        V = self._ref_phys(V)
+        if VV is None:
+            VV = np.zeros((self.p.ny + 2, self.p.nz + 2, self.p.nx // 2 + 1), dtype=np.complex128)
+        self._call("diablo_fft_xz_to_fourier", _ptr(V), _ptr(VV), jmin, jmax, _lib.DG_HOST)
+        return VV
+
+    def fft_xz_to_physical(self, VV: np.ndarray, V: np.ndarray | None = None, jmin=0, jmax=None):
+        jmax = self.p.ny + 1 if jmax is None else jmax
+        VV = np.ascontiguousarray(VV, dtype=np.complex128)
+        if V is None:
+            V = np.zeros((self.p.ny + 2, self.p.nz + 2, self.p.nx + 2), dtype=np.float64)
+        self._call("diablo_fft_xz_to_physical", _ptr(VV), _ptr(V), jmin, jmax, _lib.DG_HOST)
+        return V
+
+    # ---- initial condition (CREATE_FLOW_CHAN tail, for/set_ics.f:109-182)
+    def create_flow(self, u1, u2, u3, th=None):
+        """Physical fields [NY+2][NZ][NX] -> spectral state: FFT, APPLY_BC_VEL,
+        REM_DIV_CHAN, APPLY_BC_VEL (the SAVE_STATS_CHAN side effect)."""
+        names = [("CU1", u1), ("CU2", u2), ("CU3", u3)]
+        if th is not None:
+            names += [(f"CTH{n}", th[n]) for n in range(self.p.n_th)]
+        zero = np.zeros(self.spec_shape, dtype=np.complex128)
+        for nm in ["CP", "CF1", "CF2", "CF3"] + [f"CFTH{n}" for n in range(self.p.n_th)]:
+            self.set_field(nm, zero)
+        for nm, a in names:
+            self.set_field(nm, self.to_fourier(a))
+        self.apply_bc_vel()
+        self.rem_div_chan()
+        self.apply_bc_vel()
+
+    def to_fourier(self, phys: np.ndarray) -> np.ndarray:
+        """Compact physical [NY+2][NZ][NX] -> compact spectral, via FFT_XZ_TO_FOURIER."""
+        p = self.p
+        V = np.zeros((p.ny + 2, p.nz + 2, p.nx + 2))
+        V[:, : p.nz, : p.nx] = phys
+        VV = self.fft_xz_to_fourier(V)
+        return np.ascontiguousarray(VV[:, : p.tnkz + 1, : p.nkx + 1])
+
+    def to_physical(self, spec: np.ndarray) -> np.ndarray:
+        p = self.p
+        VV = np.zeros((p.ny + 2, p.nz + 2, p.nx // 2 + 1), dtype=np.complex128)
+        VV[:, : p.tnkz + 1, : p.nkx + 1] = spec
+        V = self.fft_xz_to_physical(VV)
+        return np.ascontiguousarray(V[:, : p.nz, : p.nx])
+
+
+class Periodic(_Solver):
+    """Device-resident triply periodic state driven through RK_PER_1."""
+
+    def __init__(self, p: Params, stream=None):
+        if p.num_per_dir != 3:
+            raise ValueError("Periodic needs num_per_dir = 3")
+        super().__init__(p, None, stream)
+
+    def rk_per_1(self, rk_step: int):
+        self._call("diablo_rk_per_1", rk_step)
+
+    def rem_div_per(self):
+        self._call("diablo_rem_div_per")
+
+    def poisson_p_per(self):
+        self._call("diablo_poisson_p_per")
+
+    def step(self, time_step: int = 0):
+        for rk in (1, 2, 3):
+            self.rk_per_1(rk)
+        self.advance_time()
+
+
+def thomas_real(a, b, c, g, ny: int, nx: int):
+    """THOMAS_REAL(A,B,C,G,NY,NX) on host arrays shaped (NY+1, NX+1); returns
+    (A, B, G) as modified by the reference routine."""
+    L = _lib.load()
+    arrs = [np.ascontiguousarray(x, dtype=np.float64).copy() for x in (a, b, c, g)]
+    _lib.check("diablo_thomas_real",
+               L.diablo_thomas_real(*[_ptr(x) for x in arrs], ny, nx, _lib.DG_HOST))
+    return arrs[0], arrs[1], arrs[3]
+
+
+def thomas_complex(a, b, c, g, ny: int, nx: int):
+    L = _lib.load()
+    arrs = [np.ascontiguousarray(x, dtype=np.float64).copy() for x in (a, b, c)]
+    gg = np.ascontiguousarray(g, dtype=np.complex128).copy()
+    _lib.check("diablo_thomas_complex",
+               L.diablo_thomas_complex(*[_ptr(x) for x in arrs], _ptr(gg), ny, nx, _lib.DG_HOST))
+    return arrs[0], arrs[1], gg

@@ -1,0 +1,166 @@
+/*
+ * diablo_b200 -- C-ABI of the B200 (sm_100a) replacement for DIABLO's
+ * RK3 / Crank-Nicolson hot path.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status
+ * (DG_OK = 0) and never aborts the caller.  A Fortran host binds them with
+ * ISO_C_BINDING; the Python mirror in
+ * diablo_b200/_lib.py binds them with ctypes.
+ *
+ * Ownership: the caller's arrays (the reference's COMMON blocks) stay the
+ * owner of record on the host; the library keeps device-resident mirrors
+ * across substeps and copies only in diablo_set_field / diablo_get_field
+ * and in the FFT_XZ / Thomas entry points called on host arrays.
+ *
+ * Array layouts accepted (DG_LAYOUT_*):
+ *   REFERENCE : the reference's own arrays, first index fastest:
+ *               spectral  COMPLEX*16 CU(0:NX/2, 0:NZ+1, 0:NY+1)
+ *               physical  REAL*8     U (0:NX+1, 0:NZ+1, 0:NY+1)
+ *               (for/header:214-245 with NPROCY = NPROCZ = 1)
+ *   COMPACT   : retained modes only, [NY+2][TNKZ+1][NKX+1] complex (channel)
+ *               or [TNKY+1][TNKZ+1][NKX+1] (periodic); physical [NY+2][NZ][NX]
+ *               or [NY][NZ][NX].
+ * Complex values are interleaved (re, im) doubles.
+ */
+#ifndef DIABLO_B200_H
+#define DIABLO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DG_MAX_TH 4
+
+enum dg_status {
+  DG_OK = 0,
+  DG_ERR_ARG = 1,      /* bad argument / unsupported option */
+  DG_ERR_DIMS = 2,     /* grid sizes not supported (the reference STOPs) */
+  DG_ERR_OOM = 3,      /* device allocation failed */
+  DG_ERR_CUDA = 4,     /* CUDA runtime error (message via dg_last_error) */
+  DG_ERR_NAN = 5,      /* non-finite value detected in the state */
+  DG_ERR_TIMEOUT = 6,  /* a bounded device wait gave up */
+  DG_ERR_NODEV = 7     /* no usable sm_100 device */
+};
+
+enum { DG_HOST = 0, DG_DEVICE = 1 };
+enum { DG_LAYOUT_COMPACT = 0, DG_LAYOUT_REFERENCE = 1 };
+
+/* field ids for diablo_set_field / diablo_get_field */
+enum {
+  DG_CU1 = 0, DG_CU2 = 1, DG_CU3 = 2, DG_CP = 3,
+  DG_CF1 = 4, DG_CF2 = 5, DG_CF3 = 6,
+  DG_CR1 = 7,               /* phi left by REM_DIV_CHAN (for/channel.f:1189) */
+  DG_CTH = 16,              /* + scalar index n (0-based) */
+  DG_CFTH = 32              /* + scalar index n */
+};
+
+/* What the reference holds in COMMON /INPUT/ and friends (for/header:83-302)
+ * plus grid_def's NX, NY, NZ, N_TH.  Field order is ABI. */
+typedef struct dg_params {
+  int32_t nx, ny, nz, n_th;
+  int32_t num_per_dir;        /* 2 = channel (RK_CHAN_1), 3 = periodic (RK_PER_1) */
+  int32_t precision;          /* 0 = FP64 throughout, 1 = mixed (FP32 FFT/products) */
+  double nu, beta, lx, ly, lz, nu_v_scale;
+  double delta_t, cfl;
+  int32_t variable_dt, update_dt;
+  double i_ro, grav_x, grav_y, grav_z;
+  int32_t f_type, pad0;
+  double ubulk0, px0, omega0, amp_omega0;
+  int32_t u_bc_ymin, v_bc_ymin, w_bc_ymin, u_bc_ymax, v_bc_ymax, w_bc_ymax;
+  double u_bc_ymin_c1, v_bc_ymin_c1, w_bc_ymin_c1;
+  double u_bc_ymax_c1, v_bc_ymax_c1, w_bc_ymax_c1;
+  int32_t th_bc_ymin[DG_MAX_TH], th_bc_ymax[DG_MAX_TH];
+  double th_bc_ymin_c1[DG_MAX_TH], th_bc_ymax_c1[DG_MAX_TH];
+  double ri[DG_MAX_TH], pr[DG_MAX_TH], drhodx[DG_MAX_TH], drhodz[DG_MAX_TH];
+  int32_t background_grad[DG_MAX_TH];
+  double epsilon_target;
+} dg_params;
+
+/* Parity statistics (SAVE_STATS_CHAN, for/save_stats.f:112-203,470-489). */
+typedef struct dg_stats {
+  double ubulk, urms_b, vrms_b, wrms_b, ke, div_max;
+  double thrms_b[DG_MAX_TH], th_var[DG_MAX_TH];
+} dg_stats;
+
+typedef struct dg_handle dg_handle;
+
+/* ---------------------------------------------------------------- misc */
+int dg_version(void);
+const char *dg_last_error(void);
+/* Kernels launched by this library since load (for launch accounting). */
+int64_t dg_kernel_launches(void);
+
+/* -------------------------------------------------------------- lifecycle
+ * Replaces the device-side parts of INITIALIZE: INIT_FFT (for/fft.f:55-147),
+ * CREATE_GRID_CHAN's metrics (for/channel.f:1645-1652 via
+ * for/hdf5.f:676-703), INIT_CHAN_MPI's JSTART/JEND (for/mpi.f:1067-1135) and
+ * the RK3 coefficients (for/diablo_io.f:116-124).
+ * gy: GY(1..NY+1) (NY+1 doubles) for the channel, NULL for periodic.
+ * stream: a cudaStream_t to run on, or NULL for a library-owned stream. */
+int diablo_gpu_init(const dg_params *p, const double *gy, void *stream, dg_handle **out);
+int diablo_gpu_finalize(dg_handle *h);
+int diablo_synchronize(dg_handle *h);
+
+/* COMMON /RUNTIME_VARS/ TIME and DELTA_T (device-resident; COURANT updates
+ * DELTA_T on the device). */
+int diablo_set_time(dg_handle *h, double time, double delta_t);
+int diablo_get_time(dg_handle *h, double *time, double *delta_t);
+/* TIME = TIME + DELTA_T on the device (for/diablo.f:109). */
+int diablo_advance_time(dg_handle *h);
+
+/* Host <-> device copies of one spectral field (ids above). */
+int diablo_set_field(dg_handle *h, int field, const double *src, int layout, int where);
+int diablo_get_field(dg_handle *h, int field, double *dst, int layout, int where);
+
+/* ------------------------------------------------------- channel hot path */
+/* SUBROUTINE RK_CHAN_1 (for/channel.f:62-1073): one RK3 substep on the
+ * device-resident state.  time_step/rk_step are COMMON /RUNTIME_VARS/. */
+int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step);
+/* SUBROUTINE REM_DIV_CHAN (for/channel.f:1103-1214): projects CU1..3, leaves
+ * phi in CR1. */
+int diablo_rem_div_chan(dg_handle *h);
+/* SUBROUTINE POISSON_P_CHAN (for/channel.f:1217-1453): CP from CU1..3, CTH. */
+int diablo_poisson_p_chan(dg_handle *h);
+/* APPLY_BC_VEL_MPI = APPLY_BC_VEL_LOWER + _UPPER (for/channel.f:2285-2492). */
+int diablo_apply_bc_vel(dg_handle *h);
+/* SUBROUTINE COURANT (for/courant.f:1-65) evaluated on the physical velocity
+ * of the current spectral state; updates DELTA_T and H_BAR on the device. */
+int diablo_courant(dg_handle *h);
+
+/* FFT_XZ_TO_FOURIER(V,VV,JMIN,JMAX) (for/mpi.f:1530-1611) and
+ * FFT_XZ_TO_PHYSICAL(VV,V,JMIN,JMAX) (for/mpi.f:1613-1674), REFERENCE layout.
+ * V and VV may alias (the reference passes EQUIVALENCEd arrays).
+ * where = DG_HOST or DG_DEVICE for both pointers. */
+int diablo_fft_xz_to_fourier(dg_handle *h, const double *V, double *VV, int jmin, int jmax,
+                             int where);
+int diablo_fft_xz_to_physical(dg_handle *h, const double *VV, double *V, int jmin, int jmax,
+                              int where);
+
+/* THOMAS_REAL(A,B,C,G,NY,NX) (for/channel.f:2653-2684) and
+ * THOMAS_COMPLEX(A,B,C,G,NY,NX) (for/channel.f:2687-2720): NX+1 independent
+ * systems of NY+1 rows, arrays (0:NX,0:NY) first index fastest; A and B are
+ * destroyed, the solution is returned in G (complex interleaved for
+ * THOMAS_COMPLEX).  where = DG_HOST or DG_DEVICE. */
+int diablo_thomas_real(double *A, double *B, double *C, double *G, int ny, int nx, int where);
+int diablo_thomas_complex(double *A, double *B, double *C, double *G, int ny, int nx,
+                          int where);
+
+/* ------------------------------------------------------ periodic hot path */
+/* SUBROUTINE RK_PER_1 (for/periodic.f:23-285). */
+int diablo_rk_per_1(dg_handle *h, int rk_step);
+/* SUBROUTINE REM_DIV_PER (for/periodic.f:299-326). */
+int diablo_rem_div_per(dg_handle *h);
+/* SUBROUTINE POISSON_P_PER (for/periodic.f:329-393). */
+int diablo_poisson_p_per(dg_handle *h);
+
+/* ------------------------------------------------------------ statistics */
+/* Parity statistics of the current state (channel or periodic); also checks
+ * the state for non-finite values (returns DG_ERR_NAN if any). */
+int diablo_stats(dg_handle *h, dg_stats *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,7 +1,7 @@
 // Channel substep kernels (RK_CHAN_1, for/channel.f:62-1073) on the
 // retained-mode layout [j][kz][kx].
 //
-// One substep is five launches:
+// One substep is five launches (six when COURANT runs):
 //   zinv        spectral U1..U3, TH -> half-physical H (z inverse per kx)
 //   k_xrow_nl   per physical z-row, marching up in y: x c2r of every field,
 //               all products/fluxes of for/channel.f:409-571,665-720, x r2c,
@@ -11,13 +11,14 @@
 //               terms -> CF (new), and the Crank-Nicolson right-hand side
 //               R = CU + zeta h CF_old - h grad P + beta h CF_new
 //                   + (nu h / 2) d2/dy2 CU           (for/channel.f:88-626)
-//   k_cn_solve  per (mode, field): tridiagonal CN solve in Fourier space
+//   k_cn_col    per (mode tile, field): tridiagonal CN solve in Fourier space
 //               (the reference solves the same x-z independent operator per
 //               physical column, for/channel.f:767-1029; the operator is linear
 //               and identical for every column, so it commutes with the FFT)
-//   k_remdiv    per mode: REM_DIV_CHAN's complex tridiagonal, projection and
-//               CP += phi / h (for/channel.f:1103-1214, 1059-1065)
+//   k_rd_col    per mode tile: REM_DIV_CHAN's complex tridiagonal, projection
+//               and CP += phi / h (for/channel.f:1103-1214, 1059-1065)
 #include <math.h>
+#include <string.h>
 #include "dg_internal.cuh"
 #include "fft.cuh"
 
@@ -26,7 +27,6 @@ using namespace dgfft;
 namespace {
 
 constexpr int XR_ROWS = 2;     // physical z-rows per CTA in k_xrow_nl
-constexpr int ZF_KXG = 4;      // kx columns per CTA in k_zfwd_rhs
 
 struct ChanConst {
   int NX, NY, NZ, NKX, NKZ, nkxp, nkzt, nf, nth;
@@ -63,21 +63,25 @@ ChanConst make_const(const dg_handle *h) {
 // The y-flux terms of for/channel.f:511-571,704-720 are differences of these
 // fluxes between neighbouring planes; they are differenced after the x
 // transform (linearity), so each flux is transformed once.
-__global__ void __launch_bounds__(256) k_xrow_nl(
+constexpr int XR_THR = 128;
+
+template <int NT>
+__global__ void __launch_bounds__(XR_THR) k_xrow_nl(
     ChanConst C, const double2 *__restrict__ H, long Hfield, int chunk, FftPlan pl,
     const double2 *__restrict__ tw, const double *__restrict__ dyf, const double *__restrict__ dy,
     const double *__restrict__ kxv, double2 *__restrict__ G, long Gfield) {
   extern __shared__ double2 sm[];
-  const int NX = C.NX, nkxp = C.nkxp, nf = C.nf, nth = C.nth;
+  const int NX = NT ? NT : C.NX;
+  const int nkxp = C.nkxp, nf = C.nf, nth = C.nth;
   const int npin = (nf + 1) / 2;            // c2r signals per row
   const int nprod = 8 + 3 * nth;
   const int npp = (nprod + 1) / 2;          // r2c signals per row
   const int maxp = npin > npp ? npin : npp;
-  const int sstr = NX + 1;
+  const int sstr = padded_len(NX);
   double2 *stw = sm;
   double2 *b0 = stw + NX;
   double2 *b1 = b0 + XR_ROWS * maxp * sstr;
-  double2 *prev = b1 + XR_ROWS * maxp * sstr;               // [row][3+nth][nkxp]
+  double2 *prev = b0 + fft_bufs(NX) * XR_ROWS * maxp * sstr;  // [row][3+nth][nkxp]
   double *ring = (double *)(prev + XR_ROWS * (3 + nth) * nkxp);  // [3][row][nf][NX]
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int z0 = blockIdx.x * XR_ROWS;
@@ -113,15 +117,15 @@ __global__ void __launch_bounds__(256) k_xrow_nl(
         if (kk == 0) { a.y = 0.0; b.y = 0.0; }
         v = (k == kk) ? make_double2(a.x - b.y, a.y + b.x) : make_double2(a.x + b.y, -a.y + b.x);
       }
-      b0[(r * maxp + q) * sstr + k] = v;
+      b0[(r * npin + q) * sstr + pad(k)] = v;
     }
     __syncthreads();
-    double2 *res = run(b0, b1, pl, XR_ROWS * maxp, sstr, stw, +1);
+    double2 *res = fft<NT>(b0, b1, pl, XR_ROWS * npin, sstr, stw, +1);
     for (int idx = tid; idx < XR_ROWS * npin * NX; idx += nthr) {
       const int x = idx % NX;
       const int q = (idx / NX) % npin;
       const int r = idx / (NX * npin);
-      const double2 v = res[(r * maxp + q) * sstr + x];
+      const double2 v = res[(r * npin + q) * sstr + pad(x)];
       ringp(plane, r, 2 * q)[x] = v.x;
       if (2 * q + 1 < nf) ringp(plane, r, 2 * q + 1)[x] = v.y;
     }
@@ -140,39 +144,38 @@ __global__ void __launch_bounds__(256) k_xrow_nl(
       const int x = idx % NX;
       const int q = (idx / NX) % npp;
       const int r = idx / (NX * npp);
+      const double *U1c = ringp(j, r, 0), *U2c = ringp(j, r, 1), *U3c = ringp(j, r, 2);
+      const double *U1p = ringp(j + 1, r, 0), *U2p = ringp(j + 1, r, 1), *U3p = ringp(j + 1, r, 2);
+      const double *U1m = ringp(j - 1, r, 0), *U3m = ringp(j - 1, r, 2);
       double pv[2];
 #pragma unroll
       for (int h2 = 0; h2 < 2; h2++) {
         const int p = 2 * q + h2;
         double v = 0.0;
-        if (p < nprod) {
-          const double *U1c = ringp(j, r, 0), *U2c = ringp(j, r, 1), *U3c = ringp(j, r, 2);
-          const double *U1p = ringp(j + 1, r, 0), *U2p = ringp(j + 1, r, 1), *U3p = ringp(j + 1, r, 2);
-          const double *U1m = ringp(j - 1, r, 0), *U3m = ringp(j - 1, r, 2);
-          switch (p) {
-            case 0: v = U3c[x] * U1c[x]; break;
-            case 1: v = U1c[x] * U1c[x]; break;
-            case 2: v = U3c[x] * U3c[x]; break;
-            case 3: { double s = U2c[x] + U2p[x]; v = 0.25 * (s * s); } break;
-            case 4: v = (U1p[x] + U1c[x]) * U2p[x]; break;
-            case 5: v = (U3p[x] + U3c[x]) * U2p[x]; break;
-            case 6: v = ((dyfj * U1c[x] + dyfm * U1m[x]) / (2. * dyj)) * U2c[x]; break;
-            case 7: v = ((dyfj * U3c[x] + dyfm * U3m[x]) / (2. * dyj)) * U2c[x]; break;
-            default: {
+        switch (p) {
+          case 0: v = U3c[x] * U1c[x]; break;
+          case 1: v = U1c[x] * U1c[x]; break;
+          case 2: v = U3c[x] * U3c[x]; break;
+          case 3: { double s = U2c[x] + U2p[x]; v = 0.25 * (s * s); } break;
+          case 4: v = (U1p[x] + U1c[x]) * U2p[x]; break;
+          case 5: v = (U3p[x] + U3c[x]) * U2p[x]; break;
+          case 6: v = ((dyfj * U1c[x] + dyfm * U1m[x]) / (2. * dyj)) * U2c[x]; break;
+          case 7: v = ((dyfj * U3c[x] + dyfm * U3m[x]) / (2. * dyj)) * U2c[x]; break;
+          default:
+            if (p < nprod) {
               const int n = (p - 8) / 3, w = (p - 8) % 3;
               const double *Tc = ringp(j, r, 3 + n), *Tp = ringp(j + 1, r, 3 + n);
               if (w == 0) v = Tc[x] * U1c[x];
               else if (w == 1) v = Tc[x] * U3c[x];
               else v = (Tp[x] + Tc[x]) * U2p[x];
             }
-          }
         }
         pv[h2] = v;
       }
-      b0[(r * maxp + q) * sstr + x] = make_double2(pv[0], pv[1]);
+      b0[(r * npp + q) * sstr + pad(x)] = make_double2(pv[0], pv[1]);
     }
     __syncthreads();
-    double2 *res = run(b0, b1, pl, XR_ROWS * maxp, sstr, stw, -1);
+    double2 *res = fft<NT>(b0, b1, pl, XR_ROWS * npp, sstr, stw, -1);
     // separate, scale by 1/NX, combine, write
     const double rnx = (double)NX;
     const bool out = (j >= j0);
@@ -183,8 +186,8 @@ __global__ void __launch_bounds__(256) k_xrow_nl(
       if (z >= NZ) continue;
       auto X = [&](int p) -> double2 {
         const int q = p >> 1;
-        const double2 zk = res[(r * maxp + q) * sstr + k];
-        const double2 zm = res[(r * maxp + q) * sstr + ((NX - k) % NX)];
+        const double2 zk = res[(r * npp + q) * sstr + pad(k)];
+        const double2 zm = res[(r * npp + q) * sstr + pad((NX - k) % NX)];
         double2 v;
         if ((p & 1) == 0) v = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
         else v = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
@@ -232,24 +235,31 @@ size_t xrow_smem(const dg_handle *h) {
   const int nf = h->nf, nth = h->NTH, NX = h->NX;
   const int npin = (nf + 1) / 2, npp = (8 + 3 * nth + 1) / 2;
   const int maxp = npin > npp ? npin : npp;
-  return sizeof(double2) * (NX + 2 * XR_ROWS * maxp * (NX + 1) + XR_ROWS * (3 + nth) * h->nkxp) +
+  return sizeof(double2) * (NX + fft_bufs(NX) * XR_ROWS * maxp * padded_len(NX) +
+                            XR_ROWS * (3 + nth) * h->nkxp) +
          sizeof(double) * 3 * XR_ROWS * nf * NX;
 }
 
 // ------------------------------------------------------------- zfwd + rhs
-__global__ void __launch_bounds__(256) k_zfwd_rhs(
+constexpr int ZF_THR = 128;
+__host__ __device__ constexpr int zf_kxg(int nz) { return nz <= 128 ? 8 : (nz <= 256 ? 4 : 2); }
+
+template <int NT>
+__global__ void __launch_bounds__(ZF_THR) k_zfwd_rhs(
     ChanConst C, const double2 *__restrict__ G, long Gfield, FftPlan pl,
     const double2 *__restrict__ tw, const double *__restrict__ dscal, int rk_step,
     const double *__restrict__ kxv, const double *__restrict__ kzv, const double *__restrict__ dy,
     const double *__restrict__ dyf, FieldPtrs cu, FieldPtrs cf, FieldPtrs rhs,
     const double2 *__restrict__ cp) {
   extern __shared__ double2 sm[];
-  const int NZ = C.NZ, nkxp = C.nkxp, nkzt = C.nkzt, nf = C.nf, NKZ = C.NKZ;
-  const int sstr = NZ + 1;
+  const int NZ = NT ? NT : C.NZ;
+  const int nkxp = C.nkxp, nkzt = C.nkzt, nf = C.nf, NKZ = C.NKZ;
+  const int ZF_KXG = zf_kxg(NZ);
+  const int sstr = padded_len(NZ);
   double2 *stw = sm;
   double2 *b0 = stw + NZ;
   double2 *b1 = b0 + 2 * ZF_KXG * sstr;
-  double2 *nl = b1 + 2 * ZF_KXG * sstr;  // [f][c][kp]
+  double2 *nl = b0 + fft_bufs(NZ) * 2 * ZF_KXG * sstr;  // [f][c][kp]
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int kx0 = blockIdx.x * ZF_KXG;
   const int j = 1 + blockIdx.y;
@@ -264,15 +274,15 @@ __global__ void __launch_bounds__(256) k_zfwd_rhs(
       double2 v = make_double2(0.0, 0.0);
       if (kx0 + c < nkxp)
         v = G[(2 * f + ab) * Gfield + (long)j * NZ * nkxp + (long)z * nkxp + kx0 + c];
-      b0[(ab * ZF_KXG + c) * sstr + z] = v;
+      b0[(ab * ZF_KXG + c) * sstr + pad(z)] = v;
     }
     __syncthreads();
-    double2 *res = run(b0, b1, pl, 2 * ZF_KXG, sstr, stw, -1);
+    double2 *res = fft<NT>(b0, b1, pl, 2 * ZF_KXG, sstr, stw, -1);
     for (int idx = tid; idx < ZF_KXG * nkzt; idx += nthr) {
       const int c = idx % ZF_KXG, kp = idx / ZF_KXG;
       const int z = (kp <= NKZ) ? kp : (NZ - 1 + (kp - NKZ) - NKZ);
-      double2 a = res[(0 * ZF_KXG + c) * sstr + z];
-      double2 b = res[(1 * ZF_KXG + c) * sstr + z];
+      double2 a = res[(0 * ZF_KXG + c) * sstr + pad(z)];
+      double2 b = res[(1 * ZF_KXG + c) * sstr + pad(z)];
       a = make_double2(a.x / rnz, a.y / rnz);
       b = make_double2(b.x / rnz, b.y / rnz);
       const double KZ = kzv[kp];
@@ -281,7 +291,6 @@ __global__ void __launch_bounds__(256) k_zfwd_rhs(
     }
     __syncthreads();
   }
-
   // explicit terms and CN right-hand side per retained mode of plane j
   const double h = dscal[1 + rk_step];
   const double time = dscal[0];
@@ -395,127 +404,65 @@ __global__ void __launch_bounds__(256) k_zfwd_rhs(
 }
 
 size_t zfwd_smem(const dg_handle *h) {
-  return sizeof(double2) * (h->NZ + 4 * ZF_KXG * (h->NZ + 1) + h->nf * ZF_KXG * h->nkzt);
+  const int kxg = zf_kxg(h->NZ);
+  return sizeof(double2) * (h->NZ + fft_bufs(h->NZ) * 2 * kxg * padded_len(h->NZ) +
+                            h->nf * kxg * h->nkzt);
 }
 
 // ------------------------------------------------------------ CN tables
-// One thread per field builds the reference's physical-space system exactly
-// (identity init, CN rows over the build range, lower then upper BC rows,
-// for/channel.f:771-1029 and 1660-2282) and runs the MPI forward elimination
-// (for/mpi.f:672-700): a(j) = -a(j)/b(j-1), b(j) += a(j) c(j-1).
-struct CnParams {
-  int NY, nth, JS, JE, JSt[DG_MAX_TH], JEt[DG_MAX_TH];
-  int bct[3 + DG_MAX_TH][2];        // BC types lower/upper per field
-  double bcc[3 + DG_MAX_TH][2];     // BC values
-  double nu, nuv, pr[DG_MAX_TH];
+// The reference builds, per physical column, identity rows, CN rows over the
+// build range, then the lower and upper BC rows (for/channel.f:771-1029,
+// 1660-2282), and eliminates forward (for/mpi.f:672-700):
+// a(j) = -a(j)/b(j-1), b(j) += a(j) c(j-1).  The rows are the same for every
+// column and linear in TEMP1 = NU H_BAR / 2, so the host stores per row
+//   CN row : l = t l1, d = 1 + t d1, u = t u1   with t = TEMP1 (or TEMP1/PR)
+//   fixed  : l0, d0, u0 and the BC value
+// and one thread per (substep, field) runs the elimination whenever DELTA_T
+// changes.  Output per (rk, field): [5][NY+2] = a', 1/b', c, kind, bc value.
+struct CnRows {
+  int NY, nfld;
+  double nu, nuv, pr[3 + DG_MAX_TH];  // pr = 1 for velocity
 };
 
-__global__ void k_cn_tables(CnParams P, const double *__restrict__ dscal, int rk_step,
-                            const double *__restrict__ dy, const double *__restrict__ dyf,
-                            double *__restrict__ tab, int *__restrict__ kind,
-                            double *__restrict__ bcv) {
-  const int f = threadIdx.x;
-  if (f >= 3 + P.nth) return;
-  const int NY = P.NY, L = NY + 2;
-  double *A = tab + (long)(f * 4 + 0) * L;   // becomes the multiplier
-  double *B = tab + (long)(f * 4 + 1) * L;   // becomes 1/b'
-  double *Cc = tab + (long)(f * 4 + 2) * L;
-  int *K = kind + f * L;
-  double *V = bcv + f * L;
-  const double h = dscal[1 + rk_step];
-  const double T1 = P.nu * h / 2.0, NUV = P.nuv;
-  for (int j = 0; j < L; j++) { A[j] = 0.; B[j] = 1.; Cc[j] = 0.; K[j] = ROW_ZERO; V[j] = 0.; }
-  auto row = [&](int j, double l, double d, double u, double v) {
-    A[j] = l; B[j] = d; Cc[j] = u; V[j] = v; K[j] = (v != 0.0) ? ROW_BC : ROW_ZERO;
-  };
-  const int lo = P.bct[f][0], up = P.bct[f][1];
-  const double clo = P.bcc[f][0], cup = P.bcc[f][1];
-  if (f == F_U2) {
-    for (int j = 2; j <= NY; j++) {
-      A[j] = -T1 * NUV / (dyf[j - 1] * dy[j]);
-      B[j] = 1. + T1 * NUV / (dyf[j] * dy[j]) + T1 * NUV / (dyf[j - 1] * dy[j]);
-      Cc[j] = -T1 * NUV / (dyf[j] * dy[j]);
-      K[j] = ROW_RHS;
-    }
-    // APPLY_BC_2_LOWER / _UPPER (for/channel.f:1822-1933)
-    if (lo == 0) { row(1, 0., 1., 0., clo); row(2, 0., 1., 0., clo); }
-    else if (lo == 1) row(1, 0., -1., 1., dyf[1] * clo);
-    row(0, 0., 1., 0., 0.);
-    if (up == 0) { row(NY + 1, 0., 1., 0., cup); row(NY, 0., 1., 0., cup); }
-    else if (up == 1) row(NY + 1, -1., 1., 0., dyf[NY] * cup);
-  } else {
-    int j0, j1;
-    double a;
-    if (f < 3) { j0 = P.JS; j1 = P.JE; a = T1 * NUV; }
-    else { j0 = P.JSt[f - 3]; j1 = P.JEt[f - 3]; a = T1 / P.pr[f - 3] * NUV; }
-    for (int j = j0; j <= j1; j++) {
-      if (f < 3) {
-        A[j] = -T1 * NUV / (dy[j] * dyf[j]);
-        B[j] = 1. - T1 * NUV * (-1. / (dy[j + 1] * dyf[j]) - 1. / (dy[j] * dyf[j]));
-        Cc[j] = -T1 * NUV / (dy[j + 1] * dyf[j]);
-      } else {
-        A[j] = -(a) / (dy[j] * dyf[j]);
-        B[j] = 1. + (a) / (dy[j + 1] * dyf[j]) + (a) / (dy[j] * dyf[j]);
-        Cc[j] = -(a) / (dy[j + 1] * dyf[j]);
-      }
-      K[j] = ROW_RHS;
-    }
-    // APPLY_BC_1/3/TH_LOWER and _UPPER share one form
-    if (lo == 0) { row(0, 0., 1., 0., 0.); row(1, 0., 1., 0., clo); }
-    else { row(0, 0., 1., 0., 0.); row(1, 0., -1., 1., dy[2] * clo); }
-    if (up == 0) { row(NY + 1, 0., 1., 0., 0.); row(NY, 0., 1., 0., cup); }
-    else { row(NY, -1., 1., 0., dy[NY] * cup); row(NY + 1, 0., 1., 0., 0.); }
-  }
-  // forward elimination (THOMAS_FORWARD_REAL_MPI, single rank)
-  for (int j = 1; j < L; j++) {
-    A[j] = -A[j] / B[j - 1];
-    B[j] = B[j] + A[j] * Cc[j - 1];
-  }
-  for (int j = 0; j < L; j++) B[j] = (B[j] != 0.0) ? 1.0 / B[j] : 0.0;
-}
-
-// --------------------------------------------------------------- CN solve
-__global__ void __launch_bounds__(128) k_cn_solve(
-    int NY, long ss, int nf, const double *__restrict__ tab, const int *__restrict__ kind,
-    const double *__restrict__ bcv, FieldPtrs rhs, FieldPtrs cu, int wlo0, int wlo1, int wlo2,
-    int wlo3, int wlo4, int wlo5, int wlo6) {
-  const long m = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int f = blockIdx.y;
-  if (m >= ss || f >= nf) return;
-  const int L = NY + 2;
-  const double *A = tab + (long)(f * 4 + 0) * L;
-  const double *RB = tab + (long)(f * 4 + 1) * L;
-  const double *Cc = tab + (long)(f * 4 + 2) * L;
-  const int *K = kind + f * L;
-  const double *V = bcv + f * L;
-  const double2 *R = rhs.p[f];
-  double2 *U = cu.p[f];
-  const int wl[7] = {wlo0, wlo1, wlo2, wlo3, wlo4, wlo5, wlo6};
-  const int wlo = wl[f];
-  const bool mean = (m == 0);
-  // forward sweep; g(j) is parked in U(j) for j >= wlo
-  double2 g = make_double2(0.0, 0.0);
+__global__ void k_cn_tables(CnRows P, const double *__restrict__ dscal,
+                            const double *__restrict__ rows, double *__restrict__ tab) {
+  // rows: [field][8][L] = kind, l1, d1, u1, l0, d0, u0, v
+  extern __shared__ double rsm[];
+  const int L = P.NY + 2;
+  for (int i = threadIdx.x; i < P.nfld * 8 * L; i += blockDim.x) rsm[i] = rows[i];
+  __syncthreads();
+  const int t = threadIdx.x;
+  if (t >= 3 * P.nfld) return;
+  const int rk = t / P.nfld, f = t % P.nfld;
+  const double *R = rsm + (long)f * 8 * L;
+  double *T = tab + (long)(rk * (3 + DG_MAX_TH) + f) * 5 * L;
+  const double h = dscal[2 + rk];
+  const double s = (P.nu * h / 2.0) / P.pr[f] * P.nuv;
+  double bprev = 1.0, cprev = 0.0;
   for (int j = 0; j < L; j++) {
-    double2 r = make_double2(0.0, 0.0);
-    const int k = K[j];
-    if (k == ROW_RHS) r = R[(long)j * ss + m];
-    else if (k == ROW_BC && mean) r = make_double2(V[j], 0.0);
-    if (j > 0) {
-      const double a = A[j];
-      r.x += a * g.x;
-      r.y += a * g.y;
+    const double kind = R[j];
+    double l, d, u;
+    if (kind == (double)ROW_RHS) {
+      l = s * R[1 * L + j];
+      d = 1.0 + s * R[2 * L + j];
+      u = s * R[3 * L + j];
+    } else {
+      l = R[4 * L + j];
+      d = R[5 * L + j];
+      u = R[6 * L + j];
     }
-    g = r;
-    if (j >= wlo) U[(long)j * ss + m] = g;
-  }
-  // backward sweep (THOMAS_BACKWARD_REAL_MPI, single rank)
-  double2 x = make_double2(g.x * RB[L - 1], g.y * RB[L - 1]);
-  U[(long)(L - 1) * ss + m] = x;
-  for (int j = L - 2; j >= wlo; j--) {
-    const double2 gj = U[(long)j * ss + m];
-    const double c = Cc[j], rb = RB[j];
-    x = make_double2((gj.x - c * x.x) * rb, (gj.y - c * x.y) * rb);
-    U[(long)j * ss + m] = x;
+    double a = 0.0, b = d;
+    if (j > 0) {
+      a = -l / bprev;
+      b = d + a * cprev;
+    }
+    T[0 * L + j] = a;
+    T[1 * L + j] = (b != 0.0) ? 1.0 / b : 0.0;
+    T[2 * L + j] = u;
+    T[3 * L + j] = kind;
+    T[4 * L + j] = R[7 * L + j];
+    bprev = b;
+    cprev = u;
   }
 }
 
@@ -532,7 +479,6 @@ __global__ void k_remdiv_init(int NY, long ss, int nkxp, const double *__restric
   const int kx = (int)(m % nkxp), kp = (int)(m / nkxp);
   const double kx2 = kxv[kx] * kxv[kx], kz2 = kzv[kp] * kzv[kp];
   const bool mean = (m == 0);
-  // row 1
   double bprev = 1.0;
   double cprev = mean ? 0.0 : -1.0;
   ra[1 * ss + m] = 0.0;
@@ -557,44 +503,153 @@ __global__ void k_remdiv_init(int NY, long ss, int nkxp, const double *__restric
   }
 }
 
-__global__ void __launch_bounds__(128) k_remdiv(
-    int NY, long ss, int nkxp, int JS, int JE, const double *__restrict__ kxv,
+// ------------------------------------------------------- column kernels
+// Each CTA owns MT = 16 modes and their whole y-column.  Inputs are staged
+// into shared memory with coalesced loads from all 128 threads; the
+// sequential sweeps then run with one lane per (mode, re/im) part -- the
+// operators are real, so real and imaginary parts are independent systems --
+// touching only shared memory; results leave with coalesced stores.
+constexpr int COL_THR = 128;
+constexpr int COL_MT = 16;
+
+// CN solve of one field for MT modes (rows 0..NY+1, tables of this substep).
+__global__ void __launch_bounds__(COL_THR) k_cn_col(int NY, long ss, const double *__restrict__ tab_rk,
+                                                   FieldPtrs rhs, FieldPtrs cu, int4 wlo_a,
+                                                   int4 wlo_b) {
+  extern __shared__ double2 csm[];
+  const int L = NY + 2;
+  const int f = blockIdx.y;
+  const long m0 = (long)blockIdx.x * COL_MT;
+  const int mt = (int)((ss - m0) < COL_MT ? (ss - m0) : COL_MT);
+  double2 *X = csm;                                 // [j][MT]
+  double *TB = (double *)(X + (long)L * COL_MT);    // [5][L]
+  const double2 *__restrict__ R = rhs.p[f];
+  double2 *__restrict__ U = cu.p[f];
+  const int wl[8] = {wlo_a.x, wlo_a.y, wlo_a.z, wlo_a.w, wlo_b.x, wlo_b.y, wlo_b.z, wlo_b.w};
+  const int wlo = wl[f];
+  const int tid = threadIdx.x;
+  const double *T = tab_rk + (long)f * 5 * L;
+  for (int i = tid; i < 5 * L; i += COL_THR) TB[i] = T[i];
+  for (int i = tid; i < L * COL_MT; i += COL_THR) {
+    const int m = i % COL_MT, j = i / COL_MT;
+    X[i] = (m < mt) ? R[(long)j * ss + m0 + m] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  if (tid < 2 * COL_MT) {
+    const int m = tid >> 1, part = tid & 1;
+    const double *Aa = TB, *Rb = TB + L, *Cc = TB + 2 * L, *K = TB + 3 * L, *V = TB + 4 * L;
+    double *x = (double *)X + tid;
+    constexpr int st = 2 * COL_MT;
+    const bool mean_re = (m0 + m == 0) && part == 0;
+    double g = 0.0;
+#pragma unroll 8
+    for (int j = 0; j < L; j++) {
+      const double kind = K[j];
+      const double xr = x[j * st];
+      const double r = (kind == (double)ROW_RHS) ? xr : ((kind == (double)ROW_BC && mean_re) ? V[j] : 0.0);
+      g = r + Aa[j] * g;
+      x[j * st] = g;
+    }
+    double xv = g * Rb[L - 1];
+    x[(L - 1) * st] = xv;
+#pragma unroll 8
+    for (int j = L - 2; j >= wlo; j--) {
+      xv = (x[j * st] - Cc[j] * xv) * Rb[j];
+      x[j * st] = xv;
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < L * COL_MT; i += COL_THR) {
+    const int m = i % COL_MT, j = i / COL_MT;
+    if (m < mt && j >= wlo) U[(long)j * ss + m0 + m] = X[i];
+  }
+}
+
+// REM_DIV_CHAN for MT modes: divergence (parallel) -> forward and backward
+// sweeps (per part) -> projection, phi and CP update (parallel).
+__global__ void __launch_bounds__(COL_THR) k_rd_col(
+    int NY, long ss, int nkxp, int JS, int JE, int rk_step, const double *__restrict__ kxv,
     const double *__restrict__ kzv, const double *__restrict__ dy, const double *__restrict__ dyf,
     const double *__restrict__ ra, const double *__restrict__ rrb, double2 *__restrict__ u1,
     double2 *__restrict__ u2, double2 *__restrict__ u3, double2 *__restrict__ cp,
-    double2 *__restrict__ phi_out, double2 *__restrict__ gs, const double *__restrict__ dscal,
-    int rk_step) {
-  const long m = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= ss) return;
-  const int kx = (int)(m % nkxp), kp = (int)(m / nkxp);
-  const double KX = kxv[kx], KZ = kzv[kp];
-  const bool mean = (m == 0);
-  // forward sweep rows 2..NY; RHS = i kx U1 + (U2(j+1)-U2(j))/DYF(j) + i kz U3
-  double2 g = make_double2(0.0, 0.0);  // g(1) = 0
-  for (int j = 2; j <= NY; j++) {
+    double2 *__restrict__ phi_out, const double *__restrict__ dscal) {
+  extern __shared__ double2 csm[];
+  const int L = NY + 2;
+  const long m0 = (long)blockIdx.x * COL_MT;
+  const int mt = (int)((ss - m0) < COL_MT ? (ss - m0) : COL_MT);
+  double2 *GX = csm;                                // [j][MT]: rhs -> g -> phi
+  double *RA = (double *)(GX + (long)L * COL_MT);   // [j][MT]
+  double *RB = RA + (long)L * COL_MT;               // [j][MT]
+  double *UU = RB + (long)L * COL_MT;               // [j] upper diagonal rows 2..NY-1
+  const int tid = threadIdx.x;
+  for (int j = tid; j < L; j += COL_THR) UU[j] = (j >= 2 && j < NY) ? 1. / (dy[j + 1] * dyf[j]) : 0.0;
+  for (int i = tid; i < L * COL_MT; i += COL_THR) {
+    const int m = i % COL_MT, j = i / COL_MT;
+    const long mg = m0 + m;
     double2 r = make_double2(0.0, 0.0);
-    if (j < NY) {
-      const long o = (long)j * ss + m;
-      const double2 a1 = u1[o], a3 = u3[o], b2 = u2[o], b2p = u2[o + ss];
-      const double d = dyf[j];
-      r.x = (-KX * a1.y) + (b2p.x - b2.x) / d + (-KZ * a3.y);
-      r.y = (KX * a1.x) + (b2p.y - b2.y) / d + (KZ * a3.x);
+    double a = 0.0, b = 0.0;
+    if (m < mt && j >= 1 && j <= NY) {
+      const long o = (long)j * ss + mg;
+      a = ra[o];
+      b = rrb[o];
+      if (j >= 2 && j < NY) {
+        const double KX = kxv[mg % nkxp], KZ = kzv[mg / nkxp];
+        const double2 a1 = u1[o], a3 = u3[o], b2 = u2[o], b2p = u2[o + ss];
+        const double d = dyf[j];
+        r.x = (-KX * a1.y) + (b2p.x - b2.x) / d + (-KZ * a3.y);
+        r.y = (KX * a1.x) + (b2p.y - b2.y) / d + (KZ * a3.x);
+      }
     }
-    const double a = ra[(long)j * ss + m];
-    g = make_double2(r.x + a * g.x, r.y + a * g.y);
-    gs[(long)j * ss + m] = g;
+    GX[i] = r;
+    RA[i] = a;
+    RB[i] = b;
   }
+  __syncthreads();
+  if (tid < 2 * COL_MT) {
+    const int m = tid >> 1;
+    const bool mean = (m0 + m == 0);
+    double *x = (double *)GX + tid;
+    constexpr int st = 2 * COL_MT;
+    double g = 0.0;  // row 1 has a zero right-hand side
+    x[1 * st] = 0.0;
+#pragma unroll 8
+    for (int j = 2; j <= NY; j++) {
+      g = x[j * st] + RA[j * COL_MT + m] * g;
+      x[j * st] = g;
+    }
+    double ph = g * RB[NY * COL_MT + m];
+    x[NY * st] = ph;
+#pragma unroll 8
+    for (int j = NY - 1; j >= 2; j--) {
+      ph = (x[j * st] - UU[j] * ph) * RB[j * COL_MT + m];
+      x[j * st] = ph;
+    }
+    const double u1r = mean ? 0.0 : -1.0;
+    ph = (x[1 * st] - u1r * ph) * RB[1 * COL_MT + m];
+    x[1 * st] = ph;
+  }
+  __syncthreads();
   const double hh = (rk_step > 0) ? dscal[1 + rk_step] : 1.0;
-  // backward sweep with projection
-  double2 phin = make_double2(g.x * rrb[(long)NY * ss + m], g.y * rrb[(long)NY * ss + m]);
-  auto project = [&](int j, double2 ph) {
-    const long o = (long)j * ss + m;
+  for (int i = tid; i < L * COL_MT; i += COL_THR) {
+    const int m = i % COL_MT, j = i / COL_MT;
+    if (m >= mt || j < 1 || j > NY) continue;
+    const long mg = m0 + m, o = (long)j * ss + mg;
+    const double KX = kxv[mg % nkxp], KZ = kzv[mg / nkxp];
+    const double2 ph = GX[i];
     double2 a1 = u1[o], a3 = u3[o];
     // U1 -= i kx phi, U3 -= i kz phi
     a1.x -= -KX * ph.y; a1.y -= KX * ph.x;
     a3.x -= -KZ * ph.y; a3.y -= KZ * ph.x;
     u1[o] = a1;
     u3[o] = a3;
+    if (j >= 2) {
+      // U2(j) -= (phi(j) - phi(j-1)) / DY(j)
+      const double2 pm = GX[i - COL_MT];
+      double2 b = u2[o];
+      b.x -= (ph.x - pm.x) / dy[j];
+      b.y -= (ph.y - pm.y) / dy[j];
+      u2[o] = b;
+    }
     phi_out[o] = ph;
     if (rk_step > 0 && j >= JS && j <= JE) {
       double2 p = cp[o];
@@ -602,23 +657,6 @@ __global__ void __launch_bounds__(128) k_remdiv(
       p.y = p.y + ph.y / hh;
       cp[o] = p;
     }
-  };
-  project(NY, phin);
-  for (int j = NY - 1; j >= 1; j--) {
-    double u;
-    if (j == 1) u = mean ? 0.0 : -1.0;
-    else u = 1. / (dy[j + 1] * dyf[j]);
-    const double2 gj = (j >= 2) ? gs[(long)j * ss + m] : make_double2(0.0, 0.0);
-    const double rb = rrb[(long)j * ss + m];
-    const double2 ph = make_double2((gj.x - u * phin.x) * rb, (gj.y - u * phin.y) * rb);
-    project(j, ph);
-    // U2(j+1) -= (phi(j+1) - phi(j)) / DY(j+1)
-    const long o = (long)(j + 1) * ss + m;
-    double2 b = u2[o];
-    b.x -= (phin.x - ph.x) / dy[j + 1];
-    b.y -= (phin.y - ph.y) / dy[j + 1];
-    u2[o] = b;
-    phin = ph;
   }
 }
 
@@ -731,12 +769,20 @@ __global__ void k_cfl_min(const double *__restrict__ phys, long pfield, int NY, 
 }
 
 __global__ void k_dt_update(double *dscal, const unsigned long long *minbits, double dt0) {
-  // for/courant.f:15-62: dt0 carries the velocity-independent limits
+  // for/courant.f:15-59: dt0 carries the velocity-independent limits.  The
+  // new DELTA_T is parked in dscal[8]: the substep that called COURANT still
+  // uses its own H_BAR for the pressure update (TEMP4 was set on entry).
   double dt = fmin(dt0, __longlong_as_double((long long)*minbits));
   double nd;
   if (dt <= 0) nd = 0.0001;
   else if (dt >= 999.) nd = 999.0;
   else nd = dt;
+  dscal[8] = nd;
+}
+
+// DELTA_T = pending value; H_BAR from it (for/courant.f:60-62)
+__global__ void k_dt_commit(double *dscal) {
+  const double nd = dscal[8];
   dscal[1] = nd;
   dscal[2] = nd * (8.0 / 15.0);
   dscal[3] = nd * (2.0 / 15.0);
@@ -812,23 +858,70 @@ __global__ void k_absmax(const double *__restrict__ a, long n, unsigned long lon
 }  // namespace
 
 // ================================================================ host side
-static int cn_tables(dg_handle *h, int rk_step) {
-  CnParams P;
-  P.NY = h->NY; P.nth = h->NTH; P.JS = h->jstart; P.JE = h->jend;
-  P.nu = h->p.nu; P.nuv = h->p.nu_v_scale;
-  for (int n = 0; n < DG_MAX_TH; n++) { P.JSt[n] = h->jstart_th[n]; P.JEt[n] = h->jend_th[n]; P.pr[n] = h->p.pr[n]; }
-  P.bct[0][0] = h->p.u_bc_ymin; P.bct[0][1] = h->p.u_bc_ymax;
-  P.bcc[0][0] = h->p.u_bc_ymin_c1; P.bcc[0][1] = h->p.u_bc_ymax_c1;
-  P.bct[1][0] = h->p.v_bc_ymin; P.bct[1][1] = h->p.v_bc_ymax;
-  P.bcc[1][0] = h->p.v_bc_ymin_c1; P.bcc[1][1] = h->p.v_bc_ymax_c1;
-  P.bct[2][0] = h->p.w_bc_ymin; P.bct[2][1] = h->p.w_bc_ymax;
-  P.bcc[2][0] = h->p.w_bc_ymin_c1; P.bcc[2][1] = h->p.w_bc_ymax_c1;
-  for (int n = 0; n < h->NTH; n++) {
-    P.bct[3 + n][0] = h->p.th_bc_ymin[n]; P.bct[3 + n][1] = h->p.th_bc_ymax[n];
-    P.bcc[3 + n][0] = h->p.th_bc_ymin_c1[n]; P.bcc[3 + n][1] = h->p.th_bc_ymax_c1[n];
+// Row templates of the CN systems (host, once per handle).
+static void cn_row_templates(const dg_handle *h, double *rows) {
+  const int NY = h->NY, L = NY + 2, nfld = h->nf;
+  const double *dy = h->h_dy, *dyf = h->h_dyf;
+  for (int f = 0; f < nfld; f++) {
+    double *K = rows + (long)f * 8 * L;
+    double *l1 = K + L, *d1 = K + 2 * L, *u1 = K + 3 * L, *l0 = K + 4 * L, *d0 = K + 5 * L,
+           *u0 = K + 6 * L, *v = K + 7 * L;
+    for (int j = 0; j < L; j++) {
+      K[j] = ROW_ZERO; l1[j] = d1[j] = u1[j] = 0.0; l0[j] = 0.0; d0[j] = 1.0; u0[j] = 0.0; v[j] = 0.0;
+    }
+    auto fixed = [&](int j, double l, double d, double u, double val) {
+      K[j] = (val != 0.0) ? ROW_BC : ROW_ZERO; l0[j] = l; d0[j] = d; u0[j] = u; v[j] = val;
+    };
+    int lo, up;
+    double clo, cup;
+    if (f == F_U1) { lo = h->p.u_bc_ymin; up = h->p.u_bc_ymax; clo = h->p.u_bc_ymin_c1; cup = h->p.u_bc_ymax_c1; }
+    else if (f == F_U2) { lo = h->p.v_bc_ymin; up = h->p.v_bc_ymax; clo = h->p.v_bc_ymin_c1; cup = h->p.v_bc_ymax_c1; }
+    else if (f == F_U3) { lo = h->p.w_bc_ymin; up = h->p.w_bc_ymax; clo = h->p.w_bc_ymin_c1; cup = h->p.w_bc_ymax_c1; }
+    else { const int n = f - 3; lo = h->p.th_bc_ymin[n]; up = h->p.th_bc_ymax[n]; clo = h->p.th_bc_ymin_c1[n]; cup = h->p.th_bc_ymax_c1[n]; }
+    if (f == F_U2) {
+      for (int j = 2; j <= NY; j++) {
+        K[j] = ROW_RHS;
+        l1[j] = -1.0 / (dyf[j - 1] * dy[j]);
+        d1[j] = 1.0 / (dyf[j] * dy[j]) + 1.0 / (dyf[j - 1] * dy[j]);
+        u1[j] = -1.0 / (dyf[j] * dy[j]);
+      }
+      if (lo == 0) { fixed(1, 0., 1., 0., clo); fixed(2, 0., 1., 0., clo); }
+      else if (lo == 1) fixed(1, 0., -1., 1., dyf[1] * clo);
+      fixed(0, 0., 1., 0., 0.);
+      if (up == 0) { fixed(NY + 1, 0., 1., 0., cup); fixed(NY, 0., 1., 0., cup); }
+      else if (up == 1) fixed(NY + 1, -1., 1., 0., dyf[NY] * cup);
+    } else {
+      const int j0 = (f < 3) ? h->jstart : h->jstart_th[f - 3];
+      const int j1 = (f < 3) ? h->jend : h->jend_th[f - 3];
+      for (int j = j0; j <= j1; j++) {
+        K[j] = ROW_RHS;
+        l1[j] = -1.0 / (dy[j] * dyf[j]);
+        d1[j] = 1.0 / (dy[j + 1] * dyf[j]) + 1.0 / (dy[j] * dyf[j]);
+        u1[j] = -1.0 / (dy[j + 1] * dyf[j]);
+      }
+      if (lo == 0) { fixed(0, 0., 1., 0., 0.); fixed(1, 0., 1., 0., clo); }
+      else { fixed(0, 0., 1., 0., 0.); fixed(1, 0., -1., 1., dy[2] * clo); }
+      if (up == 0) { fixed(NY + 1, 0., 1., 0., 0.); fixed(NY, 0., 1., 0., cup); }
+      else { fixed(NY, -1., 1., 0., dy[NY] * cup); fixed(NY + 1, 0., 1., 0., 0.); }
+    }
   }
-  k_cn_tables<<<1, 32, 0, h->st>>>(P, h->dscal, rk_step, h->dy, h->dyf, h->cn_tab, h->cn_kind,
-                                   h->cn_bc);
+}
+
+int dg_cn_tables(dg_handle *h) {
+  if (h->periodic) return DG_OK;
+  const int L = h->NY + 2;
+  if (!h->cn_rows) {
+    double *rows = (double *)malloc(sizeof(double) * h->nf * 8 * L);
+    cn_row_templates(h, rows);
+    DG_CUDA(cudaMalloc((void **)&h->cn_rows, sizeof(double) * h->nf * 8 * L));
+    cudaError_t e = cudaMemcpy(h->cn_rows, rows, sizeof(double) * h->nf * 8 * L, cudaMemcpyHostToDevice);
+    free(rows);
+    DG_CUDA(e);
+  }
+  CnRows P;
+  P.NY = h->NY; P.nfld = h->nf; P.nu = h->p.nu; P.nuv = h->p.nu_v_scale;
+  for (int f = 0; f < 3 + DG_MAX_TH; f++) P.pr[f] = (f >= 3 && f - 3 < h->NTH) ? h->p.pr[f - 3] : 1.0;
+  k_cn_tables<<<1, 32, sizeof(double) * h->nf * 8 * L, h->st>>>(P, h->dscal, h->cn_rows, h->cn_tab);
   DG_LAUNCHED();
   return DG_OK;
 }
@@ -846,11 +939,30 @@ int dg_apply_bc_vel_dev(dg_handle *h) {
   return DG_OK;
 }
 
+int dg_cn_solve_dev(dg_handle *h, int rk_step) {
+  FieldPtrs cu, rhs;
+  for (int f = 0; f < h->nf; f++) { cu.p[f] = h->cu[f]; rhs.p[f] = h->rhs[f]; }
+  int wl[8] = {1, 1, 1, 1, 1, 1, 1, 1};
+  for (int n = 0; n < h->NTH; n++) wl[3 + n] = h->jstart_th[n] - 1;
+  const int L = h->NY + 2;
+  const double *tab = h->cn_tab + (long)(rk_step - 1) * (3 + DG_MAX_TH) * 5 * L;
+  const size_t sm = sizeof(double2) * L * COL_MT + sizeof(double) * 5 * L;
+  dg_big_smem((const void *)k_cn_col);
+  dim3 grid(dg_cdiv(h->ss, COL_MT), h->nf);
+  k_cn_col<<<grid, COL_THR, sm, h->st>>>(h->NY, h->ss, tab, rhs, cu,
+                                         make_int4(wl[0], wl[1], wl[2], wl[3]),
+                                         make_int4(wl[4], wl[5], wl[6], wl[7]));
+  DG_LAUNCHED();
+  return DG_OK;
+}
+
 int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step) {
-  k_remdiv<<<dg_cdiv(h->ss, 128), 128, 0, h->st>>>(
-      h->NY, h->ss, h->nkxp, h->jstart, h->jend, h->kx, h->kz, h->dy, h->dyf, h->rem_a,
-      h->rem_rb, h->cu[0], h->cu[1], h->cu[2], h->cp, h->cr1, h->gphi, h->dscal,
-      update_cp ? rk_step : 0);
+  const int L = h->NY + 2;
+  const size_t sm = sizeof(double2) * L * COL_MT + sizeof(double) * (2 * L * COL_MT + L);
+  dg_big_smem((const void *)k_rd_col);
+  k_rd_col<<<dg_cdiv(h->ss, COL_MT), COL_THR, sm, h->st>>>(
+      h->NY, h->ss, h->nkxp, h->jstart, h->jend, update_cp ? rk_step : 0, h->kx, h->kz, h->dy,
+      h->dyf, h->rem_a, h->rem_rb, h->cu[0], h->cu[1], h->cu[2], h->cp, h->cr1, h->dscal);
   DG_LAUNCHED();
   return DG_OK;
 }
@@ -897,13 +1009,17 @@ int dg_courant_dev(dg_handle *h, const double2 *const *u) {
   return DG_OK;
 }
 
+int dg_dt_commit(dg_handle *h) {
+  k_dt_commit<<<1, 1, 0, h->st>>>(h->dscal);
+  DG_LAUNCHED();
+  return dg_cn_tables(h);
+}
+
 int dg_chan_init(dg_handle *h) {
   k_remdiv_init<<<dg_cdiv(h->ss, 128), 128, 0, h->st>>>(h->NY, h->ss, h->nkxp, h->kx, h->kz, h->dy,
                                                         h->dyf, h->rem_a, h->rem_rb);
   DG_LAUNCHED();
-  cudaFuncSetAttribute(k_xrow_nl, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_zfwd_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  return DG_OK;
+  return dg_cn_tables(h);
 }
 
 extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
@@ -914,44 +1030,50 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
   for (int f = 0; f < h->nf; f++) in[f] = h->cu[f];
   DG_TRY(dg_zinv(h, in, h->nf, 0, h->NY + 1, h->H, 0));
   // 2. x-row nonlinear products, y-marching chunks
-  const int chunk = 16;
+  const int chunk = 8;
   const long Hfield = (long)h->nplanes * h->NZ * h->nkxp;
   {
     dim3 grid(dg_cdiv(h->NZ, XR_ROWS), dg_cdiv(h->NY, chunk));
-    k_xrow_nl<<<grid, 256, xrow_smem(h), h->st>>>(C, h->H, Hfield, chunk, h->plx, h->twx, h->dyf,
-                                                  h->dy, h->kx, h->G, Hfield);
+    const size_t sm = xrow_smem(h);
+#define KERNEL_BODY(N)                                                                          \
+  dg_big_smem((const void *)k_xrow_nl<N>);                                                      \
+  k_xrow_nl<N><<<grid, XR_THR, sm, h->st>>>(C, h->H, Hfield, chunk, h->plx, h->twx, h->dyf, h->dy, \
+                                            h->kx, h->G, Hfield)
+    switch (h->NX) {
+      DG_FOR_EACH_N(DG_CASE_N)
+      default: KERNEL_BODY(0); break;
+    }
+#undef KERNEL_BODY
     DG_LAUNCHED();
   }
   // 3. z forward, explicit terms, CN right-hand side
   {
     FieldPtrs cu, cf, rhs;
     for (int f = 0; f < h->nf; f++) { cu.p[f] = h->cu[f]; cf.p[f] = h->cf[f]; rhs.p[f] = h->rhs[f]; }
-    dim3 grid(dg_cdiv(h->nkxp, ZF_KXG), h->NY);
-    k_zfwd_rhs<<<grid, 256, zfwd_smem(h), h->st>>>(C, h->G, Hfield, h->plz, h->twz, h->dscal,
-                                                   rk_step, h->kx, h->kz, h->dy, h->dyf, cu, cf,
-                                                   rhs, h->cp);
+    dim3 grid(dg_cdiv(h->nkxp, zf_kxg(h->NZ)), h->NY);
+    const size_t sm = zfwd_smem(h);
+#define KERNEL_BODY(N)                                                                          \
+  dg_big_smem((const void *)k_zfwd_rhs<N>);                                                     \
+  k_zfwd_rhs<N><<<grid, ZF_THR, sm, h->st>>>(C, h->G, Hfield, h->plz, h->twz, h->dscal, rk_step, \
+                                             h->kx, h->kz, h->dy, h->dyf, cu, cf, rhs, h->cp)
+    switch (h->NZ) {
+      DG_FOR_EACH_N(DG_CASE_N)
+      default: KERNEL_BODY(0); break;
+    }
+#undef KERNEL_BODY
     DG_LAUNCHED();
   }
-  // 4. CN tables for this substep and the per-mode solves
-  DG_TRY(cn_tables(h, rk_step));
-  {
-    FieldPtrs cu, rhs;
-    for (int f = 0; f < h->nf; f++) { cu.p[f] = h->cu[f]; rhs.p[f] = h->rhs[f]; }
-    int wl[7] = {1, 1, 1, 1, 1, 1, 1};
-    for (int n = 0; n < h->NTH; n++) wl[3 + n] = h->jstart_th[n] - 1;
-    dim3 grid(dg_cdiv(h->ss, 128), h->nf);
-    k_cn_solve<<<grid, 128, 0, h->st>>>(h->NY, h->ss, h->nf, h->cn_tab, h->cn_kind, h->cn_bc, rhs,
-                                        cu, wl[0], wl[1], wl[2], wl[3], wl[4], wl[5], wl[6]);
-    DG_LAUNCHED();
-  }
-  // 5. COURANT on the post-CN velocity (for/channel.f:1037-1040)
-  if (h->p.variable_dt && rk_step == 3 && h->p.update_dt > 0 &&
-      (time_step % h->p.update_dt) == 0) {
+  // 4. per-mode CN solves, then COURANT on the post-CN velocity
+  //    (for/channel.f:1037-1040), then REM_DIV_CHAN and CP += phi / H_BAR
+  DG_TRY(dg_cn_solve_dev(h, rk_step));
+  const bool cfl = h->p.variable_dt && rk_step == 3 && h->p.update_dt > 0 &&
+                   (time_step % h->p.update_dt) == 0;
+  if (cfl) {
     const double2 *u[3] = {h->cu[0], h->cu[1], h->cu[2]};
     DG_TRY(dg_courant_dev(h, u));
   }
-  // 6. REM_DIV_CHAN + CP update
   DG_TRY(dg_rem_div_dev(h, 1, rk_step));
+  if (cfl) DG_TRY(dg_dt_commit(h));
   return DG_OK;
 }
 
@@ -968,7 +1090,8 @@ extern "C" int diablo_apply_bc_vel(dg_handle *h) {
 extern "C" int diablo_courant(dg_handle *h) {
   if (!h || h->periodic) return DG_ERR_ARG;
   const double2 *u[3] = {h->cu[0], h->cu[1], h->cu[2]};
-  return dg_courant_dev(h, u);
+  DG_TRY(dg_courant_dev(h, u));
+  return dg_dt_commit(h);
 }
 
 int dg_stats_dev(dg_handle *h, dg_stats *s) {

@@ -98,9 +98,8 @@ struct dg_handle {
   double2 *rhs[3 + DG_MAX_TH];  // CN right-hand sides
   double2 *gphi;                // REM_DIV forward-sweep scratch
   double *rem_a, *rem_rb;       // REM_DIV multipliers and reciprocal pivots [NY+2][ss]
-  double *cn_tab;               // CN tables [field][4][NY+2]
-  int *cn_kind;                 // row kinds [field][NY+2]
-  double *cn_bc;                // BC row values [field][NY+2]
+  double *cn_tab;               // CN tables [rk][field][5][NY+2]
+  double *cn_rows;              // CN row templates [field][8][NY+2]
 
   // work arrays
   double2 *H;                   // half-physical [nf][planes][NZ][nkxp]
@@ -133,5 +132,14 @@ int dg_apply_bc_vel_dev(dg_handle *h);
 int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step);
 int dg_courant_dev(dg_handle *h, const double2 *const *u);
 int dg_stats_dev(dg_handle *h, dg_stats *s);
+int dg_cn_tables(dg_handle *h);
+int dg_dt_commit(dg_handle *h);
+
+#define DG_CASE_N(N) \
+  case N:            \
+    KERNEL_BODY(N);  \
+    break;
+
+void dg_big_smem(const void *kern);
 
 static inline int dg_cdiv(long a, long b) { return (int)((a + b - 1) / b); }

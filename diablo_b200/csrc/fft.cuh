@@ -1,8 +1,10 @@
 // Shared-memory mixed-radix Stockham FFT used by all transform kernels.
 //
 // A batch of `nsig` complex signals of length N lives in shared memory, one
-// signal per `sig_stride` double2.  Every thread of the CTA takes butterflies
-// of every signal in turn; one __syncthreads() separates passes.  The
+// signal per `sig_stride` double2, element i of a signal stored at pad(i) =
+// i + i/16 (one spare slot per 16 keeps the strided stores of the early
+// passes off a single bank).  Every thread of the CTA takes butterflies of
+// every signal in turn; one __syncthreads() separates passes.  The
 // autosorting (Stockham) form needs a second buffer of the same size and
 // gives naturally ordered output.  Pass with radix R and running span Ns:
 //   butterfly b in [0, N/R): k = b mod Ns,
@@ -11,6 +13,10 @@
 // W_N = exp(sign 2 pi i / N); the table holds exp(-2 pi i m / N) and the
 // inverse direction conjugates it.  Unnormalised in both directions, which
 // is FFTW's convention (forward sign -1).
+//
+// Two front ends: run<N>() with the transform length and radix plan fixed at
+// compile time (all index arithmetic folds), and run() with a runtime plan
+// for lengths without a specialisation.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -29,6 +35,9 @@ __device__ __forceinline__ double2 conjg(double2 a) { return make_double2(a.x, -
 __device__ __forceinline__ double2 mul_si(double2 a, int sign) {
   return sign < 0 ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
 }
+
+__host__ __device__ constexpr int pad(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr int padded_len(int n) { return n + (n >> 4) + 1; }
 
 template <int R>
 __device__ __forceinline__ void dft(double2 *v, int sign);
@@ -84,6 +93,44 @@ __device__ __forceinline__ void dft<8>(double2 *v, int sign) {
   v[7] = csub(e[3], t3);
 }
 
+// 16-point DFT as 4 x 4: n = 4 n1 + n2, k = k1 + 4 k2
+template <>
+__device__ __forceinline__ void dft<16>(double2 *v, int sign) {
+  // cos and sin of 2 pi m / 16, m = 0..9
+  const double C[10] = {1.0, 0.92387953251128675613, 0.70710678118654752440,
+                        0.38268343236508977173, 0.0, -0.38268343236508977173,
+                        -0.70710678118654752440, -0.92387953251128675613, -1.0,
+                        -0.92387953251128675613};
+  const double S[10] = {0.0, 0.38268343236508977173, 0.70710678118654752440,
+                        0.92387953251128675613, 1.0, 0.92387953251128675613,
+                        0.70710678118654752440, 0.38268343236508977173, 0.0,
+                        -0.38268343236508977173};
+  double2 a[4][4];
+#pragma unroll
+  for (int n2 = 0; n2 < 4; n2++) {
+    double2 t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+    dft<4>(t, sign);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) {
+      const int m = n2 * k1;
+      double2 x = t[k1];
+      if (m != 0) {
+        const double2 w = make_double2(C[m], sign * S[m]);
+        x = cmul(x, w);
+      }
+      a[n2][k1] = x;
+    }
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < 4; k1++) {
+    double2 t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+    dft<4>(t, sign);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; k2++) v[k1 + 4 * k2] = t[k2];
+  }
+}
+
+// -------------------------------------------------------- runtime-plan pass
 template <int R>
 __device__ __forceinline__ void pass(const double2 *__restrict__ src, double2 *__restrict__ dst,
                                      int N, int Ns, int nsig, int sig_stride,
@@ -100,7 +147,7 @@ __device__ __forceinline__ void pass(const double2 *__restrict__ src, double2 *_
     double2 v[R];
 #pragma unroll
     for (int r = 0; r < R; r++) {
-      double2 x = in[b + r * nb];
+      double2 x = in[pad(b + r * nb)];
       if (r > 0 && k > 0) {
         double2 t = tw[r * k * tmul];
         if (sign > 0) t.y = -t.y;
@@ -111,11 +158,11 @@ __device__ __forceinline__ void pass(const double2 *__restrict__ src, double2 *_
     dft<R>(v, sign);
     const int idx = (b / Ns) * Ns * R + k;
 #pragma unroll
-    for (int r = 0; r < R; r++) out[idx + r * Ns] = v[r];
+    for (int r = 0; r < R; r++) out[pad(idx + r * Ns)] = v[r];
   }
 }
 
-// Runs the whole plan; returns the buffer holding the result (buf0 or buf1).
+// Runs a runtime plan; returns the buffer holding the result (buf0 or buf1).
 // Must be called by every thread of the CTA.
 __device__ inline double2 *run(double2 *buf0, double2 *buf1, const FftPlan &pl, int nsig,
                                int sig_stride, const double2 *tw, int sign) {
@@ -126,6 +173,7 @@ __device__ inline double2 *run(double2 *buf0, double2 *buf1, const FftPlan &pl, 
   for (int p = 0; p < pl.np; p++) {
     const int R = pl.r[p];
     switch (R) {
+      case 16: pass<16>(src, dst, pl.n, Ns, nsig, sig_stride, tw, sign, tid, nthr); break;
       case 8: pass<8>(src, dst, pl.n, Ns, nsig, sig_stride, tw, sign, tid, nthr); break;
       case 4: pass<4>(src, dst, pl.n, Ns, nsig, sig_stride, tw, sign, tid, nthr); break;
       case 3: pass<3>(src, dst, pl.n, Ns, nsig, sig_stride, tw, sign, tid, nthr); break;
@@ -140,4 +188,160 @@ __device__ inline double2 *run(double2 *buf0, double2 *buf1, const FftPlan &pl, 
   return src;
 }
 
+// ----------------------------------------------------- compile-time plans
+// radix of pass p for length N (0 = no pass).  Lengths 2^a 3^b; every pass
+// keeps N/R <= 128 so a 128-thread CTA holds whole signals per round.
+__host__ __device__ constexpr int plan_radix(int N, int p) {
+  int m = N, r = 0;
+  for (int q = 0; q <= p; q++) {
+    if (m == 1) return 0;
+    if (m == 512 || m == 64 || m == 8 * 3 || m == 96) r = 8;
+    else if (m % 16 == 0) r = 16;
+    else if (m % 8 == 0) r = 8;
+    else if (m % 4 == 0) r = 4;
+    else if (m % 2 == 0) r = 2;
+    else if (m % 3 == 0) r = 3;
+    else return 0;
+    m /= r;
+  }
+  return r;
+}
+
+__host__ __device__ constexpr int plan_ns(int N, int p) {
+  int ns = 1;
+  for (int q = 0; q < p; q++) ns *= plan_radix(N, q);
+  return ns;
+}
+
+template <int N, int R, int NS, int SIGN>
+__device__ __forceinline__ void cpass(const double2 *__restrict__ src, double2 *__restrict__ dst,
+                                      int nsig, int sig_stride, const double2 *__restrict__ tw,
+                                      int tid, int nthr) {
+  constexpr int NB = N / R;
+  constexpr int TMUL = N / (NS * R);
+  const int total = nsig * NB;
+  for (int w = tid; w < total; w += nthr) {
+    const int s = w / NB;
+    const int b = w - s * NB;
+    const double2 *in = src + (long)s * sig_stride;
+    double2 *out = dst + (long)s * sig_stride;
+    const int k = b % NS;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      double2 x = in[pad(b + r * NB)];
+      if (NS > 1 && r > 0) {
+        double2 t = tw[r * k * TMUL];
+        if (SIGN > 0) t.y = -t.y;
+        x = cmul(x, t);
+      }
+      v[r] = x;
+    }
+    dft<R>(v, SIGN);
+    const int idx = (b / NS) * NS * R + k;
+#pragma unroll
+    for (int r = 0; r < R; r++) out[pad(idx + r * NS)] = v[r];
+  }
+}
+
+template <int N, int SIGN, int P>
+__device__ __forceinline__ void cpasses(double2 *&src, double2 *&dst, int nsig, int sig_stride,
+                                        const double2 *tw, int tid, int nthr) {
+  constexpr int R = plan_radix(N, P);
+  if constexpr (R != 0) {
+    constexpr int NS = plan_ns(N, P);
+    cpass<N, R, NS, SIGN>(src, dst, nsig, sig_stride, tw, tid, nthr);
+    __syncthreads();
+    double2 *t = src;
+    src = dst;
+    dst = t;
+    cpasses<N, SIGN, P + 1>(src, dst, nsig, sig_stride, tw, tid, nthr);
+  }
+}
+
+// In-place variant: each round covers whole signals (nthr / (N/R) of them);
+// every thread of the round loads its butterfly, the CTA syncs, then stores.
+template <int N, int R, int NS, int SIGN>
+__device__ __forceinline__ void ippass(double2 *__restrict__ buf, int nsig, int sig_stride,
+                                       const double2 *__restrict__ tw, int tid, int nthr) {
+  constexpr int NB = N / R;
+  constexpr int TMUL = N / (NS * R);
+  const int spr = nthr / NB;
+  const int nrounds = (nsig + spr - 1) / spr;
+  const int sl = tid / NB, b = tid % NB, k = b % NS;
+  const int idx = (b / NS) * NS * R + k;
+  for (int rd = 0; rd < nrounds; rd++) {
+    const int s = rd * spr + sl;
+    const bool act = (sl < spr) && (s < nsig);
+    double2 v[R];
+    if (act) {
+      const double2 *in = buf + (long)s * sig_stride;
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        double2 x = in[pad(b + r * NB)];
+        if (NS > 1 && r > 0) {
+          double2 t = tw[r * k * TMUL];
+          if (SIGN > 0) t.y = -t.y;
+          x = cmul(x, t);
+        }
+        v[r] = x;
+      }
+      dft<R>(v, SIGN);
+    }
+    __syncthreads();
+    if (act) {
+      double2 *out = buf + (long)s * sig_stride;
+#pragma unroll
+      for (int r = 0; r < R; r++) out[pad(idx + r * NS)] = v[r];
+    }
+    __syncthreads();
+  }
+}
+
+template <int N, int SIGN, int P>
+__device__ __forceinline__ void ippasses(double2 *buf, int nsig, int sig_stride, const double2 *tw,
+                                         int tid, int nthr) {
+  constexpr int R = plan_radix(N, P);
+  if constexpr (R != 0) {
+    constexpr int NS = plan_ns(N, P);
+    ippass<N, R, NS, SIGN>(buf, nsig, sig_stride, tw, tid, nthr);
+    ippasses<N, SIGN, P + 1>(buf, nsig, sig_stride, tw, tid, nthr);
+  }
+}
+
+template <int N, int SIGN>
+__device__ __forceinline__ double2 *run_ct(double2 *buf0, double2 *buf1, int nsig, int sig_stride,
+                                           const double2 *tw) {
+  const int tid = threadIdx.x;
+  const int nthr = blockDim.x;
+  double2 *src = buf0, *dst = buf1;
+  cpasses<N, SIGN, 0>(src, dst, nsig, sig_stride, tw, tid, nthr);
+  return src;
+}
+
+// Dispatch helper: N == 0 selects the runtime plan.
+// Compile-time lengths run in place in buf0 (buf1 unused); the runtime plan
+// ping-pongs between buf0 and buf1.
+template <int N>
+__device__ __forceinline__ double2 *fft(double2 *buf0, double2 *buf1, const FftPlan &pl, int nsig,
+                                        int sig_stride, const double2 *tw, int sign) {
+  if constexpr (N == 0) {
+    return run(buf0, buf1, pl, nsig, sig_stride, tw, sign);
+  } else {
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    if (sign < 0) ippasses<N, -1, 0>(buf0, nsig, sig_stride, tw, tid, nthr);
+    else ippasses<N, +1, 0>(buf0, nsig, sig_stride, tw, tid, nthr);
+    return buf0;
+  }
+}
+
+// shared buffers a transform of length n needs (1 in place, 2 ping-pong)
+__host__ __device__ constexpr int fft_bufs(int n) {
+  return (n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 192 ||
+          n == 256 || n == 384 || n == 512) ? 1 : 2;
+}
+
 }  // namespace dgfft
+
+// Supported compile-time lengths; anything else takes the runtime plan.
+#define DG_FOR_EACH_N(X) X(16) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512)

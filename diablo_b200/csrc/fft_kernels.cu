@@ -12,6 +12,9 @@
 // transforms use the two-real-rows-per-complex-transform identity; the
 // imaginary parts of the x-DC and x-Nyquist bins are ignored by the c2r, as in
 // FFTW's complex-to-real.
+#include <mutex>
+#include <unordered_set>
+
 #include "dg_internal.cuh"
 #include "fft.cuh"
 
@@ -19,8 +22,12 @@ using namespace dgfft;
 
 namespace {
 
-constexpr int KXG = 8;     // kx columns per CTA in the z transforms
-constexpr int RPAIR = 4;   // row pairs per CTA in the x transforms
+// signals per CTA: 16 for lengths <= 128, fewer for longer transforms so the
+// two shared buffers stay near 70 KB
+__host__ __device__ constexpr int batch_for(int n) {
+  return n <= 128 ? 16 : (n <= 256 ? 8 : 4);
+}
+constexpr int NTHR = 128;
 
 __device__ __forceinline__ int packed_index(int z, int NZ, int NKZ) {
   // physical-order z bin -> packed kz slot, or -1 if not retained
@@ -29,11 +36,15 @@ __device__ __forceinline__ int packed_index(int z, int NZ, int NKZ) {
   return -1;
 }
 
-__global__ void k_zinv(CFieldPtrs fields, int jmin, long ss, int nkxp,
-                       int NZ, int NKZ, FftPlan pl, const double2 *__restrict__ tw,
-                       double2 *__restrict__ H, long Hfield) {
+template <int NT>
+__global__ void __launch_bounds__(NTHR) k_zinv(CFieldPtrs fields, int jmin, long ss, int nkxp,
+                                              int NZr, int NKZ, FftPlan pl,
+                                              const double2 *__restrict__ tw,
+                                              double2 *__restrict__ H, long Hfield) {
   extern __shared__ double2 sm[];
-  const int sstr = NZ + 1;
+  const int NZ = NT ? NT : NZr;
+  const int KXG = batch_for(NZ);
+  const int sstr = padded_len(NZ);
   double2 *stw = sm;
   double2 *b0 = stw + NZ;
   double2 *b1 = b0 + KXG * sstr;
@@ -48,22 +59,26 @@ __global__ void k_zinv(CFieldPtrs fields, int jmin, long ss, int nkxp,
     double2 v = make_double2(0.0, 0.0);
     const int kp = packed_index(z, NZ, NKZ);
     if (kp >= 0 && kx0 + c < nkxp) v = in[(long)kp * nkxp + kx0 + c];
-    b0[c * sstr + z] = v;
+    b0[c * sstr + pad(z)] = v;
   }
   __syncthreads();
-  double2 *res = run(b0, b1, pl, KXG, sstr, stw, +1);
+  double2 *res = fft<NT>(b0, b1, pl, KXG, sstr, stw, +1);
   double2 *out = H + f * Hfield + (long)j * NZ * nkxp;
   for (int idx = tid; idx < KXG * NZ; idx += nthr) {
     const int c = idx % KXG, z = idx / KXG;
-    if (kx0 + c < nkxp) out[(long)z * nkxp + kx0 + c] = res[c * sstr + z];
+    if (kx0 + c < nkxp) out[(long)z * nkxp + kx0 + c] = res[c * sstr + pad(z)];
   }
 }
 
-__global__ void k_zfwd(const double2 *__restrict__ H, long Hfield, int jmin, int nkxp, int nkzt,
-                       int NZ, int NKZ, FftPlan pl, const double2 *__restrict__ tw,
-                       FieldPtrs fields, long ss) {
+template <int NT>
+__global__ void __launch_bounds__(NTHR) k_zfwd(const double2 *__restrict__ H, long Hfield, int jmin,
+                                              int nkxp, int nkzt, int NZr, int NKZ, FftPlan pl,
+                                              const double2 *__restrict__ tw, FieldPtrs fields,
+                                              long ss) {
   extern __shared__ double2 sm[];
-  const int sstr = NZ + 1;
+  const int NZ = NT ? NT : NZr;
+  const int KXG = batch_for(NZ);
+  const int sstr = padded_len(NZ);
   double2 *stw = sm;
   double2 *b0 = stw + NZ;
   double2 *b1 = b0 + KXG * sstr;
@@ -77,27 +92,32 @@ __global__ void k_zfwd(const double2 *__restrict__ H, long Hfield, int jmin, int
     const int c = idx % KXG, z = idx / KXG;
     double2 v = make_double2(0.0, 0.0);
     if (kx0 + c < nkxp) v = in[(long)z * nkxp + kx0 + c];
-    b0[c * sstr + z] = v;
+    b0[c * sstr + pad(z)] = v;
   }
   __syncthreads();
-  double2 *res = run(b0, b1, pl, KXG, sstr, stw, -1);
+  double2 *res = fft<NT>(b0, b1, pl, KXG, sstr, stw, -1);
   double2 *out = fields.p[f] + (long)j * ss;
   const double rnz = (double)NZ;
   for (int idx = tid; idx < KXG * nkzt; idx += nthr) {
     const int c = idx % KXG, kp = idx / KXG;
     if (kx0 + c >= nkxp) continue;
     const int z = (kp <= NKZ) ? kp : (NZ - 1 + (kp - NKZ) - NKZ);
-    const double2 v = res[c * sstr + z];
+    const double2 v = res[c * sstr + pad(z)];
     out[(long)kp * nkxp + kx0 + c] = make_double2(v.x / rnz, v.y / rnz);
   }
 }
 
 // c2r of RPAIR row pairs of one plane of one field.
-__global__ void k_xc2r(const double2 *__restrict__ H, long Hfield, int jmin, int nkxp, int NX,
-                       int NZ, FftPlan pl, const double2 *__restrict__ tw, double *__restrict__ phys,
-                       long pplane, long prow, long pfield) {
+template <int NT>
+__global__ void __launch_bounds__(NTHR) k_xc2r(const double2 *__restrict__ H, long Hfield, int jmin,
+                                              int nkxp, int NXr, int NZ, FftPlan pl,
+                                              const double2 *__restrict__ tw,
+                                              double *__restrict__ phys, long pplane, long prow,
+                                              long pfield) {
   extern __shared__ double2 sm[];
-  const int sstr = NX + 1;
+  const int NX = NT ? NT : NXr;
+  const int RPAIR = batch_for(NX);
+  const int sstr = padded_len(NX);
   double2 *stw = sm;
   double2 *b0 = stw + NX;
   double2 *b1 = b0 + RPAIR * sstr;
@@ -128,26 +148,30 @@ __global__ void k_xc2r(const double2 *__restrict__ H, long Hfield, int jmin, int
           v = make_double2(a.x + b.y, -a.y + b.x);
       }
     }
-    b0[q * sstr + k] = v;
+    b0[q * sstr + pad(k)] = v;
   }
   __syncthreads();
-  double2 *res = run(b0, b1, pl, RPAIR, sstr, stw, +1);
+  double2 *res = fft<NT>(b0, b1, pl, RPAIR, sstr, stw, +1);
   double *out = phys + f * pfield + (long)j * pplane;
   for (int idx = tid; idx < RPAIR * NX; idx += nthr) {
     const int q = idx / NX, x = idx % NX;
     const int za = z0 + 2 * q, zb = za + 1;
-    const double2 v = res[q * sstr + x];
+    const double2 v = res[q * sstr + pad(x)];
     if (za < NZ) out[(long)za * prow + x] = v.x;
     if (zb < NZ) out[(long)zb * prow + x] = v.y;
   }
 }
 
 // r2c of RPAIR row pairs of one plane of one field; keeps kx = 0..NKX, / NX.
-__global__ void k_xr2c(const double *__restrict__ phys, long pplane, long prow, long pfield,
-                       int jmin, int nkxp, int NX, int NZ, FftPlan pl,
-                       const double2 *__restrict__ tw, double2 *__restrict__ H, long Hfield) {
+template <int NT>
+__global__ void __launch_bounds__(NTHR) k_xr2c(const double *__restrict__ phys, long pplane,
+                                              long prow, long pfield, int jmin, int nkxp, int NXr,
+                                              int NZ, FftPlan pl, const double2 *__restrict__ tw,
+                                              double2 *__restrict__ H, long Hfield) {
   extern __shared__ double2 sm[];
-  const int sstr = NX + 1;
+  const int NX = NT ? NT : NXr;
+  const int RPAIR = batch_for(NX);
+  const int sstr = padded_len(NX);
   double2 *stw = sm;
   double2 *b0 = stw + NX;
   double2 *b1 = b0 + RPAIR * sstr;
@@ -162,17 +186,17 @@ __global__ void k_xr2c(const double *__restrict__ phys, long pplane, long prow, 
     const int za = z0 + 2 * q, zb = za + 1;
     double a = (za < NZ) ? in[(long)za * prow + x] : 0.0;
     double b = (zb < NZ) ? in[(long)zb * prow + x] : 0.0;
-    b0[q * sstr + x] = make_double2(a, b);
+    b0[q * sstr + pad(x)] = make_double2(a, b);
   }
   __syncthreads();
-  double2 *res = run(b0, b1, pl, RPAIR, sstr, stw, -1);
+  double2 *res = fft<NT>(b0, b1, pl, RPAIR, sstr, stw, -1);
   double2 *out = H + f * Hfield + (long)j * NZ * nkxp;
   const double rnx = (double)NX;
   for (int idx = tid; idx < RPAIR * nkxp; idx += nthr) {
     const int q = idx / nkxp, k = idx % nkxp;
     const int za = z0 + 2 * q, zb = za + 1;
-    const double2 zk = res[q * sstr + k];
-    const double2 zm = res[q * sstr + ((NX - k) % NX)];
+    const double2 zk = res[q * sstr + pad(k)];
+    const double2 zm = res[q * sstr + pad((NX - k) % NX)];
     // A = (Z_k + conj Z_{N-k})/2, B = -i/2 (Z_k - conj Z_{N-k})
     const double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
     const double2 B = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
@@ -181,20 +205,46 @@ __global__ void k_xr2c(const double *__restrict__ phys, long pplane, long prow, 
   }
 }
 
-size_t zsmem(int NZ) { return sizeof(double2) * (NZ + 2 * KXG * (NZ + 1)); }
-size_t xsmem(int NX) { return sizeof(double2) * (NX + 2 * RPAIR * (NX + 1)); }
+size_t zsmem(int NZ) { return sizeof(double2) * (NZ + fft_bufs(NZ) * batch_for(NZ) * padded_len(NZ)); }
+size_t xsmem(int NX) { return sizeof(double2) * (NX + fft_bufs(NX) * batch_for(NX) * padded_len(NX)); }
+
+}  // namespace
+
+void dg_big_smem(const void *kern) {
+  static std::mutex mu;
+  static std::unordered_set<const void *> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.insert(kern).second)
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+}
+
+namespace {
+template <typename K>
+void big_smem(K kern) {
+  dg_big_smem((const void *)kern);
+}
 
 }  // namespace
 
 // ------------------------------------------------------------- host wrappers
+
 int dg_zinv(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax, double2 *H,
             int) {
   if (jmax < jmin || nf <= 0) return DG_OK;
   CFieldPtrs fp;
   for (int f = 0; f < nf; f++) fp.p[f] = fields[f];
-  dim3 grid(dg_cdiv(h->nkxp, KXG), jmax - jmin + 1, nf);
-  k_zinv<<<grid, 256, zsmem(h->NZ), h->st>>>(fp, jmin, h->ss, h->nkxp, h->NZ, h->NKZ, h->plz,
-                                             h->twz, H, (long)h->nplanes * h->NZ * h->nkxp);
+  dim3 grid(dg_cdiv(h->nkxp, batch_for(h->NZ)), jmax - jmin + 1, nf);
+  const size_t sm = zsmem(h->NZ);
+  const long Hf = (long)h->nplanes * h->NZ * h->nkxp;
+#define KERNEL_BODY(N)                                                                      \
+  big_smem(k_zinv<N>);                                                                      \
+  k_zinv<N><<<grid, NTHR, sm, h->st>>>(fp, jmin, h->ss, h->nkxp, h->NZ, h->NKZ, h->plz, h->twz, \
+                                      H, Hf)
+  switch (h->NZ) {
+    DG_FOR_EACH_N(DG_CASE_N)
+    default: KERNEL_BODY(0); break;
+  }
+#undef KERNEL_BODY
   DG_LAUNCHED();
   return DG_OK;
 }
@@ -204,9 +254,18 @@ int dg_zfwd_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax,
   if (jmax < jmin || nf <= 0) return DG_OK;
   FieldPtrs fp;
   for (int f = 0; f < nf; f++) fp.p[f] = fields[f];
-  dim3 grid(dg_cdiv(h->nkxp, KXG), jmax - jmin + 1, nf);
-  k_zfwd<<<grid, 256, zsmem(h->NZ), h->st>>>(H, (long)h->nplanes * h->NZ * h->nkxp, jmin, h->nkxp,
-                                             h->nkzt, h->NZ, h->NKZ, h->plz, h->twz, fp, h->ss);
+  dim3 grid(dg_cdiv(h->nkxp, batch_for(h->NZ)), jmax - jmin + 1, nf);
+  const size_t sm = zsmem(h->NZ);
+  const long Hf = (long)h->nplanes * h->NZ * h->nkxp;
+#define KERNEL_BODY(N)                                                                          \
+  big_smem(k_zfwd<N>);                                                                          \
+  k_zfwd<N><<<grid, NTHR, sm, h->st>>>(H, Hf, jmin, h->nkxp, h->nkzt, h->NZ, h->NKZ, h->plz, h->twz, \
+                                      fp, h->ss)
+  switch (h->NZ) {
+    DG_FOR_EACH_N(DG_CASE_N)
+    default: KERNEL_BODY(0); break;
+  }
+#undef KERNEL_BODY
   DG_LAUNCHED();
   return DG_OK;
 }
@@ -214,10 +273,18 @@ int dg_zfwd_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax,
 int dg_xc2r_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax, double *phys,
                    long pplane, long prow, long pfield) {
   if (jmax < jmin || nf <= 0) return DG_OK;
-  dim3 grid(dg_cdiv(h->NZ, 2 * RPAIR), jmax - jmin + 1, nf);
-  k_xc2r<<<grid, 256, xsmem(h->NX), h->st>>>(H, (long)h->nplanes * h->NZ * h->nkxp, jmin, h->nkxp,
-                                             h->NX, h->NZ, h->plx, h->twx, phys, pplane, prow,
-                                             pfield);
+  dim3 grid(dg_cdiv(h->NZ, 2 * batch_for(h->NX)), jmax - jmin + 1, nf);
+  const size_t sm = xsmem(h->NX);
+  const long Hf = (long)h->nplanes * h->NZ * h->nkxp;
+#define KERNEL_BODY(N)                                                                     \
+  big_smem(k_xc2r<N>);                                                                     \
+  k_xc2r<N><<<grid, NTHR, sm, h->st>>>(H, Hf, jmin, h->nkxp, h->NX, h->NZ, h->plx, h->twx, phys, \
+                                      pplane, prow, pfield)
+  switch (h->NX) {
+    DG_FOR_EACH_N(DG_CASE_N)
+    default: KERNEL_BODY(0); break;
+  }
+#undef KERNEL_BODY
   DG_LAUNCHED();
   return DG_OK;
 }
@@ -225,10 +292,18 @@ int dg_xc2r_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax, d
 int dg_xr2c_planes(dg_handle *h, const double *phys, int nf, int jmin, int jmax, long pplane,
                    long prow, long pfield, double2 *H) {
   if (jmax < jmin || nf <= 0) return DG_OK;
-  dim3 grid(dg_cdiv(h->NZ, 2 * RPAIR), jmax - jmin + 1, nf);
-  k_xr2c<<<grid, 256, xsmem(h->NX), h->st>>>(phys, pplane, prow, pfield, jmin, h->nkxp, h->NX,
-                                             h->NZ, h->plx, h->twx, H,
-                                             (long)h->nplanes * h->NZ * h->nkxp);
+  dim3 grid(dg_cdiv(h->NZ, 2 * batch_for(h->NX)), jmax - jmin + 1, nf);
+  const size_t sm = xsmem(h->NX);
+  const long Hf = (long)h->nplanes * h->NZ * h->nkxp;
+#define KERNEL_BODY(N)                                                                        \
+  big_smem(k_xr2c<N>);                                                                        \
+  k_xr2c<N><<<grid, NTHR, sm, h->st>>>(phys, pplane, prow, pfield, jmin, h->nkxp, h->NX, h->NZ,   \
+                                      h->plx, h->twx, H, Hf)
+  switch (h->NX) {
+    DG_FOR_EACH_N(DG_CASE_N)
+    default: KERNEL_BODY(0); break;
+  }
+#undef KERNEL_BODY
   DG_LAUNCHED();
   return DG_OK;
 }
@@ -239,7 +314,8 @@ bool dg_make_plan(int n, FftPlan *pl) {
   int m = n;
   while (m > 1) {
     int r;
-    if (m % 8 == 0) r = 8;
+    if (m % 16 == 0) r = 16;
+    else if (m % 8 == 0) r = 8;
     else if (m % 4 == 0) r = 4;
     else if (m % 2 == 0) r = 2;
     else if (m % 3 == 0) r = 3;

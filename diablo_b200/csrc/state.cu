@@ -251,9 +251,7 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
     DG_TRY(dalloc(&h->gphi, ns));
     DG_TRY(dalloc(&h->rem_a, ns));
     DG_TRY(dalloc(&h->rem_rb, ns));
-    DG_TRY(dalloc(&h->cn_tab, (size_t)(3 + DG_MAX_TH) * 4 * L));
-    DG_TRY(dalloc(&h->cn_kind, (size_t)(3 + DG_MAX_TH) * L));
-    DG_TRY(dalloc(&h->cn_bc, (size_t)(3 + DG_MAX_TH) * L));
+    DG_TRY(dalloc(&h->cn_tab, (size_t)3 * (3 + DG_MAX_TH) * 5 * L));
     const size_t hsz = (size_t)h->nplanes * h->NZ * h->nkxp;
     DG_TRY(dalloc(&h->H, hsz * h->nf));
     DG_TRY(dalloc(&h->G, hsz * 2 * h->nf));
@@ -274,8 +272,7 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
   if (!h) return DG_OK;
   cudaStreamSynchronize(h->st);
   void *dp[] = {h->gyf, h->dy, h->dyf, h->kx, h->kz, h->ky, h->kx2, h->kz2, h->ky2, h->twx, h->twz,
-                h->twy, h->dscal, h->cp, h->cr1, h->gphi, h->rem_a, h->rem_rb, h->cn_tab,
-                h->cn_kind, h->cn_bc, h->H, h->G, h->work, h->dmin_bits, h->dflag, h->Hy, h->P,
+                h->twy, h->dscal, h->cp, h->cr1, h->gphi, h->rem_a, h->rem_rb, h->cn_tab, h->cn_rows, h->H, h->G, h->work, h->dmin_bits, h->dflag, h->Hy, h->P,
                 h->Q};
   for (void *q : dp)
     if (q) cudaFree(q);
@@ -302,6 +299,7 @@ extern "C" int diablo_set_time(dg_handle *h, double time, double delta_t) {
   double s[5] = {time, delta_t, delta_t * (8.0 / 15.0), delta_t * (2.0 / 15.0),
                  delta_t * (5.0 / 15.0)};
   DG_CUDA(cudaMemcpyAsync(h->dscal, s, sizeof(s), cudaMemcpyHostToDevice, h->st));
+  if (h->cn_tab) DG_TRY(dg_cn_tables(h));
   DG_CUDA(cudaStreamSynchronize(h->st));
   return DG_OK;
 }

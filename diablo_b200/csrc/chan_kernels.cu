@@ -18,6 +18,7 @@
 //   k_rd_col    per mode tile: REM_DIV_CHAN's complex tridiagonal, projection
 //               and CP += phi / h (for/channel.f:1103-1214, 1059-1065)
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 #include "dg_internal.cuh"
 #include "fft.cuh"
@@ -240,6 +241,194 @@ size_t xrow_smem(const dg_handle *h) {
          sizeof(double) * 3 * XR_ROWS * nf * NX;
 }
 
+// ------------------------------------------------------- xrow, one warp/row
+// Same products as k_xrow_nl, organised so a warp owns one physical z-row and
+// marches up through its chunk of planes with no CTA-wide barrier: the two
+// physical planes it needs (j and j+1) live in registers (lane l holds
+// x = l + 32 i), the transforms run in a per-warp shared buffer with
+// __syncwarp between passes, and the x-spectra carried from one plane to the
+// next (fluxes at GY j, Ubar U2 at GY j, g at GYF j-1) live in registers
+// (lane l holds kx = l + 32 s).  At step j it forms the GYF-j products and
+// the GY-(j+1) products, so only planes j and j+1 are needed.
+constexpr int XW_WARPS = 4;
+
+__host__ __device__ constexpr bool xw_supported(int n) {
+  return n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 256;
+}
+
+template <int NX, int NTH>
+__global__ void __launch_bounds__(32 * XW_WARPS, 3) k_xrow_w(
+    ChanConst C, const double2 *__restrict__ H, long Hfield, int chunk, int jbase, int jtop,
+    const double2 *__restrict__ tw, const double *__restrict__ dyf, const double *__restrict__ dy,
+    const double *__restrict__ kxv, double2 *__restrict__ G, long Gfield) {
+  constexpr int NF = 3 + NTH;
+  constexpr int NPIN = (NF + 1) / 2;
+  constexpr int NPROD = 8 + 3 * NTH;
+  constexpr int NPP = (NPROD + 1) / 2;
+  constexpr int MAXP = NPIN > NPP ? NPIN : NPP;
+  constexpr int XPL = (NX + 31) / 32;              // physical points per lane
+  constexpr int NKXP = NX / 3 + 1;
+  constexpr int KS = (NKXP + 31) / 32;             // kx slots per lane
+  constexpr int SSTR = padded_len(NX);
+  extern __shared__ double2 sm[];
+  double2 *stw = sm;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2 *buf = stw + NX + warp * MAXP * SSTR;
+  // carried x-spectra: 0 fl1, 1 fl3, 2 ubar1 u2, 3 ubar3 u2, 4 g, 5+n flth
+  double2 *pvs = stw + NX + XW_WARPS * MAXP * SSTR + warp * (5 + NTH) * NKXP;
+  for (int i = threadIdx.x; i < NX; i += blockDim.x) stw[i] = tw[i];
+  __syncthreads();
+  const int z = blockIdx.x * XW_WARPS + warp;
+  const int NZ = C.NZ;
+  if (z >= NZ) return;
+  const int j0 = jbase + blockIdx.y * chunk;
+  int j1 = j0 + chunk - 1;
+  if (j1 > jtop) j1 = jtop;
+  const double rnx = 1.0 / (double)NX;            // exact: NX is 2^a 3^b ... see below
+  const bool pow2 = (NX & (NX - 1)) == 0;
+  const long plane = (long)NZ * NKXP;
+
+  double cur[NF][XPL], nxt[NF][XPL];
+#define PV(q, s) pvs[(q) * NKXP + lane + 32 * (s)]
+
+  auto load_plane = [&](int pl, double (&dst)[NF][XPL]) {
+    const double2 *row = H + (long)pl * plane + (long)z * NKXP;
+#pragma unroll
+    for (int q = 0; q < NPIN; q++) {
+      const int fa = 2 * q, fb = 2 * q + 1;
+#pragma unroll
+      for (int i = 0; i < (NX + 31) / 32; i++) {
+        const int k = lane + 32 * i;
+        if (k < NX) {
+          const int kk = (k <= NX / 2) ? k : NX - k;
+          double2 v = make_double2(0.0, 0.0);
+          if (kk < NKXP && kk < NX / 2) {
+            double2 a = row[fa * Hfield + kk];
+            double2 bb = (fb < NF) ? row[fb * Hfield + kk] : make_double2(0.0, 0.0);
+            if (kk == 0) { a.y = 0.0; bb.y = 0.0; }
+            v = (k == kk) ? make_double2(a.x - bb.y, a.y + bb.x)
+                          : make_double2(a.x + bb.y, -a.y + bb.x);
+          }
+          buf[q * SSTR + pad(k)] = v;
+        }
+      }
+    }
+    __syncwarp();
+    wpasses<NX, +1, 0>(buf, NPIN, SSTR, stw, lane);
+#pragma unroll
+    for (int q = 0; q < NPIN; q++)
+#pragma unroll
+      for (int i = 0; i < XPL; i++) {
+        const int x = lane + 32 * i;
+        const double2 v = (x < NX) ? buf[q * SSTR + pad(x)] : make_double2(0.0, 0.0);
+        dst[2 * q][i] = v.x;
+        if (2 * q + 1 < NF) dst[2 * q + 1][i] = v.y;
+      }
+    __syncwarp();
+  };
+
+  load_plane(j0 - 1, cur);
+  for (int j = j0 - 1; j <= j1; j++) {
+    load_plane(j + 1, nxt);
+    const double dyf_j = dyf[j], dyf_p = dyf[j + 1], dy_p = dy[j + 1];
+    const double wgy = 1.0 / (2. * dy_p);
+    // products: GYF j (U1U3, U1U1, U3U3, g, TH U1, TH U3) and GY j+1 (fl1, fl3,
+    // ubar1 u2, ubar3 u2, flth)
+#pragma unroll
+    for (int i = 0; i < XPL; i++) {
+      const int x = lane + 32 * i;
+      if (x >= NX) continue;
+      const double u1 = cur[0][i], u2 = cur[1][i], u3 = cur[2][i];
+      const double u1p = nxt[0][i], u2p = nxt[1][i], u3p = nxt[2][i];
+      double P[2 * NPP];
+      P[0] = u3 * u1;
+      P[1] = u1 * u1;
+      P[2] = u3 * u3;
+      { const double s = u2 + u2p; P[3] = 0.25 * (s * s); }
+      P[4] = (u1p + u1) * u2p;
+      P[5] = (u3p + u3) * u2p;
+      P[6] = ((dyf_p * u1p + dyf_j * u1) * wgy) * u2p;
+      P[7] = ((dyf_p * u3p + dyf_j * u3) * wgy) * u2p;
+#pragma unroll
+      for (int n = 0; n < NTH; n++) {
+        const double t = cur[3 + n][i], tp = nxt[3 + n][i];
+        P[8 + 3 * n] = t * u1;
+        P[9 + 3 * n] = t * u3;
+        P[10 + 3 * n] = (tp + t) * u2p;
+      }
+      if (2 * NPP > NPROD) P[2 * NPP - 1] = 0.0;
+#pragma unroll
+      for (int q = 0; q < NPP; q++) buf[q * SSTR + pad(x)] = make_double2(P[2 * q], P[2 * q + 1]);
+    }
+    __syncwarp();
+    wpasses<NX, -1, 0>(buf, NPP, SSTR, stw, lane);
+    const bool out = (j >= j0);
+    const double d2 = 2.0 * dyf_j, dyj = dy[j];
+#pragma unroll
+    for (int s = 0; s < KS; s++) {
+      const int k = lane + 32 * s;
+      if (k >= NKXP) continue;
+      auto X = [&](int p) -> double2 {
+        const int q = p >> 1;
+        const double2 zk = buf[q * SSTR + pad(k)];
+        const double2 zm = buf[q * SSTR + pad((NX - k) % NX)];
+        double2 v;
+        if ((p & 1) == 0) v = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+        else v = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
+        if (pow2) return make_double2(v.x * rnx, v.y * rnx);
+        return make_double2(v.x / (double)NX, v.y / (double)NX);
+      };
+      const double KX = kxv[k];
+      auto mikx = [&](double2 a) { return make_double2(KX * a.y, -KX * a.x); };  // -i kx a
+      const double2 x3 = X(3), x4 = X(4), x5 = X(5), x6 = X(6), x7 = X(7);
+      if (out) {
+        const long off = (long)j * NZ * NKXP + (long)z * NKXP + k;
+        const double2 x0 = X(0), x1 = X(1), x2 = X(2);
+        // U1: A = U1U3, B = -ikx U1U1 - (fl1(j+1) - fl1(j)) / (2 DYF(j))
+        G[0 * Gfield + off] = x0;
+        double2 t = mikx(x1);
+        G[1 * Gfield + off] = make_double2(t.x - (x4.x - PV(0, s).x) / d2, t.y - (x4.y - PV(0, s).y) / d2);
+        // U2 (GY j): A = ubar3 u2(j), B = -ikx ubar1 u2(j) - (g(j) - g(j-1)) / DY(j)
+        G[2 * Gfield + off] = PV(3, s);
+        t = mikx(PV(2, s));
+        G[3 * Gfield + off] = make_double2(t.x - (x3.x - PV(4, s).x) / dyj, t.y - (x3.y - PV(4, s).y) / dyj);
+        // U3: A = U3U3, B = -ikx U1U3 - (fl3(j+1) - fl3(j)) / (2 DYF(j))
+        G[4 * Gfield + off] = x2;
+        t = mikx(x0);
+        G[5 * Gfield + off] = make_double2(t.x - (x5.x - PV(1, s).x) / d2, t.y - (x5.y - PV(1, s).y) / d2);
+#pragma unroll
+        for (int n = 0; n < NTH; n++) {
+          const double2 a = X(8 + 3 * n), b = X(9 + 3 * n), c = X(10 + 3 * n);
+          G[(6 + 2 * n) * Gfield + off] = b;
+          t = mikx(a);
+          G[(7 + 2 * n) * Gfield + off] =
+              make_double2(t.x - (c.x - PV(5 + n, s).x) / d2, t.y - (c.y - PV(5 + n, s).y) / d2);
+        }
+      }
+      PV(0, s) = x4;
+      PV(1, s) = x5;
+      PV(2, s) = x6;
+      PV(3, s) = x7;
+      PV(4, s) = x3;
+#pragma unroll
+      for (int n = 0; n < NTH; n++) PV(5 + n, s) = X(10 + 3 * n);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int f = 0; f < NF; f++)
+#pragma unroll
+      for (int i = 0; i < XPL; i++) cur[f][i] = nxt[f][i];
+  }
+#undef PV
+}
+
+template <int NX, int NTH>
+size_t xw_smem() {
+  constexpr int NF = 3 + NTH, NPIN = (NF + 1) / 2, NPP = (8 + 3 * NTH + 1) / 2;
+  constexpr int MAXP = NPIN > NPP ? NPIN : NPP;
+  return sizeof(double2) * (NX + XW_WARPS * MAXP * padded_len(NX) + XW_WARPS * (5 + NTH) * (NX / 3 + 1));
+}
+
 // ------------------------------------------------------------- zfwd + rhs
 constexpr int ZF_THR = 128;
 __host__ __device__ constexpr int zf_kxg(int nz) { return nz <= 128 ? 8 : (nz <= 256 ? 4 : 2); }
@@ -403,6 +592,177 @@ __global__ void __launch_bounds__(ZF_THR) k_zfwd_rhs(
   }
 }
 
+// Warp-per-column-pair variant: a CTA of four warps takes 8 kx columns of one
+// field on one plane; the A and B columns are staged with one coalesced load,
+// then each warp transforms its 2 x (A, B) signals and finishes those modes.
+constexpr int ZW_KXG = 8;
+
+template <int NZ>
+__global__ void __launch_bounds__(128, 4) k_zfwd_w(
+    ChanConst C, const double2 *__restrict__ G, long Gfield, const double2 *__restrict__ tw,
+    const double *__restrict__ dscal, int rk_step, const double *__restrict__ kxv,
+    const double *__restrict__ kzv, const double *__restrict__ dy, const double *__restrict__ dyf,
+    FieldPtrs cu, FieldPtrs cf, FieldPtrs rhs, const double2 *__restrict__ cp, int jbase) {
+  constexpr int SSTR = padded_len(NZ);
+  extern __shared__ double2 sm[];
+  double2 *stw = sm;
+  double2 *buf = stw + NZ;                     // [warp][A0 A1 B0 B1][SSTR]
+  const int nkxp = C.nkxp, nkzt = C.nkzt, NKZ = C.NKZ;
+  const int kx0 = blockIdx.x * ZW_KXG;
+  const int j = jbase + blockIdx.y;
+  const int f = blockIdx.z;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // skip planes outside this field's rows
+  const int jlo = (f == 0 || f == 2) ? C.JS : (f == 1 ? 2 : C.JSt[f - 3]);
+  const int jhi = (f == 0 || f == 2) ? C.JE : (f == 1 ? C.NY : C.JEt[f - 3]);
+  if (j < jlo || j > jhi) return;
+  for (int i = threadIdx.x; i < NZ; i += blockDim.x) stw[i] = tw[i];
+  const double2 *GA = G + (2 * f) * Gfield + (long)j * NZ * nkxp;
+  const double2 *GB = G + (2 * f + 1) * Gfield + (long)j * NZ * nkxp;
+  for (int base = 0; base < 2 * ZW_KXG * NZ; base += 8 * 128) {
+    double2 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int i = base + u * 128 + threadIdx.x;
+      const int c = i % ZW_KXG, z = (i / ZW_KXG) % NZ, ab = i / (ZW_KXG * NZ);
+      v[u] = (i < 2 * ZW_KXG * NZ && kx0 + c < nkxp) ? (ab ? GB : GA)[(long)z * nkxp + kx0 + c]
+                                                     : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int i = base + u * 128 + threadIdx.x;
+      if (i >= 2 * ZW_KXG * NZ) continue;
+      const int c = i % ZW_KXG, z = (i / ZW_KXG) % NZ, ab = i / (ZW_KXG * NZ);
+      const int w = c >> 1, s = (ab << 1) | (c & 1);
+      buf[(w * 4 + s) * SSTR + pad(z)] = v[u];
+    }
+  }
+  __syncthreads();
+  double2 *wb = buf + warp * 4 * SSTR;
+  wpasses<NZ, -1, 0>(wb, 4, SSTR, stw, lane);
+
+  const double h = dscal[1 + rk_step];
+  const double time = dscal[0];
+  const double zeta = (rk_step == 2) ? -17.0 / 8.0 : (rk_step == 3) ? -5.0 / 4.0 : 0.0;
+  const double bbar = (rk_step == 2) ? 25.0 / 8.0 : (rk_step == 3) ? 9.0 / 4.0 : 1.0;
+  const double T1 = C.nu * h / 2.0, T3 = zeta * h, T4 = h, T5 = bbar * h;
+  const double NU = C.nu, NUV = C.nuv;
+  const long ss = C.ss;
+  const double dyj = dy[j], dyj1 = dy[j + 1], dyfj = dyf[j], dyfm = dyf[j - 1];
+  const double rnz = (double)NZ;
+  for (int it = lane; it < 2 * nkzt; it += 32) {
+    const int cc = it & 1, kp = it >> 1;
+    const int kx = kx0 + 2 * warp + cc;
+    if (kx >= nkxp) continue;
+    const int z = (kp <= NKZ) ? kp : (NZ - 1 + (kp - NKZ) - NKZ);
+    double2 a = wb[(0 + cc) * SSTR + pad(z)], b = wb[(2 + cc) * SSTR + pad(z)];
+    a = make_double2(a.x / rnz, a.y / rnz);
+    b = make_double2(b.x / rnz, b.y / rnz);
+    const double KX = kxv[kx], KZ = kzv[kp];
+    const double2 nlv = make_double2(KZ * a.y + b.x, -KZ * a.x + b.y);  // -i kz A + B
+    const long o = (long)j * ss + (long)kp * nkxp + kx;
+    const double k2 = KX * KX + KZ * KZ;
+    const double kk = (C.beta == 1.0) ? k2 : pow(k2, C.beta);
+    const bool mean = (kx == 0 && kp == 0);
+    if (f == 0 || f == 2) {
+      // U1 / U3 (rows JSTART..JEND)
+      const double2 u = cu.p[f][o], um = cu.p[f][o - ss], up = cu.p[f][o + ss];
+      const double2 uo = cu.p[2 - f][o];  // the other horizontal component (Coriolis)
+      const double sgn = (f == 0) ? 1.0 : -1.0;
+      const double gr = (f == 0) ? C.grav_x : C.grav_z;
+      double2 fv = make_double2(-NU * kk * u.x + sgn * C.i_ro * uo.x, -NU * kk * u.y + sgn * C.i_ro * uo.y);
+      for (int n = 0; n < C.nth; n++) {
+        const double2 t = cu.p[3 + n][o];
+        fv.x += C.ri[n] * gr * t.x;
+        fv.y += C.ri[n] * gr * t.y;
+      }
+      fv.x += nlv.x;
+      fv.y += nlv.y;
+      double2 r = u;
+      if (rk_step > 1) {
+        const double2 old = cf.p[f][o];
+        r.x += T3 * old.x;
+        r.y += T3 * old.y;
+      }
+      const double2 p0 = cp[o];
+      const double K = (f == 0) ? KX : KZ;
+      r.x -= T4 * (-K * p0.y);
+      r.y -= T4 * (K * p0.x);
+      if (mean && f == 0) {
+        if (C.f_type == 1) r.x -= T4 * C.px0;
+        else if (C.f_type == 2) r.x -= T4 * (C.px0 + C.amp_omega0 * cos(C.omega0 * time));
+      }
+      r.x += T5 * fv.x;
+      r.y += T5 * fv.y;
+      const double aa = T1 * NUV;
+      r.x += aa * (((up.x - u.x) / dyj1 - (u.x - um.x) / dyj) / dyfj);
+      r.y += aa * (((up.y - u.y) / dyj1 - (u.y - um.y) / dyj) / dyfj);
+      cf.p[f][o] = fv;
+      rhs.p[f][o] = r;
+    } else if (f == 1) {
+      // U2 (rows 2..NY)
+      const double2 u = cu.p[1][o], um = cu.p[1][o - ss], up = cu.p[1][o + ss];
+      double2 fv = make_double2(-NU * kk * u.x, -NU * kk * u.y);
+      if (!mean) {
+        for (int n = 0; n < C.nth; n++) {
+          const double2 t = cu.p[3 + n][o], tm = cu.p[3 + n][o - ss];
+          const double w = C.ri[n] * C.grav_y;
+          fv.x += w * (t.x * dyfm + tm.x * dyfj) / (2.0 * dyj);
+          fv.y += w * (t.y * dyfm + tm.y * dyfj) / (2.0 * dyj);
+        }
+      }
+      fv.x += nlv.x;
+      fv.y += nlv.y;
+      double2 r = u;
+      if (rk_step > 1) {
+        const double2 old = cf.p[1][o];
+        r.x += T3 * old.x;
+        r.y += T3 * old.y;
+      }
+      const double2 p0 = cp[o], pm = cp[o - ss];
+      r.x -= T4 * ((p0.x - pm.x) / dyj);
+      r.y -= T4 * ((p0.y - pm.y) / dyj);
+      r.x += T5 * fv.x;
+      r.y += T5 * fv.y;
+      const double aa = T1 * NUV;
+      r.x += aa * (((up.x - u.x) / dyfj - (u.x - um.x) / dyfm) / dyj);
+      r.y += aa * (((up.y - u.y) / dyfj - (u.y - um.y) / dyfm) / dyj);
+      cf.p[1][o] = fv;
+      rhs.p[1][o] = r;
+    } else {
+      // scalar n (rows JSTART_TH..JEND_TH)
+      const int n = f - 3;
+      const double2 t = cu.p[f][o], tm = cu.p[f][o - ss], tp = cu.p[f][o + ss];
+      const double nup = NU / C.pr[n];
+      double2 fv = make_double2(-nup * kk * t.x, -nup * kk * t.y);
+      if (C.drhodx[n] != 0.0 || C.drhodz[n] != 0.0) {
+        const double2 u1 = cu.p[0][o], u3 = cu.p[2][o];
+        fv.x = fv.x - u1.x * C.drhodx[n] - u3.x * C.drhodz[n];
+        fv.y = fv.y - u1.y * C.drhodx[n] - u3.y * C.drhodz[n];
+      }
+      fv.x += nlv.x;
+      fv.y += nlv.y;
+      double2 r = t;
+      if (rk_step > 1) {
+        const double2 old = cf.p[f][o];
+        r.x += T3 * old.x;
+        r.y += T3 * old.y;
+      }
+      r.x += T5 * fv.x;
+      r.y += T5 * fv.y;
+      const double aa = (T1 / C.pr[n]) * NUV;
+      r.x += aa * (((tp.x - t.x) / dyj1 - (t.x - tm.x) / dyj) / dyfj);
+      r.y += aa * (((tp.y - t.y) / dyj1 - (t.y - tm.y) / dyj) / dyfj);
+      cf.p[f][o] = fv;
+      rhs.p[f][o] = r;
+    }
+  }
+}
+
+__host__ __device__ constexpr bool zw_supported(int n) {
+  return n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 256;
+}
+
 size_t zfwd_smem(const dg_handle *h) {
   const int kxg = zf_kxg(h->NZ);
   return sizeof(double2) * (h->NZ + fft_bufs(h->NZ) * 2 * kxg * padded_len(h->NZ) +
@@ -530,9 +890,20 @@ __global__ void __launch_bounds__(COL_THR) k_cn_col(int NY, long ss, const doubl
   const int tid = threadIdx.x;
   const double *T = tab_rk + (long)f * 5 * L;
   for (int i = tid; i < 5 * L; i += COL_THR) TB[i] = T[i];
-  for (int i = tid; i < L * COL_MT; i += COL_THR) {
-    const int m = i % COL_MT, j = i / COL_MT;
-    X[i] = (m < mt) ? R[(long)j * ss + m0 + m] : make_double2(0.0, 0.0);
+  // staging with eight loads in flight per thread
+  for (int base = 0; base < L * COL_MT; base += 8 * COL_THR) {
+    double2 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int i = base + u * COL_THR + tid;
+      const int m = i % COL_MT, j = i / COL_MT;
+      v[u] = (i < L * COL_MT && m < mt) ? R[(long)j * ss + m0 + m] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int i = base + u * COL_THR + tid;
+      if (i < L * COL_MT) X[i] = v[u];
+    }
   }
   __syncthreads();
   if (tid < 2 * COL_MT) {
@@ -540,22 +911,51 @@ __global__ void __launch_bounds__(COL_THR) k_cn_col(int NY, long ss, const doubl
     const double *Aa = TB, *Rb = TB + L, *Cc = TB + 2 * L, *K = TB + 3 * L, *V = TB + 4 * L;
     double *x = (double *)X + tid;
     constexpr int st = 2 * COL_MT;
+    constexpr int B = 8;  // rows per register block: loads first, then the recurrence
     const bool mean_re = (m0 + m == 0) && part == 0;
     double g = 0.0;
-#pragma unroll 8
-    for (int j = 0; j < L; j++) {
-      const double kind = K[j];
-      const double xr = x[j * st];
-      const double r = (kind == (double)ROW_RHS) ? xr : ((kind == (double)ROW_BC && mean_re) ? V[j] : 0.0);
-      g = r + Aa[j] * g;
-      x[j * st] = g;
+    for (int j0 = 0; j0 < L; j0 += B) {
+      double r[B], a[B];
+#pragma unroll
+      for (int q = 0; q < B; q++) {
+        const int j = j0 + q < L ? j0 + q : L - 1;
+        const double kind = K[j];
+        const double xr = x[j * st];
+        r[q] = (kind == (double)ROW_RHS) ? xr : ((kind == (double)ROW_BC && mean_re) ? V[j] : 0.0);
+        a[q] = Aa[j];
+      }
+#pragma unroll
+      for (int q = 0; q < B; q++) {
+        if (j0 + q < L) {
+          g = r[q] + a[q] * g;
+          r[q] = g;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < B; q++)
+        if (j0 + q < L) x[(j0 + q) * st] = r[q];
     }
     double xv = g * Rb[L - 1];
     x[(L - 1) * st] = xv;
-#pragma unroll 8
-    for (int j = L - 2; j >= wlo; j--) {
-      xv = (x[j * st] - Cc[j] * xv) * Rb[j];
-      x[j * st] = xv;
+    for (int j1 = L - 2; j1 >= wlo; j1 -= B) {
+      double gq[B], cq[B], rq[B];
+#pragma unroll
+      for (int q = 0; q < B; q++) {
+        const int j = j1 - q >= wlo ? j1 - q : wlo;
+        gq[q] = x[j * st];
+        cq[q] = Cc[j];
+        rq[q] = Rb[j];
+      }
+#pragma unroll
+      for (int q = 0; q < B; q++) {
+        if (j1 - q >= wlo) {
+          xv = (gq[q] - cq[q] * xv) * rq[q];
+          gq[q] = xv;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < B; q++)
+        if (j1 - q >= wlo) x[(j1 - q) * st] = gq[q];
     }
   }
   __syncthreads();
@@ -583,26 +983,40 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
   double *UU = RB + (long)L * COL_MT;               // [j] upper diagonal rows 2..NY-1
   const int tid = threadIdx.x;
   for (int j = tid; j < L; j += COL_THR) UU[j] = (j >= 2 && j < NY) ? 1. / (dy[j + 1] * dyf[j]) : 0.0;
-  for (int i = tid; i < L * COL_MT; i += COL_THR) {
-    const int m = i % COL_MT, j = i / COL_MT;
-    const long mg = m0 + m;
-    double2 r = make_double2(0.0, 0.0);
-    double a = 0.0, b = 0.0;
-    if (m < mt && j >= 1 && j <= NY) {
-      const long o = (long)j * ss + mg;
-      a = ra[o];
-      b = rrb[o];
-      if (j >= 2 && j < NY) {
-        const double KX = kxv[mg % nkxp], KZ = kzv[mg / nkxp];
-        const double2 a1 = u1[o], a3 = u3[o], b2 = u2[o], b2p = u2[o + ss];
-        const double d = dyf[j];
-        r.x = (-KX * a1.y) + (b2p.x - b2.x) / d + (-KZ * a3.y);
-        r.y = (KX * a1.x) + (b2p.y - b2.y) / d + (KZ * a3.x);
-      }
+  for (int base = 0; base < L * COL_MT; base += 4 * COL_THR) {
+    double2 a1[4], a3[4], b2[4], b2p[4];
+    double av[4], bv[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int i = base + u * COL_THR + tid;
+      const int m = i % COL_MT, j = i / COL_MT;
+      const bool ok = i < L * COL_MT && m < mt && j >= 1 && j <= NY;
+      const bool in = ok && j >= 2 && j < NY;
+      const long o = (long)j * ss + m0 + m;
+      av[u] = ok ? ra[o] : 0.0;
+      bv[u] = ok ? rrb[o] : 0.0;
+      a1[u] = in ? u1[o] : make_double2(0.0, 0.0);
+      a3[u] = in ? u3[o] : make_double2(0.0, 0.0);
+      b2[u] = in ? u2[o] : make_double2(0.0, 0.0);
+      b2p[u] = in ? u2[o + ss] : make_double2(0.0, 0.0);
     }
-    GX[i] = r;
-    RA[i] = a;
-    RB[i] = b;
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int i = base + u * COL_THR + tid;
+      if (i >= L * COL_MT) continue;
+      const int m = i % COL_MT, j = i / COL_MT;
+      const long mg = m0 + m;
+      double2 r = make_double2(0.0, 0.0);
+      if (m < mt && j >= 2 && j < NY) {
+        const double KX = kxv[mg % nkxp], KZ = kzv[mg / nkxp];
+        const double d = dyf[j];
+        r.x = (-KX * a1[u].y) + (b2p[u].x - b2[u].x) / d + (-KZ * a3[u].y);
+        r.y = (KX * a1[u].x) + (b2p[u].y - b2[u].y) / d + (KZ * a3[u].x);
+      }
+      GX[i] = r;
+      RA[i] = av[u];
+      RB[i] = bv[u];
+    }
   }
   __syncthreads();
   if (tid < 2 * COL_MT) {
@@ -610,19 +1024,49 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
     const bool mean = (m0 + m == 0);
     double *x = (double *)GX + tid;
     constexpr int st = 2 * COL_MT;
+    constexpr int B = 8;
     double g = 0.0;  // row 1 has a zero right-hand side
     x[1 * st] = 0.0;
-#pragma unroll 8
-    for (int j = 2; j <= NY; j++) {
-      g = x[j * st] + RA[j * COL_MT + m] * g;
-      x[j * st] = g;
+    for (int j0 = 2; j0 <= NY; j0 += B) {
+      double r[B], a[B];
+#pragma unroll
+      for (int q = 0; q < B; q++) {
+        const int j = j0 + q <= NY ? j0 + q : NY;
+        r[q] = x[j * st];
+        a[q] = RA[j * COL_MT + m];
+      }
+#pragma unroll
+      for (int q = 0; q < B; q++) {
+        if (j0 + q <= NY) {
+          g = r[q] + a[q] * g;
+          r[q] = g;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < B; q++)
+        if (j0 + q <= NY) x[(j0 + q) * st] = r[q];
     }
     double ph = g * RB[NY * COL_MT + m];
     x[NY * st] = ph;
-#pragma unroll 8
-    for (int j = NY - 1; j >= 2; j--) {
-      ph = (x[j * st] - UU[j] * ph) * RB[j * COL_MT + m];
-      x[j * st] = ph;
+    for (int j1 = NY - 1; j1 >= 2; j1 -= B) {
+      double gq[B], uq[B], bq[B];
+#pragma unroll
+      for (int q = 0; q < B; q++) {
+        const int j = j1 - q >= 2 ? j1 - q : 2;
+        gq[q] = x[j * st];
+        uq[q] = UU[j];
+        bq[q] = RB[j * COL_MT + m];
+      }
+#pragma unroll
+      for (int q = 0; q < B; q++) {
+        if (j1 - q >= 2) {
+          ph = (gq[q] - uq[q] * ph) * bq[q];
+          gq[q] = ph;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < B; q++)
+        if (j1 - q >= 2) x[(j1 - q) * st] = gq[q];
     }
     const double u1r = mean ? 0.0 : -1.0;
     ph = (x[1 * st] - u1r * ph) * RB[1 * COL_MT + m];
@@ -630,32 +1074,45 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
   }
   __syncthreads();
   const double hh = (rk_step > 0) ? dscal[1 + rk_step] : 1.0;
-  for (int i = tid; i < L * COL_MT; i += COL_THR) {
-    const int m = i % COL_MT, j = i / COL_MT;
-    if (m >= mt || j < 1 || j > NY) continue;
-    const long mg = m0 + m, o = (long)j * ss + mg;
-    const double KX = kxv[mg % nkxp], KZ = kzv[mg / nkxp];
-    const double2 ph = GX[i];
-    double2 a1 = u1[o], a3 = u3[o];
-    // U1 -= i kx phi, U3 -= i kz phi
-    a1.x -= -KX * ph.y; a1.y -= KX * ph.x;
-    a3.x -= -KZ * ph.y; a3.y -= KZ * ph.x;
-    u1[o] = a1;
-    u3[o] = a3;
-    if (j >= 2) {
-      // U2(j) -= (phi(j) - phi(j-1)) / DY(j)
-      const double2 pm = GX[i - COL_MT];
-      double2 b = u2[o];
-      b.x -= (ph.x - pm.x) / dy[j];
-      b.y -= (ph.y - pm.y) / dy[j];
-      u2[o] = b;
+  for (int base = 0; base < L * COL_MT; base += 4 * COL_THR) {
+    double2 a1[4], a3[4], b2[4], pc[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int i = base + u * COL_THR + tid;
+      const int m = i % COL_MT, j = i / COL_MT;
+      const bool ok = i < L * COL_MT && m < mt && j >= 1 && j <= NY;
+      const long o = (long)j * ss + m0 + m;
+      a1[u] = ok ? u1[o] : make_double2(0.0, 0.0);
+      a3[u] = ok ? u3[o] : make_double2(0.0, 0.0);
+      b2[u] = (ok && j >= 2) ? u2[o] : make_double2(0.0, 0.0);
+      pc[u] = (ok && rk_step > 0 && j >= JS && j <= JE) ? cp[o] : make_double2(0.0, 0.0);
     }
-    phi_out[o] = ph;
-    if (rk_step > 0 && j >= JS && j <= JE) {
-      double2 p = cp[o];
-      p.x = p.x + ph.x / hh;
-      p.y = p.y + ph.y / hh;
-      cp[o] = p;
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int i = base + u * COL_THR + tid;
+      const int m = i % COL_MT, j = i / COL_MT;
+      if (i >= L * COL_MT || m >= mt || j < 1 || j > NY) continue;
+      const long mg = m0 + m, o = (long)j * ss + mg;
+      const double KX = kxv[mg % nkxp], KZ = kzv[mg / nkxp];
+      const double2 ph = GX[i];
+      // U1 -= i kx phi, U3 -= i kz phi
+      a1[u].x -= -KX * ph.y; a1[u].y -= KX * ph.x;
+      a3[u].x -= -KZ * ph.y; a3[u].y -= KZ * ph.x;
+      u1[o] = a1[u];
+      u3[o] = a3[u];
+      if (j >= 2) {
+        // U2(j) -= (phi(j) - phi(j-1)) / DY(j)
+        const double2 pm = GX[i - COL_MT];
+        b2[u].x -= (ph.x - pm.x) / dy[j];
+        b2[u].y -= (ph.y - pm.y) / dy[j];
+        u2[o] = b2[u];
+      }
+      phi_out[o] = ph;
+      if (rk_step > 0 && j >= JS && j <= JE) {
+        pc[u].x = pc[u].x + ph.x / hh;
+        pc[u].y = pc[u].y + ph.y / hh;
+        cp[o] = pc[u];
+      }
     }
   }
 }
@@ -940,6 +1397,10 @@ int dg_apply_bc_vel_dev(dg_handle *h) {
 }
 
 int dg_cn_solve_dev(dg_handle *h, int rk_step) {
+  if (h->tables_pending) {
+    DG_CUDA(cudaStreamWaitEvent(h->st, h->ev_join, 0));
+    h->tables_pending = false;
+  }
   FieldPtrs cu, rhs;
   for (int f = 0; f < h->nf; f++) { cu.p[f] = h->cu[f]; rhs.p[f] = h->rhs[f]; }
   int wl[8] = {1, 1, 1, 1, 1, 1, 1, 1};
@@ -993,17 +1454,10 @@ static double courant_dt0(const dg_handle *h) {
 }
 
 int dg_courant_dev(dg_handle *h, const double2 *const *u) {
-  // physical U1..U3 on planes 1..NY into the work array
+  // physical U1..U3 on planes 1..NY, reduced to COURANT's minimum on the fly
   DG_TRY(dg_zinv(h, u, 3, 1, h->NY, h->H, 0));
-  const long pplane = (long)h->NZ * h->NX;
-  const long pfield = (long)h->NY * pplane;
-  double *phys = (double *)h->work;
-  // dg_xc2r_planes addresses phys + f*pfield + j*pplane; shift so plane 1 lands at 0
-  DG_TRY(dg_xc2r_planes(h, h->H, 3, 1, h->NY, phys - pplane, pplane, h->NX, pfield));
   DG_CUDA(cudaMemsetAsync(h->dmin_bits, 0x7f, sizeof(unsigned long long), h->st));
-  k_cfl_min<<<4 * 148, 256, 0, h->st>>>(phys, pfield, h->NY, h->NZ, h->NX, h->p.cfl,
-                                        h->p.lx / h->NX, h->p.lz / h->NZ, h->dy, h->dmin_bits);
-  DG_LAUNCHED();
+  DG_TRY(dg_xc2r_cfl(h, h->H, 1, h->NY, h->dmin_bits));
   k_dt_update<<<1, 1, 0, h->st>>>(h->dscal, h->dmin_bits, courant_dt0(h));
   DG_LAUNCHED();
   return DG_OK;
@@ -1012,7 +1466,18 @@ int dg_courant_dev(dg_handle *h, const double2 *const *u) {
 int dg_dt_commit(dg_handle *h) {
   k_dt_commit<<<1, 1, 0, h->st>>>(h->dscal);
   DG_LAUNCHED();
-  return dg_cn_tables(h);
+  // the new tables are first needed by the next substep's CN solve: build them
+  // on the side stream while the nonlinear terms of that substep run
+  DG_CUDA(cudaEventRecord(h->ev_fork, h->st));
+  DG_CUDA(cudaStreamWaitEvent(h->st2, h->ev_fork, 0));
+  cudaStream_t keep = h->st;
+  h->st = h->st2;
+  int s = dg_cn_tables(h);
+  h->st = keep;
+  DG_TRY(s);
+  DG_CUDA(cudaEventRecord(h->ev_join, h->st2));
+  h->tables_pending = true;
+  return DG_OK;
 }
 
 int dg_chan_init(dg_handle *h) {
@@ -1025,43 +1490,105 @@ int dg_chan_init(dg_handle *h) {
 extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
   if (!h || h->periodic || rk_step < 1 || rk_step > 3) return DG_ERR_ARG;
   const ChanConst C = make_const(h);
-  // 1. z inverse of every prognostic field, all planes
+  // Steps 1-3 run over y-chunks of planes so the half-physical (H) and
+  // product (G) planes a chunk produces are consumed while still in L2.
   const double2 *in[3 + DG_MAX_TH];
   for (int f = 0; f < h->nf; f++) in[f] = h->cu[f];
-  DG_TRY(dg_zinv(h, in, h->nf, 0, h->NY + 1, h->H, 0));
-  // 2. x-row nonlinear products, y-marching chunks
-  const int chunk = 8;
   const long Hfield = (long)h->nplanes * h->NZ * h->nkxp;
-  {
-    dim3 grid(dg_cdiv(h->NZ, XR_ROWS), dg_cdiv(h->NY, chunk));
-    const size_t sm = xrow_smem(h);
+  // planes per chunk: measured faster as a single chunk on B200 for the grids
+  // benchmarked (the kernels are latency- rather than bandwidth-bound), so
+  // the default is all planes; DG_YCHUNK overrides for experiments
+  int cj = h->NY;
+  if (const char *e = getenv("DG_YCHUNK")) {
+    const int v = atoi(e);
+    if (v >= 4 && v < h->NY) cj = v;
+  }
+  FieldPtrs cu, cf, rhs;
+  for (int f = 0; f < h->nf; f++) { cu.p[f] = h->cu[f]; cf.p[f] = h->cf[f]; rhs.p[f] = h->rhs[f]; }
+  int hdone = -1;  // last H plane already produced
+  for (int a = 1; a <= h->NY; a += cj) {
+    const int b = (a + cj - 1 < h->NY) ? a + cj - 1 : h->NY;
+    // 1. z inverse of the planes this chunk's x-rows need (a-1 .. b+1)
+    DG_TRY(dg_zinv(h, in, h->nf, hdone + 1, b + 1, h->H, 0));
+    hdone = b + 1;
+    // 2. x-row nonlinear products for output planes a..b
+    bool done = false;
+    if (xw_supported(h->NX) && h->NTH <= 2) {
+      const int nplan = b - a + 1;
+      int chunk = (int)((long)nplan * h->NZ / (148L * 16));
+      if (chunk < 4) chunk = 4;
+      if (chunk > nplan) chunk = nplan;
+      dim3 grid(dg_cdiv(h->NZ, XW_WARPS), dg_cdiv(nplan, chunk));
+#define XW_CASE(NXV, NTHV)                                                                         \
+  if (h->NX == NXV && h->NTH == NTHV) {                                                          \
+    dg_big_smem((const void *)k_xrow_w<NXV, NTHV>);                                              \
+    k_xrow_w<NXV, NTHV><<<grid, 32 * XW_WARPS, xw_smem<NXV, NTHV>(), h->st>>>(                    \
+        C, h->H, Hfield, chunk, a, b, h->twx, h->dyf, h->dy, h->kx, h->G, Hfield);               \
+    done = true;                                                                                 \
+  }
+#define XW_ALL(NXV) XW_CASE(NXV, 0) XW_CASE(NXV, 1) XW_CASE(NXV, 2)
+      XW_ALL(16) XW_ALL(32) XW_ALL(48) XW_ALL(64) XW_ALL(96) XW_ALL(128) XW_ALL(256)
+#undef XW_ALL
+#undef XW_CASE
+      if (done) DG_LAUNCHED();
+    }
+    if (!done) {
+      // generic CTA kernel covers all planes 1..NY in one launch
+      if (a == 1) {
+        DG_TRY(dg_zinv(h, in, h->nf, hdone + 1, h->NY + 1, h->H, 0));
+        hdone = h->NY + 1;
+        const int chunk = 8;
+        dim3 grid(dg_cdiv(h->NZ, XR_ROWS), dg_cdiv(h->NY, chunk));
+        const size_t sm = xrow_smem(h);
 #define KERNEL_BODY(N)                                                                          \
   dg_big_smem((const void *)k_xrow_nl<N>);                                                      \
   k_xrow_nl<N><<<grid, XR_THR, sm, h->st>>>(C, h->H, Hfield, chunk, h->plx, h->twx, h->dyf, h->dy, \
                                             h->kx, h->G, Hfield)
-    switch (h->NX) {
-      DG_FOR_EACH_N(DG_CASE_N)
-      default: KERNEL_BODY(0); break;
-    }
+        switch (h->NX) {
+          DG_FOR_EACH_N(DG_CASE_N)
+          default: KERNEL_BODY(0); break;
+        }
 #undef KERNEL_BODY
-    DG_LAUNCHED();
+        DG_LAUNCHED();
+      }
+    }
+    // 3. z forward, explicit terms, CN right-hand side for planes a..b
+    bool zdone = false;
+    if (zw_supported(h->NZ) && done) {
+      dim3 grid(dg_cdiv(h->nkxp, ZW_KXG), b - a + 1, h->nf);
+      const size_t sm = sizeof(double2) * (h->NZ + 16 * padded_len(h->NZ));
+#define ZW_CASE(N)                                                                             \
+  if (h->NZ == N) {                                                                            \
+    dg_big_smem((const void *)k_zfwd_w<N>);                                                    \
+    k_zfwd_w<N><<<grid, 128, sm, h->st>>>(C, h->G, Hfield, h->twz, h->dscal, rk_step, h->kx,   \
+                                          h->kz, h->dy, h->dyf, cu, cf, rhs, h->cp, a);        \
+    zdone = true;                                                                              \
   }
-  // 3. z forward, explicit terms, CN right-hand side
-  {
-    FieldPtrs cu, cf, rhs;
-    for (int f = 0; f < h->nf; f++) { cu.p[f] = h->cu[f]; cf.p[f] = h->cf[f]; rhs.p[f] = h->rhs[f]; }
-    dim3 grid(dg_cdiv(h->nkxp, zf_kxg(h->NZ)), h->NY);
-    const size_t sm = zfwd_smem(h);
+      ZW_CASE(16) ZW_CASE(32) ZW_CASE(48) ZW_CASE(64) ZW_CASE(96) ZW_CASE(128) ZW_CASE(256)
+#undef ZW_CASE
+      if (zdone) DG_LAUNCHED();
+    }
+    if (!done || !zdone) {
+      if (a == 1 || done) {
+        // generic path: one launch over all planes after all products exist
+        if (!done && a != 1) continue;
+        dim3 grid(dg_cdiv(h->nkxp, zf_kxg(h->NZ)), h->NY);
+        const size_t sm = zfwd_smem(h);
 #define KERNEL_BODY(N)                                                                          \
   dg_big_smem((const void *)k_zfwd_rhs<N>);                                                     \
   k_zfwd_rhs<N><<<grid, ZF_THR, sm, h->st>>>(C, h->G, Hfield, h->plz, h->twz, h->dscal, rk_step, \
                                              h->kx, h->kz, h->dy, h->dyf, cu, cf, rhs, h->cp)
-    switch (h->NZ) {
-      DG_FOR_EACH_N(DG_CASE_N)
-      default: KERNEL_BODY(0); break;
-    }
+        if (!zdone && (!done ? a == 1 : b == h->NY)) {
+          switch (h->NZ) {
+            DG_FOR_EACH_N(DG_CASE_N)
+            default: KERNEL_BODY(0); break;
+          }
+          DG_LAUNCHED();
+        }
 #undef KERNEL_BODY
-    DG_LAUNCHED();
+      }
+    }
+    if (!done) break;  // the generic kernels covered every plane
   }
   // 4. per-mode CN solves, then COURANT on the post-CN velocity
   //    (for/channel.f:1037-1040), then REM_DIV_CHAN and CP += phi / H_BAR

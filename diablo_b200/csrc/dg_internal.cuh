@@ -78,6 +78,9 @@ struct dg_handle {
 
   cudaStream_t st;
   bool own_stream;
+  cudaStream_t st2;             // side stream for work off the critical path
+  cudaEvent_t ev_fork, ev_join;
+  bool tables_pending;          // CN tables being rebuilt on st2
 
   // host copies of the tables
   double *h_gy, *h_gyf, *h_dy, *h_dyf, *h_kx, *h_kz, *h_ky;
@@ -120,6 +123,7 @@ int dg_zinv(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jm
             double2 *H, int field_stride_planes);
 int dg_xc2r_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax, double *phys,
                    long phys_plane_stride, long phys_row_stride, long field_stride);
+int dg_xc2r_cfl(dg_handle *h, const double2 *H, int jmin, int jmax, unsigned long long *out);
 int dg_xr2c_planes(dg_handle *h, const double *phys, int nf, int jmin, int jmax,
                    long phys_plane_stride, long phys_row_stride, long field_stride, double2 *H);
 int dg_zfwd_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax,

@@ -320,6 +320,60 @@ __device__ __forceinline__ double2 *run_ct(double2 *buf0, double2 *buf1, int nsi
 }
 
 // Dispatch helper: N == 0 selects the runtime plan.
+// ---------------------------------------------------------- warp-level passes
+// One warp transforms `nsig` signals in place with __syncwarp between the
+// load and store halves of every pass (needs N/R <= 32 in every pass).
+__host__ __device__ constexpr bool warp_fft_ok(int n) {
+  return n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 256;
+}
+
+template <int N, int R, int NS, int SIGN>
+__device__ __forceinline__ void wpass(double2 *__restrict__ buf, int nsig, int sstr,
+                                      const double2 *__restrict__ tw, int lane) {
+  constexpr int NB = N / R;
+  static_assert(NB <= 32, "warp pass needs N/R <= 32");
+  constexpr int TMUL = N / (NS * R);
+  constexpr int SPR = 32 / NB;
+  const int sl = lane / NB, b = lane % NB, k = b % NS;
+  const int idx = (b / NS) * NS * R + k;
+  for (int s0 = 0; s0 < nsig; s0 += SPR) {
+    const int s = s0 + sl;
+    const bool act = (sl < SPR) && (s < nsig);
+    double2 v[R];
+    if (act) {
+      const double2 *in = buf + s * sstr;
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        double2 x = in[pad(b + r * NB)];
+        if (NS > 1 && r > 0) {
+          double2 t = tw[r * k * TMUL];
+          if (SIGN > 0) t.y = -t.y;
+          x = cmul(x, t);
+        }
+        v[r] = x;
+      }
+      dft<R>(v, SIGN);
+    }
+    __syncwarp();
+    if (act) {
+      double2 *out = buf + s * sstr;
+#pragma unroll
+      for (int r = 0; r < R; r++) out[pad(idx + r * NS)] = v[r];
+    }
+    __syncwarp();
+  }
+}
+
+template <int N, int SIGN, int P>
+__device__ __forceinline__ void wpasses(double2 *buf, int nsig, int sstr, const double2 *tw,
+                                        int lane) {
+  constexpr int R = plan_radix(N, P);
+  if constexpr (R != 0) {
+    wpass<N, R, plan_ns(N, P), SIGN>(buf, nsig, sstr, tw, lane);
+    wpasses<N, SIGN, P + 1>(buf, nsig, sstr, tw, lane);
+  }
+}
+
 // Compile-time lengths run in place in buf0 (buf1 unused); the runtime plan
 // ping-pongs between buf0 and buf1.
 template <int N>
@@ -332,6 +386,28 @@ __device__ __forceinline__ double2 *fft(double2 *buf0, double2 *buf1, const FftP
     if (sign < 0) ippasses<N, -1, 0>(buf0, nsig, sig_stride, tw, tid, nthr);
     else ippasses<N, +1, 0>(buf0, nsig, sig_stride, tw, tid, nthr);
     return buf0;
+  }
+}
+
+// CTA front end: with a warp-capable length the signals are dealt out to the
+// warps (no CTA barrier between passes), otherwise the CTA-wide passes run.
+template <int N>
+__device__ __forceinline__ double2 *fft_cta(double2 *buf0, double2 *buf1, const FftPlan &pl,
+                                            int nsig, int sig_stride, const double2 *tw,
+                                            int sign) {
+  if constexpr (N != 0 && warp_fft_ok(N)) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int per = (nsig + nw - 1) / nw;
+    const int s0 = warp * per;
+    const int ns = (nsig - s0) < per ? (nsig - s0) : per;
+    if (ns > 0) {
+      if (sign < 0) wpasses<N, -1, 0>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
+      else wpasses<N, +1, 0>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
+    }
+    __syncthreads();
+    return buf0;
+  } else {
+    return fft<N>(buf0, buf1, pl, nsig, sig_stride, tw, sign);
   }
 }
 

@@ -54,15 +54,24 @@ __global__ void __launch_bounds__(NTHR) k_zinv(CFieldPtrs fields, int jmin, long
   const int tid = threadIdx.x, nthr = blockDim.x;
   const double2 *in = fields.p[f] + (long)j * ss;
   for (int i = tid; i < NZ; i += nthr) stw[i] = tw[i];
-  for (int idx = tid; idx < KXG * NZ; idx += nthr) {
-    const int c = idx % KXG, z = idx / KXG;
-    double2 v = make_double2(0.0, 0.0);
-    const int kp = packed_index(z, NZ, NKZ);
-    if (kp >= 0 && kx0 + c < nkxp) v = in[(long)kp * nkxp + kx0 + c];
-    b0[c * sstr + pad(z)] = v;
+  for (int base = 0; base < KXG * NZ; base += 8 * nthr) {
+    double2 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * nthr + tid;
+      const int c = idx % KXG, z = idx / KXG;
+      const int kp = packed_index(z, NZ, NKZ);
+      v[u] = (idx < KXG * NZ && kp >= 0 && kx0 + c < nkxp) ? in[(long)kp * nkxp + kx0 + c]
+                                                          : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * nthr + tid;
+      if (idx < KXG * NZ) b0[(idx % KXG) * sstr + pad(idx / KXG)] = v[u];
+    }
   }
   __syncthreads();
-  double2 *res = fft<NT>(b0, b1, pl, KXG, sstr, stw, +1);
+  double2 *res = fft_cta<NT>(b0, b1, pl, KXG, sstr, stw, +1);
   double2 *out = H + f * Hfield + (long)j * NZ * nkxp;
   for (int idx = tid; idx < KXG * NZ; idx += nthr) {
     const int c = idx % KXG, z = idx / KXG;
@@ -88,14 +97,23 @@ __global__ void __launch_bounds__(NTHR) k_zfwd(const double2 *__restrict__ H, lo
   const int tid = threadIdx.x, nthr = blockDim.x;
   const double2 *in = H + f * Hfield + (long)j * NZ * nkxp;
   for (int i = tid; i < NZ; i += nthr) stw[i] = tw[i];
-  for (int idx = tid; idx < KXG * NZ; idx += nthr) {
-    const int c = idx % KXG, z = idx / KXG;
-    double2 v = make_double2(0.0, 0.0);
-    if (kx0 + c < nkxp) v = in[(long)z * nkxp + kx0 + c];
-    b0[c * sstr + pad(z)] = v;
+  for (int base = 0; base < KXG * NZ; base += 8 * nthr) {
+    double2 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * nthr + tid;
+      const int c = idx % KXG, z = idx / KXG;
+      v[u] = (idx < KXG * NZ && kx0 + c < nkxp) ? in[(long)z * nkxp + kx0 + c]
+                                                : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * nthr + tid;
+      if (idx < KXG * NZ) b0[(idx % KXG) * sstr + pad(idx / KXG)] = v[u];
+    }
   }
   __syncthreads();
-  double2 *res = fft<NT>(b0, b1, pl, KXG, sstr, stw, -1);
+  double2 *res = fft_cta<NT>(b0, b1, pl, KXG, sstr, stw, -1);
   double2 *out = fields.p[f] + (long)j * ss;
   const double rnz = (double)NZ;
   for (int idx = tid; idx < KXG * nkzt; idx += nthr) {
@@ -151,7 +169,7 @@ __global__ void __launch_bounds__(NTHR) k_xc2r(const double2 *__restrict__ H, lo
     b0[q * sstr + pad(k)] = v;
   }
   __syncthreads();
-  double2 *res = fft<NT>(b0, b1, pl, RPAIR, sstr, stw, +1);
+  double2 *res = fft_cta<NT>(b0, b1, pl, RPAIR, sstr, stw, +1);
   double *out = phys + f * pfield + (long)j * pplane;
   for (int idx = tid; idx < RPAIR * NX; idx += nthr) {
     const int q = idx / NX, x = idx % NX;
@@ -160,6 +178,63 @@ __global__ void __launch_bounds__(NTHR) k_xc2r(const double2 *__restrict__ H, lo
     if (za < NZ) out[(long)za * prow + x] = v.x;
     if (zb < NZ) out[(long)zb * prow + x] = v.y;
   }
+}
+
+// c2r of RPAIR row pairs followed by COURANT's per-point limit
+// min(CFL d / |u|) (for/courant.f:35-44) instead of a store: field 0 uses DX,
+// field 1 DY(j), field 2 DZ.  The minimum goes to *out as ordered bits.
+template <int NT>
+__global__ void __launch_bounds__(NTHR) k_xc2r_cfl(const double2 *__restrict__ H, long Hfield,
+                                                   int jmin, int nkxp, int NXr, int NZ, FftPlan pl,
+                                                   const double2 *__restrict__ tw, double cfl,
+                                                   double dxv, double dzv,
+                                                   const double *__restrict__ dy,
+                                                   unsigned long long *__restrict__ out) {
+  extern __shared__ double2 sm[];
+  const int NX = NT ? NT : NXr;
+  const int RPAIR = batch_for(NX);
+  const int sstr = padded_len(NX);
+  double2 *stw = sm;
+  double2 *b0 = stw + NX;
+  double2 *b1 = b0 + RPAIR * sstr;
+  const int z0 = blockIdx.x * 2 * RPAIR;
+  const int j = jmin + blockIdx.y;
+  const int f = blockIdx.z;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const double2 *in = H + f * Hfield + (long)j * NZ * nkxp;
+  const int NKX = nkxp - 1;
+  for (int i = tid; i < NX; i += nthr) stw[i] = tw[i];
+  for (int idx = tid; idx < RPAIR * NX; idx += nthr) {
+    const int q = idx / NX, k = idx % NX;
+    const int za = z0 + 2 * q, zb = za + 1;
+    double2 v = make_double2(0.0, 0.0);
+    if (za < NZ) {
+      const int kk = (k <= NX / 2) ? k : NX - k;
+      if (kk <= NKX && kk < NX / 2) {
+        double2 a = in[(long)za * nkxp + kk];
+        double2 b = (zb < NZ) ? in[(long)zb * nkxp + kk] : make_double2(0.0, 0.0);
+        if (kk == 0) {
+          a.y = 0.0;
+          b.y = 0.0;
+        }
+        v = (k == kk) ? make_double2(a.x - b.y, a.y + b.x) : make_double2(a.x + b.y, -a.y + b.x);
+      }
+    }
+    b0[q * sstr + pad(k)] = v;
+  }
+  __syncthreads();
+  double2 *res = fft_cta<NT>(b0, b1, pl, RPAIR, sstr, stw, +1);
+  const double d = (f == 0) ? dxv : (f == 1 ? dy[j] : dzv);
+  double best = __longlong_as_double(0x7ff0000000000000LL);
+  for (int idx = tid; idx < RPAIR * NX; idx += nthr) {
+    const int q = idx / NX, x = idx % NX;
+    const int za = z0 + 2 * q, zb = za + 1;
+    const double2 v = res[q * sstr + pad(x)];
+    if (za < NZ) best = fmin(best, cfl * d / fabs(v.x));
+    if (zb < NZ) best = fmin(best, cfl * d / fabs(v.y));
+  }
+  for (int off = 16; off > 0; off >>= 1) best = fmin(best, __shfl_down_sync(0xffffffffu, best, off));
+  if ((tid & 31) == 0) atomicMin(out, (unsigned long long)__double_as_longlong(best));
 }
 
 // r2c of RPAIR row pairs of one plane of one field; keeps kx = 0..NKX, / NX.
@@ -189,7 +264,7 @@ __global__ void __launch_bounds__(NTHR) k_xr2c(const double *__restrict__ phys, 
     b0[q * sstr + pad(x)] = make_double2(a, b);
   }
   __syncthreads();
-  double2 *res = fft<NT>(b0, b1, pl, RPAIR, sstr, stw, -1);
+  double2 *res = fft_cta<NT>(b0, b1, pl, RPAIR, sstr, stw, -1);
   double2 *out = H + f * Hfield + (long)j * NZ * nkxp;
   const double rnx = (double)NX;
   for (int idx = tid; idx < RPAIR * nkxp; idx += nthr) {
@@ -299,6 +374,24 @@ int dg_xr2c_planes(dg_handle *h, const double *phys, int nf, int jmin, int jmax,
   big_smem(k_xr2c<N>);                                                                        \
   k_xr2c<N><<<grid, NTHR, sm, h->st>>>(phys, pplane, prow, pfield, jmin, h->nkxp, h->NX, h->NZ,   \
                                       h->plx, h->twx, H, Hf)
+  switch (h->NX) {
+    DG_FOR_EACH_N(DG_CASE_N)
+    default: KERNEL_BODY(0); break;
+  }
+#undef KERNEL_BODY
+  DG_LAUNCHED();
+  return DG_OK;
+}
+
+int dg_xc2r_cfl(dg_handle *h, const double2 *H, int jmin, int jmax, unsigned long long *out) {
+  dim3 grid(dg_cdiv(h->NZ, 2 * batch_for(h->NX)), jmax - jmin + 1, 3);
+  const size_t sm = xsmem(h->NX);
+  const long Hf = (long)h->nplanes * h->NZ * h->nkxp;
+  const double dxv = h->p.lx / h->NX, dzv = h->p.lz / h->NZ;
+#define KERNEL_BODY(N)                                                                          \
+  big_smem(k_xc2r_cfl<N>);                                                                      \
+  k_xc2r_cfl<N><<<grid, NTHR, sm, h->st>>>(H, Hf, jmin, h->nkxp, h->NX, h->NZ, h->plx, h->twx,     \
+                                          h->p.cfl, dxv, dzv, h->dy, out)
   switch (h->NX) {
     DG_FOR_EACH_N(DG_CASE_N)
     default: KERNEL_BODY(0); break;

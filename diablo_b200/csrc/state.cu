@@ -165,6 +165,14 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
     }
     h->own_stream = true;
   }
+  if (cudaStreamCreateWithFlags(&h->st2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    dg_set_error("side stream creation failed");
+    if (h->own_stream) cudaStreamDestroy(h->st);
+    free(h);
+    return DG_ERR_CUDA;
+  }
   *out = h;
   const int NY = h->NY, L = NY + 2;
 
@@ -281,6 +289,10 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
     if (h->cf[f]) cudaFree(h->cf[f]);
     if (h->rhs[f]) cudaFree(h->rhs[f]);
   }
+  cudaStreamSynchronize(h->st2);
+  cudaEventDestroy(h->ev_fork);
+  cudaEventDestroy(h->ev_join);
+  cudaStreamDestroy(h->st2);
   if (h->own_stream) cudaStreamDestroy(h->st);
   free(h->h_gy); free(h->h_gyf); free(h->h_dy); free(h->h_dyf);
   free(h->h_kx); free(h->h_kz); free(h->h_ky);
@@ -290,6 +302,7 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
 
 extern "C" int diablo_synchronize(dg_handle *h) {
   if (!h) return DG_ERR_ARG;
+  DG_CUDA(cudaStreamSynchronize(h->st2));
   DG_CUDA(cudaStreamSynchronize(h->st));
   return DG_OK;
 }
@@ -298,6 +311,10 @@ extern "C" int diablo_set_time(dg_handle *h, double time, double delta_t) {
   if (!h) return DG_ERR_ARG;
   double s[5] = {time, delta_t, delta_t * (8.0 / 15.0), delta_t * (2.0 / 15.0),
                  delta_t * (5.0 / 15.0)};
+  if (h->tables_pending) {
+    DG_CUDA(cudaStreamWaitEvent(h->st, h->ev_join, 0));
+    h->tables_pending = false;
+  }
   DG_CUDA(cudaMemcpyAsync(h->dscal, s, sizeof(s), cudaMemcpyHostToDevice, h->st));
   if (h->cn_tab) DG_TRY(dg_cn_tables(h));
   DG_CUDA(cudaStreamSynchronize(h->st));

@@ -1622,6 +1622,7 @@ extern "C" int diablo_courant(dg_handle *h) {
 }
 
 int dg_stats_dev(dg_handle *h, dg_stats *s) {
+  if (h->periodic) return dg_per_stats(h, s);
   const int NP = h->nplanes;
   double *dsum = (double *)h->work;
   CFieldPtrs u;

@@ -119,6 +119,12 @@ struct dg_handle {
 };
 
 // common kernel-launch helpers (defined in fft_kernels.cu)
+int dg_cinv_g(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax,
+              long in_plane, int rowlen, int N, int NK, const FftPlan &pl, const double2 *tw,
+              double2 *H, long out_field);
+int dg_cfwd_g(dg_handle *h, const double2 *H, long in_field, int nf, int jmin, int jmax,
+              int rowlen, int nkt, int N, int NK, const FftPlan &pl, const double2 *tw,
+              double2 *const *fields, long out_plane);
 int dg_zinv(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax,
             double2 *H, int field_stride_planes);
 int dg_xc2r_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax, double *phys,
@@ -136,6 +142,7 @@ int dg_apply_bc_vel_dev(dg_handle *h);
 int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step);
 int dg_courant_dev(dg_handle *h, const double2 *const *u);
 int dg_stats_dev(dg_handle *h, dg_stats *s);
+int dg_per_stats(dg_handle *h, dg_stats *s);
 int dg_cn_tables(dg_handle *h);
 int dg_dt_commit(dg_handle *h);
 

@@ -303,19 +303,23 @@ void big_smem(K kern) {
 
 // ------------------------------------------------------------- host wrappers
 
-int dg_zinv(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax, double2 *H,
-            int) {
+// Column transforms along one axis for a batch of planes.  Geometry (per
+// field): input plane j at fields[f] + j*in_plane, packed slot kp of column c
+// at + kp*rowlen + c; output plane j at H + f*out_field + j*N*rowlen, bin z of
+// column c at + z*rowlen + c.  z transforms: rowlen = NKX+1, planes = y;
+// y transforms (periodic): rowlen = modes per ky-plane, one plane.
+int dg_cinv_g(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax,
+              long in_plane, int rowlen, int N, int NK, const FftPlan &pl, const double2 *tw,
+              double2 *H, long out_field) {
   if (jmax < jmin || nf <= 0) return DG_OK;
   CFieldPtrs fp;
   for (int f = 0; f < nf; f++) fp.p[f] = fields[f];
-  dim3 grid(dg_cdiv(h->nkxp, batch_for(h->NZ)), jmax - jmin + 1, nf);
-  const size_t sm = zsmem(h->NZ);
-  const long Hf = (long)h->nplanes * h->NZ * h->nkxp;
-#define KERNEL_BODY(N)                                                                      \
-  big_smem(k_zinv<N>);                                                                      \
-  k_zinv<N><<<grid, NTHR, sm, h->st>>>(fp, jmin, h->ss, h->nkxp, h->NZ, h->NKZ, h->plz, h->twz, \
-                                      H, Hf)
-  switch (h->NZ) {
+  dim3 grid(dg_cdiv(rowlen, batch_for(N)), jmax - jmin + 1, nf);
+  const size_t sm = zsmem(N);
+#define KERNEL_BODY(NN)                                                                       \
+  big_smem(k_zinv<NN>);                                                                       \
+  k_zinv<NN><<<grid, NTHR, sm, h->st>>>(fp, jmin, in_plane, rowlen, N, NK, pl, tw, H, out_field)
+  switch (N) {
     DG_FOR_EACH_N(DG_CASE_N)
     default: KERNEL_BODY(0); break;
   }
@@ -324,25 +328,36 @@ int dg_zinv(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jm
   return DG_OK;
 }
 
-int dg_zfwd_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax,
-                   double2 *const *fields, double2 *, long) {
+int dg_cfwd_g(dg_handle *h, const double2 *H, long in_field, int nf, int jmin, int jmax,
+              int rowlen, int nkt, int N, int NK, const FftPlan &pl, const double2 *tw,
+              double2 *const *fields, long out_plane) {
   if (jmax < jmin || nf <= 0) return DG_OK;
   FieldPtrs fp;
   for (int f = 0; f < nf; f++) fp.p[f] = fields[f];
-  dim3 grid(dg_cdiv(h->nkxp, batch_for(h->NZ)), jmax - jmin + 1, nf);
-  const size_t sm = zsmem(h->NZ);
-  const long Hf = (long)h->nplanes * h->NZ * h->nkxp;
-#define KERNEL_BODY(N)                                                                          \
-  big_smem(k_zfwd<N>);                                                                          \
-  k_zfwd<N><<<grid, NTHR, sm, h->st>>>(H, Hf, jmin, h->nkxp, h->nkzt, h->NZ, h->NKZ, h->plz, h->twz, \
-                                      fp, h->ss)
-  switch (h->NZ) {
+  dim3 grid(dg_cdiv(rowlen, batch_for(N)), jmax - jmin + 1, nf);
+  const size_t sm = zsmem(N);
+#define KERNEL_BODY(NN)                                                                        \
+  big_smem(k_zfwd<NN>);                                                                        \
+  k_zfwd<NN><<<grid, NTHR, sm, h->st>>>(H, in_field, jmin, rowlen, nkt, N, NK, pl, tw, fp, out_plane)
+  switch (N) {
     DG_FOR_EACH_N(DG_CASE_N)
     default: KERNEL_BODY(0); break;
   }
 #undef KERNEL_BODY
   DG_LAUNCHED();
   return DG_OK;
+}
+
+int dg_zinv(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax, double2 *H,
+            int) {
+  return dg_cinv_g(h, fields, nf, jmin, jmax, h->ss, h->nkxp, h->NZ, h->NKZ, h->plz, h->twz, H,
+                   (long)h->nplanes * h->NZ * h->nkxp);
+}
+
+int dg_zfwd_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax,
+                   double2 *const *fields, double2 *, long) {
+  return dg_cfwd_g(h, H, (long)h->nplanes * h->NZ * h->nkxp, nf, jmin, jmax, h->nkxp, h->nkzt,
+                   h->NZ, h->NKZ, h->plz, h->twz, fields, h->ss);
 }
 
 int dg_xc2r_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax, double *phys,

@@ -237,6 +237,54 @@ class Periodic(_Solver):
             self.rk_per_1(rk)
         self.advance_time()
 
+    # ---- transforms
+    def fft_xzy_to_fourier(self, U: np.ndarray, CU: np.ndarray | None = None):
+        """FFT_XZY_TO_FOURIER(U, CU) on reference-layout host arrays.
+        U: (NY+2, NZ+2, NX+2) float64; returns CU (NY+2, NZ+2, NX/2+1) complex128."""
+        p = self.p
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(p.ny + 2, p.nz + 2, p.nx + 2)
+        if CU is None:
+            CU = np.zeros((p.ny + 2, p.nz + 2, p.nx // 2 + 1), dtype=np.complex128)
+        self._call("diablo_fft_xzy_to_fourier", _ptr(U), _ptr(CU), _lib.DG_HOST)
+        return CU
+
+    def fft_xzy_to_physical(self, CU: np.ndarray, U: np.ndarray | None = None):
+        p = self.p
+        CU = np.ascontiguousarray(CU, dtype=np.complex128)
+        if U is None:
+            U = np.zeros((p.ny + 2, p.nz + 2, p.nx + 2), dtype=np.float64)
+        self._call("diablo_fft_xzy_to_physical", _ptr(CU), _ptr(U), _lib.DG_HOST)
+        return U
+
+    def to_fourier(self, phys: np.ndarray) -> np.ndarray:
+        """Physical [NY][NZ][NX] -> retained modes [TNKY+1][TNKZ+1][NKX+1]."""
+        p = self.p
+        U = np.zeros((p.ny + 2, p.nz + 2, p.nx + 2))
+        U[: p.ny, : p.nz, : p.nx] = phys
+        CU = self.fft_xzy_to_fourier(U)
+        return np.ascontiguousarray(CU[: p.tnky + 1, : p.tnkz + 1, : p.nkx + 1])
+
+    def to_physical(self, spec: np.ndarray) -> np.ndarray:
+        p = self.p
+        CU = np.zeros((p.ny + 2, p.nz + 2, p.nx // 2 + 1), dtype=np.complex128)
+        CU[: p.tnky + 1, : p.tnkz + 1, : p.nkx + 1] = spec
+        U = self.fft_xzy_to_physical(CU)
+        return np.ascontiguousarray(U[: p.ny, : p.nz, : p.nx])
+
+    def create_flow(self, u1, u2, u3, th=None):
+        """CREATE_FLOW_PER tail (for/set_ics.f:278-319 then for/periodic.f
+        REM_DIV_PER and POISSON_P_PER): physical [NY][NZ][NX] fields -> state."""
+        zero = np.zeros(self.spec_shape, dtype=np.complex128)
+        for nm in ["CP", "CF1", "CF2", "CF3"] + [f"CFTH{n}" for n in range(self.p.n_th)]:
+            self.set_field(nm, zero)
+        for nm, a in (("CU1", u1), ("CU2", u2), ("CU3", u3)):
+            self.set_field(nm, self.to_fourier(a))
+        if th is not None:
+            for n in range(self.p.n_th):
+                self.set_field(f"CTH{n}", self.to_fourier(th[n]))
+        self.rem_div_per()
+        self.poisson_p_per()
+
 
 def thomas_real(a, b, c, g, ny: int, nx: int):
     """THOMAS_REAL(A,B,C,G,NY,NX) on host arrays shaped (NY+1, NX+1); returns

@@ -154,6 +154,13 @@ int diablo_rk_per_1(dg_handle *h, int rk_step);
 int diablo_rem_div_per(dg_handle *h);
 /* SUBROUTINE POISSON_P_PER (for/periodic.f:329-393). */
 int diablo_poisson_p_per(dg_handle *h);
+/* FFT_XZY_TO_FOURIER(U,CU) (for/fft.f:223-258) and FFT_XZY_TO_PHYSICAL(CU,U)
+ * (for/fft.f:261-299) on REFERENCE-layout arrays U(0:NX+1,0:NZ+1,0:NY+1) and
+ * CU(0:NX/2,0:NZ+1,0:NY+1); retained modes at CU(0:NKX,0:TNKZ,0:TNKY), every
+ * other slot of the output zeroed.  U and CU may alias.  where = DG_HOST or
+ * DG_DEVICE for both pointers. */
+int diablo_fft_xzy_to_fourier(dg_handle *h, const double *U, double *CU, int where);
+int diablo_fft_xzy_to_physical(dg_handle *h, const double *CU, double *U, int where);
 
 /* ------------------------------------------------------------ statistics */
 /* Parity statistics of the current state (channel or periodic); also checks

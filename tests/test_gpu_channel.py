@@ -216,6 +216,32 @@ def test_channel_variants_short(variant):
     ch.close()
 
 
+@pytest.mark.parametrize("case", ["kh_buoyant", "re180_stretched"])
+def test_poisson_p_chan_matches_oracle(case):
+    """POISSON_P_CHAN on a developed state: CP rows 1..NY."""
+    if case == "kh_buoyant":
+        p, gy = configs.kh_shear_layer(nx=64, ny=33, nz=32)
+        p = p.replace(n_th=2)
+        p.ri = [0.1, -0.05, 0, 0]
+        p.th_bc_ymin = [0, 1, 0, 0]
+        p.th_bc_ymax = [0, 1, 0, 0]
+        maker = ics.kh_shear_layer
+    else:
+        p, gy = configs.channel_re180(nx=64, ny=65, nz=48)
+        maker = ics.channel_laminar
+    ref, ch, _ = start_pair(p, gy, maker, seed=4)
+    for s in range(1, 4):
+        ref.step(s)
+        ch.step(s)
+    ref.poisson_p_chan()
+    ch.poisson_p_chan()
+    cp_o = ref.get("CP")[1: p.ny + 1]
+    cp_g = ch.get_field("CP")[1: p.ny + 1]
+    assert rel(cp_g, cp_o) <= 1e-11
+    compare(ref, ch, fields(p))
+    ch.close()
+
+
 def test_courant_matches_oracle():
     p, gy = configs.channel_re180(nx=64, ny=65, nz=64)
     ref, ch, _ = start_pair(p, gy, ics.channel_laminar, seed=9)

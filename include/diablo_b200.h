@@ -4,7 +4,7 @@
  *
  * Every entry point takes plain pointers and sizes, returns an int status
  * (DG_OK = 0) and never aborts the caller.  A Fortran host binds them with
- * ISO_C_BINDING; the Python mirror in
+ * ISO_C_BINDING interfaces; the Python mirror in
  * diablo_b200/_lib.py binds them with ctypes.
  *
  * Ownership: the caller's arrays (the reference's COMMON blocks) stay the

@@ -11,7 +11,7 @@
  * is "parity unpinned" against the reference binary.  It is pinned instead
  * against numpy.fft (FFT conventions), dense linear solves (Thomas), exact
  * analytic solutions (Fourier-mode decay, laminar channel steady states)
- * and the divergence-free constraint; see tests/test_oracle_*.py.
+ * and the divergence-free constraint; see tests/test_oracle.py.
  *
  * Layouts (all row-major, last index fastest):
  *   spectral field  : complex  [NY+2][TNKZ+1][NKX+1]     (retained modes only)

@@ -83,6 +83,7 @@ def load(path: str = LIB_PATH):
         "diablo_thomas_complex": [P, P, P, P, I, I, I],
         "diablo_rk_per_1": [P, I], "diablo_rem_div_per": [P], "diablo_poisson_p_per": [P],
         "diablo_fft_xzy_to_fourier": [P, P, P, I], "diablo_fft_xzy_to_physical": [P, P, P, I],
+        "diablo_fft_xz_to_fourier_noalloc": [P, P, I, I, I, I, I, P],
         "diablo_stats": [P, ctypes.POINTER(DgStats)],
     }
     for name, args in sigs.items():

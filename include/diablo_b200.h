@@ -162,6 +162,23 @@ int diablo_poisson_p_per(dg_handle *h);
 int diablo_fft_xzy_to_fourier(dg_handle *h, const double *U, double *CU, int where);
 int diablo_fft_xzy_to_physical(dg_handle *h, const double *CU, double *U, int where);
 
+/* ------------------------------------------- allocation-free transform */
+/* No counterpart in the reference.  FFT_XZ_TO_FOURIER(V,VV,JMIN,JMAX) on
+ * DEVICE arrays in the reference layout (as diablo_fft_xz_to_fourier with
+ * DG_DEVICE), for callers that cannot have device memory allocated for
+ * them: it needs no dg_handle and allocates no device memory.  Its only
+ * scratch is a fixed DG_NOALLOC_SCRATCH_BYTES array in the library's device
+ * image, held by every GPU that loads the library until exit; one NX x NZ
+ * plane must fit in it (about 1.75 MB at 512 x 384), otherwise DG_ERR_DIMS.
+ * The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Work is queued on `stream` (NULL: the default stream) and the call
+ * returns without waiting.  All calls share the scratch: calls that overlap
+ * on the GPU race.  V and VV may alias. */
+#define DG_NOALLOC_SCRATCH_BYTES (16 * 1024 * 1024)
+int diablo_fft_xz_to_fourier_noalloc(const double *V, double *VV, int nx, int nz, int ny,
+                                     int jmin, int jmax, void *stream);
+
 /* ------------------------------------------------------------ statistics */
 /* Parity statistics of the current state (channel or periodic); also checks
  * the state for non-finite values (returns DG_ERR_NAN if any). */

@@ -50,6 +50,29 @@ def algorithmic_bytes_per_step(p):
     return (17 * nf + 6) * 16 * m
 
 
+def kernel_bytes_per_launch(p, name):
+    """Algorithmic HBM bytes of one launch of a channel-substep kernel: each
+    array the kernel must read or write, once (stencil neighbours and halo
+    rows are free).  Fields are FP64 complex (16 B); the REM_DIV factors are
+    FP64 real.  CF_old is read in substeps 2 and 3 only: counted at 2/3."""
+    nf = 3 + p.n_th
+    nkxp, nkzt = p.nkx + 1, 2 * p.nkz + 1
+    L, NY, NZ = p.ny + 2, p.ny, p.nz
+    ss = nkxp * nkzt
+    M, Si = ss * L, ss * NY                 # spectral values, all / interior planes
+    Mh, Mi = L * NZ * nkxp, NY * NZ * nkxp  # half-physical values, all / interior planes
+    c = 16
+    table = {
+        "k_zinv": c * nf * (M + Mh),
+        "k_xrow_w": c * (nf * Mh + 2 * nf * Mi),
+        "k_zfwd_w": c * (2 * nf * Mi + Si * (nf + 1 + nf * 2 / 3) + 2 * nf * Si),
+        "k_cn_col": c * 2 * nf * M,
+        "k_rd_col": c * (4 * M + 5 * M) + 8 * 2 * M,
+        "k_xc2r_cfl": c * 3 * Mh,
+    }
+    return table.get(name)
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -58,6 +81,21 @@ def measured_peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch of `kernel` (dram__bytes_read.sum +
+    dram__bytes_write.sum) from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic_channel_re180.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 2 and parts[0] == kernel:
+                    return float(parts[1])
+    except OSError:
+        pass
+    return None
 
 
 class ClockSampler:
@@ -160,19 +198,22 @@ def run_reference(args):
     o.set_time(0.0, p.delta_t)
     for s in range(args.warmup):
         o.step(1 + s)
+    # bounded sample: at most 200 timed steps (about 10-30 s on a many-core host)
+    nsteps = min(args.steps, 200)
     t0 = time.perf_counter()
-    for s in range(args.steps):
+    for s in range(nsteps):
         o.step(1 + args.warmup + s)
     dt = time.perf_counter() - t0
     o.close()
     pts = p.nx * p.ny * p.nz
-    v = pts * args.steps / dt / 1e6
+    v = pts * nsteps / dt / 1e6
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / nsteps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference", "config": workload_config(p),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{args.steps} timed RK3 steps of the full case"},
+                             "sample": f"{nsteps} timed RK3 steps of the full 128x129x128 case "
+                                       f"(FP64 oracle, {threads} OpenMP threads, {dt:.1f} s)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -213,6 +254,8 @@ def run_gpu(args):
     sampler = ClockSampler(local) if rank == 0 else None
     if sampler:
         sampler.start()
+    L = _lib.load()
+    _lib.check("dg_timing_enable", L.dg_timing_enable(ch.h, 1))
     launches0 = _lib.kernel_launches()
     times = []
     for _ in range(args.steps):
@@ -231,6 +274,16 @@ def run_gpu(args):
     torch.cuda.synchronize()
     launches = _lib.kernel_launches() - launches0
     clocks = sampler.stop() if sampler else None
+    _lib.check("dg_timing_enable", L.dg_timing_enable(ch.h, 0))
+    kt = {}
+    import ctypes
+    nm = ctypes.create_string_buffer(64)
+    cnt = ctypes.c_int64()
+    tms = ctypes.c_double()
+    i = 0
+    while L.dg_timing_read(ch.h, i, nm, 64, ctypes.byref(cnt), ctypes.byref(tms)) == 0:
+        kt[nm.value.decode()] = (int(cnt.value), float(tms.value))
+        i += 1
     total = sum(times)
     if dist:
         t = torch.tensor([total], dtype=torch.float64, device="cuda")
@@ -242,14 +295,14 @@ def run_gpu(args):
 
     # end to end through the C-ABI with host-owned state in the reference
     # layout (pinned host buffers), synced in and out every step
-    names = ["CU1", "CU2", "CU3", "CP", "CF1", "CF2", "CF3"]
+    # a step reads CU1..3 and CP (CF is rebuilt by substep 1 before use) and
+    # returns the same fields
+    names = ["CU1", "CU2", "CU3", "CP"] + [f"CTH{n}" for n in range(p.n_th)]
     refshape = (p.ny + 2, p.nz + 2, p.nx // 2 + 1)
     host = {n: torch.zeros(refshape + (2,), dtype=torch.float64).pin_memory() for n in names}
     for n in names:
         a = ch.get_field(n, layout="reference")
         host[n].numpy()[...] = np.stack([a.real, a.imag], -1)
-    import ctypes
-    L = _lib.load()
     e2e_steps = max(3, min(args.steps, 10))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -274,8 +327,9 @@ def run_gpu(args):
     e2e = {"value": ws * pts * e2e_steps / e2e_t / 1e6, "unit": UNIT,
            "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
            "steps": e2e_steps,
-           "what": "per step: H2D of CU1..3, CP, CF1..3 in the reference layout from pinned "
-                   "host memory, 3x diablo_rk_chan_1, D2H of the same fields"}
+           "what": "per step: H2D of CU1..3 and CP in the reference layout from pinned host "
+                   "memory (diablo_set_field), 3x diablo_rk_chan_1 + TIME update, D2H of the "
+                   "same fields (diablo_get_field)"}
 
     # physical sanity of the timed run
     st = ch.stats()
@@ -287,16 +341,34 @@ def run_gpu(args):
         return 0
     peak, peak_kind = measured_peaks()
     bstep = algorithmic_bytes_per_step(p)
-    achieved = bstep / (total / args.steps) / 1e9
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-            "scope": "whole RK3 step: algorithmic bytes (17 Nf + 6) x 16 B x M per step "
-                     f"= {bstep / 1e6:.1f} MB over the device time of one step"}
+    step_achieved = bstep / (total / args.steps) / 1e9
+    # dominant kernel: largest share of the event-timed device time
+    dom = max(kt.items(), key=lambda kv: kv[1][1]) if kt else None
+    roof = None
+    if dom is not None:
+        name, (n, ms_tot) = dom
+        per = kernel_bytes_per_launch(p, name)
+        avg_s = ms_tot * 1e-3 / max(n, 1)
+        achieved = per / avg_s / 1e9 if per else None
+        roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None,
+                "traffic": ncu_traffic(name), "bytes_per_launch": per,
+                "avg_launch_us": avg_s * 1e6, "launches": n,
+                "share": ms_tot / sum(v[1] for v in kt.values()),
+                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                else "fallback 6650 GB/s"}
+    kernels = {k: {"launches": v[0], "total_ms": round(v[1], 3),
+                   "avg_us": round(1e3 * v[1] / max(v[0], 1), 2)} for k, v in kt.items()}
+    roof_step = {"achieved": step_achieved, "peak": peak, "unit": "GB/s",
+                 "frac": step_achieved / peak,
+                 "scope": "whole RK3 step: algorithmic bytes (17 Nf + 6) x 16 B x M per step "
+                          f"= {bstep / 1e6:.1f} MB over the device time of one step"}
     cpu = cpu_baseline(p, gy, seconds=args.cpu_seconds) if args.cpu_seconds > 0 else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(p), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "config": workload_config(p), "roofline": roof, "roofline_step": roof_step,
+            "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clocks,
             "check": {"ke": st["ke"], "div_max": st["div_max"], "ubulk": st["ubulk"]}}
     print(json.dumps(line))
@@ -306,7 +378,7 @@ def run_gpu(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)

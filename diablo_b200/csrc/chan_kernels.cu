@@ -1378,6 +1378,7 @@ int dg_cn_tables(dg_handle *h) {
   CnRows P;
   P.NY = h->NY; P.nfld = h->nf; P.nu = h->p.nu; P.nuv = h->p.nu_v_scale;
   for (int f = 0; f < 3 + DG_MAX_TH; f++) P.pr[f] = (f >= 3 && f - 3 < h->NTH) ? h->p.pr[f - 3] : 1.0;
+  dg_kt_begin(h, "k_cn_tables", h->st);
   k_cn_tables<<<1, 32, sizeof(double) * h->nf * 8 * L, h->st>>>(P, h->dscal, h->cn_rows, h->cn_tab);
   DG_LAUNCHED();
   return DG_OK;
@@ -1390,6 +1391,7 @@ int dg_apply_bc_vel_dev(dg_handle *h) {
   B.u1 = h->p.u_bc_ymax; B.v1 = h->p.v_bc_ymax; B.w1 = h->p.w_bc_ymax;
   B.cu0 = h->p.u_bc_ymin_c1; B.cv0 = h->p.v_bc_ymin_c1; B.cw0 = h->p.w_bc_ymin_c1;
   B.cu1 = h->p.u_bc_ymax_c1; B.cv1 = h->p.v_bc_ymax_c1; B.cw1 = h->p.w_bc_ymax_c1;
+  dg_kt_begin(h, "k_bc_vel", h->st);
   k_bc_vel<<<dg_cdiv(h->ss, 128), 128, 0, h->st>>>(B, h->ss, h->dy, h->dyf, h->cu[0], h->cu[1],
                                                    h->cu[2]);
   DG_LAUNCHED();
@@ -1410,6 +1412,7 @@ int dg_cn_solve_dev(dg_handle *h, int rk_step) {
   const size_t sm = sizeof(double2) * L * COL_MT + sizeof(double) * 5 * L;
   dg_big_smem((const void *)k_cn_col);
   dim3 grid(dg_cdiv(h->ss, COL_MT), h->nf);
+  dg_kt_begin(h, "k_cn_col", h->st);
   k_cn_col<<<grid, COL_THR, sm, h->st>>>(h->NY, h->ss, tab, rhs, cu,
                                          make_int4(wl[0], wl[1], wl[2], wl[3]),
                                          make_int4(wl[4], wl[5], wl[6], wl[7]));
@@ -1421,6 +1424,7 @@ int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step) {
   const int L = h->NY + 2;
   const size_t sm = sizeof(double2) * L * COL_MT + sizeof(double) * (2 * L * COL_MT + L);
   dg_big_smem((const void *)k_rd_col);
+  dg_kt_begin(h, "k_rd_col", h->st);
   k_rd_col<<<dg_cdiv(h->ss, COL_MT), COL_THR, sm, h->st>>>(
       h->NY, h->ss, h->nkxp, h->jstart, h->jend, update_cp ? rk_step : 0, h->kx, h->kz, h->dy,
       h->dyf, h->rem_a, h->rem_rb, h->cu[0], h->cu[1], h->cu[2], h->cp, h->cr1, h->dscal);
@@ -1458,12 +1462,14 @@ int dg_courant_dev(dg_handle *h, const double2 *const *u) {
   DG_TRY(dg_zinv(h, u, 3, 1, h->NY, h->H, 0));
   DG_CUDA(cudaMemsetAsync(h->dmin_bits, 0x7f, sizeof(unsigned long long), h->st));
   DG_TRY(dg_xc2r_cfl(h, h->H, 1, h->NY, h->dmin_bits));
+  dg_kt_begin(h, "k_dt_update", h->st);
   k_dt_update<<<1, 1, 0, h->st>>>(h->dscal, h->dmin_bits, courant_dt0(h));
   DG_LAUNCHED();
   return DG_OK;
 }
 
 int dg_dt_commit(dg_handle *h) {
+  dg_kt_begin(h, "k_dt_commit", h->st);
   k_dt_commit<<<1, 1, 0, h->st>>>(h->dscal);
   DG_LAUNCHED();
   // the new tables are first needed by the next substep's CN solve: build them
@@ -1481,6 +1487,7 @@ int dg_dt_commit(dg_handle *h) {
 }
 
 int dg_chan_init(dg_handle *h) {
+  dg_kt_begin(h, "k_remdiv_init", h->st);
   k_remdiv_init<<<dg_cdiv(h->ss, 128), 128, 0, h->st>>>(h->NY, h->ss, h->nkxp, h->kx, h->kz, h->dy,
                                                         h->dyf, h->rem_a, h->rem_rb);
   DG_LAUNCHED();
@@ -1522,6 +1529,7 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
 #define XW_CASE(NXV, NTHV)                                                                         \
   if (h->NX == NXV && h->NTH == NTHV) {                                                          \
     dg_big_smem((const void *)k_xrow_w<NXV, NTHV>);                                              \
+    dg_kt_begin(h, "k_xrow_w", h->st);                                                             \
     k_xrow_w<NXV, NTHV><<<grid, 32 * XW_WARPS, xw_smem<NXV, NTHV>(), h->st>>>(                    \
         C, h->H, Hfield, chunk, a, b, h->twx, h->dyf, h->dy, h->kx, h->G, Hfield);               \
     done = true;                                                                                 \
@@ -1542,6 +1550,7 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
         const size_t sm = xrow_smem(h);
 #define KERNEL_BODY(N)                                                                          \
   dg_big_smem((const void *)k_xrow_nl<N>);                                                      \
+  dg_kt_begin(h, "k_xrow_nl", h->st);                                                               \
   k_xrow_nl<N><<<grid, XR_THR, sm, h->st>>>(C, h->H, Hfield, chunk, h->plx, h->twx, h->dyf, h->dy, \
                                             h->kx, h->G, Hfield)
         switch (h->NX) {
@@ -1560,6 +1569,7 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
 #define ZW_CASE(N)                                                                             \
   if (h->NZ == N) {                                                                            \
     dg_big_smem((const void *)k_zfwd_w<N>);                                                    \
+    dg_kt_begin(h, "k_zfwd_w", h->st);                                                          \
     k_zfwd_w<N><<<grid, 128, sm, h->st>>>(C, h->G, Hfield, h->twz, h->dscal, rk_step, h->kx,   \
                                           h->kz, h->dy, h->dyf, cu, cf, rhs, h->cp, a);        \
     zdone = true;                                                                              \
@@ -1576,6 +1586,7 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
         const size_t sm = zfwd_smem(h);
 #define KERNEL_BODY(N)                                                                          \
   dg_big_smem((const void *)k_zfwd_rhs<N>);                                                     \
+  dg_kt_begin(h, "k_zfwd_rhs", h->st);                                                            \
   k_zfwd_rhs<N><<<grid, ZF_THR, sm, h->st>>>(C, h->G, Hfield, h->plz, h->twz, h->dscal, rk_step, \
                                              h->kx, h->kz, h->dy, h->dyf, cu, cf, rhs, h->cp)
         if (!zdone && (!done ? a == 1 : b == h->NY)) {
@@ -1628,6 +1639,7 @@ int dg_stats_dev(dg_handle *h, dg_stats *s) {
   CFieldPtrs u;
   for (int f = 0; f < h->nf; f++) u.p[f] = h->cu[f];
   DG_CUDA(cudaMemsetAsync(h->dflag, 0, sizeof(int), h->st));
+  dg_kt_begin(h, "k_stats_planes", h->st);
   k_stats_planes<<<NP, 256, 0, h->st>>>(NP, h->ss, h->nkxp, u, h->nf, dsum, h->dflag);
   DG_LAUNCHED();
   double *hs = (double *)malloc(sizeof(double) * 8 * NP);
@@ -1685,6 +1697,7 @@ int dg_stats_dev(dg_handle *h, dg_stats *s) {
   free(hs);
   // max |div u| on rows 2..NY-1 in physical space
   double2 *dspec = h->rhs[0];
+  dg_kt_begin(h, "k_div_spec", h->st);
   k_div_spec<<<dg_cdiv((long)(NY + 2) * h->ss, 256), 256, 0, h->st>>>(
       NY, h->ss, h->nkxp, h->kx, h->kz, h->dyf, h->cu[0], h->cu[1], h->cu[2], dspec);
   DG_LAUNCHED();
@@ -1694,6 +1707,7 @@ int dg_stats_dev(dg_handle *h, dg_stats *s) {
   double *phys = (double *)h->work;
   DG_TRY(dg_xc2r_planes(h, h->H, 1, 2, NY - 1, phys - 2 * pplane, pplane, h->NX, 0));
   DG_CUDA(cudaMemsetAsync(h->dmin_bits, 0, sizeof(unsigned long long), h->st));
+  dg_kt_begin(h, "k_absmax", h->st);
   k_absmax<<<4 * 148, 256, 0, h->st>>>(phys, (long)(NY - 2) * pplane, h->dmin_bits);
   DG_LAUNCHED();
   unsigned long long bits = 0;

@@ -128,6 +128,7 @@ extern "C" int diablo_poisson_p_chan(dg_handle *h) {
   const long nint = (long)(NY - 1) * ss;  // rows 2..NY
   const long nphys = (long)(NY - 1) * pplane;
   for (int stage = 0; stage < 4; stage++) {
+    dg_kt_begin(h, "k_ppc_prep", h->st);
     k_ppc_prep<<<dg_cdiv(nint, 256), 256, 0, h->st>>>(stage, NY, ss, h->nkxp, h->kx, h->kz,
                                                       h->dyf, h->cu[0], h->cu[1], h->cu[2], s[0],
                                                       s[1], s[2]);
@@ -138,6 +139,7 @@ extern "C" int diablo_poisson_p_chan(dg_handle *h) {
     // stage 0 fills W0..W2, later stages W1..W2
     double *dst = (stage == 0) ? W : W + pfield;
     DG_TRY(dg_xc2r_planes(h, h->H, nf, 2, NY, dst, pplane, h->NX, pfield));
+    dg_kt_begin(h, "k_ppc_accum", h->st);
     k_ppc_accum<<<4 * 148, 256, 0, h->st>>>(stage, nphys, W + 2 * pplane,
                                             W + pfield + 2 * pplane, W + 2 * pfield + 2 * pplane);
     DG_LAUNCHED();
@@ -149,6 +151,7 @@ extern "C" int diablo_poisson_p_chan(dg_handle *h) {
   for (int n = 0; n < h->NTH; n++) th.p[n] = h->cu[3 + n];
   RiVals ri;
   for (int n = 0; n < DG_MAX_TH; n++) ri.v[n] = (n < h->NTH) ? h->p.ri[n] : 0.0;
+  dg_kt_begin(h, "k_ppc_col", h->st);
   k_ppc_col<<<dg_cdiv(ss, 128), 128, 0, h->st>>>(NY, ss, h->NTH, ri, h->gyf, h->dy, h->dyf,
                                                  h->rem_a, h->rem_rb, s[0], th, h->cp);
   DG_LAUNCHED();

@@ -64,6 +64,8 @@ enum { ROW_ZERO = 0, ROW_RHS = 1, ROW_BC = 2 };
 // field slots in the solver (velocity then scalars)
 enum { F_U1 = 0, F_U2 = 1, F_U3 = 2, F_TH0 = 3 };
 
+struct dg_ktimer;
+
 struct dg_handle {
   dg_params p;
   int NX, NY, NZ, NTH, NKX, NKZ, TNKZ, NKY, TNKY;
@@ -116,7 +118,15 @@ struct dg_handle {
   double2 *Hy;                  // y-inverse output [nf][NY][nkzt][nkxp]
   double2 *P;                   // products [9][NY][NZ][nkxp] then [9][NY][nkzt][nkxp]
   double2 *Q;                   // z-forward products [9][NY][nkzt][nkxp]
+
+  dg_ktimer *kt;                // per-kernel event timing (null unless enabled)
 };
+
+// kernel timing: begin before a launch on stream st; the launch accounting
+// after the launch ends it
+void dg_kt_begin(dg_handle *h, const char *name, cudaStream_t st);
+void dg_kt_end();
+void dg_kt_free(dg_handle *h);
 
 // common kernel-launch helpers (defined in fft_kernels.cu)
 int dg_cinv_g(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax,

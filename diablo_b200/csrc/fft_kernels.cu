@@ -318,6 +318,7 @@ int dg_cinv_g(dg_handle *h, const double2 *const *fields, int nf, int jmin, int 
   const size_t sm = zsmem(N);
 #define KERNEL_BODY(NN)                                                                       \
   big_smem(k_zinv<NN>);                                                                       \
+  dg_kt_begin(h, "k_zinv", h->st);                                                              \
   k_zinv<NN><<<grid, NTHR, sm, h->st>>>(fp, jmin, in_plane, rowlen, N, NK, pl, tw, H, out_field)
   switch (N) {
     DG_FOR_EACH_N(DG_CASE_N)
@@ -338,6 +339,7 @@ int dg_cfwd_g(dg_handle *h, const double2 *H, long in_field, int nf, int jmin, i
   const size_t sm = zsmem(N);
 #define KERNEL_BODY(NN)                                                                        \
   big_smem(k_zfwd<NN>);                                                                        \
+  dg_kt_begin(h, "k_zfwd", h->st);                                                              \
   k_zfwd<NN><<<grid, NTHR, sm, h->st>>>(H, in_field, jmin, rowlen, nkt, N, NK, pl, tw, fp, out_plane)
   switch (N) {
     DG_FOR_EACH_N(DG_CASE_N)
@@ -368,6 +370,7 @@ int dg_xc2r_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax, d
   const long Hf = (long)h->nplanes * h->NZ * h->nkxp;
 #define KERNEL_BODY(N)                                                                     \
   big_smem(k_xc2r<N>);                                                                     \
+  dg_kt_begin(h, "k_xc2r", h->st);                                                                \
   k_xc2r<N><<<grid, NTHR, sm, h->st>>>(H, Hf, jmin, h->nkxp, h->NX, h->NZ, h->plx, h->twx, phys, \
                                       pplane, prow, pfield)
   switch (h->NX) {
@@ -387,6 +390,7 @@ int dg_xr2c_planes(dg_handle *h, const double *phys, int nf, int jmin, int jmax,
   const long Hf = (long)h->nplanes * h->NZ * h->nkxp;
 #define KERNEL_BODY(N)                                                                        \
   big_smem(k_xr2c<N>);                                                                        \
+  dg_kt_begin(h, "k_xr2c", h->st);                                                                 \
   k_xr2c<N><<<grid, NTHR, sm, h->st>>>(phys, pplane, prow, pfield, jmin, h->nkxp, h->NX, h->NZ,   \
                                       h->plx, h->twx, H, Hf)
   switch (h->NX) {
@@ -405,6 +409,7 @@ int dg_xc2r_cfl(dg_handle *h, const double2 *H, int jmin, int jmax, unsigned lon
   const double dxv = h->p.lx / h->NX, dzv = h->p.lz / h->NZ;
 #define KERNEL_BODY(N)                                                                          \
   big_smem(k_xc2r_cfl<N>);                                                                      \
+  dg_kt_begin(h, "k_xc2r_cfl", h->st);                                                              \
   k_xc2r_cfl<N><<<grid, NTHR, sm, h->st>>>(H, Hf, jmin, h->nkxp, h->NX, h->NZ, h->plx, h->twx,     \
                                           h->p.cfl, dxv, dzv, h->dy, out)
   switch (h->NX) {

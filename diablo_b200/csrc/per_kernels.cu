@@ -497,6 +497,7 @@ extern "C" int diablo_rk_per_1(dg_handle *h, int rk_step) {
 #define PW_CASE(NXV, NTHV)                                                                     \
   if (!done && h->NX == NXV && h->NTH == NTHV) {                                               \
     dg_big_smem((const void *)k_prod_per_w<NXV, NTHV>);                                        \
+    dg_kt_begin(h, "k_prod_per_w", h->st);                                                       \
     k_prod_per_w<NXV, NTHV><<<dg_cdiv(rows, 4), 128, prod_smem<NXV, NTHV>(), h->st>>>(          \
         C, h->H, h_field(h), h->twx, h->P, h_field(h));                                       \
     done = true;                                                                               \
@@ -516,6 +517,7 @@ extern "C" int diablo_rk_per_1(dg_handle *h, int rk_step) {
       DG_TRY(dg_xc2r_planes(&tmp, h->H + f * h_field(h), 1, 0, h->NY - 1, phys + f * phys_field(h),
                             (long)h->NZ * h->NX, h->NX, 0));
     double *prod = phys + (long)nf * phys_field(h);
+    dg_kt_begin(h, "k_prod_phys", h->st);
     k_prod_phys<<<4 * 148, 256, 0, h->st>>>(phys, phys_field(h), h->NTH, phys_field(h), prod);
     DG_LAUNCHED();
     for (int p = 0; p < np; p++)
@@ -541,6 +543,7 @@ extern "C" int diablo_rk_per_1(dg_handle *h, int rk_step) {
   FieldPtrs cu, cf;
   for (int f = 0; f < nf; f++) { cu.p[f] = h->cu[f]; cf.p[f] = h->cf[f]; }
   const long tot = (long)h->nkyt * h->ss;
+  dg_kt_begin(h, "k_per_final", h->st);
   k_per_final<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(C, rk_step, h->dscal, h->kx, h->ky, h->kz,
                                                     h->Q, fy_field(h), cu, cf, h->cp, h->cr1,
                                                     forcing);
@@ -552,6 +555,7 @@ extern "C" int diablo_rem_div_per(dg_handle *h) {
   if (!h || !h->periodic) return DG_ERR_ARG;
   const PerConst C = make_pc(h);
   const long tot = (long)h->nkyt * h->ss;
+  dg_kt_begin(h, "k_rem_div_per", h->st);
   k_rem_div_per<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[0], h->cu[1],
                                                       h->cu[2], h->cr1);
   DG_LAUNCHED();
@@ -566,13 +570,16 @@ extern "C" int diablo_poisson_p_per(dg_handle *h) {
   double *W = (double *)h->work;  // 6 physical fields
   double2 *s0 = h->rhs[0], *s1 = h->rhs[1];
   // R1 = IFFT(i kx U1), R2 = IFFT(i kz U3); P = R1^2 + R1 R2 + R2^2
+  dg_kt_begin(h, "k_ik", h->st);
   k_ik<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[0], 0, s0);
   DG_LAUNCHED();
+  dg_kt_begin(h, "k_ik", h->st);
   k_ik<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[2], 2, s1);
   DG_LAUNCHED();
   const double2 *pr[2] = {s0, s1};
   DG_TRY(per_to_physical(h, pr, 2, W));
   double *P = W + 2 * n;
+  dg_kt_begin(h, "k_pp_first", h->st);
   k_pp_first<<<4 * 148, 256, 0, h->st>>>(n, W, W + n, P);
   DG_LAUNCHED();
   // copy P aside (W is reused), then the six gradient products
@@ -580,18 +587,22 @@ extern "C" int diablo_poisson_p_per(dg_handle *h) {
   DG_CUDA(cudaMemcpyAsync(Psave, P, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->st));
   struct G { int src, axis; } g[6] = {{0, 1}, {1, 0}, {0, 2}, {2, 0}, {1, 2}, {2, 1}};
   for (int k = 0; k < 6; k += 2) {
+    dg_kt_begin(h, "k_ik", h->st);
     k_ik<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[g[k].src], g[k].axis, s0);
     DG_LAUNCHED();
+    dg_kt_begin(h, "k_ik", h->st);
     k_ik<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[g[k + 1].src],
                                                g[k + 1].axis, s1);
     DG_LAUNCHED();
     DG_TRY(per_to_physical(h, pr, 2, W + k * n));
   }
+  dg_kt_begin(h, "k_pp_second", h->st);
   k_pp_second<<<4 * 148, 256, 0, h->st>>>(n, W, Psave);
   DG_LAUNCHED();
   DG_CUDA(cudaMemcpyAsync(W, Psave, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->st));
   double2 *out[1] = {h->cp};
   DG_TRY(per_to_fourier(h, W, 1, out));
+  dg_kt_begin(h, "k_pp_solve", h->st);
   k_pp_solve<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cp);
   DG_LAUNCHED();
   return DG_OK;
@@ -605,6 +616,7 @@ static int per_sums(dg_handle *h, double tot[8]) {
   CFieldPtrs u;
   for (int f = 0; f < h->nf; f++) u.p[f] = h->cu[f];
   DG_CUDA(cudaMemsetAsync(h->dflag, 0, sizeof(int), h->st));
+  dg_kt_begin(h, "k_per_sums", h->st);
   k_per_sums<<<h->nkyt, 256, 0, h->st>>>(C, u, dsum, h->dflag);
   DG_LAUNCHED();
   double *hs = (double *)malloc(sizeof(double) * 8 * h->nkyt);
@@ -644,6 +656,7 @@ int dg_per_stats(dg_handle *h, dg_stats *s) {
   }
   // max |div u| in physical space
   const long tot_m = (long)h->nkyt * h->ss;
+  dg_kt_begin(h, "k_div_per", h->st);
   k_div_per<<<dg_cdiv(tot_m, 256), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[0], h->cu[1],
                                                     h->cu[2], h->rhs[0]);
   DG_LAUNCHED();
@@ -651,6 +664,7 @@ int dg_per_stats(dg_handle *h, dg_stats *s) {
   double *W = (double *)h->work;
   DG_TRY(per_to_physical(h, d, 1, W));
   DG_CUDA(cudaMemsetAsync(h->dmin_bits, 0, sizeof(unsigned long long), h->st));
+  dg_kt_begin(h, "k_absmax_p", h->st);
   k_absmax_p<<<4 * 148, 256, 0, h->st>>>(W, phys_field(h), h->dmin_bits);
   DG_LAUNCHED();
   unsigned long long bits = 0;
@@ -728,6 +742,7 @@ extern "C" int diablo_fft_xzy_to_fourier(dg_handle *h, const double *U, double *
   double *out = (where == DG_DEVICE) ? CU : b.d;
   if (s == DG_OK) {
     const long tot = (long)ny2 * nz2 * (nxp2 / 2);
+    dg_kt_begin(h, "k_xzy_compact_to_ref", h->st);
     k_xzy_compact_to_ref<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(h->rhs[0], (double2 *)out, ny2,
                                                                 h->nkyt, h->nkzt, h->nkxp,
                                                                 nxp2 / 2, nz2);
@@ -750,6 +765,7 @@ extern "C" int diablo_fft_xzy_to_physical(dg_handle *h, const double *CU, double
   RefBuf b;
   DG_TRY(ref_acquire(h, CU, where, bytes, &b));
   const long tot = (long)h->nkyt * h->ss;
+  dg_kt_begin(h, "k_xzy_ref_to_compact", h->st);
   k_xzy_ref_to_compact<<<dg_cdiv(tot, 256), 256, 0, h->st>>>((const double2 *)b.d, h->rhs[0],
                                                               h->nkyt, h->nkzt, h->nkxp, nxp2 / 2,
                                                               nz2);

@@ -63,7 +63,10 @@ __global__ void k_advance_time(double *dscal) { dscal[0] = dscal[0] + dscal[1]; 
 }  // namespace
 
 void dg_set_error(const char *msg) { g_err = msg ? msg : ""; }
-void dg_count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void dg_count_launch(int n) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+  dg_kt_end();
+}
 
 extern "C" int dg_version(void) { return 100; }
 extern "C" const char *dg_last_error(void) { return g_err.c_str(); }
@@ -290,6 +293,7 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
     if (h->rhs[f]) cudaFree(h->rhs[f]);
   }
   cudaStreamSynchronize(h->st2);
+  dg_kt_free(h);
   cudaEventDestroy(h->ev_fork);
   cudaEventDestroy(h->ev_join);
   cudaStreamDestroy(h->st2);

@@ -162,6 +162,16 @@ int diablo_poisson_p_per(dg_handle *h);
 int diablo_fft_xzy_to_fourier(dg_handle *h, const double *U, double *CU, int where);
 int diablo_fft_xzy_to_physical(dg_handle *h, const double *CU, double *U, int where);
 
+/* ------------------------------------------------------ kernel timing */
+/* No counterpart in the reference (measurement and tuning).  on = 1 clears
+ * the totals and brackets every later launch of this handle's kernels with a
+ * CUDA event pair on the launch's stream; on = 0 stops recording.
+ * dg_timing_read waits for the recorded pairs and returns, for the i-th
+ * kernel name seen (0-based), its launch count and total device time. */
+int dg_timing_enable(dg_handle *h, int on);
+int dg_timing_read(dg_handle *h, int i, char *name, int name_len, int64_t *launches,
+                   double *total_ms);
+
 /* ------------------------------------------- allocation-free transform */
 /* No counterpart in the reference.  FFT_XZ_TO_FOURIER(V,VV,JMIN,JMAX) on
  * DEVICE arrays in the reference layout (as diablo_fft_xz_to_fourier with

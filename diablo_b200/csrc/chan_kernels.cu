@@ -1472,6 +1472,7 @@ int dg_dt_commit(dg_handle *h) {
   dg_kt_begin(h, "k_dt_commit", h->st);
   k_dt_commit<<<1, 1, 0, h->st>>>(h->dscal);
   DG_LAUNCHED();
+  if (h->defer_tables) return DG_OK;  // the next full step rebuilds them first
   // the new tables are first needed by the next substep's CN solve: build them
   // on the side stream while the nonlinear terms of that substep run
   DG_CUDA(cudaEventRecord(h->ev_fork, h->st));

@@ -120,7 +120,16 @@ struct dg_handle {
   double2 *Q;                   // z-forward products [9][NY][nkzt][nkxp]
 
   dg_ktimer *kt;                // per-kernel event timing (null unless enabled)
+
+  // full-step CUDA graphs (variant 0: no COURANT, 1: with COURANT)
+  cudaGraphExec_t gexec[2];
+  bool gwarm[2];
+  long long gkernels[2];        // kernels per replay of each variant
+  bool capturing;
+  bool defer_tables;            // dt commit leaves the CN tables to the next step
 };
+
+void dg_graphs_free(dg_handle *h);
 
 // kernel timing: begin before a launch on stream st; the launch accounting
 // after the launch ends it

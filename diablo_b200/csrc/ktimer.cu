@@ -44,7 +44,7 @@ void settle(dg_ktimer *t, int s) {
 
 void dg_kt_begin(dg_handle *h, const char *name, cudaStream_t st) {
   dg_ktimer *t = h ? h->kt : nullptr;
-  if (!t || !t->on) return;
+  if (!t || !t->on || h->capturing) return;
   int k = -1;
   for (size_t i = 0; i < t->names.size(); i++)
     if (t->names[i] == name) {

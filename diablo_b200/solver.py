@@ -67,6 +67,11 @@ class _Solver:
     def _call(self, name, *args):
         _lib.check(name, getattr(self.L, name)(self.h, *args))
 
+    def steps(self, time_step: int, nsteps: int):
+        """nsteps full RK3 steps from time_step (the driver loop body,
+        for/diablo.f:70-109), replayed as CUDA graphs after the first."""
+        self._call("diablo_step", time_step, nsteps)
+
     # ---- state I/O
     def set_field(self, name: str, arr: np.ndarray, layout: str = "compact"):
         a = np.ascontiguousarray(arr, dtype=np.complex128)

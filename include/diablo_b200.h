@@ -147,6 +147,13 @@ int diablo_thomas_real(double *A, double *B, double *C, double *G, int ny, int n
 int diablo_thomas_complex(double *A, double *B, double *C, double *G, int ny, int nx,
                           int where);
 
+/* The driver's time-step loop body (for/diablo.f:70-109) for nsteps steps
+ * starting at time_step: RK_CHAN_1 / RK_PER_1 for RK_STEP = 1..3, then
+ * TIME = TIME + DELTA_T.  After the first step of a kind, steps replay a
+ * captured CUDA graph (one host launch per step); results are identical to
+ * calling the substep entry points. */
+int diablo_step(dg_handle *h, int time_step, int nsteps);
+
 /* ------------------------------------------------------ periodic hot path */
 /* SUBROUTINE RK_PER_1 (for/periodic.f:23-285). */
 int diablo_rk_per_1(dg_handle *h, int rk_step);

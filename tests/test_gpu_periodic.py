@@ -211,3 +211,19 @@ def test_periodic_256_cubed_parity():
     assert abs(sg["ke"] - so["ke"]) <= 1e-12 * so["ke"]
     assert sg["div_max"] <= 1e-12 * 256
     g.close()
+
+
+def test_graph_steps_match_substep_calls():
+    p = box((32, 32, 32), n_th=1)
+    p.ri = [0.2, 0, 0, 0]
+    ref, a = seeded_pair(p, seed=9, scalars=[0.5])
+    b = periodic(p)
+    b.set_state(ref.state())
+    b.set_time(0.0, p.delta_t)
+    for s in range(1, 9):
+        a.step(s)
+    b.steps(1, 8)
+    for nm in fields(p) + ["CP"]:
+        assert np.array_equal(a.get_field(nm), b.get_field(nm)), nm
+    a.close()
+    b.close()

@@ -85,6 +85,8 @@ def load(path: str = LIB_PATH):
         "diablo_fft_xzy_to_fourier": [P, P, P, I], "diablo_fft_xzy_to_physical": [P, P, P, I],
         "diablo_fft_xz_to_fourier_noalloc": [P, P, I, I, I, I, I, P],
         "dg_timing_enable": [P, I], "diablo_step": [P, I, I],
+        "dg_tune_set": [P, I, I], "dg_tune_get": [P, I, ctypes.POINTER(I)],
+        "dg_autotune": [P, I],
         "dg_timing_read": [P, I, ctypes.c_char_p, I, ctypes.POINTER(ctypes.c_int64),
                            ctypes.POINTER(D)],
         "diablo_stats": [P, ctypes.POINTER(DgStats)],

@@ -257,7 +257,7 @@ __host__ __device__ constexpr bool xw_supported(int n) {
 }
 
 template <int NX, int NTH>
-__global__ void __launch_bounds__(32 * XW_WARPS, 3) k_xrow_w(
+__global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? 3 : 2) k_xrow_w(
     ChanConst C, const double2 *__restrict__ H, long Hfield, int chunk, int jbase, int jtop,
     const double2 *__restrict__ tw, const double *__restrict__ dyf, const double *__restrict__ dy,
     const double *__restrict__ kxv, double2 *__restrict__ G, long Gfield) {
@@ -498,16 +498,16 @@ __global__ void __launch_bounds__(ZF_THR) k_zfwd_rhs(
     const double k2 = KX * KX + KZ * KZ;
     const double kk = (C.beta == 1.0) ? k2 : pow(k2, C.beta);
     const bool mean = (kx == 0 && kp == 0);
-    const double2 u1 = cu.p[0][o], u2 = cu.p[1][o], u3 = cu.p[2][o];
+    const double2 u1 = cu(0)[o], u2 = cu(1)[o], u3 = cu(2)[o];
     const double2 p0 = cp[o];
     // ---- U1 and U3 (rows JSTART..JEND)
     if (j >= C.JS && j <= C.JE) {
-      const double2 u1m = cu.p[0][o - ss], u1p = cu.p[0][o + ss];
-      const double2 u3m = cu.p[2][o - ss], u3p = cu.p[2][o + ss];
+      const double2 u1m = cu(0)[o - ss], u1p = cu(0)[o + ss];
+      const double2 u3m = cu(2)[o - ss], u3p = cu(2)[o + ss];
       double2 f1 = make_double2(-NU * kk * u1.x + C.i_ro * u3.x, -NU * kk * u1.y + C.i_ro * u3.y);
       double2 f3 = make_double2(-NU * kk * u3.x - C.i_ro * u1.x, -NU * kk * u3.y - C.i_ro * u1.y);
       for (int n = 0; n < C.nth; n++) {
-        const double2 t = cu.p[3 + n][o];
+        const double2 t = cu(3 + n)[o];
         f1.x += C.ri[n] * C.grav_x * t.x; f1.y += C.ri[n] * C.grav_x * t.y;
         f3.x += C.ri[n] * C.grav_z * t.x; f3.y += C.ri[n] * C.grav_z * t.y;
       }
@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(ZF_THR) k_zfwd_rhs(
       f3.x += n3.x; f3.y += n3.y;
       double2 r1 = u1, r3 = u3;
       if (rk_step > 1) {
-        const double2 o1 = cf.p[0][o], o3 = cf.p[2][o];
+        const double2 o1 = cf(0)[o], o3 = cf(2)[o];
         r1.x += T3 * o1.x; r1.y += T3 * o1.y;
         r3.x += T3 * o3.x; r3.y += T3 * o3.y;
       }
@@ -534,18 +534,18 @@ __global__ void __launch_bounds__(ZF_THR) k_zfwd_rhs(
       r1.y += a * (((u1p.y - u1.y) / dyj1 - (u1.y - u1m.y) / dyj) / dyfj);
       r3.x += a * (((u3p.x - u3.x) / dyj1 - (u3.x - u3m.x) / dyj) / dyfj);
       r3.y += a * (((u3p.y - u3.y) / dyj1 - (u3.y - u3m.y) / dyj) / dyfj);
-      cf.p[0][o] = f1;
-      cf.p[2][o] = f3;
-      rhs.p[0][o] = r1;
-      rhs.p[2][o] = r3;
+      cf(0)[o] = f1;
+      cf(2)[o] = f3;
+      rhs(0)[o] = r1;
+      rhs(2)[o] = r3;
     }
     // ---- U2 (rows 2..NY)
     if (j >= 2 && j <= C.NY) {
-      const double2 u2m = cu.p[1][o - ss], u2p = cu.p[1][o + ss];
+      const double2 u2m = cu(1)[o - ss], u2p = cu(1)[o + ss];
       double2 f2 = make_double2(-NU * kk * u2.x, -NU * kk * u2.y);
       if (!mean) {
         for (int n = 0; n < C.nth; n++) {
-          const double2 t = cu.p[3 + n][o], tm = cu.p[3 + n][o - ss];
+          const double2 t = cu(3 + n)[o], tm = cu(3 + n)[o - ss];
           const double w = C.ri[n] * C.grav_y;
           f2.x += w * (t.x * dyfm + tm.x * dyfj) / (2.0 * dyj);
           f2.y += w * (t.y * dyfm + tm.y * dyfj) / (2.0 * dyj);
@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(ZF_THR) k_zfwd_rhs(
       f2.x += n2.x; f2.y += n2.y;
       double2 r2 = u2;
       if (rk_step > 1) {
-        const double2 o2 = cf.p[1][o];
+        const double2 o2 = cf(1)[o];
         r2.x += T3 * o2.x; r2.y += T3 * o2.y;
       }
       const double2 pm = cp[o - ss];
@@ -565,13 +565,13 @@ __global__ void __launch_bounds__(ZF_THR) k_zfwd_rhs(
       const double a = T1 * NUV;
       r2.x += a * (((u2p.x - u2.x) / dyfj - (u2.x - u2m.x) / dyfm) / dyj);
       r2.y += a * (((u2p.y - u2.y) / dyfj - (u2.y - u2m.y) / dyfm) / dyj);
-      cf.p[1][o] = f2;
-      rhs.p[1][o] = r2;
+      cf(1)[o] = f2;
+      rhs(1)[o] = r2;
     }
     // ---- scalars (rows JSTART_TH..JEND_TH)
     for (int n = 0; n < C.nth; n++) {
       if (j < C.JSt[n] || j > C.JEt[n]) continue;
-      const double2 t = cu.p[3 + n][o], tm = cu.p[3 + n][o - ss], tp = cu.p[3 + n][o + ss];
+      const double2 t = cu(3 + n)[o], tm = cu(3 + n)[o - ss], tp = cu(3 + n)[o + ss];
       const double nup = NU / C.pr[n];
       double2 ft = make_double2(-nup * kk * t.x - u1.x * C.drhodx[n] - u3.x * C.drhodz[n],
                                 -nup * kk * t.y - u1.y * C.drhodx[n] - u3.y * C.drhodz[n]);
@@ -579,15 +579,15 @@ __global__ void __launch_bounds__(ZF_THR) k_zfwd_rhs(
       ft.x += nt.x; ft.y += nt.y;
       double2 rt = t;
       if (rk_step > 1) {
-        const double2 ot = cf.p[3 + n][o];
+        const double2 ot = cf(3 + n)[o];
         rt.x += T3 * ot.x; rt.y += T3 * ot.y;
       }
       rt.x += T5 * ft.x; rt.y += T5 * ft.y;
       const double a = (T1 / C.pr[n]) * NUV;
       rt.x += a * (((tp.x - t.x) / dyj1 - (t.x - tm.x) / dyj) / dyfj);
       rt.y += a * (((tp.y - t.y) / dyj1 - (t.y - tm.y) / dyj) / dyfj);
-      cf.p[3 + n][o] = ft;
-      rhs.p[3 + n][o] = rt;
+      cf(3 + n)[o] = ft;
+      rhs(3 + n)[o] = rt;
     }
   }
 }
@@ -666,13 +666,13 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
     const bool mean = (kx == 0 && kp == 0);
     if (f == 0 || f == 2) {
       // U1 / U3 (rows JSTART..JEND)
-      const double2 u = cu.p[f][o], um = cu.p[f][o - ss], up = cu.p[f][o + ss];
-      const double2 uo = cu.p[2 - f][o];  // the other horizontal component (Coriolis)
+      const double2 u = cu(f)[o], um = cu(f)[o - ss], up = cu(f)[o + ss];
+      const double2 uo = cu(2 - f)[o];  // the other horizontal component (Coriolis)
       const double sgn = (f == 0) ? 1.0 : -1.0;
       const double gr = (f == 0) ? C.grav_x : C.grav_z;
       double2 fv = make_double2(-NU * kk * u.x + sgn * C.i_ro * uo.x, -NU * kk * u.y + sgn * C.i_ro * uo.y);
       for (int n = 0; n < C.nth; n++) {
-        const double2 t = cu.p[3 + n][o];
+        const double2 t = cu(3 + n)[o];
         fv.x += C.ri[n] * gr * t.x;
         fv.y += C.ri[n] * gr * t.y;
       }
@@ -680,7 +680,7 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
       fv.y += nlv.y;
       double2 r = u;
       if (rk_step > 1) {
-        const double2 old = cf.p[f][o];
+        const double2 old = cf(f)[o];
         r.x += T3 * old.x;
         r.y += T3 * old.y;
       }
@@ -697,15 +697,15 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
       const double aa = T1 * NUV;
       r.x += aa * (((up.x - u.x) / dyj1 - (u.x - um.x) / dyj) / dyfj);
       r.y += aa * (((up.y - u.y) / dyj1 - (u.y - um.y) / dyj) / dyfj);
-      cf.p[f][o] = fv;
-      rhs.p[f][o] = r;
+      cf(f)[o] = fv;
+      rhs(f)[o] = r;
     } else if (f == 1) {
       // U2 (rows 2..NY)
-      const double2 u = cu.p[1][o], um = cu.p[1][o - ss], up = cu.p[1][o + ss];
+      const double2 u = cu(1)[o], um = cu(1)[o - ss], up = cu(1)[o + ss];
       double2 fv = make_double2(-NU * kk * u.x, -NU * kk * u.y);
       if (!mean) {
         for (int n = 0; n < C.nth; n++) {
-          const double2 t = cu.p[3 + n][o], tm = cu.p[3 + n][o - ss];
+          const double2 t = cu(3 + n)[o], tm = cu(3 + n)[o - ss];
           const double w = C.ri[n] * C.grav_y;
           fv.x += w * (t.x * dyfm + tm.x * dyfj) / (2.0 * dyj);
           fv.y += w * (t.y * dyfm + tm.y * dyfj) / (2.0 * dyj);
@@ -715,7 +715,7 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
       fv.y += nlv.y;
       double2 r = u;
       if (rk_step > 1) {
-        const double2 old = cf.p[1][o];
+        const double2 old = cf(1)[o];
         r.x += T3 * old.x;
         r.y += T3 * old.y;
       }
@@ -727,16 +727,16 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
       const double aa = T1 * NUV;
       r.x += aa * (((up.x - u.x) / dyfj - (u.x - um.x) / dyfm) / dyj);
       r.y += aa * (((up.y - u.y) / dyfj - (u.y - um.y) / dyfm) / dyj);
-      cf.p[1][o] = fv;
-      rhs.p[1][o] = r;
+      cf(1)[o] = fv;
+      rhs(1)[o] = r;
     } else {
       // scalar n (rows JSTART_TH..JEND_TH)
       const int n = f - 3;
-      const double2 t = cu.p[f][o], tm = cu.p[f][o - ss], tp = cu.p[f][o + ss];
+      const double2 t = cu(f)[o], tm = cu(f)[o - ss], tp = cu(f)[o + ss];
       const double nup = NU / C.pr[n];
       double2 fv = make_double2(-nup * kk * t.x, -nup * kk * t.y);
       if (C.drhodx[n] != 0.0 || C.drhodz[n] != 0.0) {
-        const double2 u1 = cu.p[0][o], u3 = cu.p[2][o];
+        const double2 u1 = cu(0)[o], u3 = cu(2)[o];
         fv.x = fv.x - u1.x * C.drhodx[n] - u3.x * C.drhodz[n];
         fv.y = fv.y - u1.y * C.drhodx[n] - u3.y * C.drhodz[n];
       }
@@ -744,7 +744,7 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
       fv.y += nlv.y;
       double2 r = t;
       if (rk_step > 1) {
-        const double2 old = cf.p[f][o];
+        const double2 old = cf(f)[o];
         r.x += T3 * old.x;
         r.y += T3 * old.y;
       }
@@ -753,8 +753,8 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
       const double aa = (T1 / C.pr[n]) * NUV;
       r.x += aa * (((tp.x - t.x) / dyj1 - (t.x - tm.x) / dyj) / dyfj);
       r.y += aa * (((tp.y - t.y) / dyj1 - (t.y - tm.y) / dyj) / dyfj);
-      cf.p[f][o] = fv;
-      rhs.p[f][o] = r;
+      cf(f)[o] = fv;
+      rhs(f)[o] = r;
     }
   }
 }
@@ -870,47 +870,47 @@ __global__ void k_remdiv_init(int NY, long ss, int nkxp, const double *__restric
 // operators are real, so real and imaginary parts are independent systems --
 // touching only shared memory; results leave with coalesced stores.
 constexpr int COL_THR = 128;
-constexpr int COL_MT = 16;
 
 // CN solve of one field for MT modes (rows 0..NY+1, tables of this substep).
+template <int MT>
 __global__ void __launch_bounds__(COL_THR) k_cn_col(int NY, long ss, const double *__restrict__ tab_rk,
                                                    FieldPtrs rhs, FieldPtrs cu, int4 wlo_a,
                                                    int4 wlo_b) {
   extern __shared__ double2 csm[];
   const int L = NY + 2;
   const int f = blockIdx.y;
-  const long m0 = (long)blockIdx.x * COL_MT;
-  const int mt = (int)((ss - m0) < COL_MT ? (ss - m0) : COL_MT);
+  const long m0 = (long)blockIdx.x * MT;
+  const int mt = (int)((ss - m0) < MT ? (ss - m0) : MT);
   double2 *X = csm;                                 // [j][MT]
-  double *TB = (double *)(X + (long)L * COL_MT);    // [5][L]
-  const double2 *__restrict__ R = rhs.p[f];
-  double2 *__restrict__ U = cu.p[f];
+  double *TB = (double *)(X + (long)L * MT);    // [5][L]
+  const double2 *__restrict__ R = rhs(f);
+  double2 *__restrict__ U = cu(f);
   const int wl[8] = {wlo_a.x, wlo_a.y, wlo_a.z, wlo_a.w, wlo_b.x, wlo_b.y, wlo_b.z, wlo_b.w};
   const int wlo = wl[f];
   const int tid = threadIdx.x;
   const double *T = tab_rk + (long)f * 5 * L;
   for (int i = tid; i < 5 * L; i += COL_THR) TB[i] = T[i];
   // staging with eight loads in flight per thread
-  for (int base = 0; base < L * COL_MT; base += 8 * COL_THR) {
+  for (int base = 0; base < L * MT; base += 8 * COL_THR) {
     double2 v[8];
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       const int i = base + u * COL_THR + tid;
-      const int m = i % COL_MT, j = i / COL_MT;
-      v[u] = (i < L * COL_MT && m < mt) ? R[(long)j * ss + m0 + m] : make_double2(0.0, 0.0);
+      const int m = i % MT, j = i / MT;
+      v[u] = (i < L * MT && m < mt) ? R[(long)j * ss + m0 + m] : make_double2(0.0, 0.0);
     }
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       const int i = base + u * COL_THR + tid;
-      if (i < L * COL_MT) X[i] = v[u];
+      if (i < L * MT) X[i] = v[u];
     }
   }
   __syncthreads();
-  if (tid < 2 * COL_MT) {
+  if (tid < 2 * MT) {
     const int m = tid >> 1, part = tid & 1;
     const double *Aa = TB, *Rb = TB + L, *Cc = TB + 2 * L, *K = TB + 3 * L, *V = TB + 4 * L;
     double *x = (double *)X + tid;
-    constexpr int st = 2 * COL_MT;
+    constexpr int st = 2 * MT;
     constexpr int B = 8;  // rows per register block: loads first, then the recurrence
     const bool mean_re = (m0 + m == 0) && part == 0;
     double g = 0.0;
@@ -959,14 +959,15 @@ __global__ void __launch_bounds__(COL_THR) k_cn_col(int NY, long ss, const doubl
     }
   }
   __syncthreads();
-  for (int i = tid; i < L * COL_MT; i += COL_THR) {
-    const int m = i % COL_MT, j = i / COL_MT;
+  for (int i = tid; i < L * MT; i += COL_THR) {
+    const int m = i % MT, j = i / MT;
     if (m < mt && j >= wlo) U[(long)j * ss + m0 + m] = X[i];
   }
 }
 
 // REM_DIV_CHAN for MT modes: divergence (parallel) -> forward and backward
 // sweeps (per part) -> projection, phi and CP update (parallel).
+template <int MT>
 __global__ void __launch_bounds__(COL_THR) k_rd_col(
     int NY, long ss, int nkxp, int JS, int JE, int rk_step, const double *__restrict__ kxv,
     const double *__restrict__ kzv, const double *__restrict__ dy, const double *__restrict__ dyf,
@@ -975,22 +976,22 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
     double2 *__restrict__ phi_out, const double *__restrict__ dscal) {
   extern __shared__ double2 csm[];
   const int L = NY + 2;
-  const long m0 = (long)blockIdx.x * COL_MT;
-  const int mt = (int)((ss - m0) < COL_MT ? (ss - m0) : COL_MT);
+  const long m0 = (long)blockIdx.x * MT;
+  const int mt = (int)((ss - m0) < MT ? (ss - m0) : MT);
   double2 *GX = csm;                                // [j][MT]: rhs -> g -> phi
-  double *RA = (double *)(GX + (long)L * COL_MT);   // [j][MT]
-  double *RB = RA + (long)L * COL_MT;               // [j][MT]
-  double *UU = RB + (long)L * COL_MT;               // [j] upper diagonal rows 2..NY-1
+  double *RA = (double *)(GX + (long)L * MT);   // [j][MT]
+  double *RB = RA + (long)L * MT;               // [j][MT]
+  double *UU = RB + (long)L * MT;               // [j] upper diagonal rows 2..NY-1
   const int tid = threadIdx.x;
   for (int j = tid; j < L; j += COL_THR) UU[j] = (j >= 2 && j < NY) ? 1. / (dy[j + 1] * dyf[j]) : 0.0;
-  for (int base = 0; base < L * COL_MT; base += 4 * COL_THR) {
+  for (int base = 0; base < L * MT; base += 4 * COL_THR) {
     double2 a1[4], a3[4], b2[4], b2p[4];
     double av[4], bv[4];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       const int i = base + u * COL_THR + tid;
-      const int m = i % COL_MT, j = i / COL_MT;
-      const bool ok = i < L * COL_MT && m < mt && j >= 1 && j <= NY;
+      const int m = i % MT, j = i / MT;
+      const bool ok = i < L * MT && m < mt && j >= 1 && j <= NY;
       const bool in = ok && j >= 2 && j < NY;
       const long o = (long)j * ss + m0 + m;
       av[u] = ok ? ra[o] : 0.0;
@@ -1003,8 +1004,8 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       const int i = base + u * COL_THR + tid;
-      if (i >= L * COL_MT) continue;
-      const int m = i % COL_MT, j = i / COL_MT;
+      if (i >= L * MT) continue;
+      const int m = i % MT, j = i / MT;
       const long mg = m0 + m;
       double2 r = make_double2(0.0, 0.0);
       if (m < mt && j >= 2 && j < NY) {
@@ -1019,11 +1020,11 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
     }
   }
   __syncthreads();
-  if (tid < 2 * COL_MT) {
+  if (tid < 2 * MT) {
     const int m = tid >> 1;
     const bool mean = (m0 + m == 0);
     double *x = (double *)GX + tid;
-    constexpr int st = 2 * COL_MT;
+    constexpr int st = 2 * MT;
     constexpr int B = 8;
     double g = 0.0;  // row 1 has a zero right-hand side
     x[1 * st] = 0.0;
@@ -1033,7 +1034,7 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
       for (int q = 0; q < B; q++) {
         const int j = j0 + q <= NY ? j0 + q : NY;
         r[q] = x[j * st];
-        a[q] = RA[j * COL_MT + m];
+        a[q] = RA[j * MT + m];
       }
 #pragma unroll
       for (int q = 0; q < B; q++) {
@@ -1046,7 +1047,7 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
       for (int q = 0; q < B; q++)
         if (j0 + q <= NY) x[(j0 + q) * st] = r[q];
     }
-    double ph = g * RB[NY * COL_MT + m];
+    double ph = g * RB[NY * MT + m];
     x[NY * st] = ph;
     for (int j1 = NY - 1; j1 >= 2; j1 -= B) {
       double gq[B], uq[B], bq[B];
@@ -1055,7 +1056,7 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
         const int j = j1 - q >= 2 ? j1 - q : 2;
         gq[q] = x[j * st];
         uq[q] = UU[j];
-        bq[q] = RB[j * COL_MT + m];
+        bq[q] = RB[j * MT + m];
       }
 #pragma unroll
       for (int q = 0; q < B; q++) {
@@ -1069,18 +1070,18 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
         if (j1 - q >= 2) x[(j1 - q) * st] = gq[q];
     }
     const double u1r = mean ? 0.0 : -1.0;
-    ph = (x[1 * st] - u1r * ph) * RB[1 * COL_MT + m];
+    ph = (x[1 * st] - u1r * ph) * RB[1 * MT + m];
     x[1 * st] = ph;
   }
   __syncthreads();
   const double hh = (rk_step > 0) ? dscal[1 + rk_step] : 1.0;
-  for (int base = 0; base < L * COL_MT; base += 4 * COL_THR) {
+  for (int base = 0; base < L * MT; base += 4 * COL_THR) {
     double2 a1[4], a3[4], b2[4], pc[4];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       const int i = base + u * COL_THR + tid;
-      const int m = i % COL_MT, j = i / COL_MT;
-      const bool ok = i < L * COL_MT && m < mt && j >= 1 && j <= NY;
+      const int m = i % MT, j = i / MT;
+      const bool ok = i < L * MT && m < mt && j >= 1 && j <= NY;
       const long o = (long)j * ss + m0 + m;
       a1[u] = ok ? u1[o] : make_double2(0.0, 0.0);
       a3[u] = ok ? u3[o] : make_double2(0.0, 0.0);
@@ -1090,8 +1091,8 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       const int i = base + u * COL_THR + tid;
-      const int m = i % COL_MT, j = i / COL_MT;
-      if (i >= L * COL_MT || m >= mt || j < 1 || j > NY) continue;
+      const int m = i % MT, j = i / MT;
+      if (i >= L * MT || m >= mt || j < 1 || j > NY) continue;
       const long mg = m0 + m, o = (long)j * ss + mg;
       const double KX = kxv[mg % nkxp], KZ = kzv[mg / nkxp];
       const double2 ph = GX[i];
@@ -1102,7 +1103,7 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
       u3[o] = a3[u];
       if (j >= 2) {
         // U2(j) -= (phi(j) - phi(j-1)) / DY(j)
-        const double2 pm = GX[i - COL_MT];
+        const double2 pm = GX[i - MT];
         b2[u].x -= (ph.x - pm.x) / dy[j];
         b2[u].y -= (ph.y - pm.y) / dy[j];
         u2[o] = b2[u];
@@ -1261,7 +1262,7 @@ __global__ void k_stats_planes(int nplanes, long ss, int nkxp, CFieldPtrs u, int
     const double w = ((m % nkxp) == 0) ? 1.0 : 2.0;
     const bool mean = (m == 0);
     for (int f = 0; f < nf; f++) {
-      const double2 v = u.p[f][(long)j * ss + m];
+      const double2 v = u(f)[(long)j * ss + m];
       if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
       const double e = w * (v.x * v.x + v.y * v.y);
       if (f < 3) {
@@ -1409,25 +1410,38 @@ int dg_cn_solve_dev(dg_handle *h, int rk_step) {
   for (int n = 0; n < h->NTH; n++) wl[3 + n] = h->jstart_th[n] - 1;
   const int L = h->NY + 2;
   const double *tab = h->cn_tab + (long)(rk_step - 1) * (3 + DG_MAX_TH) * 5 * L;
-  const size_t sm = sizeof(double2) * L * COL_MT + sizeof(double) * 5 * L;
-  dg_big_smem((const void *)k_cn_col);
-  dim3 grid(dg_cdiv(h->ss, COL_MT), h->nf);
-  dg_kt_begin(h, "k_cn_col", h->st);
-  k_cn_col<<<grid, COL_THR, sm, h->st>>>(h->NY, h->ss, tab, rhs, cu,
-                                         make_int4(wl[0], wl[1], wl[2], wl[3]),
-                                         make_int4(wl[4], wl[5], wl[6], wl[7]));
+  const int mt = h->cn_mt;
+  const size_t sm = sizeof(double2) * L * mt + sizeof(double) * 5 * L;
+  dim3 grid(dg_cdiv(h->ss, mt), h->nf);
+#define CN_CASE(MTV)                                                                    \
+  if (mt == MTV) {                                                                      \
+    dg_big_smem((const void *)k_cn_col<MTV>);                                           \
+    dg_kt_begin(h, "k_cn_col", h->st);                                                  \
+    k_cn_col<MTV><<<grid, COL_THR, sm, h->st>>>(h->NY, h->ss, tab, rhs, cu,              \
+                                               make_int4(wl[0], wl[1], wl[2], wl[3]),    \
+                                               make_int4(wl[4], wl[5], wl[6], wl[7]));   \
+  }
+  CN_CASE(4) CN_CASE(8) CN_CASE(16)
+#undef CN_CASE
   DG_LAUNCHED();
   return DG_OK;
 }
 
 int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step) {
   const int L = h->NY + 2;
-  const size_t sm = sizeof(double2) * L * COL_MT + sizeof(double) * (2 * L * COL_MT + L);
-  dg_big_smem((const void *)k_rd_col);
-  dg_kt_begin(h, "k_rd_col", h->st);
-  k_rd_col<<<dg_cdiv(h->ss, COL_MT), COL_THR, sm, h->st>>>(
-      h->NY, h->ss, h->nkxp, h->jstart, h->jend, update_cp ? rk_step : 0, h->kx, h->kz, h->dy,
-      h->dyf, h->rem_a, h->rem_rb, h->cu[0], h->cu[1], h->cu[2], h->cp, h->cr1, h->dscal);
+  const int mt = h->col_mt;
+  const size_t sm = sizeof(double2) * L * mt + sizeof(double) * (2 * L * mt + L);
+#define RD_CASE(MTV)                                                                          \
+  if (mt == MTV) {                                                                            \
+    dg_big_smem((const void *)k_rd_col<MTV>);                                                 \
+    dg_kt_begin(h, "k_rd_col", h->st);                                                        \
+    k_rd_col<MTV><<<dg_cdiv(h->ss, MTV), COL_THR, sm, h->st>>>(                               \
+        h->NY, h->ss, h->nkxp, h->jstart, h->jend, update_cp ? rk_step : 0, h->kx, h->kz,     \
+        h->dy, h->dyf, h->rem_a, h->rem_rb, h->cu[0], h->cu[1], h->cu[2], h->cp, h->cr1,      \
+        h->dscal);                                                                            \
+  }
+  RD_CASE(4) RD_CASE(8) RD_CASE(16)
+#undef RD_CASE
   DG_LAUNCHED();
   return DG_OK;
 }
@@ -1503,14 +1517,10 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
   const double2 *in[3 + DG_MAX_TH];
   for (int f = 0; f < h->nf; f++) in[f] = h->cu[f];
   const long Hfield = (long)h->nplanes * h->NZ * h->nkxp;
-  // planes per chunk: measured faster as a single chunk on B200 for the grids
-  // benchmarked (the kernels are latency- rather than bandwidth-bound), so
-  // the default is all planes; DG_YCHUNK overrides for experiments
+  // planes per y-chunk (tunable DG_TUNE_YCHUNK; 0 = all planes in one chunk,
+  // the measured default on B200 for the grids benchmarked)
   int cj = h->NY;
-  if (const char *e = getenv("DG_YCHUNK")) {
-    const int v = atoi(e);
-    if (v >= 4 && v < h->NY) cj = v;
-  }
+  if (h->ychunk >= 4 && h->ychunk < h->NY) cj = h->ychunk;
   FieldPtrs cu, cf, rhs;
   for (int f = 0; f < h->nf; f++) { cu.p[f] = h->cu[f]; cf.p[f] = h->cf[f]; rhs.p[f] = h->rhs[f]; }
   int hdone = -1;  // last H plane already produced
@@ -1523,8 +1533,13 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
     bool done = false;
     if (xw_supported(h->NX) && h->NTH <= 2) {
       const int nplan = b - a + 1;
-      int chunk = (int)((long)nplan * h->NZ / (148L * 16));
-      if (chunk < 4) chunk = 4;
+      // planes marched by one CTA (tunable DG_TUNE_XROW_CHUNK; 0 = about 16
+      // x-rows of work per SM-slot)
+      int chunk = h->xrow_chunk;
+      if (chunk <= 0) {
+        chunk = (int)((long)nplan * h->NZ / (148L * 16));
+        if (chunk < 4) chunk = 4;
+      }
       if (chunk > nplan) chunk = nplan;
       dim3 grid(dg_cdiv(h->NZ, XW_WARPS), dg_cdiv(nplan, chunk));
 #define XW_CASE(NXV, NTHV)                                                                         \

@@ -92,7 +92,7 @@ __global__ void k_ppc_col(int NY, long ss, int nth, RiVals ri,
       if (!mean)
         for (int n = 0; n < nth; n++) {
           const double r = ri.v[n] / (gyf[j + 1] - gyf[j - 1]);
-          const double2 a = th.p[n][q + ss], b = th.p[n][q - ss];
+          const double2 a = th(n)[q + ss], b = th(n)[q - ss];
           s.x += r * (a.x - b.x);
           s.y += r * (a.y - b.y);
         }

@@ -47,13 +47,21 @@ struct FftPlan {
 
 bool dg_make_plan(int n, FftPlan *pl);
 
-// up to 3 + DG_MAX_TH field pointers passed by value to kernels
-struct FieldPtrs {
-  double2 *p[3 + DG_MAX_TH + 1];
+// up to 3 + DG_MAX_TH field pointers passed by value to kernels.  Device code
+// reads them through operator(), an unrolled select: indexing the parameter
+// array with a run-time index would make the compiler copy it to local memory.
+template <typename T>
+struct PtrArray {
+  T *p[3 + DG_MAX_TH + 1];
+  __device__ __forceinline__ T *operator()(int i) const {
+    T *r = p[0];
+#pragma unroll
+    for (int k = 1; k < 3 + DG_MAX_TH + 1; k++) r = (i == k) ? p[k] : r;
+    return r;
+  }
 };
-struct CFieldPtrs {
-  const double2 *p[3 + DG_MAX_TH + 1];
-};
+struct FieldPtrs : PtrArray<double2> {};
+struct CFieldPtrs : PtrArray<const double2> {};
 
 // ---------------------------------------------------------- CN system tables
 // Per field type, the mode-independent tridiagonal system of one RK substep
@@ -127,7 +135,15 @@ struct dg_handle {
   long long gkernels[2];        // kernels per replay of each variant
   bool capturing;
   bool defer_tables;            // dt commit leaves the CN tables to the next step
+
+  // tunables (dg_tune_set / dg_autotune)
+  int col_mt;                   // modes per CTA of the REM_DIV column kernel (4, 8, 16)
+  int cn_mt;                    // modes per CTA of the CN column kernel (4, 8, 16)
+  int xrow_chunk;               // planes per CTA of the x-row product kernel (0 = auto)
+  int ychunk;                   // planes per y-chunk of a substep (0 = all)
 };
+
+int dg_default_col_mt(const dg_handle *h);
 
 void dg_graphs_free(dg_handle *h);
 

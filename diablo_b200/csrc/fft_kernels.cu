@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(NTHR) k_zinv(CFieldPtrs fields, int jmin, long
   const int j = jmin + blockIdx.y;
   const int f = blockIdx.z;
   const int tid = threadIdx.x, nthr = blockDim.x;
-  const double2 *in = fields.p[f] + (long)j * ss;
+  const double2 *in = fields(f) + (long)j * ss;
   for (int i = tid; i < NZ; i += nthr) stw[i] = tw[i];
   for (int base = 0; base < KXG * NZ; base += 8 * nthr) {
     double2 v[8];
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(NTHR) k_zfwd(const double2 *__restrict__ H, lo
   }
   __syncthreads();
   double2 *res = fft_cta<NT>(b0, b1, pl, KXG, sstr, stw, -1);
-  double2 *out = fields.p[f] + (long)j * ss;
+  double2 *out = fields(f) + (long)j * ss;
   const double rnz = (double)NZ;
   for (int idx = tid; idx < KXG * nkzt; idx += nthr) {
     const int c = idx % KXG, kp = idx / KXG;

@@ -204,13 +204,13 @@ __global__ void k_per_final(PerConst C, int rk_step, const double *__restrict__ 
   const double2 f0 = F(0), f1 = F(1), f2 = F(2), f3 = F(3), f4 = F(4), f5 = F(5);
   double2 nf[3] = {mdiv(f0, f1, f2), mdiv(f1, f3, f4), mdiv(f2, f4, f5)};
   double2 u[3], p0 = cp[q];
-  for (int d = 0; d < 3; d++) u[d] = cu.p[d][q];
+  for (int d = 0; d < 3; d++) u[d] = cu(d)[q];
   // USER_RHS_PER_PHYSICAL: CF_i += (EPSILON_TARGET / EK) U_i (exact in
   // spectral space for band-limited U)
   if (forcing != 0.0)
     for (int d = 0; d < 3; d++) { nf[d].x += forcing * u[d].x; nf[d].y += forcing * u[d].y; }
   for (int n = 0; n < C.nth; n++) {
-    const double2 t = cu.p[3 + n][q];
+    const double2 t = cu(3 + n)[q];
     nf[1].x += C.ri[n] * t.x;
     nf[1].y += C.ri[n] * t.y;
   }
@@ -221,17 +221,17 @@ __global__ void k_per_final(PerConst C, int rk_step, const double *__restrict__ 
     // CR = (1 - T1 k^2) CU - h (i k_d CP) [+ zeta h CF_old] + beta h CF
     double2 r = make_double2(t5 * u[d].x - T4 * (-Kd[d] * p0.y), t5 * u[d].y - T4 * (Kd[d] * p0.x));
     if (rk_step > 1) {
-      const double2 o = cf.p[d][q];
+      const double2 o = cf(d)[q];
       r.x += T3 * o.x;
       r.y += T3 * o.y;
     }
     r.x += T2 * nf[d].x;
     r.y += T2 * nf[d].y;
     un[d] = make_double2(r.x / t5i, r.y / t5i);
-    cf.p[d][q] = nf[d];
+    cf(d)[q] = nf[d];
   }
   for (int n = 0; n < C.nth; n++) {
-    const double2 t = cu.p[3 + n][q];
+    const double2 t = cu(3 + n)[q];
     double2 ft = C.bg[n] ? make_double2(-u[1].x, -u[1].y) : make_double2(0.0, 0.0);
     const double2 g = mdiv(F(6 + 3 * n), F(7 + 3 * n), F(8 + 3 * n));
     ft.x += g.x;
@@ -239,14 +239,14 @@ __global__ void k_per_final(PerConst C, int rk_step, const double *__restrict__ 
     const double t6 = 1 - (T1 / C.pr[n]) * k2, t6i = 1 + (T1 / C.pr[n]) * k2;
     double2 r = make_double2(t6 * t.x, t6 * t.y);
     if (rk_step > 1) {
-      const double2 o = cf.p[3 + n][q];
+      const double2 o = cf(3 + n)[q];
       r.x += T3 * o.x;
       r.y += T3 * o.y;
     }
     r.x += T2 * ft.x;
     r.y += T2 * ft.y;
-    cu.p[3 + n][q] = make_double2(r.x / t6i, r.y / t6i);
-    cf.p[3 + n][q] = ft;
+    cu(3 + n)[q] = make_double2(r.x / t6i, r.y / t6i);
+    cf(3 + n)[q] = ft;
   }
   // REM_DIV_PER: phi = (i k . U) / -(k^2 + EPS); U -= i k phi; CP += phi / h
   const double den = -(KX * KX + KY * KY + KZ * KZ + C.eps);
@@ -256,7 +256,7 @@ __global__ void k_per_final(PerConst C, int rk_step, const double *__restrict__ 
   for (int d = 0; d < 3; d++) {
     un[d].x -= -Kd[d] * ph.y;
     un[d].y -= Kd[d] * ph.x;
-    cu.p[d][q] = un[d];
+    cu(d)[q] = un[d];
   }
   phi[q] = ph;
   cp[q] = make_double2(p0.x + ph.x / T4, p0.y + ph.y / T4);
@@ -333,7 +333,7 @@ __global__ void k_per_sums(PerConst C, CFieldPtrs u, double *__restrict__ out, i
     const double w = ((m % C.nkxp) == 0) ? 1.0 : 2.0;
     const long q = (long)jy * C.ss + m;
     for (int f = 0; f < C.nf && f < 8; f++) {
-      const double2 v = u.p[f][q];
+      const double2 v = u(f)[q];
       if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
       if (f >= 3 && q == 0) continue;
       acc[f] += w * (v.x * v.x + v.y * v.y);

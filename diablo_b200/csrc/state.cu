@@ -148,6 +148,8 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
   h->ss = (long)h->nkxp * h->nkzt;
   h->nspec = h->ss * h->nplanes;
   h->nf = 3 + h->NTH;
+  h->col_mt = dg_default_col_mt(h);
+  h->cn_mt = h->col_mt;
   h->pi = 4.0 * atan(1.0);
   h->eps = (double)(float)0.000000001;  // default-real literal, for/fft.f:74
   // INIT_CHAN_MPI with NPROCY = 1 (for/mpi.f:1080-1100)

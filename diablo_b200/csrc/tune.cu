@@ -1,0 +1,190 @@
+// Tunable launch shapes of the channel substep and the autotuner that picks
+// them by timing.
+//
+//   DG_TUNE_COL_MT      modes per CTA of the REM_DIV column kernel (k_rd_col),
+//   DG_TUNE_CN_MT       and of the CN column kernel (k_cn_col): 4, 8 or 16.
+//                       Fewer modes per CTA means more CTAs resident per SM to
+//                       hide the column loads; more means more sweep lanes per
+//                       CTA.
+//   DG_TUNE_XROW_CHUNK  y-planes one CTA of the x-row product kernel marches
+//                       through (0 = automatic).  Longer marches re-read fewer
+//                       halo planes; shorter ones give more CTAs.
+//   DG_TUNE_YCHUNK      planes per y-chunk of a substep (0 = all): smaller
+//                       chunks keep the intermediate planes in L2.
+//
+// dg_autotune times candidate values one tunable at a time (coordinate
+// descent) on the handle's own state with CUDA events over a few eager
+// steps, keeps the fastest, and restores the state, TIME and DELTA_T it found.
+// The choice depends only on the grid and field count, so a caller that
+// serves many cases can tune once per shape and copy the values across with
+// dg_tune_set.
+#include <vector>
+
+#include "dg_internal.cuh"
+
+int dg_default_col_mt(const dg_handle *h) {
+  // enough CTAs for about three per SM
+  for (int mt : {16, 8})
+    if ((h->ss + mt - 1) / mt >= 3 * 148) return mt;
+  return 4;
+}
+
+static void invalidate_graphs(dg_handle *h) {
+  dg_graphs_free(h);
+  h->gwarm[0] = h->gwarm[1] = false;
+}
+
+extern "C" int dg_tune_set(dg_handle *h, int key, int value) {
+  if (!h) return DG_ERR_ARG;
+  switch (key) {
+    case DG_TUNE_COL_MT:
+      if (value != 4 && value != 8 && value != 16) return DG_ERR_ARG;
+      h->col_mt = value;
+      break;
+    case DG_TUNE_CN_MT:
+      if (value != 4 && value != 8 && value != 16) return DG_ERR_ARG;
+      h->cn_mt = value;
+      break;
+    case DG_TUNE_XROW_CHUNK:
+      if (value < 0 || value > 1024) return DG_ERR_ARG;
+      h->xrow_chunk = value;
+      break;
+    case DG_TUNE_YCHUNK:
+      if (value < 0 || value > 1 << 20) return DG_ERR_ARG;
+      h->ychunk = value;
+      break;
+    default:
+      return DG_ERR_ARG;
+  }
+  invalidate_graphs(h);
+  return DG_OK;
+}
+
+extern "C" int dg_tune_get(dg_handle *h, int key, int *value) {
+  if (!h || !value) return DG_ERR_ARG;
+  switch (key) {
+    case DG_TUNE_COL_MT: *value = h->col_mt; return DG_OK;
+    case DG_TUNE_CN_MT: *value = h->cn_mt; return DG_OK;
+    case DG_TUNE_XROW_CHUNK: *value = h->xrow_chunk; return DG_OK;
+    case DG_TUNE_YCHUNK: *value = h->ychunk; return DG_OK;
+    default: return DG_ERR_ARG;
+  }
+}
+
+namespace {
+
+struct Saved {
+  std::vector<double2 *> bufs;
+  double scal[16];
+};
+
+int save_state(dg_handle *h, Saved *sv) {
+  const size_t bytes = sizeof(double2) * h->nspec;
+  auto keep = [&](const double2 *src) -> int {
+    double2 *d = nullptr;
+    DG_CUDA(cudaMalloc((void **)&d, bytes));
+    sv->bufs.push_back(d);
+    DG_CUDA(cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToDevice, h->st));
+    return DG_OK;
+  };
+  for (int f = 0; f < h->nf; f++) {
+    DG_TRY(keep(h->cu[f]));
+    DG_TRY(keep(h->cf[f]));
+  }
+  DG_TRY(keep(h->cp));
+  DG_CUDA(cudaMemcpyAsync(sv->scal, h->dscal, sizeof(sv->scal), cudaMemcpyDeviceToHost, h->st));
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  return DG_OK;
+}
+
+int restore_state(dg_handle *h, Saved *sv) {
+  const size_t bytes = sizeof(double2) * h->nspec;
+  size_t k = 0;
+  for (int f = 0; f < h->nf; f++) {
+    DG_CUDA(cudaMemcpyAsync(h->cu[f], sv->bufs[k++], bytes, cudaMemcpyDeviceToDevice, h->st));
+    DG_CUDA(cudaMemcpyAsync(h->cf[f], sv->bufs[k++], bytes, cudaMemcpyDeviceToDevice, h->st));
+  }
+  DG_CUDA(cudaMemcpyAsync(h->cp, sv->bufs[k++], bytes, cudaMemcpyDeviceToDevice, h->st));
+  DG_CUDA(cudaMemcpyAsync(h->dscal, sv->scal, sizeof(sv->scal), cudaMemcpyHostToDevice, h->st));
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  return DG_OK;
+}
+
+void free_saved(Saved *sv) {
+  for (double2 *p : sv->bufs) cudaFree(p);
+  sv->bufs.clear();
+}
+
+// device time of `steps` eager RK3 steps, in ms
+int time_steps(dg_handle *h, int steps, float *ms) {
+  cudaEvent_t e0, e1;
+  DG_CUDA(cudaEventCreate(&e0));
+  DG_CUDA(cudaEventCreate(&e1));
+  int s = DG_OK;
+  // one untimed step with the new shape (first launches, table joins)
+  for (int rk = 1; rk <= 3 && s == DG_OK; rk++) s = diablo_rk_chan_1(h, 1, rk);
+  if (s == DG_OK) cudaEventRecord(e0, h->st);
+  for (int i = 0; i < steps && s == DG_OK; i++)
+    for (int rk = 1; rk <= 3 && s == DG_OK; rk++) s = diablo_rk_chan_1(h, 2 + i, rk);
+  if (s == DG_OK) {
+    cudaEventRecord(e1, h->st);
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(ms, e0, e1) != cudaSuccess)
+      s = DG_ERR_CUDA;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return s;
+}
+
+}  // namespace
+
+extern "C" int dg_autotune(dg_handle *h, int steps_per_trial) {
+  if (!h || steps_per_trial < 1) return DG_ERR_ARG;
+  if (h->periodic) return DG_OK;  // the periodic path has no tunable shapes
+  Saved sv;
+  int s = save_state(h, &sv);
+  if (s != DG_OK) {
+    free_saved(&sv);
+    return s;
+  }
+  struct Knob {
+    int key;
+    std::vector<int> vals;
+  };
+  std::vector<Knob> knobs = {
+      {DG_TUNE_COL_MT, {4, 8, 16}},
+      {DG_TUNE_CN_MT, {4, 8, 16}},
+      {DG_TUNE_XROW_CHUNK, {0, 2, 4, 8, 16}},
+      {DG_TUNE_YCHUNK, {0, 16, 32, 64}},
+  };
+  for (const Knob &k : knobs) {
+    int best = 0;
+    dg_tune_get(h, k.key, &best);
+    float best_ms = 1e30f;
+    for (int v : k.vals) {
+      if (k.key == DG_TUNE_YCHUNK && v != 0 && v >= h->NY) continue;
+      if ((s = dg_tune_set(h, k.key, v)) != DG_OK) break;
+      float ms = 0.f;
+      if ((s = time_steps(h, steps_per_trial, &ms)) != DG_OK) break;
+      if ((s = restore_state(h, &sv)) != DG_OK) break;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = v;
+      }
+    }
+    if (s != DG_OK) break;
+    dg_tune_set(h, k.key, best);
+  }
+  const int r = restore_state(h, &sv);
+  free_saved(&sv);
+  DG_TRY(s);
+  DG_TRY(r);
+  // the tables of the restored DELTA_T
+  if (h->tables_pending) {
+    DG_CUDA(cudaStreamWaitEvent(h->st, h->ev_join, 0));
+    h->tables_pending = false;
+  }
+  DG_TRY(dg_cn_tables(h));
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  return DG_OK;
+}

@@ -67,6 +67,27 @@ class _Solver:
     def _call(self, name, *args):
         _lib.check(name, getattr(self.L, name)(self.h, *args))
 
+    TUNE_KEYS = {"col_mt": 0, "xrow_chunk": 1, "ychunk": 2, "cn_mt": 3}
+
+    def tune_set(self, **kw):
+        """Launch-shape tunables (results do not depend on them)."""
+        for k, v in kw.items():
+            self._call("dg_tune_set", self.TUNE_KEYS[k], int(v))
+
+    def tune_get(self) -> dict:
+        out = {}
+        for k, key in self.TUNE_KEYS.items():
+            v = ctypes.c_int()
+            self._call("dg_tune_get", key, ctypes.byref(v))
+            out[k] = v.value
+        return out
+
+    def autotune(self, steps_per_trial: int = 3) -> dict:
+        """Time candidate launch shapes on this state, keep the fastest; the
+        state, TIME and DELTA_T are restored afterwards."""
+        self._call("dg_autotune", steps_per_trial)
+        return self.tune_get()
+
     def steps(self, time_step: int, nsteps: int):
         """nsteps full RK3 steps from time_step (the driver loop body,
         for/diablo.f:70-109), replayed as CUDA graphs after the first."""

@@ -179,6 +179,19 @@ int dg_timing_enable(dg_handle *h, int on);
 int dg_timing_read(dg_handle *h, int i, char *name, int name_len, int64_t *launches,
                    double *total_ms);
 
+/* -------------------------------------------------------------- tuning */
+/* No counterpart in the reference.  Launch shapes of the channel substep:
+ * modes per CTA of the REM_DIV and CN y-column kernels (4, 8, 16), y-planes per CTA of the
+ * x-row product kernel (0 = automatic), planes per y-chunk of a substep
+ * (0 = all).  Results do not depend on them.  dg_autotune times candidates on
+ * the handle's own state (steps_per_trial eager RK3 steps each), keeps the
+ * fastest and restores the state, TIME and DELTA_T; it allocates temporary
+ * device copies of the state while it runs. */
+enum { DG_TUNE_COL_MT = 0, DG_TUNE_XROW_CHUNK = 1, DG_TUNE_YCHUNK = 2, DG_TUNE_CN_MT = 3 };
+int dg_tune_set(dg_handle *h, int key, int value);
+int dg_tune_get(dg_handle *h, int key, int *value);
+int dg_autotune(dg_handle *h, int steps_per_trial);
+
 /* ------------------------------------------- allocation-free transform */
 /* No counterpart in the reference.  FFT_XZ_TO_FOURIER(V,VV,JMIN,JMAX) on
  * DEVICE arrays in the reference layout (as diablo_fft_xz_to_fourier with

@@ -292,3 +292,39 @@ def test_graph_steps_match_substep_calls(case):
     assert a.get_time() == b.get_time()
     a.close()
     b.close()
+
+
+def test_autotune_restores_state_and_keeps_results():
+    """dg_autotune leaves the state, TIME and DELTA_T as it found them, and
+    the launch shapes it picks do not change results (bit for bit)."""
+    p, gy = configs.channel_re180(nx=64, ny=65, nz=48)
+    ref, a, _ = start_pair(p, gy, ics.channel_laminar, seed=8)
+    b = channel(p, gy)
+    b.set_state(ref.state())
+    b.set_time(0.0, p.delta_t)
+    before = {nm: b.get_field(nm) for nm in fields(p) + ["CP"]}
+    t0 = b.get_time()
+    chosen = b.autotune(2)
+    assert chosen["col_mt"] in (4, 8, 16)
+    for nm, v in before.items():
+        assert np.array_equal(b.get_field(nm), v), nm
+    assert b.get_time() == t0
+    for s in range(1, 6):
+        a.step(s)
+    b.steps(1, 5)
+    for nm in fields(p) + ["CP"]:
+        assert np.array_equal(a.get_field(nm), b.get_field(nm)), nm
+    for mt in (4, 16):
+        b.tune_set(col_mt=mt, cn_mt=20 - mt, xrow_chunk=3, ychunk=20)
+        c = channel(p, gy)
+        c.set_state(ref.state())
+        c.set_time(0.0, p.delta_t)
+        b.set_state(ref.state())
+        b.set_time(0.0, p.delta_t)
+        b.steps(1, 3)
+        c.steps(1, 3)
+        for nm in fields(p) + ["CP"]:
+            assert np.array_equal(b.get_field(nm), c.get_field(nm)), (mt, nm)
+        c.close()
+    a.close()
+    b.close()

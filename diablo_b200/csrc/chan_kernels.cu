@@ -256,11 +256,11 @@ __host__ __device__ constexpr bool xw_supported(int n) {
   return n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 256;
 }
 
-template <int NX, int NTH>
+template <int NX, int NTH, typename CX = double2>
 __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? 3 : 2) k_xrow_w(
-    ChanConst C, const double2 *__restrict__ H, long Hfield, int chunk, int jbase, int jtop,
-    const double2 *__restrict__ tw, const double *__restrict__ dyf, const double *__restrict__ dy,
-    const double *__restrict__ kxv, double2 *__restrict__ G, long Gfield) {
+    ChanConst C, const CX *__restrict__ H, long Hfield, int chunk, int jbase, int jtop,
+    const CX *__restrict__ tw, const double *__restrict__ dyf, const double *__restrict__ dy,
+    const double *__restrict__ kxv, CX *__restrict__ G, long Gfield) {
   constexpr int NF = 3 + NTH;
   constexpr int NPIN = (NF + 1) / 2;
   constexpr int NPROD = 8 + 3 * NTH;
@@ -270,12 +270,14 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? 3 : 2) k_xrow_w(
   constexpr int NKXP = NX / 3 + 1;
   constexpr int KS = (NKXP + 31) / 32;             // kx slots per lane
   constexpr int SSTR = padded_len(NX);
-  extern __shared__ double2 sm[];
-  double2 *stw = sm;
+  extern __shared__ double2 sm_raw[];
+  using T = typename CT<CX>::T;
+  CX *sm = reinterpret_cast<CX *>(sm_raw);
+  CX *stw = sm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double2 *buf = stw + NX + warp * MAXP * SSTR;
+  CX *buf = stw + NX + warp * MAXP * SSTR;
   // carried x-spectra: 0 fl1, 1 fl3, 2 ubar1 u2, 3 ubar3 u2, 4 g, 5+n flth
-  double2 *pvs = stw + NX + XW_WARPS * MAXP * SSTR + warp * (5 + NTH) * NKXP;
+  CX *pvs = stw + NX + XW_WARPS * MAXP * SSTR + warp * (5 + NTH) * NKXP;
   for (int i = threadIdx.x; i < NX; i += blockDim.x) stw[i] = tw[i];
   __syncthreads();
   const int z = blockIdx.x * XW_WARPS + warp;
@@ -284,15 +286,26 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? 3 : 2) k_xrow_w(
   const int j0 = jbase + blockIdx.y * chunk;
   int j1 = j0 + chunk - 1;
   if (j1 > jtop) j1 = jtop;
-  const double rnx = 1.0 / (double)NX;            // exact: NX is 2^a 3^b ... see below
+  const T rnx = (T)1 / (T)NX;            // exact: NX is 2^a 3^b ... see below
   const bool pow2 = (NX & (NX - 1)) == 0;
   const long plane = (long)NZ * NKXP;
 
-  double cur[NF][XPL], nxt[NF][XPL];
+  T cur[NF][XPL], nxt[NF][XPL];
 #define PV(q, s) pvs[(q) * NKXP + lane + 32 * (s)]
 
-  auto load_plane = [&](int pl, double (&dst)[NF][XPL]) {
-    const double2 *row = H + (long)pl * plane + (long)z * NKXP;
+  // FP32 form: each x-row is split into its x-mean (kept in FP64, uniform
+  // across the row) and the fluctuation (FP32).  The transforms see only
+  // fluctuations, so the two real rows packed into one complex transform
+  // have comparable magnitude, and the row means of the products are formed
+  // in FP64 from the means and the fluctuations.
+  constexpr bool F32 = sizeof(T) == 4;
+  double dcur[NF], dnxt[NF];
+  auto load_plane = [&](int pl, T (&dst)[NF][XPL], double (&dcv)[NF]) {
+    const CX *row = H + (long)pl * plane + (long)z * NKXP;
+    if constexpr (F32) {
+#pragma unroll
+      for (int f = 0; f < NF; f++) dcv[f] = (double)row[f * Hfield].x;
+    }
 #pragma unroll
     for (int q = 0; q < NPIN; q++) {
       const int fa = 2 * q, fb = 2 * q + 1;
@@ -301,13 +314,14 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? 3 : 2) k_xrow_w(
         const int k = lane + 32 * i;
         if (k < NX) {
           const int kk = (k <= NX / 2) ? k : NX - k;
-          double2 v = make_double2(0.0, 0.0);
+          CX v = CT<CX>::mk(0, 0);
           if (kk < NKXP && kk < NX / 2) {
-            double2 a = row[fa * Hfield + kk];
-            double2 bb = (fb < NF) ? row[fb * Hfield + kk] : make_double2(0.0, 0.0);
+            CX a = row[fa * Hfield + kk];
+            CX bb = (fb < NF) ? row[fb * Hfield + kk] : CT<CX>::mk(0, 0);
             if (kk == 0) { a.y = 0.0; bb.y = 0.0; }
-            v = (k == kk) ? make_double2(a.x - bb.y, a.y + bb.x)
-                          : make_double2(a.x + bb.y, -a.y + bb.x);
+            if (F32 && kk == 0) { a.x = 0.0; bb.x = 0.0; }
+            v = (k == kk) ? CT<CX>::mk(a.x - bb.y, a.y + bb.x)
+                          : CT<CX>::mk(a.x + bb.y, -a.y + bb.x);
           }
           buf[q * SSTR + pad(k)] = v;
         }
@@ -320,89 +334,158 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? 3 : 2) k_xrow_w(
 #pragma unroll
       for (int i = 0; i < XPL; i++) {
         const int x = lane + 32 * i;
-        const double2 v = (x < NX) ? buf[q * SSTR + pad(x)] : make_double2(0.0, 0.0);
+        const CX v = (x < NX) ? buf[q * SSTR + pad(x)] : CT<CX>::mk(0, 0);
         dst[2 * q][i] = v.x;
         if (2 * q + 1 < NF) dst[2 * q + 1][i] = v.y;
       }
     __syncwarp();
   };
 
-  load_plane(j0 - 1, cur);
+  load_plane(j0 - 1, cur, dcur);
   for (int j = j0 - 1; j <= j1; j++) {
-    load_plane(j + 1, nxt);
-    const double dyf_j = dyf[j], dyf_p = dyf[j + 1], dy_p = dy[j + 1];
-    const double wgy = 1.0 / (2. * dy_p);
+    load_plane(j + 1, nxt, dnxt);
+    const T dyf_j = dyf[j], dyf_p = dyf[j + 1], dy_p = dy[j + 1];
+    const T wgy = (T)1 / ((T)2 * dy_p);
     // products: GYF j (U1U3, U1U1, U3U3, g, TH U1, TH U3) and GY j+1 (fl1, fl3,
     // ubar1 u2, ubar3 u2, flth)
+    // FP32 form: row means of the products, P = L1 L2 with L = D + L'
+    double pdc[F32 ? NPROD : 1];
+    if constexpr (F32) {
+      double acc[NPROD];
+#pragma unroll
+      for (int p = 0; p < NPROD; p++) acc[p] = 0.0;
+      const double wgyd = 1.0 / (2. * (double)dy[j + 1]);
+      const double dfj = dyf[j], dfp = dyf[j + 1];
+      double L1d[NPROD], L2d[NPROD];
+      // (L1, L2) row means of each product, in the order of P[] below
+      L1d[0] = dcur[2]; L2d[0] = dcur[0];
+      L1d[1] = dcur[0]; L2d[1] = dcur[0];
+      L1d[2] = dcur[2]; L2d[2] = dcur[2];
+      L1d[3] = 0.5 * (dcur[1] + dnxt[1]); L2d[3] = L1d[3];
+      L1d[4] = dnxt[0] + dcur[0]; L2d[4] = dnxt[1];
+      L1d[5] = dnxt[2] + dcur[2]; L2d[5] = dnxt[1];
+      L1d[6] = (dfp * dnxt[0] + dfj * dcur[0]) * wgyd; L2d[6] = dnxt[1];
+      L1d[7] = (dfp * dnxt[2] + dfj * dcur[2]) * wgyd; L2d[7] = dnxt[1];
+#pragma unroll
+      for (int n = 0; n < NTH; n++) {
+        L1d[8 + 3 * n] = dcur[3 + n]; L2d[8 + 3 * n] = dcur[0];
+        L1d[9 + 3 * n] = dcur[3 + n]; L2d[9 + 3 * n] = dcur[2];
+        L1d[10 + 3 * n] = dnxt[3 + n] + dcur[3 + n]; L2d[10 + 3 * n] = dnxt[1];
+      }
+#pragma unroll
+      for (int i = 0; i < XPL; i++) {
+        const int x = lane + 32 * i;
+        if (x >= NX) continue;
+        const float u1 = cur[0][i], u2 = cur[1][i], u3 = cur[2][i];
+        const float u1p = nxt[0][i], u2p = nxt[1][i], u3p = nxt[2][i];
+        float L1f[NPROD], L2f[NPROD];
+        L1f[0] = u3; L2f[0] = u1;
+        L1f[1] = u1; L2f[1] = u1;
+        L1f[2] = u3; L2f[2] = u3;
+        L1f[3] = 0.5f * (u2 + u2p); L2f[3] = L1f[3];
+        L1f[4] = u1p + u1; L2f[4] = u2p;
+        L1f[5] = u3p + u3; L2f[5] = u2p;
+        L1f[6] = ((T)dyf_p * u1p + (T)dyf_j * u1) * wgy; L2f[6] = u2p;
+        L1f[7] = ((T)dyf_p * u3p + (T)dyf_j * u3) * wgy; L2f[7] = u2p;
+#pragma unroll
+        for (int n = 0; n < NTH; n++) {
+          const float t = cur[3 + n][i], tp = nxt[3 + n][i];
+          L1f[8 + 3 * n] = t; L2f[8 + 3 * n] = u1;
+          L1f[9 + 3 * n] = t; L2f[9 + 3 * n] = u3;
+          L1f[10 + 3 * n] = tp + t; L2f[10 + 3 * n] = u2p;
+        }
+        T P[2 * NPP];
+#pragma unroll
+        for (int p = 0; p < NPROD; p++) {
+          const float ff = L1f[p] * L2f[p];
+          acc[p] += (double)ff;
+          P[p] = (float)L1d[p] * L2f[p] + (float)L2d[p] * L1f[p] + ff;
+        }
+        if (2 * NPP > NPROD) P[2 * NPP - 1] = 0.0f;
+#pragma unroll
+        for (int q = 0; q < NPP; q++) buf[q * SSTR + pad(x)] = CT<CX>::mk(P[2 * q], P[2 * q + 1]);
+      }
+#pragma unroll
+      for (int p = 0; p < NPROD; p++) {
+        double v = acc[p];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        pdc[p] = L1d[p] * L2d[p] + v / (double)NX;
+      }
+    } else {
 #pragma unroll
     for (int i = 0; i < XPL; i++) {
       const int x = lane + 32 * i;
       if (x >= NX) continue;
-      const double u1 = cur[0][i], u2 = cur[1][i], u3 = cur[2][i];
-      const double u1p = nxt[0][i], u2p = nxt[1][i], u3p = nxt[2][i];
-      double P[2 * NPP];
+      const T u1 = cur[0][i], u2 = cur[1][i], u3 = cur[2][i];
+      const T u1p = nxt[0][i], u2p = nxt[1][i], u3p = nxt[2][i];
+      T P[2 * NPP];
       P[0] = u3 * u1;
       P[1] = u1 * u1;
       P[2] = u3 * u3;
-      { const double s = u2 + u2p; P[3] = 0.25 * (s * s); }
+      { const T s = u2 + u2p; P[3] = (T)0.25 * (s * s); }
       P[4] = (u1p + u1) * u2p;
       P[5] = (u3p + u3) * u2p;
       P[6] = ((dyf_p * u1p + dyf_j * u1) * wgy) * u2p;
       P[7] = ((dyf_p * u3p + dyf_j * u3) * wgy) * u2p;
 #pragma unroll
       for (int n = 0; n < NTH; n++) {
-        const double t = cur[3 + n][i], tp = nxt[3 + n][i];
+        const T t = cur[3 + n][i], tp = nxt[3 + n][i];
         P[8 + 3 * n] = t * u1;
         P[9 + 3 * n] = t * u3;
         P[10 + 3 * n] = (tp + t) * u2p;
       }
       if (2 * NPP > NPROD) P[2 * NPP - 1] = 0.0;
 #pragma unroll
-      for (int q = 0; q < NPP; q++) buf[q * SSTR + pad(x)] = make_double2(P[2 * q], P[2 * q + 1]);
+      for (int q = 0; q < NPP; q++) buf[q * SSTR + pad(x)] = CT<CX>::mk(P[2 * q], P[2 * q + 1]);
+    }
     }
     __syncwarp();
     wpasses<NX, -1, 0>(buf, NPP, SSTR, stw, lane);
     const bool out = (j >= j0);
-    const double d2 = 2.0 * dyf_j, dyj = dy[j];
+    const T d2 = (T)2 * dyf_j, dyj = dy[j];
 #pragma unroll
     for (int s = 0; s < KS; s++) {
       const int k = lane + 32 * s;
       if (k >= NKXP) continue;
-      auto X = [&](int p) -> double2 {
+      auto X = [&](int p) -> CX {
+        if constexpr (F32) {
+          if (k == 0) return CT<CX>::mk((T)pdc[p], (T)0);
+        }
         const int q = p >> 1;
-        const double2 zk = buf[q * SSTR + pad(k)];
-        const double2 zm = buf[q * SSTR + pad((NX - k) % NX)];
-        double2 v;
-        if ((p & 1) == 0) v = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
-        else v = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
-        if (pow2) return make_double2(v.x * rnx, v.y * rnx);
-        return make_double2(v.x / (double)NX, v.y / (double)NX);
+        const CX zk = buf[q * SSTR + pad(k)];
+        const CX zm = buf[q * SSTR + pad((NX - k) % NX)];
+        CX v;
+        if ((p & 1) == 0) v = CT<CX>::mk((T)0.5 * (zk.x + zm.x), (T)0.5 * (zk.y - zm.y));
+        else v = CT<CX>::mk((T)0.5 * (zk.y + zm.y), -(T)0.5 * (zk.x - zm.x));
+        if (pow2) return CT<CX>::mk(v.x * rnx, v.y * rnx);
+        return CT<CX>::mk(v.x / (T)NX, v.y / (T)NX);
       };
-      const double KX = kxv[k];
-      auto mikx = [&](double2 a) { return make_double2(KX * a.y, -KX * a.x); };  // -i kx a
-      const double2 x3 = X(3), x4 = X(4), x5 = X(5), x6 = X(6), x7 = X(7);
+      const T KX = kxv[k];
+      auto mikx = [&](CX a) { return CT<CX>::mk(KX * a.y, -KX * a.x); };  // -i kx a
+      const CX x3 = X(3), x4 = X(4), x5 = X(5), x6 = X(6), x7 = X(7);
       if (out) {
         const long off = (long)j * NZ * NKXP + (long)z * NKXP + k;
-        const double2 x0 = X(0), x1 = X(1), x2 = X(2);
+        const CX x0 = X(0), x1 = X(1), x2 = X(2);
         // U1: A = U1U3, B = -ikx U1U1 - (fl1(j+1) - fl1(j)) / (2 DYF(j))
         G[0 * Gfield + off] = x0;
-        double2 t = mikx(x1);
-        G[1 * Gfield + off] = make_double2(t.x - (x4.x - PV(0, s).x) / d2, t.y - (x4.y - PV(0, s).y) / d2);
+        CX t = mikx(x1);
+        G[1 * Gfield + off] = CT<CX>::mk(t.x - (x4.x - PV(0, s).x) / d2, t.y - (x4.y - PV(0, s).y) / d2);
         // U2 (GY j): A = ubar3 u2(j), B = -ikx ubar1 u2(j) - (g(j) - g(j-1)) / DY(j)
         G[2 * Gfield + off] = PV(3, s);
         t = mikx(PV(2, s));
-        G[3 * Gfield + off] = make_double2(t.x - (x3.x - PV(4, s).x) / dyj, t.y - (x3.y - PV(4, s).y) / dyj);
+        G[3 * Gfield + off] = CT<CX>::mk(t.x - (x3.x - PV(4, s).x) / dyj, t.y - (x3.y - PV(4, s).y) / dyj);
         // U3: A = U3U3, B = -ikx U1U3 - (fl3(j+1) - fl3(j)) / (2 DYF(j))
         G[4 * Gfield + off] = x2;
         t = mikx(x0);
-        G[5 * Gfield + off] = make_double2(t.x - (x5.x - PV(1, s).x) / d2, t.y - (x5.y - PV(1, s).y) / d2);
+        G[5 * Gfield + off] = CT<CX>::mk(t.x - (x5.x - PV(1, s).x) / d2, t.y - (x5.y - PV(1, s).y) / d2);
 #pragma unroll
         for (int n = 0; n < NTH; n++) {
-          const double2 a = X(8 + 3 * n), b = X(9 + 3 * n), c = X(10 + 3 * n);
+          const CX a = X(8 + 3 * n), b = X(9 + 3 * n), c = X(10 + 3 * n);
           G[(6 + 2 * n) * Gfield + off] = b;
           t = mikx(a);
           G[(7 + 2 * n) * Gfield + off] =
-              make_double2(t.x - (c.x - PV(5 + n, s).x) / d2, t.y - (c.y - PV(5 + n, s).y) / d2);
+              CT<CX>::mk(t.x - (c.x - PV(5 + n, s).x) / d2, t.y - (c.y - PV(5 + n, s).y) / d2);
         }
       }
       PV(0, s) = x4;
@@ -415,18 +498,20 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? 3 : 2) k_xrow_w(
     }
     __syncwarp();
 #pragma unroll
-    for (int f = 0; f < NF; f++)
+    for (int f = 0; f < NF; f++) {
 #pragma unroll
       for (int i = 0; i < XPL; i++) cur[f][i] = nxt[f][i];
+      dcur[f] = dnxt[f];
+    }
   }
 #undef PV
 }
 
-template <int NX, int NTH>
+template <int NX, int NTH, typename CX = double2>
 size_t xw_smem() {
   constexpr int NF = 3 + NTH, NPIN = (NF + 1) / 2, NPP = (8 + 3 * NTH + 1) / 2;
   constexpr int MAXP = NPIN > NPP ? NPIN : NPP;
-  return sizeof(double2) * (NX + XW_WARPS * MAXP * padded_len(NX) + XW_WARPS * (5 + NTH) * (NX / 3 + 1));
+  return sizeof(CX) * (NX + XW_WARPS * MAXP * padded_len(NX) + XW_WARPS * (5 + NTH) * (NX / 3 + 1));
 }
 
 // ------------------------------------------------------------- zfwd + rhs
@@ -597,16 +682,17 @@ __global__ void __launch_bounds__(ZF_THR) k_zfwd_rhs(
 // then each warp transforms its 2 x (A, B) signals and finishes those modes.
 constexpr int ZW_KXG = 8;
 
-template <int NZ>
+template <int NZ, typename CX = double2>
 __global__ void __launch_bounds__(128, 4) k_zfwd_w(
-    ChanConst C, const double2 *__restrict__ G, long Gfield, const double2 *__restrict__ tw,
+    ChanConst C, const CX *__restrict__ G, long Gfield, const CX *__restrict__ tw,
     const double *__restrict__ dscal, int rk_step, const double *__restrict__ kxv,
     const double *__restrict__ kzv, const double *__restrict__ dy, const double *__restrict__ dyf,
     FieldPtrs cu, FieldPtrs cf, FieldPtrs rhs, const double2 *__restrict__ cp, int jbase) {
   constexpr int SSTR = padded_len(NZ);
-  extern __shared__ double2 sm[];
-  double2 *stw = sm;
-  double2 *buf = stw + NZ;                     // [warp][A0 A1 B0 B1][SSTR]
+  extern __shared__ double2 sm_raw[];
+  CX *sm = reinterpret_cast<CX *>(sm_raw);
+  CX *stw = sm;
+  CX *buf = stw + NZ;                          // [warp][A0 A1 B0 B1][SSTR]
   const int nkxp = C.nkxp, nkzt = C.nkzt, NKZ = C.NKZ;
   const int kx0 = blockIdx.x * ZW_KXG;
   const int j = jbase + blockIdx.y;
@@ -617,16 +703,16 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
   const int jhi = (f == 0 || f == 2) ? C.JE : (f == 1 ? C.NY : C.JEt[f - 3]);
   if (j < jlo || j > jhi) return;
   for (int i = threadIdx.x; i < NZ; i += blockDim.x) stw[i] = tw[i];
-  const double2 *GA = G + (2 * f) * Gfield + (long)j * NZ * nkxp;
-  const double2 *GB = G + (2 * f + 1) * Gfield + (long)j * NZ * nkxp;
+  const CX *GA = G + (2 * f) * Gfield + (long)j * NZ * nkxp;
+  const CX *GB = G + (2 * f + 1) * Gfield + (long)j * NZ * nkxp;
   for (int base = 0; base < 2 * ZW_KXG * NZ; base += 8 * 128) {
-    double2 v[8];
+    CX v[8];
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       const int i = base + u * 128 + threadIdx.x;
       const int c = i % ZW_KXG, z = (i / ZW_KXG) % NZ, ab = i / (ZW_KXG * NZ);
       v[u] = (i < 2 * ZW_KXG * NZ && kx0 + c < nkxp) ? (ab ? GB : GA)[(long)z * nkxp + kx0 + c]
-                                                     : make_double2(0.0, 0.0);
+                                                     : CT<CX>::mk(0, 0);
     }
 #pragma unroll
     for (int u = 0; u < 8; u++) {
@@ -638,7 +724,7 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
     }
   }
   __syncthreads();
-  double2 *wb = buf + warp * 4 * SSTR;
+  CX *wb = buf + warp * 4 * SSTR;
   wpasses<NZ, -1, 0>(wb, 4, SSTR, stw, lane);
 
   const double h = dscal[1 + rk_step];
@@ -655,9 +741,10 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
     const int kx = kx0 + 2 * warp + cc;
     if (kx >= nkxp) continue;
     const int z = (kp <= NKZ) ? kp : (NZ - 1 + (kp - NKZ) - NKZ);
-    double2 a = wb[(0 + cc) * SSTR + pad(z)], b = wb[(2 + cc) * SSTR + pad(z)];
-    a = make_double2(a.x / rnz, a.y / rnz);
-    b = make_double2(b.x / rnz, b.y / rnz);
+    // the transform's working precision ends here: everything below is FP64
+    const CX aw = wb[(0 + cc) * SSTR + pad(z)], bw = wb[(2 + cc) * SSTR + pad(z)];
+    const double2 a = make_double2((double)aw.x / rnz, (double)aw.y / rnz);
+    const double2 b = make_double2((double)bw.x / rnz, (double)bw.y / rnz);
     const double KX = kxv[kx], KZ = kzv[kp];
     const double2 nlv = make_double2(KZ * a.y + b.x, -KZ * a.x + b.y);  // -i kz A + B
     const long o = (long)j * ss + (long)kp * nkxp + kx;
@@ -1509,6 +1596,70 @@ int dg_chan_init(dg_handle *h) {
   return dg_cn_tables(h);
 }
 
+bool dg_mixed_ok(int nx, int nz, int n_th) {
+  return xw_supported(nx) && zw_supported(nz) && n_th <= 2;
+}
+
+// Steps 1-3 of a substep in the mixed form: the z inverse converts the FP64
+// state to FP32 half-physical planes, the x-row products and both x
+// transforms run in FP32, the z forward runs in FP32 and its epilogue (the
+// explicit terms, CF and the CN right-hand side) in FP64.
+static int nl_chunk_mixed(dg_handle *h, const ChanConst &C, int rk_step, int a, int b, int &hdone,
+                          const double2 *const *in, FieldPtrs cu, FieldPtrs cf, FieldPtrs rhs) {
+  float2 *Hf = reinterpret_cast<float2 *>(h->H);
+  float2 *Gf = reinterpret_cast<float2 *>(h->G);
+  const long Hfield = (long)h->nplanes * h->NZ * h->nkxp;
+  DG_TRY(dg_cinv_gf(h, in, h->nf, hdone + 1, b + 1, h->ss, h->nkxp, h->NZ, h->NKZ, h->plz, h->twz_f,
+                    Hf, Hfield));
+  hdone = b + 1;
+  const int nplan = b - a + 1;
+  int chunk = h->xrow_chunk;
+  if (chunk <= 0) {
+    chunk = (int)((long)nplan * h->NZ / (148L * 16));
+    if (chunk < 4) chunk = 4;
+  }
+  if (chunk > nplan) chunk = nplan;
+  dim3 grid(dg_cdiv(h->NZ, XW_WARPS), dg_cdiv(nplan, chunk));
+  bool done = false;
+#define XW_CASE(NXV, NTHV)                                                                      \
+  if (!done && h->NX == NXV && h->NTH == NTHV) {                                                \
+    dg_big_smem((const void *)k_xrow_w<NXV, NTHV, float2>);                                     \
+    dg_kt_begin(h, "k_xrow_w_f32", h->st);                                                      \
+    k_xrow_w<NXV, NTHV, float2><<<grid, 32 * XW_WARPS, xw_smem<NXV, NTHV, float2>(), h->st>>>(  \
+        C, Hf, Hfield, chunk, a, b, h->twx_f, h->dyf, h->dy, h->kx, Gf, Hfield);                \
+    done = true;                                                                                \
+  }
+#define XW_ALL(NXV) XW_CASE(NXV, 0) XW_CASE(NXV, 1) XW_CASE(NXV, 2)
+  XW_ALL(16) XW_ALL(32) XW_ALL(48) XW_ALL(64) XW_ALL(96) XW_ALL(128) XW_ALL(256)
+#undef XW_ALL
+#undef XW_CASE
+  if (!done) {
+    dg_set_error("mixed precision: no FP32 x-row kernel for this NX / N_TH");
+    return DG_ERR_DIMS;
+  }
+  DG_LAUNCHED();
+  dim3 zgrid(dg_cdiv(h->nkxp, ZW_KXG), nplan, h->nf);
+  const size_t sm = sizeof(float2) * (h->NZ + 16 * padded_len(h->NZ));
+  done = false;
+#define ZW_CASE(N)                                                                              \
+  if (!done && h->NZ == N) {                                                                    \
+    dg_big_smem((const void *)k_zfwd_w<N, float2>);                                             \
+    dg_kt_begin(h, "k_zfwd_w_f32", h->st);                                                      \
+    k_zfwd_w<N, float2><<<zgrid, 128, sm, h->st>>>(C, Gf, Hfield, h->twz_f, h->dscal, rk_step,   \
+                                                   h->kx, h->kz, h->dy, h->dyf, cu, cf, rhs,    \
+                                                   h->cp, a);                                   \
+    done = true;                                                                                \
+  }
+  ZW_CASE(16) ZW_CASE(32) ZW_CASE(48) ZW_CASE(64) ZW_CASE(96) ZW_CASE(128) ZW_CASE(256)
+#undef ZW_CASE
+  if (!done) {
+    dg_set_error("mixed precision: no FP32 z-forward kernel for this NZ");
+    return DG_ERR_DIMS;
+  }
+  DG_LAUNCHED();
+  return DG_OK;
+}
+
 extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
   if (!h || h->periodic || rk_step < 1 || rk_step > 3) return DG_ERR_ARG;
   const ChanConst C = make_const(h);
@@ -1526,6 +1677,10 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
   int hdone = -1;  // last H plane already produced
   for (int a = 1; a <= h->NY; a += cj) {
     const int b = (a + cj - 1 < h->NY) ? a + cj - 1 : h->NY;
+    if (h->mixed) {
+      DG_TRY(nl_chunk_mixed(h, C, rk_step, a, b, hdone, in, cu, cf, rhs));
+      continue;
+    }
     // 1. z inverse of the planes this chunk's x-rows need (a-1 .. b+1)
     DG_TRY(dg_zinv(h, in, h->nf, hdone + 1, b + 1, h->H, 0));
     hdone = b + 1;

@@ -24,132 +24,158 @@
 
 namespace dgfft {
 
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+// Complex helpers for double2 (FP64 path) and float2 (mixed path); CT<C>
+// gives the real type and a constructor.
+template <typename C> struct CT;
+template <> struct CT<double2> {
+  using T = double;
+  static __device__ __forceinline__ double2 mk(double a, double b) { return make_double2(a, b); }
+};
+template <> struct CT<float2> {
+  using T = float;
+  static __device__ __forceinline__ float2 mk(float a, float b) { return make_float2(a, b); }
+};
+
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return CT<C>::mk(a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return CT<C>::mk(a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  return CT<C>::mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
-__device__ __forceinline__ double2 conjg(double2 a) { return make_double2(a.x, -a.y); }
+template <typename C> __device__ __forceinline__ C cscale(C a, typename CT<C>::T s) {
+  return CT<C>::mk(a.x * s, a.y * s);
+}
+template <typename C> __device__ __forceinline__ C conjg(C a) { return CT<C>::mk(a.x, -a.y); }
 // multiply by sign*i
-__device__ __forceinline__ double2 mul_si(double2 a, int sign) {
-  return sign < 0 ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
+template <typename C> __device__ __forceinline__ C mul_si(C a, int sign) {
+  return sign < 0 ? CT<C>::mk(a.y, -a.x) : CT<C>::mk(-a.y, a.x);
 }
 
 __host__ __device__ constexpr int pad(int i) { return i + (i >> 4); }
 __host__ __device__ constexpr int padded_len(int n) { return n + (n >> 4) + 1; }
 
-template <int R>
-__device__ __forceinline__ void dft(double2 *v, int sign);
+template <int R> struct DFT;
 
-template <>
-__device__ __forceinline__ void dft<2>(double2 *v, int) {
-  double2 a = v[0], b = v[1];
-  v[0] = cadd(a, b);
-  v[1] = csub(a, b);
-}
+template <> struct DFT<2> {
+  template <typename C> static __device__ __forceinline__ void run(C *v, int) {
+    C a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
 
-template <>
-__device__ __forceinline__ void dft<3>(double2 *v, int sign) {
-  const double s3 = 0.86602540378443864676;  // sqrt(3)/2
-  double2 t1 = cadd(v[1], v[2]);
-  double2 t2 = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
-  double2 d = csub(v[1], v[2]);
-  double2 t3 = mul_si(cscale(d, s3), sign);
-  v[0] = cadd(v[0], t1);
-  v[1] = cadd(t2, t3);
-  v[2] = csub(t2, t3);
-}
+template <> struct DFT<3> {
+  template <typename C> static __device__ __forceinline__ void run(C *v, int sign) {
+    using T = typename CT<C>::T;
+    const T s3 = (T)0.86602540378443864676;  // sqrt(3)/2
+    C t1 = cadd(v[1], v[2]);
+    C t2 = CT<C>::mk(v[0].x - (T)0.5 * t1.x, v[0].y - (T)0.5 * t1.y);
+    C d = csub(v[1], v[2]);
+    C t3 = mul_si(cscale(d, s3), sign);
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(t2, t3);
+    v[2] = csub(t2, t3);
+  }
+};
 
-template <>
-__device__ __forceinline__ void dft<4>(double2 *v, int sign) {
-  double2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
-  double2 s13 = cadd(v[1], v[3]), d13 = mul_si(csub(v[1], v[3]), sign);
-  v[0] = cadd(s02, s13);
-  v[1] = cadd(d02, d13);
-  v[2] = csub(s02, s13);
-  v[3] = csub(d02, d13);
-}
+template <> struct DFT<4> {
+  template <typename C> static __device__ __forceinline__ void run(C *v, int sign) {
+    C s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+    C s13 = cadd(v[1], v[3]), d13 = mul_si(csub(v[1], v[3]), sign);
+    v[0] = cadd(s02, s13);
+    v[1] = cadd(d02, d13);
+    v[2] = csub(s02, s13);
+    v[3] = csub(d02, d13);
+  }
+};
 
-template <>
-__device__ __forceinline__ void dft<8>(double2 *v, int sign) {
-  const double h = 0.70710678118654752440;  // 1/sqrt(2)
-  double2 e[4] = {v[0], v[2], v[4], v[6]};
-  double2 o[4] = {v[1], v[3], v[5], v[7]};
-  dft<4>(e, sign);
-  dft<4>(o, sign);
-  // twiddles w8^t, w8 = exp(sign 2 pi i / 8) = (1 + sign i)/sqrt(2)
-  double2 o1 = o[1], o2 = o[2], o3 = o[3];
-  double2 t1 = make_double2(h * (o1.x - sign * o1.y), h * (o1.y + sign * o1.x));
-  double2 t2 = mul_si(o2, sign);
-  double2 t3 = make_double2(h * (-o3.x - sign * o3.y), h * (-o3.y + sign * o3.x));
-  v[0] = cadd(e[0], o[0]);
-  v[4] = csub(e[0], o[0]);
-  v[1] = cadd(e[1], t1);
-  v[5] = csub(e[1], t1);
-  v[2] = cadd(e[2], t2);
-  v[6] = csub(e[2], t2);
-  v[3] = cadd(e[3], t3);
-  v[7] = csub(e[3], t3);
-}
+template <> struct DFT<8> {
+  template <typename C> static __device__ __forceinline__ void run(C *v, int sign) {
+    using T = typename CT<C>::T;
+    const T h = (T)0.70710678118654752440;  // 1/sqrt(2)
+    C e[4] = {v[0], v[2], v[4], v[6]};
+    C o[4] = {v[1], v[3], v[5], v[7]};
+    DFT<4>::run(e, sign);
+    DFT<4>::run(o, sign);
+    // twiddles w8^t, w8 = exp(sign 2 pi i / 8) = (1 + sign i)/sqrt(2)
+    C o1 = o[1], o2 = o[2], o3 = o[3];
+    C t1 = CT<C>::mk(h * (o1.x - sign * o1.y), h * (o1.y + sign * o1.x));
+    C t2 = mul_si(o2, sign);
+    C t3 = CT<C>::mk(h * (-o3.x - sign * o3.y), h * (-o3.y + sign * o3.x));
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], t1);
+    v[5] = csub(e[1], t1);
+    v[2] = cadd(e[2], t2);
+    v[6] = csub(e[2], t2);
+    v[3] = cadd(e[3], t3);
+    v[7] = csub(e[3], t3);
+  }
+};
 
 // 16-point DFT as 4 x 4: n = 4 n1 + n2, k = k1 + 4 k2
-template <>
-__device__ __forceinline__ void dft<16>(double2 *v, int sign) {
-  // cos and sin of 2 pi m / 16, m = 0..9
-  const double C[10] = {1.0, 0.92387953251128675613, 0.70710678118654752440,
-                        0.38268343236508977173, 0.0, -0.38268343236508977173,
-                        -0.70710678118654752440, -0.92387953251128675613, -1.0,
-                        -0.92387953251128675613};
-  const double S[10] = {0.0, 0.38268343236508977173, 0.70710678118654752440,
-                        0.92387953251128675613, 1.0, 0.92387953251128675613,
-                        0.70710678118654752440, 0.38268343236508977173, 0.0,
-                        -0.38268343236508977173};
-  double2 a[4][4];
+template <> struct DFT<16> {
+  template <typename C> static __device__ __forceinline__ void run(C *v, int sign) {
+    using T = typename CT<C>::T;
+    // cos and sin of 2 pi m / 16, m = 0..9
+    const T Cs[10] = {(T)1.0, (T)0.92387953251128675613, (T)0.70710678118654752440,
+                      (T)0.38268343236508977173, (T)0.0, (T)-0.38268343236508977173,
+                      (T)-0.70710678118654752440, (T)-0.92387953251128675613, (T)-1.0,
+                      (T)-0.92387953251128675613};
+    const T Sn[10] = {(T)0.0, (T)0.38268343236508977173, (T)0.70710678118654752440,
+                      (T)0.92387953251128675613, (T)1.0, (T)0.92387953251128675613,
+                      (T)0.70710678118654752440, (T)0.38268343236508977173, (T)0.0,
+                      (T)-0.38268343236508977173};
+    C a[4][4];
 #pragma unroll
-  for (int n2 = 0; n2 < 4; n2++) {
-    double2 t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
-    dft<4>(t, sign);
+    for (int n2 = 0; n2 < 4; n2++) {
+      C t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+      DFT<4>::run(t, sign);
+#pragma unroll
+      for (int k1 = 0; k1 < 4; k1++) {
+        const int m = n2 * k1;
+        C x = t[k1];
+        if (m != 0) {
+          const C w = CT<C>::mk(Cs[m], sign * Sn[m]);
+          x = cmul(x, w);
+        }
+        a[n2][k1] = x;
+      }
+    }
 #pragma unroll
     for (int k1 = 0; k1 < 4; k1++) {
-      const int m = n2 * k1;
-      double2 x = t[k1];
-      if (m != 0) {
-        const double2 w = make_double2(C[m], sign * S[m]);
-        x = cmul(x, w);
-      }
-      a[n2][k1] = x;
+      C t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+      DFT<4>::run(t, sign);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; k2++) v[k1 + 4 * k2] = t[k2];
     }
   }
-#pragma unroll
-  for (int k1 = 0; k1 < 4; k1++) {
-    double2 t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
-    dft<4>(t, sign);
-#pragma unroll
-    for (int k2 = 0; k2 < 4; k2++) v[k1 + 4 * k2] = t[k2];
-  }
+};
+
+template <int R, typename C>
+__device__ __forceinline__ void dft(C *v, int sign) {
+  DFT<R>::run(v, sign);
 }
 
 // -------------------------------------------------------- runtime-plan pass
-template <int R>
-__device__ __forceinline__ void pass(const double2 *__restrict__ src, double2 *__restrict__ dst,
+template <int R, typename C>
+__device__ __forceinline__ void pass(const C *__restrict__ src, C *__restrict__ dst,
                                      int N, int Ns, int nsig, int sig_stride,
-                                     const double2 *__restrict__ tw, int sign, int tid, int nthr) {
+                                     const C *__restrict__ tw, int sign, int tid, int nthr) {
   const int nb = N / R;
   const int tmul = N / (Ns * R);
   const int total = nsig * nb;
   for (int w = tid; w < total; w += nthr) {
     const int s = w / nb;
     const int b = w - s * nb;
-    const double2 *in = src + (long)s * sig_stride;
-    double2 *out = dst + (long)s * sig_stride;
+    const C *in = src + (long)s * sig_stride;
+    C *out = dst + (long)s * sig_stride;
     const int k = b % Ns;
-    double2 v[R];
+    C v[R];
 #pragma unroll
     for (int r = 0; r < R; r++) {
-      double2 x = in[pad(b + r * nb)];
+      C x = in[pad(b + r * nb)];
       if (r > 0 && k > 0) {
-        double2 t = tw[r * k * tmul];
+        C t = tw[r * k * tmul];
         if (sign > 0) t.y = -t.y;
         x = cmul(x, t);
       }
@@ -164,11 +190,12 @@ __device__ __forceinline__ void pass(const double2 *__restrict__ src, double2 *_
 
 // Runs a runtime plan; returns the buffer holding the result (buf0 or buf1).
 // Must be called by every thread of the CTA.
-__device__ inline double2 *run(double2 *buf0, double2 *buf1, const FftPlan &pl, int nsig,
-                               int sig_stride, const double2 *tw, int sign) {
+template <typename C>
+__device__ inline C *run(C *buf0, C *buf1, const FftPlan &pl, int nsig,
+                               int sig_stride, const C *tw, int sign) {
   const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
   const int nthr = blockDim.x * blockDim.y * blockDim.z;
-  double2 *src = buf0, *dst = buf1;
+  C *src = buf0, *dst = buf1;
   int Ns = 1;
   for (int p = 0; p < pl.np; p++) {
     const int R = pl.r[p];
@@ -180,7 +207,7 @@ __device__ inline double2 *run(double2 *buf0, double2 *buf1, const FftPlan &pl, 
       default: pass<2>(src, dst, pl.n, Ns, nsig, sig_stride, tw, sign, tid, nthr); break;
     }
     __syncthreads();
-    double2 *t = src;
+    C *t = src;
     src = dst;
     dst = t;
     Ns *= R;
@@ -213,9 +240,9 @@ __host__ __device__ constexpr int plan_ns(int N, int p) {
   return ns;
 }
 
-template <int N, int R, int NS, int SIGN>
-__device__ __forceinline__ void cpass(const double2 *__restrict__ src, double2 *__restrict__ dst,
-                                      int nsig, int sig_stride, const double2 *__restrict__ tw,
+template <int N, int R, int NS, int SIGN, typename C>
+__device__ __forceinline__ void cpass(const C *__restrict__ src, C *__restrict__ dst,
+                                      int nsig, int sig_stride, const C *__restrict__ tw,
                                       int tid, int nthr) {
   constexpr int NB = N / R;
   constexpr int TMUL = N / (NS * R);
@@ -223,15 +250,15 @@ __device__ __forceinline__ void cpass(const double2 *__restrict__ src, double2 *
   for (int w = tid; w < total; w += nthr) {
     const int s = w / NB;
     const int b = w - s * NB;
-    const double2 *in = src + (long)s * sig_stride;
-    double2 *out = dst + (long)s * sig_stride;
+    const C *in = src + (long)s * sig_stride;
+    C *out = dst + (long)s * sig_stride;
     const int k = b % NS;
-    double2 v[R];
+    C v[R];
 #pragma unroll
     for (int r = 0; r < R; r++) {
-      double2 x = in[pad(b + r * NB)];
+      C x = in[pad(b + r * NB)];
       if (NS > 1 && r > 0) {
-        double2 t = tw[r * k * TMUL];
+        C t = tw[r * k * TMUL];
         if (SIGN > 0) t.y = -t.y;
         x = cmul(x, t);
       }
@@ -244,15 +271,15 @@ __device__ __forceinline__ void cpass(const double2 *__restrict__ src, double2 *
   }
 }
 
-template <int N, int SIGN, int P>
-__device__ __forceinline__ void cpasses(double2 *&src, double2 *&dst, int nsig, int sig_stride,
-                                        const double2 *tw, int tid, int nthr) {
+template <int N, int SIGN, int P, typename C>
+__device__ __forceinline__ void cpasses(C *&src, C *&dst, int nsig, int sig_stride,
+                                        const C *tw, int tid, int nthr) {
   constexpr int R = plan_radix(N, P);
   if constexpr (R != 0) {
     constexpr int NS = plan_ns(N, P);
     cpass<N, R, NS, SIGN>(src, dst, nsig, sig_stride, tw, tid, nthr);
     __syncthreads();
-    double2 *t = src;
+    C *t = src;
     src = dst;
     dst = t;
     cpasses<N, SIGN, P + 1>(src, dst, nsig, sig_stride, tw, tid, nthr);
@@ -261,9 +288,9 @@ __device__ __forceinline__ void cpasses(double2 *&src, double2 *&dst, int nsig, 
 
 // In-place variant: each round covers whole signals (nthr / (N/R) of them);
 // every thread of the round loads its butterfly, the CTA syncs, then stores.
-template <int N, int R, int NS, int SIGN>
-__device__ __forceinline__ void ippass(double2 *__restrict__ buf, int nsig, int sig_stride,
-                                       const double2 *__restrict__ tw, int tid, int nthr) {
+template <int N, int R, int NS, int SIGN, typename C>
+__device__ __forceinline__ void ippass(C *__restrict__ buf, int nsig, int sig_stride,
+                                       const C *__restrict__ tw, int tid, int nthr) {
   constexpr int NB = N / R;
   constexpr int TMUL = N / (NS * R);
   const int spr = nthr / NB;
@@ -273,14 +300,14 @@ __device__ __forceinline__ void ippass(double2 *__restrict__ buf, int nsig, int 
   for (int rd = 0; rd < nrounds; rd++) {
     const int s = rd * spr + sl;
     const bool act = (sl < spr) && (s < nsig);
-    double2 v[R];
+    C v[R];
     if (act) {
-      const double2 *in = buf + (long)s * sig_stride;
+      const C *in = buf + (long)s * sig_stride;
 #pragma unroll
       for (int r = 0; r < R; r++) {
-        double2 x = in[pad(b + r * NB)];
+        C x = in[pad(b + r * NB)];
         if (NS > 1 && r > 0) {
-          double2 t = tw[r * k * TMUL];
+          C t = tw[r * k * TMUL];
           if (SIGN > 0) t.y = -t.y;
           x = cmul(x, t);
         }
@@ -290,7 +317,7 @@ __device__ __forceinline__ void ippass(double2 *__restrict__ buf, int nsig, int 
     }
     __syncthreads();
     if (act) {
-      double2 *out = buf + (long)s * sig_stride;
+      C *out = buf + (long)s * sig_stride;
 #pragma unroll
       for (int r = 0; r < R; r++) out[pad(idx + r * NS)] = v[r];
     }
@@ -298,8 +325,8 @@ __device__ __forceinline__ void ippass(double2 *__restrict__ buf, int nsig, int 
   }
 }
 
-template <int N, int SIGN, int P>
-__device__ __forceinline__ void ippasses(double2 *buf, int nsig, int sig_stride, const double2 *tw,
+template <int N, int SIGN, int P, typename C>
+__device__ __forceinline__ void ippasses(C *buf, int nsig, int sig_stride, const C *tw,
                                          int tid, int nthr) {
   constexpr int R = plan_radix(N, P);
   if constexpr (R != 0) {
@@ -309,12 +336,12 @@ __device__ __forceinline__ void ippasses(double2 *buf, int nsig, int sig_stride,
   }
 }
 
-template <int N, int SIGN>
-__device__ __forceinline__ double2 *run_ct(double2 *buf0, double2 *buf1, int nsig, int sig_stride,
-                                           const double2 *tw) {
+template <int N, int SIGN, typename C>
+__device__ __forceinline__ C *run_ct(C *buf0, C *buf1, int nsig, int sig_stride,
+                                           const C *tw) {
   const int tid = threadIdx.x;
   const int nthr = blockDim.x;
-  double2 *src = buf0, *dst = buf1;
+  C *src = buf0, *dst = buf1;
   cpasses<N, SIGN, 0>(src, dst, nsig, sig_stride, tw, tid, nthr);
   return src;
 }
@@ -327,9 +354,9 @@ __host__ __device__ constexpr bool warp_fft_ok(int n) {
   return n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 256;
 }
 
-template <int N, int R, int NS, int SIGN>
-__device__ __forceinline__ void wpass(double2 *__restrict__ buf, int nsig, int sstr,
-                                      const double2 *__restrict__ tw, int lane) {
+template <int N, int R, int NS, int SIGN, typename C>
+__device__ __forceinline__ void wpass(C *__restrict__ buf, int nsig, int sstr,
+                                      const C *__restrict__ tw, int lane) {
   constexpr int NB = N / R;
   static_assert(NB <= 32, "warp pass needs N/R <= 32");
   constexpr int TMUL = N / (NS * R);
@@ -339,14 +366,14 @@ __device__ __forceinline__ void wpass(double2 *__restrict__ buf, int nsig, int s
   for (int s0 = 0; s0 < nsig; s0 += SPR) {
     const int s = s0 + sl;
     const bool act = (sl < SPR) && (s < nsig);
-    double2 v[R];
+    C v[R];
     if (act) {
-      const double2 *in = buf + s * sstr;
+      const C *in = buf + s * sstr;
 #pragma unroll
       for (int r = 0; r < R; r++) {
-        double2 x = in[pad(b + r * NB)];
+        C x = in[pad(b + r * NB)];
         if (NS > 1 && r > 0) {
-          double2 t = tw[r * k * TMUL];
+          C t = tw[r * k * TMUL];
           if (SIGN > 0) t.y = -t.y;
           x = cmul(x, t);
         }
@@ -356,7 +383,7 @@ __device__ __forceinline__ void wpass(double2 *__restrict__ buf, int nsig, int s
     }
     __syncwarp();
     if (act) {
-      double2 *out = buf + s * sstr;
+      C *out = buf + s * sstr;
 #pragma unroll
       for (int r = 0; r < R; r++) out[pad(idx + r * NS)] = v[r];
     }
@@ -364,8 +391,8 @@ __device__ __forceinline__ void wpass(double2 *__restrict__ buf, int nsig, int s
   }
 }
 
-template <int N, int SIGN, int P>
-__device__ __forceinline__ void wpasses(double2 *buf, int nsig, int sstr, const double2 *tw,
+template <int N, int SIGN, int P, typename C>
+__device__ __forceinline__ void wpasses(C *buf, int nsig, int sstr, const C *tw,
                                         int lane) {
   constexpr int R = plan_radix(N, P);
   if constexpr (R != 0) {
@@ -376,9 +403,9 @@ __device__ __forceinline__ void wpasses(double2 *buf, int nsig, int sstr, const 
 
 // Compile-time lengths run in place in buf0 (buf1 unused); the runtime plan
 // ping-pongs between buf0 and buf1.
-template <int N>
-__device__ __forceinline__ double2 *fft(double2 *buf0, double2 *buf1, const FftPlan &pl, int nsig,
-                                        int sig_stride, const double2 *tw, int sign) {
+template <int N, typename C>
+__device__ __forceinline__ C *fft(C *buf0, C *buf1, const FftPlan &pl, int nsig,
+                                        int sig_stride, const C *tw, int sign) {
   if constexpr (N == 0) {
     return run(buf0, buf1, pl, nsig, sig_stride, tw, sign);
   } else {
@@ -391,9 +418,9 @@ __device__ __forceinline__ double2 *fft(double2 *buf0, double2 *buf1, const FftP
 
 // CTA front end: with a warp-capable length the signals are dealt out to the
 // warps (no CTA barrier between passes), otherwise the CTA-wide passes run.
-template <int N>
-__device__ __forceinline__ double2 *fft_cta(double2 *buf0, double2 *buf1, const FftPlan &pl,
-                                            int nsig, int sig_stride, const double2 *tw,
+template <int N, typename C>
+__device__ __forceinline__ C *fft_cta(C *buf0, C *buf1, const FftPlan &pl,
+                                            int nsig, int sig_stride, const C *tw,
                                             int sign) {
   if constexpr (N != 0 && warp_fft_ok(N)) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;

@@ -36,18 +36,19 @@ __device__ __forceinline__ int packed_index(int z, int NZ, int NKZ) {
   return -1;
 }
 
-template <int NT>
+template <int NT, typename CX>
 __global__ void __launch_bounds__(NTHR) k_zinv(CFieldPtrs fields, int jmin, long ss, int nkxp,
                                               int NZr, int NKZ, FftPlan pl,
-                                              const double2 *__restrict__ tw,
-                                              double2 *__restrict__ H, long Hfield) {
-  extern __shared__ double2 sm[];
+                                              const CX *__restrict__ tw,
+                                              CX *__restrict__ H, long Hfield) {
+  extern __shared__ double2 sm_raw[];
+  CX *sm = reinterpret_cast<CX *>(sm_raw);
   const int NZ = NT ? NT : NZr;
   const int KXG = batch_for(NZ);
   const int sstr = padded_len(NZ);
-  double2 *stw = sm;
-  double2 *b0 = stw + NZ;
-  double2 *b1 = b0 + KXG * sstr;
+  CX *stw = sm;
+  CX *b0 = stw + NZ;
+  CX *b1 = b0 + KXG * sstr;
   const int kx0 = blockIdx.x * KXG;
   const int j = jmin + blockIdx.y;
   const int f = blockIdx.z;
@@ -67,12 +68,14 @@ __global__ void __launch_bounds__(NTHR) k_zinv(CFieldPtrs fields, int jmin, long
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       const int idx = base + u * nthr + tid;
-      if (idx < KXG * NZ) b0[(idx % KXG) * sstr + pad(idx / KXG)] = v[u];
+      if (idx < KXG * NZ)
+        b0[(idx % KXG) * sstr + pad(idx / KXG)] =
+            CT<CX>::mk((typename CT<CX>::T)v[u].x, (typename CT<CX>::T)v[u].y);
     }
   }
   __syncthreads();
-  double2 *res = fft_cta<NT>(b0, b1, pl, KXG, sstr, stw, +1);
-  double2 *out = H + f * Hfield + (long)j * NZ * nkxp;
+  CX *res = fft_cta<NT>(b0, b1, pl, KXG, sstr, stw, +1);
+  CX *out = H + f * Hfield + (long)j * NZ * nkxp;
   for (int idx = tid; idx < KXG * NZ; idx += nthr) {
     const int c = idx % KXG, z = idx / KXG;
     if (kx0 + c < nkxp) out[(long)z * nkxp + kx0 + c] = res[c * sstr + pad(z)];
@@ -280,7 +283,9 @@ __global__ void __launch_bounds__(NTHR) k_xr2c(const double *__restrict__ phys, 
   }
 }
 
-size_t zsmem(int NZ) { return sizeof(double2) * (NZ + fft_bufs(NZ) * batch_for(NZ) * padded_len(NZ)); }
+size_t zsmem(int NZ, size_t esz = sizeof(double2)) {
+  return esz * (NZ + fft_bufs(NZ) * batch_for(NZ) * padded_len(NZ));
+}
 size_t xsmem(int NX) { return sizeof(double2) * (NX + fft_bufs(NX) * batch_for(NX) * padded_len(NX)); }
 
 }  // namespace
@@ -308,18 +313,19 @@ void big_smem(K kern) {
 // at + kp*rowlen + c; output plane j at H + f*out_field + j*N*rowlen, bin z of
 // column c at + z*rowlen + c.  z transforms: rowlen = NKX+1, planes = y;
 // y transforms (periodic): rowlen = modes per ky-plane, one plane.
-int dg_cinv_g(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax,
-              long in_plane, int rowlen, int N, int NK, const FftPlan &pl, const double2 *tw,
-              double2 *H, long out_field) {
+template <typename CX>
+static int cinv_t(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax,
+                  long in_plane, int rowlen, int N, int NK, const FftPlan &pl, const CX *tw, CX *H,
+                  long out_field) {
   if (jmax < jmin || nf <= 0) return DG_OK;
   CFieldPtrs fp;
   for (int f = 0; f < nf; f++) fp.p[f] = fields[f];
   dim3 grid(dg_cdiv(rowlen, batch_for(N)), jmax - jmin + 1, nf);
-  const size_t sm = zsmem(N);
+  const size_t sm = zsmem(N, sizeof(CX));
 #define KERNEL_BODY(NN)                                                                       \
-  big_smem(k_zinv<NN>);                                                                       \
-  dg_kt_begin(h, "k_zinv", h->st);                                                              \
-  k_zinv<NN><<<grid, NTHR, sm, h->st>>>(fp, jmin, in_plane, rowlen, N, NK, pl, tw, H, out_field)
+  big_smem(k_zinv<NN, CX>);                                                                   \
+  dg_kt_begin(h, "k_zinv", h->st);                                                            \
+  k_zinv<NN, CX><<<grid, NTHR, sm, h->st>>>(fp, jmin, in_plane, rowlen, N, NK, pl, tw, H, out_field)
   switch (N) {
     DG_FOR_EACH_N(DG_CASE_N)
     default: KERNEL_BODY(0); break;
@@ -327,6 +333,18 @@ int dg_cinv_g(dg_handle *h, const double2 *const *fields, int nf, int jmin, int 
 #undef KERNEL_BODY
   DG_LAUNCHED();
   return DG_OK;
+}
+
+int dg_cinv_g(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax,
+              long in_plane, int rowlen, int N, int NK, const FftPlan &pl, const double2 *tw,
+              double2 *H, long out_field) {
+  return cinv_t(h, fields, nf, jmin, jmax, in_plane, rowlen, N, NK, pl, tw, H, out_field);
+}
+
+int dg_cinv_gf(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax,
+               long in_plane, int rowlen, int N, int NK, const FftPlan &pl, const float2 *tw,
+               float2 *H, long out_field) {
+  return cinv_t(h, fields, nf, jmin, jmax, in_plane, rowlen, N, NK, pl, tw, H, out_field);
 }
 
 int dg_cfwd_g(dg_handle *h, const double2 *H, long in_field, int nf, int jmin, int jmax,

@@ -107,11 +107,20 @@ static int validate(const dg_params *p, const double *gy) {
         dg_set_error("Error: V_BC_Y* must be 0, 1, or 2");
         return DG_ERR_ARG;
       }
-    if (p->precision != 0) {
-      dg_set_error("channel mixed precision is not available");
+    if (p->precision != 0 && p->precision != 1) {
+      dg_set_error("precision must be 0 (FP64) or 1 (mixed)");
       return DG_ERR_ARG;
     }
+    if (p->precision == 1 && !dg_mixed_ok(p->nx, p->nz, p->n_th)) {
+      dg_set_error("mixed precision needs NX and NZ in {16, 32, 48, 64, 96, 128, 256} and "
+                   "N_TH <= 2");
+      return DG_ERR_DIMS;
+    }
   } else {
+    if (p->precision != 0) {
+      dg_set_error("the periodic path runs in FP64 only (precision = 0)");
+      return DG_ERR_ARG;
+    }
     if (!dg_make_plan(p->ny, &t) || p->ny < 8) {
       dg_set_error("periodic NY must be >= 8 and factor into 2 and 3");
       return DG_ERR_DIMS;
@@ -235,6 +244,19 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
     DG_TRY(dalloc(&h->twz, h->NZ));
     twiddles(h->NZ, tmp);
     DG_CUDA(cudaMemcpy(h->twz, tmp, sizeof(double2) * h->NZ, cudaMemcpyHostToDevice));
+    if (p->precision == 1) {
+      h->mixed = 1;
+      float2 *tf = (float2 *)malloc(sizeof(float2) * nmax);
+      twiddles(h->NX, tmp);
+      for (int m = 0; m < h->NX; m++) tf[m] = make_float2((float)tmp[m].x, (float)tmp[m].y);
+      DG_CUDA(cudaMalloc((void **)&h->twx_f, sizeof(float2) * h->NX));
+      DG_CUDA(cudaMemcpy(h->twx_f, tf, sizeof(float2) * h->NX, cudaMemcpyHostToDevice));
+      twiddles(h->NZ, tmp);
+      for (int m = 0; m < h->NZ; m++) tf[m] = make_float2((float)tmp[m].x, (float)tmp[m].y);
+      DG_CUDA(cudaMalloc((void **)&h->twz_f, sizeof(float2) * h->NZ));
+      DG_CUDA(cudaMemcpy(h->twz_f, tf, sizeof(float2) * h->NZ, cudaMemcpyHostToDevice));
+      free(tf);
+    }
     if (h->periodic) {
       DG_TRY(dalloc(&h->twy, h->NY));
       twiddles(h->NY, tmp);
@@ -285,7 +307,7 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
   if (!h) return DG_OK;
   cudaStreamSynchronize(h->st);
   void *dp[] = {h->gyf, h->dy, h->dyf, h->kx, h->kz, h->ky, h->kx2, h->kz2, h->ky2, h->twx, h->twz,
-                h->twy, h->dscal, h->cp, h->cr1, h->gphi, h->rem_a, h->rem_rb, h->cn_tab, h->cn_rows, h->H, h->G, h->work, h->dmin_bits, h->dflag, h->Hy, h->P,
+                h->twy, h->twx_f, h->twz_f, h->dscal, h->cp, h->cr1, h->gphi, h->rem_a, h->rem_rb, h->cn_tab, h->cn_rows, h->H, h->G, h->work, h->dmin_bits, h->dflag, h->Hy, h->P,
                 h->Q};
   for (void *q : dp)
     if (q) cudaFree(q);

@@ -44,3 +44,19 @@ def test_init_refuses_without_device_or_bad_args():
                                  g.ctypes.data_as(ctypes.c_void_p), None, ctypes.byref(h))
         assert code == 7  # DG_ERR_NODEV
         assert b"device" in L.dg_last_error()
+
+
+def test_mixed_precision_refuses_unsupported_sizes():
+    L = _lib.load()
+    import numpy as np
+    p, gy = configs.kh_shear_layer(nx=36, ny=17, nz=18)
+    g = np.ascontiguousarray(gy)
+    h = ctypes.c_void_p()
+    code = L.diablo_gpu_init(ctypes.byref(p.replace(precision=1).to_struct(DgParams)),
+                             g.ctypes.data_as(ctypes.c_void_p), None, ctypes.byref(h))
+    assert code == 2  # DG_ERR_DIMS, before any device call
+    assert b"mixed precision" in L.dg_last_error()
+    q, _ = configs.periodic_256(n=32)
+    code = L.diablo_gpu_init(ctypes.byref(q.replace(precision=1).to_struct(DgParams)), None, None,
+                             ctypes.byref(h))
+    assert code == 1

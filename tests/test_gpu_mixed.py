@@ -1,0 +1,93 @@
+"""Mixed-precision channel path (dg_params.precision = 1) against the FP64
+oracle (needs a B200).
+
+FFTs, the physical-space products and the x/z transforms of the nonlinear
+terms run in FP32; the explicit-term assembly, the CN and REM_DIV solves, the
+(0,0) mode and the statistics stay FP64.  Bar: relative L2 <= 1e-5 on U1, U2,
+U3 and TH after 100 steps, divergence at the FP64 level (the projection is
+FP64), and the KH growth rate of the vertical-velocity energy within 1e-4 of
+the oracle's.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from diablo_b200 import configs, ics
+
+pytestmark = pytest.mark.gpu
+
+TOL_MIXED = 1e-5
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def pair(p, gy, maker, seed):
+    from diablo_b200.solver import Channel
+    ref = O.Oracle(p, gy)
+    u1, u2, u3, th = maker(p, gy, seed=seed)
+    ref.create_flow_chan(u1, u2, u3, th if p.n_th else None)
+    g = Channel(p.replace(precision=1), gy)
+    g.set_state(ref.state())
+    g.set_time(0.0, p.delta_t)
+    return ref, g
+
+
+def fields(p):
+    return ["CU1", "CU2", "CU3"] + [f"CTH{n}" for n in range(p.n_th)]
+
+
+def test_mixed_kh_100_steps_and_growth_rate():
+    p, gy = configs.kh_shear_layer()
+    ref, g = pair(p, gy, ics.kh_shear_layer, seed=1)
+    vo, vg, t = [], [], []
+    for s in range(1, 101):
+        ref.step(s)
+        g.steps(s, 1)
+        if s % 10 == 0:
+            so, sg = ref.stats(), g.stats()
+            vo.append(so["vrms_b"] ** 2)
+            vg.append(sg["vrms_b"] ** 2)
+            t.append(s * p.delta_t)
+            assert sg["div_max"] <= 1e-12
+    err = {nm: rel(g.get_field(nm), ref.get(nm)) for nm in fields(p)}
+    assert all(v <= TOL_MIXED for v in err.values()), err
+    # growth rate of the vertical-velocity energy, least squares on ln E2(t)
+    ro = np.polyfit(t, np.log(vo), 1)[0]
+    rg = np.polyfit(t, np.log(vg), 1)[0]
+    assert abs(rg - ro) <= 1e-4 * max(abs(ro), 1e-30), (rg, ro)
+    g.close()
+
+
+def test_mixed_re180_100_steps():
+    p, gy = configs.channel_re180()
+    ref, g = pair(p, gy, ics.channel_laminar, seed=2)
+    for s in range(1, 101):
+        ref.step(s)
+        g.steps(s, 1)
+    err = {nm: rel(g.get_field(nm), ref.get(nm)) for nm in fields(p)}
+    assert all(v <= TOL_MIXED for v in err.values()), err
+    so, sg = ref.stats(), g.stats()
+    assert abs(sg["ke"] - so["ke"]) <= 1e-6 * so["ke"]
+    assert sg["div_max"] <= 1e-12
+    t_o, dt_o = ref.get_time()
+    t_g, dt_g = g.get_time()
+    assert abs(dt_g - dt_o) <= 1e-6 * dt_o
+    g.close()
+
+
+def test_mixed_two_scalars_short():
+    p, gy = configs.kh_shear_layer(nx=64, ny=33, nz=32)
+    p = p.replace(n_th=2)
+    p.ri = [0.1, 0.05, 0, 0]
+    p.pr = [1.0, 2.0, 1, 1]
+    p.th_bc_ymin = [0, 1, 0, 0]
+    p.th_bc_ymax = [0, 1, 0, 0]
+    ref, g = pair(p, gy, ics.kh_shear_layer, seed=3)
+    for s in range(1, 21):
+        ref.step(s)
+        g.steps(s, 1)
+    err = {nm: rel(g.get_field(nm), ref.get(nm)) for nm in fields(p)}
+    assert all(v <= TOL_MIXED for v in err.values()), err
+    g.close()

@@ -30,6 +30,10 @@ import time
 
 import numpy as np
 
+# the served ensemble runs one stream per active case: give the device more
+# hardware work queues than the default 8 (read when the CUDA context starts)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -179,6 +183,81 @@ def cpu_baseline(p, gy, seconds=15.0, threads=None):
     return {"value": pts * n / dt / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{n} full RK3 steps of the same 128x129x128 case (FP64 oracle, "
                       f"{threads} OpenMP threads, {dt:.1f} s)"}
+
+
+def run_ensemble(args):
+    """The served-ensemble workload: KH cases with NX in {64,128,256}, NZ in
+    {16,32,64}, NY in {33,65,129} (uniform on [-10,10]), Re ~ U[500,5000],
+    Ri ~ U[0.05,0.25], seeded 1e-3 noise, Poisson arrivals at `rate`/s, each
+    run for `steps` RK3 steps in mixed precision under a 150 GB budget through
+    the continuous-batching server.  Beside it, the plain per-case FP64 path
+    (one case at a time, graph-replayed steps) on a sample of the same cases."""
+    import torch
+    from diablo_b200 import configs, ics
+    from diablo_b200.grid import uniform_grid
+    from diablo_b200.serve import Server
+    from diablo_b200.solver import Channel
+    rng = np.random.default_rng(5)
+    base, _ = configs.kh_shear_layer()
+    cases = []
+    for _ in range(args.ensemble_cases):
+        q = ics.ensemble_kh_params(rng, base)
+        cases.append((q, uniform_grid(q.ny, -10.0, 10.0)))
+    arrivals = np.cumsum(rng.exponential(1.0 / args.ensemble_rate, len(cases)))
+    # plain per-case FP64 path on a sample: device time of each case alone
+    sample = cases[: min(16, len(cases))]
+    plain_pts, plain_s = 0.0, 0.0
+    psteps = min(args.ensemble_steps, 100)
+    for i, (q, gy) in enumerate(sample):
+        st = torch.cuda.Stream()
+        ch = Channel(q, gy, stream=st.cuda_stream)
+        for k, v in ics.kh_state(q, gy, seed=100 + i).items():
+            ch.set_field(k, v)
+        ch.set_time(0.0, q.delta_t)
+        ch.apply_bc_vel()
+        ch.rem_div_chan()
+        ch.apply_bc_vel()
+        ch.steps(1, 3)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        ch.steps(4, psteps)
+        e1.record(st)
+        e1.synchronize()
+        plain_s += e0.elapsed_time(e1) * 1e-3
+        plain_pts += q.nx * q.ny * q.nz * psteps
+        ch.close()
+    plain = plain_pts / plain_s / 1e6
+    # served, mixed precision, continuous batching
+    srv = Server(max_active=args.ensemble_active, budget_gb=150.0, autotune=True)
+    t0 = time.perf_counter()
+    ids = []
+    for i, (q, gy) in enumerate(cases):
+        st0 = ics.kh_state(q, gy, seed=100 + i)
+        delay = t0 + arrivals[i] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(q.replace(precision=1), gy, st0, args.ensemble_steps))
+    lat = []
+    for cid in ids:
+        _, (qs, rs) = srv.wait(cid)
+        lat.append(qs + rs)
+    wall = time.perf_counter() - t0
+    s = srv.stats()
+    srv.close()
+    pts = sum(q.nx * q.ny * q.nz for q, _ in cases) * args.ensemble_steps
+    served = pts / s["wall_s"] / 1e6
+    return {"cases": len(cases), "steps_per_case": args.ensemble_steps,
+            "arrival_rate_per_s": args.ensemble_rate, "max_active": args.ensemble_active,
+            "precision": "mixed (FP32 transforms and products, FP64 solves)",
+            "cases_per_s": s["cases_per_s"], "step_ms_p50": s["step_ms_p50"],
+            "step_ms_p99": s["step_ms_p99"], "mpoint_steps_per_s": served,
+            "case_latency_s_p50": float(np.percentile(lat, 50)),
+            "case_latency_s_p99": float(np.percentile(lat, 99)),
+            "hbm_peak_gb": s["bytes_peak"] / 1e9, "wall_s": wall,
+            "plain_fp64_mpoint_steps_per_s": plain,
+            "plain_sample": f"{len(sample)} of the cases alone, {psteps} steps each, FP64",
+            "served_over_plain": served / plain}
 
 
 def run_reference(args):
@@ -385,11 +464,12 @@ def run_gpu(args):
                  "scope": "whole RK3 step: algorithmic bytes (17 Nf + 6) x 16 B x M per step "
                           f"= {bstep / 1e6:.1f} MB over the device time of one step"}
     cpu = cpu_baseline(p, gy, seconds=args.cpu_seconds) if args.cpu_seconds > 0 else None
+    ens = run_ensemble(args) if args.ensemble_cases > 0 else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(workload_config(p), tuning=tuned), "roofline": roof, "roofline_step": roof_step,
-            "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
+            "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "ensemble": ens,
             "gpu_launches": int(launches), "clocks": clocks,
             "check": {"ke": st["ke"], "div_max": st["div_max"], "ubulk": st["ubulk"]}}
     print(json.dumps(line))
@@ -403,6 +483,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ensemble-cases", type=int, default=256)
+    ap.add_argument("--ensemble-steps", type=int, default=500)
+    ap.add_argument("--ensemble-rate", type=float, default=20.0)
+    ap.add_argument("--ensemble-active", type=int, default=32)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -87,10 +87,16 @@ def load(path: str = LIB_PATH):
         "dg_timing_enable": [P, I], "diablo_step": [P, I, I],
         "dg_tune_set": [P, I, I], "dg_tune_get": [P, I, ctypes.POINTER(I)],
         "dg_autotune": [P, I],
+        "dg_server_create": [I, D, I, ctypes.POINTER(P)],
+        "dg_server_submit": [P, P, P, P, I, I, ctypes.POINTER(ctypes.c_int64)],
+        "dg_server_wait": [P, ctypes.c_int64, P, P],
+        "dg_server_query": [P, P], "dg_server_destroy": [P],
         "dg_timing_read": [P, I, ctypes.c_char_p, I, ctypes.POINTER(ctypes.c_int64),
                            ctypes.POINTER(D)],
         "diablo_stats": [P, ctypes.POINTER(DgStats)],
     }
+    L.dg_state_bytes.argtypes = [P]
+    L.dg_state_bytes.restype = ctypes.c_int64
     for name, args in sigs.items():
         fn = getattr(L, name)
         fn.argtypes = args

@@ -1458,7 +1458,7 @@ int dg_cn_tables(dg_handle *h) {
   if (!h->cn_rows) {
     double *rows = (double *)malloc(sizeof(double) * h->nf * 8 * L);
     cn_row_templates(h, rows);
-    DG_CUDA(cudaMalloc((void **)&h->cn_rows, sizeof(double) * h->nf * 8 * L));
+    DG_CUDA(dg_malloc(h, (void **)&h->cn_rows, sizeof(double) * h->nf * 8 * L));
     cudaError_t e = cudaMemcpy(h->cn_rows, rows, sizeof(double) * h->nf * 8 * L, cudaMemcpyHostToDevice);
     free(rows);
     DG_CUDA(e);

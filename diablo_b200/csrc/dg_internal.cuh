@@ -150,6 +150,10 @@ bool dg_mixed_ok(int nx, int nz, int n_th);
 
 void dg_graphs_free(dg_handle *h);
 
+// stream-ordered device allocation of a handle's arrays (on h->st)
+cudaError_t dg_malloc(dg_handle *h, void **p, size_t bytes);
+void dg_free(dg_handle *h, void *p);
+
 // kernel timing: begin before a launch on stream st; the launch accounting
 // after the launch ends it
 void dg_kt_begin(dg_handle *h, const char *name, cudaStream_t st);

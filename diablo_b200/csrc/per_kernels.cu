@@ -438,9 +438,9 @@ int dg_per_init(dg_handle *h) {
   const int np = 6 + 3 * h->NTH;
   const int nmax = np > h->nf ? np : h->nf;
   auto al = [&](double2 **p, size_t n) -> int {
-    cudaError_t e = cudaMalloc((void **)p, n * sizeof(double2));
+    cudaError_t e = dg_malloc(h, (void **)p, n * sizeof(double2));
     if (e != cudaSuccess) {
-      dg_set_error("cudaMalloc failed (periodic work arrays)");
+      dg_set_error("device allocation failed (periodic work arrays)");
       return e == cudaErrorMemoryAllocation ? DG_ERR_OOM : DG_ERR_CUDA;
     }
     return DG_OK;
@@ -455,9 +455,9 @@ int dg_per_init(dg_handle *h) {
   h->work_bytes = sizeof(double) * (size_t)phys_field(h) * nphys;
   if (h->work_bytes < sizeof(double) * 8 * (size_t)h->nkyt)
     h->work_bytes = sizeof(double) * 8 * (size_t)h->nkyt;
-  cudaError_t e = cudaMalloc((void **)&h->work, h->work_bytes);
+  cudaError_t e = dg_malloc(h, (void **)&h->work, h->work_bytes);
   if (e != cudaSuccess) {
-    dg_set_error("cudaMalloc failed (periodic physical scratch)");
+    dg_set_error("device allocation failed (periodic physical scratch)");
     return DG_ERR_OOM;
   }
   return DG_OK;

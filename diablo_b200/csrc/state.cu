@@ -24,12 +24,12 @@ void twiddles(int n, double2 *out) {
 }
 
 template <typename T>
-int dalloc(T **p, size_t count) {
+int dalloc(dg_handle *h, T **p, size_t count) {
   *p = nullptr;
   if (count == 0) count = 1;
-  cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+  cudaError_t e = dg_malloc(h, (void **)p, count * sizeof(T));
   if (e != cudaSuccess) {
-    dg_set_error((std::string("cudaMalloc: ") + cudaGetErrorString(e)).c_str());
+    dg_set_error((std::string("device allocation: ") + cudaGetErrorString(e)).c_str());
     return e == cudaErrorMemoryAllocation ? DG_ERR_OOM : DG_ERR_CUDA;
   }
   return DG_OK;
@@ -61,6 +61,39 @@ __global__ void k_compact_to_ref(const double2 *__restrict__ cmp, double2 *__res
 
 __global__ void k_advance_time(double *dscal) { dscal[0] = dscal[0] + dscal[1]; }
 }  // namespace
+
+// Device memory of a handle comes from the device's default stream-ordered
+// pool (cudaMallocAsync / cudaFreeAsync on the handle's stream).  Freeing a
+// handle then does not synchronise the device, so a process that creates and
+// destroys handles while others run (the ensemble server) does not stall
+// them; the pool keeps freed blocks for reuse (release threshold raised once
+// per device, for this process's pool only).
+cudaError_t dg_malloc(dg_handle *h, void **p, size_t bytes) {
+  static std::mutex mu;
+  static bool raised[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev >= 0 && dev < 64 && !raised[dev]) {
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+      }
+      raised[dev] = true;
+    }
+  }
+  cudaError_t e = cudaMallocAsync(p, bytes, h->st);
+  // complete before the block is touched from another stream or a
+  // synchronous copy
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  return e;
+}
+
+void dg_free(dg_handle *h, void *p) {
+  if (p) cudaFreeAsync(p, h->st);
+}
 
 void dg_set_error(const char *msg) { g_err = msg ? msg : ""; }
 void dg_count_launch(int n) {
@@ -127,6 +160,34 @@ static int validate(const dg_params *p, const double *gy) {
     }
   }
   return DG_OK;
+}
+
+// Device bytes diablo_gpu_init allocates for these parameters (the sum of
+// the allocations below and in dg_per_init), for admission against a budget.
+extern "C" int64_t dg_state_bytes(const dg_params *p) {
+  if (!p || p->nx <= 0 || p->ny <= 0 || p->nz <= 0) return -1;
+  const int64_t nkxp = p->nx / 3 + 1, nkzt = 2 * (p->nz / 3) + 1, nkyt = 2 * (p->ny / 3) + 1;
+  const int64_t nf = 3 + p->n_th, L = p->ny + 2;
+  const bool per = p->num_per_dir == 3;
+  const int64_t planes = per ? nkyt : L;
+  const int64_t ns = nkxp * nkzt * planes;
+  int64_t b = 16 * ns * (3 * nf + 2);                      // cu, cf, rhs, cp, cr1
+  b += 8 * (3 * L + nkxp + nkzt + nkyt) + 16 * (p->nx + p->nz + p->ny) + 8 * 16 + 256;
+  if (!per) {
+    const int64_t hsz = planes * p->nz * nkxp;
+    b += 16 * ns + 8 * 2 * ns;                              // gphi, rem_a, rem_rb
+    b += 8 * 3 * (3 + DG_MAX_TH) * 5 * L + 8 * nf * 8 * L;  // cn_tab, cn_rows
+    b += 16 * hsz * nf + 16 * hsz * 2 * nf;                 // H, G
+    int64_t w = 8 * L * p->nz * p->nx * (nf > 3 ? nf : 3);
+    if (w < 8 * 8 * L) w = 8 * 8 * L;
+    b += w;
+  } else {
+    const int64_t np = 6 + 3 * p->n_th, nmax = np > nf ? np : nf;
+    const int64_t hy = (int64_t)p->ny * nkxp * nkzt, hf = (int64_t)p->ny * p->nz * nkxp;
+    b += 16 * (nmax * hy + nf * hf + nmax * hf + np * nkyt * nkxp * nkzt);
+    b += 8 * (int64_t)p->ny * p->nz * p->nx * (nf + np > 6 ? nf + np : 6);
+  }
+  return b;
 }
 
 extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *stream,
@@ -218,12 +279,12 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
   }
 
   // ---- device allocations
-  DG_TRY(dalloc(&h->gyf, L));
-  DG_TRY(dalloc(&h->dy, L));
-  DG_TRY(dalloc(&h->dyf, L));
-  DG_TRY(dalloc(&h->kx, h->nkxp));
-  DG_TRY(dalloc(&h->kz, h->nkzt));
-  DG_TRY(dalloc(&h->ky, h->nkyt));
+  DG_TRY(dalloc(h, &h->gyf, L));
+  DG_TRY(dalloc(h, &h->dy, L));
+  DG_TRY(dalloc(h, &h->dyf, L));
+  DG_TRY(dalloc(h, &h->kx, h->nkxp));
+  DG_TRY(dalloc(h, &h->kz, h->nkzt));
+  DG_TRY(dalloc(h, &h->ky, h->nkyt));
   DG_CUDA(cudaMemcpy(h->gyf, h->h_gyf, sizeof(double) * L, cudaMemcpyHostToDevice));
   DG_CUDA(cudaMemcpy(h->dy, h->h_dy, sizeof(double) * L, cudaMemcpyHostToDevice));
   DG_CUDA(cudaMemcpy(h->dyf, h->h_dyf, sizeof(double) * L, cudaMemcpyHostToDevice));
@@ -238,10 +299,10 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
     int nmax = h->NX > h->NZ ? h->NX : h->NZ;
     if (h->NY > nmax) nmax = h->NY;
     double2 *tmp = (double2 *)malloc(sizeof(double2) * nmax);
-    DG_TRY(dalloc(&h->twx, h->NX));
+    DG_TRY(dalloc(h, &h->twx, h->NX));
     twiddles(h->NX, tmp);
     DG_CUDA(cudaMemcpy(h->twx, tmp, sizeof(double2) * h->NX, cudaMemcpyHostToDevice));
-    DG_TRY(dalloc(&h->twz, h->NZ));
+    DG_TRY(dalloc(h, &h->twz, h->NZ));
     twiddles(h->NZ, tmp);
     DG_CUDA(cudaMemcpy(h->twz, tmp, sizeof(double2) * h->NZ, cudaMemcpyHostToDevice));
     if (p->precision == 1) {
@@ -249,51 +310,51 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
       float2 *tf = (float2 *)malloc(sizeof(float2) * nmax);
       twiddles(h->NX, tmp);
       for (int m = 0; m < h->NX; m++) tf[m] = make_float2((float)tmp[m].x, (float)tmp[m].y);
-      DG_CUDA(cudaMalloc((void **)&h->twx_f, sizeof(float2) * h->NX));
+      DG_CUDA(dg_malloc(h, (void **)&h->twx_f, sizeof(float2) * h->NX));
       DG_CUDA(cudaMemcpy(h->twx_f, tf, sizeof(float2) * h->NX, cudaMemcpyHostToDevice));
       twiddles(h->NZ, tmp);
       for (int m = 0; m < h->NZ; m++) tf[m] = make_float2((float)tmp[m].x, (float)tmp[m].y);
-      DG_CUDA(cudaMalloc((void **)&h->twz_f, sizeof(float2) * h->NZ));
+      DG_CUDA(dg_malloc(h, (void **)&h->twz_f, sizeof(float2) * h->NZ));
       DG_CUDA(cudaMemcpy(h->twz_f, tf, sizeof(float2) * h->NZ, cudaMemcpyHostToDevice));
       free(tf);
     }
     if (h->periodic) {
-      DG_TRY(dalloc(&h->twy, h->NY));
+      DG_TRY(dalloc(h, &h->twy, h->NY));
       twiddles(h->NY, tmp);
       DG_CUDA(cudaMemcpy(h->twy, tmp, sizeof(double2) * h->NY, cudaMemcpyHostToDevice));
     }
     free(tmp);
   }
 
-  DG_TRY(dalloc(&h->dscal, 16));
-  DG_TRY(dalloc(&h->dmin_bits, 32));
-  DG_TRY(dalloc(&h->dflag, 4));
+  DG_TRY(dalloc(h, &h->dscal, 16));
+  DG_TRY(dalloc(h, &h->dmin_bits, 32));
+  DG_TRY(dalloc(h, &h->dflag, 4));
   const size_t ns = (size_t)h->nspec;
   for (int f = 0; f < h->nf; f++) {
-    DG_TRY(dalloc(&h->cu[f], ns));
-    DG_TRY(dalloc(&h->cf[f], ns));
-    DG_TRY(dalloc(&h->rhs[f], ns));
+    DG_TRY(dalloc(h, &h->cu[f], ns));
+    DG_TRY(dalloc(h, &h->cf[f], ns));
+    DG_TRY(dalloc(h, &h->rhs[f], ns));
     DG_CUDA(cudaMemset(h->cu[f], 0, ns * sizeof(double2)));
     DG_CUDA(cudaMemset(h->cf[f], 0, ns * sizeof(double2)));
     DG_CUDA(cudaMemset(h->rhs[f], 0, ns * sizeof(double2)));
   }
-  DG_TRY(dalloc(&h->cp, ns));
-  DG_TRY(dalloc(&h->cr1, ns));
+  DG_TRY(dalloc(h, &h->cp, ns));
+  DG_TRY(dalloc(h, &h->cr1, ns));
   DG_CUDA(cudaMemset(h->cp, 0, ns * sizeof(double2)));
   DG_CUDA(cudaMemset(h->cr1, 0, ns * sizeof(double2)));
 
   if (!h->periodic) {
-    DG_TRY(dalloc(&h->gphi, ns));
-    DG_TRY(dalloc(&h->rem_a, ns));
-    DG_TRY(dalloc(&h->rem_rb, ns));
-    DG_TRY(dalloc(&h->cn_tab, (size_t)3 * (3 + DG_MAX_TH) * 5 * L));
+    DG_TRY(dalloc(h, &h->gphi, ns));
+    DG_TRY(dalloc(h, &h->rem_a, ns));
+    DG_TRY(dalloc(h, &h->rem_rb, ns));
+    DG_TRY(dalloc(h, &h->cn_tab, (size_t)3 * (3 + DG_MAX_TH) * 5 * L));
     const size_t hsz = (size_t)h->nplanes * h->NZ * h->nkxp;
-    DG_TRY(dalloc(&h->H, hsz * h->nf));
-    DG_TRY(dalloc(&h->G, hsz * 2 * h->nf));
+    DG_TRY(dalloc(h, &h->H, hsz * h->nf));
+    DG_TRY(dalloc(h, &h->G, hsz * 2 * h->nf));
     const size_t phys = (size_t)(NY + 2) * h->NZ * h->NX;
     h->work_bytes = sizeof(double) * phys * (h->nf > 3 ? h->nf : 3);
     if (h->work_bytes < sizeof(double) * 8 * L) h->work_bytes = sizeof(double) * 8 * L;
-    DG_TRY(dalloc((double **)&h->work, h->work_bytes / sizeof(double)));
+    DG_TRY(dalloc(h, (double **)&h->work, h->work_bytes / sizeof(double)));
   } else {
     DG_TRY(dg_per_init(h));
   }
@@ -306,15 +367,15 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
 extern "C" int diablo_gpu_finalize(dg_handle *h) {
   if (!h) return DG_OK;
   cudaStreamSynchronize(h->st);
+  cudaStreamSynchronize(h->st2);
   void *dp[] = {h->gyf, h->dy, h->dyf, h->kx, h->kz, h->ky, h->kx2, h->kz2, h->ky2, h->twx, h->twz,
                 h->twy, h->twx_f, h->twz_f, h->dscal, h->cp, h->cr1, h->gphi, h->rem_a, h->rem_rb, h->cn_tab, h->cn_rows, h->H, h->G, h->work, h->dmin_bits, h->dflag, h->Hy, h->P,
                 h->Q};
-  for (void *q : dp)
-    if (q) cudaFree(q);
+  for (void *q : dp) dg_free(h, q);
   for (int f = 0; f < 3 + DG_MAX_TH; f++) {
-    if (h->cu[f]) cudaFree(h->cu[f]);
-    if (h->cf[f]) cudaFree(h->cf[f]);
-    if (h->rhs[f]) cudaFree(h->rhs[f]);
+    dg_free(h, h->cu[f]);
+    dg_free(h, h->cf[f]);
+    dg_free(h, h->rhs[f]);
   }
   cudaStreamSynchronize(h->st2);
   dg_kt_free(h);

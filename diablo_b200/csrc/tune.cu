@@ -82,7 +82,7 @@ int save_state(dg_handle *h, Saved *sv) {
   const size_t bytes = sizeof(double2) * h->nspec;
   auto keep = [&](const double2 *src) -> int {
     double2 *d = nullptr;
-    DG_CUDA(cudaMalloc((void **)&d, bytes));
+    DG_CUDA(dg_malloc(h, (void **)&d, bytes));
     sv->bufs.push_back(d);
     DG_CUDA(cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToDevice, h->st));
     return DG_OK;
@@ -110,8 +110,8 @@ int restore_state(dg_handle *h, Saved *sv) {
   return DG_OK;
 }
 
-void free_saved(Saved *sv) {
-  for (double2 *p : sv->bufs) cudaFree(p);
+void free_saved(dg_handle *h, Saved *sv) {
+  for (double2 *p : sv->bufs) dg_free(h, p);
   sv->bufs.clear();
 }
 
@@ -144,7 +144,7 @@ extern "C" int dg_autotune(dg_handle *h, int steps_per_trial) {
   Saved sv;
   int s = save_state(h, &sv);
   if (s != DG_OK) {
-    free_saved(&sv);
+    free_saved(h, &sv);
     return s;
   }
   struct Knob {
@@ -176,7 +176,7 @@ extern "C" int dg_autotune(dg_handle *h, int steps_per_trial) {
     dg_tune_set(h, k.key, best);
   }
   const int r = restore_state(h, &sv);
-  free_saved(&sv);
+  free_saved(h, &sv);
   DG_TRY(s);
   DG_TRY(r);
   // the tables of the restored DELTA_T

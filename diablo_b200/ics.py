@@ -16,7 +16,8 @@ import numpy as np
 from .grid import grid_metrics
 from .params import Params
 
-__all__ = ["kh_shear_layer", "channel_laminar", "periodic_spectrum", "ensemble_kh_params"]
+__all__ = ["kh_shear_layer", "channel_laminar", "periodic_spectrum", "ensemble_kh_params",
+           "to_spectral_chan", "kh_state"]
 
 
 def _noise(rng, shape, kind, amp):
@@ -112,3 +113,26 @@ def ensemble_kh_params(rng: np.random.Generator, base: Params):
     q.ri = list(q.ri)
     q.ri[0] = ri
     return q
+
+
+def to_spectral_chan(phys: np.ndarray, p: Params) -> np.ndarray:
+    """FFT_XZ_TO_FOURIER of physical planes [NY+2][NZ][NX] on the host with
+    numpy (the packing and scaling of for/mpi.f:1530-1611): retained modes
+    [NY+2][TNKZ+1][NKX+1].  For preparing initial states off the GPU."""
+    t = np.fft.fft(np.fft.rfft(phys, axis=2)[:, :, : p.nkx + 1] / p.nx, axis=1) / p.nz
+    out = np.zeros((phys.shape[0], 2 * p.nkz + 1, p.nkx + 1), dtype=np.complex128)
+    out[:, : p.nkz + 1] = t[:, : p.nkz + 1]
+    out[:, p.nkz + 1:] = t[:, p.nz - p.nkz:]
+    return out
+
+
+def kh_state(p: Params, gy: np.ndarray, seed: int = 1, kick: float = 1e-3) -> dict:
+    """Spectral KH initial state (CU1..3, CP = 0, CTHn) for the ensemble
+    server; the server's prepare step applies the BCs and REM_DIV_CHAN."""
+    u1, u2, u3, th = kh_shear_layer(p, gy, seed=seed, kick=kick)
+    st = {"CU1": to_spectral_chan(u1, p), "CU2": to_spectral_chan(u2, p),
+          "CU3": to_spectral_chan(u3, p),
+          "CP": np.zeros((p.ny + 2, 2 * p.nkz + 1, p.nkx + 1), dtype=np.complex128)}
+    for n in range(p.n_th):
+        st[f"CTH{n}"] = to_spectral_chan(th[n], p)
+    return st

@@ -209,6 +209,36 @@ int dg_autotune(dg_handle *h, int steps_per_trial);
 int diablo_fft_xz_to_fourier_noalloc(const double *V, double *VV, int nx, int nz, int ny,
                                      int jmin, int jmax, void *stream);
 
+/* ------------------------------------------------------- ensemble server */
+/* No counterpart in the reference (it runs one case per job).  Continuous
+ * batching of independent channel solves on one GPU: requests are admitted
+ * while fewer than max_active cases run and their device bytes
+ * (dg_state_bytes) fit hbm_budget_gb (0 = no budget); each active case has
+ * its own handle and stream and advances by replayed step graphs, so steps
+ * of different cases overlap on the device; launch shapes are autotuned once
+ * per grid shape when autotune != 0.  A request's state is the compact
+ * spectral CU1, CU2, CU3, CP, CTH(0..N_TH-1), each
+ * [NY+2][TNKZ+1][NKX+1] complex; prepare != 0 applies APPLY_BC_VEL,
+ * REM_DIV_CHAN, APPLY_BC_VEL on admission (the tail of CREATE_FLOW_CHAN).
+ * dg_server_wait blocks until the request is done, copies its final state
+ * into `state` (same layout) and, if times != NULL, stores the seconds spent
+ * queued and on the device. */
+typedef struct dg_server dg_server;
+typedef struct dg_server_stats {
+  int64_t cases_done, steps_done;
+  int32_t active, queued;
+  int64_t bytes_active, bytes_peak;
+  double step_ms_p50, step_ms_p99;   /* device time of one RK3 step of a case */
+  double cases_per_s, mpoint_steps_per_s, wall_s;  /* first submit .. last completion */
+} dg_server_stats;
+int64_t dg_state_bytes(const dg_params *p);
+int dg_server_create(int max_active, double hbm_budget_gb, int autotune, dg_server **out);
+int dg_server_submit(dg_server *s, const dg_params *p, const double *gy,
+                     const double *const *state, int nsteps, int prepare, int64_t *id);
+int dg_server_wait(dg_server *s, int64_t id, double *const *state, double *times);
+int dg_server_query(dg_server *s, dg_server_stats *st);
+int dg_server_destroy(dg_server *s);
+
 /* ------------------------------------------------------------ statistics */
 /* Parity statistics of the current state (channel or periodic); also checks
  * the state for non-finite values (returns DG_ERR_NAN if any). */

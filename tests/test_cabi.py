@@ -60,3 +60,12 @@ def test_mixed_precision_refuses_unsupported_sizes():
     code = L.diablo_gpu_init(ctypes.byref(q.replace(precision=1).to_struct(DgParams)), None, None,
                              ctypes.byref(h))
     assert code == 1
+
+
+def test_state_bytes_estimate():
+    from diablo_b200.serve import state_bytes
+    p, _ = configs.channel_re180()
+    b = state_bytes(p)
+    m = 43 * 85 * 131 * 16                     # one retained-mode FP64 field
+    assert 12 * m < b < 60 * m                  # state, work arrays, H and G planes
+    assert state_bytes(p.replace(nx=64)) < b

@@ -166,3 +166,14 @@ def test_kh_oracle_runs_and_conserves_structure():
     s1 = o.stats()
     assert np.isfinite(s1["ke"]) and abs(s1["ke"] - s0["ke"]) < 1e-3 * s0["ke"]
     assert s1["div_max"] < 1e-12
+
+
+def test_host_spectral_ic_matches_oracle_transform():
+    """ics.to_spectral_chan (numpy, for preparing server requests) equals the
+    oracle's FFT_XZ_TO_FOURIER."""
+    p, gy = configs.kh_shear_layer(nx=32, ny=17, nz=16)
+    o = O.Oracle(p, gy)
+    rng = np.random.default_rng(12)
+    phys = rng.standard_normal(p.phys_shape())
+    np.testing.assert_allclose(ics.to_spectral_chan(phys, p), o.to_fourier(phys), rtol=0,
+                               atol=1e-15)

@@ -38,6 +38,16 @@ struct ChanConst {
   double ri[DG_MAX_TH], pr[DG_MAX_TH], drhodx[DG_MAX_TH], drhodz[DG_MAX_TH];
 };
 
+// uniform selects from the parameter arrays (a run-time index into a kernel
+// parameter array would copy the array to local memory)
+template <typename T>
+__device__ __forceinline__ T sel(const T (&a)[DG_MAX_TH], int i) {
+  T r = a[0];
+#pragma unroll
+  for (int k = 1; k < DG_MAX_TH; k++) r = (i == k) ? a[k] : r;
+  return r;
+}
+
 ChanConst make_const(const dg_handle *h) {
   ChanConst c;
   c.NX = h->NX; c.NY = h->NY; c.NZ = h->NZ; c.NKX = h->NKX; c.NKZ = h->NKZ;
@@ -257,7 +267,7 @@ __host__ __device__ constexpr bool xw_supported(int n) {
 }
 
 template <int NX, int NTH, typename CX = double2>
-__global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? 3 : 2) k_xrow_w(
+__global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? (sizeof(CX) == 8 ? 4 : 3) : 2) k_xrow_w(
     ChanConst C, const CX *__restrict__ H, long Hfield, int chunk, int jbase, int jtop,
     const CX *__restrict__ tw, const double *__restrict__ dyf, const double *__restrict__ dy,
     const double *__restrict__ kxv, CX *__restrict__ G, long Gfield) {
@@ -444,6 +454,7 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? 3 : 2) k_xrow_w(
     wpasses<NX, -1, 0>(buf, NPP, SSTR, stw, lane);
     const bool out = (j >= j0);
     const T d2 = (T)2 * dyf_j, dyj = dy[j];
+    const T id2 = (T)1 / d2, idyj = (T)1 / dyj;  // per plane: multiply in the row loop
 #pragma unroll
     for (int s = 0; s < KS; s++) {
       const int k = lane + 32 * s;
@@ -470,22 +481,22 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? 3 : 2) k_xrow_w(
         // U1: A = U1U3, B = -ikx U1U1 - (fl1(j+1) - fl1(j)) / (2 DYF(j))
         G[0 * Gfield + off] = x0;
         CX t = mikx(x1);
-        G[1 * Gfield + off] = CT<CX>::mk(t.x - (x4.x - PV(0, s).x) / d2, t.y - (x4.y - PV(0, s).y) / d2);
+        G[1 * Gfield + off] = CT<CX>::mk(t.x - (x4.x - PV(0, s).x) * id2, t.y - (x4.y - PV(0, s).y) * id2);
         // U2 (GY j): A = ubar3 u2(j), B = -ikx ubar1 u2(j) - (g(j) - g(j-1)) / DY(j)
         G[2 * Gfield + off] = PV(3, s);
         t = mikx(PV(2, s));
-        G[3 * Gfield + off] = CT<CX>::mk(t.x - (x3.x - PV(4, s).x) / dyj, t.y - (x3.y - PV(4, s).y) / dyj);
+        G[3 * Gfield + off] = CT<CX>::mk(t.x - (x3.x - PV(4, s).x) * idyj, t.y - (x3.y - PV(4, s).y) * idyj);
         // U3: A = U3U3, B = -ikx U1U3 - (fl3(j+1) - fl3(j)) / (2 DYF(j))
         G[4 * Gfield + off] = x2;
         t = mikx(x0);
-        G[5 * Gfield + off] = CT<CX>::mk(t.x - (x5.x - PV(1, s).x) / d2, t.y - (x5.y - PV(1, s).y) / d2);
+        G[5 * Gfield + off] = CT<CX>::mk(t.x - (x5.x - PV(1, s).x) * id2, t.y - (x5.y - PV(1, s).y) * id2);
 #pragma unroll
         for (int n = 0; n < NTH; n++) {
           const CX a = X(8 + 3 * n), b = X(9 + 3 * n), c = X(10 + 3 * n);
           G[(6 + 2 * n) * Gfield + off] = b;
           t = mikx(a);
           G[(7 + 2 * n) * Gfield + off] =
-              CT<CX>::mk(t.x - (c.x - PV(5 + n, s).x) / d2, t.y - (c.y - PV(5 + n, s).y) / d2);
+              CT<CX>::mk(t.x - (c.x - PV(5 + n, s).x) * id2, t.y - (c.y - PV(5 + n, s).y) * id2);
         }
       }
       PV(0, s) = x4;
@@ -683,7 +694,7 @@ __global__ void __launch_bounds__(ZF_THR) k_zfwd_rhs(
 constexpr int ZW_KXG = 8;
 
 template <int NZ, typename CX = double2>
-__global__ void __launch_bounds__(128, 4) k_zfwd_w(
+__global__ void __launch_bounds__(128, sizeof(CX) == 16 ? 6 : 5) k_zfwd_w(
     ChanConst C, const CX *__restrict__ G, long Gfield, const CX *__restrict__ tw,
     const double *__restrict__ dscal, int rk_step, const double *__restrict__ kxv,
     const double *__restrict__ kzv, const double *__restrict__ dy, const double *__restrict__ dyf,
@@ -699,8 +710,8 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
   const int f = blockIdx.z;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // skip planes outside this field's rows
-  const int jlo = (f == 0 || f == 2) ? C.JS : (f == 1 ? 2 : C.JSt[f - 3]);
-  const int jhi = (f == 0 || f == 2) ? C.JE : (f == 1 ? C.NY : C.JEt[f - 3]);
+  const int jlo = (f == 0 || f == 2) ? C.JS : (f == 1 ? 2 : sel(C.JSt, f - 3));
+  const int jhi = (f == 0 || f == 2) ? C.JE : (f == 1 ? C.NY : sel(C.JEt, f - 3));
   if (j < jlo || j > jhi) return;
   for (int i = threadIdx.x; i < NZ; i += blockDim.x) stw[i] = tw[i];
   const CX *GA = G + (2 * f) * Gfield + (long)j * NZ * nkxp;
@@ -726,6 +737,7 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
   __syncthreads();
   CX *wb = buf + warp * 4 * SSTR;
   wpasses<NZ, -1, 0>(wb, 4, SSTR, stw, lane);
+  __syncthreads();  // the epilogue below reads every warp's columns
 
   const double h = dscal[1 + rk_step];
   const double time = dscal[0];
@@ -735,16 +747,26 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
   const double NU = C.nu, NUV = C.nuv;
   const long ss = C.ss;
   const double dyj = dy[j], dyj1 = dy[j + 1], dyfj = dyf[j], dyfm = dyf[j - 1];
-  const double rnz = (double)NZ;
-  for (int it = lane; it < 2 * nkzt; it += 32) {
-    const int cc = it & 1, kp = it >> 1;
-    const int kx = kx0 + 2 * warp + cc;
+  // per-plane coefficients: the epilogue multiplies instead of dividing (FP64
+  // division is a long instruction sequence on the FP64 pipe)
+  const double inz = 1.0 / (double)NZ;
+  const double aaU = T1 * NUV;
+  const double cup = aaU / (dyj1 * dyfj), cdn = aaU / (dyj * dyfj);         // GYF rows
+  const double cup2 = aaU / (dyfj * dyj), cdn2 = aaU / (dyfm * dyj);        // GY rows (U2)
+  const double idy = 1.0 / dyj, bw2 = 1.0 / (2.0 * dyj);
+  // all 128 threads over the CTA's (kz, kx) modes, kx fastest: consecutive
+  // threads touch consecutive modes of a kz row
+  for (int it = threadIdx.x; it < ZW_KXG * nkzt; it += 128) {
+    const int c = it % ZW_KXG, kp = it / ZW_KXG;
+    const int kx = kx0 + c;
     if (kx >= nkxp) continue;
     const int z = (kp <= NKZ) ? kp : (NZ - 1 + (kp - NKZ) - NKZ);
     // the transform's working precision ends here: everything below is FP64
-    const CX aw = wb[(0 + cc) * SSTR + pad(z)], bw = wb[(2 + cc) * SSTR + pad(z)];
-    const double2 a = make_double2((double)aw.x / rnz, (double)aw.y / rnz);
-    const double2 b = make_double2((double)bw.x / rnz, (double)bw.y / rnz);
+    const CX *cb = buf + (c >> 1) * 4 * SSTR;
+    const int cc = c & 1;
+    const CX aw = cb[(0 + cc) * SSTR + pad(z)], bw = cb[(2 + cc) * SSTR + pad(z)];
+    const double2 a = make_double2((double)aw.x * inz, (double)aw.y * inz);
+    const double2 b = make_double2((double)bw.x * inz, (double)bw.y * inz);
     const double KX = kxv[kx], KZ = kzv[kp];
     const double2 nlv = make_double2(KZ * a.y + b.x, -KZ * a.x + b.y);  // -i kz A + B
     const long o = (long)j * ss + (long)kp * nkxp + kx;
@@ -753,13 +775,16 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
     const bool mean = (kx == 0 && kp == 0);
     if (f == 0 || f == 2) {
       // U1 / U3 (rows JSTART..JEND)
-      const double2 u = cu(f)[o], um = cu(f)[o - ss], up = cu(f)[o + ss];
-      const double2 uo = cu(2 - f)[o];  // the other horizontal component (Coriolis)
+      const double2 u = __ldg(cu(f) + (o)), um = __ldg(cu(f) + (o - ss)), up = __ldg(cu(f) + (o + ss));
+      // the other horizontal component (Coriolis), only with rotation
+      const double2 uo = (C.i_ro != 0.0) ? __ldg(cu(2 - f) + (o)) : make_double2(0.0, 0.0);
       const double sgn = (f == 0) ? 1.0 : -1.0;
       const double gr = (f == 0) ? C.grav_x : C.grav_z;
       double2 fv = make_double2(-NU * kk * u.x + sgn * C.i_ro * uo.x, -NU * kk * u.y + sgn * C.i_ro * uo.y);
-      for (int n = 0; n < C.nth; n++) {
-        const double2 t = cu(3 + n)[o];
+#pragma unroll
+      for (int n = 0; n < DG_MAX_TH; n++) {
+        if (n >= C.nth) break;
+        const double2 t = __ldg(cu(3 + n) + (o));
         fv.x += C.ri[n] * gr * t.x;
         fv.y += C.ri[n] * gr * t.y;
       }
@@ -767,11 +792,11 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
       fv.y += nlv.y;
       double2 r = u;
       if (rk_step > 1) {
-        const double2 old = cf(f)[o];
+        const double2 old = __ldg(cf(f) + o);
         r.x += T3 * old.x;
         r.y += T3 * old.y;
       }
-      const double2 p0 = cp[o];
+      const double2 p0 = __ldg(cp + o);
       const double K = (f == 0) ? KX : KZ;
       r.x -= T4 * (-K * p0.y);
       r.y -= T4 * (K * p0.x);
@@ -781,65 +806,65 @@ __global__ void __launch_bounds__(128, 4) k_zfwd_w(
       }
       r.x += T5 * fv.x;
       r.y += T5 * fv.y;
-      const double aa = T1 * NUV;
-      r.x += aa * (((up.x - u.x) / dyj1 - (u.x - um.x) / dyj) / dyfj);
-      r.y += aa * (((up.y - u.y) / dyj1 - (u.y - um.y) / dyj) / dyfj);
+      r.x += cup * (up.x - u.x) - cdn * (u.x - um.x);
+      r.y += cup * (up.y - u.y) - cdn * (u.y - um.y);
       cf(f)[o] = fv;
       rhs(f)[o] = r;
     } else if (f == 1) {
       // U2 (rows 2..NY)
-      const double2 u = cu(1)[o], um = cu(1)[o - ss], up = cu(1)[o + ss];
+      const double2 u = __ldg(cu(1) + (o)), um = __ldg(cu(1) + (o - ss)), up = __ldg(cu(1) + (o + ss));
       double2 fv = make_double2(-NU * kk * u.x, -NU * kk * u.y);
       if (!mean) {
-        for (int n = 0; n < C.nth; n++) {
-          const double2 t = cu(3 + n)[o], tm = cu(3 + n)[o - ss];
-          const double w = C.ri[n] * C.grav_y;
-          fv.x += w * (t.x * dyfm + tm.x * dyfj) / (2.0 * dyj);
-          fv.y += w * (t.y * dyfm + tm.y * dyfj) / (2.0 * dyj);
+#pragma unroll
+        for (int n = 0; n < DG_MAX_TH; n++) {
+          if (n >= C.nth) break;
+          const double2 t = __ldg(cu(3 + n) + (o)), tm = __ldg(cu(3 + n) + (o - ss));
+          const double w = C.ri[n] * C.grav_y * bw2;
+          fv.x += w * (t.x * dyfm + tm.x * dyfj);
+          fv.y += w * (t.y * dyfm + tm.y * dyfj);
         }
       }
       fv.x += nlv.x;
       fv.y += nlv.y;
       double2 r = u;
       if (rk_step > 1) {
-        const double2 old = cf(1)[o];
+        const double2 old = __ldg(cf(1) + o);
         r.x += T3 * old.x;
         r.y += T3 * old.y;
       }
-      const double2 p0 = cp[o], pm = cp[o - ss];
-      r.x -= T4 * ((p0.x - pm.x) / dyj);
-      r.y -= T4 * ((p0.y - pm.y) / dyj);
+      const double2 p0 = __ldg(cp + o), pm = __ldg(cp + (o - ss));
+      r.x -= T4 * ((p0.x - pm.x) * idy);
+      r.y -= T4 * ((p0.y - pm.y) * idy);
       r.x += T5 * fv.x;
       r.y += T5 * fv.y;
-      const double aa = T1 * NUV;
-      r.x += aa * (((up.x - u.x) / dyfj - (u.x - um.x) / dyfm) / dyj);
-      r.y += aa * (((up.y - u.y) / dyfj - (u.y - um.y) / dyfm) / dyj);
+      r.x += cup2 * (up.x - u.x) - cdn2 * (u.x - um.x);
+      r.y += cup2 * (up.y - u.y) - cdn2 * (u.y - um.y);
       cf(1)[o] = fv;
       rhs(1)[o] = r;
     } else {
       // scalar n (rows JSTART_TH..JEND_TH)
       const int n = f - 3;
-      const double2 t = cu(f)[o], tm = cu(f)[o - ss], tp = cu(f)[o + ss];
-      const double nup = NU / C.pr[n];
+      const double2 t = __ldg(cu(f) + (o)), tm = __ldg(cu(f) + (o - ss)), tp = __ldg(cu(f) + (o + ss));
+      const double nup = NU / sel(C.pr, n);  // once per item: scalar fields only
       double2 fv = make_double2(-nup * kk * t.x, -nup * kk * t.y);
-      if (C.drhodx[n] != 0.0 || C.drhodz[n] != 0.0) {
-        const double2 u1 = cu(0)[o], u3 = cu(2)[o];
-        fv.x = fv.x - u1.x * C.drhodx[n] - u3.x * C.drhodz[n];
-        fv.y = fv.y - u1.y * C.drhodx[n] - u3.y * C.drhodz[n];
+      if (sel(C.drhodx, n) != 0.0 || sel(C.drhodz, n) != 0.0) {
+        const double2 u1 = __ldg(cu(0) + (o)), u3 = __ldg(cu(2) + (o));
+        fv.x = fv.x - u1.x * sel(C.drhodx, n) - u3.x * sel(C.drhodz, n);
+        fv.y = fv.y - u1.y * sel(C.drhodx, n) - u3.y * sel(C.drhodz, n);
       }
       fv.x += nlv.x;
       fv.y += nlv.y;
       double2 r = t;
       if (rk_step > 1) {
-        const double2 old = cf(f)[o];
+        const double2 old = __ldg(cf(f) + o);
         r.x += T3 * old.x;
         r.y += T3 * old.y;
       }
       r.x += T5 * fv.x;
       r.y += T5 * fv.y;
-      const double aa = (T1 / C.pr[n]) * NUV;
-      r.x += aa * (((tp.x - t.x) / dyj1 - (t.x - tm.x) / dyj) / dyfj);
-      r.y += aa * (((tp.y - t.y) / dyj1 - (t.y - tm.y) / dyj) / dyfj);
+      const double ipr = 1.0 / sel(C.pr, n);
+      r.x += ipr * (cup * (tp.x - t.x) - cdn * (t.x - tm.x));
+      r.y += ipr * (cup * (tp.y - t.y) - cdn * (t.y - tm.y));
       cf(f)[o] = fv;
       rhs(f)[o] = r;
     }

@@ -149,27 +149,34 @@ __global__ void __launch_bounds__(NTHR) k_xc2r(const double2 *__restrict__ H, lo
   const double2 *in = H + f * Hfield + (long)j * NZ * nkxp;
   const int NKX = nkxp - 1;
   for (int i = tid; i < NX; i += nthr) stw[i] = tw[i];
-  for (int idx = tid; idx < RPAIR * NX; idx += nthr) {
-    const int q = idx / NX, k = idx % NX;
-    const int za = z0 + 2 * q, zb = za + 1;
-    double2 v = make_double2(0.0, 0.0);
-    if (za < NZ) {
-      // bin k of Z = A + iB with Hermitian extension of A and B
+  // bin k of Z = A + iB with the Hermitian extension of A and B (A_k + i B_k
+  // for k <= NX/2, conj(A_k) + i conj(B_k) above); loads four bins at a time
+  for (int base = 0; base < RPAIR * NX; base += 4 * nthr) {
+    double2 av[4], bv[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int idx = base + u * nthr + tid;
+      const int q = idx / NX, k = idx % NX;
+      const int za = z0 + 2 * q, zb = za + 1;
       const int kk = (k <= NX / 2) ? k : NX - k;
-      if (kk <= NKX && kk < NX / 2) {
-        double2 a = in[(long)za * nkxp + kk];
-        double2 b = (zb < NZ) ? in[(long)zb * nkxp + kk] : make_double2(0.0, 0.0);
-        if (kk == 0) {
-          a.y = 0.0;
-          b.y = 0.0;
-        }
-        if (k == kk)  // A_k + i B_k
-          v = make_double2(a.x - b.y, a.y + b.x);
-        else          // conj(A_k) + i conj(B_k)
-          v = make_double2(a.x + b.y, -a.y + b.x);
-      }
+      const bool ok = idx < RPAIR * NX && za < NZ && kk <= NKX && kk < NX / 2;
+      av[u] = ok ? in[(long)za * nkxp + kk] : make_double2(0.0, 0.0);
+      bv[u] = (ok && zb < NZ) ? in[(long)zb * nkxp + kk] : make_double2(0.0, 0.0);
     }
-    b0[q * sstr + pad(k)] = v;
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int idx = base + u * nthr + tid;
+      if (idx >= RPAIR * NX) continue;
+      const int q = idx / NX, k = idx % NX;
+      const int kk = (k <= NX / 2) ? k : NX - k;
+      double2 a = av[u], b = bv[u];
+      if (kk == 0) {
+        a.y = 0.0;
+        b.y = 0.0;
+      }
+      b0[q * sstr + pad(k)] =
+          (k == kk) ? make_double2(a.x - b.y, a.y + b.x) : make_double2(a.x + b.y, -a.y + b.x);
+    }
   }
   __syncthreads();
   double2 *res = fft_cta<NT>(b0, b1, pl, RPAIR, sstr, stw, +1);
@@ -207,37 +214,53 @@ __global__ void __launch_bounds__(NTHR) k_xc2r_cfl(const double2 *__restrict__ H
   const double2 *in = H + f * Hfield + (long)j * NZ * nkxp;
   const int NKX = nkxp - 1;
   for (int i = tid; i < NX; i += nthr) stw[i] = tw[i];
-  for (int idx = tid; idx < RPAIR * NX; idx += nthr) {
-    const int q = idx / NX, k = idx % NX;
-    const int za = z0 + 2 * q, zb = za + 1;
-    double2 v = make_double2(0.0, 0.0);
-    if (za < NZ) {
+  // bin k of Z = A + iB with the Hermitian extension of A and B; the row-pair
+  // loads are issued four bins at a time per thread
+  for (int base = 0; base < RPAIR * NX; base += 4 * nthr) {
+    double2 av[4], bv[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int idx = base + u * nthr + tid;
+      const int q = idx / NX, k = idx % NX;
+      const int za = z0 + 2 * q, zb = za + 1;
       const int kk = (k <= NX / 2) ? k : NX - k;
-      if (kk <= NKX && kk < NX / 2) {
-        double2 a = in[(long)za * nkxp + kk];
-        double2 b = (zb < NZ) ? in[(long)zb * nkxp + kk] : make_double2(0.0, 0.0);
-        if (kk == 0) {
-          a.y = 0.0;
-          b.y = 0.0;
-        }
-        v = (k == kk) ? make_double2(a.x - b.y, a.y + b.x) : make_double2(a.x + b.y, -a.y + b.x);
-      }
+      const bool ok = idx < RPAIR * NX && za < NZ && kk <= NKX && kk < NX / 2;
+      av[u] = ok ? in[(long)za * nkxp + kk] : make_double2(0.0, 0.0);
+      bv[u] = (ok && zb < NZ) ? in[(long)zb * nkxp + kk] : make_double2(0.0, 0.0);
     }
-    b0[q * sstr + pad(k)] = v;
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int idx = base + u * nthr + tid;
+      if (idx >= RPAIR * NX) continue;
+      const int q = idx / NX, k = idx % NX;
+      const int kk = (k <= NX / 2) ? k : NX - k;
+      double2 a = av[u], b = bv[u];
+      if (kk == 0) {
+        a.y = 0.0;
+        b.y = 0.0;
+      }
+      b0[q * sstr + pad(k)] =
+          (k == kk) ? make_double2(a.x - b.y, a.y + b.x) : make_double2(a.x + b.y, -a.y + b.x);
+    }
   }
   __syncthreads();
   double2 *res = fft_cta<NT>(b0, b1, pl, RPAIR, sstr, stw, +1);
   const double d = (f == 0) ? dxv : (f == 1 ? dy[j] : dzv);
-  double best = __longlong_as_double(0x7ff0000000000000LL);
+  // min over points of CFL d / |u| is CFL d / max |u| (division is correctly
+  // rounded and monotone), so only the largest |u| of the CTA is divided
+  double big = 0.0;
   for (int idx = tid; idx < RPAIR * NX; idx += nthr) {
     const int q = idx / NX, x = idx % NX;
     const int za = z0 + 2 * q, zb = za + 1;
     const double2 v = res[q * sstr + pad(x)];
-    if (za < NZ) best = fmin(best, cfl * d / fabs(v.x));
-    if (zb < NZ) best = fmin(best, cfl * d / fabs(v.y));
+    if (za < NZ) big = fmax(big, fabs(v.x));
+    if (zb < NZ) big = fmax(big, fabs(v.y));
   }
-  for (int off = 16; off > 0; off >>= 1) best = fmin(best, __shfl_down_sync(0xffffffffu, best, off));
-  if ((tid & 31) == 0) atomicMin(out, (unsigned long long)__double_as_longlong(best));
+  for (int off = 16; off > 0; off >>= 1) big = fmax(big, __shfl_down_sync(0xffffffffu, big, off));
+  if ((tid & 31) == 0) {
+    const double best = cfl * d / big;  // +inf for an all-zero slab, as before
+    atomicMin(out, (unsigned long long)__double_as_longlong(best));
+  }
 }
 
 // r2c of RPAIR row pairs of one plane of one field; keeps kx = 0..NKX, / NX.

@@ -486,7 +486,7 @@ def main():
     ap.add_argument("--ensemble-cases", type=int, default=256)
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--ensemble-rate", type=float, default=20.0)
-    ap.add_argument("--ensemble-active", type=int, default=32)
+    ap.add_argument("--ensemble-active", type=int, default=16)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

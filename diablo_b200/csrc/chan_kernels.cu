@@ -1094,8 +1094,15 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
   double *RA = (double *)(GX + (long)L * MT);   // [j][MT]
   double *RB = RA + (long)L * MT;               // [j][MT]
   double *UU = RB + (long)L * MT;               // [j] upper diagonal rows 2..NY-1
+  double *IDY = UU + L;                         // [j] 1 / DY(j)
+  double *IDYF = IDY + L;                       // [j] 1 / DYF(j)
   const int tid = threadIdx.x;
-  for (int j = tid; j < L; j += COL_THR) UU[j] = (j >= 2 && j < NY) ? 1. / (dy[j + 1] * dyf[j]) : 0.0;
+  for (int j = tid; j < L; j += COL_THR) {
+    UU[j] = (j >= 2 && j < NY) ? 1. / (dy[j + 1] * dyf[j]) : 0.0;
+    IDY[j] = (j >= 1) ? 1. / dy[j] : 0.0;
+    IDYF[j] = (j >= 1 && j <= NY) ? 1. / dyf[j] : 0.0;
+  }
+  __syncthreads();
   for (int base = 0; base < L * MT; base += 4 * COL_THR) {
     double2 a1[4], a3[4], b2[4], b2p[4];
     double av[4], bv[4];
@@ -1122,9 +1129,9 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
       double2 r = make_double2(0.0, 0.0);
       if (m < mt && j >= 2 && j < NY) {
         const double KX = kxv[mg % nkxp], KZ = kzv[mg / nkxp];
-        const double d = dyf[j];
-        r.x = (-KX * a1[u].y) + (b2p[u].x - b2[u].x) / d + (-KZ * a3[u].y);
-        r.y = (KX * a1[u].x) + (b2p[u].y - b2[u].y) / d + (KZ * a3[u].x);
+        const double id = IDYF[j];
+        r.x = (-KX * a1[u].y) + (b2p[u].x - b2[u].x) * id + (-KZ * a3[u].y);
+        r.y = (KX * a1[u].x) + (b2p[u].y - b2[u].y) * id + (KZ * a3[u].x);
       }
       GX[i] = r;
       RA[i] = av[u];
@@ -1186,7 +1193,7 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
     x[1 * st] = ph;
   }
   __syncthreads();
-  const double hh = (rk_step > 0) ? dscal[1 + rk_step] : 1.0;
+  const double ihh = (rk_step > 0) ? 1.0 / dscal[1 + rk_step] : 1.0;
   for (int base = 0; base < L * MT; base += 4 * COL_THR) {
     double2 a1[4], a3[4], b2[4], pc[4];
 #pragma unroll
@@ -1216,14 +1223,14 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
       if (j >= 2) {
         // U2(j) -= (phi(j) - phi(j-1)) / DY(j)
         const double2 pm = GX[i - MT];
-        b2[u].x -= (ph.x - pm.x) / dy[j];
-        b2[u].y -= (ph.y - pm.y) / dy[j];
+        b2[u].x -= (ph.x - pm.x) * IDY[j];
+        b2[u].y -= (ph.y - pm.y) * IDY[j];
         u2[o] = b2[u];
       }
       phi_out[o] = ph;
       if (rk_step > 0 && j >= JS && j <= JE) {
-        pc[u].x = pc[u].x + ph.x / hh;
-        pc[u].y = pc[u].y + ph.y / hh;
+        pc[u].x = pc[u].x + ph.x * ihh;
+        pc[u].y = pc[u].y + ph.y * ihh;
         cp[o] = pc[u];
       }
     }
@@ -1484,7 +1491,8 @@ int dg_cn_tables(dg_handle *h) {
     double *rows = (double *)malloc(sizeof(double) * h->nf * 8 * L);
     cn_row_templates(h, rows);
     DG_CUDA(dg_malloc(h, (void **)&h->cn_rows, sizeof(double) * h->nf * 8 * L));
-    cudaError_t e = cudaMemcpy(h->cn_rows, rows, sizeof(double) * h->nf * 8 * L, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpyAsync(h->cn_rows, rows, sizeof(double) * h->nf * 8 * L,
+                                    cudaMemcpyHostToDevice, h->st);
     free(rows);
     DG_CUDA(e);
   }
@@ -1542,7 +1550,7 @@ int dg_cn_solve_dev(dg_handle *h, int rk_step) {
 int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step) {
   const int L = h->NY + 2;
   const int mt = h->col_mt;
-  const size_t sm = sizeof(double2) * L * mt + sizeof(double) * (2 * L * mt + L);
+  const size_t sm = sizeof(double2) * L * mt + sizeof(double) * (2 * L * mt + 3 * L);
 #define RD_CASE(MTV)                                                                          \
   if (mt == MTV) {                                                                            \
     dg_big_smem((const void *)k_rd_col<MTV>);                                                 \

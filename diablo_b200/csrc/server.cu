@@ -6,8 +6,10 @@
 // slot is free and the device bytes of the active cases plus the newcomer
 // (dg_state_bytes) fit the HBM budget; an admitted case gets its own handle
 // and stream, its state is uploaded, and, on request, APPLY_BC_VEL,
-// REM_DIV_CHAN, APPLY_BC_VEL prepare it as CREATE_FLOW_CHAN does.  The
-// scheduler then keeps up to two RK3 steps of every active case in flight:
+// REM_DIV_CHAN, APPLY_BC_VEL prepare it as CREATE_FLOW_CHAN does.  An
+// admission thread does this set-up (and the first two steps, which capture
+// the case's step graph) so that a stepping thread never waits on it; the
+// stepping thread keeps up to two RK3 steps of every active case in flight:
 // each step is one replay of the case's captured graph (diablo_step) on the
 // case's stream, so steps of different cases overlap on the device.  Launch
 // shapes are tuned once per grid shape (dg_autotune on the first case of a
@@ -87,10 +89,12 @@ struct dg_server {
   int64_t budget = 0;
   int autotune = 1;
   std::mutex mu;
-  std::condition_variable cv_work, cv_done;
+  std::condition_variable cv_work, cv_done, cv_step;
   std::deque<std::shared_ptr<Request>> queue;
   std::map<int64_t, std::shared_ptr<Request>> all;
-  std::vector<Active> active;
+  std::vector<Active> active;     // stepping thread only
+  std::deque<Active> ready;       // prepared, handed to the stepping thread
+  int preparing = 0;
   std::map<ShapeKey, std::vector<int>> tuned;
   std::vector<float> step_ms;
   int64_t next_id = 1;
@@ -99,20 +103,28 @@ struct dg_server {
   double point_steps = 0;
   double t_first_submit = -1, t_last_done = 0;
   bool stop = false;
-  std::thread worker;
+  std::thread worker, admitter;
   int device = 0;
+  int n_active = 0;               // active.size(), readable under mu
 
   void fail(Active &a, int code, const char *msg) {
     a.r->status = -code;
     a.r->err = msg ? msg : "";
   }
 
-  // admit one request; returns false if it must wait (no slot or memory)
+  // set up one request (on failure its status carries the error code)
   bool try_admit(std::shared_ptr<Request> r, int64_t est) {
     Active a;
     a.r = r;
     a.bytes = est;
-    if (cudaStreamCreateWithFlags(&a.st, cudaStreamNonBlocking) != cudaSuccess) return false;
+    if (cudaStreamCreateWithFlags(&a.st, cudaStreamNonBlocking) != cudaSuccess) {
+      std::lock_guard<std::mutex> lk(mu);
+      r->status = -DG_ERR_CUDA;
+      r->err = "stream creation failed";
+      r->t_done = now_s();
+      cv_done.notify_all();
+      return true;
+    }
     int code = diablo_gpu_init(&r->p, r->gy.empty() ? nullptr : r->gy.data(), a.st, &a.h);
     if (code != DG_OK) {
       cudaStreamDestroy(a.st);
@@ -163,12 +175,33 @@ struct dg_server {
       cudaEventCreate(&f.e1);
       a.pool.push_back(f);
     }
+    // the first steps run here: the first is eager, the second captures the
+    // case's step graph
+    const int warm = r->nsteps < 2 ? r->nsteps : 2;
+    code = diablo_step(a.h, 1, warm);
+    if (code == DG_OK && cudaStreamSynchronize(a.st) != cudaSuccess) code = DG_ERR_CUDA;
+    if (code != DG_OK) {
+      const std::string msg = dg_last_error();
+      for (InFlight &f : a.pool) {
+        cudaEventDestroy(f.e0);
+        cudaEventDestroy(f.e1);
+      }
+      diablo_gpu_finalize(a.h);
+      cudaStreamDestroy(a.st);
+      std::lock_guard<std::mutex> lk(mu);
+      r->status = -code;
+      r->err = msg;
+      r->t_done = now_s();
+      cv_done.notify_all();
+      return true;
+    }
+    a.launched = a.completed = warm;
     std::lock_guard<std::mutex> lk(mu);
     r->status = 2;
     r->t_admit = now_s();
-    bytes_active += est;
-    bytes_peak = std::max(bytes_peak, bytes_active);
-    active.push_back(std::move(a));
+    steps_done += warm;
+    point_steps += (double)warm * r->p.nx * r->p.ny * r->p.nz;
+    ready.push_back(std::move(a));
     return true;
   }
 
@@ -204,36 +237,64 @@ struct dg_server {
     cv_done.notify_all();
   }
 
+  // admission thread: set-up of queued requests in arrival order while a
+  // slot is free and the budget allows
+  void admit_loop() {
+    cudaSetDevice(device);
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+      cv_work.wait(lk, [&] {
+        return stop || (!queue.empty() &&
+                        n_active + (int)ready.size() + preparing < max_active);
+      });
+      if (stop) return;
+      std::shared_ptr<Request> r = queue.front();
+      const int64_t est = dg_state_bytes(&r->p);
+      if (est < 0 || (budget > 0 && est > budget)) {
+        queue.pop_front();
+        r->status = -DG_ERR_OOM;
+        r->err = "case exceeds the HBM budget";
+        r->t_done = now_s();
+        cv_done.notify_all();
+        continue;
+      }
+      if (budget > 0 && bytes_active + est > budget) {
+        // wait for a retirement to free memory
+        cv_work.wait(lk, [&] { return stop || bytes_active + est <= budget; });
+        continue;
+      }
+      queue.pop_front();
+      preparing++;
+      bytes_active += est;
+      bytes_peak = std::max(bytes_peak, bytes_active);
+      lk.unlock();
+      const bool ok = try_admit(r, est);
+      lk.lock();
+      preparing--;
+      if (!ok || r->status < 0) bytes_active -= est;  // failed set-up frees its share
+      cv_step.notify_one();
+    }
+  }
+
+  // stepping thread: collects finished steps and keeps two steps of every
+  // active case in flight
   void loop() {
     cudaSetDevice(device);
     for (;;) {
       {
         std::unique_lock<std::mutex> lk(mu);
-        if (active.empty() && queue.empty()) {
-          if (stop) return;
-          cv_work.wait(lk, [&] { return stop || !queue.empty(); });
-          if (stop && queue.empty()) return;
+        if (active.empty() && ready.empty()) {
+          cv_step.wait(lk, [&] {
+            return !ready.empty() || (stop && queue.empty() && preparing == 0);
+          });
+          if (ready.empty() && stop && queue.empty() && preparing == 0) return;
         }
-        // admission in arrival order
-        while (!queue.empty() && (int)active.size() < max_active) {
-          std::shared_ptr<Request> r = queue.front();
-          const int64_t est = dg_state_bytes(&r->p);
-          if (est < 0 || (budget > 0 && est > budget)) {
-            queue.pop_front();
-            r->status = -DG_ERR_OOM;
-            r->err = "case exceeds the HBM budget";
-            r->t_done = now_s();
-            cv_done.notify_all();
-            continue;
-          }
-          if (budget > 0 && bytes_active + est > budget) break;  // wait for memory
-          queue.pop_front();
-          lk.unlock();
-          try_admit(r, est);
-          lk.lock();
+        while (!ready.empty()) {
+          active.push_back(std::move(ready.front()));
+          ready.pop_front();
         }
+        n_active = (int)active.size();
       }
-      // advance: collect finished steps, keep two steps of every case in flight
       bool progressed = false;
       for (size_t i = 0; i < active.size();) {
         Active &a = active[i];
@@ -256,6 +317,8 @@ struct dg_server {
           if (a.inflight.empty()) {
             std::lock_guard<std::mutex> lk(mu);
             retire(i);
+            n_active = (int)active.size();
+            cv_work.notify_all();
             progressed = true;
             continue;
           }
@@ -297,6 +360,7 @@ extern "C" int dg_server_create(int max_active, double hbm_budget_gb, int autotu
   s->autotune = autotune;
   cudaGetDevice(&s->device);
   s->worker = std::thread([s] { s->loop(); });
+  s->admitter = std::thread([s] { s->admit_loop(); });
   *out = s;
   return DG_OK;
 }
@@ -358,7 +422,7 @@ extern "C" int dg_server_query(dg_server *s, dg_server_stats *st) {
   memset(st, 0, sizeof(*st));
   st->cases_done = s->cases_done;
   st->steps_done = s->steps_done;
-  st->active = (int)s->active.size();
+  st->active = s->n_active;
   st->queued = (int)s->queue.size();
   st->bytes_active = s->bytes_active;
   st->bytes_peak = s->bytes_peak;
@@ -385,7 +449,20 @@ extern "C" int dg_server_destroy(dg_server *s) {
     s->stop = true;
   }
   s->cv_work.notify_all();
+  s->cv_step.notify_all();
+  if (s->admitter.joinable()) s->admitter.join();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    // requests never admitted end with an error
+    for (auto &r : s->queue) {
+      r->status = -DG_ERR_ARG;
+      r->err = "server destroyed before admission";
+    }
+    s->queue.clear();
+  }
+  s->cv_step.notify_all();
   if (s->worker.joinable()) s->worker.join();
+  s->cv_done.notify_all();
   delete s;
   return DG_OK;
 }

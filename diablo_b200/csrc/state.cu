@@ -84,11 +84,9 @@ cudaError_t dg_malloc(dg_handle *h, void **p, size_t bytes) {
       raised[dev] = true;
     }
   }
-  cudaError_t e = cudaMallocAsync(p, bytes, h->st);
-  // complete before the block is touched from another stream or a
-  // synchronous copy
-  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
-  return e;
+  // ordered on the handle's stream: every first use of a block is queued on
+  // that stream too (set-up copies included), or comes after a join with it
+  return cudaMallocAsync(p, bytes, h->st);
 }
 
 void dg_free(dg_handle *h, void *p) {
@@ -285,12 +283,12 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
   DG_TRY(dalloc(h, &h->kx, h->nkxp));
   DG_TRY(dalloc(h, &h->kz, h->nkzt));
   DG_TRY(dalloc(h, &h->ky, h->nkyt));
-  DG_CUDA(cudaMemcpy(h->gyf, h->h_gyf, sizeof(double) * L, cudaMemcpyHostToDevice));
-  DG_CUDA(cudaMemcpy(h->dy, h->h_dy, sizeof(double) * L, cudaMemcpyHostToDevice));
-  DG_CUDA(cudaMemcpy(h->dyf, h->h_dyf, sizeof(double) * L, cudaMemcpyHostToDevice));
-  DG_CUDA(cudaMemcpy(h->kx, h->h_kx, sizeof(double) * h->nkxp, cudaMemcpyHostToDevice));
-  DG_CUDA(cudaMemcpy(h->kz, h->h_kz, sizeof(double) * h->nkzt, cudaMemcpyHostToDevice));
-  DG_CUDA(cudaMemcpy(h->ky, h->h_ky, sizeof(double) * h->nkyt, cudaMemcpyHostToDevice));
+  DG_CUDA(cudaMemcpyAsync(h->gyf, h->h_gyf, sizeof(double) * L, cudaMemcpyHostToDevice, h->st));
+  DG_CUDA(cudaMemcpyAsync(h->dy, h->h_dy, sizeof(double) * L, cudaMemcpyHostToDevice, h->st));
+  DG_CUDA(cudaMemcpyAsync(h->dyf, h->h_dyf, sizeof(double) * L, cudaMemcpyHostToDevice, h->st));
+  DG_CUDA(cudaMemcpyAsync(h->kx, h->h_kx, sizeof(double) * h->nkxp, cudaMemcpyHostToDevice, h->st));
+  DG_CUDA(cudaMemcpyAsync(h->kz, h->h_kz, sizeof(double) * h->nkzt, cudaMemcpyHostToDevice, h->st));
+  DG_CUDA(cudaMemcpyAsync(h->ky, h->h_ky, sizeof(double) * h->nkyt, cudaMemcpyHostToDevice, h->st));
 
   dg_make_plan(h->NX, &h->plx);
   dg_make_plan(h->NZ, &h->plz);
@@ -301,27 +299,27 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
     double2 *tmp = (double2 *)malloc(sizeof(double2) * nmax);
     DG_TRY(dalloc(h, &h->twx, h->NX));
     twiddles(h->NX, tmp);
-    DG_CUDA(cudaMemcpy(h->twx, tmp, sizeof(double2) * h->NX, cudaMemcpyHostToDevice));
+    DG_CUDA(cudaMemcpyAsync(h->twx, tmp, sizeof(double2) * h->NX, cudaMemcpyHostToDevice, h->st));
     DG_TRY(dalloc(h, &h->twz, h->NZ));
     twiddles(h->NZ, tmp);
-    DG_CUDA(cudaMemcpy(h->twz, tmp, sizeof(double2) * h->NZ, cudaMemcpyHostToDevice));
+    DG_CUDA(cudaMemcpyAsync(h->twz, tmp, sizeof(double2) * h->NZ, cudaMemcpyHostToDevice, h->st));
     if (p->precision == 1) {
       h->mixed = 1;
       float2 *tf = (float2 *)malloc(sizeof(float2) * nmax);
       twiddles(h->NX, tmp);
       for (int m = 0; m < h->NX; m++) tf[m] = make_float2((float)tmp[m].x, (float)tmp[m].y);
       DG_CUDA(dg_malloc(h, (void **)&h->twx_f, sizeof(float2) * h->NX));
-      DG_CUDA(cudaMemcpy(h->twx_f, tf, sizeof(float2) * h->NX, cudaMemcpyHostToDevice));
+      DG_CUDA(cudaMemcpyAsync(h->twx_f, tf, sizeof(float2) * h->NX, cudaMemcpyHostToDevice, h->st));
       twiddles(h->NZ, tmp);
       for (int m = 0; m < h->NZ; m++) tf[m] = make_float2((float)tmp[m].x, (float)tmp[m].y);
       DG_CUDA(dg_malloc(h, (void **)&h->twz_f, sizeof(float2) * h->NZ));
-      DG_CUDA(cudaMemcpy(h->twz_f, tf, sizeof(float2) * h->NZ, cudaMemcpyHostToDevice));
+      DG_CUDA(cudaMemcpyAsync(h->twz_f, tf, sizeof(float2) * h->NZ, cudaMemcpyHostToDevice, h->st));
       free(tf);
     }
     if (h->periodic) {
       DG_TRY(dalloc(h, &h->twy, h->NY));
       twiddles(h->NY, tmp);
-      DG_CUDA(cudaMemcpy(h->twy, tmp, sizeof(double2) * h->NY, cudaMemcpyHostToDevice));
+      DG_CUDA(cudaMemcpyAsync(h->twy, tmp, sizeof(double2) * h->NY, cudaMemcpyHostToDevice, h->st));
     }
     free(tmp);
   }

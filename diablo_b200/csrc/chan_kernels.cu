@@ -27,7 +27,7 @@ using namespace dgfft;
 
 namespace {
 
-constexpr int XR_ROWS = 2;     // physical z-rows per CTA in k_xrow_nl
+constexpr int XR_ROWS = 2;     // physical z-rows per CTA in k_xrow_nl (1 for the largest rows)
 
 struct ChanConst {
   int NX, NY, NZ, NKX, NKZ, nkxp, nkzt, nf, nth;
@@ -78,7 +78,7 @@ constexpr int XR_THR = 128;
 
 template <int NT>
 __global__ void __launch_bounds__(XR_THR) k_xrow_nl(
-    ChanConst C, const double2 *__restrict__ H, long Hfield, int chunk, FftPlan pl,
+    ChanConst C, const double2 *__restrict__ H, long Hfield, int chunk, int xr, FftPlan pl,
     const double2 *__restrict__ tw, const double *__restrict__ dyf, const double *__restrict__ dy,
     const double *__restrict__ kxv, double2 *__restrict__ G, long Gfield) {
   extern __shared__ double2 sm[];
@@ -91,11 +91,11 @@ __global__ void __launch_bounds__(XR_THR) k_xrow_nl(
   const int sstr = padded_len(NX);
   double2 *stw = sm;
   double2 *b0 = stw + NX;
-  double2 *b1 = b0 + XR_ROWS * maxp * sstr;
-  double2 *prev = b0 + fft_bufs(NX) * XR_ROWS * maxp * sstr;  // [row][3+nth][nkxp]
-  double *ring = (double *)(prev + XR_ROWS * (3 + nth) * nkxp);  // [3][row][nf][NX]
+  double2 *b1 = b0 + xr * maxp * sstr;
+  double2 *prev = b0 + fft_bufs(NX) * xr * maxp * sstr;  // [row][3+nth][nkxp]
+  double *ring = (double *)(prev + xr * (3 + nth) * nkxp);  // [3][row][nf][NX]
   const int tid = threadIdx.x, nthr = blockDim.x;
-  const int z0 = blockIdx.x * XR_ROWS;
+  const int z0 = blockIdx.x * xr;
   const int j0 = 1 + blockIdx.y * chunk;
   int j1 = j0 + chunk - 1;
   if (j1 > C.NY) j1 = C.NY;
@@ -103,17 +103,17 @@ __global__ void __launch_bounds__(XR_THR) k_xrow_nl(
 
   for (int i = tid; i < NX; i += nthr) stw[i] = tw[i];
   // plane j0-2 may be -1: zero the whole ring once
-  for (int i = tid; i < 3 * XR_ROWS * nf * NX; i += nthr) ring[i] = 0.0;
+  for (int i = tid; i < 3 * xr * nf * NX; i += nthr) ring[i] = 0.0;
   __syncthreads();
 
   auto ringp = [&](int plane, int r, int f) -> double * {
     int s = (plane + 3) % 3;
-    return ring + (((long)s * XR_ROWS + r) * nf + f) * NX;
+    return ring + (((long)s * xr + r) * nf + f) * NX;
   };
 
   // load + c2r of one plane into its ring slot
   auto load_plane = [&](int plane) {
-    for (int idx = tid; idx < XR_ROWS * npin * NX; idx += nthr) {
+    for (int idx = tid; idx < xr * npin * NX; idx += nthr) {
       const int k = idx % NX;
       const int q = (idx / NX) % npin;
       const int r = idx / (NX * npin);
@@ -131,8 +131,8 @@ __global__ void __launch_bounds__(XR_THR) k_xrow_nl(
       b0[(r * npin + q) * sstr + pad(k)] = v;
     }
     __syncthreads();
-    double2 *res = fft<NT>(b0, b1, pl, XR_ROWS * npin, sstr, stw, +1);
-    for (int idx = tid; idx < XR_ROWS * npin * NX; idx += nthr) {
+    double2 *res = fft<NT>(b0, b1, pl, xr * npin, sstr, stw, +1);
+    for (int idx = tid; idx < xr * npin * NX; idx += nthr) {
       const int x = idx % NX;
       const int q = (idx / NX) % npin;
       const int r = idx / (NX * npin);
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(XR_THR) k_xrow_nl(
     // products of plane j into complex pairs
     const double dyfj = (j >= 1) ? dyf[j] : 0.0, dyfm = (j >= 1) ? dyf[j - 1] : 0.0;
     const double dyj = (j >= 1) ? dy[j] : 1.0;
-    for (int idx = tid; idx < XR_ROWS * npp * NX; idx += nthr) {
+    for (int idx = tid; idx < xr * npp * NX; idx += nthr) {
       const int x = idx % NX;
       const int q = (idx / NX) % npp;
       const int r = idx / (NX * npp);
@@ -186,11 +186,11 @@ __global__ void __launch_bounds__(XR_THR) k_xrow_nl(
       b0[(r * npp + q) * sstr + pad(x)] = make_double2(pv[0], pv[1]);
     }
     __syncthreads();
-    double2 *res = fft<NT>(b0, b1, pl, XR_ROWS * npp, sstr, stw, -1);
+    double2 *res = fft<NT>(b0, b1, pl, xr * npp, sstr, stw, -1);
     // separate, scale by 1/NX, combine, write
     const double rnx = (double)NX;
     const bool out = (j >= j0);
-    for (int idx = tid; idx < XR_ROWS * nkxp; idx += nthr) {
+    for (int idx = tid; idx < xr * nkxp; idx += nthr) {
       const int k = idx % nkxp;
       const int r = idx / nkxp;
       const int z = z0 + r;
@@ -242,14 +242,17 @@ __global__ void __launch_bounds__(XR_THR) k_xrow_nl(
   }
 }
 
-size_t xrow_smem(const dg_handle *h) {
+size_t xrow_smem(const dg_handle *h, int xr) {
   const int nf = h->nf, nth = h->NTH, NX = h->NX;
   const int npin = (nf + 1) / 2, npp = (8 + 3 * nth + 1) / 2;
   const int maxp = npin > npp ? npin : npp;
-  return sizeof(double2) * (NX + fft_bufs(NX) * XR_ROWS * maxp * padded_len(NX) +
-                            XR_ROWS * (3 + nth) * h->nkxp) +
-         sizeof(double) * 3 * XR_ROWS * nf * NX;
+  return sizeof(double2) * (NX + fft_bufs(NX) * xr * maxp * padded_len(NX) +
+                            xr * (3 + nth) * h->nkxp) +
+         sizeof(double) * 3 * xr * nf * NX;
 }
+
+// z-rows per CTA of k_xrow_nl: two where the shared memory allows, else one
+int xrow_rows(const dg_handle *h) { return xrow_smem(h, XR_ROWS) <= 220 * 1024 ? XR_ROWS : 1; }
 
 // ------------------------------------------------------- xrow, one warp/row
 // Same products as k_xrow_nl, organised so a warp owns one physical z-row and
@@ -898,15 +901,13 @@ struct CnRows {
 
 __global__ void k_cn_tables(CnRows P, const double *__restrict__ dscal,
                             const double *__restrict__ rows, double *__restrict__ tab) {
-  // rows: [field][8][L] = kind, l1, d1, u1, l0, d0, u0, v
-  extern __shared__ double rsm[];
+  // rows: [field][8][L] = kind, l1, d1, u1, l0, d0, u0, v (read through L1:
+  // the three substeps of a field read the same rows)
   const int L = P.NY + 2;
-  for (int i = threadIdx.x; i < P.nfld * 8 * L; i += blockDim.x) rsm[i] = rows[i];
-  __syncthreads();
   const int t = threadIdx.x;
   if (t >= 3 * P.nfld) return;
   const int rk = t / P.nfld, f = t % P.nfld;
-  const double *R = rsm + (long)f * 8 * L;
+  const double *R = rows + (long)f * 8 * L;
   double *T = tab + (long)(rk * (3 + DG_MAX_TH) + f) * 5 * L;
   const double h = dscal[2 + rk];
   const double s = (P.nu * h / 2.0) / P.pr[f] * P.nuv;
@@ -1096,7 +1097,13 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
   double *UU = RB + (long)L * MT;               // [j] upper diagonal rows 2..NY-1
   double *IDY = UU + L;                         // [j] 1 / DY(j)
   double *IDYF = IDY + L;                       // [j] 1 / DYF(j)
+  double *KXS = IDYF + L, *KZS = KXS + MT;      // wavenumbers of the CTA's modes
   const int tid = threadIdx.x;
+  if (tid < MT) {
+    const int mi = (int)(m0 + tid) < (int)ss ? (int)(m0 + tid) : 0;
+    KXS[tid] = kxv[mi % nkxp];
+    KZS[tid] = kzv[mi / nkxp];
+  }
   for (int j = tid; j < L; j += COL_THR) {
     UU[j] = (j >= 2 && j < NY) ? 1. / (dy[j + 1] * dyf[j]) : 0.0;
     IDY[j] = (j >= 1) ? 1. / dy[j] : 0.0;
@@ -1128,7 +1135,7 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
       const long mg = m0 + m;
       double2 r = make_double2(0.0, 0.0);
       if (m < mt && j >= 2 && j < NY) {
-        const double KX = kxv[mg % nkxp], KZ = kzv[mg / nkxp];
+        const double KX = KXS[m], KZ = KZS[m];
         const double id = IDYF[j];
         r.x = (-KX * a1[u].y) + (b2p[u].x - b2[u].x) * id + (-KZ * a3[u].y);
         r.y = (KX * a1[u].x) + (b2p[u].y - b2[u].y) * id + (KZ * a3[u].x);
@@ -1213,7 +1220,7 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
       const int m = i % MT, j = i / MT;
       if (i >= L * MT || m >= mt || j < 1 || j > NY) continue;
       const long mg = m0 + m, o = (long)j * ss + mg;
-      const double KX = kxv[mg % nkxp], KZ = kzv[mg / nkxp];
+      const double KX = KXS[m], KZ = KZS[m];
       const double2 ph = GX[i];
       // U1 -= i kx phi, U3 -= i kz phi
       a1[u].x -= -KX * ph.y; a1[u].y -= KX * ph.x;
@@ -1500,7 +1507,7 @@ int dg_cn_tables(dg_handle *h) {
   P.NY = h->NY; P.nfld = h->nf; P.nu = h->p.nu; P.nuv = h->p.nu_v_scale;
   for (int f = 0; f < 3 + DG_MAX_TH; f++) P.pr[f] = (f >= 3 && f - 3 < h->NTH) ? h->p.pr[f - 3] : 1.0;
   dg_kt_begin(h, "k_cn_tables", h->st);
-  k_cn_tables<<<1, 32, sizeof(double) * h->nf * 8 * L, h->st>>>(P, h->dscal, h->cn_rows, h->cn_tab);
+  k_cn_tables<<<1, 32, 0, h->st>>>(P, h->dscal, h->cn_rows, h->cn_tab);
   DG_LAUNCHED();
   return DG_OK;
 }
@@ -1530,7 +1537,8 @@ int dg_cn_solve_dev(dg_handle *h, int rk_step) {
   for (int n = 0; n < h->NTH; n++) wl[3 + n] = h->jstart_th[n] - 1;
   const int L = h->NY + 2;
   const double *tab = h->cn_tab + (long)(rk_step - 1) * (3 + DG_MAX_TH) * 5 * L;
-  const int mt = h->cn_mt;
+  int mt = h->cn_mt;  // fewer modes per CTA where a tall column needs it
+  while (mt > 4 && sizeof(double2) * L * mt + sizeof(double) * 5 * L > 220 * 1024) mt /= 2;
   const size_t sm = sizeof(double2) * L * mt + sizeof(double) * 5 * L;
   dim3 grid(dg_cdiv(h->ss, mt), h->nf);
 #define CN_CASE(MTV)                                                                    \
@@ -1549,8 +1557,12 @@ int dg_cn_solve_dev(dg_handle *h, int rk_step) {
 
 int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step) {
   const int L = h->NY + 2;
-  const int mt = h->col_mt;
-  const size_t sm = sizeof(double2) * L * mt + sizeof(double) * (2 * L * mt + 3 * L);
+  auto rd_smem = [&](int m) {
+    return sizeof(double2) * L * m + sizeof(double) * (2 * L * m + 3 * L + 2 * m);
+  };
+  int mt = h->col_mt;  // fewer modes per CTA where a tall column needs it
+  while (mt > 4 && rd_smem(mt) > 220 * 1024) mt /= 2;
+  const size_t sm = rd_smem(mt);
 #define RD_CASE(MTV)                                                                          \
   if (mt == MTV) {                                                                            \
     dg_big_smem((const void *)k_rd_col<MTV>);                                                 \
@@ -1750,12 +1762,13 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
         DG_TRY(dg_zinv(h, in, h->nf, hdone + 1, h->NY + 1, h->H, 0));
         hdone = h->NY + 1;
         const int chunk = 8;
-        dim3 grid(dg_cdiv(h->NZ, XR_ROWS), dg_cdiv(h->NY, chunk));
-        const size_t sm = xrow_smem(h);
+        const int xr = xrow_rows(h);
+        dim3 grid(dg_cdiv(h->NZ, xr), dg_cdiv(h->NY, chunk));
+        const size_t sm = xrow_smem(h, xr);
 #define KERNEL_BODY(N)                                                                          \
   dg_big_smem((const void *)k_xrow_nl<N>);                                                      \
   dg_kt_begin(h, "k_xrow_nl", h->st);                                                               \
-  k_xrow_nl<N><<<grid, XR_THR, sm, h->st>>>(C, h->H, Hfield, chunk, h->plx, h->twx, h->dyf, h->dy, \
+  k_xrow_nl<N><<<grid, XR_THR, sm, h->st>>>(C, h->H, Hfield, chunk, xr, h->plx, h->twx, h->dyf, h->dy, \
                                             h->kx, h->G, Hfield)
         switch (h->NX) {
           DG_FOR_EACH_N(DG_CASE_N)

@@ -184,12 +184,12 @@ __global__ void k_per_final(PerConst C, int rk_step, const double *__restrict__ 
                             const double *__restrict__ kzv, const double2 *__restrict__ Fy,
                             long Ffield, FieldPtrs cu, FieldPtrs cf, double2 *__restrict__ cp,
                             double2 *__restrict__ phi, double forcing) {
-  const long total = (long)C.nkyt * C.ss;
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= total) return;
-  const int jy = (int)(q / C.ss);
-  const long m = q % C.ss;
-  const int kx = (int)(m % C.nkxp), kz = (int)(m / C.nkxp);
+  // grid: x over the modes of a ky plane, y over the ky planes
+  const int jy = blockIdx.y;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= (int)C.ss) return;
+  const long q = (long)jy * C.ss + m;
+  const int kz = m / C.nkxp, kx = m - kz * C.nkxp;
   const double KX = kxv[kx], KY = kyv[jy], KZ = kzv[kz];
   const double k2 = KX * KX + KY * KY + KZ * KZ;
   const double h = dscal[1 + rk_step];
@@ -204,19 +204,26 @@ __global__ void k_per_final(PerConst C, int rk_step, const double *__restrict__ 
   const double2 f0 = F(0), f1 = F(1), f2 = F(2), f3 = F(3), f4 = F(4), f5 = F(5);
   double2 nf[3] = {mdiv(f0, f1, f2), mdiv(f1, f3, f4), mdiv(f2, f4, f5)};
   double2 u[3], p0 = cp[q];
+#pragma unroll
   for (int d = 0; d < 3; d++) u[d] = cu(d)[q];
   // USER_RHS_PER_PHYSICAL: CF_i += (EPSILON_TARGET / EK) U_i (exact in
   // spectral space for band-limited U)
-  if (forcing != 0.0)
+  if (forcing != 0.0) {
+#pragma unroll
     for (int d = 0; d < 3; d++) { nf[d].x += forcing * u[d].x; nf[d].y += forcing * u[d].y; }
-  for (int n = 0; n < C.nth; n++) {
+  }
+#pragma unroll
+  for (int n = 0; n < DG_MAX_TH; n++) {
+    if (n >= C.nth) break;
     const double2 t = cu(3 + n)[q];
     nf[1].x += C.ri[n] * t.x;
     nf[1].y += C.ri[n] * t.y;
   }
-  const double t5 = 1 - T1 * k2, t5i = 1 + T1 * k2;
+  // one reciprocal per mode instead of a division per component
+  const double t5 = 1 - T1 * k2, it5 = 1.0 / (1 + T1 * k2);
   const double Kd[3] = {KX, KY, KZ};
   double2 un[3];
+#pragma unroll
   for (int d = 0; d < 3; d++) {
     // CR = (1 - T1 k^2) CU - h (i k_d CP) [+ zeta h CF_old] + beta h CF
     double2 r = make_double2(t5 * u[d].x - T4 * (-Kd[d] * p0.y), t5 * u[d].y - T4 * (Kd[d] * p0.x));
@@ -227,16 +234,18 @@ __global__ void k_per_final(PerConst C, int rk_step, const double *__restrict__ 
     }
     r.x += T2 * nf[d].x;
     r.y += T2 * nf[d].y;
-    un[d] = make_double2(r.x / t5i, r.y / t5i);
+    un[d] = make_double2(r.x * it5, r.y * it5);
     cf(d)[q] = nf[d];
   }
-  for (int n = 0; n < C.nth; n++) {
+#pragma unroll
+  for (int n = 0; n < DG_MAX_TH; n++) {
+    if (n >= C.nth) break;
     const double2 t = cu(3 + n)[q];
     double2 ft = C.bg[n] ? make_double2(-u[1].x, -u[1].y) : make_double2(0.0, 0.0);
     const double2 g = mdiv(F(6 + 3 * n), F(7 + 3 * n), F(8 + 3 * n));
     ft.x += g.x;
     ft.y += g.y;
-    const double t6 = 1 - (T1 / C.pr[n]) * k2, t6i = 1 + (T1 / C.pr[n]) * k2;
+    const double t6 = 1 - (T1 / C.pr[n]) * k2, it6 = 1.0 / (1 + (T1 / C.pr[n]) * k2);
     double2 r = make_double2(t6 * t.x, t6 * t.y);
     if (rk_step > 1) {
       const double2 o = cf(3 + n)[q];
@@ -245,31 +254,33 @@ __global__ void k_per_final(PerConst C, int rk_step, const double *__restrict__ 
     }
     r.x += T2 * ft.x;
     r.y += T2 * ft.y;
-    cu(3 + n)[q] = make_double2(r.x / t6i, r.y / t6i);
+    cu(3 + n)[q] = make_double2(r.x * it6, r.y * it6);
     cf(3 + n)[q] = ft;
   }
   // REM_DIV_PER: phi = (i k . U) / -(k^2 + EPS); U -= i k phi; CP += phi / h
-  const double den = -(KX * KX + KY * KY + KZ * KZ + C.eps);
+  const double iden = 1.0 / -(KX * KX + KY * KY + KZ * KZ + C.eps);
   const double2 dv = make_double2(-(KX * un[0].y + KY * un[1].y + KZ * un[2].y),
                                   KX * un[0].x + KY * un[1].x + KZ * un[2].x);
-  const double2 ph = make_double2(dv.x / den, dv.y / den);
+  const double2 ph = make_double2(dv.x * iden, dv.y * iden);
+#pragma unroll
   for (int d = 0; d < 3; d++) {
     un[d].x -= -Kd[d] * ph.y;
     un[d].y -= Kd[d] * ph.x;
     cu(d)[q] = un[d];
   }
   phi[q] = ph;
-  cp[q] = make_double2(p0.x + ph.x / T4, p0.y + ph.y / T4);
+  const double iT4 = 1.0 / T4;
+  cp[q] = make_double2(p0.x + ph.x * iT4, p0.y + ph.y * iT4);
 }
 
 __global__ void k_rem_div_per(PerConst C, const double *__restrict__ kxv,
                               const double *__restrict__ kyv, const double *__restrict__ kzv,
                               double2 *__restrict__ u1, double2 *__restrict__ u2,
                               double2 *__restrict__ u3, double2 *__restrict__ phi) {
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= (long)C.nkyt * C.ss) return;
-  const int jy = (int)(q / C.ss);
-  const long m = q % C.ss;
+  const int jy = blockIdx.y;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= (int)C.ss) return;
+  const long q = (long)jy * C.ss + m;
   const double KX = kxv[m % C.nkxp], KY = kyv[jy], KZ = kzv[m / C.nkxp];
   const double den = -(KX * KX + KY * KY + KZ * KZ + C.eps);
   double2 a = u1[q], b = u2[q], c = u3[q];
@@ -288,10 +299,10 @@ __global__ void k_rem_div_per(PerConst C, const double *__restrict__ kxv,
 __global__ void k_ik(PerConst C, const double *__restrict__ kxv, const double *__restrict__ kyv,
                      const double *__restrict__ kzv, const double2 *__restrict__ src, int axis,
                      double2 *__restrict__ dst) {
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= (long)C.nkyt * C.ss) return;
-  const int jy = (int)(q / C.ss);
-  const long m = q % C.ss;
+  const int jy = blockIdx.y;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= (int)C.ss) return;
+  const long q = (long)jy * C.ss + m;
   const double K = axis == 0 ? kxv[m % C.nkxp] : (axis == 1 ? kyv[jy] : kzv[m / C.nkxp]);
   const double2 v = src[q];
   dst[q] = make_double2(-K * v.y, K * v.x);
@@ -311,10 +322,10 @@ __global__ void k_pp_second(long n, const double *__restrict__ A, double *__rest
 
 __global__ void k_pp_solve(PerConst C, const double *__restrict__ kxv, const double *__restrict__ kyv,
                            const double *__restrict__ kzv, double2 *__restrict__ cp) {
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= (long)C.nkyt * C.ss) return;
-  const int jy = (int)(q / C.ss);
-  const long m = q % C.ss;
+  const int jy = blockIdx.y;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= (int)C.ss) return;
+  const long q = (long)jy * C.ss + m;
   const double KX = kxv[m % C.nkxp], KY = kyv[jy], KZ = kzv[m / C.nkxp];
   const double d = KX * KX + KY * KY + KZ * KZ + C.eps;
   double2 v = cp[q];
@@ -330,7 +341,7 @@ __global__ void k_per_sums(PerConst C, CFieldPtrs u, double *__restrict__ out, i
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int bad = 0;
   for (long m = threadIdx.x; m < C.ss; m += blockDim.x) {
-    const double w = ((m % C.nkxp) == 0) ? 1.0 : 2.0;
+    const double w = (((int)m % C.nkxp) == 0) ? 1.0 : 2.0;
     const long q = (long)jy * C.ss + m;
     for (int f = 0; f < C.nf && f < 8; f++) {
       const double2 v = u(f)[q];
@@ -362,10 +373,10 @@ __global__ void k_div_per(PerConst C, const double *__restrict__ kxv, const doub
                           const double *__restrict__ kzv, const double2 *__restrict__ u1,
                           const double2 *__restrict__ u2, const double2 *__restrict__ u3,
                           double2 *__restrict__ d) {
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= (long)C.nkyt * C.ss) return;
-  const int jy = (int)(q / C.ss);
-  const long m = q % C.ss;
+  const int jy = blockIdx.y;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= (int)C.ss) return;
+  const long q = (long)jy * C.ss + m;
   const double KX = kxv[m % C.nkxp], KY = kyv[jy], KZ = kzv[m / C.nkxp];
   const double2 a = u1[q], b = u2[q], c = u3[q];
   d[q] = make_double2(-(KX * a.y + KY * b.y + KZ * c.y), KX * a.x + KY * b.x + KZ * c.x);
@@ -544,7 +555,7 @@ extern "C" int diablo_rk_per_1(dg_handle *h, int rk_step) {
   for (int f = 0; f < nf; f++) { cu.p[f] = h->cu[f]; cf.p[f] = h->cf[f]; }
   const long tot = (long)h->nkyt * h->ss;
   dg_kt_begin(h, "k_per_final", h->st);
-  k_per_final<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(C, rk_step, h->dscal, h->kx, h->ky, h->kz,
+  k_per_final<<<dim3(dg_cdiv(h->ss, 256), h->nkyt), 256, 0, h->st>>>(C, rk_step, h->dscal, h->kx, h->ky, h->kz,
                                                     h->Q, fy_field(h), cu, cf, h->cp, h->cr1,
                                                     forcing);
   DG_LAUNCHED();
@@ -556,7 +567,7 @@ extern "C" int diablo_rem_div_per(dg_handle *h) {
   const PerConst C = make_pc(h);
   const long tot = (long)h->nkyt * h->ss;
   dg_kt_begin(h, "k_rem_div_per", h->st);
-  k_rem_div_per<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[0], h->cu[1],
+  k_rem_div_per<<<dim3(dg_cdiv(h->ss, 256), h->nkyt), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[0], h->cu[1],
                                                       h->cu[2], h->cr1);
   DG_LAUNCHED();
   return DG_OK;
@@ -571,10 +582,10 @@ extern "C" int diablo_poisson_p_per(dg_handle *h) {
   double2 *s0 = h->rhs[0], *s1 = h->rhs[1];
   // R1 = IFFT(i kx U1), R2 = IFFT(i kz U3); P = R1^2 + R1 R2 + R2^2
   dg_kt_begin(h, "k_ik", h->st);
-  k_ik<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[0], 0, s0);
+  k_ik<<<dim3(dg_cdiv(h->ss, 256), h->nkyt), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[0], 0, s0);
   DG_LAUNCHED();
   dg_kt_begin(h, "k_ik", h->st);
-  k_ik<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[2], 2, s1);
+  k_ik<<<dim3(dg_cdiv(h->ss, 256), h->nkyt), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[2], 2, s1);
   DG_LAUNCHED();
   const double2 *pr[2] = {s0, s1};
   DG_TRY(per_to_physical(h, pr, 2, W));
@@ -588,10 +599,10 @@ extern "C" int diablo_poisson_p_per(dg_handle *h) {
   struct G { int src, axis; } g[6] = {{0, 1}, {1, 0}, {0, 2}, {2, 0}, {1, 2}, {2, 1}};
   for (int k = 0; k < 6; k += 2) {
     dg_kt_begin(h, "k_ik", h->st);
-    k_ik<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[g[k].src], g[k].axis, s0);
+    k_ik<<<dim3(dg_cdiv(h->ss, 256), h->nkyt), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[g[k].src], g[k].axis, s0);
     DG_LAUNCHED();
     dg_kt_begin(h, "k_ik", h->st);
-    k_ik<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[g[k + 1].src],
+    k_ik<<<dim3(dg_cdiv(h->ss, 256), h->nkyt), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[g[k + 1].src],
                                                g[k + 1].axis, s1);
     DG_LAUNCHED();
     DG_TRY(per_to_physical(h, pr, 2, W + k * n));
@@ -603,7 +614,7 @@ extern "C" int diablo_poisson_p_per(dg_handle *h) {
   double2 *out[1] = {h->cp};
   DG_TRY(per_to_fourier(h, W, 1, out));
   dg_kt_begin(h, "k_pp_solve", h->st);
-  k_pp_solve<<<dg_cdiv(tot, 256), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cp);
+  k_pp_solve<<<dim3(dg_cdiv(h->ss, 256), h->nkyt), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cp);
   DG_LAUNCHED();
   return DG_OK;
 }
@@ -657,7 +668,7 @@ int dg_per_stats(dg_handle *h, dg_stats *s) {
   // max |div u| in physical space
   const long tot_m = (long)h->nkyt * h->ss;
   dg_kt_begin(h, "k_div_per", h->st);
-  k_div_per<<<dg_cdiv(tot_m, 256), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[0], h->cu[1],
+  k_div_per<<<dim3(dg_cdiv(h->ss, 256), h->nkyt), 256, 0, h->st>>>(C, h->kx, h->ky, h->kz, h->cu[0], h->cu[1],
                                                     h->cu[2], h->rhs[0]);
   DG_LAUNCHED();
   const double2 *d[1] = {h->rhs[0]};

@@ -242,6 +242,26 @@ def test_poisson_p_chan_matches_oracle(case):
     ch.close()
 
 
+@pytest.mark.parametrize("case", ["tall_ny257", "wide_512x384"])
+def test_channel_large_dims_short(case):
+    """NY = 257 (the CN row templates of four fields exceed 48 KB) and the
+    512 x 384 plane of the Re_tau=550 configuration (x and z lengths without a
+    warp-level kernel), a few steps each."""
+    if case == "tall_ny257":
+        p, gy = configs.kh_shear_layer(nx=32, ny=257, nz=16)
+        nsteps = 4
+    else:
+        p, gy = configs.channel_re550(ny=17)
+        nsteps = 2
+    maker = ics.kh_shear_layer if case == "tall_ny257" else ics.channel_laminar
+    ref, ch, _ = start_pair(p, gy, maker, seed=13)
+    for s in range(1, nsteps + 1):
+        ref.step(s)
+        ch.step(s)
+    compare(ref, ch, fields(p))
+    ch.close()
+
+
 def test_courant_matches_oracle():
     p, gy = configs.channel_re180(nx=64, ny=65, nz=64)
     ref, ch, _ = start_pair(p, gy, ics.channel_laminar, seed=9)

@@ -179,33 +179,51 @@ __global__ void k_prod_phys(const double *__restrict__ phys, long pf, int nth, l
 
 // --------------------------------------------------------------- final
 // RK_PER_1 (for/periodic.f:36-281) per retained mode, after the transforms.
-__global__ void k_per_final(PerConst C, int rk_step, const double *__restrict__ dscal,
-                            const double *__restrict__ kxv, const double *__restrict__ kyv,
-                            const double *__restrict__ kzv, const double2 *__restrict__ Fy,
-                            long Ffield, FieldPtrs cu, FieldPtrs cf, double2 *__restrict__ cp,
-                            double2 *__restrict__ phi, double forcing) {
+template <int NTHM>
+__global__ void __launch_bounds__(256) k_per_final(
+    PerConst C, int rk_step, const double *__restrict__ dscal, const double *__restrict__ kxv,
+    const double *__restrict__ kyv, const double *__restrict__ kzv,
+    const double2 *__restrict__ Fy, long Ffield, FieldPtrs cu, FieldPtrs cf,
+    double2 *__restrict__ cp, double2 *__restrict__ phi, double forcing) {
   // grid: x over the modes of a ky plane, y over the ky planes
   const int jy = blockIdx.y;
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= (int)C.ss) return;
   const long q = (long)jy * C.ss + m;
   const int kz = m / C.nkxp, kx = m - kz * C.nkxp;
+  // every load of the mode first (the stores below could alias them, so a
+  // load placed after a store would wait for the previous load's latency)
+  double2 Fp[6 + 3 * (NTHM > 0 ? NTHM : 1)], u[3], old[3], t[NTHM > 0 ? NTHM : 1],
+      oldt[NTHM > 0 ? NTHM : 1];
+#pragma unroll
+  for (int p = 0; p < 6; p++) Fp[p] = __ldg(Fy + p * Ffield + q);
+#pragma unroll
+  for (int d = 0; d < 3; d++) u[d] = __ldg(cu(d) + q);
+  const bool hist = rk_step > 1;
+#pragma unroll
+  for (int d = 0; d < 3; d++) old[d] = hist ? __ldg(cf(d) + q) : make_double2(0.0, 0.0);
+#pragma unroll
+  for (int n = 0; n < NTHM; n++) {
+    if (n < C.nth) {
+      t[n] = __ldg(cu(3 + n) + q);
+      oldt[n] = hist ? __ldg(cf(3 + n) + q) : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int r = 0; r < 3; r++) Fp[6 + 3 * n + r] = __ldg(Fy + (6 + 3 * n + r) * Ffield + q);
+    }
+  }
+  const double2 p0 = __ldg(cp + q);
   const double KX = kxv[kx], KY = kyv[jy], KZ = kzv[kz];
   const double k2 = KX * KX + KY * KY + KZ * KZ;
   const double h = dscal[1 + rk_step];
   const double zeta = (rk_step == 2) ? -17.0 / 8.0 : (rk_step == 3) ? -5.0 / 4.0 : 0.0;
   const double bbar = (rk_step == 2) ? 25.0 / 8.0 : (rk_step == 3) ? 9.0 / 4.0 : 1.0;
   const double T1 = C.nu * h / 2.0, T2 = bbar * h, T3 = zeta * h, T4 = h;
-  auto F = [&](int p) { return Fy[p * Ffield + q]; };
   // -i k . (f_a, f_b, f_c) = (KX Im a + KY Im b + KZ Im c, -(KX Re a + KY Re b + KZ Re c))
   auto mdiv = [&](double2 a, double2 b, double2 c) {
     return make_double2(KX * a.y + KY * b.y + KZ * c.y, -(KX * a.x + KY * b.x + KZ * c.x));
   };
-  const double2 f0 = F(0), f1 = F(1), f2 = F(2), f3 = F(3), f4 = F(4), f5 = F(5);
-  double2 nf[3] = {mdiv(f0, f1, f2), mdiv(f1, f3, f4), mdiv(f2, f4, f5)};
-  double2 u[3], p0 = cp[q];
-#pragma unroll
-  for (int d = 0; d < 3; d++) u[d] = cu(d)[q];
+  double2 nf[3] = {mdiv(Fp[0], Fp[1], Fp[2]), mdiv(Fp[1], Fp[3], Fp[4]),
+                   mdiv(Fp[2], Fp[4], Fp[5])};
   // USER_RHS_PER_PHYSICAL: CF_i += (EPSILON_TARGET / EK) U_i (exact in
   // spectral space for band-limited U)
   if (forcing != 0.0) {
@@ -213,11 +231,11 @@ __global__ void k_per_final(PerConst C, int rk_step, const double *__restrict__ 
     for (int d = 0; d < 3; d++) { nf[d].x += forcing * u[d].x; nf[d].y += forcing * u[d].y; }
   }
 #pragma unroll
-  for (int n = 0; n < DG_MAX_TH; n++) {
-    if (n >= C.nth) break;
-    const double2 t = cu(3 + n)[q];
-    nf[1].x += C.ri[n] * t.x;
-    nf[1].y += C.ri[n] * t.y;
+  for (int n = 0; n < NTHM; n++) {
+    if (n < C.nth) {
+      nf[1].x += C.ri[n] * t[n].x;
+      nf[1].y += C.ri[n] * t[n].y;
+    }
   }
   // one reciprocal per mode instead of a division per component
   const double t5 = 1 - T1 * k2, it5 = 1.0 / (1 + T1 * k2);
@@ -227,35 +245,32 @@ __global__ void k_per_final(PerConst C, int rk_step, const double *__restrict__ 
   for (int d = 0; d < 3; d++) {
     // CR = (1 - T1 k^2) CU - h (i k_d CP) [+ zeta h CF_old] + beta h CF
     double2 r = make_double2(t5 * u[d].x - T4 * (-Kd[d] * p0.y), t5 * u[d].y - T4 * (Kd[d] * p0.x));
-    if (rk_step > 1) {
-      const double2 o = cf(d)[q];
-      r.x += T3 * o.x;
-      r.y += T3 * o.y;
+    if (hist) {
+      r.x += T3 * old[d].x;
+      r.y += T3 * old[d].y;
     }
     r.x += T2 * nf[d].x;
     r.y += T2 * nf[d].y;
     un[d] = make_double2(r.x * it5, r.y * it5);
-    cf(d)[q] = nf[d];
   }
 #pragma unroll
-  for (int n = 0; n < DG_MAX_TH; n++) {
-    if (n >= C.nth) break;
-    const double2 t = cu(3 + n)[q];
-    double2 ft = C.bg[n] ? make_double2(-u[1].x, -u[1].y) : make_double2(0.0, 0.0);
-    const double2 g = mdiv(F(6 + 3 * n), F(7 + 3 * n), F(8 + 3 * n));
-    ft.x += g.x;
-    ft.y += g.y;
-    const double t6 = 1 - (T1 / C.pr[n]) * k2, it6 = 1.0 / (1 + (T1 / C.pr[n]) * k2);
-    double2 r = make_double2(t6 * t.x, t6 * t.y);
-    if (rk_step > 1) {
-      const double2 o = cf(3 + n)[q];
-      r.x += T3 * o.x;
-      r.y += T3 * o.y;
+  for (int n = 0; n < NTHM; n++) {
+    if (n < C.nth) {
+      double2 ft = C.bg[n] ? make_double2(-u[1].x, -u[1].y) : make_double2(0.0, 0.0);
+      const double2 g = mdiv(Fp[6 + 3 * n], Fp[7 + 3 * n], Fp[8 + 3 * n]);
+      ft.x += g.x;
+      ft.y += g.y;
+      const double t6 = 1 - (T1 / C.pr[n]) * k2, it6 = 1.0 / (1 + (T1 / C.pr[n]) * k2);
+      double2 r = make_double2(t6 * t[n].x, t6 * t[n].y);
+      if (hist) {
+        r.x += T3 * oldt[n].x;
+        r.y += T3 * oldt[n].y;
+      }
+      r.x += T2 * ft.x;
+      r.y += T2 * ft.y;
+      cu(3 + n)[q] = make_double2(r.x * it6, r.y * it6);
+      cf(3 + n)[q] = ft;
     }
-    r.x += T2 * ft.x;
-    r.y += T2 * ft.y;
-    cu(3 + n)[q] = make_double2(r.x * it6, r.y * it6);
-    cf(3 + n)[q] = ft;
   }
   // REM_DIV_PER: phi = (i k . U) / -(k^2 + EPS); U -= i k phi; CP += phi / h
   const double iden = 1.0 / -(KX * KX + KY * KY + KZ * KZ + C.eps);
@@ -267,6 +282,7 @@ __global__ void k_per_final(PerConst C, int rk_step, const double *__restrict__ 
     un[d].x -= -Kd[d] * ph.y;
     un[d].y -= Kd[d] * ph.x;
     cu(d)[q] = un[d];
+    cf(d)[q] = nf[d];
   }
   phi[q] = ph;
   const double iT4 = 1.0 / T4;
@@ -555,9 +571,14 @@ extern "C" int diablo_rk_per_1(dg_handle *h, int rk_step) {
   for (int f = 0; f < nf; f++) { cu.p[f] = h->cu[f]; cf.p[f] = h->cf[f]; }
   const long tot = (long)h->nkyt * h->ss;
   dg_kt_begin(h, "k_per_final", h->st);
-  k_per_final<<<dim3(dg_cdiv(h->ss, 256), h->nkyt), 256, 0, h->st>>>(C, rk_step, h->dscal, h->kx, h->ky, h->kz,
-                                                    h->Q, fy_field(h), cu, cf, h->cp, h->cr1,
-                                                    forcing);
+  const int nthm = h->NTH == 0 ? 0 : (h->NTH == 1 ? 1 : (h->NTH == 2 ? 2 : 4));
+#define PF_CASE(NM)                                                                             \
+  if (nthm == NM)                                                                               \
+    k_per_final<NM><<<dim3(dg_cdiv(h->ss, 256), h->nkyt), 256, 0, h->st>>>(                     \
+        C, rk_step, h->dscal, h->kx, h->ky, h->kz, h->Q, fy_field(h), cu, cf, h->cp, h->cr1,    \
+        forcing);
+  PF_CASE(0) PF_CASE(1) PF_CASE(2) PF_CASE(4)
+#undef PF_CASE
   DG_LAUNCHED();
   return DG_OK;
 }

@@ -329,8 +329,13 @@ def run_gpu(args):
         ch.advance_time()
 
     # launch shapes: the library's autotuner times candidates on this state
-    # and restores it (part of set-up, outside the timed region)
-    tuned = ch.autotune(3)
+    # and restores it (part of set-up, outside the timed region); --tuning
+    # fixes them instead (for profiling runs that must not time the tuner)
+    if args.tuning:
+        ch.tune_set(**{k: int(v) for k, v in (kv.split("=") for kv in args.tuning.split(","))})
+        tuned = ch.tune_get()
+    else:
+        tuned = ch.autotune(3)
     ts = 0
     for _ in range(args.warmup):
         ts += 1
@@ -483,6 +488,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--tuning", default="",
+                    help="fixed launch shapes, e.g. col_mt=8,cn_mt=16,xrow_chunk=0,ychunk=0")
     ap.add_argument("--ensemble-cases", type=int, default=256)
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--ensemble-rate", type=float, default=20.0)

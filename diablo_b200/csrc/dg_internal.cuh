@@ -98,7 +98,7 @@ struct dg_handle {
   // device tables
   double *gyf, *dy, *dyf, *kx, *kz, *ky, *kx2, *kz2, *ky2;
   double2 *twx, *twz, *twy;     // exp(-2 pi i m / N) for the x, z, y lengths
-  float2 *twx_f, *twz_f;        // the same in FP32 (mixed path)
+  float2 *twx_f, *twz_f, *twy_f;  // the same in FP32 (mixed path)
   int mixed;                    // dg_params.precision == 1
   FftPlan plx, plz, ply;
 
@@ -147,6 +147,7 @@ struct dg_handle {
 
 int dg_default_col_mt(const dg_handle *h);
 bool dg_mixed_ok(int nx, int nz, int n_th);
+bool dg_per_mixed_ok(int nx, int n_th);
 
 void dg_graphs_free(dg_handle *h);
 
@@ -168,6 +169,12 @@ int dg_cinv_g(dg_handle *h, const double2 *const *fields, int nf, int jmin, int 
 int dg_cinv_gf(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax,
                long in_plane, int rowlen, int N, int NK, const FftPlan &pl, const float2 *tw,
                float2 *H, long out_field);
+int dg_cinv_ff(dg_handle *h, const float2 *const *fields, int nf, int jmin, int jmax,
+               long in_plane, int rowlen, int N, int NK, const FftPlan &pl, const float2 *tw,
+               float2 *H, long out_field);
+int dg_cfwd_ff(dg_handle *h, const float2 *H, long in_field, int nf, int jmin, int jmax,
+               int rowlen, int nkt, int N, int NK, const FftPlan &pl, const float2 *tw,
+               float2 *const *fields, long out_plane);
 int dg_cfwd_g(dg_handle *h, const double2 *H, long in_field, int nf, int jmin, int jmax,
               int rowlen, int nkt, int N, int NK, const FftPlan &pl, const double2 *tw,
               double2 *const *fields, long out_plane);

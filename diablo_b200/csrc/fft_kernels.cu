@@ -13,6 +13,7 @@
 // imaginary parts of the x-DC and x-Nyquist bins are ignored by the c2r, as in
 // FFTW's complex-to-real.
 #include <mutex>
+#include <type_traits>
 #include <unordered_set>
 
 #include "dg_internal.cuh"
@@ -36,8 +37,8 @@ __device__ __forceinline__ int packed_index(int z, int NZ, int NKZ) {
   return -1;
 }
 
-template <int NT, typename CX>
-__global__ void __launch_bounds__(NTHR) k_zinv(CFieldPtrs fields, int jmin, long ss, int nkxp,
+template <int NT, typename CX, typename PA = CFieldPtrs>
+__global__ void __launch_bounds__(NTHR) k_zinv(PA fields, int jmin, long ss, int nkxp,
                                               int NZr, int NKZ, FftPlan pl,
                                               const CX *__restrict__ tw,
                                               CX *__restrict__ H, long Hfield) {
@@ -53,17 +54,18 @@ __global__ void __launch_bounds__(NTHR) k_zinv(CFieldPtrs fields, int jmin, long
   const int j = jmin + blockIdx.y;
   const int f = blockIdx.z;
   const int tid = threadIdx.x, nthr = blockDim.x;
-  const double2 *in = fields(f) + (long)j * ss;
+  const auto *in = fields(f) + (long)j * ss;
   for (int i = tid; i < NZ; i += nthr) stw[i] = tw[i];
   for (int base = 0; base < KXG * NZ; base += 8 * nthr) {
-    double2 v[8];
+    using CI = typename std::remove_const<typename std::remove_pointer<decltype(in)>::type>::type;
+    CI v[8];
+    const CI zero{};
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       const int idx = base + u * nthr + tid;
       const int c = idx % KXG, z = idx / KXG;
       const int kp = packed_index(z, NZ, NKZ);
-      v[u] = (idx < KXG * NZ && kp >= 0 && kx0 + c < nkxp) ? in[(long)kp * nkxp + kx0 + c]
-                                                          : make_double2(0.0, 0.0);
+      v[u] = (idx < KXG * NZ && kp >= 0 && kx0 + c < nkxp) ? in[(long)kp * nkxp + kx0 + c] : zero;
     }
 #pragma unroll
     for (int u = 0; u < 8; u++) {
@@ -82,32 +84,32 @@ __global__ void __launch_bounds__(NTHR) k_zinv(CFieldPtrs fields, int jmin, long
   }
 }
 
-template <int NT>
-__global__ void __launch_bounds__(NTHR) k_zfwd(const double2 *__restrict__ H, long Hfield, int jmin,
+template <int NT, typename CX = double2, typename PO = FieldPtrs>
+__global__ void __launch_bounds__(NTHR) k_zfwd(const CX *__restrict__ H, long Hfield, int jmin,
                                               int nkxp, int nkzt, int NZr, int NKZ, FftPlan pl,
-                                              const double2 *__restrict__ tw, FieldPtrs fields,
+                                              const CX *__restrict__ tw, PO fields,
                                               long ss) {
-  extern __shared__ double2 sm[];
+  extern __shared__ double2 sm_raw[];
+  CX *sm = reinterpret_cast<CX *>(sm_raw);
   const int NZ = NT ? NT : NZr;
   const int KXG = batch_for(NZ);
   const int sstr = padded_len(NZ);
-  double2 *stw = sm;
-  double2 *b0 = stw + NZ;
-  double2 *b1 = b0 + KXG * sstr;
+  CX *stw = sm;
+  CX *b0 = stw + NZ;
+  CX *b1 = b0 + KXG * sstr;
   const int kx0 = blockIdx.x * KXG;
   const int j = jmin + blockIdx.y;
   const int f = blockIdx.z;
   const int tid = threadIdx.x, nthr = blockDim.x;
-  const double2 *in = H + f * Hfield + (long)j * NZ * nkxp;
+  const CX *in = H + f * Hfield + (long)j * NZ * nkxp;
   for (int i = tid; i < NZ; i += nthr) stw[i] = tw[i];
   for (int base = 0; base < KXG * NZ; base += 8 * nthr) {
-    double2 v[8];
+    CX v[8];
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       const int idx = base + u * nthr + tid;
       const int c = idx % KXG, z = idx / KXG;
-      v[u] = (idx < KXG * NZ && kx0 + c < nkxp) ? in[(long)z * nkxp + kx0 + c]
-                                                : make_double2(0.0, 0.0);
+      v[u] = (idx < KXG * NZ && kx0 + c < nkxp) ? in[(long)z * nkxp + kx0 + c] : CT<CX>::mk(0, 0);
     }
 #pragma unroll
     for (int u = 0; u < 8; u++) {
@@ -116,15 +118,17 @@ __global__ void __launch_bounds__(NTHR) k_zfwd(const double2 *__restrict__ H, lo
     }
   }
   __syncthreads();
-  double2 *res = fft_cta<NT>(b0, b1, pl, KXG, sstr, stw, -1);
-  double2 *out = fields(f) + (long)j * ss;
+  CX *res = fft_cta<NT>(b0, b1, pl, KXG, sstr, stw, -1);
+  auto *out = fields(f) + (long)j * ss;
+  using CO = typename std::remove_pointer<decltype(out)>::type;
+  using TO = typename CT<CO>::T;
   const double rnz = (double)NZ;
   for (int idx = tid; idx < KXG * nkzt; idx += nthr) {
     const int c = idx % KXG, kp = idx / KXG;
     if (kx0 + c >= nkxp) continue;
     const int z = (kp <= NKZ) ? kp : (NZ - 1 + (kp - NKZ) - NKZ);
-    const double2 v = res[c * sstr + pad(z)];
-    out[(long)kp * nkxp + kx0 + c] = make_double2(v.x / rnz, v.y / rnz);
+    const CX v = res[c * sstr + pad(z)];
+    out[(long)kp * nkxp + kx0 + c] = CT<CO>::mk((TO)((double)v.x / rnz), (TO)((double)v.y / rnz));
   }
 }
 
@@ -336,19 +340,20 @@ void big_smem(K kern) {
 // at + kp*rowlen + c; output plane j at H + f*out_field + j*N*rowlen, bin z of
 // column c at + z*rowlen + c.  z transforms: rowlen = NKX+1, planes = y;
 // y transforms (periodic): rowlen = modes per ky-plane, one plane.
-template <typename CX>
-static int cinv_t(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax,
+template <typename CI, typename CX>
+static int cinv_t(dg_handle *h, const CI *const *fields, int nf, int jmin, int jmax,
                   long in_plane, int rowlen, int N, int NK, const FftPlan &pl, const CX *tw, CX *H,
                   long out_field) {
+  using PA = PtrArray<const CI>;
   if (jmax < jmin || nf <= 0) return DG_OK;
-  CFieldPtrs fp;
+  PA fp;
   for (int f = 0; f < nf; f++) fp.p[f] = fields[f];
   dim3 grid(dg_cdiv(rowlen, batch_for(N)), jmax - jmin + 1, nf);
   const size_t sm = zsmem(N, sizeof(CX));
 #define KERNEL_BODY(NN)                                                                       \
-  big_smem(k_zinv<NN, CX>);                                                                   \
+  big_smem(k_zinv<NN, CX, PA>);                                                               \
   dg_kt_begin(h, "k_zinv", h->st);                                                            \
-  k_zinv<NN, CX><<<grid, NTHR, sm, h->st>>>(fp, jmin, in_plane, rowlen, N, NK, pl, tw, H, out_field)
+  k_zinv<NN, CX, PA><<<grid, NTHR, sm, h->st>>>(fp, jmin, in_plane, rowlen, N, NK, pl, tw, H, out_field)
   switch (N) {
     DG_FOR_EACH_N(DG_CASE_N)
     default: KERNEL_BODY(0); break;
@@ -370,18 +375,26 @@ int dg_cinv_gf(dg_handle *h, const double2 *const *fields, int nf, int jmin, int
   return cinv_t(h, fields, nf, jmin, jmax, in_plane, rowlen, N, NK, pl, tw, H, out_field);
 }
 
-int dg_cfwd_g(dg_handle *h, const double2 *H, long in_field, int nf, int jmin, int jmax,
-              int rowlen, int nkt, int N, int NK, const FftPlan &pl, const double2 *tw,
-              double2 *const *fields, long out_plane) {
+int dg_cinv_ff(dg_handle *h, const float2 *const *fields, int nf, int jmin, int jmax,
+               long in_plane, int rowlen, int N, int NK, const FftPlan &pl, const float2 *tw,
+               float2 *H, long out_field) {
+  return cinv_t(h, fields, nf, jmin, jmax, in_plane, rowlen, N, NK, pl, tw, H, out_field);
+}
+
+template <typename CX, typename PO, typename OUT>
+static int cfwd_t(dg_handle *h, const CX *H, long in_field, int nf, int jmin, int jmax, int rowlen,
+                  int nkt, int N, int NK, const FftPlan &pl, const CX *tw, OUT *const *fields,
+                  long out_plane) {
   if (jmax < jmin || nf <= 0) return DG_OK;
-  FieldPtrs fp;
+  PO fp;
   for (int f = 0; f < nf; f++) fp.p[f] = fields[f];
   dim3 grid(dg_cdiv(rowlen, batch_for(N)), jmax - jmin + 1, nf);
-  const size_t sm = zsmem(N);
+  const size_t sm = zsmem(N, sizeof(CX));
 #define KERNEL_BODY(NN)                                                                        \
-  big_smem(k_zfwd<NN>);                                                                        \
-  dg_kt_begin(h, "k_zfwd", h->st);                                                              \
-  k_zfwd<NN><<<grid, NTHR, sm, h->st>>>(H, in_field, jmin, rowlen, nkt, N, NK, pl, tw, fp, out_plane)
+  big_smem(k_zfwd<NN, CX, PO>);                                                                \
+  dg_kt_begin(h, "k_zfwd", h->st);                                                             \
+  k_zfwd<NN, CX, PO><<<grid, NTHR, sm, h->st>>>(H, in_field, jmin, rowlen, nkt, N, NK, pl, tw, fp, \
+                                               out_plane)
   switch (N) {
     DG_FOR_EACH_N(DG_CASE_N)
     default: KERNEL_BODY(0); break;
@@ -389,6 +402,20 @@ int dg_cfwd_g(dg_handle *h, const double2 *H, long in_field, int nf, int jmin, i
 #undef KERNEL_BODY
   DG_LAUNCHED();
   return DG_OK;
+}
+
+int dg_cfwd_g(dg_handle *h, const double2 *H, long in_field, int nf, int jmin, int jmax,
+              int rowlen, int nkt, int N, int NK, const FftPlan &pl, const double2 *tw,
+              double2 *const *fields, long out_plane) {
+  return cfwd_t<double2, FieldPtrs>(h, H, in_field, nf, jmin, jmax, rowlen, nkt, N, NK, pl, tw,
+                                    fields, out_plane);
+}
+
+int dg_cfwd_ff(dg_handle *h, const float2 *H, long in_field, int nf, int jmin, int jmax,
+               int rowlen, int nkt, int N, int NK, const FftPlan &pl, const float2 *tw,
+               float2 *const *fields, long out_plane) {
+  return cfwd_t<float2, PtrArray<float2>>(h, H, in_field, nf, jmin, jmax, rowlen, nkt, N, NK, pl,
+                                          tw, fields, out_plane);
 }
 
 int dg_zinv(dg_handle *h, const double2 *const *fields, int nf, int jmin, int jmax, double2 *H,

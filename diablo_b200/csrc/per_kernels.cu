@@ -52,10 +52,10 @@ PerConst make_pc(const dg_handle *h) {
 
 // ----------------------------------------------------------- products (warp)
 // One warp per physical (y, z) row: c2r of the fields, products, r2c.
-template <int NX, int NTH>
-__global__ void __launch_bounds__(128) k_prod_per_w(PerConst C, const double2 *__restrict__ H,
-                                                    long Hfield, const double2 *__restrict__ tw,
-                                                    double2 *__restrict__ Hp, long Pfield) {
+template <int NX, int NTH, typename CX = double2>
+__global__ void __launch_bounds__(128) k_prod_per_w(PerConst C, const CX *__restrict__ H,
+                                                    long Hfield, const CX *__restrict__ tw,
+                                                    CX *__restrict__ Hp, long Pfield) {
   constexpr int NF = 3 + NTH;
   constexpr int NPIN = (NF + 1) / 2;
   constexpr int NPROD = 6 + 3 * NTH;
@@ -65,15 +65,17 @@ __global__ void __launch_bounds__(128) k_prod_per_w(PerConst C, const double2 *_
   constexpr int NKXP = NX / 3 + 1;
   constexpr int KS = (NKXP + 31) / 32;
   constexpr int SSTR = padded_len(NX);
-  extern __shared__ double2 sm[];
-  double2 *stw = sm;
+  extern __shared__ double2 sm_raw[];
+  using T = typename CT<CX>::T;
+  CX *sm = reinterpret_cast<CX *>(sm_raw);
+  CX *stw = sm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double2 *buf = stw + NX + warp * MAXP * SSTR;
+  CX *buf = stw + NX + warp * MAXP * SSTR;
   for (int i = threadIdx.x; i < NX; i += blockDim.x) stw[i] = tw[i];
   __syncthreads();
   const long row = (long)blockIdx.x * 4 + warp;  // row = y * NZ + z
   if (row >= (long)C.NY * C.NZ) return;
-  const double2 *src = H + row * NKXP;
+  const CX *src = H + row * NKXP;
   // c2r of field pairs
 #pragma unroll
   for (int q = 0; q < NPIN; q++) {
@@ -83,12 +85,12 @@ __global__ void __launch_bounds__(128) k_prod_per_w(PerConst C, const double2 *_
       const int k = lane + 32 * i;
       if (k < NX) {
         const int kk = (k <= NX / 2) ? k : NX - k;
-        double2 v = make_double2(0.0, 0.0);
+        CX v = CT<CX>::mk(0, 0);
         if (kk < NKXP && kk < NX / 2) {
-          double2 a = src[fa * Hfield + kk];
-          double2 b = (fb < NF) ? src[fb * Hfield + kk] : make_double2(0.0, 0.0);
+          CX a = src[fa * Hfield + kk];
+          CX b = (fb < NF) ? src[fb * Hfield + kk] : CT<CX>::mk(0, 0);
           if (kk == 0) { a.y = 0.0; b.y = 0.0; }
-          v = (k == kk) ? make_double2(a.x - b.y, a.y + b.x) : make_double2(a.x + b.y, -a.y + b.x);
+          v = (k == kk) ? CT<CX>::mk(a.x - b.y, a.y + b.x) : CT<CX>::mk(a.x + b.y, -a.y + b.x);
         }
         buf[q * SSTR + pad(k)] = v;
       }
@@ -96,13 +98,13 @@ __global__ void __launch_bounds__(128) k_prod_per_w(PerConst C, const double2 *_
   }
   __syncwarp();
   wpasses<NX, +1, 0>(buf, NPIN, SSTR, stw, lane);
-  double u[NF][XPL];
+  T u[NF][XPL];
 #pragma unroll
   for (int q = 0; q < NPIN; q++)
 #pragma unroll
     for (int i = 0; i < XPL; i++) {
       const int x = lane + 32 * i;
-      const double2 v = (x < NX) ? buf[q * SSTR + pad(x)] : make_double2(0.0, 0.0);
+      const CX v = (x < NX) ? buf[q * SSTR + pad(x)] : CT<CX>::mk(0, 0);
       u[2 * q][i] = v.x;
       if (2 * q + 1 < NF) u[2 * q + 1][i] = v.y;
     }
@@ -111,8 +113,8 @@ __global__ void __launch_bounds__(128) k_prod_per_w(PerConst C, const double2 *_
   for (int i = 0; i < XPL; i++) {
     const int x = lane + 32 * i;
     if (x >= NX) continue;
-    const double u1 = u[0][i], u2 = u[1][i], u3 = u[2][i];
-    double P[2 * NPP];
+    const T u1 = u[0][i], u2 = u[1][i], u3 = u[2][i];
+    T P[2 * NPP];
     P[0] = u1 * u1;
     P[1] = u1 * u2;
     P[2] = u1 * u3;
@@ -121,18 +123,18 @@ __global__ void __launch_bounds__(128) k_prod_per_w(PerConst C, const double2 *_
     P[5] = u3 * u3;
 #pragma unroll
     for (int n = 0; n < NTH; n++) {
-      const double t = u[3 + n][i];
+      const T t = u[3 + n][i];
       P[6 + 3 * n] = u1 * t;
       P[7 + 3 * n] = u2 * t;
       P[8 + 3 * n] = u3 * t;
     }
     if (2 * NPP > NPROD) P[2 * NPP - 1] = 0.0;
 #pragma unroll
-    for (int q = 0; q < NPP; q++) buf[q * SSTR + pad(x)] = make_double2(P[2 * q], P[2 * q + 1]);
+    for (int q = 0; q < NPP; q++) buf[q * SSTR + pad(x)] = CT<CX>::mk(P[2 * q], P[2 * q + 1]);
   }
   __syncwarp();
   wpasses<NX, -1, 0>(buf, NPP, SSTR, stw, lane);
-  double2 *dst = Hp + row * NKXP;
+  CX *dst = Hp + row * NKXP;
 #pragma unroll
   for (int s = 0; s < KS; s++) {
     const int k = lane + 32 * s;
@@ -140,21 +142,21 @@ __global__ void __launch_bounds__(128) k_prod_per_w(PerConst C, const double2 *_
 #pragma unroll
     for (int p = 0; p < NPROD; p++) {
       const int q = p >> 1;
-      const double2 zk = buf[q * SSTR + pad(k)];
-      const double2 zm = buf[q * SSTR + pad((NX - k) % NX)];
-      double2 v;
-      if ((p & 1) == 0) v = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
-      else v = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
-      dst[p * Pfield + k] = make_double2(v.x / (double)NX, v.y / (double)NX);
+      const CX zk = buf[q * SSTR + pad(k)];
+      const CX zm = buf[q * SSTR + pad((NX - k) % NX)];
+      CX v;
+      if ((p & 1) == 0) v = CT<CX>::mk((T)0.5 * (zk.x + zm.x), (T)0.5 * (zk.y - zm.y));
+      else v = CT<CX>::mk((T)0.5 * (zk.y + zm.y), -(T)0.5 * (zk.x - zm.x));
+      dst[p * Pfield + k] = CT<CX>::mk(v.x / (T)NX, v.y / (T)NX);
     }
   }
 }
 
-template <int NX, int NTH>
+template <int NX, int NTH, typename CX = double2>
 size_t prod_smem() {
   constexpr int NF = 3 + NTH, NPIN = (NF + 1) / 2, NPP = (6 + 3 * NTH + 1) / 2;
   constexpr int MAXP = NPIN > NPP ? NPIN : NPP;
-  return sizeof(double2) * (NX + 4 * MAXP * padded_len(NX));
+  return sizeof(CX) * (NX + 4 * MAXP * padded_len(NX));
 }
 
 // generic products from physical fields (any NX): phys [f][y][z][x] -> prod [p][y][z][x]
@@ -179,11 +181,18 @@ __global__ void k_prod_phys(const double *__restrict__ phys, long pf, int nth, l
 
 // --------------------------------------------------------------- final
 // RK_PER_1 (for/periodic.f:36-281) per retained mode, after the transforms.
-template <int NTHM>
+// product spectra in the working precision, widened to FP64
+__device__ __forceinline__ double2 ldF(const double2 *p) { return __ldg(p); }
+__device__ __forceinline__ double2 ldF(const float2 *p) {
+  const float2 v = __ldg(p);
+  return make_double2((double)v.x, (double)v.y);
+}
+
+template <int NTHM, typename CF = double2>
 __global__ void __launch_bounds__(256) k_per_final(
     PerConst C, int rk_step, const double *__restrict__ dscal, const double *__restrict__ kxv,
     const double *__restrict__ kyv, const double *__restrict__ kzv,
-    const double2 *__restrict__ Fy, long Ffield, FieldPtrs cu, FieldPtrs cf,
+    const CF *__restrict__ Fy, long Ffield, FieldPtrs cu, FieldPtrs cf,
     double2 *__restrict__ cp, double2 *__restrict__ phi, double forcing) {
   // grid: x over the modes of a ky plane, y over the ky planes
   const int jy = blockIdx.y;
@@ -196,7 +205,7 @@ __global__ void __launch_bounds__(256) k_per_final(
   double2 Fp[6 + 3 * (NTHM > 0 ? NTHM : 1)], u[3], old[3], t[NTHM > 0 ? NTHM : 1],
       oldt[NTHM > 0 ? NTHM : 1];
 #pragma unroll
-  for (int p = 0; p < 6; p++) Fp[p] = __ldg(Fy + p * Ffield + q);
+  for (int p = 0; p < 6; p++) Fp[p] = ldF(Fy + p * Ffield + q);
 #pragma unroll
   for (int d = 0; d < 3; d++) u[d] = __ldg(cu(d) + q);
   const bool hist = rk_step > 1;
@@ -208,7 +217,7 @@ __global__ void __launch_bounds__(256) k_per_final(
       t[n] = __ldg(cu(3 + n) + q);
       oldt[n] = hist ? __ldg(cf(3 + n) + q) : make_double2(0.0, 0.0);
 #pragma unroll
-      for (int r = 0; r < 3; r++) Fp[6 + 3 * n + r] = __ldg(Fy + (6 + 3 * n + r) * Ffield + q);
+      for (int r = 0; r < 3; r++) Fp[6 + 3 * n + r] = ldF(Fy + (6 + 3 * n + r) * Ffield + q);
     }
   }
   const double2 p0 = __ldg(cp + q);
@@ -503,12 +512,86 @@ static int per_forcing(dg_handle *h, double *coef) {
   return DG_OK;
 }
 
+// Mixed form of the transforms and products of a periodic substep: the y
+// inverse converts the FP64 state to FP32, everything up to the product
+// spectra Fy runs in FP32, and the completion kernel widens Fy to FP64.
+static int per_nonlinear_mixed(dg_handle *h, const PerConst &C) {
+  const int nf = h->nf, np = C.np;
+  float2 *Hyf = reinterpret_cast<float2 *>(h->Hy), *Hf = reinterpret_cast<float2 *>(h->H);
+  float2 *Pf = reinterpret_cast<float2 *>(h->P), *Qf = reinterpret_cast<float2 *>(h->Q);
+  const double2 *in[3 + DG_MAX_TH];
+  for (int f = 0; f < nf; f++) in[f] = h->cu[f];
+  DG_TRY(dg_cinv_gf(h, in, nf, 0, 0, 0, (int)h->ss, h->NY, h->NKY, h->ply, h->twy_f, Hyf,
+                    hy_field(h)));
+  const float2 *hy[3 + DG_MAX_TH];
+  for (int f = 0; f < nf; f++) hy[f] = Hyf + f * hy_field(h);
+  DG_TRY(dg_cinv_ff(h, hy, nf, 0, h->NY - 1, h->ss, h->nkxp, h->NZ, h->NKZ, h->plz, h->twz_f, Hf,
+                    h_field(h)));
+  bool done = false;
+  const long rows = (long)h->NY * h->NZ;
+#define PW_CASE(NXV, NTHV)                                                                      \
+  if (!done && h->NX == NXV && h->NTH == NTHV) {                                                \
+    dg_big_smem((const void *)k_prod_per_w<NXV, NTHV, float2>);                                 \
+    dg_kt_begin(h, "k_prod_per_w_f32", h->st);                                                  \
+    k_prod_per_w<NXV, NTHV, float2><<<dg_cdiv(rows, 4), 128, prod_smem<NXV, NTHV, float2>(),    \
+                                      h->st>>>(C, Hf, h_field(h), h->twx_f, Pf, h_field(h));    \
+    done = true;                                                                                \
+  }
+#define PW_ALL(NXV) PW_CASE(NXV, 0) PW_CASE(NXV, 1) PW_CASE(NXV, 2)
+  PW_ALL(16) PW_ALL(32) PW_ALL(48) PW_ALL(64) PW_ALL(96) PW_ALL(128) PW_ALL(256)
+#undef PW_ALL
+#undef PW_CASE
+  if (!done) {
+    dg_set_error("mixed precision: no FP32 product kernel for this NX / N_TH");
+    return DG_ERR_DIMS;
+  }
+  DG_LAUNCHED();
+  float2 *qz[6 + 3 * DG_MAX_TH], *fy[6 + 3 * DG_MAX_TH];
+  for (int p = 0; p < np; p++) {
+    qz[p] = Hyf + p * hy_field(h);
+    fy[p] = Qf + p * fy_field(h);
+  }
+  for (int p0 = 0; p0 < np; p0 += 3 + DG_MAX_TH) {
+    const int cnt = (np - p0) < 3 + DG_MAX_TH ? (np - p0) : 3 + DG_MAX_TH;
+    DG_TRY(dg_cfwd_ff(h, Pf + p0 * h_field(h), h_field(h), cnt, 0, h->NY - 1, h->nkxp, h->nkzt,
+                      h->NZ, h->NKZ, h->plz, h->twz_f, qz + p0, h->ss));
+  }
+  for (int p0 = 0; p0 < np; p0 += 3 + DG_MAX_TH) {
+    const int cnt = (np - p0) < 3 + DG_MAX_TH ? (np - p0) : 3 + DG_MAX_TH;
+    DG_TRY(dg_cfwd_ff(h, Hyf + p0 * hy_field(h), hy_field(h), cnt, 0, 0, (int)h->ss, h->nkyt,
+                      h->NY, h->NKY, h->ply, h->twy_f, fy + p0, 0));
+  }
+  return DG_OK;
+}
+
+bool dg_per_mixed_ok(int nx, int n_th) {
+  return n_th <= 2 && (nx == 16 || nx == 32 || nx == 48 || nx == 64 || nx == 96 || nx == 128 ||
+                       nx == 256);
+}
+
 extern "C" int diablo_rk_per_1(dg_handle *h, int rk_step) {
   if (!h || !h->periodic || rk_step < 1 || rk_step > 3) return DG_ERR_ARG;
   const PerConst C = make_pc(h);
   const int nf = h->nf, np = C.np;
   double forcing = 0.0;
   DG_TRY(per_forcing(h, &forcing));
+  if (h->mixed) {
+    DG_TRY(per_nonlinear_mixed(h, C));
+    FieldPtrs cu, cf;
+    for (int f = 0; f < nf; f++) { cu.p[f] = h->cu[f]; cf.p[f] = h->cf[f]; }
+    const float2 *Qf = reinterpret_cast<const float2 *>(h->Q);
+    const int nthm = h->NTH == 0 ? 0 : (h->NTH == 1 ? 1 : 2);
+    dg_kt_begin(h, "k_per_final", h->st);
+#define PF_CASE(NM)                                                                             \
+  if (nthm == NM)                                                                               \
+    k_per_final<NM, float2><<<dim3(dg_cdiv(h->ss, 256), h->nkyt), 256, 0, h->st>>>(             \
+        C, rk_step, h->dscal, h->kx, h->ky, h->kz, Qf, fy_field(h), cu, cf, h->cp, h->cr1,      \
+        forcing);
+    PF_CASE(0) PF_CASE(1) PF_CASE(2)
+#undef PF_CASE
+    DG_LAUNCHED();
+    return DG_OK;
+  }
   // y inverse, z inverse
   const double2 *in[3 + DG_MAX_TH];
   for (int f = 0; f < nf; f++) in[f] = h->cu[f];

@@ -148,9 +148,14 @@ static int validate(const dg_params *p, const double *gy) {
       return DG_ERR_DIMS;
     }
   } else {
-    if (p->precision != 0) {
-      dg_set_error("the periodic path runs in FP64 only (precision = 0)");
+    if (p->precision != 0 && p->precision != 1) {
+      dg_set_error("precision must be 0 (FP64) or 1 (mixed)");
       return DG_ERR_ARG;
+    }
+    if (p->precision == 1 && !dg_per_mixed_ok(p->nx, p->n_th)) {
+      dg_set_error("periodic mixed precision needs NX in {16, 32, 48, 64, 96, 128, 256} and "
+                   "N_TH <= 2");
+      return DG_ERR_DIMS;
     }
     if (!dg_make_plan(p->ny, &t) || p->ny < 8) {
       dg_set_error("periodic NY must be >= 8 and factor into 2 and 3");
@@ -316,6 +321,14 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
       DG_CUDA(cudaMemcpyAsync(h->twz_f, tf, sizeof(float2) * h->NZ, cudaMemcpyHostToDevice, h->st));
       free(tf);
     }
+    if (h->periodic && p->precision == 1) {
+      float2 *tf = (float2 *)malloc(sizeof(float2) * nmax);
+      twiddles(h->NY, tmp);
+      for (int m = 0; m < h->NY; m++) tf[m] = make_float2((float)tmp[m].x, (float)tmp[m].y);
+      DG_CUDA(dg_malloc(h, (void **)&h->twy_f, sizeof(float2) * h->NY));
+      DG_CUDA(cudaMemcpyAsync(h->twy_f, tf, sizeof(float2) * h->NY, cudaMemcpyHostToDevice, h->st));
+      free(tf);
+    }
     if (h->periodic) {
       DG_TRY(dalloc(h, &h->twy, h->NY));
       twiddles(h->NY, tmp);
@@ -367,7 +380,7 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
   cudaStreamSynchronize(h->st);
   cudaStreamSynchronize(h->st2);
   void *dp[] = {h->gyf, h->dy, h->dyf, h->kx, h->kz, h->ky, h->kx2, h->kz2, h->ky2, h->twx, h->twz,
-                h->twy, h->twx_f, h->twz_f, h->dscal, h->cp, h->cr1, h->gphi, h->rem_a, h->rem_rb, h->cn_tab, h->cn_rows, h->H, h->G, h->work, h->dmin_bits, h->dflag, h->Hy, h->P,
+                h->twy, h->twx_f, h->twz_f, h->twy_f, h->dscal, h->cp, h->cr1, h->gphi, h->rem_a, h->rem_rb, h->cn_tab, h->cn_rows, h->H, h->G, h->work, h->dmin_bits, h->dflag, h->Hy, h->P,
                 h->Q};
   for (void *q : dp) dg_free(h, q);
   for (int f = 0; f < 3 + DG_MAX_TH; f++) {

@@ -56,8 +56,11 @@ def test_mixed_precision_refuses_unsupported_sizes():
                              g.ctypes.data_as(ctypes.c_void_p), None, ctypes.byref(h))
     assert code == 2  # DG_ERR_DIMS, before any device call
     assert b"mixed precision" in L.dg_last_error()
-    q, _ = configs.periodic_256(n=32)
+    q, _ = configs.periodic_256(n=36)       # no FP32 product kernel for NX = 36
     code = L.diablo_gpu_init(ctypes.byref(q.replace(precision=1).to_struct(DgParams)), None, None,
+                             ctypes.byref(h))
+    assert code == 2
+    code = L.diablo_gpu_init(ctypes.byref(q.replace(precision=2).to_struct(DgParams)), None, None,
                              ctypes.byref(h))
     assert code == 1
 

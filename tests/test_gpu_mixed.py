@@ -1,5 +1,5 @@
-"""Mixed-precision channel path (dg_params.precision = 1) against the FP64
-oracle (needs a B200).
+"""Mixed-precision channel and periodic paths (dg_params.precision = 1)
+against the FP64 oracle (needs a B200).
 
 FFTs, the physical-space products and the x/z transforms of the nonlinear
 terms run in FP32; the explicit-term assembly, the CN and REM_DIV solves, the
@@ -89,5 +89,62 @@ def test_mixed_two_scalars_short():
         ref.step(s)
         g.steps(s, 1)
     err = {nm: rel(g.get_field(nm), ref.get(nm)) for nm in fields(p)}
+    assert all(v <= TOL_MIXED for v in err.values()), err
+    g.close()
+
+
+def periodic_pair(p, seed=3, scalars=None):
+    import math
+    from diablo_b200.solver import Periodic
+    ref = O.Oracle(p, None)
+    for nm, a in zip(("CU1", "CU2", "CU3"), ics.periodic_spectrum(p, seed=seed)):
+        ref.set(nm, a)
+    for n in range(p.n_th):
+        ref.set(f"CTH{n}", 0.5 * ics.periodic_spectrum(p, seed=seed + 10 + n)[0])
+    ref.rem_div_per()
+    ref.poisson_p_per()
+    g = Periodic(p.replace(precision=1))
+    g.set_state(ref.state())
+    g.set_time(0.0, p.delta_t)
+    return ref, g
+
+
+def test_mixed_periodic_64_cubed_100_steps():
+    import math
+    from diablo_b200.params import Params
+    p = Params(nx=64, ny=64, nz=64, num_per_dir=3, nu=5e-3, lx=2 * math.pi, ly=2 * math.pi,
+               lz=2 * math.pi, delta_t=4e-3)
+    ref, g = periodic_pair(p)
+    for s in range(1, 101):
+        ref.step(s)
+        g.steps(s, 1)
+    err = {nm: rel(g.get_field(nm), ref.get(nm)) for nm in fields(p)}
+    assert all(v <= TOL_MIXED for v in err.values()), err
+    so, sg = ref.stats(), g.stats()
+    assert abs(sg["ke"] - so["ke"]) <= 1e-6 * so["ke"]
+    assert sg["div_max"] <= 1e-12 * 64
+    g.close()
+
+
+def test_mixed_periodic_256_cubed_and_scalar():
+    import math
+    from diablo_b200.params import Params
+    p, _ = configs.periodic_256()
+    ref, g = periodic_pair(p)
+    for s in range(1, 6):
+        ref.step(s)
+        g.steps(s, 1)
+    err = {nm: rel(g.get_field(nm), ref.get(nm)) for nm in fields(p)}
+    assert all(v <= TOL_MIXED for v in err.values()), err
+    g.close()
+    q = Params(nx=32, ny=48, nz=32, n_th=1, num_per_dir=3, nu=0.01, lx=2 * math.pi,
+               ly=2 * math.pi, lz=2 * math.pi, delta_t=0.005)
+    q.ri = [0.2, 0, 0, 0]
+    q.background_grad = [1, 0, 0, 0]
+    ref, g = periodic_pair(q, seed=7)
+    for s in range(1, 21):
+        ref.step(s)
+        g.steps(s, 1)
+    err = {nm: rel(g.get_field(nm), ref.get(nm)) for nm in fields(q)}
     assert all(v <= TOL_MIXED for v in err.values()), err
     g.close()

@@ -152,6 +152,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def replica_throughput(dist, ws, seconds, pts_per_step, steps, device="cuda"):
+    """Whole-job Mpoint-steps/s of ws independent replicas: every rank did
+    `steps` steps of `pts_per_step` points in `seconds` of its own device
+    time; the job took as long as the slowest rank (max over ranks)."""
+    if dist is not None:
+        import torch
+        t = torch.tensor([seconds], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        seconds = float(t.item())
+    return ws * pts_per_step * steps / seconds / 1e6, seconds
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -387,13 +399,8 @@ def run_gpu(args):
     while L.dg_timing_read(ch.h, i, nm, 64, ctypes.byref(cnt), ctypes.byref(tms)) == 0:
         kt[nm.value.decode()] = (int(cnt.value), float(tms.value))
         i += 1
-    total = sum(times)
-    if dist:
-        t = torch.tensor([total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
     pts = p.nx * p.ny * p.nz
-    value = ws * pts * args.steps / total / 1e6
+    value, total = replica_throughput(dist, ws, sum(times), pts, args.steps)
     ms = 1e3 * total / args.steps
 
     # end to end through the C-ABI with host-owned state in the reference
@@ -421,13 +428,9 @@ def run_gpu(args):
                 ch.h, _lib.field_id(n), ctypes.c_void_p(host[n].data_ptr()),
                 _lib.DG_LAYOUT_REFERENCE, _lib.DG_HOST))
     ch.synchronize()
-    e2e_t = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    e2e_value, e2e_t = replica_throughput(dist, ws, time.perf_counter() - t0, pts, e2e_steps)
     state_bytes = len(names) * int(np.prod(refshape)) * 16
-    e2e = {"value": ws * pts * e2e_steps / e2e_t / 1e6, "unit": UNIT,
+    e2e = {"value": e2e_value, "unit": UNIT,
            "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
            "steps": e2e_steps,
            "what": "per step: H2D of CU1..3 and CP in the reference layout from pinned host "

@@ -272,6 +272,72 @@ def run_ensemble(args):
             "served_over_plain": served / plain}
 
 
+def run_other_configs(args):
+    """The other configurations of the workload list, each timed for a few
+    graph-replayed steps (CUDA events, L2 not flushed): FP64 and mixed where
+    both exist.  Parity for each is in the test suite."""
+    import torch
+    from diablo_b200 import configs, ics
+    from diablo_b200.solver import Channel, Periodic
+
+    ts = torch.cuda.Stream()     # the solvers run on this stream; events are recorded on it
+    stream = ts.cuda_stream
+
+    def timed(solver, nsteps, warm=3):
+        st = ts
+        solver.steps(1, warm)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        solver.steps(warm + 1, nsteps)
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / nsteps
+
+    out = {}
+    # KH shear layer 128 x 65 x 32 and Re_tau = 180, FP64 and mixed
+    for name, (p, gy), maker in (("kh_shear_layer_128x65x32", configs.kh_shear_layer(),
+                                  ics.kh_shear_layer),
+                                 ("channel_re180_128x129x128", configs.channel_re180(),
+                                  ics.channel_laminar)):
+        for prec in (0, 1):
+            ch = Channel(p.replace(precision=prec), gy, stream=stream)
+            u1, u2, u3, th = maker(p, gy, seed=2)
+            ch.create_flow(u1, u2, u3, th if p.n_th else None)
+            ch.set_time(0.0, p.delta_t)
+            ch.autotune(2)
+            ms = timed(ch, 100)
+            ch.close()
+            out[f"{name}_{'mixed' if prec else 'fp64'}"] = {
+                "ms_per_step": ms, "mpoint_steps_per_s": p.nx * p.ny * p.nz / ms / 1e3}
+    # periodic 256^3, FP64 and mixed
+    p, _ = configs.periodic_256()
+    for prec in (0, 1):
+        g = Periodic(p.replace(precision=prec), stream=stream)
+        for nm, a in zip(("CU1", "CU2", "CU3"), ics.periodic_spectrum(p, seed=3)):
+            g.set_field(nm, a)
+        g.set_time(0.0, p.delta_t)
+        g.rem_div_per()
+        g.poisson_p_per()
+        ms = timed(g, 20)
+        g.close()
+        out[f"periodic_256cubed_{'mixed' if prec else 'fp64'}"] = {
+            "ms_per_step": ms, "mpoint_steps_per_s": 256 ** 3 / ms / 1e3}
+    # Re_tau ~ 550, 512 x 257 x 384, one scalar: FP64 only (no mixed kernels
+    # for 512-point rows)
+    p, gy = configs.channel_re550()
+    ch = Channel(p, gy, stream=stream)
+    u1, u2, u3, th = ics.channel_laminar(p, gy, seed=4)
+    ch.create_flow(u1, u2, u3, th)
+    ch.set_time(0.0, p.delta_t)
+    ms = timed(ch, 5, warm=2)
+    ch.close()
+    out["channel_re550_512x257x384_fp64"] = {"ms_per_step": ms,
+                                              "mpoint_steps_per_s": p.nx * p.ny * p.nz / ms / 1e3}
+    return out
+
+
 def run_reference(args):
     """--impl reference: the oracle restatement on all host cores, rank 0 only."""
     ws, rank, _ = dist_env()
@@ -473,11 +539,13 @@ def run_gpu(args):
                           f"= {bstep / 1e6:.1f} MB over the device time of one step"}
     cpu = cpu_baseline(p, gy, seconds=args.cpu_seconds) if args.cpu_seconds > 0 else None
     ens = run_ensemble(args) if args.ensemble_cases > 0 else None
+    others = run_other_configs(args) if args.other_configs else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(workload_config(p), tuning=tuned), "roofline": roof, "roofline_step": roof_step,
             "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "ensemble": ens,
+            "other_configs": others,
             "gpu_launches": int(launches), "clocks": clocks,
             "check": {"ke": st["ke"], "div_max": st["div_max"], "ubulk": st["ubulk"]}}
     print(json.dumps(line))
@@ -493,6 +561,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--tuning", default="",
                     help="fixed launch shapes, e.g. col_mt=8,cn_mt=16,xrow_chunk=0,ychunk=0")
+    ap.add_argument("--other-configs", type=int, default=1,
+                    help="also time the other workload configurations (0 = skip)")
     ap.add_argument("--ensemble-cases", type=int, default=256)
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--ensemble-rate", type=float, default=20.0)

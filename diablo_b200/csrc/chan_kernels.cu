@@ -3,10 +3,13 @@
 //
 // One substep is five launches (six when COURANT runs):
 //   zinv        spectral U1..U3, TH -> half-physical H (z inverse per kx)
-//   k_xrow_nl   per physical z-row, marching up in y: x c2r of every field,
+//   k_xrow_w    per physical z-row, marching up in y: x c2r of every field,
 //               all products/fluxes of for/channel.f:409-571,665-720, x r2c,
 //               and the combination into 2 arrays per field
-//               (A: to be multiplied by -i kz, B: the rest)
+//               (A: to be multiplied by -i kz, B: the rest).  Row lengths
+//               without a warp kernel take two launches instead: k_xc2r of
+//               every plane into physical space, then k_xprod (products, x
+//               r2c and the combination, one product pair per CTA).
 //   k_zfwd_rhs  per plane: z forward of A/B, nonlinear + explicit linear
 //               terms -> CF (new), and the Crank-Nicolson right-hand side
 //               R = CU + zeta h CF_old - h grad P + beta h CF_new
@@ -26,8 +29,6 @@
 using namespace dgfft;
 
 namespace {
-
-constexpr int XR_ROWS = 2;     // physical z-rows per CTA in k_xrow_nl (1 for the largest rows)
 
 struct ChanConst {
   int NX, NY, NZ, NKX, NKZ, nkxp, nkzt, nf, nth;
@@ -71,191 +72,171 @@ ChanConst make_const(const dg_handle *h) {
 //  4 fl1(j+1) = (U1(j+1)+U1(j)) U2(j+1)   5 fl3(j+1)
 //  6 Ubar1 U2(j)   7 Ubar3 U2(j)   (Ubar = (DYF(j) U(j) + DYF(j-1) U(j-1)) / (2 DY(j)))
 //  8+3n TH U1(j)   9+3n TH U3(j)   10+3n flth(j+1) = (TH(j+1)+TH(j)) U2(j+1)
-// The y-flux terms of for/channel.f:511-571,704-720 are differences of these
-// fluxes between neighbouring planes; they are differenced after the x
-// transform (linearity), so each flux is transformed once.
-constexpr int XR_THR = 128;
+// Generic x-row stage (any NX, any N_TH).  The half-physical planes 0..NY+1
+// are first taken to physical space by the x c2r kernel (into the work array,
+// layout [field][plane][z][x]).  k_xprod then forms the products of output
+// plane j for a batch of z-rows and x-transforms them in complex pairs.  The
+// flux differences are taken in physical space (the x transform is linear),
+// so each pair maps straight onto the A/B arrays of G:
+//   pair 0          U1U3(j)       | fl3(j+1) - fl3(j)      -> G0, G5
+//   pair 1          U1U1(j)       | fl1(j+1) - fl1(j)      -> G1
+//   pair 2          Ubar1 U2(j)   | g(j) - g(j-1)          -> G3
+//   pair 3          Ubar3 U2(j)   | U3U3(j)                -> G2, G4
+//   pair 4+n        TH_n U1(j)    | flth_n(j+1) - flth_n(j) -> G(7+2n)
+//   pair 4+N_TH+m   TH_2m U3(j)   | TH_2m+1 U3(j)          -> G(6+4m), G(8+4m)
+// One CTA transforms one pair for `rz` z-rows of one plane (one z-row per
+// warp for the compile-time lengths).  The pairs of a plane are adjacent in
+// launch order, so the physical rows they share come from HBM once and from
+// L2 after that.
+constexpr int XP_THR = 128;
+
+__host__ __device__ constexpr int xp_rows_max(int nx) {
+  return nx <= 128 ? 16 : (nx <= 256 ? 8 : 4);
+}
+int xp_pairs(int nth) { return 4 + nth + (nth + 1) / 2; }
+size_t xp_smem(int nx, int rz) {
+  return sizeof(double2) * (nx + fft_bufs(nx) * (size_t)rz * padded_len(nx));
+}
+// z-rows per CTA: one per warp for the compile-time lengths; otherwise the
+// batch for this length, halved until the shared memory fits
+int xp_rows(int nx) {
+  if (fft_bufs(nx) == 1) return XP_THR / 32;
+  int rz = xp_rows_max(nx);
+  while (rz > 1 && xp_smem(nx, rz) > 220 * 1024) rz >>= 1;
+  return rz;
+}
 
 template <int NT>
-__global__ void __launch_bounds__(XR_THR) k_xrow_nl(
-    ChanConst C, const double2 *__restrict__ H, long Hfield, int chunk, int xr, FftPlan pl,
+__global__ void __launch_bounds__(XP_THR, 5) k_xprod(
+    ChanConst C, const double *__restrict__ phys, long pfield, int rz, FftPlan pl,
     const double2 *__restrict__ tw, const double *__restrict__ dyf, const double *__restrict__ dy,
     const double *__restrict__ kxv, double2 *__restrict__ G, long Gfield) {
   extern __shared__ double2 sm[];
   const int NX = NT ? NT : C.NX;
-  const int nkxp = C.nkxp, nf = C.nf, nth = C.nth;
-  const int npin = (nf + 1) / 2;            // c2r signals per row
-  const int nprod = 8 + 3 * nth;
-  const int npp = (nprod + 1) / 2;          // r2c signals per row
-  const int maxp = npin > npp ? npin : npp;
+  const int NZ = C.NZ, nkxp = C.nkxp, nth = C.nth;
   const int sstr = padded_len(NX);
   double2 *stw = sm;
   double2 *b0 = stw + NX;
-  double2 *b1 = b0 + xr * maxp * sstr;
-  double2 *prev = b0 + fft_bufs(NX) * xr * maxp * sstr;  // [row][3+nth][nkxp]
-  double *ring = (double *)(prev + xr * (3 + nth) * nkxp);  // [3][row][nf][NX]
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  const int z0 = blockIdx.x * xr;
-  const int j0 = 1 + blockIdx.y * chunk;
-  int j1 = j0 + chunk - 1;
-  if (j1 > C.NY) j1 = C.NY;
-  const int NZ = C.NZ;
+  const int s = blockIdx.x;
+  const int z0 = blockIdx.y * rz;
+  const int j = 1 + blockIdx.z;
+  const int tid = threadIdx.x;
+  const long pplane = (long)NZ * NX;
+  for (int i = tid; i < NX; i += XP_THR) stw[i] = tw[i];
+  const double dyfj = dyf[j], dyfm = dyf[j - 1];
+  const double wgy = 1.0 / (2.0 * dy[j]);
+  const double *base = phys + (long)j * pplane + (long)z0 * NX;
 
-  for (int i = tid; i < NX; i += nthr) stw[i] = tw[i];
-  // plane j0-2 may be -1: zero the whole ring once
-  for (int i = tid; i < 3 * xr * nf * NX; i += nthr) ring[i] = 0.0;
-  __syncthreads();
-
-  auto ringp = [&](int plane, int r, int f) -> double * {
-    int s = (plane + 3) % 3;
-    return ring + (((long)s * xr + r) * nf + f) * NX;
+  // the pair at element e = r NX + x of the CTA's rows
+  auto pair_at = [&](int e) -> double2 {
+    const double *pc = base + e;  // field 0, plane j
+    auto U = [&](int f, int dj) { return __ldg(pc + f * pfield + dj * pplane); };
+    double a, b = 0.0;
+    if (s == 0) {
+      const double u1 = U(0, 0), u2 = U(1, 0), u2p = U(1, 1);
+      const double u3 = U(2, 0), u3p = U(2, 1), u3m = U(2, -1);
+      a = u3 * u1;
+      b = (u3p + u3) * u2p - (u3 + u3m) * u2;
+    } else if (s == 1) {
+      const double u1 = U(0, 0), u1p = U(0, 1), u1m = U(0, -1), u2 = U(1, 0), u2p = U(1, 1);
+      a = u1 * u1;
+      b = (u1p + u1) * u2p - (u1 + u1m) * u2;
+    } else if (s == 2) {
+      const double u1 = U(0, 0), u1m = U(0, -1);
+      const double u2 = U(1, 0), u2p = U(1, 1), u2m = U(1, -1);
+      a = ((dyfj * u1 + dyfm * u1m) * wgy) * u2;
+      const double gp = u2 + u2p, gm = u2m + u2;
+      b = 0.25 * (gp * gp) - 0.25 * (gm * gm);
+    } else if (s == 3) {
+      const double u3 = U(2, 0), u3m = U(2, -1), u2 = U(1, 0);
+      a = ((dyfj * u3 + dyfm * u3m) * wgy) * u2;
+      b = u3 * u3;
+    } else if (s < 4 + nth) {
+      const int f = 3 + (s - 4);
+      const double t = U(f, 0), tp = U(f, 1), tm = U(f, -1);
+      const double u1 = U(0, 0), u2 = U(1, 0), u2p = U(1, 1);
+      a = t * u1;
+      b = (tp + t) * u2p - (t + tm) * u2;
+    } else {
+      const int n = 2 * (s - 4 - nth);
+      const double u3 = U(2, 0);
+      a = U(3 + n, 0) * u3;
+      if (n + 1 < nth) b = U(4 + n, 0) * u3;
+    }
+    return make_double2(a, b);
   };
 
-  // load + c2r of one plane into its ring slot
-  auto load_plane = [&](int plane) {
-    for (int idx = tid; idx < xr * npin * NX; idx += nthr) {
-      const int k = idx % NX;
-      const int q = (idx / NX) % npin;
-      const int r = idx / (NX * npin);
-      const int z = z0 + r;
-      const int fa = 2 * q, fb = 2 * q + 1;
-      const int kk = (k <= NX / 2) ? k : NX - k;
-      double2 v = make_double2(0.0, 0.0);
-      if (z < NZ && kk <= C.NKX && kk < NX / 2) {
-        const long off = (long)plane * NZ * nkxp + (long)z * nkxp + kk;
-        double2 a = H[fa * Hfield + off];
-        double2 b = (fb < nf) ? H[fb * Hfield + off] : make_double2(0.0, 0.0);
-        if (kk == 0) { a.y = 0.0; b.y = 0.0; }
-        v = (k == kk) ? make_double2(a.x - b.y, a.y + b.x) : make_double2(a.x + b.y, -a.y + b.x);
-      }
-      b0[(r * npin + q) * sstr + pad(k)] = v;
+  const bool pow2 = (NX & (NX - 1)) == 0;
+  const double rnx = 1.0 / (double)NX;  // exact for a power of two
+  const double id2 = 1.0 / (2.0 * dyfj), idyj = 1.0 / dy[j];
+  const long jo = (long)j * NZ * nkxp;
+  // mode k of row z from its transformed signal
+  auto finish = [&](const double2 *sig, int z, int k) {
+    const double2 zk = sig[pad(k)];
+    const double2 zm = sig[pad((NX - k) % NX)];
+    // the real and imaginary members of the pair: A = (Z_k + conj Z_{N-k})/2,
+    // B = -i/2 (Z_k - conj Z_{N-k}), scaled by 1/NX
+    double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+    double2 B = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
+    if (pow2) {
+      A = make_double2(A.x * rnx, A.y * rnx);
+      B = make_double2(B.x * rnx, B.y * rnx);
+    } else {
+      A = make_double2(A.x / NX, A.y / NX);
+      B = make_double2(B.x / NX, B.y / NX);
     }
-    __syncthreads();
-    double2 *res = fft<NT>(b0, b1, pl, xr * npin, sstr, stw, +1);
-    for (int idx = tid; idx < xr * npin * NX; idx += nthr) {
-      const int x = idx % NX;
-      const int q = (idx / NX) % npin;
-      const int r = idx / (NX * npin);
-      const double2 v = res[(r * npin + q) * sstr + pad(x)];
-      ringp(plane, r, 2 * q)[x] = v.x;
-      if (2 * q + 1 < nf) ringp(plane, r, 2 * q + 1)[x] = v.y;
+    const double KX = kxv[k];
+    // -i kx A - c B
+    auto flux = [&](double c) { return make_double2(KX * A.y - B.x * c, -KX * A.x - B.y * c); };
+    double2 *o = G + jo + (long)z * nkxp + k;
+    if (s == 0) {
+      o[0] = A;                       // U1: A = U1U3
+      o[5 * Gfield] = flux(id2);      // U3: B = -ikx U1U3 - (fl3(j+1) - fl3(j)) / (2 DYF)
+    } else if (s == 1) {
+      o[Gfield] = flux(id2);          // U1: B = -ikx U1U1 - (fl1(j+1) - fl1(j)) / (2 DYF)
+    } else if (s == 2) {
+      o[3 * Gfield] = flux(idyj);     // U2: B = -ikx Ubar1 U2 - (g(j) - g(j-1)) / DY
+    } else if (s == 3) {
+      o[2 * Gfield] = A;              // U2: A = Ubar3 U2
+      o[4 * Gfield] = B;              // U3: A = U3U3
+    } else if (s < 4 + nth) {
+      o[(7 + 2 * (s - 4)) * Gfield] = flux(id2);  // TH: B = -ikx TH U1 - dflth / (2 DYF)
+    } else {
+      const int n = 2 * (s - 4 - nth);
+      o[(6 + 2 * n) * Gfield] = A;                // TH: A = TH U3
+      if (n + 1 < nth) o[(8 + 2 * n) * Gfield] = B;
     }
-    __syncthreads();
   };
 
-  if (j0 - 2 >= 0) load_plane(j0 - 2);
-  load_plane(j0 - 1);
-
-  for (int j = j0 - 1; j <= j1; j++) {
-    load_plane(j + 1);
-    // products of plane j into complex pairs
-    const double dyfj = (j >= 1) ? dyf[j] : 0.0, dyfm = (j >= 1) ? dyf[j - 1] : 0.0;
-    const double dyj = (j >= 1) ? dy[j] : 1.0;
-    for (int idx = tid; idx < xr * npp * NX; idx += nthr) {
-      const int x = idx % NX;
-      const int q = (idx / NX) % npp;
-      const int r = idx / (NX * npp);
-      const double *U1c = ringp(j, r, 0), *U2c = ringp(j, r, 1), *U3c = ringp(j, r, 2);
-      const double *U1p = ringp(j + 1, r, 0), *U2p = ringp(j + 1, r, 1), *U3p = ringp(j + 1, r, 2);
-      const double *U1m = ringp(j - 1, r, 0), *U3m = ringp(j - 1, r, 2);
-      double pv[2];
-#pragma unroll
-      for (int h2 = 0; h2 < 2; h2++) {
-        const int p = 2 * q + h2;
-        double v = 0.0;
-        switch (p) {
-          case 0: v = U3c[x] * U1c[x]; break;
-          case 1: v = U1c[x] * U1c[x]; break;
-          case 2: v = U3c[x] * U3c[x]; break;
-          case 3: { double s = U2c[x] + U2p[x]; v = 0.25 * (s * s); } break;
-          case 4: v = (U1p[x] + U1c[x]) * U2p[x]; break;
-          case 5: v = (U3p[x] + U3c[x]) * U2p[x]; break;
-          case 6: v = ((dyfj * U1c[x] + dyfm * U1m[x]) / (2. * dyj)) * U2c[x]; break;
-          case 7: v = ((dyfj * U3c[x] + dyfm * U3m[x]) / (2. * dyj)) * U2c[x]; break;
-          default:
-            if (p < nprod) {
-              const int n = (p - 8) / 3, w = (p - 8) % 3;
-              const double *Tc = ringp(j, r, 3 + n), *Tp = ringp(j + 1, r, 3 + n);
-              if (w == 0) v = Tc[x] * U1c[x];
-              else if (w == 1) v = Tc[x] * U3c[x];
-              else v = (Tp[x] + Tc[x]) * U2p[x];
-            }
-        }
-        pv[h2] = v;
-      }
-      b0[(r * npp + q) * sstr + pad(x)] = make_double2(pv[0], pv[1]);
+  if constexpr (NT != 0) {
+    // one warp per z-row (rz = 4): past the twiddle staging, no CTA barrier
+    __syncthreads();
+    const int warp = tid >> 5, lane = tid & 31;
+    const int z = z0 + warp;
+    if (z >= NZ) return;
+    double2 *sig = b0 + warp * sstr;
+#pragma unroll 4
+    for (int x = lane; x < NX; x += 32) sig[pad(x)] = pair_at(warp * NX + x);
+    __syncwarp();
+    wpasses_any<NT, -1, 0>(sig, 1, sstr, stw, lane);
+    for (int k = lane; k < nkxp; k += 32) finish(sig, z, k);
+  } else {
+    double2 *b1 = b0 + rz * sstr;
+    for (int idx = tid; idx < rz * NX; idx += XP_THR) {
+      const int r = idx / NX, x = idx - r * NX;
+      b0[r * sstr + pad(x)] = (z0 + r < NZ) ? pair_at(idx) : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    double2 *res = fft<NT>(b0, b1, pl, xr * npp, sstr, stw, -1);
-    // separate, scale by 1/NX, combine, write
-    const double rnx = (double)NX;
-    const bool out = (j >= j0);
-    for (int idx = tid; idx < xr * nkxp; idx += nthr) {
-      const int k = idx % nkxp;
-      const int r = idx / nkxp;
-      const int z = z0 + r;
-      if (z >= NZ) continue;
-      auto X = [&](int p) -> double2 {
-        const int q = p >> 1;
-        const double2 zk = res[(r * npp + q) * sstr + pad(k)];
-        const double2 zm = res[(r * npp + q) * sstr + pad((NX - k) % NX)];
-        double2 v;
-        if ((p & 1) == 0) v = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
-        else v = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
-        return make_double2(v.x / rnx, v.y / rnx);
-      };
-      double2 *pv = prev + (r * (3 + nth)) * nkxp;  // [0]=fl1 [1]=fl3 [2]=g [3+n]=flth
-      const double KX = kxv[k];
-      auto mikx = [&](double2 a) { return make_double2(KX * a.y, -KX * a.x); };  // -i kx a
-      const double2 x3 = X(3), x4 = X(4), x5 = X(5);
-      if (out) {
-        const long off = (long)j * NZ * nkxp + (long)z * nkxp + k;
-        const double2 x0 = X(0), x1 = X(1), x2 = X(2), x6 = X(6), x7 = X(7);
-        const double2 f1p = pv[0 * nkxp + k], f3p = pv[1 * nkxp + k], gp = pv[2 * nkxp + k];
-        const double d2 = 2.0 * dyfj;
-        // U1: A = U1U3, B = -ikx U1U1 - (fl1(j+1) - fl1(j)) / (2 DYF)
-        G[0 * Gfield + off] = x0;
-        double2 t = mikx(x1);
-        G[1 * Gfield + off] = make_double2(t.x - (x4.x - f1p.x) / d2, t.y - (x4.y - f1p.y) / d2);
-        // U2: A = Ubar3 U2, B = -ikx Ubar1 U2 - (g(j) - g(j-1)) / DY
-        G[2 * Gfield + off] = x7;
-        t = mikx(x6);
-        G[3 * Gfield + off] = make_double2(t.x - (x3.x - gp.x) / dyj, t.y - (x3.y - gp.y) / dyj);
-        // U3: A = U3U3, B = -ikx U1U3 - (fl3(j+1) - fl3(j)) / (2 DYF)
-        G[4 * Gfield + off] = x2;
-        t = mikx(x0);
-        G[5 * Gfield + off] = make_double2(t.x - (x5.x - f3p.x) / d2, t.y - (x5.y - f3p.y) / d2);
-        for (int n = 0; n < nth; n++) {
-          const double2 a = X(8 + 3 * n), b = X(9 + 3 * n), c = X(10 + 3 * n);
-          const double2 fp = pv[(3 + n) * nkxp + k];
-          G[(6 + 2 * n) * Gfield + off] = b;
-          t = mikx(a);
-          G[(7 + 2 * n) * Gfield + off] = make_double2(t.x - (c.x - fp.x) / d2, t.y - (c.y - fp.y) / d2);
-        }
-      }
-      pv[0 * nkxp + k] = x4;
-      pv[1 * nkxp + k] = x5;
-      pv[2 * nkxp + k] = x3;
-      for (int n = 0; n < nth; n++) pv[(3 + n) * nkxp + k] = X(10 + 3 * n);
+    double2 *res = fft<0>(b0, b1, pl, rz, sstr, stw, -1);
+    for (int idx = tid; idx < rz * nkxp; idx += XP_THR) {
+      const int r = idx / nkxp, k = idx - r * nkxp;
+      if (z0 + r < NZ) finish(res + r * sstr, z0 + r, k);
     }
-    __syncthreads();
   }
 }
 
-size_t xrow_smem(const dg_handle *h, int xr) {
-  const int nf = h->nf, nth = h->NTH, NX = h->NX;
-  const int npin = (nf + 1) / 2, npp = (8 + 3 * nth + 1) / 2;
-  const int maxp = npin > npp ? npin : npp;
-  return sizeof(double2) * (NX + fft_bufs(NX) * xr * maxp * padded_len(NX) +
-                            xr * (3 + nth) * h->nkxp) +
-         sizeof(double) * 3 * xr * nf * NX;
-}
-
-// z-rows per CTA of k_xrow_nl: two where the shared memory allows, else one
-int xrow_rows(const dg_handle *h) { return xrow_smem(h, XR_ROWS) <= 220 * 1024 ? XR_ROWS : 1; }
-
 // ------------------------------------------------------- xrow, one warp/row
-// Same products as k_xrow_nl, organised so a warp owns one physical z-row and
+// Same products as listed above, organised so a warp owns one physical z-row and
 // marches up through its chunk of planes with no CTA-wide barrier: the two
 // physical planes it needs (j and j+1) live in registers (lane l holds
 // x = l + 32 i), the transforms run in a per-warp shared buffer with
@@ -691,24 +672,36 @@ __global__ void __launch_bounds__(ZF_THR) k_zfwd_rhs(
   }
 }
 
-// Warp-per-column-pair variant: a CTA of four warps takes 8 kx columns of one
-// field on one plane; the A and B columns are staged with one coalesced load,
-// then each warp transforms its 2 x (A, B) signals and finishes those modes.
-constexpr int ZW_KXG = 8;
+// Warp-per-column variant: a CTA of four warps takes 4 x zw_kpw kx columns of
+// one field on one plane; the A and B columns are staged with one coalesced
+// load, then each warp transforms its zw_kpw x (A, B) signals (warp passes;
+// butterfly-parallel where a pass has more than 32 butterflies) and the CTA
+// finishes those modes.  Two columns per warp up to NZ = 256, one above (the
+// shared memory of a CTA grows with NZ).
+__host__ __device__ constexpr int zw_kpw(int nz) { return nz <= 256 ? 2 : 1; }
+__host__ __device__ constexpr int zw_kxg(int nz) { return 4 * zw_kpw(nz); }
+__host__ __device__ constexpr int zw_minb(int nz, int esz) {
+  return nz <= 256 ? (esz == 16 ? 6 : 5) : (nz <= 384 ? 3 : 2);
+}
+template <typename CX>
+size_t zw_smem(int nz) {
+  return sizeof(CX) * (nz + 4 * 2 * zw_kpw(nz) * (size_t)padded_len(nz));
+}
 
 template <int NZ, typename CX = double2>
-__global__ void __launch_bounds__(128, sizeof(CX) == 16 ? 6 : 5) k_zfwd_w(
+__global__ void __launch_bounds__(128, zw_minb(NZ, sizeof(CX))) k_zfwd_w(
     ChanConst C, const CX *__restrict__ G, long Gfield, const CX *__restrict__ tw,
     const double *__restrict__ dscal, int rk_step, const double *__restrict__ kxv,
     const double *__restrict__ kzv, const double *__restrict__ dy, const double *__restrict__ dyf,
     FieldPtrs cu, FieldPtrs cf, FieldPtrs rhs, const double2 *__restrict__ cp, int jbase) {
   constexpr int SSTR = padded_len(NZ);
+  constexpr int KPW = zw_kpw(NZ), KXG = zw_kxg(NZ);
   extern __shared__ double2 sm_raw[];
   CX *sm = reinterpret_cast<CX *>(sm_raw);
   CX *stw = sm;
-  CX *buf = stw + NZ;                          // [warp][A0 A1 B0 B1][SSTR]
+  CX *buf = stw + NZ;                          // [warp][A_0..A_KPW-1 B_0..B_KPW-1][SSTR]
   const int nkxp = C.nkxp, nkzt = C.nkzt, NKZ = C.NKZ;
-  const int kx0 = blockIdx.x * ZW_KXG;
+  const int kx0 = blockIdx.x * KXG;
   const int j = jbase + blockIdx.y;
   const int f = blockIdx.z;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -719,27 +712,27 @@ __global__ void __launch_bounds__(128, sizeof(CX) == 16 ? 6 : 5) k_zfwd_w(
   for (int i = threadIdx.x; i < NZ; i += blockDim.x) stw[i] = tw[i];
   const CX *GA = G + (2 * f) * Gfield + (long)j * NZ * nkxp;
   const CX *GB = G + (2 * f + 1) * Gfield + (long)j * NZ * nkxp;
-  for (int base = 0; base < 2 * ZW_KXG * NZ; base += 8 * 128) {
+  for (int base = 0; base < 2 * KXG * NZ; base += 8 * 128) {
     CX v[8];
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       const int i = base + u * 128 + threadIdx.x;
-      const int c = i % ZW_KXG, z = (i / ZW_KXG) % NZ, ab = i / (ZW_KXG * NZ);
-      v[u] = (i < 2 * ZW_KXG * NZ && kx0 + c < nkxp) ? (ab ? GB : GA)[(long)z * nkxp + kx0 + c]
-                                                     : CT<CX>::mk(0, 0);
+      const int c = i % KXG, z = (i / KXG) % NZ, ab = i / (KXG * NZ);
+      v[u] = (i < 2 * KXG * NZ && kx0 + c < nkxp) ? (ab ? GB : GA)[(long)z * nkxp + kx0 + c]
+                                                 : CT<CX>::mk(0, 0);
     }
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       const int i = base + u * 128 + threadIdx.x;
-      if (i >= 2 * ZW_KXG * NZ) continue;
-      const int c = i % ZW_KXG, z = (i / ZW_KXG) % NZ, ab = i / (ZW_KXG * NZ);
-      const int w = c >> 1, s = (ab << 1) | (c & 1);
-      buf[(w * 4 + s) * SSTR + pad(z)] = v[u];
+      if (i >= 2 * KXG * NZ) continue;
+      const int c = i % KXG, z = (i / KXG) % NZ, ab = i / (KXG * NZ);
+      const int w = c / KPW, s = ab * KPW + c % KPW;
+      buf[(w * 2 * KPW + s) * SSTR + pad(z)] = v[u];
     }
   }
   __syncthreads();
-  CX *wb = buf + warp * 4 * SSTR;
-  wpasses<NZ, -1, 0>(wb, 4, SSTR, stw, lane);
+  CX *wb = buf + warp * 2 * KPW * SSTR;
+  wpasses_any<NZ, -1, 0>(wb, 2 * KPW, SSTR, stw, lane);
   __syncthreads();  // the epilogue below reads every warp's columns
 
   const double h = dscal[1 + rk_step];
@@ -759,15 +752,15 @@ __global__ void __launch_bounds__(128, sizeof(CX) == 16 ? 6 : 5) k_zfwd_w(
   const double idy = 1.0 / dyj, bw2 = 1.0 / (2.0 * dyj);
   // all 128 threads over the CTA's (kz, kx) modes, kx fastest: consecutive
   // threads touch consecutive modes of a kz row
-  for (int it = threadIdx.x; it < ZW_KXG * nkzt; it += 128) {
-    const int c = it % ZW_KXG, kp = it / ZW_KXG;
+  for (int it = threadIdx.x; it < KXG * nkzt; it += 128) {
+    const int c = it % KXG, kp = it / KXG;
     const int kx = kx0 + c;
     if (kx >= nkxp) continue;
     const int z = (kp <= NKZ) ? kp : (NZ - 1 + (kp - NKZ) - NKZ);
     // the transform's working precision ends here: everything below is FP64
-    const CX *cb = buf + (c >> 1) * 4 * SSTR;
-    const int cc = c & 1;
-    const CX aw = cb[(0 + cc) * SSTR + pad(z)], bw = cb[(2 + cc) * SSTR + pad(z)];
+    const CX *cb = buf + (c / KPW) * 2 * KPW * SSTR;
+    const int cc = c % KPW;
+    const CX aw = cb[cc * SSTR + pad(z)], bw = cb[(KPW + cc) * SSTR + pad(z)];
     const double2 a = make_double2((double)aw.x * inz, (double)aw.y * inz);
     const double2 b = make_double2((double)bw.x * inz, (double)bw.y * inz);
     const double KX = kxv[kx], KZ = kzv[kp];
@@ -877,6 +870,8 @@ __global__ void __launch_bounds__(128, sizeof(CX) == 16 ? 6 : 5) k_zfwd_w(
 __host__ __device__ constexpr bool zw_supported(int n) {
   return n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 256;
 }
+// lengths with a compile-time plan above the warp-signal lengths (FP64 only)
+__host__ __device__ constexpr bool zw_big(int n) { return n == 192 || n == 384 || n == 512; }
 
 size_t zfwd_smem(const dg_handle *h) {
   const int kxg = zf_kxg(h->NZ);
@@ -1683,8 +1678,8 @@ static int nl_chunk_mixed(dg_handle *h, const ChanConst &C, int rk_step, int a, 
     return DG_ERR_DIMS;
   }
   DG_LAUNCHED();
-  dim3 zgrid(dg_cdiv(h->nkxp, ZW_KXG), nplan, h->nf);
-  const size_t sm = sizeof(float2) * (h->NZ + 16 * padded_len(h->NZ));
+  dim3 zgrid(dg_cdiv(h->nkxp, zw_kxg(h->NZ)), nplan, h->nf);
+  const size_t sm = zw_smem<float2>(h->NZ);
   done = false;
 #define ZW_CASE(N)                                                                              \
   if (!done && h->NZ == N) {                                                                    \
@@ -1761,15 +1756,19 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
       if (a == 1) {
         DG_TRY(dg_zinv(h, in, h->nf, hdone + 1, h->NY + 1, h->H, 0));
         hdone = h->NY + 1;
-        const int chunk = 8;
-        const int xr = xrow_rows(h);
-        dim3 grid(dg_cdiv(h->NZ, xr), dg_cdiv(h->NY, chunk));
-        const size_t sm = xrow_smem(h, xr);
+        // every plane to physical space (the work array holds nf stacks of
+        // NY+2 planes), then the products of planes 1..NY
+        const long pplane = (long)h->NZ * h->NX, pfield = (long)(h->NY + 2) * pplane;
+        double *phys = (double *)h->work;
+        DG_TRY(dg_xc2r_planes(h, h->H, h->nf, 0, h->NY + 1, phys, pplane, h->NX, pfield));
+        const int rz = xp_rows(h->NX);
+        dim3 grid(xp_pairs(h->NTH), dg_cdiv(h->NZ, rz), h->NY);
+        const size_t sm = xp_smem(h->NX, rz);
 #define KERNEL_BODY(N)                                                                          \
-  dg_big_smem((const void *)k_xrow_nl<N>);                                                      \
-  dg_kt_begin(h, "k_xrow_nl", h->st);                                                               \
-  k_xrow_nl<N><<<grid, XR_THR, sm, h->st>>>(C, h->H, Hfield, chunk, xr, h->plx, h->twx, h->dyf, h->dy, \
-                                            h->kx, h->G, Hfield)
+  dg_big_smem((const void *)k_xprod<N>);                                                        \
+  dg_kt_begin(h, "k_xprod", h->st);                                                             \
+  k_xprod<N><<<grid, XP_THR, sm, h->st>>>(C, phys, pfield, rz, h->plx, h->twx, h->dyf, h->dy,   \
+                                          h->kx, h->G, Hfield)
         switch (h->NX) {
           DG_FOR_EACH_N(DG_CASE_N)
           default: KERNEL_BODY(0); break;
@@ -1778,43 +1777,41 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
         DG_LAUNCHED();
       }
     }
-    // 3. z forward, explicit terms, CN right-hand side for planes a..b
+    // 3. z forward, explicit terms, CN right-hand side for planes a..b (all
+    //    planes 1..NY after the generic x-row stage)
+    const int za = done ? a : 1, zb = done ? b : h->NY;
     bool zdone = false;
-    if (zw_supported(h->NZ) && done) {
-      dim3 grid(dg_cdiv(h->nkxp, ZW_KXG), b - a + 1, h->nf);
-      const size_t sm = sizeof(double2) * (h->NZ + 16 * padded_len(h->NZ));
+    if (zw_supported(h->NZ) || zw_big(h->NZ)) {
+      dim3 grid(dg_cdiv(h->nkxp, zw_kxg(h->NZ)), zb - za + 1, h->nf);
+      const size_t sm = zw_smem<double2>(h->NZ);
 #define ZW_CASE(N)                                                                             \
   if (h->NZ == N) {                                                                            \
     dg_big_smem((const void *)k_zfwd_w<N>);                                                    \
     dg_kt_begin(h, "k_zfwd_w", h->st);                                                          \
     k_zfwd_w<N><<<grid, 128, sm, h->st>>>(C, h->G, Hfield, h->twz, h->dscal, rk_step, h->kx,   \
-                                          h->kz, h->dy, h->dyf, cu, cf, rhs, h->cp, a);        \
+                                          h->kz, h->dy, h->dyf, cu, cf, rhs, h->cp, za);       \
     zdone = true;                                                                              \
   }
-      ZW_CASE(16) ZW_CASE(32) ZW_CASE(48) ZW_CASE(64) ZW_CASE(96) ZW_CASE(128) ZW_CASE(256)
+      ZW_CASE(16) ZW_CASE(32) ZW_CASE(48) ZW_CASE(64) ZW_CASE(96) ZW_CASE(128) ZW_CASE(192)
+      ZW_CASE(256) ZW_CASE(384) ZW_CASE(512)
 #undef ZW_CASE
       if (zdone) DG_LAUNCHED();
     }
-    if (!done || !zdone) {
-      if (a == 1 || done) {
-        // generic path: one launch over all planes after all products exist
-        if (!done && a != 1) continue;
-        dim3 grid(dg_cdiv(h->nkxp, zf_kxg(h->NZ)), h->NY);
-        const size_t sm = zfwd_smem(h);
+    // generic path: one launch over all planes after all products exist
+    if (!zdone && (!done || b == h->NY)) {
+      dim3 grid(dg_cdiv(h->nkxp, zf_kxg(h->NZ)), h->NY);
+      const size_t sm = zfwd_smem(h);
 #define KERNEL_BODY(N)                                                                          \
   dg_big_smem((const void *)k_zfwd_rhs<N>);                                                     \
   dg_kt_begin(h, "k_zfwd_rhs", h->st);                                                            \
   k_zfwd_rhs<N><<<grid, ZF_THR, sm, h->st>>>(C, h->G, Hfield, h->plz, h->twz, h->dscal, rk_step, \
                                              h->kx, h->kz, h->dy, h->dyf, cu, cf, rhs, h->cp)
-        if (!zdone && (!done ? a == 1 : b == h->NY)) {
-          switch (h->NZ) {
-            DG_FOR_EACH_N(DG_CASE_N)
-            default: KERNEL_BODY(0); break;
-          }
-          DG_LAUNCHED();
-        }
-#undef KERNEL_BODY
+      switch (h->NZ) {
+        DG_FOR_EACH_N(DG_CASE_N)
+        default: KERNEL_BODY(0); break;
       }
+#undef KERNEL_BODY
+      DG_LAUNCHED();
     }
     if (!done) break;  // the generic kernels covered every plane
   }

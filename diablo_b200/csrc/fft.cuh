@@ -401,6 +401,65 @@ __device__ __forceinline__ void wpasses(C *buf, int nsig, int sstr, const C *tw,
   }
 }
 
+// Warp pass with more butterflies than lanes (N/R > 32): lane l takes
+// butterflies l, l + 32, ... of one signal at a time, all loaded before the
+// __syncwarp and stored after it.  Same butterflies and twiddles as the CTA
+// passes, so the results are identical.
+template <int N, int R, int NS, int SIGN, typename C>
+__device__ __forceinline__ void wpass_m(C *__restrict__ buf, int nsig, int sstr,
+                                        const C *__restrict__ tw, int lane) {
+  constexpr int NB = N / R;
+  constexpr int M = (NB + 31) / 32;
+  constexpr int TMUL = N / (NS * R);
+  for (int s = 0; s < nsig; s++) {
+    C v[M][R];
+    const C *in = buf + s * sstr;
+#pragma unroll
+    for (int m = 0; m < M; m++) {
+      const int b = lane + 32 * m;
+      if (NB % 32 == 0 || b < NB) {
+        const int k = b % NS;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          C x = in[pad(b + r * NB)];
+          if (NS > 1 && r > 0) {
+            C t = tw[r * k * TMUL];
+            if (SIGN > 0) t.y = -t.y;
+            x = cmul(x, t);
+          }
+          v[m][r] = x;
+        }
+        dft<R>(v[m], SIGN);
+      }
+    }
+    __syncwarp();
+    C *out = buf + s * sstr;
+#pragma unroll
+    for (int m = 0; m < M; m++) {
+      const int b = lane + 32 * m;
+      if (NB % 32 == 0 || b < NB) {
+        const int k = b % NS;
+        const int idx = (b / NS) * NS * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) out[pad(idx + r * NS)] = v[m][r];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// warp passes for any compile-time length: signal-parallel where N/R <= 32,
+// butterfly-parallel above
+template <int N, int SIGN, int P, typename C>
+__device__ __forceinline__ void wpasses_any(C *buf, int nsig, int sstr, const C *tw, int lane) {
+  constexpr int R = plan_radix(N, P);
+  if constexpr (R != 0) {
+    if constexpr (N / R <= 32) wpass<N, R, plan_ns(N, P), SIGN>(buf, nsig, sstr, tw, lane);
+    else wpass_m<N, R, plan_ns(N, P), SIGN>(buf, nsig, sstr, tw, lane);
+    wpasses_any<N, SIGN, P + 1>(buf, nsig, sstr, tw, lane);
+  }
+}
+
 // Compile-time lengths run in place in buf0 (buf1 unused); the runtime plan
 // ping-pongs between buf0 and buf1.
 template <int N, typename C>
@@ -418,6 +477,8 @@ __device__ __forceinline__ C *fft(C *buf0, C *buf1, const FftPlan &pl, int nsig,
 
 // CTA front end: with a warp-capable length the signals are dealt out to the
 // warps (no CTA barrier between passes), otherwise the CTA-wide passes run.
+// (For 192, 384 and 512 the CTA-wide passes measured faster here than
+// butterfly-parallel warp passes: fewer registers, more resident CTAs.)
 template <int N, typename C>
 __device__ __forceinline__ C *fft_cta(C *buf0, C *buf1, const FftPlan &pl,
                                             int nsig, int sig_stride, const C *tw,
@@ -428,8 +489,8 @@ __device__ __forceinline__ C *fft_cta(C *buf0, C *buf1, const FftPlan &pl,
     const int s0 = warp * per;
     const int ns = (nsig - s0) < per ? (nsig - s0) : per;
     if (ns > 0) {
-      if (sign < 0) wpasses<N, -1, 0>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
-      else wpasses<N, +1, 0>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
+      if (sign < 0) wpasses_any<N, -1, 0>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
+      else wpasses_any<N, +1, 0>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
     }
     __syncthreads();
     return buf0;

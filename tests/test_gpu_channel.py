@@ -174,7 +174,7 @@ def test_channel_re180_100_steps_variable_dt():
 
 
 @pytest.mark.parametrize("variant", ["ftype2_rotation_gravity", "th_neumann_drho",
-                                     "stretched_two_scalars", "odd_sizes"])
+                                     "stretched_two_scalars", "odd_sizes", "three_scalars"])
 def test_channel_variants_short(variant):
     """Paths the two configurations above do not exercise."""
     if variant == "ftype2_rotation_gravity":
@@ -201,6 +201,14 @@ def test_channel_variants_short(variant):
         p.th_bc_ymax = [0, 1, 0, 0]
         p.th_bc_ymin_c1 = [-1.0, 0.0, 0, 0]
         p.th_bc_ymax_c1 = [1.0, 0.0, 0, 0]
+    elif variant == "three_scalars":                         # N_TH = 3: generic x-row path
+        p, gy = configs.kh_shear_layer(nx=32, ny=25, nz=16)
+        p = p.replace(n_th=3)
+        p.ri = [0.1, 0.05, -0.02, 0]
+        p.pr = [1.0, 2.0, 0.5, 1]
+        p.th_bc_ymin = [0, 1, 0, 0]
+        p.th_bc_ymax = [0, 1, 1, 0]
+        p.th_bc_ymax_c1 = [0, 0, 0.2, 0]
     else:
         p, gy = configs.kh_shear_layer(nx=36, ny=11, nz=18)  # lengths without a specialisation
     ref, ch, _ = start_pair(p, gy, ics.kh_shear_layer, seed=11)

@@ -1598,14 +1598,30 @@ static double courant_dt0(const dg_handle *h) {
   return dt;
 }
 
-int dg_courant_dev(dg_handle *h, const double2 *const *u) {
+// With `side`, the x c2r and the reduction run on the side stream (they read
+// only H, dmin_bits and write the parked DELTA_T), so they overlap whatever
+// the main stream runs next; the caller joins ev_cfl1 before the commit.
+int dg_courant_dev(dg_handle *h, const double2 *const *u, bool side) {
   // physical U1..U3 on planes 1..NY, reduced to COURANT's minimum on the fly
   DG_TRY(dg_zinv(h, u, 3, 1, h->NY, h->H, 0));
-  DG_CUDA(cudaMemsetAsync(h->dmin_bits, 0x7f, sizeof(unsigned long long), h->st));
-  DG_TRY(dg_xc2r_cfl(h, h->H, 1, h->NY, h->dmin_bits));
-  dg_kt_begin(h, "k_dt_update", h->st);
-  k_dt_update<<<1, 1, 0, h->st>>>(h->dscal, h->dmin_bits, courant_dt0(h));
-  DG_LAUNCHED();
+  cudaStream_t keep = h->st;
+  if (side) {
+    DG_CUDA(cudaEventRecord(h->ev_cfl0, h->st));
+    DG_CUDA(cudaStreamWaitEvent(h->st2, h->ev_cfl0, 0));
+    h->st = h->st2;
+  }
+  auto reduce = [&]() -> int {
+    DG_CUDA(cudaMemsetAsync(h->dmin_bits, 0x7f, sizeof(unsigned long long), h->st));
+    DG_TRY(dg_xc2r_cfl(h, h->H, 1, h->NY, h->dmin_bits));
+    dg_kt_begin(h, "k_dt_update", h->st);
+    k_dt_update<<<1, 1, 0, h->st>>>(h->dscal, h->dmin_bits, courant_dt0(h));
+    DG_LAUNCHED();
+    return DG_OK;
+  };
+  const int s = reduce();
+  h->st = keep;
+  DG_TRY(s);
+  if (side) DG_CUDA(cudaEventRecord(h->ev_cfl1, h->st2));
   return DG_OK;
 }
 
@@ -1821,11 +1837,16 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
   const bool cfl = h->p.variable_dt && rk_step == 3 && h->p.update_dt > 0 &&
                    (time_step % h->p.update_dt) == 0;
   if (cfl) {
+    // the reduction overlaps REM_DIV (which only waits for the z inverse of
+    // the velocity it overwrites)
     const double2 *u[3] = {h->cu[0], h->cu[1], h->cu[2]};
-    DG_TRY(dg_courant_dev(h, u));
+    DG_TRY(dg_courant_dev(h, u, true));
   }
   DG_TRY(dg_rem_div_dev(h, 1, rk_step));
-  if (cfl) DG_TRY(dg_dt_commit(h));
+  if (cfl) {
+    DG_CUDA(cudaStreamWaitEvent(h->st, h->ev_cfl1, 0));
+    DG_TRY(dg_dt_commit(h));
+  }
   return DG_OK;
 }
 

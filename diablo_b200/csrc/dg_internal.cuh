@@ -90,6 +90,7 @@ struct dg_handle {
   bool own_stream;
   cudaStream_t st2;             // side stream for work off the critical path
   cudaEvent_t ev_fork, ev_join;
+  cudaEvent_t ev_cfl0, ev_cfl1;  // COURANT's reduction on the side stream
   bool tables_pending;          // CN tables being rebuilt on st2
 
   // host copies of the tables
@@ -193,7 +194,7 @@ int dg_chan_init(dg_handle *h);
 int dg_per_init(dg_handle *h);
 int dg_apply_bc_vel_dev(dg_handle *h);
 int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step);
-int dg_courant_dev(dg_handle *h, const double2 *const *u);
+int dg_courant_dev(dg_handle *h, const double2 *const *u, bool side = false);
 int dg_stats_dev(dg_handle *h, dg_stats *s);
 int dg_per_stats(dg_handle *h, dg_stats *s);
 int dg_cn_tables(dg_handle *h);

@@ -245,7 +245,9 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
   }
   if (cudaStreamCreateWithFlags(&h->st2, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_cfl0, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_cfl1, cudaEventDisableTiming) != cudaSuccess) {
     dg_set_error("side stream creation failed");
     if (h->own_stream) cudaStreamDestroy(h->st);
     free(h);
@@ -393,6 +395,8 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
   dg_graphs_free(h);
   cudaEventDestroy(h->ev_fork);
   cudaEventDestroy(h->ev_join);
+  cudaEventDestroy(h->ev_cfl0);
+  cudaEventDestroy(h->ev_cfl1);
   cudaStreamDestroy(h->st2);
   if (h->own_stream) cudaStreamDestroy(h->st);
   free(h->h_gy); free(h->h_gyf); free(h->h_dy); free(h->h_dyf);

@@ -21,6 +21,12 @@ ERRORS = {1: "DG_ERR_ARG", 2: "DG_ERR_DIMS", 3: "DG_ERR_OOM", 4: "DG_ERR_CUDA", 
           6: "DG_ERR_TIMEOUT", 7: "DG_ERR_NODEV"}
 DG_HOST, DG_DEVICE = 0, 1
 DG_LAYOUT_COMPACT, DG_LAYOUT_REFERENCE = 0, 1
+# rows of diablo_save_stats_chan's profiles (DG_PR_* and DG_PRT_* in the header)
+PROFILES = ("ume", "vme", "wme", "urms", "vrms", "wrms", "uv", "uw", "wv", "dudy", "dwdy", "cp",
+            "shear", "omega_x", "omega_y", "omega_z", "epsilon")
+PROFILES_TH = ("thme", "dthdy", "thrms", "thv", "pe_diss")
+BULK = ("ubulk", "uc", "urms_b", "vrms_b", "wrms_b")
+
 FIELD_IDS = {"CU1": 0, "CU2": 1, "CU3": 2, "CP": 3, "CF1": 4, "CF2": 5, "CF3": 6, "CR1": 7}
 
 
@@ -94,6 +100,8 @@ def load(path: str = LIB_PATH):
         "dg_timing_read": [P, I, ctypes.c_char_p, I, ctypes.POINTER(ctypes.c_int64),
                            ctypes.POINTER(D)],
         "diablo_stats": [P, ctypes.POINTER(DgStats)],
+        "diablo_save_stats_chan": [P, P, P, P],
+        "diablo_stats_means": [P, P, P, P, P, ctypes.POINTER(I)],
     }
     L.dg_state_bytes.argtypes = [P]
     L.dg_state_bytes.restype = ctypes.c_int64

@@ -132,6 +132,10 @@ struct dg_handle {
 
   dg_ktimer *kt;                // per-kernel event timing (null unless enabled)
 
+  // SAVE_STATS_CHAN running means (host, allocated on first use)
+  int nsamples;
+  double *h_ubar;               // [3 + N_TH][NY+2]: UBAR, VBAR, WBAR, THBAR(n)
+
   // full-step CUDA graphs (variant 0: no COURANT, 1: with COURANT)
   cudaGraphExec_t gexec[2];
   bool gwarm[2];

@@ -393,6 +393,7 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
   cudaStreamSynchronize(h->st2);
   dg_kt_free(h);
   dg_graphs_free(h);
+  free(h->h_ubar);
   cudaEventDestroy(h->ev_fork);
   cudaEventDestroy(h->ev_join);
   cudaEventDestroy(h->ev_cfl0);

@@ -159,6 +159,32 @@ class _Solver:
 class Channel(_Solver):
     """Device-resident channel state driven through RK_CHAN_1 and helpers."""
 
+    def save_stats(self) -> dict:
+        """SAVE_STATS_CHAN(FINAL=.FALSE.) + tkebudget_chan profiles
+        (for/save_stats.f:4-690,963-1173): arrays over rows j = 0..NY+1 named
+        as the reference's variables (scalar profiles as [N_TH][NY+2]), and
+        the bulk values.  Applies the velocity BCs first and advances the
+        running means, as the reference does."""
+        L = self.p.ny + 2
+        prof = np.zeros((len(_lib.PROFILES), L))
+        prof_th = np.zeros((max(self.p.n_th, 1), len(_lib.PROFILES_TH), L))
+        bulk = np.zeros(len(_lib.BULK))
+        self._call("diablo_save_stats_chan", _ptr(prof), _ptr(prof_th), _ptr(bulk))
+        out = {nm: prof[i] for i, nm in enumerate(_lib.PROFILES)}
+        out.update({nm: prof_th[: self.p.n_th, i] for i, nm in enumerate(_lib.PROFILES_TH)})
+        out.update({nm: float(v) for nm, v in zip(_lib.BULK, bulk)})
+        return out
+
+    def stats_means(self) -> dict:
+        """NSAMPLES and the running means UBAR, VBAR, WBAR, THBAR that
+        SAVE_STATS_CHAN(FINAL=.TRUE.) writes (rows 0..NY+1)."""
+        L = self.p.ny + 2
+        u, v, w = np.zeros(L), np.zeros(L), np.zeros(L)
+        th = np.zeros((max(self.p.n_th, 1), L))
+        n = ctypes.c_int()
+        self._call("diablo_stats_means", _ptr(u), _ptr(v), _ptr(w), _ptr(th), ctypes.byref(n))
+        return {"nsamples": n.value, "ubar": u, "vbar": v, "wbar": w, "thbar": th[: self.p.n_th]}
+
     def __init__(self, p: Params, gy, stream=None):
         if p.num_per_dir != 2:
             raise ValueError("Channel needs num_per_dir = 2")

@@ -244,6 +244,35 @@ int dg_server_destroy(dg_server *s);
  * the state for non-finite values (returns DG_ERR_NAN if any). */
 int diablo_stats(dg_handle *h, dg_stats *s);
 
+/* SAVE_STATS_CHAN(FINAL=.FALSE.) (for/save_stats.f:4-31,85-690) with
+ * tkebudget_chan (for/save_stats.f:963-1173), channel only.  Runs
+ * APPLY_BC_VEL on the state (for/save_stats.f:24-36), then fills, for rows
+ * j = 0..NY+1,
+ *   prof    [DG_PR_COUNT][NY+2]          the columns of mean.txt and tke.txt
+ *   prof_th [N_TH][DG_PRT_COUNT][NY+2]   the columns of mean_th.txt (may be
+ *                                        NULL when N_TH = 0)
+ *   bulk    [5] = UBULK, centreline U1, <urms>, <vrms>, <wrms>
+ * Rows 1..NY carry what the reference writes; EPSILON rows 2..NY-1
+ * (tke.txt); the means (UME, VME, WME, CP, THME) also rows 0 and NY+1.
+ * VME is on GY (mean.txt prints 0.5 (VME(j) + VME(j+1))).  Also advances
+ * NSAMPLES and the running means UBAR, VBAR, WBAR, THBAR
+ * (for/save_stats.f:99-114).  Replaces the reference's transforms with the
+ * discrete Parseval identity on the retained modes; the spectral state is
+ * left as it was (the reference's physical round trip changes it only by
+ * round-off). */
+enum {
+  DG_PR_UME = 0, DG_PR_VME, DG_PR_WME, DG_PR_URMS, DG_PR_VRMS, DG_PR_WRMS, DG_PR_UV, DG_PR_UW,
+  DG_PR_WV, DG_PR_DUDY, DG_PR_DWDY, DG_PR_CP, DG_PR_SHEAR, DG_PR_OMEGA_X, DG_PR_OMEGA_Y,
+  DG_PR_OMEGA_Z, DG_PR_EPSILON, DG_PR_COUNT
+};
+enum { DG_PRT_THME = 0, DG_PRT_DTHDY, DG_PRT_THRMS, DG_PRT_THV, DG_PRT_PE_DISS, DG_PRT_COUNT };
+int diablo_save_stats_chan(dg_handle *h, double *prof, double *prof_th, double *bulk);
+/* SAVE_STATS_CHAN's running means, rows 0..NY+1 (rows 1..NY updated):
+ * ubar, vbar, wbar [NY+2], thbar [N_TH][NY+2] (may be NULL); *nsamples =
+ * NSAMPLES.  What SAVE_STATS_CHAN(FINAL=.TRUE.) writes to stats.txt. */
+int diablo_stats_means(dg_handle *h, double *ubar, double *vbar, double *wbar, double *thbar,
+                       int *nsamples);
+
 #ifdef __cplusplus
 }
 #endif

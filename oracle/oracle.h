@@ -120,6 +120,22 @@ typedef struct orc_stats {
 void orc_stats_chan(const orc *o, orc_stats *s);
 void orc_stats_per(const orc *o, orc_stats *s);
 double orc_div_max_chan(const orc *o);
+
+/* SAVE_STATS_CHAN (for/save_stats.f:4-690) and tkebudget_chan
+ * (for/save_stats.f:963-1173) profiles, rows j = 0..NY+1 of each:
+ * prof [ORC_PR_COUNT][NY+2], prof_th [N_TH][ORC_PRT_COUNT][NY+2],
+ * bulk = {UBULK, centreline U, <urms>, <vrms>, <wrms>}.  Rows 1..NY hold
+ * the values the reference writes (mean.txt, mean_th.txt); EPSILON rows
+ * 2..NY-1 (tke.txt); the means also rows 0 and NY+1. */
+enum {
+  ORC_PR_UME, ORC_PR_VME, ORC_PR_WME, ORC_PR_URMS, ORC_PR_VRMS, ORC_PR_WRMS, ORC_PR_UV,
+  ORC_PR_UW, ORC_PR_WV, ORC_PR_DUDY, ORC_PR_DWDY, ORC_PR_CP, ORC_PR_SHEAR, ORC_PR_OMEGA_X,
+  ORC_PR_OMEGA_Y, ORC_PR_OMEGA_Z, ORC_PR_EPSILON, ORC_PR_COUNT
+};
+enum { ORC_PRT_THME, ORC_PRT_DTHDY, ORC_PRT_THRMS, ORC_PRT_THV, ORC_PRT_PE_DISS, ORC_PRT_COUNT };
+void orc_save_stats_chan(orc *o, double *prof, double *prof_th, double *bulk);
+void orc_stats_means_update(const orc *o, int nsamples, double *ubar, double *vbar,
+                            double *wbar, double *thbar);
 double orc_div_max_per(const orc *o);
 
 #ifdef __cplusplus

@@ -47,6 +47,12 @@ class OrcStats(ctypes.Structure):
                 ("th_var", c_d * MAX_TH)]
 
 
+# profile rows of orc_save_stats_chan, in the order of ORC_PR_* / ORC_PRT_*
+PROFILES = ("ume", "vme", "wme", "urms", "vrms", "wrms", "uv", "uw", "wv", "dudy", "dwdy", "cp",
+            "shear", "omega_x", "omega_y", "omega_z", "epsilon")
+PROFILES_TH = ("thme", "dthdy", "thrms", "thv", "pe_diss")
+
+
 def build(quiet: bool = True) -> str:
     """Compile liboracle.so with the Makefile beside this file."""
     r = subprocess.run(["make", "-s", "-C", _HERE], capture_output=True, text=True)
@@ -98,6 +104,8 @@ def lib():
         L.orc_div_max_chan.restype = c_d
         L.orc_div_max_per.argtypes = [P]
         L.orc_div_max_per.restype = c_d
+        L.orc_save_stats_chan.argtypes = [P, P, P, P]
+        L.orc_stats_means_update.argtypes = [P, c_i, P, P, P, P]
         L.orc_set_threads.argtypes = [c_i]
         _lib = L
     return _lib
@@ -256,6 +264,24 @@ class Oracle:
         d["thrms_b"] = list(s.thrms_b)[: self.p.n_th]
         d["th_var"] = list(s.th_var)[: self.p.n_th]
         return d
+
+    def save_stats_chan(self) -> dict:
+        """SAVE_STATS_CHAN + tkebudget_chan profiles (see oracle.h); runs
+        APPLY_BC_VEL on the state first, as the reference does."""
+        L = self.p.ny + 2
+        prof = np.zeros((len(PROFILES), L))
+        prof_th = np.zeros((max(self.p.n_th, 1), len(PROFILES_TH), L))
+        bulk = np.zeros(5)
+        lib().orc_save_stats_chan(self.h, _ptr(prof), _ptr(prof_th), _ptr(bulk))
+        out = {nm: prof[i] for i, nm in enumerate(PROFILES)}
+        out.update({nm: prof_th[: self.p.n_th, i] for i, nm in enumerate(PROFILES_TH)})
+        out.update(dict(zip(("ubulk", "uc", "urms_b", "vrms_b", "wrms_b"), bulk)))
+        return out
+
+    def stats_means_update(self, nsamples: int, ubar, vbar, wbar, thbar):
+        """SAVE_STATS_CHAN's running means (in place; REAL*4 weights)."""
+        lib().orc_stats_means_update(self.h, nsamples, _ptr(ubar), _ptr(vbar), _ptr(wbar),
+                                     _ptr(thbar))
 
     def div_max(self) -> float:
         if self.p.num_per_dir == 3:

@@ -101,6 +101,10 @@ def load(path: str = LIB_PATH):
                            ctypes.POINTER(D)],
         "diablo_stats": [P, ctypes.POINTER(DgStats)],
         "diablo_save_stats_chan": [P, P, P, P],
+        "diablo_save_flow": [P, I, ctypes.c_char_p, P],
+        "diablo_read_flow": [P, ctypes.c_char_p, P, ctypes.POINTER(I)],
+        "diablo_flow_fields_physical": [P, P, P, P, P, P],
+        "diablo_flow_fields_from_physical": [P, P, P, P, P, P, D],
         "diablo_stats_means": [P, P, P, P, P, ctypes.POINTER(I)],
     }
     L.dg_state_bytes.argtypes = [P]

@@ -31,6 +31,15 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+def _cstrings(paths, n):
+    if not paths:
+        return None
+    arr = (ctypes.c_char_p * max(n, 1))()
+    for i in range(n):
+        arr[i] = paths[i].encode() if i < len(paths) and paths[i] else None
+    return arr
+
+
 class _Solver:
     def __init__(self, p: Params, gy=None, stream=None):
         self.L = _lib.load()
@@ -121,6 +130,19 @@ class _Solver:
         self._call("diablo_get_field", _lib.field_id(name), ctypes.c_void_p(dev_ptr),
                    _lib.DG_LAYOUT_COMPACT, _lib.DG_DEVICE)
 
+    def save_flow(self, path: str, time_step: int, th_paths=None):
+        """SAVE_FLOW without HDF5 (for/diablo_io.f:307-404)."""
+        arr = _cstrings(th_paths, self.p.n_th)
+        self._call("diablo_save_flow", int(time_step), path.encode(), arr)
+
+    def read_flow(self, path: str, th_paths=None) -> int:
+        """READ_FLOW without HDF5 (for/diablo_io.f:201-305); returns
+        TIME_STEP and sets TIME from the file."""
+        arr = _cstrings(th_paths, self.p.n_th)
+        ts = ctypes.c_int()
+        self._call("diablo_read_flow", path.encode(), arr, ctypes.byref(ts))
+        return ts.value
+
     def state_names(self):
         n = ["CU1", "CU2", "CU3", "CP", "CF1", "CF2", "CF3"]
         n += [f"CTH{k}" for k in range(self.p.n_th)] + [f"CFTH{k}" for k in range(self.p.n_th)]
@@ -158,6 +180,33 @@ class _Solver:
 
 class Channel(_Solver):
     """Device-resident channel state driven through RK_CHAN_1 and helpers."""
+
+    def flow_fields_physical(self, pressure: bool = True) -> dict:
+        """The datasets of the reference's HDF5 flow file (WriteHDF5,
+        for/hdf5.f:5-292): physical U, V (on GYF), W, TH<n> and P on planes
+        1..NY as [NZ][NY][NX] arrays."""
+        nz, ny, nx = self.p.nz, self.p.ny, self.p.nx
+        U, V, W = (np.zeros((nz, ny, nx)) for _ in range(3))
+        TH = np.zeros((max(self.p.n_th, 1), nz, ny, nx))
+        P = np.zeros((nz, ny, nx)) if pressure else None
+        self._call("diablo_flow_fields_physical", _ptr(U), _ptr(V), _ptr(W),
+                   _ptr(TH) if self.p.n_th else None, _ptr(P) if pressure else None)
+        out = {"U": U, "V": V, "W": W}
+        for n in range(self.p.n_th):
+            out[f"TH{n + 1}"] = TH[n]
+        if pressure:
+            out["P"] = P
+        return out
+
+    def flow_fields_from_physical(self, d: dict, time: float):
+        """ReadHDF5 (for/hdf5.f:296-544) from the dataset arrays of
+        flow_fields_physical (P optional: without it POISSON_P_CHAN runs)."""
+        f = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+        U, V, W = f(d["U"]), f(d["V"]), f(d["W"])
+        TH = f(np.stack([d[f"TH{n + 1}"] for n in range(self.p.n_th)])) if self.p.n_th else None
+        P = f(d["P"]) if "P" in d else None
+        self._call("diablo_flow_fields_from_physical", _ptr(U), _ptr(V), _ptr(W),
+                   None if TH is None else _ptr(TH), None if P is None else _ptr(P), time)
 
     def save_stats(self) -> dict:
         """SAVE_STATS_CHAN(FINAL=.FALSE.) + tkebudget_chan profiles

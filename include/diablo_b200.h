@@ -239,6 +239,33 @@ int dg_server_wait(dg_server *s, int64_t id, double *const *state, double *times
 int dg_server_query(dg_server *s, dg_server_stats *st);
 int dg_server_destroy(dg_server *s);
 
+/* ------------------------------------------------------------ flow files */
+/* SAVE_FLOW / READ_FLOW without HDF5 (for/diablo_io.f:201-404): Fortran
+ * unformatted sequential files (4-byte record markers, little-endian), a
+ * header record NX, NY, NZ, NUM_PER_DIR, TIME, TIME_STEP and one record of
+ * retained modes.  Channel: CU1 J=1..NY, CU2 J=2..NY, CU3 J=1..NY; each
+ * scalar in its own file (fname_th[n], NULL to skip), written J=0..NY and
+ * read J=1..NY as the reference does (a file written by SAVE_FLOW comes
+ * back one plane lower).  Periodic: all ky planes.  Write uses the handle's
+ * TIME; read checks NX, NY, NZ and NUM_PER_DIR (DG_ERR_DIMS with the
+ * reference's message), sets TIME, returns TIME_STEP and, for the channel,
+ * runs APPLY_BC_VEL.  Records above 2 GiB return DG_ERR_DIMS. */
+int diablo_save_flow(dg_handle *h, int time_step, const char *fname, const char *const *fname_th);
+int diablo_read_flow(dg_handle *h, const char *fname, const char *const *fname_th,
+                     int *time_step);
+/* The datasets of the HDF5 flow files (WriteHDF5 / ReadHDF5,
+ * for/hdf5.f:5-544), channel only, for a host that writes the file with its
+ * own HDF5 library: physical U, V, W, TH(n) and P on planes 1..NY as
+ * C arrays [NZ][NY][NX] (Fortran tmp(NX,NY,NZ)), V moved onto GYF by G2GF.
+ * Any output may be NULL; TH is [N_TH][NZ][NY][NX].  The reverse (ReadHDF5)
+ * applies GF2G to V (walls set for zero mass flux), transforms, sets TIME,
+ * runs COURANT when VARIABLE_DT and POISSON_P_CHAN when P is NULL. */
+int diablo_flow_fields_physical(dg_handle *h, double *U, double *V, double *W, double *TH,
+                                double *P);
+int diablo_flow_fields_from_physical(dg_handle *h, const double *U, const double *V,
+                                     const double *W, const double *TH, const double *P,
+                                     double time);
+
 /* ------------------------------------------------------------ statistics */
 /* Parity statistics of the current state (channel or periodic); also checks
  * the state for non-finite values (returns DG_ERR_NAN if any). */

@@ -273,6 +273,7 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? (sizeof(CX) == 8 ? 4
   // carried x-spectra: 0 fl1, 1 fl3, 2 ubar1 u2, 3 ubar3 u2, 4 g, 5+n flth
   CX *pvs = stw + NX + XW_WARPS * MAXP * SSTR + warp * (5 + NTH) * NKXP;
   for (int i = threadIdx.x; i < NX; i += blockDim.x) stw[i] = tw[i];
+  dg_pdl_wait();  // H comes from the z inverse
   __syncthreads();
   const int z = blockIdx.x * XW_WARPS + warp;
   const int NZ = C.NZ;
@@ -710,6 +711,7 @@ __global__ void __launch_bounds__(128, zw_minb(NZ, sizeof(CX))) k_zfwd_w(
   const int jhi = (f == 0 || f == 2) ? C.JE : (f == 1 ? C.NY : sel(C.JEt, f - 3));
   if (j < jlo || j > jhi) return;
   for (int i = threadIdx.x; i < NZ; i += blockDim.x) stw[i] = tw[i];
+  dg_pdl_wait();  // G comes from the x-row kernel
   const CX *GA = G + (2 * f) * Gfield + (long)j * NZ * nkxp;
   const CX *GB = G + (2 * f + 1) * Gfield + (long)j * NZ * nkxp;
   for (int base = 0; base < 2 * KXG * NZ; base += 8 * 128) {
@@ -998,6 +1000,7 @@ __global__ void __launch_bounds__(COL_THR) k_cn_col(int NY, long ss, const doubl
   const int tid = threadIdx.x;
   const double *T = tab_rk + (long)f * 5 * L;
   for (int i = tid; i < 5 * L; i += COL_THR) TB[i] = T[i];
+  dg_pdl_wait();  // R comes from the z-forward kernel
   // staging with eight loads in flight per thread
   for (int base = 0; base < L * MT; base += 8 * COL_THR) {
     double2 v[8];
@@ -1104,6 +1107,7 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
     IDY[j] = (j >= 1) ? 1. / dy[j] : 0.0;
     IDYF[j] = (j >= 1 && j <= NY) ? 1. / dyf[j] : 0.0;
   }
+  dg_pdl_wait();  // the velocity comes from the CN solve
   __syncthreads();
   for (int base = 0; base < L * MT; base += 4 * COL_THR) {
     double2 a1[4], a3[4], b2[4], b2p[4];
@@ -1540,9 +1544,9 @@ int dg_cn_solve_dev(dg_handle *h, int rk_step) {
   if (mt == MTV) {                                                                      \
     dg_big_smem((const void *)k_cn_col<MTV>);                                           \
     dg_kt_begin(h, "k_cn_col", h->st);                                                  \
-    k_cn_col<MTV><<<grid, COL_THR, sm, h->st>>>(h->NY, h->ss, tab, rhs, cu,              \
-                                               make_int4(wl[0], wl[1], wl[2], wl[3]),    \
-                                               make_int4(wl[4], wl[5], wl[6], wl[7]));   \
+    DG_CUDA(dg_launch(h->pdl, k_cn_col<MTV>, grid, dim3(COL_THR), sm, h->st, h->NY, h->ss, \
+                      tab, rhs, cu, make_int4(wl[0], wl[1], wl[2], wl[3]),               \
+                      make_int4(wl[4], wl[5], wl[6], wl[7])));                          \
   }
   CN_CASE(4) CN_CASE(8) CN_CASE(16)
 #undef CN_CASE
@@ -1562,10 +1566,10 @@ int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step) {
   if (mt == MTV) {                                                                            \
     dg_big_smem((const void *)k_rd_col<MTV>);                                                 \
     dg_kt_begin(h, "k_rd_col", h->st);                                                        \
-    k_rd_col<MTV><<<dg_cdiv(h->ss, MTV), COL_THR, sm, h->st>>>(                               \
-        h->NY, h->ss, h->nkxp, h->jstart, h->jend, update_cp ? rk_step : 0, h->kx, h->kz,     \
-        h->dy, h->dyf, h->rem_a, h->rem_rb, h->cu[0], h->cu[1], h->cu[2], h->cp, h->cr1,      \
-        h->dscal);                                                                            \
+    DG_CUDA(dg_launch(h->pdl && update_cp, k_rd_col<MTV>, dim3(dg_cdiv(h->ss, MTV)),           \
+                      dim3(COL_THR), sm, h->st, h->NY, h->ss, h->nkxp, h->jstart, h->jend,    \
+                      update_cp ? rk_step : 0, h->kx, h->kz, h->dy, h->dyf, h->rem_a,         \
+                      h->rem_rb, h->cu[0], h->cu[1], h->cu[2], h->cp, h->cr1, h->dscal));     \
   }
   RD_CASE(4) RD_CASE(8) RD_CASE(16)
 #undef RD_CASE
@@ -1603,7 +1607,11 @@ static double courant_dt0(const dg_handle *h) {
 // the main stream runs next; the caller joins ev_cfl1 before the commit.
 int dg_courant_dev(dg_handle *h, const double2 *const *u, bool side) {
   // physical U1..U3 on planes 1..NY, reduced to COURANT's minimum on the fly
-  DG_TRY(dg_zinv(h, u, 3, 1, h->NY, h->H, 0));
+  // (inside a substep the z inverse follows the CN solve kernel)
+  h->pdl_zinv = side ? h->pdl : 0;
+  const int zs = dg_zinv(h, u, 3, 1, h->NY, h->H, 0);
+  h->pdl_zinv = 0;
+  DG_TRY(zs);
   cudaStream_t keep = h->st;
   if (side) {
     DG_CUDA(cudaEventRecord(h->ev_cfl0, h->st));
@@ -1665,8 +1673,11 @@ static int nl_chunk_mixed(dg_handle *h, const ChanConst &C, int rk_step, int a, 
   float2 *Hf = reinterpret_cast<float2 *>(h->H);
   float2 *Gf = reinterpret_cast<float2 *>(h->G);
   const long Hfield = (long)h->nplanes * h->NZ * h->nkxp;
-  DG_TRY(dg_cinv_gf(h, in, h->nf, hdone + 1, b + 1, h->ss, h->nkxp, h->NZ, h->NKZ, h->plz, h->twz_f,
-                    Hf, Hfield));
+  h->pdl_zinv = h->pdl;  // follows the previous substep's REM_DIV kernel
+  const int zs = dg_cinv_gf(h, in, h->nf, hdone + 1, b + 1, h->ss, h->nkxp, h->NZ, h->NKZ, h->plz,
+                            h->twz_f, Hf, Hfield);
+  h->pdl_zinv = 0;
+  DG_TRY(zs);
   hdone = b + 1;
   const int nplan = b - a + 1;
   int chunk = h->xrow_chunk;
@@ -1681,8 +1692,9 @@ static int nl_chunk_mixed(dg_handle *h, const ChanConst &C, int rk_step, int a, 
   if (!done && h->NX == NXV && h->NTH == NTHV) {                                                \
     dg_big_smem((const void *)k_xrow_w<NXV, NTHV, float2>);                                     \
     dg_kt_begin(h, "k_xrow_w_f32", h->st);                                                      \
-    k_xrow_w<NXV, NTHV, float2><<<grid, 32 * XW_WARPS, xw_smem<NXV, NTHV, float2>(), h->st>>>(  \
-        C, Hf, Hfield, chunk, a, b, h->twx_f, h->dyf, h->dy, h->kx, Gf, Hfield);                \
+    DG_CUDA(dg_launch(h->pdl, k_xrow_w<NXV, NTHV, float2>, grid, dim3(32 * XW_WARPS),           \
+                      xw_smem<NXV, NTHV, float2>(), h->st, C, Hf, Hfield, chunk, a, b,          \
+                      h->twx_f, h->dyf, h->dy, h->kx, Gf, Hfield));                             \
     done = true;                                                                                \
   }
 #define XW_ALL(NXV) XW_CASE(NXV, 0) XW_CASE(NXV, 1) XW_CASE(NXV, 2)
@@ -1701,9 +1713,9 @@ static int nl_chunk_mixed(dg_handle *h, const ChanConst &C, int rk_step, int a, 
   if (!done && h->NZ == N) {                                                                    \
     dg_big_smem((const void *)k_zfwd_w<N, float2>);                                             \
     dg_kt_begin(h, "k_zfwd_w_f32", h->st);                                                      \
-    k_zfwd_w<N, float2><<<zgrid, 128, sm, h->st>>>(C, Gf, Hfield, h->twz_f, h->dscal, rk_step,   \
-                                                   h->kx, h->kz, h->dy, h->dyf, cu, cf, rhs,    \
-                                                   h->cp, a);                                   \
+    DG_CUDA(dg_launch(h->pdl, k_zfwd_w<N, float2>, zgrid, dim3(128), sm, h->st, C, Gf, Hfield,  \
+                      h->twz_f, h->dscal, rk_step, h->kx, h->kz, h->dy, h->dyf, cu, cf, rhs,    \
+                      h->cp, a));                                                               \
     done = true;                                                                                \
   }
   ZW_CASE(16) ZW_CASE(32) ZW_CASE(48) ZW_CASE(64) ZW_CASE(96) ZW_CASE(128) ZW_CASE(256)
@@ -1738,7 +1750,10 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
       continue;
     }
     // 1. z inverse of the planes this chunk's x-rows need (a-1 .. b+1)
-    DG_TRY(dg_zinv(h, in, h->nf, hdone + 1, b + 1, h->H, 0));
+    h->pdl_zinv = h->pdl;
+    const int zs = dg_zinv(h, in, h->nf, hdone + 1, b + 1, h->H, 0);
+    h->pdl_zinv = 0;
+    DG_TRY(zs);
     hdone = b + 1;
     // 2. x-row nonlinear products for output planes a..b
     bool done = false;
@@ -1757,8 +1772,9 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
   if (h->NX == NXV && h->NTH == NTHV) {                                                          \
     dg_big_smem((const void *)k_xrow_w<NXV, NTHV>);                                              \
     dg_kt_begin(h, "k_xrow_w", h->st);                                                             \
-    k_xrow_w<NXV, NTHV><<<grid, 32 * XW_WARPS, xw_smem<NXV, NTHV>(), h->st>>>(                    \
-        C, h->H, Hfield, chunk, a, b, h->twx, h->dyf, h->dy, h->kx, h->G, Hfield);               \
+    DG_CUDA(dg_launch(h->pdl, k_xrow_w<NXV, NTHV>, grid, dim3(32 * XW_WARPS),                    \
+                      xw_smem<NXV, NTHV>(), h->st, C, h->H, Hfield, chunk, a, b, h->twx,        \
+                      h->dyf, h->dy, h->kx, h->G, Hfield));                                     \
     done = true;                                                                                 \
   }
 #define XW_ALL(NXV) XW_CASE(NXV, 0) XW_CASE(NXV, 1) XW_CASE(NXV, 2)
@@ -1804,8 +1820,8 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
   if (h->NZ == N) {                                                                            \
     dg_big_smem((const void *)k_zfwd_w<N>);                                                    \
     dg_kt_begin(h, "k_zfwd_w", h->st);                                                          \
-    k_zfwd_w<N><<<grid, 128, sm, h->st>>>(C, h->G, Hfield, h->twz, h->dscal, rk_step, h->kx,   \
-                                          h->kz, h->dy, h->dyf, cu, cf, rhs, h->cp, za);       \
+    DG_CUDA(dg_launch(h->pdl, k_zfwd_w<N>, grid, dim3(128), sm, h->st, C, h->G, Hfield, h->twz, \
+                      h->dscal, rk_step, h->kx, h->kz, h->dy, h->dyf, cu, cf, rhs, h->cp, za)); \
     zdone = true;                                                                              \
   }
       ZW_CASE(16) ZW_CASE(32) ZW_CASE(48) ZW_CASE(64) ZW_CASE(96) ZW_CASE(128) ZW_CASE(192)

@@ -144,6 +144,8 @@ struct dg_handle {
   bool defer_tables;            // dt commit leaves the CN tables to the next step
 
   // tunables (dg_tune_set / dg_autotune)
+  int pdl;                      // substep kernels use programmatic dependent launch
+  int pdl_zinv;                 // the next z inverse follows a kernel of the substep path
   int col_mt;                   // modes per CTA of the REM_DIV column kernel (4, 8, 16)
   int cn_mt;                    // modes per CTA of the CN column kernel (4, 8, 16)
   int xrow_chunk;               // planes per CTA of the x-row product kernel (0 = auto)
@@ -212,3 +214,28 @@ int dg_dt_commit(dg_handle *h);
 void dg_big_smem(const void *kern);
 
 static inline int dg_cdiv(long a, long b) { return (int)((a + b - 1) / b); }
+
+// Programmatic dependent launch.  A kernel launched with dg_launch(pdl = 1)
+// right after another kernel in the same stream may be scheduled as that
+// kernel's CTAs exit, before its completion is flushed: it must call
+// dg_pdl_wait() before it reads anything the predecessor writes (or writes
+// anything the predecessor reads); only constant tables may be touched
+// before.  The predecessors trigger implicitly as their CTAs exit (an explicit
+// trigger at kernel entry measured slower: the waiting CTAs held SM slots).
+// dg_pdl_wait() is a no-op for a plain launch.
+__device__ __forceinline__ void dg_pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+template <typename... KArgs, typename... Args>
+static inline cudaError_t dg_launch(int pdl, void (*kern)(KArgs...), dim3 grid, dim3 block,
+                                    size_t smem, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}

@@ -56,6 +56,7 @@ __global__ void __launch_bounds__(NTHR) k_zinv(PA fields, int jmin, long ss, int
   const int tid = threadIdx.x, nthr = blockDim.x;
   const auto *in = fields(f) + (long)j * ss;
   for (int i = tid; i < NZ; i += nthr) stw[i] = tw[i];
+  dg_pdl_wait();
   for (int base = 0; base < KXG * NZ; base += 8 * nthr) {
     using CI = typename std::remove_const<typename std::remove_pointer<decltype(in)>::type>::type;
     CI v[8];
@@ -218,6 +219,7 @@ __global__ void __launch_bounds__(NTHR) k_xc2r_cfl(const double2 *__restrict__ H
   const double2 *in = H + f * Hfield + (long)j * NZ * nkxp;
   const int NKX = nkxp - 1;
   for (int i = tid; i < NX; i += nthr) stw[i] = tw[i];
+  dg_pdl_wait();
   // bin k of Z = A + iB with the Hermitian extension of A and B; the row-pair
   // loads are issued four bins at a time per thread
   for (int base = 0; base < RPAIR * NX; base += 4 * nthr) {
@@ -353,7 +355,8 @@ static int cinv_t(dg_handle *h, const CI *const *fields, int nf, int jmin, int j
 #define KERNEL_BODY(NN)                                                                       \
   big_smem(k_zinv<NN, CX, PA>);                                                               \
   dg_kt_begin(h, "k_zinv", h->st);                                                            \
-  k_zinv<NN, CX, PA><<<grid, NTHR, sm, h->st>>>(fp, jmin, in_plane, rowlen, N, NK, pl, tw, H, out_field)
+  DG_CUDA(dg_launch(h->pdl_zinv, k_zinv<NN, CX, PA>, grid, dim3(NTHR), sm, h->st, fp, jmin,      \
+                    in_plane, rowlen, N, NK, pl, tw, H, out_field))
   switch (N) {
     DG_FOR_EACH_N(DG_CASE_N)
     default: KERNEL_BODY(0); break;
@@ -478,8 +481,8 @@ int dg_xc2r_cfl(dg_handle *h, const double2 *H, int jmin, int jmax, unsigned lon
 #define KERNEL_BODY(N)                                                                          \
   big_smem(k_xc2r_cfl<N>);                                                                      \
   dg_kt_begin(h, "k_xc2r_cfl", h->st);                                                              \
-  k_xc2r_cfl<N><<<grid, NTHR, sm, h->st>>>(H, Hf, jmin, h->nkxp, h->NX, h->NZ, h->plx, h->twx,     \
-                                          h->p.cfl, dxv, dzv, h->dy, out)
+  DG_CUDA(dg_launch(0, k_xc2r_cfl<N>, grid, dim3(NTHR), sm, h->st, H, Hf, jmin, h->nkxp,          \
+                    h->NX, h->NZ, h->plx, h->twx, h->p.cfl, dxv, dzv, h->dy, out))
   switch (h->NX) {
     DG_FOR_EACH_N(DG_CASE_N)
     default: KERNEL_BODY(0); break;

@@ -223,6 +223,7 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
   h->nf = 3 + h->NTH;
   h->col_mt = dg_default_col_mt(h);
   h->cn_mt = h->col_mt;
+  h->pdl = 1;
   h->pi = 4.0 * atan(1.0);
   h->eps = (double)(float)0.000000001;  // default-real literal, for/fft.f:74
   // INIT_CHAN_MPI with NPROCY = 1 (for/mpi.f:1080-1100)

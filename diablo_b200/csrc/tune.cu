@@ -11,6 +11,8 @@
 //                       halo planes; shorter ones give more CTAs.
 //   DG_TUNE_YCHUNK      planes per y-chunk of a substep (0 = all): smaller
 //                       chunks keep the intermediate planes in L2.
+//   DG_TUNE_PDL         1 (default): the substep kernels are launched with
+//                       programmatic dependent launch; 0: plain launches.
 //
 // dg_autotune times candidate values one tunable at a time (coordinate
 // descent) on the handle's own state with CUDA events over a few eager
@@ -53,6 +55,10 @@ extern "C" int dg_tune_set(dg_handle *h, int key, int value) {
       if (value < 0 || value > 1 << 20) return DG_ERR_ARG;
       h->ychunk = value;
       break;
+    case DG_TUNE_PDL:
+      if (value != 0 && value != 1) return DG_ERR_ARG;
+      h->pdl = value;
+      break;
     default:
       return DG_ERR_ARG;
   }
@@ -67,6 +73,7 @@ extern "C" int dg_tune_get(dg_handle *h, int key, int *value) {
     case DG_TUNE_CN_MT: *value = h->cn_mt; return DG_OK;
     case DG_TUNE_XROW_CHUNK: *value = h->xrow_chunk; return DG_OK;
     case DG_TUNE_YCHUNK: *value = h->ychunk; return DG_OK;
+    case DG_TUNE_PDL: *value = h->pdl; return DG_OK;
     default: return DG_ERR_ARG;
   }
 }

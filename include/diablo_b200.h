@@ -187,7 +187,8 @@ int dg_timing_read(dg_handle *h, int i, char *name, int name_len, int64_t *launc
  * the handle's own state (steps_per_trial eager RK3 steps each), keeps the
  * fastest and restores the state, TIME and DELTA_T; it allocates temporary
  * device copies of the state while it runs. */
-enum { DG_TUNE_COL_MT = 0, DG_TUNE_XROW_CHUNK = 1, DG_TUNE_YCHUNK = 2, DG_TUNE_CN_MT = 3 };
+enum { DG_TUNE_COL_MT = 0, DG_TUNE_XROW_CHUNK = 1, DG_TUNE_YCHUNK = 2, DG_TUNE_CN_MT = 3,
+       DG_TUNE_PDL = 4 };
 int dg_tune_set(dg_handle *h, int key, int value);
 int dg_tune_get(dg_handle *h, int key, int *value);
 int dg_autotune(dg_handle *h, int steps_per_trial);

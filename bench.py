@@ -324,17 +324,28 @@ def run_other_configs(args):
         g.close()
         out[f"periodic_256cubed_{'mixed' if prec else 'fp64'}"] = {
             "ms_per_step": ms, "mpoint_steps_per_s": 256 ** 3 / ms / 1e3}
-    # Re_tau ~ 550, 512 x 257 x 384, one scalar: FP64 only (no mixed kernels
-    # for 512-point rows)
+    # Re_tau ~ 550, 512 x 257 x 384, one scalar: FP64 and mixed from the same
+    # state, each timed over the same steps; the mixed fields are compared with
+    # the FP64 ones afterwards (relative L2, the configuration's comparison)
     p, gy = configs.channel_re550()
-    ch = Channel(p, gy, stream=stream)
     u1, u2, u3, th = ics.channel_laminar(p, gy, seed=4)
-    ch.create_flow(u1, u2, u3, th)
-    ch.set_time(0.0, p.delta_t)
-    ms = timed(ch, 5, warm=2)
-    ch.close()
-    out["channel_re550_512x257x384_fp64"] = {"ms_per_step": ms,
-                                              "mpoint_steps_per_s": p.nx * p.ny * p.nz / ms / 1e3}
+    fin = {}
+    for prec in (0, 1):
+        ch = Channel(p.replace(precision=prec), gy, stream=stream)
+        if prec == 0:
+            ch.create_flow(u1, u2, u3, th)
+            start = ch.get_state()
+        else:
+            ch.set_state(start)
+        ch.set_time(0.0, p.delta_t)
+        ms = timed(ch, 10, warm=3)
+        fin[prec] = {nm: ch.get_field(nm) for nm in ("CU1", "CU2", "CU3", "CTH0")}
+        ch.close()
+        out[f"channel_re550_512x257x384_{'mixed' if prec else 'fp64'}"] = {
+            "ms_per_step": ms, "mpoint_steps_per_s": p.nx * p.ny * p.nz / ms / 1e3}
+    out["channel_re550_512x257x384_mixed"]["rel_l2_vs_fp64_after_13_steps"] = {
+        nm: float(np.linalg.norm(fin[1][nm] - fin[0][nm]) / np.linalg.norm(fin[0][nm]))
+        for nm in fin[0]}
     return out
 
 

@@ -235,6 +235,225 @@ __global__ void __launch_bounds__(XP_THR, 5) k_xprod(
   }
 }
 
+// ------------------------------------------------- generic x-row stage, FP32
+// The mixed form of the two launches above, for the compile-time row lengths
+// without a warp x-row kernel (and for N_TH > 2).  As in k_xrow_w's FP32
+// form, every x-row is split into its mean (FP64) and its fluctuation
+// (FP32): k_xc2r_f takes the FP32 half-physical planes to physical
+// fluctuation rows (the kx = 0 bin removed) and keeps each row's mean;
+// k_xprod_f forms every product L1 L2 as D1 L2' + D2 L1' + L1' L2' in FP32
+// (D the means, L' the fluctuations), transforms the pairs in FP32 and puts
+// the FP64 row mean of the product, D1 D2 + <L1' L2'>, in the kx = 0 bin.
+
+// c2r of two z-rows of one field per warp (4 warps, 8 rows per CTA)
+template <int NT>
+__global__ void __launch_bounds__(128) k_xc2r_f(const float2 *__restrict__ H, long Hfield,
+                                               int NZ, int nkxp, const float2 *__restrict__ tw,
+                                               float *__restrict__ out, long ofield,
+                                               double *__restrict__ dc, long dfield) {
+  extern __shared__ double2 sm_raw[];
+  constexpr int NX = NT, SSTR = padded_len(NT);
+  float2 *stw = reinterpret_cast<float2 *>(sm_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2 *sig = stw + NX + warp * SSTR;
+  const int j = blockIdx.y, f = blockIdx.z;
+  const int za = blockIdx.x * 8 + 2 * warp, zb = za + 1;
+  for (int i = threadIdx.x; i < NX; i += 128) stw[i] = tw[i];
+  dg_pdl_wait();  // H comes from the z inverse
+  __syncthreads();
+  if (za >= NZ) return;
+  const float2 *ra = H + f * Hfield + ((long)j * NZ + za) * nkxp;
+  const bool hb = zb < NZ;
+  if (lane == 0) {
+    dc[f * dfield + (long)j * NZ + za] = (double)ra[0].x;
+    if (hb) dc[f * dfield + (long)j * NZ + zb] = (double)ra[nkxp].x;
+  }
+  for (int k = lane; k < NX; k += 32) {
+    const int kk = (k <= NX / 2) ? k : NX - k;
+    float2 v = make_float2(0.f, 0.f);
+    if (kk > 0 && kk < nkxp && kk < NX / 2) {
+      const float2 a = ra[kk];
+      const float2 b = hb ? ra[nkxp + kk] : make_float2(0.f, 0.f);
+      v = (k == kk) ? make_float2(a.x - b.y, a.y + b.x) : make_float2(a.x + b.y, -a.y + b.x);
+    }
+    sig[pad(k)] = v;
+  }
+  __syncwarp();
+  wpasses_any<NT, +1, 0>(sig, 1, SSTR, stw, lane);
+  float *oa = out + f * ofield + ((long)j * NZ + za) * NX;
+  for (int x = lane; x < NX; x += 32) {
+    const float2 v = sig[pad(x)];
+    oa[x] = v.x;
+    if (hb) oa[NX + x] = v.y;
+  }
+}
+
+// c0 F(f0, j+d0) + c1 F(f1, j+d1) (f1 < 0: one term)
+struct XLin {
+  int f0, d0, f1, d1;
+  double c0, c1;
+};
+struct XTerm {
+  double sg;
+  XLin l1, l2;
+};
+
+__device__ __forceinline__ XLin xl(int f, int d, double c = 1.0) { return {f, d, -1, 0, c, 0.0}; }
+__device__ __forceinline__ XLin xl2(int f0, int d0, double c0, int f1, int d1, double c1) {
+  return {f0, d0, f1, d1, c0, c1};
+}
+
+// the products of pair s (as listed before k_xprod), each a sum of +-L1 L2
+__device__ __forceinline__ void xpair_terms(int s, int nth, double dyfj, double dyfm, double wgy,
+                                            XTerm (&ta)[2], int &na, XTerm (&tb)[2], int &nb) {
+  na = 1;
+  nb = 2;
+  if (s == 0) {
+    ta[0] = {1.0, xl(2, 0), xl(0, 0)};
+    tb[0] = {1.0, xl2(2, 1, 1.0, 2, 0, 1.0), xl(1, 1)};
+    tb[1] = {-1.0, xl2(2, 0, 1.0, 2, -1, 1.0), xl(1, 0)};
+  } else if (s == 1) {
+    ta[0] = {1.0, xl(0, 0), xl(0, 0)};
+    tb[0] = {1.0, xl2(0, 1, 1.0, 0, 0, 1.0), xl(1, 1)};
+    tb[1] = {-1.0, xl2(0, 0, 1.0, 0, -1, 1.0), xl(1, 0)};
+  } else if (s == 2) {
+    ta[0] = {1.0, xl2(0, 0, dyfj * wgy, 0, -1, dyfm * wgy), xl(1, 0)};
+    tb[0] = {1.0, xl2(1, 0, 0.5, 1, 1, 0.5), xl2(1, 0, 0.5, 1, 1, 0.5)};
+    tb[1] = {-1.0, xl2(1, -1, 0.5, 1, 0, 0.5), xl2(1, -1, 0.5, 1, 0, 0.5)};
+  } else if (s == 3) {
+    ta[0] = {1.0, xl2(2, 0, dyfj * wgy, 2, -1, dyfm * wgy), xl(1, 0)};
+    tb[0] = {1.0, xl(2, 0), xl(2, 0)};
+    nb = 1;
+  } else if (s < 4 + nth) {
+    const int t = 3 + (s - 4);
+    ta[0] = {1.0, xl(t, 0), xl(0, 0)};
+    tb[0] = {1.0, xl2(t, 1, 1.0, t, 0, 1.0), xl(1, 1)};
+    tb[1] = {-1.0, xl2(t, 0, 1.0, t, -1, 1.0), xl(1, 0)};
+  } else {
+    const int n = 2 * (s - 4 - nth);
+    ta[0] = {1.0, xl(3 + n, 0), xl(2, 0)};
+    tb[0] = {1.0, xl(4 + n, 0), xl(2, 0)};
+    nb = (n + 1 < nth) ? 1 : 0;
+  }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(XP_THR) k_xprod_f(
+    ChanConst C, const float *__restrict__ ph, long pfield, const double *__restrict__ dc,
+    long dfield, const float2 *__restrict__ tw, const double *__restrict__ dyf,
+    const double *__restrict__ dy, const double *__restrict__ kxv, float2 *__restrict__ G,
+    long Gfield) {
+  extern __shared__ double2 sm_raw[];
+  constexpr int NX = NT, SSTR = padded_len(NT);
+  float2 *stw = reinterpret_cast<float2 *>(sm_raw);
+  const int NZ = C.NZ, nkxp = C.nkxp, nth = C.nth;
+  const int s = blockIdx.x, j = 1 + blockIdx.z;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int z = blockIdx.y * (XP_THR / 32) + warp;
+  for (int i = threadIdx.x; i < NX; i += XP_THR) stw[i] = tw[i];
+  dg_pdl_wait();  // the physical rows come from k_xc2r_f
+  __syncthreads();
+  if (z >= NZ) return;
+  const long pplane = (long)NZ * NX;
+  const double dyfj = dyf[j], dyfm = dyf[j - 1];
+  const double wgy = 1.0 / (2.0 * dy[j]);
+  XTerm ta[2], tb[2];
+  int na, nb;
+  xpair_terms(s, nth, dyfj, dyfm, wgy, ta, na, tb, nb);
+  const float *row0 = ph + (long)j * pplane + (long)z * NX;
+  auto Dm = [&](int f, int d) { return __ldg(dc + f * dfield + (long)(j + d) * NZ + z); };
+  auto lin_d = [&](const XLin &l) {
+    double v = l.c0 * Dm(l.f0, l.d0);
+    if (l.f1 >= 0) v += l.c1 * Dm(l.f1, l.d1);
+    return v;
+  };
+  auto lin_f = [&](const XLin &l, int x) {
+    float v = (float)l.c0 * __ldg(row0 + l.f0 * pfield + l.d0 * pplane + x);
+    if (l.f1 >= 0) v += (float)l.c1 * __ldg(row0 + l.f1 * pfield + l.d1 * pplane + x);
+    return v;
+  };
+  // means of L1, L2 per term and the mean-mean part of the product means
+  double Da[2][2], Db[2][2], dda = 0.0, ddb = 0.0;
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    if (t < na) {
+      Da[t][0] = lin_d(ta[t].l1);
+      Da[t][1] = lin_d(ta[t].l2);
+      dda += ta[t].sg * Da[t][0] * Da[t][1];
+    }
+    if (t < nb) {
+      Db[t][0] = lin_d(tb[t].l1);
+      Db[t][1] = lin_d(tb[t].l2);
+      ddb += tb[t].sg * Db[t][0] * Db[t][1];
+    }
+  }
+  float2 *sig = stw + NX + warp * SSTR;
+  double sa = 0.0, sb = 0.0;
+  for (int x = lane; x < NX; x += 32) {
+    float a = 0.f, b = 0.f;
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      if (t < na) {
+        const float l1 = lin_f(ta[t].l1, x), l2 = lin_f(ta[t].l2, x), ff = l1 * l2;
+        a += (float)ta[t].sg * ((float)Da[t][0] * l2 + (float)Da[t][1] * l1 + ff);
+        sa += ta[t].sg * (double)ff;
+      }
+      if (t < nb) {
+        const float l1 = lin_f(tb[t].l1, x), l2 = lin_f(tb[t].l2, x), ff = l1 * l2;
+        b += (float)tb[t].sg * ((float)Db[t][0] * l2 + (float)Db[t][1] * l1 + ff);
+        sb += tb[t].sg * (double)ff;
+      }
+    }
+    sig[pad(x)] = make_float2(a, b);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sa += __shfl_xor_sync(0xffffffffu, sa, o);
+    sb += __shfl_xor_sync(0xffffffffu, sb, o);
+  }
+  const double dca = dda + sa / (double)NX, dcb = ddb + sb / (double)NX;
+  __syncwarp();
+  wpasses_any<NT, -1, 0>(sig, 1, SSTR, stw, lane);
+  const double id2 = 1.0 / (2.0 * dyfj), idyj = 1.0 / dy[j];
+  float2 *obase = G + (long)j * NZ * nkxp + (long)z * nkxp;
+  for (int k = lane; k < nkxp; k += 32) {
+    double2 A, B;
+    if (k == 0) {
+      A = make_double2(dca, 0.0);
+      B = make_double2(dcb, 0.0);
+    } else {
+      const float2 zk = sig[pad(k)], zm = sig[pad(NX - k)];
+      const double ax = 0.5 * ((double)zk.x + (double)zm.x), ay = 0.5 * ((double)zk.y - (double)zm.y);
+      const double bx = 0.5 * ((double)zk.y + (double)zm.y), by = -0.5 * ((double)zk.x - (double)zm.x);
+      A = make_double2(ax / NX, ay / NX);
+      B = make_double2(bx / NX, by / NX);
+    }
+    const double KX = kxv[k];
+    auto flux = [&](double c) {
+      return make_float2((float)(KX * A.y - B.x * c), (float)(-KX * A.x - B.y * c));
+    };
+    const float2 Af = make_float2((float)A.x, (float)A.y), Bf = make_float2((float)B.x, (float)B.y);
+    float2 *o = obase + k;
+    if (s == 0) {
+      o[0] = Af;
+      o[5 * Gfield] = flux(id2);
+    } else if (s == 1) {
+      o[Gfield] = flux(id2);
+    } else if (s == 2) {
+      o[3 * Gfield] = flux(idyj);
+    } else if (s == 3) {
+      o[2 * Gfield] = Af;
+      o[4 * Gfield] = Bf;
+    } else if (s < 4 + nth) {
+      o[(7 + 2 * (s - 4)) * Gfield] = flux(id2);
+    } else {
+      const int n = 2 * (s - 4 - nth);
+      o[(6 + 2 * n) * Gfield] = Af;
+      if (n + 1 < nth) o[(8 + 2 * n) * Gfield] = Bf;
+    }
+  }
+}
+
 // ------------------------------------------------------- xrow, one warp/row
 // Same products as listed above, organised so a warp owns one physical z-row and
 // marches up through its chunk of planes with no CTA-wide barrier: the two
@@ -1660,8 +1879,11 @@ int dg_chan_init(dg_handle *h) {
   return dg_cn_tables(h);
 }
 
+// The mixed form needs a compile-time x length (the warp x-row kernel, or
+// the FP32 two-launch stage) and a warp z-forward length.
 bool dg_mixed_ok(int nx, int nz, int n_th) {
-  return xw_supported(nx) && zw_supported(nz) && n_th <= 2;
+  (void)n_th;
+  return fft_bufs(nx) == 1 && (zw_supported(nz) || zw_big(nz));
 }
 
 // Steps 1-3 of a substep in the mixed form: the z inverse converts the FP64
@@ -1718,7 +1940,86 @@ static int nl_chunk_mixed(dg_handle *h, const ChanConst &C, int rk_step, int a, 
                       h->cp, a));                                                               \
     done = true;                                                                                \
   }
-  ZW_CASE(16) ZW_CASE(32) ZW_CASE(48) ZW_CASE(64) ZW_CASE(96) ZW_CASE(128) ZW_CASE(256)
+  ZW_CASE(16) ZW_CASE(32) ZW_CASE(48) ZW_CASE(64) ZW_CASE(96) ZW_CASE(128) ZW_CASE(192)
+  ZW_CASE(256) ZW_CASE(384) ZW_CASE(512)
+#undef ZW_CASE
+  if (!done) {
+    dg_set_error("mixed precision: no FP32 z-forward kernel for this NZ");
+    return DG_ERR_DIMS;
+  }
+  DG_LAUNCHED();
+  return DG_OK;
+}
+
+// Steps 1-3 in the mixed form for x lengths without an FP32 warp x-row
+// kernel (or N_TH > 2): all planes at once through k_xc2r_f and k_xprod_f,
+// then the FP32 warp z-forward with its FP64 epilogue.
+static int nl_generic_mixed(dg_handle *h, const ChanConst &C, int rk_step,
+                            const double2 *const *in, FieldPtrs cu, FieldPtrs cf, FieldPtrs rhs) {
+  float2 *Hf = reinterpret_cast<float2 *>(h->H);
+  float2 *Gf = reinterpret_cast<float2 *>(h->G);
+  const long Hfield = (long)h->nplanes * h->NZ * h->nkxp;
+  const int NX = h->NX, NY = h->NY, NZ = h->NZ;
+  h->pdl_zinv = h->pdl;
+  const int zs = dg_cinv_gf(h, in, h->nf, 0, NY + 1, h->ss, h->nkxp, NZ, h->NKZ, h->plz, h->twz_f,
+                            Hf, Hfield);
+  h->pdl_zinv = 0;
+  DG_TRY(zs);
+  // work: FP32 fluctuation rows [nf][NY+2][NZ][NX], then FP64 row means [nf][NY+2][NZ]
+  const long pplane = (long)NZ * NX, pfield = (long)(NY + 2) * pplane;
+  float *phys = reinterpret_cast<float *>(h->work);
+  double *dc = reinterpret_cast<double *>(phys + h->nf * pfield);
+  const long dfield = (long)(NY + 2) * NZ;
+  bool done = false;
+  {
+    dim3 grid(dg_cdiv(NZ, 8), NY + 2, h->nf);
+    const size_t sm = sizeof(float2) * (NX + 4 * (size_t)padded_len(NX));
+#define XC_CASE(N)                                                                              \
+  if (!done && NX == N) {                                                                       \
+    dg_big_smem((const void *)k_xc2r_f<N>);                                                     \
+    dg_kt_begin(h, "k_xc2r_f32", h->st);                                                        \
+    DG_CUDA(dg_launch(h->pdl, k_xc2r_f<N>, grid, dim3(128), sm, h->st, Hf, Hfield, NZ, h->nkxp, \
+                      h->twx_f, phys, pfield, dc, dfield));                                     \
+    done = true;                                                                                \
+  }
+    DG_FOR_EACH_N(XC_CASE)
+#undef XC_CASE
+  }
+  if (!done) {
+    dg_set_error("mixed precision: no FP32 x-row kernel for this NX");
+    return DG_ERR_DIMS;
+  }
+  DG_LAUNCHED();
+  done = false;
+  {
+    dim3 grid(xp_pairs(h->NTH), dg_cdiv(NZ, XP_THR / 32), NY);
+    const size_t sm = sizeof(float2) * (NX + (XP_THR / 32) * (size_t)padded_len(NX));
+#define XP_CASE(N)                                                                              \
+  if (!done && NX == N) {                                                                       \
+    dg_big_smem((const void *)k_xprod_f<N>);                                                    \
+    dg_kt_begin(h, "k_xprod_f32", h->st);                                                       \
+    DG_CUDA(dg_launch(h->pdl, k_xprod_f<N>, grid, dim3(XP_THR), sm, h->st, C, phys, pfield, dc, \
+                      dfield, h->twx_f, h->dyf, h->dy, h->kx, Gf, Hfield));                     \
+    done = true;                                                                                \
+  }
+    DG_FOR_EACH_N(XP_CASE)
+#undef XP_CASE
+  }
+  DG_LAUNCHED();
+  done = false;
+  dim3 zgrid(dg_cdiv(h->nkxp, zw_kxg(NZ)), NY, h->nf);
+  const size_t sm = zw_smem<float2>(NZ);
+#define ZW_CASE(N)                                                                              \
+  if (!done && NZ == N) {                                                                       \
+    dg_big_smem((const void *)k_zfwd_w<N, float2>);                                             \
+    dg_kt_begin(h, "k_zfwd_w_f32", h->st);                                                      \
+    DG_CUDA(dg_launch(h->pdl, k_zfwd_w<N, float2>, zgrid, dim3(128), sm, h->st, C, Gf, Hfield,  \
+                      h->twz_f, h->dscal, rk_step, h->kx, h->kz, h->dy, h->dyf, cu, cf, rhs,    \
+                      h->cp, 1));                                                               \
+    done = true;                                                                                \
+  }
+  ZW_CASE(16) ZW_CASE(32) ZW_CASE(48) ZW_CASE(64) ZW_CASE(96) ZW_CASE(128) ZW_CASE(192)
+  ZW_CASE(256) ZW_CASE(384) ZW_CASE(512)
 #undef ZW_CASE
   if (!done) {
     dg_set_error("mixed precision: no FP32 z-forward kernel for this NZ");
@@ -1743,7 +2044,12 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
   FieldPtrs cu, cf, rhs;
   for (int f = 0; f < h->nf; f++) { cu.p[f] = h->cu[f]; cf.p[f] = h->cf[f]; rhs.p[f] = h->rhs[f]; }
   int hdone = -1;  // last H plane already produced
-  for (int a = 1; a <= h->NY; a += cj) {
+  int a0 = 1;
+  if (h->mixed && !(xw_supported(h->NX) && h->NTH <= 2)) {
+    DG_TRY(nl_generic_mixed(h, C, rk_step, in, cu, cf, rhs));
+    a0 = h->NY + 1;  // every plane done: no chunk loop
+  }
+  for (int a = a0; a <= h->NY; a += cj) {
     const int b = (a + cj - 1 < h->NY) ? a + cj - 1 : h->NY;
     if (h->mixed) {
       DG_TRY(nl_chunk_mixed(h, C, rk_step, a, b, hdone, in, cu, cf, rhs));

@@ -93,6 +93,59 @@ def test_mixed_two_scalars_short():
     g.close()
 
 
+def test_mixed_generic_rows_three_scalars():
+    """N_TH = 3 takes the FP32 two-launch x-row stage (k_xc2r_f, k_xprod_f)."""
+    p, gy = configs.kh_shear_layer(nx=64, ny=33, nz=32)
+    p = p.replace(n_th=3)
+    p.ri = [0.1, 0.05, -0.02, 0]
+    p.pr = [1.0, 2.0, 0.5, 1]
+    p.th_bc_ymin = [0, 1, 0, 0]
+    p.th_bc_ymax = [0, 1, 1, 0]
+    ref, g = pair(p, gy, ics.kh_shear_layer, seed=3)
+    for s in range(1, 41):
+        ref.step(s)
+        g.steps(s, 1)
+    err = {nm: rel(g.get_field(nm), ref.get(nm)) for nm in fields(p)}
+    assert all(v <= TOL_MIXED for v in err.values()), err
+    assert g.stats()["div_max"] <= 1e-12
+    g.close()
+
+
+def test_mixed_wide_512x384_rows():
+    """The 512 x 384 plane of the Re_tau~550 configuration in the mixed form
+    (FP32 two-launch x-row stage, FP32 384-point warp z-forward)."""
+    p, gy = configs.channel_re550(ny=17)
+    ref, g = pair(p, gy, ics.channel_laminar, seed=13)
+    for s in range(1, 11):
+        ref.step(s)
+        g.steps(s, 1)
+    err = {nm: rel(g.get_field(nm), ref.get(nm)) for nm in fields(p)}
+    assert all(v <= TOL_MIXED for v in err.values()), err
+    g.close()
+
+
+def test_mixed_re550_full_against_fp64_gpu():
+    """Re_tau~550 at full size, 512x257x384 with one scalar: the mixed form
+    against the FP64 path on the same GPU after 100 steps (the configuration's
+    stated comparison), at the same 1e-5 bar."""
+    from diablo_b200.solver import Channel
+    p, gy = configs.channel_re550()
+    u1, u2, u3, th = ics.channel_laminar(p, gy, seed=4)
+    a = Channel(p, gy)
+    a.create_flow(u1, u2, u3, th)
+    a.set_time(0.0, p.delta_t)
+    b = Channel(p.replace(precision=1), gy)
+    b.set_state(a.get_state())
+    b.set_time(0.0, p.delta_t)
+    a.steps(1, 100)
+    b.steps(1, 100)
+    err = {nm: rel(b.get_field(nm), a.get_field(nm)) for nm in fields(p)}
+    assert all(v <= TOL_MIXED for v in err.values()), err
+    assert abs(b.get_time()[0] - a.get_time()[0]) <= 1e-6 * a.get_time()[0]
+    a.close()
+    b.close()
+
+
 def periodic_pair(p, seed=3, scalars=None):
     import math
     from diablo_b200.solver import Periodic

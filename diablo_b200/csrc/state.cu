@@ -35,17 +35,6 @@ int dalloc(dg_handle *h, T **p, size_t count) {
   return DG_OK;
 }
 
-__global__ void k_ref_to_compact(const double2 *__restrict__ ref, double2 *__restrict__ cmp,
-                                 int nplanes, int nzt, int nkxp, int nxp1, int nz2) {
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long tot = (long)nplanes * nzt * nkxp;
-  if (q >= tot) return;
-  const int i = (int)(q % nkxp);
-  const int k = (int)((q / nkxp) % nzt);
-  const int j = (int)(q / ((long)nkxp * nzt));
-  cmp[q] = ref[((long)j * nz2 + k) * nxp1 + i];
-}
-
 __global__ void k_compact_to_ref(const double2 *__restrict__ cmp, double2 *__restrict__ ref,
                                  int nplanes, int nzt, int nkxp, int nxp1, int nz2) {
   const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -477,20 +466,17 @@ extern "C" int diablo_set_field(dg_handle *h, int field, const double *src, int 
                             where == DG_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
                             h->st));
   } else {
+    // the retained block of the reference array -- kx 0..NKX of kz slots
+    // 0..TNKZ of every plane -- is the compact array with a wider row and
+    // plane pitch: one strided copy, and the padding never crosses the bus
     int nxp1, nz2;
     ref_dims(h, &nxp1, &nz2);
-    const size_t nr = (size_t)h->nplanes * nz2 * nxp1;
-    const double2 *dref = (const double2 *)src;
-    double2 *tmp = nullptr;
-    if (where == DG_HOST) {
-      DG_CUDA(cudaMallocAsync((void **)&tmp, nr * sizeof(double2), h->st));
-      DG_CUDA(cudaMemcpyAsync(tmp, src, nr * sizeof(double2), cudaMemcpyHostToDevice, h->st));
-      dref = tmp;
-    }
-    k_ref_to_compact<<<dg_cdiv(nc, 256), 256, 0, h->st>>>(dref, dst, h->nplanes, h->nkzt, h->nkxp,
-                                                         nxp1, nz2);
-    DG_LAUNCHED();
-    if (tmp) DG_CUDA(cudaFreeAsync(tmp, h->st));
+    cudaMemcpy3DParms prm = {};
+    prm.srcPtr = make_cudaPitchedPtr((void *)src, sizeof(double2) * nxp1, nxp1, nz2);
+    prm.dstPtr = make_cudaPitchedPtr(dst, sizeof(double2) * h->nkxp, h->nkxp, h->nkzt);
+    prm.extent = make_cudaExtent(sizeof(double2) * h->nkxp, h->nkzt, h->nplanes);
+    prm.kind = where == DG_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    DG_CUDA(cudaMemcpy3DAsync(&prm, h->st));
   }
   DG_CUDA(cudaStreamSynchronize(h->st));
   return DG_OK;

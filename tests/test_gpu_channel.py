@@ -356,3 +356,31 @@ def test_autotune_restores_state_and_keeps_results():
         c.close()
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("periodic", [False, True])
+def test_reference_layout_round_trip(periodic):
+    """diablo_set_field / diablo_get_field in the reference layout
+    (0:NX/2, 0:NZ+1, planes): set reads only the retained block, get writes
+    the retained block and zeros elsewhere."""
+    import math
+    from diablo_b200.solver import Channel, Periodic
+    if periodic:
+        p = Params(nx=48, ny=24, nz=36, num_per_dir=3, nu=0.01, lx=2 * math.pi,
+                   ly=2 * math.pi, lz=2 * math.pi, delta_t=0.005, variable_dt=0)
+        s = Periodic(p)
+    else:
+        p, gy = configs.kh_shear_layer(nx=48, ny=17, nz=36)
+        s = Channel(p, gy)
+    cmp_shape = s.get_field("CU1").shape                 # (planes, TNKZ+1, NKX+1)
+    planes, nkzt, nkxp = cmp_shape
+    rng = np.random.default_rng(21)
+    ref = rng.standard_normal((planes, p.nz + 2, p.nx // 2 + 1)) \
+        + 1j * rng.standard_normal((planes, p.nz + 2, p.nx // 2 + 1))
+    s.set_field("CU2", ref, layout="reference")
+    assert np.array_equal(s.get_field("CU2"), ref[:, :nkzt, :nkxp])
+    back = s.get_field("CU2", layout="reference")
+    want = np.zeros_like(ref)
+    want[:, :nkzt, :nkxp] = ref[:, :nkzt, :nkxp]
+    assert np.array_equal(back, want)
+    s.close()

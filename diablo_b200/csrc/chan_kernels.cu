@@ -1201,41 +1201,44 @@ __global__ void k_remdiv_init(int NY, long ss, int nkxp, const double *__restric
 constexpr int COL_THR = 128;
 
 // CN solve of one field for MT modes (rows 0..NY+1, tables of this substep).
+// The R tile (all planes x MT modes) arrives by bulk tensor copies, nbox
+// boxes of `by` planes, while the threads stage the CN tables.
 template <int MT>
 __global__ void __launch_bounds__(COL_THR) k_cn_col(int NY, long ss, const double *__restrict__ tab_rk,
-                                                   FieldPtrs rhs, FieldPtrs cu, int4 wlo_a,
-                                                   int4 wlo_b) {
-  extern __shared__ double2 csm[];
+                                                   const __grid_constant__ CnMaps maps, int by,
+                                                   int nbox, FieldPtrs cu, int4 wlo_a,
+                                                   int4 wlo_b, int *__restrict__ err) {
+  extern __shared__ __align__(128) unsigned char csm_raw[];
+  unsigned char *sbase = csm_raw + ((128u - (dg_smem_addr(csm_raw) & 127u)) & 127u);
   const int L = NY + 2;
   const int f = blockIdx.y;
   const long m0 = (long)blockIdx.x * MT;
-  const int mt = (int)((ss - m0) < MT ? (ss - m0) : MT);
-  double2 *X = csm;                                 // [j][MT]
-  double *TB = (double *)(X + (long)L * MT);    // [5][L]
-  const double2 *__restrict__ R = rhs(f);
+  double2 *X = reinterpret_cast<double2 *>(sbase);                    // [nbox * by][MT]
+  double *TB = reinterpret_cast<double *>(X + (long)nbox * by * MT);  // [5][L]
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(TB + 5 * L);
   double2 *__restrict__ U = cu(f);
   const int wl[8] = {wlo_a.x, wlo_a.y, wlo_a.z, wlo_a.w, wlo_b.x, wlo_b.y, wlo_b.z, wlo_b.w};
   const int wlo = wl[f];
   const int tid = threadIdx.x;
+  if (tid == 0) dg_mbar_init(bar, 1);
+  __syncthreads();
+  dg_pdl_wait();  // R comes from the z-forward kernel
+  if (tid == 0) {
+    // columns beyond ss and planes beyond L arrive as zeros
+    dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * nbox * by * MT));
+    for (int q = 0; q < nbox; q++)
+      dg_tma_load_2d(X + (long)q * by * MT, &maps.m[f], (int)(2 * m0), q * by, bar);
+  }
   const double *T = tab_rk + (long)f * 5 * L;
   for (int i = tid; i < 5 * L; i += COL_THR) TB[i] = T[i];
-  dg_pdl_wait();  // R comes from the z-forward kernel
-  // staging with eight loads in flight per thread
-  for (int base = 0; base < L * MT; base += 8 * COL_THR) {
-    double2 v[8];
-#pragma unroll
-    for (int u = 0; u < 8; u++) {
-      const int i = base + u * COL_THR + tid;
-      const int m = i % MT, j = i / MT;
-      v[u] = (i < L * MT && m < mt) ? R[(long)j * ss + m0 + m] : make_double2(0.0, 0.0);
-    }
-#pragma unroll
-    for (int u = 0; u < 8; u++) {
-      const int i = base + u * COL_THR + tid;
-      if (i < L * MT) X[i] = v[u];
-    }
-  }
+  const bool landed = dg_mbar_wait(bar, 0);
   __syncthreads();
+  if (!landed) {
+    if (tid == 0) atomicExch(err + 1, 1);
+    dg_mbar_wait(bar, 0);  // give the copies in flight one more bounded wait
+    return;
+  }
+  const int mt = (int)((ss - m0) < MT ? (ss - m0) : MT);
   if (tid < 2 * MT) {
     const int m = tid >> 1, part = tid & 1;
     const double *Aa = TB, *Rb = TB + L, *Cc = TB + 2 * L, *K = TB + 3 * L, *V = TB + 4 * L;
@@ -1749,23 +1752,36 @@ int dg_cn_solve_dev(dg_handle *h, int rk_step) {
     DG_CUDA(cudaStreamWaitEvent(h->st, h->ev_join, 0));
     h->tables_pending = false;
   }
-  FieldPtrs cu, rhs;
-  for (int f = 0; f < h->nf; f++) { cu.p[f] = h->cu[f]; rhs.p[f] = h->rhs[f]; }
+  FieldPtrs cu;
+  for (int f = 0; f < h->nf; f++) cu.p[f] = h->cu[f];
   int wl[8] = {1, 1, 1, 1, 1, 1, 1, 1};
   for (int n = 0; n < h->NTH; n++) wl[3 + n] = h->jstart_th[n] - 1;
   const int L = h->NY + 2;
   const double *tab = h->cn_tab + (long)(rk_step - 1) * (3 + DG_MAX_TH) * 5 * L;
+  // the column arrives in nbox boxes of `by` planes (a box is at most 256
+  // planes; a multiple of 8 planes keeps every box's shared-memory
+  // destination 128-byte aligned for any modes per CTA)
+  const int nbox = dg_cdiv(L, 256), by = (dg_cdiv(L, nbox) + 7) / 8 * 8;
+  auto cn_smem = [&](int m) {
+    return sizeof(double2) * (size_t)nbox * by * m + sizeof(double) * 5 * L + 8 + 128;
+  };
   int mt = h->cn_mt;  // fewer modes per CTA where a tall column needs it
-  while (mt > 4 && sizeof(double2) * L * mt + sizeof(double) * 5 * L > 220 * 1024) mt /= 2;
-  const size_t sm = sizeof(double2) * L * mt + sizeof(double) * 5 * L;
+  while (mt > 4 && cn_smem(mt) > 220 * 1024) mt /= 2;
+  const size_t sm = cn_smem(mt);
+  if (h->cn_maps_mt != mt) {
+    for (int f = 0; f < h->nf; f++)
+      DG_TRY(dg_tmap_planes(h->rhs[f], h->ss, L, mt, by, &h->cn_maps->m[f]));
+    h->cn_maps_mt = mt;
+  }
+  const CnMaps maps = *h->cn_maps;
   dim3 grid(dg_cdiv(h->ss, mt), h->nf);
 #define CN_CASE(MTV)                                                                    \
   if (mt == MTV) {                                                                      \
     dg_big_smem((const void *)k_cn_col<MTV>);                                           \
     dg_kt_begin(h, "k_cn_col", h->st);                                                  \
     DG_CUDA(dg_launch(h->pdl, k_cn_col<MTV>, grid, dim3(COL_THR), sm, h->st, h->NY, h->ss, \
-                      tab, rhs, cu, make_int4(wl[0], wl[1], wl[2], wl[3]),               \
-                      make_int4(wl[4], wl[5], wl[6], wl[7])));                          \
+                      tab, maps, by, nbox, cu, make_int4(wl[0], wl[1], wl[2], wl[3]),    \
+                      make_int4(wl[4], wl[5], wl[6], wl[7]), h->dflag));                \
   }
   CN_CASE(4) CN_CASE(8) CN_CASE(16)
 #undef CN_CASE
@@ -1872,6 +1888,8 @@ int dg_dt_commit(dg_handle *h) {
 }
 
 int dg_chan_init(dg_handle *h) {
+  h->cn_maps = new CnMaps();
+  h->cn_maps_mt = 0;
   dg_kt_begin(h, "k_remdiv_init", h->st);
   k_remdiv_init<<<dg_cdiv(h->ss, 128), 128, 0, h->st>>>(h->NY, h->ss, h->nkxp, h->kx, h->kz, h->dy,
                                                         h->dyf, h->rem_a, h->rem_rb);

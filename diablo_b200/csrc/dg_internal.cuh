@@ -1,6 +1,7 @@
 // Internal declarations shared by the diablo_b200 CUDA sources.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
@@ -74,6 +75,12 @@ enum { F_U1 = 0, F_U2 = 1, F_U3 = 2, F_TH0 = 3 };
 
 struct dg_ktimer;
 
+// Tensor maps of the CN right-hand-side columns, one per field: 2-D over
+// [plane][2 ss doubles] (the CN column kernel's grid row is the field).
+struct CnMaps {
+  CUtensorMap m[3 + DG_MAX_TH];
+};
+
 struct dg_handle {
   dg_params p;
   int NX, NY, NZ, NTH, NKX, NKZ, TNKZ, NKY, TNKY;
@@ -146,6 +153,8 @@ struct dg_handle {
   // tunables (dg_tune_set / dg_autotune)
   int pdl;                      // substep kernels use programmatic dependent launch
   int pdl_zinv;                 // the next z inverse follows a kernel of the substep path
+  CnMaps *cn_maps;              // tensor maps of the CN right-hand sides (built per modes/CTA)
+  int cn_maps_mt;               // modes per CTA the maps were built for (0: none)
   int col_mt;                   // modes per CTA of the REM_DIV column kernel (4, 8, 16)
   int cn_mt;                    // modes per CTA of the CN column kernel (4, 8, 16)
   int xrow_chunk;               // planes per CTA of the x-row product kernel (0 = auto)
@@ -224,6 +233,54 @@ static inline int dg_cdiv(long a, long b) { return (int)((a + b - 1) / b); }
 // trigger at kernel entry measured slower: the waiting CTAs held SM slots).
 // dg_pdl_wait() is a no-op for a plain launch.
 __device__ __forceinline__ void dg_pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// ------------------------------------------------------------------- TMA
+// Bulk tensor copies (cp.async.bulk.tensor, no multicast) into shared memory,
+// completed on an mbarrier.  Waits are bounded: a copy that does not land
+// within DG_ASYNC_SPIN polls sets dg_handle::dflag[1] (reported by the next
+// diablo_stats / diablo_synchronize) and the kernel skips its work.
+#define DG_ASYNC_SPIN (1L << 24)
+
+__device__ __forceinline__ unsigned dg_smem_addr(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void dg_mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(dg_smem_addr(bar)), "r"(count)
+               : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void dg_mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(dg_smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// 2-D tiled load of box (x, y) of the tensor map into shared memory at dst
+__device__ __forceinline__ void dg_tma_load_2d(void *dst, const CUtensorMap *map, int x, int y,
+                                               unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dg_smem_addr(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(dg_smem_addr(bar))
+      : "memory");
+}
+// true once phase `parity` of the barrier completed; false after the limit
+__device__ __forceinline__ bool dg_mbar_wait(unsigned long long *bar, unsigned parity) {
+  const unsigned a = dg_smem_addr(bar);
+  for (long it = 0; it < DG_ASYNC_SPIN; it++) {
+    unsigned done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// host: a 2-D FP64 tensor map over planes of complex modes -- x = 2*ss
+// doubles of a plane (row stride ss complex), y = rows planes; box 2*mt x by
+int dg_tmap_planes(const void *base, long ss, int rows, int mt, int by, CUtensorMap *out);
+
 template <typename... KArgs, typename... Args>
 static inline cudaError_t dg_launch(int pdl, void (*kern)(KArgs...), dim3 grid, dim3 block,
                                     size_t smem, cudaStream_t st, Args... args) {

@@ -332,6 +332,7 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
   DG_TRY(dalloc(h, &h->dscal, 16));
   DG_TRY(dalloc(h, &h->dmin_bits, 32));
   DG_TRY(dalloc(h, &h->dflag, 4));
+  DG_CUDA(cudaMemsetAsync(h->dflag, 0, 4 * sizeof(int), h->st));
   const size_t ns = (size_t)h->nspec;
   for (int f = 0; f < h->nf; f++) {
     DG_TRY(dalloc(h, &h->cu[f], ns));
@@ -384,6 +385,7 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
   dg_kt_free(h);
   dg_graphs_free(h);
   free(h->h_ubar);
+  delete h->cn_maps;
   cudaEventDestroy(h->ev_fork);
   cudaEventDestroy(h->ev_join);
   cudaEventDestroy(h->ev_cfl0);
@@ -396,11 +398,24 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
   return DG_OK;
 }
 
+// dflag[1] is set by a kernel whose bulk tensor copies did not land within
+// its bounded wait (the kernel then skipped its work)
+static int check_async_flag(dg_handle *h) {
+  int f = 0;
+  DG_CUDA(cudaMemcpyAsync(&f, h->dflag + 1, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  if (f) {
+    dg_set_error("a bulk tensor copy did not complete within its wait limit; results are invalid");
+    return DG_ERR_CUDA;
+  }
+  return DG_OK;
+}
+
 extern "C" int diablo_synchronize(dg_handle *h) {
   if (!h) return DG_ERR_ARG;
   DG_CUDA(cudaStreamSynchronize(h->st2));
   DG_CUDA(cudaStreamSynchronize(h->st));
-  return DG_OK;
+  return check_async_flag(h);
 }
 
 extern "C" int diablo_set_time(dg_handle *h, double time, double delta_t) {
@@ -515,5 +530,6 @@ extern "C" int diablo_get_field(dg_handle *h, int field, double *dst, int layout
 
 extern "C" int diablo_stats(dg_handle *h, dg_stats *s) {
   if (!h || !s) return DG_ERR_ARG;
+  DG_TRY(check_async_flag(h));
   return dg_stats_dev(h, s);
 }

@@ -71,6 +71,9 @@ class Params:
     drhodz: List[float] = field(default_factory=lambda: [0.0] * MAX_TH)
     background_grad: List[int] = field(default_factory=lambda: [0] * MAX_TH)
     epsilon_target: float = 0.0
+    les: int = 0                    # USE_LES (input.dat)
+    les_model_type: int = 1         # input_chan.dat; the MPI build runs only 1
+    create_new_flow: int = 0        # input.dat; the subgrid model waits 100 steps
 
     # derived sizes (for/header:22-28)
     @property
@@ -141,6 +144,7 @@ def _c_fields():
         ("ri", d * MAX_TH), ("pr", d * MAX_TH), ("drhodx", d * MAX_TH), ("drhodz", d * MAX_TH),
         ("background_grad", i * MAX_TH),
         ("epsilon_target", d),
+        ("les", i), ("les_model_type", i), ("create_new_flow", i), ("_pad1", i),
     ]
 
 
@@ -189,8 +193,10 @@ def read_input_dat(path, p: Params | None = None, n_th: int | None = None) -> Pa
     t = _tok(L[8])
     p.nu, p.beta, p.lx, p.ly, p.lz = map(_f, t[:5])
     p.nu_v_scale = _f(_tok(L[10])[0])
+    p.les = int(_b(_tok(L[6])[1]))
     t = _tok(L[12])
     p.num_per_dir = int(t[0])
+    p.create_new_flow = int(_b(t[1]))
     t = _tok(L[14])
     p.delta_t = _f(t[2])
     p.variable_dt = int(_b(t[4]))
@@ -209,6 +215,7 @@ def read_input_chan(path, p: Params) -> Params:
     L = _data_lines(path)
     if float(_tok(L[4])[0]) != 2.0:
         raise ValueError("Wrong input data format input_chan")
+    p.les_model_type = int(_tok(L[8])[0])
     t = _tok(L[12])
     p.i_ro = _f(t[0])
     t = _tok(L[14])

@@ -76,6 +76,10 @@ typedef struct dg_params {
   double ri[DG_MAX_TH], pr[DG_MAX_TH], drhodx[DG_MAX_TH], drhodz[DG_MAX_TH];
   int32_t background_grad[DG_MAX_TH];
   double epsilon_target;
+  int32_t les;                /* USE_LES (input.dat, for/diablo_io.f:25) */
+  int32_t les_model_type;     /* for/channel.f:1477; the MPI build runs only 1 */
+  int32_t create_new_flow;    /* for/diablo_io.f:31: the model waits 100 steps */
+  int32_t pad1;
 } dg_params;
 
 /* Parity statistics (SAVE_STATS_CHAN, for/save_stats.f:112-203,470-489). */

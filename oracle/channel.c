@@ -41,6 +41,8 @@ static void *zalloc(long n, long sz) { return calloc((size_t)(n > 0 ? n : 1), (s
 
 /* ------------------------------------------------------------------ setup */
 orc *orc_create(const orc_params *p, const double *gy) {
+  /* LES_MODEL_TYPE 2 and 3 stop the MPI build (for/les.f:269-272) */
+  if (p->les && p->num_per_dir == 2 && p->les_model_type != 1) return NULL;
   orc *o = (orc *)calloc(1, sizeof(orc));
   o->p = *p;
   o->NX = p->nx;
@@ -150,6 +152,15 @@ orc *orc_create(const orc_params *p, const double *gy) {
     o->TH[n] = zalloc(np, sizeof(double));
     o->RTH[n] = zalloc(np, sizeof(double));
   }
+  if (p->les && !per) {
+    o->NU_T = zalloc(np, sizeof(double));
+    o->TEMP = zalloc(np, sizeof(double));
+    o->CTEMP = zalloc(ns, sizeof(cplx));
+    for (int c = 0; c < 6; c++) {
+      o->Sij[c] = zalloc(np, sizeof(double));
+      o->CSij[c] = zalloc(ns, sizeof(cplx));
+    }
+  }
   return o;
 }
 
@@ -166,6 +177,13 @@ void orc_destroy(orc *o) {
     free(o->CRTH[n]);
     free(o->TH[n]);
     free(o->RTH[n]);
+  }
+  free(o->NU_T);
+  free(o->TEMP);
+  free(o->CTEMP);
+  for (int c = 0; c < 6; c++) {
+    free(o->Sij[c]);
+    free(o->CSij[c]);
   }
   free(o);
 }
@@ -706,7 +724,8 @@ void orc_courant(orc *o) {
 }
 
 /* ------------------------------------------------------------ RK_CHAN_1 */
-/* for/channel.f:62-1073 (LES = .FALSE.; USER_RHS_CHAN_* are empty). */
+/* for/channel.f:62-1073 (USER_RHS_CHAN_* are empty); the LES parts are in
+ * les.c and in the eddy-viscosity terms of the implicit solves below. */
 void orc_rk_chan_1(orc *o, int time_step, int rk_step) {
   const orc_params *p = &o->p;
   const int NY = o->NY, NX = o->NX, NZ = o->NZ, nkxp = o->nkxp, nkzt = o->nkzt;
@@ -715,6 +734,8 @@ void orc_rk_chan_1(orc *o, int time_step, int rk_step) {
   const int r = rk_step - 1;
   const double NU = p->nu, NUV = p->nu_v_scale;
   const double TEMP1 = NU * o->h_bar[r] / 2.0;
+  const double TEMP2 = o->h_bar[r] / 2.0;
+  const double *NUT = o->NU_T;
   const double TEMP3 = o->zeta_bar[r] * o->h_bar[r];
   const double TEMP4 = o->h_bar[r];
   const double TEMP5 = o->beta_bar[r] * o->h_bar[r];
@@ -795,11 +816,19 @@ void orc_rk_chan_1(orc *o, int time_step, int rk_step) {
     }
   }
 
-  /* to physical space */
-  spec_to_phys(o, CU1, U1, 0, NY + 1);
-  spec_to_phys(o, CU2, U2, 0, NY + 1);
-  spec_to_phys(o, CU3, U3, 0, NY + 1);
-  for (int n = 0; n < o->NTH; n++) spec_to_phys(o, o->CTH[n], o->TH[n], 0, NY + 1);
+  /* the subgrid model waits 100 steps after a new flow (for/channel.f:303) */
+  if (p->les && (!p->create_new_flow || time_step > 100)) {
+    orc_les_chan(o);
+    orc_apply_bc_vel_phys(o);
+    for (int n = 0; n < o->NTH; n++) orc_les_scalar_terms(o, n);
+    for (int n = 0; n < o->NTH; n++) spec_to_phys(o, o->CTH[n], o->TH[n], 0, NY + 1);
+  } else {
+    /* to physical space */
+    spec_to_phys(o, CU1, U1, 0, NY + 1);
+    spec_to_phys(o, CU2, U2, 0, NY + 1);
+    spec_to_phys(o, CU3, U3, 0, NY + 1);
+    for (int n = 0; n < o->NTH; n++) spec_to_phys(o, o->CTH[n], o->TH[n], 0, NY + 1);
+  }
 
   /* nonlinear terms (for/channel.f:409-571) */
   LOOPP(JS, JE) { S1[P(j, k, i)] = U3[P(j, k, i)] * U1[P(j, k, i)]; }
@@ -879,6 +908,23 @@ void orc_rk_chan_1(orc *o, int time_step, int rk_step) {
                            (U2[P(j, k, i)] - U2[P(j - 1, k, i)]) / DYF[j - 1]) /
                           DY[j]);
   }
+  /* eddy viscosity, Crank-Nicolson like the molecular term (NU_T on GY
+   * points; interpolated to GYF for U2), for/channel.f:631-659 */
+  if (p->les) {
+    LOOPP(JS, JE) {
+      const long q = P(j, k, i), qp = P(j + 1, k, i), qm = P(j - 1, k, i);
+      R1[q] = R1[q] + TEMP2 * ((NUT[qp] * (U1[qp] - U1[q]) / DY[j + 1] -
+                                NUT[q] * (U1[q] - U1[qm]) / DY[j]) / DYF[j]);
+      R3[q] = R3[q] + TEMP2 * ((NUT[qp] * (U3[qp] - U3[q]) / DY[j + 1] -
+                                NUT[q] * (U3[q] - U3[qm]) / DY[j]) / DYF[j]);
+    }
+    LOOPP(2, NY) {
+      const long q = P(j, k, i), qp = P(j + 1, k, i), qm = P(j - 1, k, i);
+      R2[q] = R2[q] + TEMP2 * ((0.5 * (NUT[q] + NUT[qp]) * (U2[qp] - U2[q]) / DYF[j] -
+                                0.5 * (NUT[q] + NUT[qm]) * (U2[q] - U2[qm]) / DYF[j - 1]) /
+                               DY[j]);
+    }
+  }
 
   /* scalars: nonlinear terms, RHS, implicit solve (for/channel.f:665-836) */
   for (int n = 0; n < o->NTH; n++) {
@@ -908,6 +954,14 @@ void orc_rk_chan_1(orc *o, int time_step, int rk_step) {
                               (TH[P(j, k, i)] - TH[P(j - 1, k, i)]) / DY[j]) /
                              DYF[j]);
     }
+    if (p->les) {
+      /* KAPPA_T = NU_T (for/channel.f:314-322, 748-760) */
+      LOOPP(JSt, JEt) {
+        const long q = P(j, k, i), qp = P(j + 1, k, i), qm = P(j - 1, k, i);
+        RTH[q] = RTH[q] + TEMP2 * ((NUT[qp] * (TH[qp] - TH[q]) / DY[j + 1] -
+                                    NUT[q] * (TH[q] - TH[qm]) / DY[j]) / DYF[j]);
+      }
+    }
 #pragma omp parallel
     {
       const long nm = (long)NX * (NY + 2);
@@ -924,6 +978,12 @@ void orc_rk_chan_1(orc *o, int time_step, int rk_step) {
             m.D[c] = 1. + (a) / (DY[j + 1] * DYF[j]) + (a) / (DY[j] * DYF[j]);
             m.U[c] = -(a) / (DY[j + 1] * DYF[j]);
             m.V[c] = RTH[P(j, k, i)];
+            if (p->les) {
+              const double kj = NUT[P(j, k, i)], kp = NUT[P(j + 1, k, i)];
+              m.L[c] = m.L[c] - TEMP2 * kj / (DY[j] * DYF[j]);
+              m.D[c] = m.D[c] + TEMP2 * kp / (DY[j + 1] * DYF[j]) + TEMP2 * kj / (DY[j] * DYF[j]);
+              m.U[c] = m.U[c] - TEMP2 * kp / (DY[j + 1] * DYF[j]);
+            }
           }
         bc_gyf_lower(&m, p->th_bc_ymin[n], p->th_bc_ymin_c1[n], o);
         bc_gyf_upper(&m, p->th_bc_ymax[n], p->th_bc_ymax_c1[n], o);
@@ -956,6 +1016,13 @@ void orc_rk_chan_1(orc *o, int time_step, int rk_step) {
               m.D[c] = 1. + TEMP1 * NUV / (DYF[j] * DY[j]) + TEMP1 * NUV / (DYF[j - 1] * DY[j]);
               m.U[c] = -TEMP1 * NUV / (DYF[j] * DY[j]);
               m.V[c] = R2[P(j, k, i)];
+              if (p->les) {
+                const double nm = 0.5 * (NUT[P(j, k, i)] + NUT[P(j - 1, k, i)]);
+                const double npl = 0.5 * (NUT[P(j, k, i)] + NUT[P(j + 1, k, i)]);
+                m.L[c] = m.L[c] - TEMP2 * nm / (DYF[j - 1] * DY[j]);
+                m.D[c] = m.D[c] + TEMP2 * npl / (DYF[j] * DY[j]) + TEMP2 * nm / (DYF[j - 1] * DY[j]);
+                m.U[c] = m.U[c] - TEMP2 * npl / (DYF[j] * DY[j]);
+              }
             }
           bc_gy_lower(&m, p->v_bc_ymin, p->v_bc_ymin_c1, o);
           bc_gy_upper(&m, p->v_bc_ymax, p->v_bc_ymax_c1, o);
@@ -972,6 +1039,12 @@ void orc_rk_chan_1(orc *o, int time_step, int rk_step) {
               m.D[c] = 1. - TEMP1 * NUV * (-1. / (DY[j + 1] * DYF[j]) - 1. / (DY[j] * DYF[j]));
               m.U[c] = -TEMP1 * NUV / (DY[j + 1] * DYF[j]);
               m.V[c] = R[P(j, k, i)];
+              if (p->les) {
+                const double nj = NUT[P(j, k, i)], np1 = NUT[P(j + 1, k, i)];
+                m.L[c] = m.L[c] - TEMP2 * nj / (DY[j] * DYF[j]);
+                m.D[c] = m.D[c] + TEMP2 * np1 / (DY[j + 1] * DYF[j]) + TEMP2 * nj / (DY[j] * DYF[j]);
+                m.U[c] = m.U[c] - TEMP2 * np1 / (DY[j + 1] * DYF[j]);
+              }
             }
           if (comp == 1) {
             bc_gyf_lower(&m, p->u_bc_ymin, p->u_bc_ymin_c1, o);

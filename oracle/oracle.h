@@ -50,6 +50,9 @@ typedef struct orc_params {
   double drhodx[ORC_MAX_TH], drhodz[ORC_MAX_TH];
   int background_grad[ORC_MAX_TH];
   double epsilon_target;      /* periodic linear forcing (user_rhs.f:124) */
+  int les;                    /* USE_LES (input.dat, for/diablo_io.f:25) */
+  int les_model_type;         /* input_chan.dat (for/channel.f:1477); only 1 runs */
+  int create_new_flow;        /* input.dat (for/diablo_io.f:31): LES waits 100 steps */
 } orc_params;
 
 typedef struct orc orc;
@@ -137,6 +140,8 @@ void orc_save_stats_chan(orc *o, double *prof, double *prof_th, double *bulk);
 void orc_stats_means_update(const orc *o, int nsamples, double *ubar, double *vbar,
                             double *wbar, double *thbar);
 double orc_div_max_per(const orc *o);
+/* NU_T of the last LES substep, physical layout; -1 without LES */
+int orc_get_nu_t(const orc *o, double *out);
 
 #ifdef __cplusplus
 }

@@ -38,6 +38,7 @@ class OrcParams(ctypes.Structure):
         ("ri", c_d * MAX_TH), ("pr", c_d * MAX_TH), ("drhodx", c_d * MAX_TH),
         ("drhodz", c_d * MAX_TH), ("background_grad", c_i * MAX_TH),
         ("epsilon_target", c_d),
+        ("les", c_i), ("les_model_type", c_i), ("create_new_flow", c_i),
     ]
 
 
@@ -107,6 +108,7 @@ def lib():
         L.orc_save_stats_chan.argtypes = [P, P, P, P]
         L.orc_stats_means_update.argtypes = [P, c_i, P, P, P, P]
         L.orc_set_threads.argtypes = [c_i]
+        L.orc_get_nu_t.argtypes = [P, P]
         _lib = L
     return _lib
 
@@ -141,6 +143,8 @@ class Oracle:
             self._gy = np.ascontiguousarray(gy, dtype=np.float64)
             gyp = _ptr(self._gy)
         self.h = L.orc_create(ctypes.byref(self._op), gyp)
+        if not self.h:
+            raise ValueError("ERROR: LES_MODEL_TYPE=2, 3 not supported yet in MPI")
         self.spec_shape = p.spec_shape()
         self.phys_shape = p.phys_shape()
 
@@ -172,6 +176,13 @@ class Oracle:
         names += [f"CTH{n}" for n in range(self.p.n_th)]
         names += [f"CFTH{n}" for n in range(self.p.n_th)]
         return {n: self.get(n) for n in names}
+
+    def nu_t(self) -> np.ndarray:
+        """NU_T (physical, GY points) after the last LES substep."""
+        out = np.zeros(self.phys_shape)
+        if lib().orc_get_nu_t(self.h, _ptr(out)) != 0:
+            raise ValueError("no LES state")
+        return out
 
     def set_state(self, st: dict):
         for k, v in st.items():

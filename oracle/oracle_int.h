@@ -32,6 +32,9 @@ struct orc {
   /* physical fields */
   double *U1, *U2, *U3, *R1, *R2, *R3, *S1, *F1, *F2, *F3;
   double *TH[ORC_MAX_TH], *RTH[ORC_MAX_TH];
+  /* LES (allocated when p.les): NU_T at GY points, S_ij / CS_ij, TEMP / CTEMP */
+  double *NU_T, *Sij[6], *TEMP;
+  cplx *CSij[6], *CTEMP;
 };
 
 void orc_r2c_pair(int n, const double *a, const double *b, cplx *A, cplx *B, cplx *work);
@@ -39,5 +42,8 @@ void orc_c2r_pair(int n, const cplx *A, const cplx *B, double *a, double *b, cpl
 void orc_plane_to_fourier(const orc *o, const double *phys, cplx *spec, cplx *wk);
 void orc_plane_to_physical(const orc *o, const cplx *spec, double *phys, cplx *wk);
 long orc_plane_work_size(const orc *o);
+void orc_les_chan(orc *o);
+void orc_les_scalar_terms(orc *o, int n);
+void orc_apply_bc_vel_phys(orc *o);
 
 #endif

@@ -25,7 +25,9 @@ def test_input_dat_and_input_chan():
     assert p.nu_v_scale == 1.0 and p.num_per_dir == 2
     assert p.delta_t == 0.1 and p.variable_dt == 1 and p.cfl == 0.5 and p.update_dt == 1
     assert p.ri[0] == 0.15 and p.pr[0] == 1.0
+    assert p.les == 1 and p.create_new_flow == 1   # USE_LES, CREATE_NEW_FLOW
     p = params.read_input_chan(os.path.join(KH, "input_chan.dat"), p)
+    assert p.les_model_type == 1
     assert (p.i_ro, p.grav_x, p.grav_y, p.grav_z) == (0.0, 0.0, 1.0, 0.0)
     assert (p.f_type, p.ubulk0, p.px0, p.omega0, p.amp_omega0) == (3, 0.0, -1.0, 6.28, 0.0)
     assert (p.u_bc_ymin, p.v_bc_ymin, p.w_bc_ymin) == (1, 0, 1)

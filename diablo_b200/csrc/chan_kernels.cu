@@ -1868,6 +1868,20 @@ int dg_courant_dev(dg_handle *h, const double2 *const *u, bool side) {
   return DG_OK;
 }
 
+// COURANT on physical U1..U3 that already exist (planes 1..NY at u_plane1,
+// u_plane1 + pfield, u_plane1 + 2 pfield; the LES path's post-solve velocity)
+int dg_courant_phys(dg_handle *h, const double *u_plane1, long pfield) {
+  DG_CUDA(cudaMemsetAsync(h->dmin_bits, 0x7f, sizeof(unsigned long long), h->st));
+  dg_kt_begin(h, "k_cfl_min", h->st);
+  k_cfl_min<<<4 * 148, 256, 0, h->st>>>(u_plane1, pfield, h->NY, h->NZ, h->NX, h->p.cfl,
+                                         h->p.lx / h->NX, h->p.lz / h->NZ, h->dy, h->dmin_bits);
+  DG_LAUNCHED();
+  dg_kt_begin(h, "k_dt_update", h->st);
+  k_dt_update<<<1, 1, 0, h->st>>>(h->dscal, h->dmin_bits, courant_dt0(h));
+  DG_LAUNCHED();
+  return DG_OK;
+}
+
 int dg_dt_commit(dg_handle *h) {
   dg_kt_begin(h, "k_dt_commit", h->st);
   k_dt_commit<<<1, 1, 0, h->st>>>(h->dscal);
@@ -2063,6 +2077,11 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
   for (int f = 0; f < h->nf; f++) { cu.p[f] = h->cu[f]; cf.p[f] = h->cf[f]; rhs.p[f] = h->rhs[f]; }
   int hdone = -1;  // last H plane already produced
   int a0 = 1;
+  // LES: the subgrid model wraps the nonlinear stage; once NU_T exists the
+  // Crank-Nicolson solves run on physical columns (for/channel.f:303,631)
+  const bool sgs = dg_les_active(h, time_step);
+  const bool les_solve = h->p.les && (sgs || h->les_nut);
+  if (sgs) DG_TRY(dg_les_pre(h, rk_step));
   if (h->mixed && !(xw_supported(h->NX) && h->NTH <= 2)) {
     DG_TRY(nl_generic_mixed(h, C, rk_step, in, cu, cf, rhs));
     a0 = h->NY + 1;  // every plane done: no chunk loop
@@ -2171,6 +2190,7 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
     }
     if (!done) break;  // the generic kernels covered every plane
   }
+  if (les_solve) return dg_les_post(h, time_step, rk_step, sgs);
   // 4. per-mode CN solves, then COURANT on the post-CN velocity
   //    (for/channel.f:1037-1040), then REM_DIV_CHAN and CP += phi / H_BAR
   DG_TRY(dg_cn_solve_dev(h, rk_step));

@@ -159,6 +159,14 @@ struct dg_handle {
   int cn_mt;                    // modes per CTA of the CN column kernel (4, 8, 16)
   int xrow_chunk;               // planes per CTA of the x-row product kernel (0 = auto)
   int ychunk;                   // planes per y-chunk of a substep (0 = all)
+
+  // LES (dg_params.les): physical slots [nslots][NY+2][NZ][NX], spectral slots
+  // [nslots][NY+2][ss], filter-width factors [2][NY+2] (DYF, DY), mean U1/U3
+  double *les_phys;
+  double2 *les_spec;
+  double *les_dfac;
+  double *les_ubar;
+  bool les_nut;                 // NU_T has been computed (it stays in use from then on)
 };
 
 int dg_default_col_mt(const dg_handle *h);
@@ -214,6 +222,11 @@ int dg_stats_dev(dg_handle *h, dg_stats *s);
 int dg_per_stats(dg_handle *h, dg_stats *s);
 int dg_cn_tables(dg_handle *h);
 int dg_dt_commit(dg_handle *h);
+int dg_courant_phys(dg_handle *h, const double *u_plane1, long pfield);
+int dg_les_init(dg_handle *h);
+bool dg_les_active(const dg_handle *h, int time_step);
+int dg_les_pre(dg_handle *h, int rk_step);
+int dg_les_post(dg_handle *h, int time_step, int rk_step, bool sgs);
 
 #define DG_CASE_N(N) \
   case N:            \

@@ -1,0 +1,680 @@
+// Channel LES: constant Smagorinsky subgrid model (LES_MODEL_TYPE = 1, the
+// only model the MPI build runs) inside RK_CHAN_1.
+//
+// The reference (for/les.f:1-275, for/channel.f:299-372,631-659,748-1029)
+// computes S_ij in physical space, the eddy viscosity NU_T = C_S^2 DELTA^2 |S|
+// at GY points, the SGS stress divergence (explicit, into CF), and moves the
+// Crank-Nicolson solves to physical columns because NU_T varies in x and z.
+// Here the substep keeps its fused spectral stages for everything the DNS
+// does, and wraps them:
+//   pre  : APPLY_BC_VEL + APPLY_BC_LES on CU, strain rates (spectral) -> S_ij
+//          and U (physical), APPLY_BC_VEL_PHYS, one column pass for |S|, NU_T,
+//          |S| S_ij and the NU_T dU/dy cross terms, forward transforms, the SGS
+//          forcing G per field, the scalar eddy diffusion; the boundary planes
+//          of CU are refreshed from the physical velocity so the nonlinear
+//          stage sees what the reference's physical U holds;
+//   (the fused z inverse / x-row products / z forward write CF and the
+//    spectral right-hand side R as in the DNS)
+//   post : CF += G, R += BETA_BAR H_BAR G; R, TH to physical; one thread per
+//          physical column builds the CN rows with the eddy-viscosity terms and
+//          the BC rows, runs the MPI Thomas sweeps and writes U / TH; COURANT on
+//          that velocity; forward transforms to CU / CTH; REM_DIV_CHAN.
+// Slots (physical): 0-5 S_ij (then R), 6-7 cross terms, 8-10 U1-U3, 11 NU_T,
+// 12.. TH(n), then 2 nf Thomas scratch (pivots b', upper diagonals c).
+// Slots (spectral): 0-5 CS_ij (then the products, then scalar temporaries),
+// 6-7 cross terms, 8.. G(f).
+#include "dg_internal.cuh"
+
+namespace {
+
+constexpr int PS_S = 0, PS_X = 6, PS_U = 8, PS_NUT = 11, PS_TH = 12;
+constexpr int SS_S = 0, SS_X = 6, SS_G = 8;
+
+inline int phys_slots(const dg_handle *h) { return PS_TH + h->NTH + 2 * h->nf; }
+inline int spec_slots(const dg_handle *h) { return SS_G + h->nf; }
+inline long pfield_of(const dg_handle *h) { return (long)(h->NY + 2) * h->NZ * h->NX; }
+inline double *pslot(dg_handle *h, int s) { return h->les_phys + (long)s * pfield_of(h); }
+inline double2 *sslot(dg_handle *h, int s) { return h->les_spec + (long)s * h->nspec; }
+
+struct LesBc {
+  int u_lo, w_lo, v_lo, u_hi, w_hi, v_hi;
+  double u_lo_c1, w_lo_c1, v_lo_c1, u_hi_c1, w_hi_c1, v_hi_c1;
+};
+
+LesBc make_bc(const dg_params &p) {
+  return {p.u_bc_ymin, p.w_bc_ymin, p.v_bc_ymin, p.u_bc_ymax, p.w_bc_ymax, p.v_bc_ymax,
+          p.u_bc_ymin_c1, p.w_bc_ymin_c1, p.v_bc_ymin_c1, p.u_bc_ymax_c1, p.w_bc_ymax_c1,
+          p.v_bc_ymax_c1};
+}
+
+// APPLY_BC_LES (for/les.f:805-865): Neumann walls copy the first interior
+// plane of CU1 / CU3 into the wall and ghost planes.
+__global__ void k_les_bc_spec(LesBc B, int NY, long ss, double2 *u1, double2 *u3) {
+  const long m = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= ss) return;
+  if (B.u_hi == 1) {
+    u1[NY * ss + m] = u1[(NY - 1) * ss + m];
+    u1[(NY + 1) * ss + m] = u1[NY * ss + m];
+  }
+  if (B.w_hi == 1) {
+    u3[NY * ss + m] = u3[(NY - 1) * ss + m];
+    u3[(NY + 1) * ss + m] = u3[NY * ss + m];
+  }
+  if (B.u_lo == 1) {
+    u1[ss + m] = u1[2 * ss + m];
+    u1[m] = u1[ss + m];
+  }
+  if (B.w_lo == 1) {
+    u3[ss + m] = u3[2 * ss + m];
+    u3[m] = u3[ss + m];
+  }
+}
+
+__device__ __forceinline__ double2 cmul_i(double k, double2 a) {  // (i k) a
+  return make_double2(-k * a.y, k * a.x);
+}
+
+// compute_strain_chan (for/les.f:526-569) into six spectral slots, zero on
+// the planes it does not write; the mean U1, U3 per plane for les_chan.
+__global__ void k_les_strain(int NY, long ss, int nkxp, const double *__restrict__ kxv,
+                             const double *__restrict__ kzv, const double *__restrict__ dy,
+                             const double *__restrict__ dyf, const double2 *__restrict__ u1,
+                             const double2 *__restrict__ u2, const double2 *__restrict__ u3,
+                             double2 *__restrict__ cs, long nspec, double *__restrict__ ubar) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long)(NY + 2) * ss) return;
+  const int j = (int)(q / ss);
+  const long m = q % ss;
+  const double KX = kxv[m % nkxp], KZ = kzv[m / nkxp];
+  const double2 z = make_double2(0.0, 0.0);
+  double2 s0 = z, s1 = z, s2 = z, s3 = z, s4 = z, s5 = z;
+  if (j >= 1 && j <= NY) {
+    const double2 a1 = u1[q], a3 = u3[q], b2 = u2[q], b2p = u2[q + ss];
+    s0 = cmul_i(KX, a1);
+    s1 = make_double2((b2p.x - b2.x) / dyf[j], (b2p.y - b2.y) / dyf[j]);
+    s2 = cmul_i(KZ, a3);
+    const double2 t1 = cmul_i(KZ, a1), t3 = cmul_i(KX, a3);
+    s4 = make_double2(0.5 * (t1.x + t3.x), 0.5 * (t1.y + t3.y));
+  }
+  if (j >= 1) {
+    const double2 a1 = u1[q], a1m = u1[q - ss], a3 = u3[q], a3m = u3[q - ss], b2 = u2[q];
+    const double2 k2 = cmul_i(KX, b2), k2z = cmul_i(KZ, b2);
+    s3 = make_double2(0.5 * ((a1.x - a1m.x) / dy[j] + k2.x), 0.5 * ((a1.y - a1m.y) / dy[j] + k2.y));
+    s5 = make_double2(0.5 * (k2z.x + (a3.x - a3m.x) / dy[j]), 0.5 * (k2z.y + (a3.y - a3m.y) / dy[j]));
+  }
+  cs[q] = s0;
+  cs[nspec + q] = s1;
+  cs[2 * nspec + q] = s2;
+  cs[3 * nspec + q] = s3;
+  cs[4 * nspec + q] = s4;
+  cs[5 * nspec + q] = s5;
+  if (m == 0) {
+    ubar[j] = u1[q].x;
+    ubar[NY + 2 + j] = u3[q].x;
+  }
+}
+
+// APPLY_BC_VEL_PHYS_LOWER / _UPPER (for/channel.f:2495-2652) on the physical
+// U1..U3 (slots at stride pfield).
+__global__ void k_les_bc_phys(LesBc B, int NY, long np, long pfield, const double *__restrict__ dy,
+                              const double *__restrict__ dyf, double *__restrict__ U) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= np) return;
+  double *U1 = U, *U2 = U + pfield, *U3 = U + 2 * pfield;
+  const long j0 = q, j1 = np + q, j2 = 2 * np + q;
+  const long jm = (long)(NY - 1) * np + q, jn = (long)NY * np + q, jn1 = (long)(NY + 1) * np + q;
+  if (B.u_lo == 0) {
+    U1[j0] = B.u_lo_c1;
+    U1[j1] = B.u_lo_c1;
+  } else {
+    U1[j1] = U1[j2] - dy[2] * B.u_lo_c1;
+    U1[j0] = U1[j1] - dy[1] * B.u_lo_c1;
+  }
+  if (B.w_lo == 0) {
+    U3[j0] = B.w_lo_c1;
+    U3[j1] = B.w_lo_c1;
+  } else {
+    U3[j1] = U3[j2] - dy[2] * B.w_lo_c1;
+    U3[j0] = U3[j1] - dy[1] * B.w_lo_c1;
+  }
+  if (B.v_lo == 0) {
+    U2[j1] = 2.0 * B.v_lo_c1 - U2[j2];
+    U2[j0] = U2[j1];
+  } else {
+    U2[j1] = U2[j2] - dyf[1] * B.v_lo_c1;
+    U2[j0] = U2[j1] - dyf[1] * B.v_lo_c1;
+  }
+  if (B.u_hi == 0) {
+    U1[jn] = B.u_hi_c1;
+    U1[jn1] = B.u_hi_c1;
+  } else {
+    U1[jn] = U1[jm] + dy[NY] * B.u_hi_c1;
+    U1[jn1] = U1[jn] + dy[NY] * B.u_hi_c1;
+  }
+  if (B.w_hi == 0) {
+    U3[jn] = B.w_hi_c1;
+    U3[jn1] = B.w_hi_c1;
+  } else {
+    U3[jn] = U3[jm] + dy[NY] * B.w_hi_c1;
+    U3[jn1] = U3[jn] + dy[NY] * B.w_hi_c1;
+  }
+  if (B.v_hi == 0)
+    U2[jn1] = 2.0 * B.v_hi_c1 - U2[jn];
+  else
+    U2[jn1] = U2[jn] + dy[NY] * B.v_hi_c1;
+}
+
+// The model, one thread per physical column (i, k), marching j upwards with
+// the raw S_ij of planes j-1, j, j+1 in registers (for/les.f:114-227):
+// |S| at GYF for JSTART..JEND, |S| at GY for 2..NY+1, |S| S_ij in place,
+// NU_T at GY (zero on planes 1, 2, NY, NY+1: GHOST_LES_MPI for one rank) and
+// the cross terms NU_T dU1/dy, NU_T dU3/dy on planes 2..NY.
+__global__ void k_les_model(int NY, long np, long pfield, int JS, int JE,
+                            const double *__restrict__ dy, const double *__restrict__ dyf,
+                            const double *__restrict__ dfac, const double *__restrict__ ubar,
+                            double *__restrict__ S, double *__restrict__ X,
+                            const double *__restrict__ U, double *__restrict__ NUT) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= np) return;
+  const double *u1b = ubar, *u3b = ubar + NY + 2;
+  const double *U1 = U, *U3 = U + 2 * pfield;
+  double *X1 = X, *X3 = X + pfield;
+  double p0 = S[q], p1 = S[pfield + q], p2 = S[2 * pfield + q], p4 = S[4 * pfield + q];
+  for (int j = 1; j <= NY + 1; j++) {
+    const long o = (long)j * np + q;
+    const double r0 = S[o], r1 = S[pfield + o], r2 = S[2 * pfield + o], r3 = S[3 * pfield + o];
+    const double r4 = S[4 * pfield + o], r5 = S[5 * pfield + o];
+    double tg = 0.0;  // |S| at GY
+    if (j >= 2) {
+      const double w = 2.0 * dy[j];
+      const double b1 = (r0 * dyf[j - 1] + p0 * dyf[j]) / w;
+      const double b4 = r3 - 0.5 * (u1b[j] - u1b[j - 1]) / dy[j];
+      const double b5 = (r4 * dyf[j - 1] + p4 * dyf[j]) / w;
+      const double b2 = (r1 * dyf[j - 1] + p1 * dyf[j]) / w;
+      const double b6 = r5 - 0.5 * (u3b[j] - u3b[j - 1]) / dy[j];
+      const double b3 = (r2 * dyf[j - 1] + p2 * dyf[j]) / w;
+      tg = sqrt(2.0 * (b1 * b1) + 4.0 * (b4 * b4) + 4.0 * (b5 * b5) + 2.0 * (b2 * b2) +
+                4.0 * (b6 * b6) + 2.0 * (b3 * b3));
+    }
+    if (j >= JS && j <= JE) {
+      const double n3 = S[3 * pfield + o + np], n5 = S[5 * pfield + o + np];
+      const double a4 = 0.5 * (n3 + r3 - 0.5 * (u1b[j] - u1b[j - 1]) / dy[j] -
+                               0.5 * (u1b[j + 1] - u1b[j]) / dy[j + 1]);
+      const double a6 = 0.5 * (n5 + r5 - 0.5 * (u3b[j] - u3b[j - 1]) / dy[j] -
+                               0.5 * (u3b[j + 1] - u3b[j]) / dy[j + 1]);
+      const double sf = sqrt(2.0 * (r0 * r0) + 4.0 * (a4 * a4) + 4.0 * (r4 * r4) +
+                             2.0 * (r1 * r1) + 4.0 * (a6 * a6) + 2.0 * (r2 * r2));
+      S[o] = sf * r0;
+      S[4 * pfield + o] = sf * r4;
+      S[pfield + o] = 0.0;
+      S[2 * pfield + o] = sf * r2;
+    }
+    double nut = 0.0;
+    if (j >= 2) {
+      const double du1 = 0.5 * (U1[o] - U1[o - np]) / dy[j];
+      const double du3 = 0.5 * (U3[o] - U3[o - np]) / dy[j];
+      S[3 * pfield + o] = tg * (r3 - du1);
+      S[5 * pfield + o] = tg * (r5 - du3);
+      if (j >= 3 && j <= NY - 1) nut = -0.5 * dfac[NY + 2 + j] * tg;
+    }
+    NUT[o] = nut;
+    if (j >= 2 && j <= NY) {
+      X1[o] = nut * (U1[o] - U1[o - np]) / dy[j];
+      X3[o] = nut * (U3[o] - U3[o - np]) / dy[j];
+    }
+    p0 = r0;
+    p1 = r1;
+    p2 = r2;
+    p4 = r4;
+  }
+}
+
+// SGS stress divergence per field (for/les.f:236-333) from the transformed
+// |S| S_ij (slots 0, 2-5) and cross terms (slots 6-7), with the filter-width
+// factors applied as the reference scales CS_ij.  G1, G3 on J1..J2 = JSTART..
+// NY-1, G2 on 2..NY, zero elsewhere.
+__global__ void k_les_force(int NY, long ss, int nkxp, int JS, const double *__restrict__ kxv,
+                            const double *__restrict__ kzv, const double *__restrict__ dyf,
+                            const double *__restrict__ dfac, const double2 *__restrict__ cs,
+                            long nspec, double2 *__restrict__ g) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long)(NY + 2) * ss) return;
+  const int j = (int)(q / ss);
+  const long m = q % ss;
+  const double KX = kxv[m % nkxp], KZ = kzv[m / nkxp];
+  const double *ff = dfac, *fy = dfac + NY + 2;
+  const double2 *C0 = cs, *C2 = cs + 2 * nspec, *C3 = cs + 3 * nspec, *C4 = cs + 4 * nspec;
+  const double2 *C5 = cs + 5 * nspec, *X1 = cs + 6 * nspec, *X3 = cs + 7 * nspec;
+  auto sc = [](double f, double2 a) { return make_double2(f * a.x, f * a.y); };
+  double2 g1 = make_double2(0.0, 0.0), g2 = g1, g3 = g1;
+  if (j >= JS && j <= NY - 1) {
+    const double2 t1 = sc(ff[j], C0[q]), t5 = sc(ff[j], C4[q]), t3 = sc(ff[j], C2[q]);
+    const double2 t4 = sc(fy[j], C3[q]), t4p = sc(fy[j + 1], C3[q + ss]);
+    const double2 t6 = sc(fy[j], C5[q]), t6p = sc(fy[j + 1], C5[q + ss]);
+    const double2 a = cmul_i(KX, t1), b = cmul_i(KZ, t5);
+    g1.x = -a.x - (t4p.x - t4.x) / dyf[j] - b.x;
+    g1.y = -a.y - (t4p.y - t4.y) / dyf[j] - b.y;
+    const double2 c = cmul_i(KX, t5), d = cmul_i(KZ, t3);
+    g3.x = -c.x - (t6p.x - t6.x) / dyf[j] - d.x;
+    g3.y = -c.y - (t6p.y - t6.y) / dyf[j] - d.y;
+  }
+  if (j >= 2 && j <= NY) {
+    const double2 a = cmul_i(KX, sc(fy[j], C3[q])), b = cmul_i(KZ, sc(fy[j], C5[q]));
+    const double2 c = cmul_i(KX, X1[q]), d = cmul_i(KZ, X3[q]);
+    g2.x = -a.x - b.x + c.x + d.x;
+    g2.y = -a.y - b.y + c.y + d.y;
+  }
+  g[q] = g1;
+  g[nspec + q] = g2;
+  g[2 * nspec + q] = g3;
+}
+
+// i kx CTH and i kz CTH on planes 1..NY+1 (for/channel.f:326-355)
+__global__ void k_les_th_grad(int NY, long ss, int nkxp, const double *__restrict__ kxv,
+                              const double *__restrict__ kzv, const double2 *__restrict__ th,
+                              double2 *__restrict__ out, long nspec) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long)(NY + 2) * ss) return;
+  const int j = (int)(q / ss);
+  const long m = q % ss;
+  double2 a = make_double2(0.0, 0.0), b = a;
+  if (j >= 1) {
+    a = cmul_i(kxv[m % nkxp], th[q]);
+    b = cmul_i(kzv[m / nkxp], th[q]);
+  }
+  out[q] = a;
+  out[nspec + q] = b;
+}
+
+// KAPPA_T = NU_T times both physical gradients on planes 1..NY+1
+__global__ void k_les_th_scale(int NY, long np, long pfield, const double *__restrict__ nut,
+                               double *__restrict__ a) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long)NY * np + np) return;
+  const long o = np + q;  // planes 1..NY+1
+  a[o] = nut[o] * a[o];
+  a[pfield + o] = nut[o] * a[pfield + o];
+}
+
+// G(TH) = i kx F(K_T dTH/dx) + i kz F(K_T dTH/dz) on JSTART_TH..JEND_TH
+__global__ void k_les_th_force(int NY, long ss, int nkxp, int jlo, int jhi,
+                               const double *__restrict__ kxv, const double *__restrict__ kzv,
+                               const double2 *__restrict__ c, long nspec, double2 *__restrict__ g) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long)(NY + 2) * ss) return;
+  const int j = (int)(q / ss);
+  const long m = q % ss;
+  double2 r = make_double2(0.0, 0.0);
+  if (j >= jlo && j <= jhi) {
+    const double2 a = cmul_i(kxv[m % nkxp], c[q]), b = cmul_i(kzv[m / nkxp], c[nspec + q]);
+    r = make_double2(a.x + b.x, a.y + b.y);
+  }
+  g[q] = r;
+}
+
+// CF += G, R += BETA_BAR H_BAR G for every field (G is zero outside its rows)
+__global__ void k_les_add(int nf, long nspec, const double *__restrict__ dscal, int rk_step,
+                          const double2 *__restrict__ g, FieldPtrs cf, FieldPtrs rhs) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int f = blockIdx.y;
+  if (q >= nspec || f >= nf) return;
+  const double h = dscal[1 + rk_step];
+  const double bbar = (rk_step == 2) ? 25.0 / 8.0 : (rk_step == 3) ? 9.0 / 4.0 : 1.0;
+  const double T5 = bbar * h;
+  const double2 a = g[(long)f * nspec + q];
+  double2 *c = cf(f) + q, *r = rhs(f) + q;
+  const double2 cv = *c, rv = *r;
+  *c = make_double2(cv.x + a.x, cv.y + a.y);
+  *r = make_double2(rv.x + T5 * a.x, rv.y + T5 * a.y);
+}
+
+// ------------------------------------------------ physical-column CN solve
+struct LesCn {
+  int NY, nf, JS, JE, jst[DG_MAX_TH], jet[DG_MAX_TH];
+  int bc_lo[3 + DG_MAX_TH], bc_hi[3 + DG_MAX_TH];
+  double c1_lo[3 + DG_MAX_TH], c1_hi[3 + DG_MAX_TH];
+  double nu, nuv, pr[DG_MAX_TH];
+};
+
+// Row j of field f (0 U1, 1 U2, 2 U3, 3+n TH(n)) as the reference builds it:
+// identity, then CN rows with the eddy-viscosity terms over the update range,
+// then the lower and upper BC rows (APPLY_BC_*_MPI, for/mpi.f:1137-1291 with
+// for/channel.f:1660-2241).  The right-hand side of a CN row is R plus the
+// explicit eddy-viscosity half.
+__device__ __forceinline__ void les_row(const LesCn &P, int f, int j, double T1, double T2,
+                                        const double *dy, const double *dyf, const double *nut,
+                                        const double *R, const double *U, long np, double &l,
+                                        double &d, double &u, double &v) {
+  const int NY = P.NY;
+  l = 0.0, d = 1.0, u = 0.0, v = 0.0;
+  const long o = (long)j * np;
+  if (f == 1) {
+    if (j >= 2 && j <= NY) {
+      const double a = T1 * P.nuv;
+      l = -a / (dyf[j - 1] * dy[j]);
+      d = 1. + a / (dyf[j] * dy[j]) + a / (dyf[j - 1] * dy[j]);
+      u = -a / (dyf[j] * dy[j]);
+      const double nm = 0.5 * (nut[o] + nut[o - np]), npl = 0.5 * (nut[o] + nut[o + np]);
+      v = R[o] + T2 * ((npl * (U[o + np] - U[o]) / dyf[j] - nm * (U[o] - U[o - np]) / dyf[j - 1]) /
+                       dy[j]);
+      l = l - T2 * nm / (dyf[j - 1] * dy[j]);
+      d = d + T2 * npl / (dyf[j] * dy[j]) + T2 * nm / (dyf[j - 1] * dy[j]);
+      u = u - T2 * npl / (dyf[j] * dy[j]);
+    }
+    // APPLY_BC_2_LOWER / _UPPER
+    const int lo = P.bc_lo[1], hi = P.bc_hi[1];
+    if (j == 0) { l = 0.; d = 1.; u = 0.; v = 0.; }
+    if (lo == 0 && (j == 1 || j == 2)) { l = 0.; d = 1.; u = 0.; v = P.c1_lo[1]; }
+    if (lo == 1 && j == 1) { l = 0.; d = -1.; u = 1.; v = dyf[1] * P.c1_lo[1]; }
+    if (hi == 0 && (j == NY || j == NY + 1)) { l = 0.; d = 1.; u = 0.; v = P.c1_hi[1]; }
+    if (hi == 1 && j == NY + 1) { l = -1.; d = 1.; u = 0.; v = dyf[NY] * P.c1_hi[1]; }
+    return;
+  }
+  const bool th = f >= 3;
+  const int js = th ? P.jst[f - 3] : P.JS, je = th ? P.jet[f - 3] : P.JE;
+  if (j >= js && j <= je) {
+    const double nj = nut[o], np1 = nut[o + np];
+    if (th) {
+      const double a = T1 / P.pr[f - 3] * P.nuv;
+      l = -(a) / (dy[j] * dyf[j]);
+      d = 1. + (a) / (dy[j + 1] * dyf[j]) + (a) / (dy[j] * dyf[j]);
+      u = -(a) / (dy[j + 1] * dyf[j]);
+    } else {
+      l = -T1 * P.nuv / (dy[j] * dyf[j]);
+      d = 1. - T1 * P.nuv * (-1. / (dy[j + 1] * dyf[j]) - 1. / (dy[j] * dyf[j]));
+      u = -T1 * P.nuv / (dy[j + 1] * dyf[j]);
+    }
+    v = R[o] + T2 * ((np1 * (U[o + np] - U[o]) / dy[j + 1] - nj * (U[o] - U[o - np]) / dy[j]) /
+                     dyf[j]);
+    l = l - T2 * nj / (dy[j] * dyf[j]);
+    d = d + T2 * np1 / (dy[j + 1] * dyf[j]) + T2 * nj / (dy[j] * dyf[j]);
+    u = u - T2 * np1 / (dy[j + 1] * dyf[j]);
+  }
+  // APPLY_BC_1/3/TH_LOWER / _UPPER
+  const int lo = P.bc_lo[f], hi = P.bc_hi[f];
+  if (j == 0) { l = 0.; d = 1.; u = 0.; v = 0.; }
+  if (j == 1) {
+    if (lo == 0) { l = 0.; d = 1.; u = 0.; v = P.c1_lo[f]; }
+    else { l = 0.; d = -1.; u = 1.; v = dy[2] * P.c1_lo[f]; }
+  }
+  if (j == NY + 1) { l = 0.; d = 1.; u = 0.; v = 0.; }
+  if (j == NY) {
+    if (hi == 0) { l = 0.; d = 1.; u = 0.; v = P.c1_hi[f]; }
+    else { l = -1.; d = 1.; u = 0.; v = dy[NY] * P.c1_hi[f]; }
+  }
+}
+
+// One thread per physical column of one field: rows, THOMAS_FORWARD_REAL_MPI
+// and THOMAS_BACKWARD_REAL_MPI for the only rank (for/mpi.f:630-703,767-809),
+// the solution written back over the reference's ranges.  R (slot f) holds
+// the right-hand side and then the eliminated one; B (scratch) the pivots, C
+// the upper diagonals.
+__global__ void k_les_cn(LesCn P, long np, long pfield, const double *__restrict__ dscal,
+                         int rk_step, const double *__restrict__ dy, const double *__restrict__ dyf,
+                         const double *__restrict__ nut, double *__restrict__ Rbase,
+                         double *__restrict__ Ubase, double *__restrict__ THbase,
+                         double *__restrict__ Bbase) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int f = blockIdx.y;
+  if (q >= np || f >= P.nf) return;
+  const double h = dscal[1 + rk_step];
+  const double T1 = P.nu * h / 2.0, T2 = h / 2.0;
+  const int NY = P.NY;
+  double *R = Rbase + (long)f * pfield + q;
+  double *U = (f < 3 ? Ubase + (long)f * pfield : THbase + (long)(f - 3) * pfield) + q;
+  double *B = Bbase + (long)f * pfield + q, *C = Bbase + (long)(P.nf + f) * pfield + q;
+  const double *nq = nut + q;
+  double l, d, u, v;
+  les_row(P, f, 0, T1, T2, dy, dyf, nq, R, U, np, l, d, u, v);
+  double bprev = d, cprev = u, gprev = v;
+  B[0] = d;
+  C[0] = u;
+  R[0] = v;
+  for (int j = 1; j <= NY + 1; j++) {
+    les_row(P, f, j, T1, T2, dy, dyf, nq, R, U, np, l, d, u, v);
+    const double a = -l / bprev;
+    const double b = d + a * cprev;
+    const double g = v + a * gprev;
+    const long o = (long)j * np;
+    B[o] = b;
+    C[o] = u;
+    R[o] = g;
+    bprev = b;
+    cprev = u;
+    gprev = g;
+  }
+  // back substitution; rows written back: U1/U3 JSTART-1..JEND+1, U2
+  // 1..NY+1, TH(n) JSTART_TH-1..JEND_TH+1
+  int wlo, whi;
+  if (f == 1) { wlo = 1; whi = NY + 1; }
+  else if (f >= 3) { wlo = P.jst[f - 3] - 1; whi = P.jet[f - 3] + 1; }
+  else { wlo = P.JS - 1; whi = P.JE + 1; }
+  double x = gprev / bprev;
+  if (NY + 1 >= wlo && NY + 1 <= whi) U[(long)(NY + 1) * np] = x;
+  for (int j = NY; j >= 0; j--) {
+    const long o = (long)j * np;
+    const double bj = B[o];
+    x = (bj != 0.0) ? (R[o] - C[o] * x) / bj : 0.0;
+    if (j >= wlo && j <= whi) U[o] = x;
+  }
+}
+
+int to_physical(dg_handle *h, const double2 *const *in, int n, int jmin, int jmax, double *out) {
+  const long pplane = (long)h->NZ * h->NX, pf = pfield_of(h);
+  for (int b = 0; b < n; b += h->nf) {
+    const int k = (n - b < h->nf) ? n - b : h->nf;
+    DG_TRY(dg_zinv(h, in + b, k, jmin, jmax, h->H, 0));
+    DG_TRY(dg_xc2r_planes(h, h->H, k, jmin, jmax, out + (long)b * pf, pplane, h->NX, pf));
+  }
+  return DG_OK;
+}
+
+int to_fourier(dg_handle *h, const double *in, int n, int jmin, int jmax, double2 *const *out) {
+  const long pplane = (long)h->NZ * h->NX, pf = pfield_of(h);
+  for (int b = 0; b < n; b += h->nf) {
+    const int k = (n - b < h->nf) ? n - b : h->nf;
+    DG_TRY(dg_xr2c_planes(h, in + (long)b * pf, k, jmin, jmax, pplane, h->NX, pf, h->H));
+    DG_TRY(dg_zfwd_planes(h, h->H, k, jmin, jmax, out + b, nullptr, 0));
+  }
+  return DG_OK;
+}
+
+}  // namespace
+
+int dg_les_init(dg_handle *h) {
+  const int NY = h->NY;
+  const size_t pf = (size_t)pfield_of(h), ns = (size_t)h->nspec;
+  DG_CUDA(dg_malloc(h, (void **)&h->les_phys, sizeof(double) * pf * phys_slots(h)));
+  DG_CUDA(dg_malloc(h, (void **)&h->les_spec, sizeof(double2) * ns * spec_slots(h)));
+  DG_CUDA(dg_malloc(h, (void **)&h->les_dfac, sizeof(double) * 2 * (NY + 2)));
+  DG_CUDA(dg_malloc(h, (void **)&h->les_ubar, sizeof(double) * 2 * (NY + 2)));
+  DG_CUDA(cudaMemsetAsync(h->les_phys, 0, sizeof(double) * pf * phys_slots(h), h->st));
+  DG_CUDA(cudaMemsetAsync(h->les_spec, 0, sizeof(double2) * ns * spec_slots(h), h->st));
+  // -2 C_S^2 (DX BETA DY 2 DZ BETA)^(2/3), C_S = 0.13, BETA = 1 (for/les.f:194-217),
+  // on GYF (DYF) and GY (DY) spacings, planes 1..NY+1
+  double *t = (double *)calloc(2 * (NY + 2), sizeof(double));
+  const double dx = h->p.lx / h->NX, dz = h->p.lz / h->NZ, cs = 0.13, beta_sgs = 1.0;
+  for (int j = 1; j <= NY + 1; j++) {
+    t[j] = -2.0 * cs * cs * pow(dx * beta_sgs * h->h_dyf[j] * 2.0 * dz * beta_sgs, 2.0 / 3.0);
+    t[NY + 2 + j] = -2.0 * cs * cs * pow(dx * beta_sgs * h->h_dy[j] * 2.0 * dz * beta_sgs, 2.0 / 3.0);
+  }
+  cudaError_t e = cudaMemcpyAsync(h->les_dfac, t, sizeof(double) * 2 * (NY + 2),
+                                  cudaMemcpyHostToDevice, h->st);
+  cudaError_t e2 = cudaStreamSynchronize(h->st);
+  free(t);
+  DG_CUDA(e);
+  DG_CUDA(e2);
+  h->les_nut = false;
+  return DG_OK;
+}
+
+// The subgrid model runs from the first step, or after 100 steps of a new
+// flow (for/channel.f:303).
+bool dg_les_active(const dg_handle *h, int time_step) {
+  return h->p.les && !h->periodic && (!h->p.create_new_flow || time_step > 100);
+}
+
+int dg_les_pre(dg_handle *h, int rk_step) {
+  (void)rk_step;
+  const int NY = h->NY;
+  const long ss = h->ss, ns = h->nspec, np = (long)h->NZ * h->NX, pf = pfield_of(h);
+  const LesBc B = make_bc(h->p);
+  // APPLY_BC_VEL_MPI, APPLY_BC_LES
+  DG_TRY(dg_apply_bc_vel_dev(h));
+  dg_kt_begin(h, "k_les_bc_spec", h->st);
+  k_les_bc_spec<<<dg_cdiv(ss, 256), 256, 0, h->st>>>(B, NY, ss, h->cu[0], h->cu[2]);
+  DG_LAUNCHED();
+  // strain rates and the plane means, then S_ij and U in physical space
+  dg_kt_begin(h, "k_les_strain", h->st);
+  k_les_strain<<<dg_cdiv((long)(NY + 2) * ss, 256), 256, 0, h->st>>>(
+      NY, ss, h->nkxp, h->kx, h->kz, h->dy, h->dyf, h->cu[0], h->cu[1], h->cu[2], sslot(h, SS_S),
+      ns, h->les_ubar);
+  DG_LAUNCHED();
+  const double2 *cs[6];
+  for (int c = 0; c < 6; c++) cs[c] = sslot(h, SS_S + c);
+  DG_TRY(to_physical(h, cs, 6, 0, NY + 1, pslot(h, PS_S)));
+  const double2 *cu[3] = {h->cu[0], h->cu[1], h->cu[2]};
+  DG_TRY(to_physical(h, cu, 3, 0, NY + 1, pslot(h, PS_U)));
+  dg_kt_begin(h, "k_les_bc_phys", h->st);
+  k_les_bc_phys<<<dg_cdiv(np, 256), 256, 0, h->st>>>(B, NY, np, pf, h->dy, h->dyf, pslot(h, PS_U));
+  DG_LAUNCHED();
+  dg_kt_begin(h, "k_les_model", h->st);
+  k_les_model<<<dg_cdiv(np, 128), 128, 0, h->st>>>(NY, np, pf, h->jstart, h->jend, h->dy, h->dyf,
+                                                   h->les_dfac, h->les_ubar, pslot(h, PS_S),
+                                                   pslot(h, PS_X), pslot(h, PS_U),
+                                                   pslot(h, PS_NUT));
+  DG_LAUNCHED();
+  h->les_nut = true;
+  // |S| S_ij (S_22 excluded) and the cross terms to Fourier space
+  double2 *o0[1] = {sslot(h, SS_S)};
+  DG_TRY(to_fourier(h, pslot(h, PS_S), 1, 0, NY + 1, o0));
+  double2 *o2[4] = {sslot(h, SS_S + 2), sslot(h, SS_S + 3), sslot(h, SS_S + 4), sslot(h, SS_S + 5)};
+  DG_TRY(to_fourier(h, pslot(h, PS_S + 2), 4, 0, NY + 1, o2));
+  double2 *ox[2] = {sslot(h, SS_X), sslot(h, SS_X + 1)};
+  DG_TRY(to_fourier(h, pslot(h, PS_X), 2, 2, NY, ox));
+  dg_kt_begin(h, "k_les_force", h->st);
+  k_les_force<<<dg_cdiv((long)(NY + 2) * ss, 256), 256, 0, h->st>>>(
+      NY, ss, h->nkxp, h->jstart, h->kx, h->kz, h->dyf, h->les_dfac, sslot(h, SS_S), ns,
+      sslot(h, SS_G));
+  DG_LAUNCHED();
+  // scalar eddy diffusion, KAPPA_T = NU_T
+  for (int n = 0; n < h->NTH; n++) {
+    dg_kt_begin(h, "k_les_th_grad", h->st);
+    k_les_th_grad<<<dg_cdiv((long)(NY + 2) * ss, 256), 256, 0, h->st>>>(
+        NY, ss, h->nkxp, h->kx, h->kz, h->cu[3 + n], sslot(h, SS_S), ns);
+    DG_LAUNCHED();
+    const double2 *tg[2] = {sslot(h, SS_S), sslot(h, SS_S + 1)};
+    DG_TRY(to_physical(h, tg, 2, 0, NY + 1, pslot(h, PS_S)));
+    dg_kt_begin(h, "k_les_th_scale", h->st);
+    k_les_th_scale<<<dg_cdiv((long)(NY + 1) * np, 256), 256, 0, h->st>>>(NY, np, pf,
+                                                                       pslot(h, PS_NUT),
+                                                                       pslot(h, PS_S));
+    DG_LAUNCHED();
+    double2 *tf[2] = {sslot(h, SS_S), sslot(h, SS_S + 1)};
+    DG_TRY(to_fourier(h, pslot(h, PS_S), 2, 0, NY + 1, tf));
+    dg_kt_begin(h, "k_les_th_force", h->st);
+    k_les_th_force<<<dg_cdiv((long)(NY + 2) * ss, 256), 256, 0, h->st>>>(
+        NY, ss, h->nkxp, h->jstart_th[n], h->jend_th[n], h->kx, h->kz, sslot(h, SS_S), ns,
+        sslot(h, SS_G + 3 + n));
+    DG_LAUNCHED();
+  }
+  // the nonlinear stage reads the velocity from CU: give its boundary planes
+  // the values APPLY_BC_VEL_PHYS left in the physical velocity (retained
+  // modes only, so the transform is exact)
+  double2 *v[3] = {h->cu[0], h->cu[1], h->cu[2]};
+  DG_TRY(to_fourier(h, pslot(h, PS_U), 3, 0, 1, v));
+  DG_TRY(to_fourier(h, pslot(h, PS_U), 3, NY, NY + 1, v));
+  return DG_OK;
+}
+
+int dg_les_post(dg_handle *h, int time_step, int rk_step, bool sgs) {
+  const int NY = h->NY;
+  const long ns = h->nspec, np = (long)h->NZ * h->NX, pf = pfield_of(h);
+  FieldPtrs cf, rhs;
+  for (int f = 0; f < h->nf; f++) {
+    cf.p[f] = h->cf[f];
+    rhs.p[f] = h->rhs[f];
+  }
+  if (sgs) {
+    dg_kt_begin(h, "k_les_add", h->st);
+    k_les_add<<<dim3(dg_cdiv(ns, 256), h->nf), 256, 0, h->st>>>(h->nf, ns, h->dscal, rk_step,
+                                                                sslot(h, SS_G), cf, rhs);
+    DG_LAUNCHED();
+  } else {
+    // the model is idle this substep but NU_T stays in the solves; the
+    // velocity enters them as the plain transform of CU
+    const double2 *cu[3] = {h->cu[0], h->cu[1], h->cu[2]};
+    DG_TRY(to_physical(h, cu, 3, 0, NY + 1, pslot(h, PS_U)));
+  }
+  // right-hand sides and scalars to physical space
+  const double2 *r[3 + DG_MAX_TH];
+  for (int f = 0; f < h->nf; f++) r[f] = h->rhs[f];
+  DG_TRY(to_physical(h, r, h->nf, 1, NY, pslot(h, PS_S)));
+  if (h->NTH > 0) {
+    const double2 *th[DG_MAX_TH];
+    for (int n = 0; n < h->NTH; n++) th[n] = h->cu[3 + n];
+    DG_TRY(to_physical(h, th, h->NTH, 0, NY + 1, pslot(h, PS_TH)));
+  }
+  LesCn P;
+  memset(&P, 0, sizeof(P));
+  const dg_params &p = h->p;
+  P.NY = NY;
+  P.nf = h->nf;
+  P.JS = h->jstart;
+  P.JE = h->jend;
+  P.nu = p.nu;
+  P.nuv = p.nu_v_scale;
+  const int lo[3] = {p.u_bc_ymin, p.v_bc_ymin, p.w_bc_ymin}, hi[3] = {p.u_bc_ymax, p.v_bc_ymax, p.w_bc_ymax};
+  const double clo[3] = {p.u_bc_ymin_c1, p.v_bc_ymin_c1, p.w_bc_ymin_c1};
+  const double chi[3] = {p.u_bc_ymax_c1, p.v_bc_ymax_c1, p.w_bc_ymax_c1};
+  for (int f = 0; f < 3; f++) {
+    P.bc_lo[f] = lo[f];
+    P.bc_hi[f] = hi[f];
+    P.c1_lo[f] = clo[f];
+    P.c1_hi[f] = chi[f];
+  }
+  for (int n = 0; n < h->NTH; n++) {
+    P.jst[n] = h->jstart_th[n];
+    P.jet[n] = h->jend_th[n];
+    P.pr[n] = p.pr[n];
+    P.bc_lo[3 + n] = p.th_bc_ymin[n];
+    P.bc_hi[3 + n] = p.th_bc_ymax[n];
+    P.c1_lo[3 + n] = p.th_bc_ymin_c1[n];
+    P.c1_hi[3 + n] = p.th_bc_ymax_c1[n];
+  }
+  dg_kt_begin(h, "k_les_cn", h->st);
+  k_les_cn<<<dim3(dg_cdiv(np, 128), h->nf), 128, 0, h->st>>>(
+      P, np, pf, h->dscal, rk_step, h->dy, h->dyf, pslot(h, PS_NUT), pslot(h, PS_S),
+      pslot(h, PS_U), pslot(h, PS_TH), pslot(h, PS_TH + h->NTH));
+  DG_LAUNCHED();
+  // COURANT on the solved velocity (for/channel.f:1037-1040)
+  const bool cfl = p.variable_dt && rk_step == 3 && p.update_dt > 0 &&
+                   (time_step % p.update_dt) == 0;
+  if (cfl) DG_TRY(dg_courant_phys(h, pslot(h, PS_U) + np, pf));
+  double2 *v[3] = {h->cu[0], h->cu[1], h->cu[2]};
+  DG_TRY(to_fourier(h, pslot(h, PS_U), 3, 0, NY + 1, v));
+  if (h->NTH > 0) {
+    double2 *th[DG_MAX_TH];
+    for (int n = 0; n < h->NTH; n++) th[n] = h->cu[3 + n];
+    DG_TRY(to_fourier(h, pslot(h, PS_TH), h->NTH, 0, NY + 1, th));
+  }
+  DG_TRY(dg_rem_div_dev(h, 1, rk_step));
+  if (cfl) DG_TRY(dg_dt_commit(h));
+  return DG_OK;
+}
+
+// NU_T (COMMON /LES_VARS/, for/header:166) of the last LES substep, physical
+// layout [NY+2][NZ][NX].
+extern "C" int diablo_les_nu_t(dg_handle *h, double *dst, int where) {
+  if (!h || h->periodic || !dst) return DG_ERR_ARG;
+  if (!h->p.les || !h->les_phys) {
+    dg_set_error("the handle was created without LES");
+    return DG_ERR_ARG;
+  }
+  const size_t bytes = sizeof(double) * (size_t)pfield_of(h);
+  DG_CUDA(cudaMemcpyAsync(dst, pslot(h, PS_NUT), bytes,
+                          where == DG_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                          h->st));
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  return DG_OK;
+}

@@ -127,6 +127,27 @@ static int validate(const dg_params *p, const double *gy) {
         dg_set_error("Error: V_BC_Y* must be 0, 1, or 2");
         return DG_ERR_ARG;
       }
+    if (p->les) {
+      // for/les.f:269-272 and APPLY_BC_VEL_PHYS (for/channel.f:2537,2633)
+      if (p->les_model_type != 1) {
+        dg_set_error("ERROR: LES_MODEL_TYPE=2, 3 not supported yet in MPI");
+        return DG_ERR_ARG;
+      }
+      if (p->v_bc_ymin > 1 || p->v_bc_ymax > 1) {
+        dg_set_error("Error: V_BC_YMIN/V_BC_YMAX must be 0, 1 with LES");
+        return DG_ERR_ARG;
+      }
+      if (p->v_bc_ymax == 1) {
+        dg_set_error("LES with a Neumann V at the upper wall is not supported: APPLY_BC_VEL "
+                     "rewrites CU2(NY) after CR2(NY) was formed, which the fused stage cannot "
+                     "reproduce");
+        return DG_ERR_ARG;
+      }
+      if (p->precision != 0) {
+        dg_set_error("LES runs in FP64 (precision 0)");
+        return DG_ERR_ARG;
+      }
+    }
     if (p->precision != 0 && p->precision != 1) {
       dg_set_error("precision must be 0 (FP64) or 1 (mixed)");
       return DG_ERR_ARG;
@@ -364,6 +385,7 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
   }
   DG_TRY(diablo_set_time(h, 0.0, p->delta_t));
   if (!h->periodic) DG_TRY(dg_chan_init(h));
+  if (!h->periodic && p->les) DG_TRY(dg_les_init(h));
   DG_CUDA(cudaStreamSynchronize(h->st));
   return DG_OK;
 }
@@ -376,6 +398,10 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
                 h->twy, h->twx_f, h->twz_f, h->twy_f, h->dscal, h->cp, h->cr1, h->gphi, h->rem_a, h->rem_rb, h->cn_tab, h->cn_rows, h->H, h->G, h->work, h->dmin_bits, h->dflag, h->Hy, h->P,
                 h->Q};
   for (void *q : dp) dg_free(h, q);
+  dg_free(h, h->les_phys);
+  dg_free(h, h->les_spec);
+  dg_free(h, h->les_dfac);
+  dg_free(h, h->les_ubar);
   for (int f = 0; f < 3 + DG_MAX_TH; f++) {
     dg_free(h, h->cu[f]);
     dg_free(h, h->cf[f]);

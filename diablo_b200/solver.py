@@ -244,6 +244,12 @@ class Channel(_Solver):
     def rk_chan_1(self, time_step: int, rk_step: int):
         self._call("diablo_rk_chan_1", time_step, rk_step)
 
+    def nu_t(self) -> np.ndarray:
+        """NU_T of the last LES substep (physical, GY points)."""
+        out = np.zeros(self.phys_shape)
+        self._call("diablo_les_nu_t", _ptr(out), _lib.DG_HOST)
+        return out
+
     def rem_div_chan(self):
         self._call("diablo_rem_div_chan")
 

@@ -122,6 +122,11 @@ int diablo_get_field(dg_handle *h, int field, double *dst, int layout, int where
 /* SUBROUTINE RK_CHAN_1 (for/channel.f:62-1073): one RK3 substep on the
  * device-resident state.  time_step/rk_step are COMMON /RUNTIME_VARS/. */
 int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step);
+/* LES (dg_params.les = 1, LES_MODEL_TYPE 1): RK_CHAN_1 then also runs
+ * les_chan (for/les.f:1-275) and the eddy-viscosity Crank-Nicolson solves on
+ * physical columns (for/channel.f:299-372,631-659,748-1029).  NU_T at GY
+ * points (COMMON NU_T, for/header:166), physical layout [NY+2][NZ][NX]. */
+int diablo_les_nu_t(dg_handle *h, double *dst, int where);
 /* SUBROUTINE REM_DIV_CHAN (for/channel.f:1103-1214): projects CU1..3, leaves
  * phi in CR1. */
 int diablo_rem_div_chan(dg_handle *h);

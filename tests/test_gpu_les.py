@@ -1,0 +1,131 @@
+"""Channel LES (constant Smagorinsky) on the device against the oracle
+(needs a B200).
+
+The device keeps the fused spectral nonlinear stage and adds the subgrid
+model around it; the oracle follows the reference's physical-space order
+(for/les.f:1-275, for/channel.f:299-372,631-659,748-1029).  Parity bar: FP64,
+relative L2 <= 1e-11 per field after the steps below, NU_T to 1e-11 of its
+largest value, and the projected velocity divergence-free to 1e-12.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from diablo_b200 import configs, ics
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-11
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def start(p, gy, maker, seed, **kw):
+    from diablo_b200.solver import Channel
+    ref = O.Oracle(p, gy)
+    u1, u2, u3, th = maker(p, gy, seed=seed, **kw)
+    ref.create_flow_chan(u1, u2, u3, th if p.n_th else None)
+    ch = Channel(p, gy)
+    ch.set_state(ref.state())
+    ch.set_time(0.0, p.delta_t)
+    return ref, ch
+
+
+def compare(ref, ch, p, tol=TOL):
+    bad = {}
+    names = ["CU1", "CU2", "CU3", "CP"] + [f"CTH{n}" for n in range(p.n_th)]
+    for n in names:
+        r = rel(ch.get_field(n), ref.get(n))
+        if not r <= tol:
+            bad[n] = r
+    a, b = ch.nu_t(), ref.nu_t()
+    e = np.abs(a - b).max()
+    if not e <= tol * np.abs(b).max():
+        bad["NU_T"] = e
+    assert not bad, bad
+    return np.abs(b).max()
+
+
+def kh_les(**kw):
+    p, gy = configs.kh_shear_layer(nx=64, ny=33, nz=32)
+    p = p.replace(les=1, les_model_type=1, n_th=2, delta_t=0.02, **kw)
+    p.ri = [0.1, 0.05, 0, 0]
+    p.pr = [1.0, 0.7, 1, 1]
+    p.th_bc_ymin = [0, 1, 0, 0]      # the second scalar has Neumann walls: JSTART_TH = 1
+    p.th_bc_ymax = [0, 1, 0, 0]
+    p.th_bc_ymin_c1 = [-1.0, 0.0, 0, 0]
+    p.th_bc_ymax_c1 = [1.0, 0.0, 0, 0]
+    return p, gy
+
+
+def test_kh_les_neumann_walls_two_scalars():
+    p, gy = kh_les()
+    ref, ch = start(p, gy, ics.kh_shear_layer, seed=21, kick=0.3)
+    for s in range(1, 9):
+        ref.step(s)
+        ch.step(s)
+    assert compare(ref, ch, p) > 1e-4          # the model is doing work
+    assert ch.stats()["div_max"] < 1e-12
+    ch.close()
+
+
+def test_channel_les_no_slip_with_courant():
+    p, gy = configs.channel_re180(nx=64, ny=65, nz=48)
+    p = p.replace(les=1, les_model_type=1)
+    ref, ch = start(p, gy, ics.channel_laminar, seed=22)
+    for s in range(1, 6):
+        ref.step(s)
+        ch.step(s)
+    assert abs(ch.get_time()[1] - ref.get_time()[1]) <= 1e-13 * ref.get_time()[1]
+    assert compare(ref, ch, p) > 1e-6
+    assert ch.stats()["div_max"] < 1e-12
+    ch.close()
+
+
+def test_spin_up_then_model():
+    from diablo_b200.solver import Channel
+    p, gy = kh_les(create_new_flow=1)
+    ref, ch = start(p, gy, ics.kh_shear_layer, seed=23, kick=0.3)
+    dns = Channel(p.replace(les=0), gy)
+    dns.set_state(ref.state())
+    dns.set_time(0.0, p.delta_t)
+    for s in (1, 2):
+        ref.step(s)
+        ch.step(s)
+        dns.step(s)
+    # during the first 100 steps of a new flow the LES handle runs the DNS
+    for n in ("CU1", "CU2", "CU3", "CP", "CTH0", "CTH1"):
+        assert np.array_equal(ch.get_field(n), dns.get_field(n)), n
+    for s in (101, 102):
+        ref.step(s)
+        ch.step(s)
+    compare(ref, ch, p)
+    ch.close()
+    dns.close()
+
+
+def test_les_graph_steps_match_eager():
+    from diablo_b200.solver import Channel
+    p, gy = kh_les()
+    ref, eager = start(p, gy, ics.kh_shear_layer, seed=24, kick=0.3)
+    graph = Channel(p, gy)
+    graph.set_state(ref.state())
+    graph.set_time(0.0, p.delta_t)
+    for s in range(1, 5):
+        eager.step(s)
+    graph.steps(1, 4)
+    for n in ("CU1", "CU2", "CU3", "CP", "CTH0", "CTH1"):
+        assert np.array_equal(graph.get_field(n), eager.get_field(n)), n
+    eager.close()
+    graph.close()
+
+
+@pytest.mark.parametrize("bad", [dict(les_model_type=2), dict(precision=1), dict(v_bc_ymax=1)])
+def test_les_refusals(bad):
+    from diablo_b200.solver import Channel
+    from diablo_b200._lib import DiabloError
+    p, gy = configs.kh_shear_layer(nx=64, ny=33, nz=32)
+    with pytest.raises(DiabloError):
+        Channel(p.replace(les=1, **bad), gy)

@@ -311,6 +311,34 @@ def run_other_configs(args):
             ch.close()
             out[f"{name}_{'mixed' if prec else 'fp64'}"] = {
                 "ms_per_step": ms, "mpoint_steps_per_s": p.nx * p.ny * p.nz / ms / 1e3}
+    # LES (constant Smagorinsky, FP64): the reference's KH_test run and the
+    # Re_tau = 180 channel with the model on; the CPU oracle's time for the
+    # KH_test step beside it (all host threads, 2 steps)
+    for name, (p, gy), maker in (("kh_les_128x65x16", configs.kh_les(), ics.kh_shear_layer),
+                                 ("channel_re180_les_128x129x128",
+                                  (configs.channel_re180()[0].replace(les=1),
+                                   configs.channel_re180()[1]), ics.channel_laminar)):
+        kw = {"kick": 0.1} if maker is ics.kh_shear_layer else {}
+        u1, u2, u3, th = maker(p, gy, seed=2, **kw)
+        ch = Channel(p, gy, stream=stream)
+        ch.create_flow(u1, u2, u3, th if p.n_th else None)
+        ch.set_time(0.0, p.delta_t)
+        ms = timed(ch, 50)
+        rec = {"ms_per_step": ms, "mpoint_steps_per_s": p.nx * p.ny * p.nz / ms / 1e3,
+               "nu_t_max": float(ch.nu_t().max())}
+        ch.close()
+        if name.startswith("kh_les"):
+            import oracle as O
+            ref = O.Oracle(p, gy, threads=os.cpu_count() or 1)
+            ref.create_flow_chan(u1, u2, u3, th)
+            t0 = time.perf_counter()
+            for s in (1, 2):
+                ref.step(s)
+            rec["cpu_baseline"] = {"ms_per_step": (time.perf_counter() - t0) / 2 * 1e3,
+                                   "cores": os.cpu_count() or 1, "kind": "port",
+                                   "sample": "2 steps of the same case"}
+            ref.close()
+        out[name + "_fp64"] = rec
     # periodic 256^3, FP64 and mixed
     p, _ = configs.periodic_256()
     for prec in (0, 1):

@@ -7,6 +7,10 @@ channel_re180    : 128x129x128, Lx=4pi, Ly=2 (tanh stretch 1.75), Lz=4pi/3,
 periodic_256     : 256^3 on [0,2pi]^3, nu=1e-3, decaying.
 channel_re550    : 512x257x384, Lx=2pi, Ly=2 (tanh stretch 2.0), Lz=pi, one passive
                    scalar (Pr=0.71, Ri=0).
+kh_les           : the reference's KH_test run (KH_test/input.dat, input_chan.dat,
+                   grid_def.all, grid.h5): 128x65x16 stretched on [-10,10], Lx=30, Lz=4,
+                   nu=1e-3, Ri=0.15, Pr=1, free-slip U/W, V=0, Neumann TH, CFL=0.5,
+                   constant Smagorinsky LES.
 """
 from __future__ import annotations
 
@@ -50,6 +54,21 @@ def channel_re550(nx=512, ny=257, nz=384, cfl=0.5):
     p.th_bc_ymin_c1[0] = -1.0
     p.th_bc_ymax_c1[0] = 1.0
     return p, create_grid(1, ny, 2.0, 2.0)
+
+
+def kh_les(nx=128, ny=65, nz=16):
+    """The KH_test run with the subgrid model on from the first step (as after
+    a restart; a new flow would wait 100 steps) on its stretched grid
+    (KH_test/grid.h5: CREATE_GRID type 2, CS = 1.5)."""
+    p = Params(nx=nx, ny=ny, nz=nz, n_th=1, num_per_dir=2, nu=1e-3, beta=1.0, lx=30.0, ly=20.0,
+               lz=4.0, delta_t=0.1, variable_dt=1, update_dt=1, cfl=0.5, grav_y=1.0, f_type=0,
+               u_bc_ymin=1, v_bc_ymin=0, w_bc_ymin=1, u_bc_ymax=1, v_bc_ymax=0, w_bc_ymax=1,
+               les=1, les_model_type=1)
+    p.ri[0] = 0.15
+    p.pr[0] = 1.0
+    p.th_bc_ymin[0] = 1
+    p.th_bc_ymax[0] = 1
+    return p, create_grid(2, ny, 20.0, 1.5)
 
 
 def periodic_256(n=256, nu=1e-3, dt=2e-3):

@@ -166,6 +166,7 @@ struct dg_handle {
   double2 *les_spec;
   double *les_dfac;
   double *les_ubar;
+  double2 *les_H;               // half-physical staging for LES_HF fields
   bool les_nut;                 // NU_T has been computed (it stays in use from then on)
 };
 

@@ -19,16 +19,18 @@
 //          physical column builds the CN rows with the eddy-viscosity terms and
 //          the BC rows, runs the MPI Thomas sweeps and writes U / TH; COURANT on
 //          that velocity; forward transforms to CU / CTH; REM_DIV_CHAN.
-// Slots (physical): 0-5 S_ij (then R), 6-7 cross terms, 8-10 U1-U3, 11 NU_T,
-// 12.. TH(n), then 2 nf Thomas scratch (pivots b', upper diagonals c).
+// Slots (physical): 0-5 S_ij (then R), 6-7 cross terms, 8 NU_T, 9-11 U1-U3,
+// 12.. TH(n) (U and TH adjacent: one transform batch), then 2 nf Thomas scratch (pivots b', upper diagonals c; before
+// the solve they hold the five |S| S_ij products).
 // Slots (spectral): 0-5 CS_ij (then the products, then scalar temporaries),
 // 6-7 cross terms, 8.. G(f).
 #include "dg_internal.cuh"
 
 namespace {
 
-constexpr int PS_S = 0, PS_X = 6, PS_U = 8, PS_NUT = 11, PS_TH = 12;
+constexpr int PS_S = 0, PS_X = 6, PS_NUT = 8, PS_U = 9, PS_TH = 12;
 constexpr int SS_S = 0, SS_X = 6, SS_G = 8;
+constexpr int LES_HF = 8;  // fields per transform launch (the pointer-array capacity)
 
 inline int phys_slots(const dg_handle *h) { return PS_TH + h->NTH + 2 * h->nf; }
 inline int spec_slots(const dg_handle *h) { return SS_G + h->nf; }
@@ -164,68 +166,69 @@ __global__ void k_les_bc_phys(LesBc B, int NY, long np, long pfield, const doubl
     U2[jn1] = U2[jn] + dy[NY] * B.v_hi_c1;
 }
 
-// The model, one thread per physical column (i, k), marching j upwards with
-// the raw S_ij of planes j-1, j, j+1 in registers (for/les.f:114-227):
-// |S| at GYF for JSTART..JEND, |S| at GY for 2..NY+1, |S| S_ij in place,
-// NU_T at GY (zero on planes 1, 2, NY, NY+1: GHOST_LES_MPI for one rank) and
-// the cross terms NU_T dU1/dy, NU_T dU3/dy on planes 2..NY.
+// The model, one thread per physical point (for/les.f:114-227): |S| at GYF
+// for JSTART..JEND and at GY for 2..NY+1 from the raw S_ij of planes j-1,
+// j, j+1; the products |S| S_ij written out of place (P: S11, S33, S12 at
+// GY, S13, S23 at GY; raw where the reference leaves S_ij unscaled), NU_T at
+// GY (zero on planes 1, 2, NY, NY+1: GHOST_LES_MPI for one rank) and the
+// cross terms NU_T dU1/dy, NU_T dU3/dy on planes 2..NY.
 __global__ void k_les_model(int NY, long np, long pfield, int JS, int JE,
                             const double *__restrict__ dy, const double *__restrict__ dyf,
                             const double *__restrict__ dfac, const double *__restrict__ ubar,
-                            double *__restrict__ S, double *__restrict__ X,
-                            const double *__restrict__ U, double *__restrict__ NUT) {
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= np) return;
+                            const double *__restrict__ S, double *__restrict__ P,
+                            double *__restrict__ X, const double *__restrict__ U,
+                            double *__restrict__ NUT) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)(NY + 2) * np) return;
+  const int j = (int)(t / np);
+  const long o = t;
   const double *u1b = ubar, *u3b = ubar + NY + 2;
-  const double *U1 = U, *U3 = U + 2 * pfield;
-  double *X1 = X, *X3 = X + pfield;
-  double p0 = S[q], p1 = S[pfield + q], p2 = S[2 * pfield + q], p4 = S[4 * pfield + q];
-  for (int j = 1; j <= NY + 1; j++) {
-    const long o = (long)j * np + q;
-    const double r0 = S[o], r1 = S[pfield + o], r2 = S[2 * pfield + o], r3 = S[3 * pfield + o];
-    const double r4 = S[4 * pfield + o], r5 = S[5 * pfield + o];
-    double tg = 0.0;  // |S| at GY
-    if (j >= 2) {
-      const double w = 2.0 * dy[j];
-      const double b1 = (r0 * dyf[j - 1] + p0 * dyf[j]) / w;
-      const double b4 = r3 - 0.5 * (u1b[j] - u1b[j - 1]) / dy[j];
-      const double b5 = (r4 * dyf[j - 1] + p4 * dyf[j]) / w;
-      const double b2 = (r1 * dyf[j - 1] + p1 * dyf[j]) / w;
-      const double b6 = r5 - 0.5 * (u3b[j] - u3b[j - 1]) / dy[j];
-      const double b3 = (r2 * dyf[j - 1] + p2 * dyf[j]) / w;
-      tg = sqrt(2.0 * (b1 * b1) + 4.0 * (b4 * b4) + 4.0 * (b5 * b5) + 2.0 * (b2 * b2) +
-                4.0 * (b6 * b6) + 2.0 * (b3 * b3));
-    }
-    if (j >= JS && j <= JE) {
-      const double n3 = S[3 * pfield + o + np], n5 = S[5 * pfield + o + np];
-      const double a4 = 0.5 * (n3 + r3 - 0.5 * (u1b[j] - u1b[j - 1]) / dy[j] -
-                               0.5 * (u1b[j + 1] - u1b[j]) / dy[j + 1]);
-      const double a6 = 0.5 * (n5 + r5 - 0.5 * (u3b[j] - u3b[j - 1]) / dy[j] -
-                               0.5 * (u3b[j + 1] - u3b[j]) / dy[j + 1]);
-      const double sf = sqrt(2.0 * (r0 * r0) + 4.0 * (a4 * a4) + 4.0 * (r4 * r4) +
-                             2.0 * (r1 * r1) + 4.0 * (a6 * a6) + 2.0 * (r2 * r2));
-      S[o] = sf * r0;
-      S[4 * pfield + o] = sf * r4;
-      S[pfield + o] = 0.0;
-      S[2 * pfield + o] = sf * r2;
-    }
-    double nut = 0.0;
-    if (j >= 2) {
-      const double du1 = 0.5 * (U1[o] - U1[o - np]) / dy[j];
-      const double du3 = 0.5 * (U3[o] - U3[o - np]) / dy[j];
-      S[3 * pfield + o] = tg * (r3 - du1);
-      S[5 * pfield + o] = tg * (r5 - du3);
-      if (j >= 3 && j <= NY - 1) nut = -0.5 * dfac[NY + 2 + j] * tg;
-    }
+  const double r0 = S[o], r1 = S[pfield + o], r2 = S[2 * pfield + o], r3 = S[3 * pfield + o];
+  const double r4 = S[4 * pfield + o], r5 = S[5 * pfield + o];
+  double p0 = r0, p2 = r2, p3 = r3, p4 = r4, p5 = r5;
+  double tg = 0.0;  // |S| at GY
+  if (j >= 2) {
+    const long m = o - np;
+    const double w = 2.0 * dy[j];
+    const double b1 = (r0 * dyf[j - 1] + S[m] * dyf[j]) / w;
+    const double b4 = r3 - 0.5 * (u1b[j] - u1b[j - 1]) / dy[j];
+    const double b5 = (r4 * dyf[j - 1] + S[4 * pfield + m] * dyf[j]) / w;
+    const double b2 = (r1 * dyf[j - 1] + S[pfield + m] * dyf[j]) / w;
+    const double b6 = r5 - 0.5 * (u3b[j] - u3b[j - 1]) / dy[j];
+    const double b3 = (r2 * dyf[j - 1] + S[2 * pfield + m] * dyf[j]) / w;
+    tg = sqrt(2.0 * (b1 * b1) + 4.0 * (b4 * b4) + 4.0 * (b5 * b5) + 2.0 * (b2 * b2) +
+              4.0 * (b6 * b6) + 2.0 * (b3 * b3));
+    const double *U1 = U, *U3 = U + 2 * pfield;
+    const double du1 = 0.5 * (U1[o] - U1[m]) / dy[j];
+    const double du3 = 0.5 * (U3[o] - U3[m]) / dy[j];
+    p3 = tg * (r3 - du1);
+    p5 = tg * (r5 - du3);
+  }
+  if (j >= JS && j <= JE) {
+    const double n3 = S[3 * pfield + o + np], n5 = S[5 * pfield + o + np];
+    const double a4 = 0.5 * (n3 + r3 - 0.5 * (u1b[j] - u1b[j - 1]) / dy[j] -
+                             0.5 * (u1b[j + 1] - u1b[j]) / dy[j + 1]);
+    const double a6 = 0.5 * (n5 + r5 - 0.5 * (u3b[j] - u3b[j - 1]) / dy[j] -
+                             0.5 * (u3b[j + 1] - u3b[j]) / dy[j + 1]);
+    const double sf = sqrt(2.0 * (r0 * r0) + 4.0 * (a4 * a4) + 4.0 * (r4 * r4) +
+                           2.0 * (r1 * r1) + 4.0 * (a6 * a6) + 2.0 * (r2 * r2));
+    p0 = sf * r0;
+    p4 = sf * r4;
+    p2 = sf * r2;
+  }
+  P[o] = p0;
+  P[pfield + o] = p2;
+  P[2 * pfield + o] = p3;
+  P[3 * pfield + o] = p4;
+  P[4 * pfield + o] = p5;
+  if (j >= 1) {
+    const double nut = (j >= 3 && j <= NY - 1) ? -0.5 * dfac[NY + 2 + j] * tg : 0.0;
     NUT[o] = nut;
     if (j >= 2 && j <= NY) {
-      X1[o] = nut * (U1[o] - U1[o - np]) / dy[j];
-      X3[o] = nut * (U3[o] - U3[o - np]) / dy[j];
+      const double *U1 = U, *U3 = U + 2 * pfield;
+      X[o] = nut * (U1[o] - U1[o - np]) / dy[j];
+      X[pfield + o] = nut * (U3[o] - U3[o - np]) / dy[j];
     }
-    p0 = r0;
-    p1 = r1;
-    p2 = r2;
-    p4 = r4;
   }
 }
 
@@ -340,23 +343,22 @@ struct LesCn {
 // identity, then CN rows with the eddy-viscosity terms over the update range,
 // then the lower and upper BC rows (APPLY_BC_*_MPI, for/mpi.f:1137-1291 with
 // for/channel.f:1660-2241).  The right-hand side of a CN row is R plus the
-// explicit eddy-viscosity half.
+// explicit eddy-viscosity half.  um, uj, up: the field on planes j-1, j, j+1;
+// nm, nj, np1: NU_T on the same planes; r: R on plane j.
 __device__ __forceinline__ void les_row(const LesCn &P, int f, int j, double T1, double T2,
-                                        const double *dy, const double *dyf, const double *nut,
-                                        const double *R, const double *U, long np, double &l,
-                                        double &d, double &u, double &v) {
+                                        const double *dy, const double *dyf, double um, double uj,
+                                        double up, double nm_, double nj, double np1, double r,
+                                        double &l, double &d, double &u, double &v) {
   const int NY = P.NY;
   l = 0.0, d = 1.0, u = 0.0, v = 0.0;
-  const long o = (long)j * np;
   if (f == 1) {
     if (j >= 2 && j <= NY) {
       const double a = T1 * P.nuv;
       l = -a / (dyf[j - 1] * dy[j]);
       d = 1. + a / (dyf[j] * dy[j]) + a / (dyf[j - 1] * dy[j]);
       u = -a / (dyf[j] * dy[j]);
-      const double nm = 0.5 * (nut[o] + nut[o - np]), npl = 0.5 * (nut[o] + nut[o + np]);
-      v = R[o] + T2 * ((npl * (U[o + np] - U[o]) / dyf[j] - nm * (U[o] - U[o - np]) / dyf[j - 1]) /
-                       dy[j]);
+      const double nm = 0.5 * (nj + nm_), npl = 0.5 * (nj + np1);
+      v = r + T2 * ((npl * (up - uj) / dyf[j] - nm * (uj - um) / dyf[j - 1]) / dy[j]);
       l = l - T2 * nm / (dyf[j - 1] * dy[j]);
       d = d + T2 * npl / (dyf[j] * dy[j]) + T2 * nm / (dyf[j - 1] * dy[j]);
       u = u - T2 * npl / (dyf[j] * dy[j]);
@@ -373,7 +375,6 @@ __device__ __forceinline__ void les_row(const LesCn &P, int f, int j, double T1,
   const bool th = f >= 3;
   const int js = th ? P.jst[f - 3] : P.JS, je = th ? P.jet[f - 3] : P.JE;
   if (j >= js && j <= je) {
-    const double nj = nut[o], np1 = nut[o + np];
     if (th) {
       const double a = T1 / P.pr[f - 3] * P.nuv;
       l = -(a) / (dy[j] * dyf[j]);
@@ -384,8 +385,7 @@ __device__ __forceinline__ void les_row(const LesCn &P, int f, int j, double T1,
       d = 1. - T1 * P.nuv * (-1. / (dy[j + 1] * dyf[j]) - 1. / (dy[j] * dyf[j]));
       u = -T1 * P.nuv / (dy[j + 1] * dyf[j]);
     }
-    v = R[o] + T2 * ((np1 * (U[o + np] - U[o]) / dy[j + 1] - nj * (U[o] - U[o - np]) / dy[j]) /
-                     dyf[j]);
+    v = r + T2 * ((np1 * (up - uj) / dy[j + 1] - nj * (uj - um) / dy[j]) / dyf[j]);
     l = l - T2 * nj / (dy[j] * dyf[j]);
     d = d + T2 * np1 / (dy[j + 1] * dyf[j]) + T2 * nj / (dy[j] * dyf[j]);
     u = u - T2 * np1 / (dy[j + 1] * dyf[j]);
@@ -408,40 +408,67 @@ __device__ __forceinline__ void les_row(const LesCn &P, int f, int j, double T1,
 // and THOMAS_BACKWARD_REAL_MPI for the only rank (for/mpi.f:630-703,767-809),
 // the solution written back over the reference's ranges.  R (slot f) holds
 // the right-hand side and then the eliminated one; B (scratch) the pivots, C
-// the upper diagonals.
-__global__ void k_les_cn(LesCn P, long np, long pfield, const double *__restrict__ dscal,
-                         int rk_step, const double *__restrict__ dy, const double *__restrict__ dyf,
-                         const double *__restrict__ nut, double *__restrict__ Rbase,
-                         double *__restrict__ Ubase, double *__restrict__ THbase,
-                         double *__restrict__ Bbase) {
+// the upper diagonals.  Both sweeps load CB rows at a time before their
+// recurrence so the loads overlap.
+constexpr int CB = 8;
+
+__global__ void __launch_bounds__(128) k_les_cn(LesCn P, long np, long pfield,
+                                                const double *__restrict__ dscal, int rk_step,
+                                                const double *__restrict__ dy,
+                                                const double *__restrict__ dyf,
+                                                const double *__restrict__ nut,
+                                                double *__restrict__ Rbase,
+                                                double *__restrict__ Ubase,
+                                                double *__restrict__ THbase,
+                                                double *__restrict__ Bbase) {
   const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const int f = blockIdx.y;
   if (q >= np || f >= P.nf) return;
   const double h = dscal[1 + rk_step];
   const double T1 = P.nu * h / 2.0, T2 = h / 2.0;
-  const int NY = P.NY;
+  const int NY = P.NY, L = NY + 2;
   double *R = Rbase + (long)f * pfield + q;
   double *U = (f < 3 ? Ubase + (long)f * pfield : THbase + (long)(f - 3) * pfield) + q;
   double *B = Bbase + (long)f * pfield + q, *C = Bbase + (long)(P.nf + f) * pfield + q;
   const double *nq = nut + q;
   double l, d, u, v;
-  les_row(P, f, 0, T1, T2, dy, dyf, nq, R, U, np, l, d, u, v);
+  les_row(P, f, 0, T1, T2, dy, dyf, 0., 0., 0., 0., 0., 0., 0., l, d, u, v);
   double bprev = d, cprev = u, gprev = v;
   B[0] = d;
   C[0] = u;
   R[0] = v;
-  for (int j = 1; j <= NY + 1; j++) {
-    les_row(P, f, j, T1, T2, dy, dyf, nq, R, U, np, l, d, u, v);
-    const double a = -l / bprev;
-    const double b = d + a * cprev;
-    const double g = v + a * gprev;
-    const long o = (long)j * np;
-    B[o] = b;
-    C[o] = u;
-    R[o] = g;
-    bprev = b;
-    cprev = u;
-    gprev = g;
+  for (int j0 = 1; j0 < L; j0 += CB) {
+    double uu[CB + 2], nn[CB + 2], rr[CB];
+#pragma unroll
+    for (int k = 0; k < CB + 2; k++) {
+      const int j = j0 - 1 + k;
+      const bool ok = j < L;
+      uu[k] = ok ? U[(long)j * np] : 0.0;
+      nn[k] = ok ? nq[(long)j * np] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < CB; k++) {
+      const int j = j0 + k;
+      rr[k] = j < L ? R[(long)j * np] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < CB; k++) {
+      const int j = j0 + k;
+      if (j < L) {
+        les_row(P, f, j, T1, T2, dy, dyf, uu[k], uu[k + 1], uu[k + 2], nn[k], nn[k + 1], nn[k + 2],
+                rr[k], l, d, u, v);
+        const double a = -l / bprev;
+        const double b = d + a * cprev;
+        const double g = v + a * gprev;
+        const long o = (long)j * np;
+        B[o] = b;
+        C[o] = u;
+        R[o] = g;
+        bprev = b;
+        cprev = u;
+        gprev = g;
+      }
+    }
   }
   // back substitution; rows written back: U1/U3 JSTART-1..JEND+1, U2
   // 1..NY+1, TH(n) JSTART_TH-1..JEND_TH+1
@@ -451,30 +478,45 @@ __global__ void k_les_cn(LesCn P, long np, long pfield, const double *__restrict
   else { wlo = P.JS - 1; whi = P.JE + 1; }
   double x = gprev / bprev;
   if (NY + 1 >= wlo && NY + 1 <= whi) U[(long)(NY + 1) * np] = x;
-  for (int j = NY; j >= 0; j--) {
-    const long o = (long)j * np;
-    const double bj = B[o];
-    x = (bj != 0.0) ? (R[o] - C[o] * x) / bj : 0.0;
-    if (j >= wlo && j <= whi) U[o] = x;
+  for (int j1 = NY; j1 >= 0; j1 -= CB) {
+    double bb[CB], cc[CB], gg[CB];
+#pragma unroll
+    for (int k = 0; k < CB; k++) {
+      const int j = j1 - k;
+      const long o = (long)(j >= 0 ? j : 0) * np;
+      bb[k] = B[o];
+      cc[k] = C[o];
+      gg[k] = R[o];
+    }
+#pragma unroll
+    for (int k = 0; k < CB; k++) {
+      const int j = j1 - k;
+      if (j >= 0) {
+        x = (bb[k] != 0.0) ? (gg[k] - cc[k] * x) / bb[k] : 0.0;
+        if (j >= wlo && j <= whi) U[(long)j * np] = x;
+      }
+    }
   }
 }
 
+// n spectral fields (planes jmin..jmax) to physical slots at stride pfield,
+// and back, LES_HF fields per launch through the LES staging buffer
 int to_physical(dg_handle *h, const double2 *const *in, int n, int jmin, int jmax, double *out) {
   const long pplane = (long)h->NZ * h->NX, pf = pfield_of(h);
-  for (int b = 0; b < n; b += h->nf) {
-    const int k = (n - b < h->nf) ? n - b : h->nf;
-    DG_TRY(dg_zinv(h, in + b, k, jmin, jmax, h->H, 0));
-    DG_TRY(dg_xc2r_planes(h, h->H, k, jmin, jmax, out + (long)b * pf, pplane, h->NX, pf));
+  for (int b = 0; b < n; b += LES_HF) {
+    const int k = (n - b < LES_HF) ? n - b : LES_HF;
+    DG_TRY(dg_zinv(h, in + b, k, jmin, jmax, h->les_H, 0));
+    DG_TRY(dg_xc2r_planes(h, h->les_H, k, jmin, jmax, out + (long)b * pf, pplane, h->NX, pf));
   }
   return DG_OK;
 }
 
 int to_fourier(dg_handle *h, const double *in, int n, int jmin, int jmax, double2 *const *out) {
   const long pplane = (long)h->NZ * h->NX, pf = pfield_of(h);
-  for (int b = 0; b < n; b += h->nf) {
-    const int k = (n - b < h->nf) ? n - b : h->nf;
-    DG_TRY(dg_xr2c_planes(h, in + (long)b * pf, k, jmin, jmax, pplane, h->NX, pf, h->H));
-    DG_TRY(dg_zfwd_planes(h, h->H, k, jmin, jmax, out + b, nullptr, 0));
+  for (int b = 0; b < n; b += LES_HF) {
+    const int k = (n - b < LES_HF) ? n - b : LES_HF;
+    DG_TRY(dg_xr2c_planes(h, in + (long)b * pf, k, jmin, jmax, pplane, h->NX, pf, h->les_H));
+    DG_TRY(dg_zfwd_planes(h, h->les_H, k, jmin, jmax, out + b, nullptr, 0));
   }
   return DG_OK;
 }
@@ -488,6 +530,8 @@ int dg_les_init(dg_handle *h) {
   DG_CUDA(dg_malloc(h, (void **)&h->les_spec, sizeof(double2) * ns * spec_slots(h)));
   DG_CUDA(dg_malloc(h, (void **)&h->les_dfac, sizeof(double) * 2 * (NY + 2)));
   DG_CUDA(dg_malloc(h, (void **)&h->les_ubar, sizeof(double) * 2 * (NY + 2)));
+  DG_CUDA(dg_malloc(h, (void **)&h->les_H,
+                    sizeof(double2) * LES_HF * (size_t)h->nplanes * h->NZ * h->nkxp));
   DG_CUDA(cudaMemsetAsync(h->les_phys, 0, sizeof(double) * pf * phys_slots(h), h->st));
   DG_CUDA(cudaMemsetAsync(h->les_spec, 0, sizeof(double2) * ns * spec_slots(h), h->st));
   // -2 C_S^2 (DX BETA DY 2 DZ BETA)^(2/3), C_S = 0.13, BETA = 1 (for/les.f:194-217),
@@ -538,18 +582,18 @@ int dg_les_pre(dg_handle *h, int rk_step) {
   dg_kt_begin(h, "k_les_bc_phys", h->st);
   k_les_bc_phys<<<dg_cdiv(np, 256), 256, 0, h->st>>>(B, NY, np, pf, h->dy, h->dyf, pslot(h, PS_U));
   DG_LAUNCHED();
+  // the products go to the Thomas scratch slots (free until the solve)
+  double *prod = pslot(h, PS_TH + h->NTH);
   dg_kt_begin(h, "k_les_model", h->st);
-  k_les_model<<<dg_cdiv(np, 128), 128, 0, h->st>>>(NY, np, pf, h->jstart, h->jend, h->dy, h->dyf,
-                                                   h->les_dfac, h->les_ubar, pslot(h, PS_S),
-                                                   pslot(h, PS_X), pslot(h, PS_U),
-                                                   pslot(h, PS_NUT));
+  k_les_model<<<dg_cdiv((long)(NY + 2) * np, 256), 256, 0, h->st>>>(
+      NY, np, pf, h->jstart, h->jend, h->dy, h->dyf, h->les_dfac, h->les_ubar, pslot(h, PS_S),
+      prod, pslot(h, PS_X), pslot(h, PS_U), pslot(h, PS_NUT));
   DG_LAUNCHED();
   h->les_nut = true;
   // |S| S_ij (S_22 excluded) and the cross terms to Fourier space
-  double2 *o0[1] = {sslot(h, SS_S)};
-  DG_TRY(to_fourier(h, pslot(h, PS_S), 1, 0, NY + 1, o0));
-  double2 *o2[4] = {sslot(h, SS_S + 2), sslot(h, SS_S + 3), sslot(h, SS_S + 4), sslot(h, SS_S + 5)};
-  DG_TRY(to_fourier(h, pslot(h, PS_S + 2), 4, 0, NY + 1, o2));
+  double2 *op[5] = {sslot(h, SS_S), sslot(h, SS_S + 2), sslot(h, SS_S + 3), sslot(h, SS_S + 4),
+                    sslot(h, SS_S + 5)};
+  DG_TRY(to_fourier(h, prod, 5, 0, NY + 1, op));
   double2 *ox[2] = {sslot(h, SS_X), sslot(h, SS_X + 1)};
   DG_TRY(to_fourier(h, pslot(h, PS_X), 2, 2, NY, ox));
   dg_kt_begin(h, "k_les_force", h->st);
@@ -651,13 +695,9 @@ int dg_les_post(dg_handle *h, int time_step, int rk_step, bool sgs) {
   const bool cfl = p.variable_dt && rk_step == 3 && p.update_dt > 0 &&
                    (time_step % p.update_dt) == 0;
   if (cfl) DG_TRY(dg_courant_phys(h, pslot(h, PS_U) + np, pf));
-  double2 *v[3] = {h->cu[0], h->cu[1], h->cu[2]};
-  DG_TRY(to_fourier(h, pslot(h, PS_U), 3, 0, NY + 1, v));
-  if (h->NTH > 0) {
-    double2 *th[DG_MAX_TH];
-    for (int n = 0; n < h->NTH; n++) th[n] = h->cu[3 + n];
-    DG_TRY(to_fourier(h, pslot(h, PS_TH), h->NTH, 0, NY + 1, th));
-  }
+  double2 *v[3 + DG_MAX_TH];
+  for (int f = 0; f < h->nf; f++) v[f] = h->cu[f];
+  DG_TRY(to_fourier(h, pslot(h, PS_U), h->nf, 0, NY + 1, v));
   DG_TRY(dg_rem_div_dev(h, 1, rk_step));
   if (cfl) DG_TRY(dg_dt_commit(h));
   return DG_OK;

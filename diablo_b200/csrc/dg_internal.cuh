@@ -167,6 +167,8 @@ struct dg_handle {
   double *les_dfac;
   double *les_ubar;
   double2 *les_H;               // half-physical staging for LES_HF fields
+  double *les_means;            // [2][NY+2]: NU_T_MEAN, EPS_SGS1_MEAN of a requested substep
+  bool les_stats_req, les_stats_valid;
   bool les_nut;                 // NU_T has been computed (it stays in use from then on)
 };
 

@@ -272,6 +272,37 @@ __global__ void k_les_force(int NY, long ss, int nkxp, int JS, const double *__r
   g[2 * nspec + q] = g3;
 }
 
+// Plane means for mean_les (for/les.f:336-459), one block per plane:
+// NU_T_MEAN and EPS_SGS1_MEAN = <F1 U1 + F3 U3 + F2 U2>, F the SGS stress
+// divergence in physical space (slots at stride pfield, U likewise).
+__global__ void k_les_means(long np, long pfield, const double *__restrict__ F,
+                            const double *__restrict__ U, const double *__restrict__ nut,
+                            double *__restrict__ out, int L) {
+  const int j = blockIdx.x;
+  const long base = (long)j * np;
+  double a = 0.0, b = 0.0;
+  for (long q = threadIdx.x; q < np; q += blockDim.x) {
+    const long o = base + q;
+    a += F[o] * U[o] + F[2 * pfield + o] * U[2 * pfield + o] + F[pfield + o] * U[pfield + o];
+    b += nut[o];
+  }
+  __shared__ double sa[256], sb[256];
+  sa[threadIdx.x] = a;
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      sa[threadIdx.x] += sa[threadIdx.x + w];
+      sb[threadIdx.x] += sb[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[j] = sb[0] / (double)np;
+    out[L + j] = sa[0] / (double)np;
+  }
+}
+
 // i kx CTH and i kz CTH on planes 1..NY+1 (for/channel.f:326-355)
 __global__ void k_les_th_grad(int NY, long ss, int nkxp, const double *__restrict__ kxv,
                               const double *__restrict__ kzv, const double2 *__restrict__ th,
@@ -530,6 +561,7 @@ int dg_les_init(dg_handle *h) {
   DG_CUDA(dg_malloc(h, (void **)&h->les_spec, sizeof(double2) * ns * spec_slots(h)));
   DG_CUDA(dg_malloc(h, (void **)&h->les_dfac, sizeof(double) * 2 * (NY + 2)));
   DG_CUDA(dg_malloc(h, (void **)&h->les_ubar, sizeof(double) * 2 * (NY + 2)));
+  DG_CUDA(dg_malloc(h, (void **)&h->les_means, sizeof(double) * 2 * (NY + 2)));
   DG_CUDA(dg_malloc(h, (void **)&h->les_H,
                     sizeof(double2) * LES_HF * (size_t)h->nplanes * h->NZ * h->nkxp));
   DG_CUDA(cudaMemsetAsync(h->les_phys, 0, sizeof(double) * pf * phys_slots(h), h->st));
@@ -601,6 +633,19 @@ int dg_les_pre(dg_handle *h, int rk_step) {
       NY, ss, h->nkxp, h->jstart, h->kx, h->kz, h->dyf, h->les_dfac, sslot(h, SS_S), ns,
       sslot(h, SS_G));
   DG_LAUNCHED();
+  if (h->les_stats_req) {
+    // the velocity here has APPLY_BC_VEL_PHYS applied; les_chan's own is the
+    // one before it, which differs on planes 1 and NY only for non-zero BC
+    // constants
+    const double2 *g[3] = {sslot(h, SS_G), sslot(h, SS_G + 1), sslot(h, SS_G + 2)};
+    DG_TRY(to_physical(h, g, 3, 0, NY + 1, pslot(h, PS_S)));
+    dg_kt_begin(h, "k_les_means", h->st);
+    k_les_means<<<NY + 2, 256, 0, h->st>>>(np, pf, pslot(h, PS_S), pslot(h, PS_U),
+                                           pslot(h, PS_NUT), h->les_means, NY + 2);
+    DG_LAUNCHED();
+    h->les_stats_req = false;
+    h->les_stats_valid = true;
+  }
   // scalar eddy diffusion, KAPPA_T = NU_T
   for (int n = 0; n < h->NTH; n++) {
     dg_kt_begin(h, "k_les_th_grad", h->st);
@@ -714,6 +759,30 @@ extern "C" int diablo_les_nu_t(dg_handle *h, double *dst, int where) {
   const size_t bytes = sizeof(double) * (size_t)pfield_of(h);
   DG_CUDA(cudaMemcpyAsync(dst, pslot(h, PS_NUT), bytes,
                           where == DG_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                          h->st));
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  return DG_OK;
+}
+
+// les_chan's plane means at the SAVE_STATS cadence (MOD(TIME_STEP,
+// SAVE_STATS_INT) = 0 and RK_STEP = 1, for/les.f:336): the request makes the
+// next LES substep record NU_T_MEAN and EPS_SGS1_MEAN (rows 0..NY+1), which
+// diablo_les_stats returns.
+extern "C" int diablo_les_stats_request(dg_handle *h) {
+  if (!h || h->periodic || !h->p.les) return DG_ERR_ARG;
+  h->les_stats_req = true;
+  return DG_OK;
+}
+
+extern "C" int diablo_les_stats(dg_handle *h, double *nu_t_mean, double *eps_sgs1_mean) {
+  if (!h || h->periodic || !h->p.les || !nu_t_mean || !eps_sgs1_mean) return DG_ERR_ARG;
+  if (!h->les_stats_valid) {
+    dg_set_error("no LES substep has recorded statistics since the request");
+    return DG_ERR_ARG;
+  }
+  const size_t n = sizeof(double) * (h->NY + 2);
+  DG_CUDA(cudaMemcpyAsync(nu_t_mean, h->les_means, n, cudaMemcpyDeviceToHost, h->st));
+  DG_CUDA(cudaMemcpyAsync(eps_sgs1_mean, h->les_means + h->NY + 2, n, cudaMemcpyDeviceToHost,
                           h->st));
   DG_CUDA(cudaStreamSynchronize(h->st));
   return DG_OK;

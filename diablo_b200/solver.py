@@ -250,6 +250,16 @@ class Channel(_Solver):
         self._call("diablo_les_nu_t", _ptr(out), _lib.DG_HOST)
         return out
 
+    def les_stats_request(self):
+        """Record les_chan's plane means in the next LES substep."""
+        self._call("diablo_les_stats_request")
+
+    def les_stats(self) -> dict:
+        """NU_T_MEAN ('nu_sgs') and EPS_SGS1_MEAN ('eps_sgs1'), rows 0..NY+1."""
+        a, b = np.zeros(self.p.ny + 2), np.zeros(self.p.ny + 2)
+        self._call("diablo_les_stats", _ptr(a), _ptr(b))
+        return {"nu_sgs": a, "eps_sgs1": b}
+
     def rem_div_chan(self):
         self._call("diablo_rem_div_chan")
 

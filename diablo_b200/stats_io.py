@@ -1,5 +1,6 @@
-"""Text outputs of SAVE_STATS_CHAN and tkebudget_chan in the reference's
-formats (for/save_stats.f:66-81,414-420,665-674,1161-1170).
+"""Text outputs of SAVE_STATS_CHAN, tkebudget_chan and les_chan in the
+reference's formats (for/save_stats.f:66-81,414-420,665-674,1161-1170,
+for/les.f:491-503).
 
 The profile dictionaries come from ``Channel.save_stats()`` and
 ``Channel.stats_means()``.  Data rows use the reference's explicit FORMATs
@@ -71,3 +72,17 @@ def write_stats_final(path: str, means: dict, gyf: np.ndarray):
         for th in means["thbar"]:
             for j in range(1, ny + 1):
                 f.write(f"{j:3d},{gyf[j]:16.9f},{th[j]:16.9f}\n")
+
+
+def write_mean_les(path: str, st: dict, gyf: np.ndarray, time_step: int, time: float,
+                   delta_t: float):
+    """mean_les.txt of les_chan (for/les.f:498-510): j, GYF, NU_T_MEAN,
+    EPS_SGS1_MEAN for j = 1..NY under FORMAT (I3,' ',2(F30.20,' ')).  Four
+    items against a three-item format: format reversion puts EPS_SGS1_MEAN
+    on a record of its own under the repeated group."""
+    ny = len(gyf) - 2
+    with open(path, "w") as f:
+        _head(f, time_step, time, delta_t)
+        for j in range(1, ny + 1):
+            f.write(f"{j:3d} {gyf[j]:30.20f} {st['nu_sgs'][j]:30.20f} \n"
+                    f"{st['eps_sgs1'][j]:30.20f} \n")

@@ -127,6 +127,12 @@ int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step);
  * physical columns (for/channel.f:299-372,631-659,748-1029).  NU_T at GY
  * points (COMMON NU_T, for/header:166), physical layout [NY+2][NZ][NX]. */
 int diablo_les_nu_t(dg_handle *h, double *dst, int where);
+/* les_chan's mean_les output (for/les.f:336-510): after a request, the next
+ * LES substep (the reference: MOD(TIME_STEP,SAVE_STATS_INT) = 0, RK_STEP = 1)
+ * records the plane means NU_T_MEAN and EPS_SGS1_MEAN, rows 0..NY+1 (host
+ * arrays of NY+2). */
+int diablo_les_stats_request(dg_handle *h);
+int diablo_les_stats(dg_handle *h, double *nu_t_mean, double *eps_sgs1_mean);
 /* SUBROUTINE REM_DIV_CHAN (for/channel.f:1103-1214): projects CU1..3, leaves
  * phi in CR1. */
 int diablo_rem_div_chan(dg_handle *h);

@@ -156,6 +156,8 @@ orc *orc_create(const orc_params *p, const double *gy) {
     o->NU_T = zalloc(np, sizeof(double));
     o->TEMP = zalloc(np, sizeof(double));
     o->CTEMP = zalloc(ns, sizeof(cplx));
+    o->nu_t_mean = zalloc(o->NY + 2, sizeof(double));
+    o->eps_sgs1_mean = zalloc(o->NY + 2, sizeof(double));
     for (int c = 0; c < 6; c++) {
       o->Sij[c] = zalloc(np, sizeof(double));
       o->CSij[c] = zalloc(ns, sizeof(cplx));
@@ -181,6 +183,8 @@ void orc_destroy(orc *o) {
   free(o->NU_T);
   free(o->TEMP);
   free(o->CTEMP);
+  free(o->nu_t_mean);
+  free(o->eps_sgs1_mean);
   for (int c = 0; c < 6; c++) {
     free(o->Sij[c]);
     free(o->CSij[c]);

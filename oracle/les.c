@@ -2,8 +2,8 @@
  * Oracle restatement of the channel LES (constant Smagorinsky, the only
  * model the MPI build runs).  TEST INFRASTRUCTURE ONLY (see oracle.h).
  *
- * Follows for/les.f:1-275 (les_chan, LES_MODEL_TYPE = 1, without the
- * mean_les output), for/les.f:526-569 (compute_strain_chan),
+ * Follows for/les.f:1-275 (les_chan, LES_MODEL_TYPE = 1) with its plane
+ * means for mean_les (for/les.f:336-459), for/les.f:526-569 (compute_strain_chan),
  * for/les.f:805-865 (APPLY_BC_LES), for/mpi.f:352-515 (GHOST_LES_MPI with
  * NPROCY = 1: NU_T = 0 on planes 1, 2, NY, NY+1), for/channel.f:2495-2652
  * (APPLY_BC_VEL_PHYS_LOWER/UPPER) and the scalar eddy-diffusivity block of
@@ -107,6 +107,66 @@ void orc_apply_bc_vel_phys(orc *o) {
 static double delta_factor(const orc *o, double d) {
   const double cs = 0.13, beta_sgs = 1.0;
   return -2.0 * cs * cs * pow(o->DX * beta_sgs * d * 2.0 * o->DZ * beta_sgs, 2.0 / 3.0);
+}
+
+/* The plane means les_chan writes to mean_les (for/les.f:336-459): NU_T and
+ * EPS_SGS1 = <F1 U1 + F3 U3 + F2 U2>, F the SGS stress divergence in physical
+ * space (the cross terms of F2 transformed separately, as the reference
+ * does), with the velocity as les_chan holds it (before APPLY_BC_VEL_PHYS).
+ * CTEMP planes the loops do not write are zero in the reference. */
+static void les_means(orc *o, int J1, int J2) {
+  const int NY = o->NY, NX = o->NX, NZ = o->NZ, nkxp = o->nkxp, nkzt = o->nkzt;
+  const long np = (long)NX * NZ;
+  const double *DY = o->DY, *DYF = o->DYF;
+  cplx **CS = o->CSij, *CT = o->CTEMP;
+  double *T = o->TEMP, *NUT = o->NU_T;
+  const double *U[3] = {o->U1, o->U2, o->U3};
+  double *eps = o->eps_sgs1_mean, *num = o->nu_t_mean;
+  for (int j = 0; j <= NY + 1; j++) {
+    double a = 0.0, b = 0.0;
+    for (long q = 0; q < np; q++) b += NUT[j * np + q];
+    num[j] = b / (double)(NX * NZ);
+    eps[j] = a;
+  }
+  for (int part = 0; part < 5; part++) {
+    memset(CT, 0, sizeof(cplx) * o->nspec);
+    const double *Uf = part == 0 ? U[0] : part == 1 ? U[2] : U[1];
+    if (part < 3) {
+      const int j0 = part < 2 ? J1 : 2, j1 = part < 2 ? J2 : NY;
+      for (int j = j0; j <= j1; j++)
+        for (int k = 0; k < nkzt; k++)
+          for (int i = 0; i < nkxp; i++) {
+            const long s = SIDX(o, j, k, i), sp = s + o->ss;
+            if (part == 0)
+              CT[s] = -o->CIKX[i] * CS[0][s] - (CS[3][sp] - CS[3][s]) / DYF[j] - o->CIKZ[k] * CS[4][s];
+            else if (part == 1)
+              CT[s] = -o->CIKX[i] * CS[4][s] - (CS[5][sp] - CS[5][s]) / DYF[j] - o->CIKZ[k] * CS[2][s];
+            else
+              CT[s] = -o->CIKX[i] * CS[3][s] - o->CIKZ[k] * CS[5][s];
+          }
+    } else {
+      const double *Ud = part == 3 ? U[0] : U[2];
+      for (int j = 2; j <= NY; j++)
+        for (long q = 0; q < np; q++)
+          T[j * np + q] = NUT[j * np + q] * (Ud[j * np + q] - Ud[(j - 1) * np + q]) / DY[j];
+      orc_fft_xz_to_fourier(o, T, CT, 2, NY);
+      for (int j = 2; j <= NY; j++)
+        for (int k = 0; k < nkzt; k++)
+          for (int i = 0; i < nkxp; i++) {
+            const long s = SIDX(o, j, k, i);
+            CT[s] = (part == 3 ? o->CIKX[i] : o->CIKZ[k]) * CT[s];
+          }
+    }
+    orc_fft_xz_to_physical(o, CT, T, 0, NY + 1);
+    for (int j = 0; j <= NY + 1; j++) {
+      double a = 0.0;
+      for (long q = 0; q < np; q++) a += T[j * np + q] * Uf[j * np + q];
+      eps[j] += a;
+    }
+  }
+  for (int j = 0; j <= NY + 1; j++) eps[j] = eps[j] / (double)(NX * NZ);
+  o->les_stats_req = 0;
+  o->les_stats_valid = 1;
 }
 
 /* les_chan for LES_MODEL_TYPE = 1: the velocity is spectral on entry and
@@ -255,6 +315,7 @@ void orc_les_chan(orc *o) {
       o->CF2[s] = o->CF2[s] + (c == 0 ? o->CIKX[i] : o->CIKZ[k]) * o->CTEMP[s];
     }
   }
+  if (o->les_stats_req) les_means(o, J1, J2);
 #undef LOOPS
 #undef LOOPP
 #undef S_
@@ -299,5 +360,14 @@ void orc_les_scalar_terms(orc *o, int n) {
 int orc_get_nu_t(const orc *o, double *out) {
   if (!o->NU_T) return -1;
   memcpy(out, o->NU_T, sizeof(double) * o->nphys);
+  return 0;
+}
+
+void orc_les_stats_request(orc *o) { o->les_stats_req = 1; }
+
+int orc_les_stats(const orc *o, double *nu_t_mean, double *eps_sgs1_mean) {
+  if (!o->les_stats_valid) return -1;
+  memcpy(nu_t_mean, o->nu_t_mean, sizeof(double) * (o->NY + 2));
+  memcpy(eps_sgs1_mean, o->eps_sgs1_mean, sizeof(double) * (o->NY + 2));
   return 0;
 }

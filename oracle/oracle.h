@@ -142,6 +142,11 @@ void orc_stats_means_update(const orc *o, int nsamples, double *ubar, double *vb
 double orc_div_max_per(const orc *o);
 /* NU_T of the last LES substep, physical layout; -1 without LES */
 int orc_get_nu_t(const orc *o, double *out);
+/* les_chan's plane means (for/les.f:336-459): the next LES substep records
+ * NU_T_MEAN and EPS_SGS1_MEAN (rows 0..NY+1) as it does when
+ * MOD(TIME_STEP, SAVE_STATS_INT) = 0 and RK_STEP = 1. */
+void orc_les_stats_request(orc *o);
+int orc_les_stats(const orc *o, double *nu_t_mean, double *eps_sgs1_mean);
 
 #ifdef __cplusplus
 }

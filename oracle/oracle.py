@@ -109,6 +109,8 @@ def lib():
         L.orc_stats_means_update.argtypes = [P, c_i, P, P, P, P]
         L.orc_set_threads.argtypes = [c_i]
         L.orc_get_nu_t.argtypes = [P, P]
+        L.orc_les_stats_request.argtypes = [P]
+        L.orc_les_stats.argtypes = [P, P, P]
         _lib = L
     return _lib
 
@@ -183,6 +185,16 @@ class Oracle:
         if lib().orc_get_nu_t(self.h, _ptr(out)) != 0:
             raise ValueError("no LES state")
         return out
+
+    def les_stats_request(self):
+        lib().orc_les_stats_request(self.h)
+
+    def les_stats(self) -> dict:
+        """NU_T_MEAN, EPS_SGS1_MEAN (rows 0..NY+1) of the requested substep."""
+        a, b = np.zeros(self.p.ny + 2), np.zeros(self.p.ny + 2)
+        if lib().orc_les_stats(self.h, _ptr(a), _ptr(b)) != 0:
+            raise ValueError("no LES statistics recorded")
+        return {"nu_sgs": a, "eps_sgs1": b}
 
     def set_state(self, st: dict):
         for k, v in st.items():

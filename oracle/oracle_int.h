@@ -35,6 +35,8 @@ struct orc {
   /* LES (allocated when p.les): NU_T at GY points, S_ij / CS_ij, TEMP / CTEMP */
   double *NU_T, *Sij[6], *TEMP;
   cplx *CSij[6], *CTEMP;
+  int les_stats_req, les_stats_valid;
+  double *nu_t_mean, *eps_sgs1_mean;   /* [NY+2] each */
 };
 
 void orc_r2c_pair(int n, const double *a, const double *b, cplx *A, cplx *B, cplx *work);

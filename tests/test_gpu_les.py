@@ -129,3 +129,25 @@ def test_les_refusals(bad):
     p, gy = configs.kh_shear_layer(nx=64, ny=33, nz=32)
     with pytest.raises(DiabloError):
         Channel(p.replace(les=1, **bad), gy)
+
+
+def test_les_plane_means_match_oracle(tmp_path):
+    from diablo_b200 import stats_io
+    p, gy = kh_les()
+    ref, ch = start(p, gy, ics.kh_shear_layer, seed=25, kick=0.3)
+    for s in (1, 2, 3):
+        ref.step(s)
+        ch.step(s)
+    ref.les_stats_request()
+    ch.les_stats_request()
+    ref.rk_chan_1(4, 1)
+    ch.rk_chan_1(4, 1)
+    got, want = ch.les_stats(), ref.les_stats()
+    for k in ("nu_sgs", "eps_sgs1"):
+        g, w = got[k][1:-1], want[k][1:-1]
+        assert np.abs(w).max() > 0, k
+        assert np.abs(g - w).max() <= 1e-11 * np.abs(w).max() + 1e-15, k
+    path = tmp_path / "mean_les.txt"
+    stats_io.write_mean_les(str(path), got, ch.GYF, 4, 0.06, p.delta_t)
+    assert len(open(path).read().splitlines()) == 1 + 2 * p.ny
+    ch.close()

@@ -134,3 +134,25 @@ def test_les_model_types_2_and_3_refused():
     p, gy = configs.kh_shear_layer(nx=16, ny=9, nz=8)
     with pytest.raises(ValueError, match="not supported yet in MPI"):
         O.Oracle(p.replace(les=1, les_model_type=2), gy)
+
+
+def test_les_plane_means_and_mean_les_format(tmp_path):
+    from diablo_b200 import stats_io
+    p, gy, ref = les_case()
+    ref.step(1)
+    ref.les_stats_request()
+    ref.rk_chan_1(2, 1)
+    st = ref.les_stats()
+    np.testing.assert_allclose(st["nu_sgs"], ref.nu_t().mean(axis=(1, 2)), rtol=1e-13, atol=0)
+    assert np.abs(st["eps_sgs1"]).max() > 0
+    with pytest.raises(ValueError):
+        les_case()[2].les_stats()          # nothing recorded without a request
+    _gy, gyf, _dy, _dyf = ref.grid()
+    path = tmp_path / "mean_les.txt"
+    stats_io.write_mean_les(str(path), st, gyf, 2, 0.04, p.delta_t)
+    lines = open(path).read().splitlines()
+    # header, then per row "j GYF NU_T" and, by format reversion, "EPS" alone
+    assert len(lines) == 1 + 2 * p.ny
+    j, y, nu = lines[1].split()
+    assert int(j) == 1 and float(y) == pytest.approx(gyf[1]) and float(nu) == pytest.approx(st["nu_sgs"][1])
+    assert len(lines[2]) == 31 and float(lines[2]) == pytest.approx(st["eps_sgs1"][1], abs=1e-20)

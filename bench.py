@@ -272,6 +272,63 @@ def run_ensemble(args):
             "served_over_plain": served / plain}
 
 
+def step_timer(ts):
+    """ms per full step over graph-replayed steps on stream ts (CUDA events,
+    L2 not flushed), after `warm` untimed steps."""
+    import torch
+
+    def timed(solver, nsteps, warm=3):
+        solver.steps(1, warm)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ts)
+        solver.steps(warm + 1, nsteps)
+        e1.record(ts)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / nsteps
+    return timed
+
+
+def run_les_configs(ts, timed, nsteps, cpu=True, only=""):
+    """LES (constant Smagorinsky, FP64): the reference's KH_test run and the
+    Re_tau = 180 channel with the model on, each timed over nsteps
+    graph-replayed steps; the CPU oracle's time for the KH_test step beside it
+    (all host threads, 2 steps)."""
+    from diablo_b200 import configs, ics
+    from diablo_b200.solver import Channel
+    stream = ts.cuda_stream
+    out = {}
+    for name, (p, gy), maker in (("kh_les_128x65x16", configs.kh_les(), ics.kh_shear_layer),
+                                 ("channel_re180_les_128x129x128",
+                                  (configs.channel_re180()[0].replace(les=1),
+                                   configs.channel_re180()[1]), ics.channel_laminar)):
+        if only and not name.startswith(only):
+            continue
+        kw = {"kick": 0.1} if maker is ics.kh_shear_layer else {}
+        u1, u2, u3, th = maker(p, gy, seed=2, **kw)
+        ch = Channel(p, gy, stream=stream)
+        ch.create_flow(u1, u2, u3, th if p.n_th else None)
+        ch.set_time(0.0, p.delta_t)
+        ms = timed(ch, nsteps)
+        rec = {"ms_per_step": ms, "mpoint_steps_per_s": p.nx * p.ny * p.nz / ms / 1e3,
+               "nu_t_max": float(ch.nu_t().max())}
+        ch.close()
+        if cpu and name.startswith("kh_les"):
+            import oracle as O
+            ref = O.Oracle(p, gy, threads=os.cpu_count() or 1)
+            ref.create_flow_chan(u1, u2, u3, th)
+            t0 = time.perf_counter()
+            for s in (1, 2):
+                ref.step(s)
+            rec["cpu_baseline"] = {"ms_per_step": (time.perf_counter() - t0) / 2 * 1e3,
+                                   "cores": os.cpu_count() or 1, "kind": "port",
+                                   "sample": "2 steps of the same case"}
+            ref.close()
+        out[name + "_fp64"] = rec
+    return out
+
+
 def run_other_configs(args):
     """The other configurations of the workload list, each timed for a few
     graph-replayed steps (CUDA events, L2 not flushed): FP64 and mixed where
@@ -282,19 +339,7 @@ def run_other_configs(args):
 
     ts = torch.cuda.Stream()     # the solvers run on this stream; events are recorded on it
     stream = ts.cuda_stream
-
-    def timed(solver, nsteps, warm=3):
-        st = ts
-        solver.steps(1, warm)
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        solver.steps(warm + 1, nsteps)
-        e1.record(st)
-        e1.synchronize()
-        return e0.elapsed_time(e1) / nsteps
-
+    timed = step_timer(ts)
     out = {}
     # KH shear layer 128 x 65 x 32 and Re_tau = 180, FP64 and mixed
     for name, (p, gy), maker in (("kh_shear_layer_128x65x32", configs.kh_shear_layer(),
@@ -311,34 +356,7 @@ def run_other_configs(args):
             ch.close()
             out[f"{name}_{'mixed' if prec else 'fp64'}"] = {
                 "ms_per_step": ms, "mpoint_steps_per_s": p.nx * p.ny * p.nz / ms / 1e3}
-    # LES (constant Smagorinsky, FP64): the reference's KH_test run and the
-    # Re_tau = 180 channel with the model on; the CPU oracle's time for the
-    # KH_test step beside it (all host threads, 2 steps)
-    for name, (p, gy), maker in (("kh_les_128x65x16", configs.kh_les(), ics.kh_shear_layer),
-                                 ("channel_re180_les_128x129x128",
-                                  (configs.channel_re180()[0].replace(les=1),
-                                   configs.channel_re180()[1]), ics.channel_laminar)):
-        kw = {"kick": 0.1} if maker is ics.kh_shear_layer else {}
-        u1, u2, u3, th = maker(p, gy, seed=2, **kw)
-        ch = Channel(p, gy, stream=stream)
-        ch.create_flow(u1, u2, u3, th if p.n_th else None)
-        ch.set_time(0.0, p.delta_t)
-        ms = timed(ch, 50)
-        rec = {"ms_per_step": ms, "mpoint_steps_per_s": p.nx * p.ny * p.nz / ms / 1e3,
-               "nu_t_max": float(ch.nu_t().max())}
-        ch.close()
-        if name.startswith("kh_les"):
-            import oracle as O
-            ref = O.Oracle(p, gy, threads=os.cpu_count() or 1)
-            ref.create_flow_chan(u1, u2, u3, th)
-            t0 = time.perf_counter()
-            for s in (1, 2):
-                ref.step(s)
-            rec["cpu_baseline"] = {"ms_per_step": (time.perf_counter() - t0) / 2 * 1e3,
-                                   "cores": os.cpu_count() or 1, "kind": "port",
-                                   "sample": "2 steps of the same case"}
-            ref.close()
-        out[name + "_fp64"] = rec
+    out.update(run_les_configs(ts, timed, 50))
     # periodic 256^3, FP64 and mixed
     p, _ = configs.periodic_256()
     for prec in (0, 1):
@@ -612,11 +630,23 @@ def main():
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--ensemble-rate", type=float, default=20.0)
     ap.add_argument("--ensemble-active", type=int, default=16)
+    ap.add_argument("--les-only", default="", choices=["", "all", "kh_les", "channel_re180_les"],
+                    help="time only the LES workloads (all, or the one named; --steps "
+                         "graph-replayed steps each, after --warmup) and print their records; "
+                         "no contract line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.les_only:
+        import torch
+        ts = torch.cuda.Stream()
+        timed = step_timer(ts)
+        out = run_les_configs(ts, lambda ch, n: timed(ch, n, warm=args.warmup), args.steps,
+                              cpu=False, only="" if args.les_only == "all" else args.les_only)
+        print(json.dumps({"les": out}))
+        return 0
     return run_gpu(args)
 
 

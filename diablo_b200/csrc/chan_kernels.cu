@@ -1887,6 +1887,7 @@ int dg_dt_commit(dg_handle *h) {
   k_dt_commit<<<1, 1, 0, h->st>>>(h->dscal);
   DG_LAUNCHED();
   if (h->defer_tables) return DG_OK;  // the next full step rebuilds them first
+  if (h->p.les && h->les_nut) return DG_OK;  // the LES solves build their rows in place
   // the new tables are first needed by the next substep's CN solve: build them
   // on the side stream while the nonlinear terms of that substep run
   DG_CUDA(cudaEventRecord(h->ev_fork, h->st));

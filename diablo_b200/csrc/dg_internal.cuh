@@ -168,6 +168,7 @@ struct dg_handle {
   double *les_ubar;
   double2 *les_H;               // half-physical staging for LES_HF fields
   double *les_means;            // [2][NY+2]: NU_T_MEAN, EPS_SGS1_MEAN of a requested substep
+  double *les_rowtab;           // [6][NY+2] reciprocal grid factors of the LES CN rows
   bool les_stats_req, les_stats_valid;
   bool les_nut;                 // NU_T has been computed (it stays in use from then on)
 };

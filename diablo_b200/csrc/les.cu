@@ -19,20 +19,21 @@
 //          physical column builds the CN rows with the eddy-viscosity terms and
 //          the BC rows, runs the MPI Thomas sweeps and writes U / TH; COURANT on
 //          that velocity; forward transforms to CU / CTH; REM_DIV_CHAN.
-// Slots (physical): 0-5 S_ij (then R), 6-7 cross terms, 8 NU_T, 9-11 U1-U3,
-// 12.. TH(n) (U and TH adjacent: one transform batch), then 2 nf Thomas scratch (pivots b', upper diagonals c; before
-// the solve they hold the five |S| S_ij products).
+// Slots (physical): 0-5 S_ij (then R), 6-10 the |S| S_ij products, 11-12
+// cross terms (products and cross terms adjacent: one transform batch), 13
+// NU_T, 14-16 U1-U3, 17.. TH(n) (U and TH adjacent: one transform batch), then
+// nf Thomas scratch (pivots b').
 // Slots (spectral): 0-5 CS_ij (then the products, then scalar temporaries),
 // 6-7 cross terms, 8.. G(f).
 #include "dg_internal.cuh"
 
 namespace {
 
-constexpr int PS_S = 0, PS_X = 6, PS_NUT = 8, PS_U = 9, PS_TH = 12;
+constexpr int PS_S = 0, PS_P = 6, PS_X = 11, PS_NUT = 13, PS_U = 14, PS_TH = 17;
 constexpr int SS_S = 0, SS_X = 6, SS_G = 8;
 constexpr int LES_HF = 8;  // fields per transform launch (the pointer-array capacity)
 
-inline int phys_slots(const dg_handle *h) { return PS_TH + h->NTH + 2 * h->nf; }
+inline int phys_slots(const dg_handle *h) { return PS_TH + h->NTH + h->nf; }
 inline int spec_slots(const dg_handle *h) { return SS_G + h->nf; }
 inline long pfield_of(const dg_handle *h) { return (long)(h->NY + 2) * h->NZ * h->NX; }
 inline double *pslot(dg_handle *h, int s) { return h->les_phys + (long)s * pfield_of(h); }
@@ -368,6 +369,7 @@ struct LesCn {
   int bc_lo[3 + DG_MAX_TH], bc_hi[3 + DG_MAX_TH];
   double c1_lo[3 + DG_MAX_TH], c1_hi[3 + DG_MAX_TH];
   double nu, nuv, pr[DG_MAX_TH];
+  double dy2, dyn, dyf1, dyfn;  // DY(2), DY(NY), DYF(1), DYF(NY) for the Neumann BC rows
 };
 
 // Row j of field f (0 U1, 1 U2, 2 U3, 3+n TH(n)) as the reference builds it:
@@ -375,98 +377,94 @@ struct LesCn {
 // then the lower and upper BC rows (APPLY_BC_*_MPI, for/mpi.f:1137-1291 with
 // for/channel.f:1660-2241).  The right-hand side of a CN row is R plus the
 // explicit eddy-viscosity half.  um, uj, up: the field on planes j-1, j, j+1;
-// nm, nj, np1: NU_T on the same planes; r: R on plane j.
+// nm, nj, np1: NU_T on the same planes; r: R on plane j.  The grid factors
+// come as reciprocals (T, [6][L] in shared memory): 1/(DY_j DYF_j),
+// 1/(DY_j+1 DYF_j), 1/(DYF_j-1 DY_j), 1/(DYF_j DY_j), 1/DY_j, 1/DYF_j; the
+// reference divides by the products, which differs in the last bit only.
 __device__ __forceinline__ void les_row(const LesCn &P, int f, int j, double T1, double T2,
-                                        const double *dy, const double *dyf, double um, double uj,
-                                        double up, double nm_, double nj, double np1, double r,
-                                        double &l, double &d, double &u, double &v) {
+                                        const double *T, int L, double um, double uj, double up,
+                                        double nm_, double nj, double np1, double r, double &l,
+                                        double &d, double &u, double &v) {
   const int NY = P.NY;
+  const double *g0 = T, *g1 = T + L, *h0 = T + 2 * L, *h1 = T + 3 * L, *idy = T + 4 * L,
+               *idyf = T + 5 * L;
   l = 0.0, d = 1.0, u = 0.0, v = 0.0;
   if (f == 1) {
     if (j >= 2 && j <= NY) {
       const double a = T1 * P.nuv;
-      l = -a / (dyf[j - 1] * dy[j]);
-      d = 1. + a / (dyf[j] * dy[j]) + a / (dyf[j - 1] * dy[j]);
-      u = -a / (dyf[j] * dy[j]);
       const double nm = 0.5 * (nj + nm_), npl = 0.5 * (nj + np1);
-      v = r + T2 * ((npl * (up - uj) / dyf[j] - nm * (uj - um) / dyf[j - 1]) / dy[j]);
-      l = l - T2 * nm / (dyf[j - 1] * dy[j]);
-      d = d + T2 * npl / (dyf[j] * dy[j]) + T2 * nm / (dyf[j - 1] * dy[j]);
-      u = u - T2 * npl / (dyf[j] * dy[j]);
+      l = -a * h0[j] - T2 * nm * h0[j];
+      d = 1. + a * h1[j] + a * h0[j] + T2 * npl * h1[j] + T2 * nm * h0[j];
+      u = -a * h1[j] - T2 * npl * h1[j];
+      v = r + T2 * ((npl * (up - uj) * idyf[j] - nm * (uj - um) * idyf[j - 1]) * idy[j]);
     }
     // APPLY_BC_2_LOWER / _UPPER
     const int lo = P.bc_lo[1], hi = P.bc_hi[1];
     if (j == 0) { l = 0.; d = 1.; u = 0.; v = 0.; }
     if (lo == 0 && (j == 1 || j == 2)) { l = 0.; d = 1.; u = 0.; v = P.c1_lo[1]; }
-    if (lo == 1 && j == 1) { l = 0.; d = -1.; u = 1.; v = dyf[1] * P.c1_lo[1]; }
+    if (lo == 1 && j == 1) { l = 0.; d = -1.; u = 1.; v = P.dyf1 * P.c1_lo[1]; }
     if (hi == 0 && (j == NY || j == NY + 1)) { l = 0.; d = 1.; u = 0.; v = P.c1_hi[1]; }
-    if (hi == 1 && j == NY + 1) { l = -1.; d = 1.; u = 0.; v = dyf[NY] * P.c1_hi[1]; }
+    if (hi == 1 && j == NY + 1) { l = -1.; d = 1.; u = 0.; v = P.dyfn * P.c1_hi[1]; }
     return;
   }
   const bool th = f >= 3;
   const int js = th ? P.jst[f - 3] : P.JS, je = th ? P.jet[f - 3] : P.JE;
   if (j >= js && j <= je) {
-    if (th) {
-      const double a = T1 / P.pr[f - 3] * P.nuv;
-      l = -(a) / (dy[j] * dyf[j]);
-      d = 1. + (a) / (dy[j + 1] * dyf[j]) + (a) / (dy[j] * dyf[j]);
-      u = -(a) / (dy[j + 1] * dyf[j]);
-    } else {
-      l = -T1 * P.nuv / (dy[j] * dyf[j]);
-      d = 1. - T1 * P.nuv * (-1. / (dy[j + 1] * dyf[j]) - 1. / (dy[j] * dyf[j]));
-      u = -T1 * P.nuv / (dy[j + 1] * dyf[j]);
-    }
-    v = r + T2 * ((np1 * (up - uj) / dy[j + 1] - nj * (uj - um) / dy[j]) / dyf[j]);
-    l = l - T2 * nj / (dy[j] * dyf[j]);
-    d = d + T2 * np1 / (dy[j + 1] * dyf[j]) + T2 * nj / (dy[j] * dyf[j]);
-    u = u - T2 * np1 / (dy[j + 1] * dyf[j]);
+    const double a = th ? T1 / P.pr[f - 3] * P.nuv : T1 * P.nuv;
+    l = -a * g0[j] - T2 * nj * g0[j];
+    d = 1. + a * g1[j] + a * g0[j] + T2 * np1 * g1[j] + T2 * nj * g0[j];
+    u = -a * g1[j] - T2 * np1 * g1[j];
+    v = r + T2 * ((np1 * (up - uj) * idy[j + 1] - nj * (uj - um) * idy[j]) * idyf[j]);
   }
   // APPLY_BC_1/3/TH_LOWER / _UPPER
   const int lo = P.bc_lo[f], hi = P.bc_hi[f];
   if (j == 0) { l = 0.; d = 1.; u = 0.; v = 0.; }
   if (j == 1) {
     if (lo == 0) { l = 0.; d = 1.; u = 0.; v = P.c1_lo[f]; }
-    else { l = 0.; d = -1.; u = 1.; v = dy[2] * P.c1_lo[f]; }
+    else { l = 0.; d = -1.; u = 1.; v = P.dy2 * P.c1_lo[f]; }
   }
   if (j == NY + 1) { l = 0.; d = 1.; u = 0.; v = 0.; }
   if (j == NY) {
     if (hi == 0) { l = 0.; d = 1.; u = 0.; v = P.c1_hi[f]; }
-    else { l = -1.; d = 1.; u = 0.; v = dy[NY] * P.c1_hi[f]; }
+    else { l = -1.; d = 1.; u = 0.; v = P.dyn * P.c1_hi[f]; }
   }
 }
 
 // One thread per physical column of one field: rows, THOMAS_FORWARD_REAL_MPI
 // and THOMAS_BACKWARD_REAL_MPI for the only rank (for/mpi.f:630-703,767-809),
 // the solution written back over the reference's ranges.  R (slot f) holds
-// the right-hand side and then the eliminated one; B (scratch) the pivots, C
-// the upper diagonals.  Both sweeps load CB rows at a time before their
-// recurrence so the loads overlap.
+// the right-hand side and then the eliminated one, B (scratch) the reciprocal
+// pivots (0 for a zero pivot: the backward sweep then writes 0, as the
+// reference's guard does); the back substitution rebuilds each row's upper
+// diagonal from NU_T rather than storing it.  Both sweeps load CB rows at a
+// time before their recurrence so the loads overlap.
 constexpr int CB = 8;
 
 __global__ void __launch_bounds__(128) k_les_cn(LesCn P, long np, long pfield,
                                                 const double *__restrict__ dscal, int rk_step,
-                                                const double *__restrict__ dy,
-                                                const double *__restrict__ dyf,
+                                                const double *__restrict__ rowtab,
                                                 const double *__restrict__ nut,
                                                 double *__restrict__ Rbase,
                                                 double *__restrict__ Ubase,
                                                 double *__restrict__ THbase,
                                                 double *__restrict__ Bbase) {
+  extern __shared__ double tab[];
+  const int NY = P.NY, L = NY + 2;
+  for (int i = threadIdx.x; i < 6 * L; i += blockDim.x) tab[i] = rowtab[i];
+  __syncthreads();
   const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const int f = blockIdx.y;
   if (q >= np || f >= P.nf) return;
   const double h = dscal[1 + rk_step];
   const double T1 = P.nu * h / 2.0, T2 = h / 2.0;
-  const int NY = P.NY, L = NY + 2;
   double *R = Rbase + (long)f * pfield + q;
   double *U = (f < 3 ? Ubase + (long)f * pfield : THbase + (long)(f - 3) * pfield) + q;
-  double *B = Bbase + (long)f * pfield + q, *C = Bbase + (long)(P.nf + f) * pfield + q;
+  double *B = Bbase + (long)f * pfield + q;
   const double *nq = nut + q;
   double l, d, u, v;
-  les_row(P, f, 0, T1, T2, dy, dyf, 0., 0., 0., 0., 0., 0., 0., l, d, u, v);
-  double bprev = d, cprev = u, gprev = v;
-  B[0] = d;
-  C[0] = u;
+  les_row(P, f, 0, T1, T2, tab, L, 0., 0., 0., 0., 0., 0., 0., l, d, u, v);
+  double rbprev = (d != 0.0) ? 1.0 / d : 0.0, cprev = u, gprev = v, bprev = d;
+  B[0] = rbprev;
   R[0] = v;
   for (int j0 = 1; j0 < L; j0 += CB) {
     double uu[CB + 2], nn[CB + 2], rr[CB];
@@ -486,15 +484,16 @@ __global__ void __launch_bounds__(128) k_les_cn(LesCn P, long np, long pfield,
     for (int k = 0; k < CB; k++) {
       const int j = j0 + k;
       if (j < L) {
-        les_row(P, f, j, T1, T2, dy, dyf, uu[k], uu[k + 1], uu[k + 2], nn[k], nn[k + 1], nn[k + 2],
-                rr[k], l, d, u, v);
-        const double a = -l / bprev;
+        les_row(P, f, j, T1, T2, tab, L, uu[k], uu[k + 1], uu[k + 2], nn[k], nn[k + 1],
+                nn[k + 2], rr[k], l, d, u, v);
+        const double a = -l * rbprev;
         const double b = d + a * cprev;
         const double g = v + a * gprev;
+        const double rb = (b != 0.0) ? 1.0 / b : 0.0;
         const long o = (long)j * np;
-        B[o] = b;
-        C[o] = u;
+        B[o] = rb;
         R[o] = g;
+        rbprev = rb;
         bprev = b;
         cprev = u;
         gprev = g;
@@ -510,20 +509,25 @@ __global__ void __launch_bounds__(128) k_les_cn(LesCn P, long np, long pfield,
   double x = gprev / bprev;
   if (NY + 1 >= wlo && NY + 1 <= whi) U[(long)(NY + 1) * np] = x;
   for (int j1 = NY; j1 >= 0; j1 -= CB) {
-    double bb[CB], cc[CB], gg[CB];
+    double bb[CB], gg[CB], nn[CB + 2];  // nn[k]: NU_T on plane j1 + 1 - k
+#pragma unroll
+    for (int k = 0; k < CB + 2; k++) {
+      const int j = j1 + 1 - k;
+      nn[k] = (j >= 0 && j < L) ? nq[(long)j * np] : 0.0;
+    }
 #pragma unroll
     for (int k = 0; k < CB; k++) {
       const int j = j1 - k;
       const long o = (long)(j >= 0 ? j : 0) * np;
       bb[k] = B[o];
-      cc[k] = C[o];
       gg[k] = R[o];
     }
 #pragma unroll
     for (int k = 0; k < CB; k++) {
       const int j = j1 - k;
       if (j >= 0) {
-        x = (bb[k] != 0.0) ? (gg[k] - cc[k] * x) / bb[k] : 0.0;
+        les_row(P, f, j, T1, T2, tab, L, 0., 0., 0., nn[k + 2], nn[k + 1], nn[k], 0., l, d, u, v);
+        x = (gg[k] - u * x) * bb[k];
         if (j >= wlo && j <= whi) U[(long)j * np] = x;
       }
     }
@@ -574,11 +578,31 @@ int dg_les_init(dg_handle *h) {
     t[j] = -2.0 * cs * cs * pow(dx * beta_sgs * h->h_dyf[j] * 2.0 * dz * beta_sgs, 2.0 / 3.0);
     t[NY + 2 + j] = -2.0 * cs * cs * pow(dx * beta_sgs * h->h_dy[j] * 2.0 * dz * beta_sgs, 2.0 / 3.0);
   }
+  // reciprocal grid factors of the CN rows, planes 0..NY+1 (zero where a
+  // factor would reach outside the grid; those rows are BC or identity rows)
+  const int L = NY + 2;
+  double *rt = (double *)calloc(6 * L, sizeof(double));
+  const double *DY = h->h_dy, *DYF = h->h_dyf;
+  for (int j = 1; j <= NY; j++) {
+    rt[j] = 1.0 / (DY[j] * DYF[j]);
+    rt[L + j] = 1.0 / (DY[j + 1] * DYF[j]);
+    if (j >= 2) rt[2 * L + j] = 1.0 / (DYF[j - 1] * DY[j]);
+    rt[3 * L + j] = 1.0 / (DYF[j] * DY[j]);
+  }
+  for (int j = 1; j <= NY + 1; j++) {
+    rt[4 * L + j] = 1.0 / DY[j];
+    rt[5 * L + j] = 1.0 / DYF[j];
+  }
+  DG_CUDA(dg_malloc(h, (void **)&h->les_rowtab, sizeof(double) * 6 * L));
   cudaError_t e = cudaMemcpyAsync(h->les_dfac, t, sizeof(double) * 2 * (NY + 2),
                                   cudaMemcpyHostToDevice, h->st);
+  cudaError_t e1 = cudaMemcpyAsync(h->les_rowtab, rt, sizeof(double) * 6 * L,
+                                   cudaMemcpyHostToDevice, h->st);
   cudaError_t e2 = cudaStreamSynchronize(h->st);
   free(t);
+  free(rt);
   DG_CUDA(e);
+  DG_CUDA(e1);
   DG_CUDA(e2);
   h->les_nut = false;
   return DG_OK;
@@ -614,8 +638,7 @@ int dg_les_pre(dg_handle *h, int rk_step) {
   dg_kt_begin(h, "k_les_bc_phys", h->st);
   k_les_bc_phys<<<dg_cdiv(np, 256), 256, 0, h->st>>>(B, NY, np, pf, h->dy, h->dyf, pslot(h, PS_U));
   DG_LAUNCHED();
-  // the products go to the Thomas scratch slots (free until the solve)
-  double *prod = pslot(h, PS_TH + h->NTH);
+  double *prod = pslot(h, PS_P);
   dg_kt_begin(h, "k_les_model", h->st);
   k_les_model<<<dg_cdiv((long)(NY + 2) * np, 256), 256, 0, h->st>>>(
       NY, np, pf, h->jstart, h->jend, h->dy, h->dyf, h->les_dfac, h->les_ubar, pslot(h, PS_S),
@@ -623,11 +646,11 @@ int dg_les_pre(dg_handle *h, int rk_step) {
   DG_LAUNCHED();
   h->les_nut = true;
   // |S| S_ij (S_22 excluded) and the cross terms to Fourier space
-  double2 *op[5] = {sslot(h, SS_S), sslot(h, SS_S + 2), sslot(h, SS_S + 3), sslot(h, SS_S + 4),
-                    sslot(h, SS_S + 5)};
-  DG_TRY(to_fourier(h, prod, 5, 0, NY + 1, op));
-  double2 *ox[2] = {sslot(h, SS_X), sslot(h, SS_X + 1)};
-  DG_TRY(to_fourier(h, pslot(h, PS_X), 2, 2, NY, ox));
+  // (the cross-term slots are zero outside planes 2..NY, which is all the
+  // forcing reads of them)
+  double2 *op[7] = {sslot(h, SS_S),     sslot(h, SS_S + 2), sslot(h, SS_S + 3), sslot(h, SS_S + 4),
+                    sslot(h, SS_S + 5), sslot(h, SS_X),     sslot(h, SS_X + 1)};
+  DG_TRY(to_fourier(h, prod, 7, 0, NY + 1, op));
   dg_kt_begin(h, "k_les_force", h->st);
   k_les_force<<<dg_cdiv((long)(NY + 2) * ss, 256), 256, 0, h->st>>>(
       NY, ss, h->nkxp, h->jstart, h->kx, h->kz, h->dyf, h->les_dfac, sslot(h, SS_S), ns,
@@ -731,9 +754,16 @@ int dg_les_post(dg_handle *h, int time_step, int rk_step, bool sgs) {
     P.c1_lo[3 + n] = p.th_bc_ymin_c1[n];
     P.c1_hi[3 + n] = p.th_bc_ymax_c1[n];
   }
+  P.dy2 = h->h_dy[2];
+  P.dyn = h->h_dy[NY];
+  P.dyf1 = h->h_dyf[1];
+  P.dyfn = h->h_dyf[NY];
+  const size_t tsm = sizeof(double) * 6 * (NY + 2);
+  if (tsm > 48 * 1024)
+    DG_CUDA(cudaFuncSetAttribute(k_les_cn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
   dg_kt_begin(h, "k_les_cn", h->st);
-  k_les_cn<<<dim3(dg_cdiv(np, 128), h->nf), 128, 0, h->st>>>(
-      P, np, pf, h->dscal, rk_step, h->dy, h->dyf, pslot(h, PS_NUT), pslot(h, PS_S),
+  k_les_cn<<<dim3(dg_cdiv(np, 128), h->nf), 128, tsm, h->st>>>(
+      P, np, pf, h->dscal, rk_step, h->les_rowtab, pslot(h, PS_NUT), pslot(h, PS_S),
       pslot(h, PS_U), pslot(h, PS_TH), pslot(h, PS_TH + h->NTH));
   DG_LAUNCHED();
   // COURANT on the solved velocity (for/channel.f:1037-1040)

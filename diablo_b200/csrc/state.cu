@@ -404,6 +404,7 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
   dg_free(h, h->les_ubar);
   dg_free(h, h->les_H);
   dg_free(h, h->les_means);
+  dg_free(h, h->les_rowtab);
   for (int f = 0; f < 3 + DG_MAX_TH; f++) {
     dg_free(h, h->cu[f]);
     dg_free(h, h->cf[f]);

@@ -23,7 +23,7 @@ int step_body(dg_handle *h, int time_step) {
     for (int rk = 1; rk <= 3; rk++) DG_TRY(diablo_rk_per_1(h, rk));
     return diablo_advance_time(h);
   }
-  if (h->p.variable_dt) {
+  if (h->p.variable_dt && !(h->p.les && h->les_nut)) {
     DG_CUDA(cudaEventRecord(h->ev_fork, h->st));
     DG_CUDA(cudaStreamWaitEvent(h->st2, h->ev_fork, 0));
     cudaStream_t keep = h->st;

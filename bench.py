@@ -549,22 +549,22 @@ def run_gpu(args):
         for n in names:
             _lib.check("diablo_get_field", L.diablo_get_field(
                 ch.h, _lib.field_id(n), ctypes.c_void_p(host[n].data_ptr()),
-                _lib.DG_LAYOUT_REFERENCE, _lib.DG_HOST))
+                _lib.DG_LAYOUT_REFERENCE_RETAINED, _lib.DG_HOST))
     ch.synchronize()
     e2e_value, e2e_t = replica_throughput(dist, ws, time.perf_counter() - t0, pts, e2e_steps)
-    # bytes that cross the bus: set_field copies the retained block of each
-    # reference array (kx 0..NKX, packed kz 0..TNKZ, all planes), get_field
-    # writes the whole reference array (the retained block and its zeros)
+    # bytes that cross the bus: set_field and get_field copy the retained
+    # block of each reference array (kx 0..NKX, packed kz 0..TNKZ, all
+    # planes), one strided copy each way
     retained = (p.ny + 2) * (2 * (p.nz // 3) + 1) * (p.nx // 3 + 1)
     h2d_bytes = len(names) * retained * 16
-    d2h_bytes = len(names) * int(np.prod(refshape)) * 16
+    d2h_bytes = len(names) * retained * 16
     e2e = {"value": e2e_value, "unit": UNIT,
            "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
            "steps": e2e_steps,
            "what": "per step: H2D of CU1..3 and CP from reference-layout pinned host arrays "
                    "(diablo_set_field: the retained block, one strided copy each), one diablo_step "
-                   "(3 RK_CHAN_1 substeps + TIME update), D2H of the same fields in the reference "
-                   "layout (diablo_get_field)"}
+                   "(3 RK_CHAN_1 substeps + TIME update), D2H of the same fields' retained block "
+                   "into the reference-layout arrays (diablo_get_field, REFERENCE_RETAINED)"}
 
     # physical sanity of the timed run
     st = ch.stats()

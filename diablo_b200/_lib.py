@@ -20,7 +20,7 @@ DG_OK = 0
 ERRORS = {1: "DG_ERR_ARG", 2: "DG_ERR_DIMS", 3: "DG_ERR_OOM", 4: "DG_ERR_CUDA", 5: "DG_ERR_NAN",
           6: "DG_ERR_TIMEOUT", 7: "DG_ERR_NODEV"}
 DG_HOST, DG_DEVICE = 0, 1
-DG_LAYOUT_COMPACT, DG_LAYOUT_REFERENCE = 0, 1
+DG_LAYOUT_COMPACT, DG_LAYOUT_REFERENCE, DG_LAYOUT_REFERENCE_RETAINED = 0, 1, 2
 # rows of diablo_save_stats_chan's profiles (DG_PR_* and DG_PRT_* in the header)
 PROFILES = ("ume", "vme", "wme", "urms", "vrms", "wrms", "uv", "uw", "wv", "dudy", "dwdy", "cp",
             "shear", "omega_x", "omega_y", "omega_z", "epsilon")

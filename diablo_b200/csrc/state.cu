@@ -505,6 +505,9 @@ extern "C" int diablo_set_field(dg_handle *h, int field, const double *src, int 
   double2 *dst = field_ptr(h, field);
   if (!dst) return DG_ERR_ARG;
   const size_t nc = (size_t)h->nspec;
+  if (layout != DG_LAYOUT_COMPACT && layout != DG_LAYOUT_REFERENCE &&
+      layout != DG_LAYOUT_REFERENCE_RETAINED)
+    return DG_ERR_ARG;
   if (layout == DG_LAYOUT_COMPACT) {
     DG_CUDA(cudaMemcpyAsync(dst, src, nc * sizeof(double2),
                             where == DG_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
@@ -535,7 +538,18 @@ extern "C" int diablo_get_field(dg_handle *h, int field, double *dst, int layout
     DG_CUDA(cudaMemcpyAsync(dst, src, nc * sizeof(double2),
                             where == DG_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
                             h->st));
-  } else {
+  } else if (layout == DG_LAYOUT_REFERENCE_RETAINED) {
+    // the compact array into the retained block of the reference array: one
+    // strided copy, the caller's other entries untouched
+    int nxp1, nz2;
+    ref_dims(h, &nxp1, &nz2);
+    cudaMemcpy3DParms prm = {};
+    prm.srcPtr = make_cudaPitchedPtr(src, sizeof(double2) * h->nkxp, h->nkxp, h->nkzt);
+    prm.dstPtr = make_cudaPitchedPtr(dst, sizeof(double2) * nxp1, nxp1, nz2);
+    prm.extent = make_cudaExtent(sizeof(double2) * h->nkxp, h->nkzt, h->nplanes);
+    prm.kind = where == DG_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    DG_CUDA(cudaMemcpy3DAsync(&prm, h->st));
+  } else if (layout == DG_LAYOUT_REFERENCE) {
     int nxp1, nz2;
     ref_dims(h, &nxp1, &nz2);
     const size_t nr = (size_t)h->nplanes * nz2 * nxp1;
@@ -552,6 +566,8 @@ extern "C" int diablo_get_field(dg_handle *h, int field, double *dst, int layout
       DG_CUDA(cudaMemcpyAsync(dst, tmp, nr * sizeof(double2), cudaMemcpyDeviceToHost, h->st));
       DG_CUDA(cudaFreeAsync(tmp, h->st));
     }
+  } else {
+    return DG_ERR_ARG;
   }
   DG_CUDA(cudaStreamSynchronize(h->st));
   return DG_OK;

@@ -103,21 +103,29 @@ class _Solver:
         self._call("diablo_step", time_step, nsteps)
 
     # ---- state I/O
+    _LAYOUTS = {"compact": _lib.DG_LAYOUT_COMPACT, "reference": _lib.DG_LAYOUT_REFERENCE,
+                "reference_retained": _lib.DG_LAYOUT_REFERENCE_RETAINED}
+
     def set_field(self, name: str, arr: np.ndarray, layout: str = "compact"):
         a = np.ascontiguousarray(arr, dtype=np.complex128)
-        lay = _lib.DG_LAYOUT_REFERENCE if layout == "reference" else _lib.DG_LAYOUT_COMPACT
+        lay = self._LAYOUTS[layout]
         if lay == _lib.DG_LAYOUT_COMPACT and a.size != int(np.prod(self.spec_shape)):
             raise ValueError(f"{name}: expected {self.spec_shape}, got {a.shape}")
         self._call("diablo_set_field", _lib.field_id(name), _ptr(a), lay, _lib.DG_HOST)
 
-    def get_field(self, name: str, layout: str = "compact") -> np.ndarray:
-        if layout == "reference":
-            shp = (self.spec_shape[0], self.p.nz + 2, self.p.nx // 2 + 1)
-            lay = _lib.DG_LAYOUT_REFERENCE
-        else:
+    def get_field(self, name: str, layout: str = "compact", out: np.ndarray | None = None):
+        """A spectral field in the compact or the reference layout.  With
+        "reference_retained" only the retained block of `out` is written (the
+        rest keeps its contents; a new array starts at zero)."""
+        lay = self._LAYOUTS[layout]
+        if lay == _lib.DG_LAYOUT_COMPACT:
             shp = self.spec_shape
-            lay = _lib.DG_LAYOUT_COMPACT
-        out = np.zeros(shp, dtype=np.complex128)
+        else:
+            shp = (self.spec_shape[0], self.p.nz + 2, self.p.nx // 2 + 1)
+        if out is None:
+            out = np.zeros(shp, dtype=np.complex128)
+        elif out.shape != shp or out.dtype != np.complex128 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"{name}: out must be a contiguous complex128 array of {shp}")
         self._call("diablo_get_field", _lib.field_id(name), _ptr(out), lay, _lib.DG_HOST)
         return out
 

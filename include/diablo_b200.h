@@ -20,6 +20,13 @@
  *   COMPACT   : retained modes only, [NY+2][TNKZ+1][NKX+1] complex (channel)
  *               or [TNKY+1][TNKZ+1][NKX+1] (periodic); physical [NY+2][NZ][NX]
  *               or [NY][NZ][NX].
+ *   REFERENCE_RETAINED : the reference's spectral array, of which only the
+ *               retained block (kx 0..NKX, kz slots 0..TNKZ, every plane) is
+ *               read or written; diablo_get_field leaves the other entries of
+ *               the caller's array as they were.  This is the part the
+ *               reference's host consumers read (SAVE_FLOW writes
+ *               CU(0:NKX,0:TNKZ,*), for/diablo_io.f:367-391; the statistics
+ *               read retained modes), and only it crosses the bus.
  * Complex values are interleaved (re, im) doubles.
  */
 #ifndef DIABLO_B200_H
@@ -45,7 +52,7 @@ enum dg_status {
 };
 
 enum { DG_HOST = 0, DG_DEVICE = 1 };
-enum { DG_LAYOUT_COMPACT = 0, DG_LAYOUT_REFERENCE = 1 };
+enum { DG_LAYOUT_COMPACT = 0, DG_LAYOUT_REFERENCE = 1, DG_LAYOUT_REFERENCE_RETAINED = 2 };
 
 /* field ids for diablo_set_field / diablo_get_field */
 enum {

@@ -383,4 +383,13 @@ def test_reference_layout_round_trip(periodic):
     want = np.zeros_like(ref)
     want[:, :nkzt, :nkxp] = ref[:, :nkzt, :nkxp]
     assert np.array_equal(back, want)
+    # retained-only read: the block is written, every other entry keeps its value
+    assert np.array_equal(s.get_field("CU2", layout="reference_retained"), want)
+    keep = np.full(ref.shape, 7.0 - 3.0j)
+    s.get_field("CU2", layout="reference_retained", out=keep)
+    assert np.array_equal(keep[:, :nkzt, :nkxp], ref[:, :nkzt, :nkxp])
+    keep[:, :nkzt, :nkxp] = 7.0 - 3.0j
+    assert np.all(keep == 7.0 - 3.0j)
+    s.set_field("CU3", ref, layout="reference_retained")
+    assert np.array_equal(s.get_field("CU3"), ref[:, :nkzt, :nkxp])
     s.close()

@@ -13,7 +13,8 @@ update.  Metric: Mpoint-steps/s = NX*NY*NZ per RK3 step.
                                                         RK_CHAN_1 on host cores
 
 Under torchrun (N > 1) every rank advances its own independent replica (the
-single case is not sharded); value = all ranks' point-steps / max-over-ranks
+single case is not sharded), and the served ensemble deals whole cases out to
+the ranks; value = all ranks' point-steps / max-over-ranks
 time.
 """
 from __future__ import annotations
@@ -197,17 +198,19 @@ def cpu_baseline(p, gy, seconds=15.0, threads=None):
                       f"{threads} OpenMP threads, {dt:.1f} s)"}
 
 
-def run_ensemble(args):
+def run_ensemble(args, dist=None, ws=1, rank=0):
     """The served-ensemble workload: KH cases with NX in {64,128,256}, NZ in
     {16,32,64}, NY in {33,65,129} (uniform on [-10,10]), Re ~ U[500,5000],
     Ri ~ U[0.05,0.25], seeded 1e-3 noise, Poisson arrivals at `rate`/s, each
     run for `steps` RK3 steps in mixed precision under a 150 GB budget through
     the continuous-batching server.  Beside it, the plain per-case FP64 path
-    (one case at a time, graph-replayed steps) on a sample of the same cases."""
+    (one case at a time, graph-replayed steps) on a sample of the same cases.
+    Under torchrun every rank serves the cases the host-side dispatcher gives
+    it (whole cases, no data exchanged) and the ranks pool their statistics."""
     import torch
     from diablo_b200 import configs, ics
     from diablo_b200.grid import uniform_grid
-    from diablo_b200.serve import Server
+    from diablo_b200.serve import Server, assign_cases, merge_rank_stats
     from diablo_b200.solver import Channel
     rng = np.random.default_rng(5)
     base, _ = configs.kh_shear_layer()
@@ -216,11 +219,13 @@ def run_ensemble(args):
         q = ics.ensemble_kh_params(rng, base)
         cases.append((q, uniform_grid(q.ny, -10.0, 10.0)))
     arrivals = np.cumsum(rng.exponential(1.0 / args.ensemble_rate, len(cases)))
+    mine = [i for i, r in enumerate(assign_cases(
+        [q.nx * q.ny * q.nz * args.ensemble_steps for q, _ in cases], ws)) if r == rank]
     # plain per-case FP64 path on a sample: device time of each case alone
     sample = cases[: min(16, len(cases))]
     plain_pts, plain_s = 0.0, 0.0
     psteps = min(args.ensemble_steps, 100)
-    for i, (q, gy) in enumerate(sample):
+    for i, (q, gy) in enumerate(sample if rank == 0 else []):
         st = torch.cuda.Stream()
         ch = Channel(q, gy, stream=st.cuda_stream)
         for k, v in ics.kh_state(q, gy, seed=100 + i).items():
@@ -239,12 +244,16 @@ def run_ensemble(args):
         plain_s += e0.elapsed_time(e1) * 1e-3
         plain_pts += q.nx * q.ny * q.nz * psteps
         ch.close()
-    plain = plain_pts / plain_s / 1e6
-    # served, mixed precision, continuous batching
+    plain = plain_pts / plain_s / 1e6 if plain_s > 0 else None
+    # served, mixed precision, continuous batching; every rank starts its
+    # clock together so the shared arrival process lines up across ranks
+    if dist:
+        dist.barrier()
     srv = Server(max_active=args.ensemble_active, budget_gb=150.0, autotune=True)
     t0 = time.perf_counter()
     ids = []
-    for i, (q, gy) in enumerate(cases):
+    for i in mine:
+        q, gy = cases[i]
         st0 = ics.kh_state(q, gy, seed=100 + i)
         delay = t0 + arrivals[i] - time.perf_counter()
         if delay > 0:
@@ -257,19 +266,34 @@ def run_ensemble(args):
     wall = time.perf_counter() - t0
     s = srv.stats()
     srv.close()
-    pts = sum(q.nx * q.ny * q.nz for q, _ in cases) * args.ensemble_steps
-    served = pts / s["wall_s"] / 1e6
-    return {"cases": len(cases), "steps_per_case": args.ensemble_steps,
-            "arrival_rate_per_s": args.ensemble_rate, "max_active": args.ensemble_active,
-            "precision": "mixed (FP32 transforms and products, FP64 solves)",
-            "cases_per_s": s["cases_per_s"], "step_ms_p50": s["step_ms_p50"],
-            "step_ms_p99": s["step_ms_p99"], "mpoint_steps_per_s": served,
-            "case_latency_s_p50": float(np.percentile(lat, 50)),
-            "case_latency_s_p99": float(np.percentile(lat, 99)),
-            "hbm_peak_gb": s["bytes_peak"] / 1e9, "wall_s": wall,
-            "plain_fp64_mpoint_steps_per_s": plain,
-            "plain_sample": f"{len(sample)} of the cases alone, {psteps} steps each, FP64",
-            "served_over_plain": served / plain}
+    rec = {"wall_s": s["wall_s"] if mine else 0.0, "cases": len(mine),
+           "points": sum(cases[i][0].nx * cases[i][0].ny * cases[i][0].nz for i in mine)
+           * args.ensemble_steps,
+           "case_latency_s": lat, "step_ms_p50": s["step_ms_p50"], "step_ms_p99": s["step_ms_p99"],
+           "hbm_peak_gb": s["bytes_peak"] / 1e9}
+    if dist:
+        allrec = [None] * ws
+        dist.all_gather_object(allrec, rec)
+    else:
+        allrec = [rec]
+    m = merge_rank_stats(allrec)
+    out = {"cases": len(cases), "steps_per_case": args.ensemble_steps,
+           "arrival_rate_per_s": args.ensemble_rate, "max_active": args.ensemble_active,
+           "gpus": ws, "dispatch": "whole cases per GPU, longest first to the least-loaded GPU",
+           "precision": "mixed (FP32 transforms and products, FP64 solves)",
+           "cases_per_s": m["cases_per_s"], "step_ms_p50": m["step_ms_p50_worst_rank"],
+           "step_ms_p99": m["step_ms_p99_worst_rank"],
+           "mpoint_steps_per_s": m["mpoint_steps_per_s"],
+           "case_latency_s_p50": m["case_latency_s_p50"],
+           "case_latency_s_p99": m["case_latency_s_p99"],
+           "hbm_peak_gb": m["hbm_peak_gb_max"], "wall_s": wall,
+           "plain_fp64_mpoint_steps_per_s": plain,
+           "plain_sample": f"{len(sample)} of the cases alone on one GPU, {psteps} steps each, FP64"}
+    if plain and ws == 1:
+        out["served_over_plain"] = m["mpoint_steps_per_s"] / plain
+    elif plain:
+        out["served_per_gpu_over_plain"] = m["mpoint_steps_per_s"] / ws / plain
+    return out
 
 
 def step_timer(ts):
@@ -569,6 +593,7 @@ def run_gpu(args):
     # physical sanity of the timed run
     st = ch.stats()
     ch.close()
+    ens = run_ensemble(args, dist, ws, rank) if args.ensemble_cases > 0 else None
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -601,7 +626,6 @@ def run_gpu(args):
                  "scope": "whole RK3 step: algorithmic bytes (17 Nf + 6) x 16 B x M per step "
                           f"= {bstep / 1e6:.1f} MB over the device time of one step"}
     cpu = cpu_baseline(p, gy, seconds=args.cpu_seconds) if args.cpu_seconds > 0 else None
-    ens = run_ensemble(args) if args.ensemble_cases > 0 else None
     others = run_other_configs(args) if args.other_configs else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,

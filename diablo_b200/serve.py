@@ -81,3 +81,46 @@ class Server:
 
     def __exit__(self, *a):
         self.close()
+
+
+# ------------------------------------------------------------ several GPUs
+# The ensemble shards as independent units: every case runs whole on one GPU
+# (one server per GPU, one process per GPU), so no data crosses between GPUs
+# and there is no collective on the data path.  A host-side dispatcher
+# assigns the cases; the ranks exchange only their statistics at the end.
+
+def assign_cases(work, world: int):
+    """Rank of each case: longest-processing-time first, each case to the
+    least-loaded rank so far (ties to the lower rank).  `work` is any
+    per-case cost, e.g. points x steps.  Deterministic, so every rank
+    computes the same assignment without communicating."""
+    work = [float(w) for w in work]
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(work)), key=lambda i: (-work[i], i))
+    load = [0.0] * world
+    rank_of = [0] * len(work)
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        rank_of[i] = r
+        load[r] += work[i]
+    return rank_of
+
+
+def merge_rank_stats(per_rank):
+    """Whole-job ensemble figures from each rank's record: points and cases
+    summed, divided by the slowest rank's wall time (the job lasts as long
+    as its slowest GPU); case latencies pooled for exact percentiles; step
+    latency percentiles as the worst rank's (the servers keep no samples)."""
+    wall = max(r["wall_s"] for r in per_rank)
+    pts = sum(r["points"] for r in per_rank)
+    cases = sum(r["cases"] for r in per_rank)
+    lat = [x for r in per_rank for x in r["case_latency_s"]]
+    return {"ranks": len(per_rank), "cases": cases, "wall_s": wall,
+            "cases_per_s": cases / wall if wall > 0 else 0.0,
+            "mpoint_steps_per_s": pts / wall / 1e6 if wall > 0 else 0.0,
+            "step_ms_p50_worst_rank": max(r["step_ms_p50"] for r in per_rank),
+            "step_ms_p99_worst_rank": max(r["step_ms_p99"] for r in per_rank),
+            "case_latency_s_p50": float(np.percentile(lat, 50)) if lat else 0.0,
+            "case_latency_s_p99": float(np.percentile(lat, 99)) if lat else 0.0,
+            "hbm_peak_gb_max": max(r["hbm_peak_gb"] for r in per_rank)}

@@ -143,10 +143,6 @@ static int validate(const dg_params *p, const double *gy) {
                      "reproduce");
         return DG_ERR_ARG;
       }
-      if (p->precision != 0) {
-        dg_set_error("LES runs in FP64 (precision 0)");
-        return DG_ERR_ARG;
-      }
     }
     if (p->precision != 0 && p->precision != 1) {
       dg_set_error("precision must be 0 (FP64) or 1 (mixed)");

@@ -563,17 +563,15 @@ def run_gpu(args):
     e2e_steps = max(3, min(args.steps, 10))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    ids = (ctypes.c_int * len(names))(*[_lib.field_id(n) for n in names])
+    ptrs = (ctypes.c_void_p * len(names))(*[host[n].data_ptr() for n in names])
     for _ in range(e2e_steps):
-        for n in names:
-            _lib.check("diablo_set_field", L.diablo_set_field(
-                ch.h, _lib.field_id(n), ctypes.c_void_p(host[n].data_ptr()),
-                _lib.DG_LAYOUT_REFERENCE, _lib.DG_HOST))
+        _lib.check("diablo_set_fields", L.diablo_set_fields(
+            ch.h, len(names), ids, ptrs, _lib.DG_LAYOUT_REFERENCE_RETAINED, _lib.DG_HOST))
         ts += 1
         one_step(ts)
-        for n in names:
-            _lib.check("diablo_get_field", L.diablo_get_field(
-                ch.h, _lib.field_id(n), ctypes.c_void_p(host[n].data_ptr()),
-                _lib.DG_LAYOUT_REFERENCE_RETAINED, _lib.DG_HOST))
+        _lib.check("diablo_get_fields", L.diablo_get_fields(
+            ch.h, len(names), ids, ptrs, _lib.DG_LAYOUT_REFERENCE_RETAINED, _lib.DG_HOST))
     ch.synchronize()
     e2e_value, e2e_t = replica_throughput(dist, ws, time.perf_counter() - t0, pts, e2e_steps)
     # bytes that cross the bus: set_field and get_field copy the retained
@@ -586,9 +584,10 @@ def run_gpu(args):
            "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
            "steps": e2e_steps,
            "what": "per step: H2D of CU1..3 and CP from reference-layout pinned host arrays "
-                   "(diablo_set_field: the retained block, one strided copy each), one diablo_step "
-                   "(3 RK_CHAN_1 substeps + TIME update), D2H of the same fields' retained block "
-                   "into the reference-layout arrays (diablo_get_field, REFERENCE_RETAINED)"}
+                   "(diablo_set_fields: the retained block, one strided copy each, on two "
+                   "streams), one diablo_step (3 RK_CHAN_1 substeps + TIME update), D2H of the "
+                   "same fields' retained block into the reference-layout arrays "
+                   "(diablo_get_fields, REFERENCE_RETAINED)"}
 
     # physical sanity of the timed run
     st = ch.stats()

@@ -569,6 +569,66 @@ extern "C" int diablo_get_field(dg_handle *h, int field, double *dst, int layout
   return DG_OK;
 }
 
+// One strided or contiguous copy between a field and a caller's array on
+// stream st, no synchronisation (the layouts that need no staging kernel).
+static int copy_field_async(dg_handle *h, double2 *dev, double *arr, int layout, int where,
+                            bool to_device, cudaStream_t st) {
+  const size_t nc = (size_t)h->nspec;
+  if (layout == DG_LAYOUT_COMPACT) {
+    const cudaMemcpyKind k = where == DG_HOST
+                                 ? (to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost)
+                                 : cudaMemcpyDeviceToDevice;
+    DG_CUDA(to_device ? cudaMemcpyAsync(dev, arr, nc * sizeof(double2), k, st)
+                      : cudaMemcpyAsync(arr, dev, nc * sizeof(double2), k, st));
+    return DG_OK;
+  }
+  int nxp1, nz2;
+  ref_dims(h, &nxp1, &nz2);
+  cudaMemcpy3DParms prm = {};
+  cudaPitchedPtr a = make_cudaPitchedPtr(arr, sizeof(double2) * nxp1, nxp1, nz2);
+  cudaPitchedPtr d = make_cudaPitchedPtr(dev, sizeof(double2) * h->nkxp, h->nkxp, h->nkzt);
+  prm.srcPtr = to_device ? a : d;
+  prm.dstPtr = to_device ? d : a;
+  prm.extent = make_cudaExtent(sizeof(double2) * h->nkxp, h->nkzt, h->nplanes);
+  prm.kind = where == DG_HOST ? (to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost)
+                              : cudaMemcpyDeviceToDevice;
+  DG_CUDA(cudaMemcpy3DAsync(&prm, st));
+  return DG_OK;
+}
+
+// Several fields in one call: the copies alternate between the handle's two
+// streams (two copy engines work at once) and the call synchronises once.
+static int copy_fields(dg_handle *h, int n, const int *fields, double *const *arrs, int layout,
+                       int where, bool to_device) {
+  if (!h || n < 0 || (n > 0 && (!fields || !arrs))) return DG_ERR_ARG;
+  if (layout != DG_LAYOUT_COMPACT && layout != DG_LAYOUT_REFERENCE_RETAINED &&
+      !(to_device && layout == DG_LAYOUT_REFERENCE))
+    return DG_ERR_ARG;
+  for (int i = 0; i < n; i++)
+    if (!arrs[i] || !field_ptr(h, fields[i])) return DG_ERR_ARG;
+  // the side stream starts after the work queued so far on the main stream
+  DG_CUDA(cudaEventRecord(h->ev_fork, h->st));
+  DG_CUDA(cudaStreamWaitEvent(h->st2, h->ev_fork, 0));
+  for (int i = 0; i < n; i++)
+    DG_TRY(copy_field_async(h, field_ptr(h, fields[i]), arrs[i], layout, where, to_device,
+                            (i & 1) ? h->st2 : h->st));
+  DG_CUDA(cudaEventRecord(h->ev_join, h->st2));
+  DG_CUDA(cudaStreamWaitEvent(h->st, h->ev_join, 0));
+  h->tables_pending = false;  // anything pending on the side stream is joined now
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  return DG_OK;
+}
+
+extern "C" int diablo_set_fields(dg_handle *h, int n, const int *fields, const double *const *src,
+                                 int layout, int where) {
+  return copy_fields(h, n, fields, const_cast<double *const *>(src), layout, where, true);
+}
+
+extern "C" int diablo_get_fields(dg_handle *h, int n, const int *fields, double *const *dst,
+                                 int layout, int where) {
+  return copy_fields(h, n, fields, dst, layout, where, false);
+}
+
 extern "C" int diablo_stats(dg_handle *h, dg_stats *s) {
   if (!h || !s) return DG_ERR_ARG;
   DG_TRY(check_async_flag(h));

@@ -129,6 +129,29 @@ class _Solver:
         self._call("diablo_get_field", _lib.field_id(name), _ptr(out), lay, _lib.DG_HOST)
         return out
 
+    def set_fields(self, arrays: dict, layout: str = "compact"):
+        """Several fields in one call (diablo_set_fields: two copy streams, one
+        synchronisation)."""
+        names = list(arrays)
+        lay = self._LAYOUTS[layout]
+        arrs = [np.ascontiguousarray(arrays[n], dtype=np.complex128) for n in names]
+        ids = (ctypes.c_int * len(names))(*[_lib.field_id(n) for n in names])
+        ptrs = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+        self._call("diablo_set_fields", len(names), ids, ptrs, lay, _lib.DG_HOST)
+
+    def get_fields(self, out: dict, layout: str = "compact"):
+        """Fill the arrays of `out` (name -> contiguous complex128 array of the
+        layout's shape) in one call (diablo_get_fields)."""
+        names = list(out)
+        for n in names:
+            a = out[n]
+            if a.dtype != np.complex128 or not a.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"{n}: out arrays must be contiguous complex128")
+        ids = (ctypes.c_int * len(names))(*[_lib.field_id(n) for n in names])
+        ptrs = (ctypes.c_void_p * len(names))(*[out[n].ctypes.data for n in names])
+        self._call("diablo_get_fields", len(names), ids, ptrs, self._LAYOUTS[layout], _lib.DG_HOST)
+        return out
+
     def set_field_device(self, name: str, dev_ptr: int):
         """Copy a compact-layout complex128 field from device memory."""
         self._call("diablo_set_field", _lib.field_id(name), ctypes.c_void_p(dev_ptr),

@@ -124,6 +124,14 @@ int diablo_advance_time(dg_handle *h);
 /* Host <-> device copies of one spectral field (ids above). */
 int diablo_set_field(dg_handle *h, int field, const double *src, int layout, int where);
 int diablo_get_field(dg_handle *h, int field, double *dst, int layout, int where);
+/* The same for n fields at once (fields[i] <-> arrays[i]); the copies run on
+ * two streams and the call synchronises once.  Layouts COMPACT and
+ * REFERENCE_RETAINED (and REFERENCE for set, which reads only the retained
+ * block anyway). */
+int diablo_set_fields(dg_handle *h, int n, const int *fields, const double *const *src,
+                      int layout, int where);
+int diablo_get_fields(dg_handle *h, int n, const int *fields, double *const *dst, int layout,
+                      int where);
 
 /* ------------------------------------------------------- channel hot path */
 /* SUBROUTINE RK_CHAN_1 (for/channel.f:62-1073): one RK3 substep on the

@@ -392,4 +392,12 @@ def test_reference_layout_round_trip(periodic):
     assert np.all(keep == 7.0 - 3.0j)
     s.set_field("CU3", ref, layout="reference_retained")
     assert np.array_equal(s.get_field("CU3"), ref[:, :nkzt, :nkxp])
+    # several fields in one call, both ways
+    ref2 = ref[::-1].copy()
+    s.set_fields({"CU1": ref2, "CU2": ref, "CP": -ref}, layout="reference_retained")
+    out = {n: np.full(ref.shape, 5.0 + 0j) for n in ("CP", "CU1", "CU2")}
+    s.get_fields(out, layout="reference_retained")
+    for n, a in (("CU1", ref2), ("CU2", ref), ("CP", -ref)):
+        assert np.array_equal(out[n][:, :nkzt, :nkxp], a[:, :nkzt, :nkxp]), n
+        assert np.all(out[n][:, nkzt:, :] == 5.0) and np.all(out[n][:, :, nkxp:] == 5.0), n
     s.close()

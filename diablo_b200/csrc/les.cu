@@ -11,8 +11,8 @@
 //          and U (physical), APPLY_BC_VEL_PHYS, one column pass for |S|, NU_T,
 //          |S| S_ij and the NU_T dU/dy cross terms, forward transforms, the SGS
 //          forcing G per field, the scalar eddy diffusion; the boundary planes
-//          of CU are refreshed from the physical velocity so the nonlinear
-//          stage sees what the reference's physical U holds;
+//          of CU get APPLY_BC_VEL_PHYS stated on the retained modes, so the
+//          nonlinear stage sees what the reference's physical U holds;
 //   (the fused z inverse / x-row products / z forward write CF and the
 //    spectral right-hand side R as in the DNS)
 //   post : CF += G, R += BETA_BAR H_BAR G; R, TH to physical; one thread per
@@ -70,6 +70,64 @@ __global__ void k_les_bc_spec(LesBc B, int NY, long ss, double2 *u1, double2 *u3
   if (B.w_lo == 1) {
     u3[ss + m] = u3[2 * ss + m];
     u3[m] = u3[ss + m];
+  }
+}
+
+// APPLY_BC_VEL_PHYS_LOWER / _UPPER (for/channel.f:2495-2652) stated on the
+// retained modes: the physical boundary planes are the neighbouring planes
+// plus constants, so their transforms are the neighbouring modes plus the
+// constants on the (0,0) mode.  This is the transform of what
+// k_les_bc_phys leaves in the physical velocity, without a transform.
+__global__ void k_les_bc_spec_phys(LesBc B, int NY, long ss, const double *__restrict__ dy,
+                                   const double *__restrict__ dyf, double2 *u1, double2 *u2,
+                                   double2 *u3) {
+  const long m = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= ss) return;
+  const double on = (m == 0) ? 1.0 : 0.0;  // constants live on the (0,0) mode
+  const long p0 = m, p1 = ss + m, p2 = 2 * ss + m;
+  const long pm = (long)(NY - 1) * ss + m, pn = (long)NY * ss + m, pn1 = (long)(NY + 1) * ss + m;
+  auto sh = [](double2 a, double c) { return make_double2(a.x + c, a.y); };
+  if (B.u_lo == 0) {
+    u1[p0] = make_double2(on * B.u_lo_c1, 0.0);
+    u1[p1] = u1[p0];
+  } else {
+    u1[p1] = sh(u1[p2], -on * dy[2] * B.u_lo_c1);
+    u1[p0] = sh(u1[p1], -on * dy[1] * B.u_lo_c1);
+  }
+  if (B.w_lo == 0) {
+    u3[p0] = make_double2(on * B.w_lo_c1, 0.0);
+    u3[p1] = u3[p0];
+  } else {
+    u3[p1] = sh(u3[p2], -on * dy[2] * B.w_lo_c1);
+    u3[p0] = sh(u3[p1], -on * dy[1] * B.w_lo_c1);
+  }
+  if (B.v_lo == 0) {
+    const double2 a = u2[p2];
+    u2[p1] = make_double2(on * 2.0 * B.v_lo_c1 - a.x, -a.y);
+    u2[p0] = u2[p1];
+  } else {
+    u2[p1] = sh(u2[p2], -on * dyf[1] * B.v_lo_c1);
+    u2[p0] = sh(u2[p1], -on * dyf[1] * B.v_lo_c1);
+  }
+  if (B.u_hi == 0) {
+    u1[pn] = make_double2(on * B.u_hi_c1, 0.0);
+    u1[pn1] = u1[pn];
+  } else {
+    u1[pn] = sh(u1[pm], on * dy[NY] * B.u_hi_c1);
+    u1[pn1] = sh(u1[pn], on * dy[NY] * B.u_hi_c1);
+  }
+  if (B.w_hi == 0) {
+    u3[pn] = make_double2(on * B.w_hi_c1, 0.0);
+    u3[pn1] = u3[pn];
+  } else {
+    u3[pn] = sh(u3[pm], on * dy[NY] * B.w_hi_c1);
+    u3[pn1] = sh(u3[pn], on * dy[NY] * B.w_hi_c1);
+  }
+  if (B.v_hi == 0) {
+    const double2 a = u2[pn];
+    u2[pn1] = make_double2(on * 2.0 * B.v_hi_c1 - a.x, -a.y);
+  } else {
+    u2[pn1] = sh(u2[pn], on * dy[NY] * B.v_hi_c1);
   }
 }
 
@@ -691,11 +749,11 @@ int dg_les_pre(dg_handle *h, int rk_step) {
     DG_LAUNCHED();
   }
   // the nonlinear stage reads the velocity from CU: give its boundary planes
-  // the values APPLY_BC_VEL_PHYS left in the physical velocity (retained
-  // modes only, so the transform is exact)
-  double2 *v[3] = {h->cu[0], h->cu[1], h->cu[2]};
-  DG_TRY(to_fourier(h, pslot(h, PS_U), 3, 0, 1, v));
-  DG_TRY(to_fourier(h, pslot(h, PS_U), 3, NY, NY + 1, v));
+  // the values APPLY_BC_VEL_PHYS left in the physical velocity
+  dg_kt_begin(h, "k_les_bc_spec_phys", h->st);
+  k_les_bc_spec_phys<<<dg_cdiv(ss, 256), 256, 0, h->st>>>(B, NY, ss, h->dy, h->dyf, h->cu[0],
+                                                          h->cu[1], h->cu[2]);
+  DG_LAUNCHED();
   return DG_OK;
 }
 

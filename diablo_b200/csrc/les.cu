@@ -651,7 +651,12 @@ int dg_les_init(dg_handle *h) {
     rt[4 * L + j] = 1.0 / DY[j];
     rt[5 * L + j] = 1.0 / DYF[j];
   }
-  DG_CUDA(dg_malloc(h, (void **)&h->les_rowtab, sizeof(double) * 6 * L));
+  cudaError_t e0 = dg_malloc(h, (void **)&h->les_rowtab, sizeof(double) * 6 * L);
+  if (e0 != cudaSuccess) {
+    free(t);
+    free(rt);
+    DG_CUDA(e0);
+  }
   cudaError_t e = cudaMemcpyAsync(h->les_dfac, t, sizeof(double) * 2 * (NY + 2),
                                   cudaMemcpyHostToDevice, h->st);
   cudaError_t e1 = cudaMemcpyAsync(h->les_rowtab, rt, sizeof(double) * 6 * L,

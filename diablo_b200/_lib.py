@@ -83,7 +83,7 @@ def load(path: str = LIB_PATH):
         "diablo_set_field": [P, I, P, I, I], "diablo_get_field": [P, I, P, I, I],
         "diablo_set_fields": [P, I, P, P, I, I], "diablo_get_fields": [P, I, P, P, I, I],
         "diablo_rk_chan_1": [P, I, I], "diablo_les_nu_t": [P, P, I], "diablo_les_stats_request": [P],
-        "diablo_les_stats": [P, P, P], "diablo_rem_div_chan": [P], "diablo_poisson_p_chan": [P],
+        "diablo_les_stats": [P, P, P], "diablo_les_tke": [P, P], "diablo_rem_div_chan": [P], "diablo_poisson_p_chan": [P],
         "diablo_apply_bc_vel": [P], "diablo_courant": [P],
         "diablo_fft_xz_to_fourier": [P, P, P, I, I, I],
         "diablo_fft_xz_to_physical": [P, P, P, I, I, I],

@@ -362,6 +362,36 @@ __global__ void k_les_means(long np, long pfield, const double *__restrict__ F,
   }
 }
 
+// tkebudget_chan_les (for/save_stats.f:887-964): per plane J = 1..NY the sum
+// over its points of U1 d(NU_T dU1/dy)/dy + U3 (same) + U2 d(NU_T dU2/dy)/dy
+// on GY, one block per plane.  DYF(0) is 0 as in the reference (never set),
+// so plane 1's U2 term is 0/0 there and here.
+__global__ void k_les_tke(int NY, long np, long pfield, const double *__restrict__ dy,
+                          const double *__restrict__ dyf, const double *__restrict__ U,
+                          const double *__restrict__ nut, double *__restrict__ out) {
+  const int j = 1 + blockIdx.x;
+  const double *U1 = U, *U2 = U + pfield, *U3 = U + 2 * pfield;
+  double a = 0.0;
+  for (long q = threadIdx.x; q < np; q += blockDim.x) {
+    const long c = (long)j * np + q, p = c + np, m = c - np;
+    a += U1[c] * ((nut[p] * (U1[p] - U1[c]) / dy[j + 1] - nut[c] * (U1[c] - U1[m]) / dy[j]) /
+                  dyf[j]) +
+         U3[c] * ((nut[p] * (U3[p] - U3[c]) / dy[j + 1] - nut[c] * (U3[c] - U3[m]) / dy[j]) /
+                  dyf[j]) +
+         U2[c] * ((0.5 * (nut[c] + nut[p]) * (U2[p] - U2[c]) / dyf[j] -
+                   0.5 * (nut[c] + nut[m]) * (U2[c] - U2[m]) / dyf[j - 1]) /
+                  dy[j]);
+  }
+  __shared__ double sa[256];
+  sa[threadIdx.x] = a;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sa[threadIdx.x] += sa[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[j] = sa[0];
+}
+
 // i kx CTH and i kz CTH on planes 1..NY+1 (for/channel.f:326-355)
 __global__ void k_les_th_grad(int NY, long ss, int nkxp, const double *__restrict__ kxv,
                               const double *__restrict__ kzv, const double2 *__restrict__ th,
@@ -878,5 +908,28 @@ extern "C" int diablo_les_stats(dg_handle *h, double *nu_t_mean, double *eps_sgs
   DG_CUDA(cudaMemcpyAsync(eps_sgs1_mean, h->les_means + h->NY + 2, n, cudaMemcpyDeviceToHost,
                           h->st));
   DG_CUDA(cudaStreamSynchronize(h->st));
+  return DG_OK;
+}
+
+// tkebudget_chan_les as SAVE_STATS_CHAN runs it when LES is on
+// (for/save_stats.f:30-36,164-170): APPLY_BC_VEL on the state, the velocity to
+// physical space, epsilon_sgs (rows 1..NY of NY+2) with the NU_T of the last
+// LES substep.
+extern "C" int diablo_les_tke(dg_handle *h, double *epsilon_sgs) {
+  if (!h || h->periodic || !h->p.les || !epsilon_sgs) return DG_ERR_ARG;
+  const int NY = h->NY;
+  const long np = (long)h->NZ * h->NX, pf = pfield_of(h);
+  DG_TRY(dg_apply_bc_vel_dev(h));
+  const double2 *cu[3] = {h->cu[0], h->cu[1], h->cu[2]};
+  DG_TRY(to_physical(h, cu, 3, 0, NY + 1, pslot(h, PS_U)));
+  DG_CUDA(cudaMemsetAsync(h->les_means, 0, sizeof(double) * (NY + 2), h->st));
+  dg_kt_begin(h, "k_les_tke", h->st);
+  k_les_tke<<<NY, 256, 0, h->st>>>(NY, np, pf, h->dy, h->dyf, pslot(h, PS_U), pslot(h, PS_NUT),
+                                   h->les_means);
+  DG_LAUNCHED();
+  DG_CUDA(cudaMemcpyAsync(epsilon_sgs, h->les_means, sizeof(double) * (NY + 2),
+                          cudaMemcpyDeviceToHost, h->st));
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  h->les_stats_valid = false;  // the means buffer now holds epsilon_sgs
   return DG_OK;
 }

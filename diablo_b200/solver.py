@@ -291,6 +291,12 @@ class Channel(_Solver):
         self._call("diablo_les_stats", _ptr(a), _ptr(b))
         return {"nu_sgs": a, "eps_sgs1": b}
 
+    def les_tke(self) -> np.ndarray:
+        """tkebudget_chan_les: epsilon_sgs, rows 1..NY (applies APPLY_BC_VEL)."""
+        out = np.zeros(self.p.ny + 2)
+        self._call("diablo_les_tke", _ptr(out))
+        return out
+
     def rem_div_chan(self):
         self._call("diablo_rem_div_chan")
 

@@ -1,6 +1,6 @@
 """Text outputs of SAVE_STATS_CHAN, tkebudget_chan and les_chan in the
 reference's formats (for/save_stats.f:66-81,414-420,665-674,1161-1170,
-for/les.f:491-503).
+for/les.f:491-503) and tkebudget_chan_les (for/save_stats.f:887-964).
 
 The profile dictionaries come from ``Channel.save_stats()`` and
 ``Channel.stats_means()``.  Data rows use the reference's explicit FORMATs
@@ -86,3 +86,22 @@ def write_mean_les(path: str, st: dict, gyf: np.ndarray, time_step: int, time: f
         for j in range(1, ny + 1):
             f.write(f"{j:3d} {gyf[j]:30.20f} {st['nu_sgs'][j]:30.20f} \n"
                     f"{st['eps_sgs1'][j]:30.20f} \n")
+
+
+def write_tke_les(path: str, epsilon_sgs: np.ndarray, gyf: np.ndarray, time_step: int,
+                  time: float, delta_t: float):
+    """tke_les.txt of tkebudget_chan_les (for/save_stats.f:946-960): j, GYF,
+    epsilon_sgs for j = 1..NY (FORMAT I3,' ',2(F30.20,' '))."""
+    ny = len(gyf) - 2
+
+    def fw(v):
+        # gfortran's F edit descriptor spells non-finite values NaN / Infinity
+        if np.isnan(v):
+            return "NaN".rjust(30)
+        if np.isinf(v):
+            return ("Infinity" if v > 0 else "-Infinity").rjust(30)
+        return f"{v:30.20f}"
+    with open(path, "w") as f:
+        _head(f, time_step, time, delta_t)
+        for j in range(1, ny + 1):
+            f.write(f"{j:3d} {gyf[j]:30.20f} {fw(epsilon_sgs[j])} \n")

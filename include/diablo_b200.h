@@ -148,6 +148,10 @@ int diablo_les_nu_t(dg_handle *h, double *dst, int where);
  * arrays of NY+2). */
 int diablo_les_stats_request(dg_handle *h);
 int diablo_les_stats(dg_handle *h, double *nu_t_mean, double *eps_sgs1_mean);
+/* tkebudget_chan_les (for/save_stats.f:887-964), which SAVE_STATS_CHAN calls
+ * with LES: applies APPLY_BC_VEL to the state, then epsilon_sgs rows 1..NY
+ * (host array of NY+2; sums over each plane, as the reference's). */
+int diablo_les_tke(dg_handle *h, double *epsilon_sgs);
 /* SUBROUTINE REM_DIV_CHAN (for/channel.f:1103-1214): projects CU1..3, leaves
  * phi in CR1. */
 int diablo_rem_div_chan(dg_handle *h);

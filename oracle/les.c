@@ -371,3 +371,36 @@ int orc_les_stats(const orc *o, double *nu_t_mean, double *eps_sgs1_mean) {
   memcpy(eps_sgs1_mean, o->eps_sgs1_mean, sizeof(double) * (o->NY + 2));
   return 0;
 }
+
+/* tkebudget_chan_les (for/save_stats.f:887-964), called by SAVE_STATS_CHAN
+ * after its APPLY_BC_VEL and the transform of CU1..CU3: per plane J = 1..NY
+ * the SUM (not the mean) over the points of U1 d(NU_T dU1/dy)/dy + U3 ... +
+ * U2 d(NU_T dU2/dy)/dy with NU_T from the last LES substep.  DYF(0) is never
+ * set in the reference (it stays 0), so the U2 term of J = 1 is 0/0. */
+void orc_tkebudget_chan_les(orc *o, double *eps) {
+  const int NY = o->NY;
+  const long np = (long)o->NZ * o->NX;
+  const double *DY = o->DY, *DYF = o->DYF, *NUT = o->NU_T;
+  orc_apply_bc_vel(o);
+  orc_fft_xz_to_physical(o, o->CU1, o->U1, 0, NY + 1);
+  orc_fft_xz_to_physical(o, o->CU2, o->U2, 0, NY + 1);
+  orc_fft_xz_to_physical(o, o->CU3, o->U3, 0, NY + 1);
+  const double *U1 = o->U1, *U2 = o->U2, *U3 = o->U3;
+  for (int j = 0; j <= NY + 1; j++) eps[j] = 0.0;
+  for (int j = 1; j <= NY; j++) {
+    double a = 0.0;
+    for (long q = 0; q < np; q++) {
+      const long c = j * np + q, p = c + np, m = c - np;
+      const double t =
+          U1[c] * ((NUT[p] * (U1[p] - U1[c]) / DY[j + 1] - NUT[c] * (U1[c] - U1[m]) / DY[j]) /
+                   DYF[j]) +
+          U3[c] * ((NUT[p] * (U3[p] - U3[c]) / DY[j + 1] - NUT[c] * (U3[c] - U3[m]) / DY[j]) /
+                   DYF[j]) +
+          U2[c] * ((0.5 * (NUT[c] + NUT[p]) * (U2[p] - U2[c]) / DYF[j] -
+                    0.5 * (NUT[c] + NUT[m]) * (U2[c] - U2[m]) / DYF[j - 1]) /
+                   DY[j]);
+      a = a + t;
+    }
+    eps[j] = a;
+  }
+}

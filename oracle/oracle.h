@@ -147,6 +147,9 @@ int orc_get_nu_t(const orc *o, double *out);
  * MOD(TIME_STEP, SAVE_STATS_INT) = 0 and RK_STEP = 1. */
 void orc_les_stats_request(orc *o);
 int orc_les_stats(const orc *o, double *nu_t_mean, double *eps_sgs1_mean);
+/* tkebudget_chan_les: epsilon_sgs rows 1..NY (sums over the plane); applies
+ * APPLY_BC_VEL to the state as SAVE_STATS_CHAN does first. */
+void orc_tkebudget_chan_les(orc *o, double *epsilon_sgs);
 
 #ifdef __cplusplus
 }

@@ -111,6 +111,7 @@ def lib():
         L.orc_get_nu_t.argtypes = [P, P]
         L.orc_les_stats_request.argtypes = [P]
         L.orc_les_stats.argtypes = [P, P, P]
+        L.orc_tkebudget_chan_les.argtypes = [P, P]
         _lib = L
     return _lib
 
@@ -195,6 +196,12 @@ class Oracle:
         if lib().orc_les_stats(self.h, _ptr(a), _ptr(b)) != 0:
             raise ValueError("no LES statistics recorded")
         return {"nu_sgs": a, "eps_sgs1": b}
+
+    def tkebudget_chan_les(self) -> np.ndarray:
+        """epsilon_sgs (rows 1..NY; sums over each plane) after APPLY_BC_VEL."""
+        out = np.zeros(self.p.ny + 2)
+        lib().orc_tkebudget_chan_les(self.h, _ptr(out))
+        return out
 
     def set_state(self, st: dict):
         for k, v in st.items():

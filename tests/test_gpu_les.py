@@ -180,3 +180,20 @@ def test_les_mixed_precision(case):
     assert all(v <= 1e-5 for v in err.values()), err
     assert g.stats()["div_max"] < 1e-12
     g.close()
+
+
+def test_tkebudget_chan_les_matches_oracle():
+    p, gy = kh_les()
+    ref, ch = start(p, gy, ics.kh_shear_layer, seed=27, kick=0.3)
+    for s in (1, 2, 3):
+        ref.step(s)
+        ch.step(s)
+    want, got = ref.tkebudget_chan_les(), ch.les_tke()
+    # row 1 is 0/0 in both (DYF(0) unset), rows 2..NY are sums over a plane
+    assert np.isnan(want[1]) and np.isnan(got[1])
+    w, g = want[2:p.ny + 1], got[2:p.ny + 1]
+    assert np.abs(g - w).max() <= 1e-11 * np.abs(w).max() + 1e-15
+    # both applied APPLY_BC_VEL to their state first
+    for n in ("CU1", "CU2", "CU3"):
+        assert rel(ch.get_field(n), ref.get(n)) <= TOL, n
+    ch.close()

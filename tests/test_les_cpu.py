@@ -156,3 +156,26 @@ def test_les_plane_means_and_mean_les_format(tmp_path):
     j, y, nu = lines[1].split()
     assert int(j) == 1 and float(y) == pytest.approx(gyf[1]) and float(nu) == pytest.approx(st["nu_sgs"][1])
     assert len(lines[2]) == 31 and float(lines[2]) == pytest.approx(st["eps_sgs1"][1], abs=1e-20)
+
+
+def test_tkebudget_chan_les_and_tke_les_format(tmp_path):
+    import warnings
+    from diablo_b200 import stats_io
+    p, gy, ref = les_case()
+    ref.step(1)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        eps = ref.tkebudget_chan_les()
+    # DYF(0) is never set in the reference: plane 1's U2 term is 0/0
+    assert np.isnan(eps[1])
+    assert np.all(np.isfinite(eps[2:p.ny + 1])) and np.abs(eps[2:p.ny + 1]).max() > 0
+    # the model dissipates: the eddy-viscosity term removes energy overall
+    assert eps[2:p.ny + 1].sum() < 0
+    _gy, gyf, _dy, _dyf = ref.grid()
+    path = tmp_path / "tke_les.txt"
+    stats_io.write_tke_les(str(path), eps, gyf, 1, 0.02, p.delta_t)
+    lines = open(path).read().splitlines()
+    assert len(lines) == 1 + p.ny
+    assert lines[1].split()[2] == "NaN"
+    j, y, e = lines[2].split()
+    assert int(j) == 2 and float(e) == pytest.approx(eps[2], rel=1e-12)

@@ -314,6 +314,10 @@ def step_timer(ts):
     return timed
 
 
+LES_CASES = {"kh_les": "kh_les_128x65x16", "channel_re180_les": "channel_re180_les_128x129x128",
+             "channel_re180_les_mixed": "channel_re180_les_128x129x128_mixed"}
+
+
 def run_les_configs(ts, timed, nsteps, cpu=True, only=""):
     """LES (constant Smagorinsky, FP64): the reference's KH_test run and the
     Re_tau = 180 channel with the model on, each timed over nsteps
@@ -323,11 +327,13 @@ def run_les_configs(ts, timed, nsteps, cpu=True, only=""):
     from diablo_b200.solver import Channel
     stream = ts.cuda_stream
     out = {}
+    p180, gy180 = configs.channel_re180()
     for name, (p, gy), maker in (("kh_les_128x65x16", configs.kh_les(), ics.kh_shear_layer),
                                  ("channel_re180_les_128x129x128",
-                                  (configs.channel_re180()[0].replace(les=1),
-                                   configs.channel_re180()[1]), ics.channel_laminar)):
-        if only and not name.startswith(only):
+                                  (p180.replace(les=1), gy180), ics.channel_laminar),
+                                 ("channel_re180_les_128x129x128_mixed",
+                                  (p180.replace(les=1, precision=1), gy180), ics.channel_laminar)):
+        if only and name != LES_CASES[only]:
             continue
         kw = {"kick": 0.1} if maker is ics.kh_shear_layer else {}
         u1, u2, u3, th = maker(p, gy, seed=2, **kw)
@@ -349,7 +355,7 @@ def run_les_configs(ts, timed, nsteps, cpu=True, only=""):
                                    "cores": os.cpu_count() or 1, "kind": "port",
                                    "sample": "2 steps of the same case"}
             ref.close()
-        out[name + "_fp64"] = rec
+        out[name if p.precision else name + "_fp64"] = rec
     return out
 
 
@@ -653,7 +659,7 @@ def main():
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--ensemble-rate", type=float, default=20.0)
     ap.add_argument("--ensemble-active", type=int, default=16)
-    ap.add_argument("--les-only", default="", choices=["", "all", "kh_les", "channel_re180_les"],
+    ap.add_argument("--les-only", default="", choices=["", "all"] + list(LES_CASES),
                     help="time only the LES workloads (all, or the one named; --steps "
                          "graph-replayed steps each, after --warmup) and print their records; "
                          "no contract line")

@@ -609,14 +609,16 @@ static int copy_fields(dg_handle *h, int n, const int *fields, double *const *ar
   // the side stream starts after the work queued so far on the main stream
   DG_CUDA(cudaEventRecord(h->ev_fork, h->st));
   DG_CUDA(cudaStreamWaitEvent(h->st2, h->ev_fork, 0));
-  for (int i = 0; i < n; i++)
-    DG_TRY(copy_field_async(h, field_ptr(h, fields[i]), arrs[i], layout, where, to_device,
-                            (i & 1) ? h->st2 : h->st));
+  int status = DG_OK;
+  for (int i = 0; i < n && status == DG_OK; i++)
+    status = copy_field_async(h, field_ptr(h, fields[i]), arrs[i], layout, where, to_device,
+                              (i & 1) ? h->st2 : h->st);
+  // join and synchronise whatever was queued, also after a failed copy
   DG_CUDA(cudaEventRecord(h->ev_join, h->st2));
   DG_CUDA(cudaStreamWaitEvent(h->st, h->ev_join, 0));
   h->tables_pending = false;  // anything pending on the side stream is joined now
   DG_CUDA(cudaStreamSynchronize(h->st));
-  return DG_OK;
+  return status;
 }
 
 extern "C" int diablo_set_fields(dg_handle *h, int n, const int *fields, const double *const *src,

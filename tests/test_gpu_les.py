@@ -197,3 +197,20 @@ def test_tkebudget_chan_les_matches_oracle():
     for n in ("CU1", "CU2", "CU3"):
         assert rel(ch.get_field(n), ref.get(n)) <= TOL, n
     ch.close()
+
+
+def test_kh_test_les_100_steps():
+    """The reference's own KH_test run (KH_test/input*.dat, grid.h5: 128x65x16
+    stretched, CFL 0.5 with COURANT every step, Neumann scalar, constant
+    Smagorinsky from the first step) for 100 steps against the oracle."""
+    p, gy = configs.kh_les()
+    ref, ch = start(p, gy, ics.kh_shear_layer, seed=28, kick=0.1)
+    for s in range(1, 101):
+        ref.step(s)
+        ch.steps(s, 1)
+    t_ref, dt_ref = ref.get_time()
+    t, dt = ch.get_time()
+    assert abs(t - t_ref) <= 1e-12 * t_ref and abs(dt - dt_ref) <= 1e-12 * dt_ref
+    compare(ref, ch, p)
+    assert ch.stats()["div_max"] < 1e-12
+    ch.close()

@@ -8,6 +8,8 @@
 #include <mutex>
 #include <string>
 
+#include <stddef.h>
+
 #include "dg_internal.cuh"
 
 namespace {
@@ -89,6 +91,25 @@ void dg_count_launch(int n) {
 }
 
 extern "C" int dg_version(void) { return 100; }
+
+// The layout of the ABI structs as this build compiled them, for binding
+// checks: sizeof(dg_params), sizeof(dg_stats), then the byte offsets of
+// dg_params' fields nx, nu, f_type, ubulk0, th_bc_ymin, epsilon_target, les,
+// les_model_type, create_new_flow.  Returns the number of values written
+// (at most n).
+extern "C" int dg_abi_layout(int64_t *out, int n) {
+  const int64_t v[] = {(int64_t)sizeof(dg_params), (int64_t)sizeof(dg_stats),
+                       (int64_t)offsetof(dg_params, nx), (int64_t)offsetof(dg_params, nu),
+                       (int64_t)offsetof(dg_params, f_type), (int64_t)offsetof(dg_params, ubulk0),
+                       (int64_t)offsetof(dg_params, th_bc_ymin),
+                       (int64_t)offsetof(dg_params, epsilon_target),
+                       (int64_t)offsetof(dg_params, les), (int64_t)offsetof(dg_params, les_model_type),
+                       (int64_t)offsetof(dg_params, create_new_flow)};
+  const int k = (int)(sizeof(v) / sizeof(v[0]));
+  if (!out) return k;
+  for (int i = 0; i < k && i < n; i++) out[i] = v[i];
+  return k < n ? k : n;
+}
 extern "C" const char *dg_last_error(void) { return g_err.c_str(); }
 extern "C" int64_t dg_kernel_launches(void) { return (int64_t)g_launches.load(); }
 

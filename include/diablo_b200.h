@@ -102,6 +102,11 @@ int dg_version(void);
 const char *dg_last_error(void);
 /* Kernels launched by this library since load (for launch accounting). */
 int64_t dg_kernel_launches(void);
+/* The ABI structs as compiled: sizeof(dg_params), sizeof(dg_stats), then the
+ * offsets of dg_params' nx, nu, f_type, ubulk0, th_bc_ymin, epsilon_target,
+ * les, les_model_type, create_new_flow (for binding checks).  Returns the
+ * count written; with out = NULL, the count available. */
+int dg_abi_layout(int64_t *out, int n);
 
 /* -------------------------------------------------------------- lifecycle
  * Replaces the device-side parts of INITIALIZE: INIT_FFT (for/fft.f:55-147),

@@ -17,9 +17,20 @@ def test_header_symbols_exported():
 
 
 def test_params_struct_layout_matches_header():
-    # offsets of a few fields must match the C struct (checked by the library)
-    assert ctypes.sizeof(DgParams) % 8 == 0
-    assert DgParams.nu.offset == 24 and DgParams.f_type.offset < DgParams.ubulk0.offset
+    # the ctypes mirrors against the structs as the library compiled them
+    from diablo_b200._lib import DgStats
+    L = _lib.load()
+    L.dg_abi_layout.restype = ctypes.c_int
+    L.dg_abi_layout.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    n = L.dg_abi_layout(None, 0)
+    buf = (ctypes.c_int64 * n)()
+    assert L.dg_abi_layout(buf, n) == n == 11
+    sizes = list(buf)
+    assert sizes[0] == ctypes.sizeof(DgParams)
+    assert sizes[1] == ctypes.sizeof(DgStats)
+    names = ["nx", "nu", "f_type", "ubulk0", "th_bc_ymin", "epsilon_target", "les",
+             "les_model_type", "create_new_flow"]
+    assert sizes[2:] == [getattr(DgParams, f).offset for f in names]
 
 
 def test_init_refuses_without_device_or_bad_args():

@@ -1108,50 +1108,66 @@ size_t zfwd_smem(const dg_handle *h) {
 // column and linear in TEMP1 = NU H_BAR / 2, so the host stores per row
 //   CN row : l = t l1, d = 1 + t d1, u = t u1   with t = TEMP1 (or TEMP1/PR)
 //   fixed  : l0, d0, u0 and the BC value
-// and one thread per (substep, field) runs the elimination whenever DELTA_T
+// and one CTA per (substep, field) runs the elimination whenever DELTA_T
 // changes.  Output per (rk, field): [5][NY+2] = a', 1/b', c, kind, bc value.
 struct CnRows {
   int NY, nfld;
   double nu, nuv, pr[3 + DG_MAX_TH];  // pr = 1 for velocity
 };
 
-__global__ void k_cn_tables(CnRows P, const double *__restrict__ dscal,
-                            const double *__restrict__ rows, double *__restrict__ tab) {
-  // rows: [field][8][L] = kind, l1, d1, u1, l0, d0, u0, v (read through L1:
-  // the three substeps of a field read the same rows)
+// blockIdx.x = rk * nfld + field.  The CTA stages the field's row templates
+// into shared memory with coalesced loads, one thread runs the elimination
+// recurrence out of shared memory (the recurrence is sequential in j; only
+// its division and multiply-add are on the critical path), and the CTA
+// writes the table back with coalesced stores.
+constexpr int CT_THR = 128;
+
+__global__ void __launch_bounds__(CT_THR) k_cn_tables(CnRows P, const double *__restrict__ dscal,
+                                                      const double *__restrict__ rows,
+                                                      double *__restrict__ tab) {
+  // rows: [field][8][L] = kind, l1, d1, u1, l0, d0, u0, v
+  extern __shared__ double ct_sm[];
   const int L = P.NY + 2;
-  const int t = threadIdx.x;
-  if (t >= 3 * P.nfld) return;
-  const int rk = t / P.nfld, f = t % P.nfld;
-  const double *R = rows + (long)f * 8 * L;
-  double *T = tab + (long)(rk * (3 + DG_MAX_TH) + f) * 5 * L;
-  const double h = dscal[2 + rk];
-  const double s = (P.nu * h / 2.0) / P.pr[f] * P.nuv;
-  double bprev = 1.0, cprev = 0.0;
-  for (int j = 0; j < L; j++) {
-    const double kind = R[j];
-    double l, d, u;
-    if (kind == (double)ROW_RHS) {
-      l = s * R[1 * L + j];
-      d = 1.0 + s * R[2 * L + j];
-      u = s * R[3 * L + j];
-    } else {
-      l = R[4 * L + j];
-      d = R[5 * L + j];
-      u = R[6 * L + j];
+  const int rk = blockIdx.x / P.nfld, f = blockIdx.x % P.nfld;
+  double *R = ct_sm;          // [8][L]
+  double *T = ct_sm + 8 * L;  // [5][L]
+  const double *Rg = rows + (long)f * 8 * L;
+  for (int i = threadIdx.x; i < 8 * L; i += CT_THR) R[i] = Rg[i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double h = dscal[2 + rk];
+    const double s = (P.nu * h / 2.0) / P.pr[f] * P.nuv;
+    double bprev = 1.0, cprev = 0.0;
+    for (int j = 0; j < L; j++) {
+      const double kind = R[j];
+      double l, d, u;
+      if (kind == (double)ROW_RHS) {
+        l = s * R[1 * L + j];
+        d = 1.0 + s * R[2 * L + j];
+        u = s * R[3 * L + j];
+      } else {
+        l = R[4 * L + j];
+        d = R[5 * L + j];
+        u = R[6 * L + j];
+      }
+      double a = 0.0, b = d;
+      if (j > 0) {
+        a = -l / bprev;
+        b = d + a * cprev;
+      }
+      T[0 * L + j] = a;
+      T[1 * L + j] = (b != 0.0) ? 1.0 / b : 0.0;
+      T[2 * L + j] = u;
+      bprev = b;
+      cprev = u;
     }
-    double a = 0.0, b = d;
-    if (j > 0) {
-      a = -l / bprev;
-      b = d + a * cprev;
-    }
-    T[0 * L + j] = a;
-    T[1 * L + j] = (b != 0.0) ? 1.0 / b : 0.0;
-    T[2 * L + j] = u;
-    T[3 * L + j] = kind;
-    T[4 * L + j] = R[7 * L + j];
-    bprev = b;
-    cprev = u;
+  }
+  __syncthreads();
+  double *Tg = tab + (long)(rk * (3 + DG_MAX_TH) + f) * 5 * L;
+  for (int i = threadIdx.x; i < 3 * L; i += CT_THR) Tg[i] = T[i];
+  for (int i = threadIdx.x; i < L; i += CT_THR) {
+    Tg[3 * L + i] = R[i];          // kind
+    Tg[4 * L + i] = R[7 * L + i];  // bc value
   }
 }
 
@@ -1207,7 +1223,8 @@ template <int MT>
 __global__ void __launch_bounds__(COL_THR) k_cn_col(int NY, long ss, const double *__restrict__ tab_rk,
                                                    const __grid_constant__ CnMaps maps, int by,
                                                    int nbox, FieldPtrs cu, int4 wlo_a,
-                                                   int4 wlo_b, int *__restrict__ err) {
+                                                   int4 wlo_b, int *__restrict__ err, long spin,
+                                                   unsigned extra_tx) {
   extern __shared__ __align__(128) unsigned char csm_raw[];
   unsigned char *sbase = csm_raw + ((128u - (dg_smem_addr(csm_raw) & 127u)) & 127u);
   const int L = NY + 2;
@@ -1224,18 +1241,19 @@ __global__ void __launch_bounds__(COL_THR) k_cn_col(int NY, long ss, const doubl
   __syncthreads();
   dg_pdl_wait();  // R comes from the z-forward kernel
   if (tid == 0) {
-    // columns beyond ss and planes beyond L arrive as zeros
-    dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * nbox * by * MT));
+    // columns beyond ss and planes beyond L arrive as zeros (extra_tx is 0
+    // except in the wait test, where the barrier can then never complete)
+    dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * nbox * by * MT) + extra_tx);
     for (int q = 0; q < nbox; q++)
       dg_tma_load_2d(X + (long)q * by * MT, &maps.m[f], (int)(2 * m0), q * by, bar);
   }
   const double *T = tab_rk + (long)f * 5 * L;
   for (int i = tid; i < 5 * L; i += COL_THR) TB[i] = T[i];
-  const bool landed = dg_mbar_wait(bar, 0);
+  const bool landed = dg_mbar_wait(bar, 0, spin);
   __syncthreads();
   if (!landed) {
     if (tid == 0) atomicExch(err + 1, 1);
-    dg_mbar_wait(bar, 0);  // give the copies in flight one more bounded wait
+    dg_mbar_wait(bar, 0, spin);  // give the copies in flight one more bounded wait
     return;
   }
   const int mt = (int)((ss - m0) < MT ? (ss - m0) : MT);
@@ -1727,8 +1745,14 @@ int dg_cn_tables(dg_handle *h) {
   CnRows P;
   P.NY = h->NY; P.nfld = h->nf; P.nu = h->p.nu; P.nuv = h->p.nu_v_scale;
   for (int f = 0; f < 3 + DG_MAX_TH; f++) P.pr[f] = (f >= 3 && f - 3 < h->NTH) ? h->p.pr[f - 3] : 1.0;
+  const size_t sm = sizeof(double) * 13 * (size_t)L;
+  if (sm > 220 * 1024) {
+    dg_set_error("NY too large for the Crank-Nicolson table kernel (NY + 2 <= 2166)");
+    return DG_ERR_DIMS;
+  }
+  if (sm > 48 * 1024) dg_big_smem((const void *)k_cn_tables);
   dg_kt_begin(h, "k_cn_tables", h->st);
-  k_cn_tables<<<1, 32, 0, h->st>>>(P, h->dscal, h->cn_rows, h->cn_tab);
+  k_cn_tables<<<3 * h->nf, CT_THR, sm, h->st>>>(P, h->dscal, h->cn_rows, h->cn_tab);
   DG_LAUNCHED();
   return DG_OK;
 }
@@ -1775,13 +1799,17 @@ int dg_cn_solve_dev(dg_handle *h, int rk_step) {
   }
   const CnMaps maps = *h->cn_maps;
   dim3 grid(dg_cdiv(h->ss, mt), h->nf);
+  // the wait test (DG_TUNE_WAIT_TEST) applies to this one launch
+  const long spin = h->wait_test > 0 ? (long)h->wait_test : DG_ASYNC_SPIN;
+  const unsigned extra_tx = h->wait_test > 0 ? 16u : 0u;
+  h->wait_test = 0;
 #define CN_CASE(MTV)                                                                    \
   if (mt == MTV) {                                                                      \
     dg_big_smem((const void *)k_cn_col<MTV>);                                           \
     dg_kt_begin(h, "k_cn_col", h->st);                                                  \
     DG_CUDA(dg_launch(h->pdl, k_cn_col<MTV>, grid, dim3(COL_THR), sm, h->st, h->NY, h->ss, \
                       tab, maps, by, nbox, cu, make_int4(wl[0], wl[1], wl[2], wl[3]),    \
-                      make_int4(wl[4], wl[5], wl[6], wl[7]), h->dflag));                \
+                      make_int4(wl[4], wl[5], wl[6], wl[7]), h->dflag, spin, extra_tx)); \
   }
   CN_CASE(4) CN_CASE(8) CN_CASE(16)
 #undef CN_CASE

@@ -159,6 +159,8 @@ struct dg_handle {
   int cn_mt;                    // modes per CTA of the CN column kernel (4, 8, 16)
   int xrow_chunk;               // planes per CTA of the x-row product kernel (0 = auto)
   int ychunk;                   // planes per y-chunk of a substep (0 = all)
+  int wait_test;                // test only: poll limit of the next CN launch, whose
+                                // barrier then expects 16 bytes more than it receives
 
   // LES (dg_params.les): physical slots [nslots][NY+2][NZ][NX], spectral slots
   // [nslots][NY+2][ss], filter-width factors [2][NY+2] (DYF, DY), mean U1/U3
@@ -253,7 +255,8 @@ __device__ __forceinline__ void dg_pdl_wait() { asm volatile("griddepcontrol.wai
 // ------------------------------------------------------------------- TMA
 // Bulk tensor copies (cp.async.bulk.tensor, no multicast) into shared memory,
 // completed on an mbarrier.  Waits are bounded: a copy that does not land
-// within DG_ASYNC_SPIN polls sets dg_handle::dflag[1] (reported by the next
+// within the kernel's poll limit (DG_ASYNC_SPIN unless the handle's wait test
+// lowers it for one launch) sets dg_handle::dflag[1] (reported by the next
 // diablo_stats / diablo_synchronize) and the kernel skips its work.
 #define DG_ASYNC_SPIN (1L << 24)
 
@@ -279,10 +282,11 @@ __device__ __forceinline__ void dg_tma_load_2d(void *dst, const CUtensorMap *map
       "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(dg_smem_addr(bar))
       : "memory");
 }
-// true once phase `parity` of the barrier completed; false after the limit
-__device__ __forceinline__ bool dg_mbar_wait(unsigned long long *bar, unsigned parity) {
+// true once phase `parity` of the barrier completed; false after `spin` polls
+__device__ __forceinline__ bool dg_mbar_wait(unsigned long long *bar, unsigned parity,
+                                             long spin = DG_ASYNC_SPIN) {
   const unsigned a = dg_smem_addr(bar);
-  for (long it = 0; it < DG_ASYNC_SPIN; it++) {
+  for (long it = 0; it < spin; it++) {
     unsigned done;
     asm volatile(
         "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"

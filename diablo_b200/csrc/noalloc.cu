@@ -21,7 +21,9 @@
 // of one device share the array: calls that overlap on the GPU race.
 #include <string.h>
 
+#include <map>
 #include <mutex>
+#include <utility>
 
 #include "dg_internal.cuh"
 
@@ -29,13 +31,32 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[DG_NOALLOC_SCRA
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void *g_addr[kMaxDevices];  // device address of g_noalloc_scratch, per device ordinal
+// The scratch array's device address per CUDA context.  A module is loaded
+// per context, so the address belongs to the context current at the call
+// (the device's primary context for runtime-API callers; another context
+// made current, or the primary context after cudaDeviceReset, gets its own
+// entry).  The first call in a context looks it up with cudaGetSymbolAddress
+// -- in host code the array's name is only a host-side stand-in -- and later
+// calls reuse it while it is still mapped.  That first call may load the
+// module, so it belongs before any stream capture.
+typedef int (*CtxGetCurrent)(void **);
 
-// Address of the scratch on the current device.  The first call on a device
-// looks it up with cudaGetSymbolAddress (the array's name is only a host-side
-// stand-in in host code) and caches it.
+CtxGetCurrent ctx_getter() {
+  static CtxGetCurrent fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrent>(p);
+  });
+  return fn;
+}
+
+std::mutex g_mu;
+std::map<std::pair<int, void *>, void *> g_addr;  // (device, context) -> address
+
 int scratch_address(void **out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
@@ -43,22 +64,75 @@ int scratch_address(void **out) {
     dg_set_error((std::string("no current CUDA device: ") + cudaGetErrorString(e)).c_str());
     return DG_ERR_NODEV;
   }
-  if (dev < 0 || dev >= kMaxDevices) {
-    dg_set_error("device ordinal beyond the allocation-free entry point's table");
-    return DG_ERR_NODEV;
+  CtxGetCurrent get = ctx_getter();
+  if (!get) {
+    dg_set_error("cuCtxGetCurrent is not available from the driver");
+    return DG_ERR_CUDA;
   }
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_addr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
+  auto lookup = [&](void **p) -> int {
+    e = cudaGetSymbolAddress(p, g_noalloc_scratch);
+    if (e != cudaSuccess || !*p) {
       dg_set_error((std::string("cudaGetSymbolAddress of the scratch array: ") +
                     cudaGetErrorString(e)).c_str());
       return DG_ERR_CUDA;
     }
-    g_addr[dev] = p;
+    return DG_OK;
+  };
+  std::lock_guard<std::mutex> lk(g_mu);
+  void *ctx = nullptr;
+  if (get(&ctx) != 0) {
+    dg_set_error("cuCtxGetCurrent failed");
+    return DG_ERR_CUDA;
   }
-  *out = g_addr[dev];
+  void *p = nullptr;
+  if (!ctx) {
+    // no context bound to this thread yet: the lookup binds the device's
+    // primary context (the runtime does that lazily), which then identifies
+    DG_TRY(lookup(&p));
+    if (get(&ctx) != 0 || !ctx) {
+      dg_set_error("no CUDA context is current after the scratch lookup");
+      return DG_ERR_CUDA;
+    }
+    g_addr[{dev, ctx}] = p;
+    *out = p;
+    return DG_OK;
+  }
+  auto it = g_addr.find({dev, ctx});
+  if (it != g_addr.end()) {
+    // a context handle can come back with the same value after a reset, with
+    // the module reloaded elsewhere: keep the cached address only while it
+    // is still mapped device memory of this device
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, it->second) == cudaSuccess &&
+        a.type == cudaMemoryTypeDevice && a.device == dev) {
+      *out = it->second;
+      return DG_OK;
+    }
+    cudaGetLastError();
+  }
+  DG_TRY(lookup(&p));
+  g_addr[{dev, ctx}] = p;
+  *out = p;
+  return DG_OK;
+}
+
+// V and VV must be memory this device can address as device memory:
+// anything else would fault inside a kernel and poison the caller's context
+int check_device_pointer(const void *ptr, const char *name) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DG_ERR_NODEV;
+  cudaPointerAttributes a;
+  cudaError_t e = cudaPointerGetAttributes(&a, ptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // clear the query's error so the next launch check does not see it
+    dg_set_error((std::string(name) + " is not a device pointer: " + cudaGetErrorString(e)).c_str());
+    return DG_ERR_ARG;
+  }
+  if ((a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) || a.device != dev) {
+    dg_set_error((std::string(name) + " must be device (or managed) memory of the current "
+                  "device").c_str());
+    return DG_ERR_ARG;
+  }
   return DG_OK;
 }
 
@@ -98,6 +172,8 @@ extern "C" int diablo_fft_xz_to_fourier_noalloc(const double *V, double *VV, int
     dg_set_error("V and VV must be device pointers");
     return DG_ERR_ARG;
   }
+  DG_TRY(check_device_pointer(V, "V"));
+  DG_TRY(check_device_pointer(VV, "VV"));
   if (ny < 1 || jmin < 0 || jmax > ny + 1 || jmax < jmin) {
     dg_set_error("need NY >= 1 and 0 <= JMIN <= JMAX <= NY+1");
     return DG_ERR_ARG;

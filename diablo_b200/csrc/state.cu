@@ -445,14 +445,18 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
 }
 
 // dflag[1] is set by a kernel whose bulk tensor copies did not land within
-// its bounded wait (the kernel then skipped its work)
+// its bounded wait (the kernel then skipped its work).  Reported once: the
+// flag is cleared, so the next call reports only a new failure.
 static int check_async_flag(dg_handle *h) {
   int f = 0;
   DG_CUDA(cudaMemcpyAsync(&f, h->dflag + 1, sizeof(int), cudaMemcpyDeviceToHost, h->st));
   DG_CUDA(cudaStreamSynchronize(h->st));
   if (f) {
-    dg_set_error("a bulk tensor copy did not complete within its wait limit; results are invalid");
-    return DG_ERR_CUDA;
+    DG_CUDA(cudaMemsetAsync(h->dflag + 1, 0, sizeof(int), h->st));
+    DG_CUDA(cudaStreamSynchronize(h->st));
+    dg_set_error("a bulk tensor copy did not complete within its wait limit; the substep's "
+                 "results are invalid");
+    return DG_ERR_TIMEOUT;
   }
   return DG_OK;
 }

@@ -13,6 +13,13 @@
 //                       chunks keep the intermediate planes in L2.
 //   DG_TUNE_PDL         1 (default): the substep kernels are launched with
 //                       programmatic dependent launch; 0: plain launches.
+//   DG_TUNE_WAIT_TEST   test only, not a launch shape: value > 0 makes the
+//                       next CN column launch poll its bulk-copy barrier at
+//                       most `value` times and expect 16 bytes more than its
+//                       copies bring, so every copy lands but the wait runs
+//                       out; the kernel then flags the failure and skips its
+//                       work.  It exercises the bounded-wait error path
+//                       without a fault; the setting clears after that launch.
 //
 // dg_autotune times candidate values one tunable at a time (coordinate
 // descent) on the handle's own state with CUDA events over a few eager
@@ -59,6 +66,10 @@ extern "C" int dg_tune_set(dg_handle *h, int key, int value) {
       if (value != 0 && value != 1) return DG_ERR_ARG;
       h->pdl = value;
       break;
+    case DG_TUNE_WAIT_TEST:
+      if (value < 0 || value > (1 << 20)) return DG_ERR_ARG;
+      h->wait_test = value;
+      break;
     default:
       return DG_ERR_ARG;
   }
@@ -74,6 +85,7 @@ extern "C" int dg_tune_get(dg_handle *h, int key, int *value) {
     case DG_TUNE_XROW_CHUNK: *value = h->xrow_chunk; return DG_OK;
     case DG_TUNE_YCHUNK: *value = h->ychunk; return DG_OK;
     case DG_TUNE_PDL: *value = h->pdl; return DG_OK;
+    case DG_TUNE_WAIT_TEST: *value = h->wait_test; return DG_OK;
     default: return DG_ERR_ARG;
   }
 }

@@ -91,6 +91,14 @@ class _Solver:
             out[k] = v.value
         return out
 
+    def wait_test(self, polls: int):
+        """Test only: the next Crank-Nicolson column launch gives up on its
+        bulk-copy barrier after `polls` polls (its copies all land; the
+        barrier expects 16 bytes more), skips its work and flags the failure,
+        which the next synchronize / stats call reports once as
+        DG_ERR_TIMEOUT."""
+        self._call("dg_tune_set", 5, int(polls))
+
     def autotune(self, steps_per_trial: int = 3) -> dict:
         """Time candidate launch shapes on this state, keep the fastest; the
         state, TIME and DELTA_T are restored afterwards."""

@@ -227,7 +227,13 @@ int dg_timing_read(dg_handle *h, int i, char *name, int name_len, int64_t *launc
  * fastest and restores the state, TIME and DELTA_T; it allocates temporary
  * device copies of the state while it runs. */
 enum { DG_TUNE_COL_MT = 0, DG_TUNE_XROW_CHUNK = 1, DG_TUNE_YCHUNK = 2, DG_TUNE_CN_MT = 3,
-       DG_TUNE_PDL = 4 };
+       DG_TUNE_PDL = 4, DG_TUNE_WAIT_TEST = 5 };
+/* DG_TUNE_WAIT_TEST (test only): value > 0 makes the next Crank-Nicolson
+ * column launch give up on its bulk-copy barrier after `value` polls, with
+ * the barrier expecting 16 bytes more than its copies bring (every copy
+ * lands; nothing faults).  The kernel skips its work and the next
+ * diablo_synchronize / diablo_stats returns DG_ERR_TIMEOUT once.  The
+ * setting clears after that one launch. */
 int dg_tune_set(dg_handle *h, int key, int value);
 int dg_tune_get(dg_handle *h, int key, int *value);
 int dg_autotune(dg_handle *h, int steps_per_trial);
@@ -240,8 +246,12 @@ int dg_autotune(dg_handle *h, int steps_per_trial);
  * scratch is a fixed DG_NOALLOC_SCRATCH_BYTES array in the library's device
  * image, held by every GPU that loads the library until exit; one NX x NZ
  * plane must fit in it (about 1.75 MB at 512 x 384), otherwise DG_ERR_DIMS.
- * The first call on a device looks up the array's address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * The first call in a CUDA context (per device: its primary context, or
+ * another context the caller made current) looks up the array's address
+ * (cudaGetSymbolAddress) and keeps it for that context; make that first call
+ * before any stream capture.  V and VV must be device or managed memory of
+ * the current device (checked with cudaPointerGetAttributes; otherwise
+ * DG_ERR_ARG before anything is queued).
  * Work is queued on `stream` (NULL: the default stream) and the call
  * returns without waiting.  All calls share the scratch: calls that overlap
  * on the GPU race.  V and VV may alias. */

@@ -179,17 +179,11 @@ def test_mixed_periodic_64_cubed_100_steps():
     g.close()
 
 
-def test_mixed_periodic_256_cubed_and_scalar():
+def test_mixed_periodic_scalar_background_gradient():
+    """(The 256^3 configuration itself runs 200 steps against the oracle in
+    test_gpu_full_configs.py.)"""
     import math
     from diablo_b200.params import Params
-    p, _ = configs.periodic_256()
-    ref, g = periodic_pair(p)
-    for s in range(1, 6):
-        ref.step(s)
-        g.steps(s, 1)
-    err = {nm: rel(g.get_field(nm), ref.get(nm)) for nm in fields(p)}
-    assert all(v <= TOL_MIXED for v in err.values()), err
-    g.close()
     q = Params(nx=32, ny=48, nz=32, n_th=1, num_per_dir=3, nu=0.01, lx=2 * math.pi,
                ly=2 * math.pi, lz=2 * math.pi, delta_t=0.005)
     q.ri = [0.2, 0, 0, 0]

@@ -198,21 +198,6 @@ def test_periodic_variants(variant):
     g.close()
 
 
-def test_periodic_256_cubed_parity():
-    """The 256^3 decaying configuration, 5 steps from the seeded spectrum."""
-    p, _ = configs.periodic_256()
-    ref, g = seeded_pair(p)
-    for s in range(1, 6):
-        ref.step(s)
-        g.step(s)
-    for nm in fields(p):
-        assert rel(g.get_field(nm), ref.get(nm)) <= TOL, nm
-    so, sg = ref.stats(), g.stats()
-    assert abs(sg["ke"] - so["ke"]) <= 1e-12 * so["ke"]
-    assert sg["div_max"] <= 1e-12 * 256
-    g.close()
-
-
 def test_graph_steps_match_substep_calls():
     p = box((32, 32, 32), n_th=1)
     p.ri = [0.2, 0, 0, 0]

@@ -1,5 +1,5 @@
 """The allocation-free FFT_XZ_TO_FOURIER entry point against the
-handle-based one, through the C-ABI (needs a B200).
+handle-based one and the CPU oracle, through the C-ABI (needs a B200).
 
 Collected last on purpose: it shares one fixed device array across calls,
 and the two calls below run back to back on it with different sizes.
@@ -9,6 +9,7 @@ import ctypes
 import numpy as np
 import pytest
 
+import oracle as O
 from diablo_b200 import _lib
 from diablo_b200.grid import uniform_grid
 from diablo_b200.params import Params
@@ -55,6 +56,17 @@ def test_noalloc_matches_handle_entry_point_two_calls():
         if inplace:
             assert np.array_equal(got[0], V.view(np.complex128)[0])
             assert np.array_equal(got[ny + 1], V.view(np.complex128)[ny + 1])
+        if nx * nz <= 48 * 96:
+            # the small case also against the CPU oracle's FFT_XZ_TO_FOURIER:
+            # the retained block of every written plane, and zeros elsewhere
+            ref = O.Oracle(p, uniform_grid(ny, -1.0, 1.0))
+            spec = ref.to_fourier(np.ascontiguousarray(V[:, :nz, :nx]))
+            ref.close()
+            blk = got[planes][:, : p.tnkz + 1, : p.nkx + 1]
+            assert rel(blk, spec[planes]) < 1e-14
+            full = np.zeros_like(got[planes])
+            full[:, : p.tnkz + 1, : p.nkx + 1] = spec[planes]
+            assert rel(got[planes], full) < 1e-14
 
 
 def test_noalloc_rejects_planes_beyond_its_scratch():
@@ -67,3 +79,14 @@ def test_noalloc_rejects_planes_beyond_its_scratch():
     code = L.diablo_fft_xz_to_fourier_noalloc(ptr, ptr, 4096, 4096, 8, 0, 9, None)
     assert code == 2  # DG_ERR_DIMS
     assert b"DG_NOALLOC_SCRATCH_BYTES" in L.dg_last_error()
+
+
+def test_noalloc_rejects_host_memory():
+    """A host pointer would fault inside the kernels; the call refuses it
+    before anything is queued."""
+    L = _lib.load()
+    host = np.zeros((11, 18, 34))
+    hp = ctypes.c_void_p(host.ctypes.data)
+    code = L.diablo_fft_xz_to_fourier_noalloc(hp, hp, 32, 16, 9, 0, 10, None)
+    assert code == 1  # DG_ERR_ARG
+    assert b"device" in L.dg_last_error()

@@ -272,8 +272,10 @@ def run_ensemble(args, dist=None, ws=1, rank=0):
     {16,32,64}, NY in {33,65,129} (uniform on [-10,10]), Re ~ U[500,5000],
     Ri ~ U[0.05,0.25], seeded 1e-3 noise, Poisson arrivals at `rate`/s, each
     run for `steps` RK3 steps in mixed precision under a 150 GB budget through
-    the continuous-batching server.  Beside it, the plain per-case FP64 path
-    (one case at a time, graph-replayed steps) on a sample of the same cases.
+    the continuous-batching server (grouped stepping with ragged column
+    launches, and every case on its own stream).  Beside it, the plain
+    per-case FP64 path (one case at a time, graph-replayed steps) over the
+    same workload: every grid shape timed alone.
     Under torchrun every rank serves the cases the host-side dispatcher gives
     it (whole cases, no data exchanged) and the ranks pool their statistics."""
     import torch
@@ -290,78 +292,106 @@ def run_ensemble(args, dist=None, ws=1, rank=0):
     arrivals = np.cumsum(rng.exponential(1.0 / args.ensemble_rate, len(cases)))
     mine = [i for i, r in enumerate(assign_cases(
         [q.nx * q.ny * q.nz * args.ensemble_steps for q, _ in cases], ws)) if r == rank]
-    # plain per-case FP64 path on a sample: device time of each case alone
-    sample = cases[: min(16, len(cases))]
-    plain_pts, plain_s = 0.0, 0.0
+    # plain per-case FP64 path, size-stratified: every one of the 27 grid
+    # shapes timed alone (graph-replayed steps, device time), then the plain
+    # time of the whole workload is the sum over the cases of their shape's
+    # step time (the step cost does not depend on Re or Ri at fixed dt)
+    shape_ms = {}
     psteps = min(args.ensemble_steps, 100)
-    for i, (q, gy) in enumerate(sample if rank == 0 else []):
-        st = torch.cuda.Stream()
-        ch = Channel(q, gy, stream=st.cuda_stream)
-        for k, v in ics.kh_state(q, gy, seed=100 + i).items():
-            ch.set_field(k, v)
-        ch.set_time(0.0, q.delta_t)
-        ch.apply_bc_vel()
-        ch.rem_div_chan()
-        ch.apply_bc_vel()
-        ch.steps(1, 3)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        ch.steps(4, psteps)
-        e1.record(st)
-        e1.synchronize()
-        plain_s += e0.elapsed_time(e1) * 1e-3
-        plain_pts += q.nx * q.ny * q.nz * psteps
-        ch.close()
-    plain = plain_pts / plain_s / 1e6 if plain_s > 0 else None
-    # served, mixed precision, continuous batching; every rank starts its
-    # clock together so the shared arrival process lines up across ranks
-    if dist:
-        dist.barrier()
-    srv = Server(max_active=args.ensemble_active, budget_gb=150.0, autotune=True)
-    t0 = time.perf_counter()
-    ids = []
-    for i in mine:
-        q, gy = cases[i]
-        st0 = ics.kh_state(q, gy, seed=100 + i)
-        delay = t0 + arrivals[i] - time.perf_counter()
-        if delay > 0:
-            time.sleep(delay)
-        ids.append(srv.submit(q.replace(precision=1), gy, st0, args.ensemble_steps))
-    lat = []
-    for cid in ids:
-        _, (qs, rs) = srv.wait(cid)
-        lat.append(qs + rs)
-    wall = time.perf_counter() - t0
-    s = srv.stats()
-    srv.close()
-    rec = {"wall_s": s["wall_s"] if mine else 0.0, "cases": len(mine),
-           "points": sum(cases[i][0].nx * cases[i][0].ny * cases[i][0].nz for i in mine)
-           * args.ensemble_steps,
-           "case_latency_s": lat, "step_ms_p50": s["step_ms_p50"], "step_ms_p99": s["step_ms_p99"],
-           "hbm_peak_gb": s["bytes_peak"] / 1e9}
-    if dist:
-        allrec = [None] * ws
-        dist.all_gather_object(allrec, rec)
-    else:
-        allrec = [rec]
-    m = merge_rank_stats(allrec)
+    if rank == 0:
+        for nx in (64, 128, 256):
+            for ny in (33, 65, 129):
+                for nz in (16, 32, 64):
+                    q = base.replace(nx=nx, ny=ny, nz=nz)
+                    gy = uniform_grid(ny, -10.0, 10.0)
+                    st = torch.cuda.Stream()
+                    ch = Channel(q, gy, stream=st.cuda_stream)
+                    for k, v in ics.kh_state(q, gy, seed=7).items():
+                        ch.set_field(k, v)
+                    ch.set_time(0.0, q.delta_t)
+                    ch.apply_bc_vel()
+                    ch.rem_div_chan()
+                    ch.apply_bc_vel()
+                    ch.steps(1, 3)
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(st)
+                    ch.steps(4, psteps)
+                    e1.record(st)
+                    e1.synchronize()
+                    shape_ms[(nx, ny, nz)] = e0.elapsed_time(e1) / psteps
+                    ch.close()
+    plain = None
+    if shape_ms:
+        pts = sum(q.nx * q.ny * q.nz for q, _ in cases)
+        secs = sum(shape_ms[(q.nx, q.ny, q.nz)] * 1e-3 for q, _ in cases)
+        plain = pts / secs / 1e6
+
+    def serve(group):
+        # served, mixed precision, continuous batching; every rank starts its
+        # clock together so the shared arrival process lines up across ranks
+        if dist:
+            dist.barrier()
+        srv = Server(max_active=args.ensemble_active, budget_gb=150.0, autotune=True,
+                     group_cases=group)
+        t0 = time.perf_counter()
+        ids = []
+        for i in mine:
+            q, gy = cases[i]
+            st0 = ics.kh_state(q, gy, seed=100 + i)
+            delay = t0 + arrivals[i] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            ids.append(srv.submit(q.replace(precision=1), gy, st0, args.ensemble_steps))
+        lat = []
+        for cid in ids:
+            _, (qs, rs) = srv.wait(cid)
+            lat.append(qs + rs)
+        wall = time.perf_counter() - t0
+        s = srv.stats()
+        srv.close()
+        rec = {"wall_s": s["wall_s"] if mine else 0.0, "cases": len(mine),
+               "points": sum(cases[i][0].nx * cases[i][0].ny * cases[i][0].nz for i in mine)
+               * args.ensemble_steps,
+               "case_latency_s": lat, "step_ms_p50": s["step_ms_p50"], "step_ms_p99": s["step_ms_p99"],
+               "hbm_peak_gb": s["bytes_peak"] / 1e9}
+        if dist:
+            allrec = [None] * ws
+            dist.all_gather_object(allrec, rec)
+        else:
+            allrec = [rec]
+        m = merge_rank_stats(allrec)
+        out = {"cases_per_s": m["cases_per_s"], "step_ms_p50": m["step_ms_p50_worst_rank"],
+               "step_ms_p99": m["step_ms_p99_worst_rank"],
+               "mpoint_steps_per_s": m["mpoint_steps_per_s"],
+               "case_latency_s_p50": m["case_latency_s_p50"],
+               "case_latency_s_p99": m["case_latency_s_p99"],
+               "hbm_peak_gb": m["hbm_peak_gb_max"], "wall_s": wall}
+        if plain and ws == 1:
+            out["served_over_plain"] = m["mpoint_steps_per_s"] / plain
+        elif plain:
+            out["served_per_gpu_over_plain"] = m["mpoint_steps_per_s"] / ws / plain
+        return out
+
+    grouped = serve(args.ensemble_group)
+    alone = serve(0) if args.ensemble_group else None
     out = {"cases": len(cases), "steps_per_case": args.ensemble_steps,
            "arrival_rate_per_s": args.ensemble_rate, "max_active": args.ensemble_active,
            "gpus": ws, "dispatch": "whole cases per GPU, longest first to the least-loaded GPU",
            "precision": "mixed (FP32 transforms and products, FP64 solves)",
-           "cases_per_s": m["cases_per_s"], "step_ms_p50": m["step_ms_p50_worst_rank"],
-           "step_ms_p99": m["step_ms_p99_worst_rank"],
-           "mpoint_steps_per_s": m["mpoint_steps_per_s"],
-           "case_latency_s_p50": m["case_latency_s_p50"],
-           "case_latency_s_p99": m["case_latency_s_p99"],
-           "hbm_peak_gb": m["hbm_peak_gb_max"], "wall_s": wall,
+           "group_cases": args.ensemble_group,
+           "stepping": (f"groups of up to {args.ensemble_group} cases of similar size, one graph "
+                        "per group step, one ragged column launch per substep"
+                        if args.ensemble_group else "every case on its own stream"),
            "plain_fp64_mpoint_steps_per_s": plain,
-           "plain_sample": f"{len(sample)} of the cases alone on one GPU, {psteps} steps each, FP64"}
-    if plain and ws == 1:
-        out["served_over_plain"] = m["mpoint_steps_per_s"] / plain
-    elif plain:
-        out["served_per_gpu_over_plain"] = m["mpoint_steps_per_s"] / ws / plain
+           "plain_sample": (f"all 27 grid shapes alone on one GPU, {psteps} FP64 steps each; "
+                            "the workload's plain time is the sum over its cases of their "
+                            "shape's step time"),
+           "plain_shape_ms_per_step": {f"{a}x{b}x{c}": round(v, 4)
+                                       for (a, b, c), v in sorted(shape_ms.items())}}
+    out.update(grouped)
+    if alone is not None:
+        out["per_case_streams"] = alone
     return out
 
 
@@ -752,6 +782,8 @@ def main():
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--ensemble-rate", type=float, default=20.0)
     ap.add_argument("--ensemble-active", type=int, default=16)
+    ap.add_argument("--ensemble-group", type=int, default=4,
+                    help="cases per step group in the served ensemble (0: every case alone)")
     ap.add_argument("--les-only", default="", choices=["", "all"] + list(LES_CASES),
                     help="time only the LES workloads (all, or the one named; --steps "
                          "graph-replayed steps each, after --warmup) and print their records; "

@@ -98,7 +98,7 @@ def load(path: str = LIB_PATH):
         "dg_server_create": [I, D, I, ctypes.POINTER(P)],
         "dg_server_submit": [P, P, P, P, I, I, ctypes.POINTER(ctypes.c_int64)],
         "dg_server_wait": [P, ctypes.c_int64, P, P],
-        "dg_server_query": [P, P], "dg_server_destroy": [P],
+        "dg_server_query": [P, P], "dg_server_destroy": [P], "dg_server_config": [P, I, I],
         "dg_timing_read": [P, I, ctypes.c_char_p, I, ctypes.POINTER(ctypes.c_int64),
                            ctypes.POINTER(D)],
         "diablo_stats": [P, ctypes.POINTER(DgStats)],

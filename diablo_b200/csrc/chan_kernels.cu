@@ -393,15 +393,16 @@ __global__ void __launch_bounds__(XP_THR) k_xprod_f(
     float a = 0.f, b = 0.f;
 #pragma unroll
     for (int t = 0; t < 2; t++) {
+      // row means: exact products of the FP32 fluctuations, summed in FP64
       if (t < na) {
         const float l1 = lin_f(ta[t].l1, x), l2 = lin_f(ta[t].l2, x), ff = l1 * l2;
         a += (float)ta[t].sg * ((float)Da[t][0] * l2 + (float)Da[t][1] * l1 + ff);
-        sa += ta[t].sg * (double)ff;
+        sa = fma(ta[t].sg * (double)l1, (double)l2, sa);
       }
       if (t < nb) {
         const float l1 = lin_f(tb[t].l1, x), l2 = lin_f(tb[t].l2, x), ff = l1 * l2;
         b += (float)tb[t].sg * ((float)Db[t][0] * l2 + (float)Db[t][1] * l1 + ff);
-        sb += tb[t].sg * (double)ff;
+        sb = fma(tb[t].sg * (double)l1, (double)l2, sb);
       }
     }
     sig[pad(x)] = make_float2(a, b);
@@ -612,7 +613,10 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? (sizeof(CX) == 8 ? 4
 #pragma unroll
         for (int p = 0; p < NPROD; p++) {
           const float ff = L1f[p] * L2f[p];
-          acc[p] += (double)ff;
+          // the row mean takes the exact product of the FP32 fluctuations (48
+          // significant bits fit FP64) and sums it in FP64: no FP32 rounding
+          // enters the mean, whatever the row length
+          acc[p] = fma((double)L1f[p], (double)L2f[p], acc[p]);
           P[p] = (float)L1d[p] * L2f[p] + (float)L2d[p] * L1f[p] + ff;
         }
         if (2 * NPP > NPROD) P[2 * NPP - 1] = 0.0f;
@@ -733,7 +737,10 @@ size_t xw_smem() {
 constexpr int ZF_THR = 128;
 __host__ __device__ constexpr int zf_kxg(int nz) { return nz <= 128 ? 8 : (nz <= 256 ? 4 : 2); }
 
-template <int NT>
+// NLO: write only the nonlinear term -i kz A + B of every retained mode to
+// rhs (the column kernel forms the explicit terms and the right-hand side);
+// otherwise the epilogue below also forms CF and the CN right-hand side R.
+template <int NT, bool NLO>
 __global__ void __launch_bounds__(ZF_THR) k_zfwd_rhs(
     ChanConst C, const double2 *__restrict__ G, long Gfield, FftPlan pl,
     const double2 *__restrict__ tw, const double *__restrict__ dscal, int rk_step,
@@ -779,6 +786,22 @@ __global__ void __launch_bounds__(ZF_THR) k_zfwd_rhs(
       nl[(f * ZF_KXG + c) * nkzt + kp] = make_double2(KZ * a.y + b.x, -KZ * a.x + b.y);
     }
     __syncthreads();
+  }
+  if constexpr (NLO) {
+    for (int idx = tid; idx < ZF_KXG * nkzt; idx += nthr) {
+      const int c = idx % ZF_KXG, kp = idx / ZF_KXG;
+      const int kx = kx0 + c;
+      if (kx >= nkxp) continue;
+      const long o = (long)j * C.ss + (long)kp * nkxp + kx;
+      if (j >= C.JS && j <= C.JE) {
+        rhs(0)[o] = nl[(0 * ZF_KXG + c) * nkzt + kp];
+        rhs(2)[o] = nl[(2 * ZF_KXG + c) * nkzt + kp];
+      }
+      if (j >= 2 && j <= C.NY) rhs(1)[o] = nl[(1 * ZF_KXG + c) * nkzt + kp];
+      for (int n = 0; n < C.nth; n++)
+        if (j >= C.JSt[n] && j <= C.JEt[n]) rhs(3 + n)[o] = nl[((3 + n) * ZF_KXG + c) * nkzt + kp];
+    }
+    return;
   }
   // explicit terms and CN right-hand side per retained mode of plane j
   const double h = dscal[1 + rk_step];
@@ -908,7 +931,8 @@ size_t zw_smem(int nz) {
   return sizeof(CX) * (nz + 4 * 2 * zw_kpw(nz) * (size_t)padded_len(nz));
 }
 
-template <int NZ, typename CX = double2>
+// NLO as for k_zfwd_rhs: only -i kz A + B goes out, into rhs.
+template <int NZ, typename CX = double2, bool NLO = false>
 __global__ void __launch_bounds__(128, zw_minb(NZ, sizeof(CX))) k_zfwd_w(
     ChanConst C, const CX *__restrict__ G, long Gfield, const CX *__restrict__ tw,
     const double *__restrict__ dscal, int rk_step, const double *__restrict__ kxv,
@@ -987,6 +1011,10 @@ __global__ void __launch_bounds__(128, zw_minb(NZ, sizeof(CX))) k_zfwd_w(
     const double KX = kxv[kx], KZ = kzv[kp];
     const double2 nlv = make_double2(KZ * a.y + b.x, -KZ * a.x + b.y);  // -i kz A + B
     const long o = (long)j * ss + (long)kp * nkxp + kx;
+    if constexpr (NLO) {
+      rhs(f)[o] = nlv;
+      continue;
+    }
     const double k2 = KX * KX + KZ * KZ;
     const double kk = (C.beta == 1.0) ? k2 : pow(k2, C.beta);
     const bool mean = (kx == 0 && kp == 0);
@@ -1933,6 +1961,9 @@ int dg_dt_commit(dg_handle *h) {
 int dg_chan_init(dg_handle *h) {
   h->cn_maps = new CnMaps();
   h->cn_maps_mt = 0;
+  h->cs_maps = new CnMaps();
+  h->cs_maps_mt = 0;
+  DG_TRY(dg_col_init(h));
   dg_kt_begin(h, "k_remdiv_init", h->st);
   k_remdiv_init<<<dg_cdiv(h->ss, 128), 128, 0, h->st>>>(h->NY, h->ss, h->nkxp, h->kx, h->kz, h->dy,
                                                         h->dyf, h->rem_a, h->rem_rb);
@@ -1994,9 +2025,10 @@ static int nl_chunk_mixed(dg_handle *h, const ChanConst &C, int rk_step, int a, 
   done = false;
 #define ZW_CASE(N)                                                                              \
   if (!done && h->NZ == N) {                                                                    \
-    dg_big_smem((const void *)k_zfwd_w<N, float2>);                                             \
+    auto kern = h->zf_nlo ? k_zfwd_w<N, float2, true> : k_zfwd_w<N, float2, false>;             \
+    dg_big_smem((const void *)kern);                                                            \
     dg_kt_begin(h, "k_zfwd_w_f32", h->st);                                                      \
-    DG_CUDA(dg_launch(h->pdl, k_zfwd_w<N, float2>, zgrid, dim3(128), sm, h->st, C, Gf, Hfield,  \
+    DG_CUDA(dg_launch(h->pdl, kern, zgrid, dim3(128), sm, h->st, C, Gf, Hfield,                 \
                       h->twz_f, h->dscal, rk_step, h->kx, h->kz, h->dy, h->dyf, cu, cf, rhs,    \
                       h->cp, a));                                                               \
     done = true;                                                                                \
@@ -2072,9 +2104,10 @@ static int nl_generic_mixed(dg_handle *h, const ChanConst &C, int rk_step,
   const size_t sm = zw_smem<float2>(NZ);
 #define ZW_CASE(N)                                                                              \
   if (!done && NZ == N) {                                                                       \
-    dg_big_smem((const void *)k_zfwd_w<N, float2>);                                             \
+    auto kern = h->zf_nlo ? k_zfwd_w<N, float2, true> : k_zfwd_w<N, float2, false>;             \
+    dg_big_smem((const void *)kern);                                                            \
     dg_kt_begin(h, "k_zfwd_w_f32", h->st);                                                      \
-    DG_CUDA(dg_launch(h->pdl, k_zfwd_w<N, float2>, zgrid, dim3(128), sm, h->st, C, Gf, Hfield,  \
+    DG_CUDA(dg_launch(h->pdl, kern, zgrid, dim3(128), sm, h->st, C, Gf, Hfield,                 \
                       h->twz_f, h->dscal, rk_step, h->kx, h->kz, h->dy, h->dyf, cu, cf, rhs,    \
                       h->cp, 1));                                                               \
     done = true;                                                                                \
@@ -2090,8 +2123,12 @@ static int nl_generic_mixed(dg_handle *h, const ChanConst &C, int rk_step,
   return DG_OK;
 }
 
-extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
-  if (!h || h->periodic || rk_step < 1 || rk_step > 3) return DG_ERR_ARG;
+// Steps 1-3 of RK_CHAN_1 (and, with LES, the subgrid model and the LES
+// solves): everything before the per-mode column stage.  *column_next says
+// whether the column stage (dg_chan_column) must follow; LES substeps finish
+// here.
+int dg_chan_nonlinear(dg_handle *h, int time_step, int rk_step, bool *column_next) {
+  *column_next = false;
   const ChanConst C = make_const(h);
   // Steps 1-3 run over y-chunks of planes so the half-physical (H) and
   // product (G) planes a chunk produces are consumed while still in L2.
@@ -2110,6 +2147,9 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
   // Crank-Nicolson solves run on physical columns (for/channel.f:303,631)
   const bool sgs = dg_les_active(h, time_step);
   const bool les_solve = h->p.les && (sgs || h->les_nut);
+  // the z forward writes only the nonlinear terms unless the LES solves need
+  // the assembled right-hand side R and CF from it
+  h->zf_nlo = les_solve ? 0 : 1;
   if (sgs) DG_TRY(dg_les_pre(h, rk_step));
   if (h->mixed && !(xw_supported(h->NX) && h->NTH <= 2)) {
     DG_TRY(nl_generic_mixed(h, C, rk_step, in, cu, cf, rhs));
@@ -2190,9 +2230,10 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
       const size_t sm = zw_smem<double2>(h->NZ);
 #define ZW_CASE(N)                                                                             \
   if (h->NZ == N) {                                                                            \
-    dg_big_smem((const void *)k_zfwd_w<N>);                                                    \
+    auto kern = h->zf_nlo ? k_zfwd_w<N, double2, true> : k_zfwd_w<N, double2, false>;          \
+    dg_big_smem((const void *)kern);                                                           \
     dg_kt_begin(h, "k_zfwd_w", h->st);                                                          \
-    DG_CUDA(dg_launch(h->pdl, k_zfwd_w<N>, grid, dim3(128), sm, h->st, C, h->G, Hfield, h->twz, \
+    DG_CUDA(dg_launch(h->pdl, kern, grid, dim3(128), sm, h->st, C, h->G, Hfield, h->twz,       \
                       h->dscal, rk_step, h->kx, h->kz, h->dy, h->dyf, cu, cf, rhs, h->cp, za)); \
     zdone = true;                                                                              \
   }
@@ -2206,10 +2247,13 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
       dim3 grid(dg_cdiv(h->nkxp, zf_kxg(h->NZ)), h->NY);
       const size_t sm = zfwd_smem(h);
 #define KERNEL_BODY(N)                                                                          \
-  dg_big_smem((const void *)k_zfwd_rhs<N>);                                                     \
-  dg_kt_begin(h, "k_zfwd_rhs", h->st);                                                            \
-  k_zfwd_rhs<N><<<grid, ZF_THR, sm, h->st>>>(C, h->G, Hfield, h->plz, h->twz, h->dscal, rk_step, \
-                                             h->kx, h->kz, h->dy, h->dyf, cu, cf, rhs, h->cp)
+  {                                                                                             \
+    auto kern = h->zf_nlo ? k_zfwd_rhs<N, true> : k_zfwd_rhs<N, false>;                         \
+    dg_big_smem((const void *)kern);                                                            \
+    dg_kt_begin(h, "k_zfwd_rhs", h->st);                                                        \
+    kern<<<grid, ZF_THR, sm, h->st>>>(C, h->G, Hfield, h->plz, h->twz, h->dscal, rk_step,       \
+                                      h->kx, h->kz, h->dy, h->dyf, cu, cf, rhs, h->cp);         \
+  }
       switch (h->NZ) {
         DG_FOR_EACH_N(DG_CASE_N)
         default: KERNEL_BODY(0); break;
@@ -2220,22 +2264,39 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
     if (!done) break;  // the generic kernels covered every plane
   }
   if (les_solve) return dg_les_post(h, time_step, rk_step, sgs);
-  // 4. per-mode CN solves, then COURANT on the post-CN velocity
-  //    (for/channel.f:1037-1040), then REM_DIV_CHAN and CP += phi / H_BAR
-  DG_TRY(dg_cn_solve_dev(h, rk_step));
-  const bool cfl = h->p.variable_dt && rk_step == 3 && h->p.update_dt > 0 &&
-                   (time_step % h->p.update_dt) == 0;
-  if (cfl) {
-    // the reduction overlaps REM_DIV (which only waits for the z inverse of
-    // the velocity it overwrites)
-    const double2 *u[3] = {h->cu[0], h->cu[1], h->cu[2]};
-    DG_TRY(dg_courant_dev(h, u, true));
-  }
+  *column_next = true;
+  return DG_OK;
+}
+
+// COURANT runs in substep 3 at the UPDATE_DT cadence with variable DELTA_T
+bool dg_chan_cfl(const dg_handle *h, int time_step, int rk_step) {
+  return h->p.variable_dt && rk_step == 3 && h->p.update_dt > 0 &&
+         (time_step % h->p.update_dt) == 0;
+}
+
+// After a column stage that stopped at the CN solves: COURANT on the post-CN
+// velocity (for/channel.f:1037-1040), REM_DIV_CHAN and CP += phi / H_BAR
+// while COURANT's reduction finishes on the side stream, then the new
+// DELTA_T is committed.
+int dg_chan_cfl_tail(dg_handle *h, int rk_step) {
+  const double2 *u[3] = {h->cu[0], h->cu[1], h->cu[2]};
+  DG_TRY(dg_courant_dev(h, u, true));
   DG_TRY(dg_rem_div_dev(h, 1, rk_step));
-  if (cfl) {
-    DG_CUDA(cudaStreamWaitEvent(h->st, h->ev_cfl1, 0));
-    DG_TRY(dg_dt_commit(h));
-  }
+  DG_CUDA(cudaStreamWaitEvent(h->st, h->ev_cfl1, 0));
+  return dg_dt_commit(h);
+}
+
+extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
+  if (!h || h->periodic || rk_step < 1 || rk_step > 3) return DG_ERR_ARG;
+  bool column = false;
+  DG_TRY(dg_chan_nonlinear(h, time_step, rk_step, &column));
+  if (!column) return DG_OK;
+  // 4. per-mode column stage: explicit terms and right-hand sides, CN solves,
+  //    REM_DIV_CHAN and CP += phi / H_BAR in one kernel; with COURANT the
+  //    kernel stops after the CN solves and the tail above follows
+  const bool cfl = dg_chan_cfl(h, time_step, rk_step);
+  DG_TRY(dg_col_step_dev(h, rk_step, !cfl));
+  if (cfl) DG_TRY(dg_chan_cfl_tail(h, rk_step));
   return DG_OK;
 }
 

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <vector>
 
 #include "../../include/diablo_b200.h"
 
@@ -156,9 +157,14 @@ struct dg_handle {
   CnMaps *cn_maps;              // tensor maps of the CN right-hand sides (built per modes/CTA)
   int cn_maps_mt;               // modes per CTA the maps were built for (0: none)
   int col_mt;                   // modes per CTA of the REM_DIV column kernel (4, 8, 16)
-  int cn_mt;                    // modes per CTA of the CN column kernel (4, 8, 16)
+  int cn_mt;                    // modes per CTA of the column (CN) kernel (2, 4, 8, 16)
   int xrow_chunk;               // planes per CTA of the x-row product kernel (0 = auto)
   int ychunk;                   // planes per y-chunk of a substep (0 = all)
+  double *rowc;                 // per-row grid factors of the column kernel [8][NY+2]
+  CnMaps *cs_maps;              // tensor maps of CU for the column kernel
+  int cs_maps_mt;               // modes per CTA the maps were built for (0: none)
+  int zf_nlo;                   // the z forward writes only the nonlinear terms (the
+                                // column kernel assembles the right-hand sides)
   int wait_test;                // test only: poll limit of the next CN launch, whose
                                 // barrier then expects 16 bytes more than it receives
 
@@ -233,6 +239,18 @@ int dg_les_init(dg_handle *h);
 bool dg_les_active(const dg_handle *h, int time_step);
 int dg_les_pre(dg_handle *h, int rk_step);
 int dg_les_post(dg_handle *h, int time_step, int rk_step, bool sgs);
+int dg_chan_nonlinear(dg_handle *h, int time_step, int rk_step, bool *column_next);
+bool dg_chan_cfl(const dg_handle *h, int time_step, int rk_step);
+int dg_chan_cfl_tail(dg_handle *h, int rk_step);
+int dg_col_init(dg_handle *h);
+int dg_col_step_dev(dg_handle *h, int rk_step, bool rd);
+size_t dg_col_smem(const dg_handle *h, int mt, int *by_out, int *nbox_out);
+size_t dg_col_case_bytes();
+int dg_col_batch_build(dg_handle *const *hs, const int *rd, int n, int want_mt,
+                       std::vector<unsigned char> &cases, std::vector<int2> &work, int *mt_out,
+                       size_t *smem_out);
+int dg_col_batch_launch(cudaStream_t st, int mt, size_t smem, const void *dev_cases,
+                        const int2 *dev_work, int nwork, int rk_step);
 
 #define DG_CASE_N(N) \
   case N:            \

@@ -18,6 +18,20 @@
 // request: requests that arrive while others run are admitted as soon as a
 // slot and memory free up.  Step latency is the device time between events
 // recorded around each step on the case's stream.
+//
+// Grouped stepping (dg_server_config DG_SERVER_GROUP_CASES = G > 0): active
+// cases of similar size advance together in groups of up to G.  One RK3
+// step of a group is one CUDA graph: per substep, every member's transform
+// stage (z inverse, x-row products, z forward) runs on the member's own
+// stream, the members join, and ONE ragged column launch (k_col_step_ragged)
+// does the right-hand sides, CN solves and REM_DIV of every member's modes
+// -- a (case, mode tile) work list over all members -- before the members'
+// streams fork again.  Groups run concurrently on their own streams.  A
+// group is re-captured when a member joins or leaves (at step boundaries,
+// after the group's steps in flight have finished).  Results are the same
+// as per-case stepping: every mode's arithmetic is the single-case kernels'.
+// Cases that change their launch sequence from step to step (LES, COURANT
+// at an UPDATE_DT cadence other than every step) step alone as above.
 #include <math.h>
 #include <string.h>
 
@@ -70,6 +84,29 @@ struct Active {
 
 using ShapeKey = std::tuple<int, int, int, int, int>;
 
+// a case can join a group: its step's launch sequence is the same every step
+bool groupable(const dg_params &p) {
+  return !p.les && (!p.variable_dt || p.update_dt == 1);
+}
+
+struct Group {
+  std::vector<Active *> m;         // members (owned by the server's case list)
+  cudaStream_t gs = nullptr;       // the group's stream: graph launches, column launches
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_m;   // one per member: joins into gs
+  cudaEvent_t ev_col = nullptr;    // column launch done: members fork from it
+  void *d_cases[3] = {nullptr, nullptr, nullptr};  // case tables per substep (rd differs at 3)
+  int2 *d_work = nullptr;
+  int nwork = 0, mt = 0;
+  size_t smem = 0;
+  cudaGraphExec_t exec = nullptr;
+  long long gkernels = 0;
+  std::deque<InFlight> inflight;
+  std::vector<InFlight> pool;
+  bool dirty = true;               // membership changed: rebuild before the next step
+  double points = 0;               // mean points per member (grouping by size)
+};
+
 // field ids of the state a request carries: CU1..3, CP, CTH(n)
 std::vector<int> state_ids(const dg_params &p) {
   std::vector<int> ids = {DG_CU1, DG_CU2, DG_CU3, DG_CP};
@@ -84,8 +121,13 @@ size_t compact_len(const dg_params &p) {
 
 }  // namespace
 
+struct dg_server;
+void dg_server_run_grouped(dg_server *s);
+
 struct dg_server {
   int max_active = 8;
+  int group_cases = 0;            // > 0: grouped stepping with up to this many cases per group
+  bool submitted = false;
   int64_t budget = 0;
   int autotune = 1;
   std::mutex mu;
@@ -176,8 +218,9 @@ struct dg_server {
       a.pool.push_back(f);
     }
     // the first steps run here: the first is eager, the second captures the
-    // case's step graph
-    const int warm = r->nsteps < 2 ? r->nsteps : 2;
+    // case's step graph (a case that will step in a group runs one eager step)
+    const bool grouped = group_cases > 0 && groupable(r->p);
+    const int warm = r->nsteps < (grouped ? 1 : 2) ? r->nsteps : (grouped ? 1 : 2);
     code = diablo_step(a.h, 1, warm);
     if (code == DG_OK && cudaStreamSynchronize(a.st) != cudaSuccess) code = DG_ERR_CUDA;
     if (code != DG_OK) {
@@ -280,6 +323,15 @@ struct dg_server {
   // active case in flight
   void loop() {
     cudaSetDevice(device);
+    {
+      // the mode is fixed by the first submit (dg_server_config comes before it)
+      std::unique_lock<std::mutex> lk(mu);
+      cv_step.wait(lk, [&] { return submitted || stop; });
+    }
+    if (group_cases > 0) {
+      dg_server_run_grouped(this);
+      return;
+    }
     for (;;) {
       {
         std::unique_lock<std::mutex> lk(mu);
@@ -346,6 +398,373 @@ struct dg_server {
   }
 };
 
+// ------------------------------------------------------ grouped stepping
+struct GroupedLoop {
+  dg_server *s;
+  std::vector<std::unique_ptr<Active>> cases;  // every active case
+  std::vector<std::unique_ptr<Group>> groups;
+  std::vector<Active *> solo;                   // cases that step alone
+
+  explicit GroupedLoop(dg_server *sv) : s(sv) {}
+
+  static double pts(const Active *a) { return (double)a->r->p.nx * a->r->p.ny * a->r->p.nz; }
+
+  void free_graph(Group &g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    for (void *&d : g.d_cases) {
+      if (d) cudaFree(d);
+      d = nullptr;
+    }
+    if (g.d_work) cudaFree(g.d_work);
+    g.d_work = nullptr;
+  }
+
+  Group *new_group() {
+    auto g = std::make_unique<Group>();
+    cudaStreamCreateWithFlags(&g->gs, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&g->ev_col, cudaEventDisableTiming);
+    for (int k = 0; k < 2; k++) {
+      InFlight f;
+      cudaEventCreate(&f.e0);
+      cudaEventCreate(&f.e1);
+      g->pool.push_back(f);
+    }
+    groups.push_back(std::move(g));
+    return groups.back().get();
+  }
+
+  void destroy_group(size_t gi) {
+    Group &g = *groups[gi];
+    cudaStreamSynchronize(g.gs);
+    free_graph(g);
+    for (cudaEvent_t e : g.ev_m) cudaEventDestroy(e);
+    for (InFlight &f : g.pool) {
+      cudaEventDestroy(f.e0);
+      cudaEventDestroy(f.e1);
+    }
+    cudaEventDestroy(g.ev_fork);
+    cudaEventDestroy(g.ev_col);
+    cudaStreamDestroy(g.gs);
+    groups.erase(groups.begin() + gi);
+  }
+
+  // join a group of similar size with room, else open one
+  void place(Active *a) {
+    if (!groupable(a->r->p)) {
+      solo.push_back(a);
+      return;
+    }
+    Group *best = nullptr;
+    double bd = 1e30;
+    for (auto &g : groups) {
+      if ((int)g->m.size() >= s->group_cases) continue;
+      const double d = fabs(log(pts(a) / g->points));
+      if (d < log(4.0) && d < bd) {
+        bd = d;
+        best = g.get();
+      }
+    }
+    if (!best) best = new_group();
+    best->m.push_back(a);
+    double sum = 0;
+    for (Active *x : best->m) sum += pts(x);
+    best->points = sum / best->m.size();
+    best->dirty = true;
+  }
+
+  // one RK3 step of every member (captured into the group's graph)
+  int step_body(Group &g) {
+    const int n = (int)g.m.size();
+    DG_CUDA(cudaEventRecord(g.ev_fork, g.gs));
+    for (Active *a : g.m) DG_CUDA(cudaStreamWaitEvent(a->st, g.ev_fork, 0));
+    for (Active *a : g.m) {
+      dg_handle *h = a->h;
+      h->defer_tables = true;
+      if (h->p.variable_dt) {
+        // the CN tables of the DELTA_T the previous step committed
+        DG_CUDA(cudaEventRecord(h->ev_fork, h->st));
+        DG_CUDA(cudaStreamWaitEvent(h->st2, h->ev_fork, 0));
+        cudaStream_t keep = h->st;
+        h->st = h->st2;
+        const int st = dg_cn_tables(h);
+        h->st = keep;
+        DG_TRY(st);
+        DG_CUDA(cudaEventRecord(h->ev_join, h->st2));
+        h->tables_pending = true;
+      }
+    }
+    for (int rk = 1; rk <= 3; rk++) {
+      for (int c = 0; c < n; c++) {
+        dg_handle *h = g.m[c]->h;
+        bool col = false;
+        DG_TRY(dg_chan_nonlinear(h, 2, rk, &col));
+        if (h->tables_pending) {
+          DG_CUDA(cudaStreamWaitEvent(h->st, h->ev_join, 0));
+          h->tables_pending = false;
+        }
+        DG_CUDA(cudaEventRecord(g.ev_m[c], h->st));
+        DG_CUDA(cudaStreamWaitEvent(g.gs, g.ev_m[c], 0));
+      }
+      DG_TRY(dg_col_batch_launch(g.gs, g.mt, g.smem, g.d_cases[rk - 1], g.d_work, g.nwork, rk));
+      DG_CUDA(cudaEventRecord(g.ev_col, g.gs));
+      for (Active *a : g.m) {
+        dg_handle *h = a->h;
+        DG_CUDA(cudaStreamWaitEvent(h->st, g.ev_col, 0));
+        if (dg_chan_cfl(h, 2, rk)) DG_TRY(dg_chan_cfl_tail(h, rk));
+      }
+    }
+    for (int c = 0; c < n; c++) {
+      dg_handle *h = g.m[c]->h;
+      h->defer_tables = false;
+      DG_TRY(diablo_advance_time(h));
+      DG_CUDA(cudaEventRecord(g.ev_m[c], h->st));
+      DG_CUDA(cudaStreamWaitEvent(g.gs, g.ev_m[c], 0));
+    }
+    return DG_OK;
+  }
+
+  // tables, work list and graph for the current members (group idle)
+  int rebuild(Group &g) {
+    free_graph(g);
+    for (cudaEvent_t e : g.ev_m) cudaEventDestroy(e);
+    g.ev_m.assign(g.m.size(), nullptr);
+    for (cudaEvent_t &e : g.ev_m) DG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    std::vector<dg_handle *> hs;
+    for (Active *a : g.m) {
+      hs.push_back(a->h);
+      if (a->h->tables_pending) {
+        DG_CUDA(cudaStreamWaitEvent(a->h->st, a->h->ev_join, 0));
+        a->h->tables_pending = false;
+      }
+      DG_CUDA(cudaStreamSynchronize(a->h->st));
+    }
+    int want = 16;
+    for (dg_handle *h : hs) want = std::min(want, h->cn_mt);
+    for (int rk = 1; rk <= 3; rk++) {
+      std::vector<int> rd;
+      for (dg_handle *h : hs) rd.push_back(dg_chan_cfl(h, 2, rk) ? 0 : 1);
+      std::vector<unsigned char> tab;
+      std::vector<int2> work;
+      DG_TRY(dg_col_batch_build(hs.data(), rd.data(), (int)hs.size(), want, tab, work, &g.mt,
+                                &g.smem));
+      DG_CUDA(cudaMalloc(&g.d_cases[rk - 1], tab.size()));
+      DG_CUDA(cudaMemcpy(g.d_cases[rk - 1], tab.data(), tab.size(), cudaMemcpyHostToDevice));
+      if (rk == 1) {
+        g.nwork = (int)work.size();
+        DG_CUDA(cudaMalloc((void **)&g.d_work, sizeof(int2) * work.size()));
+        DG_CUDA(cudaMemcpy(g.d_work, work.data(), sizeof(int2) * work.size(),
+                           cudaMemcpyHostToDevice));
+      }
+    }
+    DG_CUDA(cudaStreamBeginCapture(g.gs, cudaStreamCaptureModeThreadLocal));
+    for (dg_handle *h : hs) h->capturing = true;
+    const long long k0 = dg_kernel_launches();
+    const int st = step_body(g);
+    g.gkernels = dg_kernel_launches() - k0;
+    for (dg_handle *h : hs) h->capturing = false;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(g.gs, &graph);
+    if (st != DG_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    if (e != cudaSuccess) {
+      dg_set_error((std::string("group graph capture: ") + cudaGetErrorString(e)).c_str());
+      return DG_ERR_CUDA;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+      g.exec = nullptr;
+      dg_set_error((std::string("group graph instantiate: ") + cudaGetErrorString(ei)).c_str());
+      return DG_ERR_CUDA;
+    }
+    g.dirty = false;
+    return DG_OK;
+  }
+
+  void retire_case(Active *a) {
+    // the server's retire() works on its `active` vector: hand it over
+    s->active.push_back(std::move(*a));
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->retire(s->active.size() - 1);
+    for (size_t i = 0; i < cases.size(); i++)
+      if (cases[i].get() == a) {
+        cases.erase(cases.begin() + i);
+        break;
+      }
+    s->n_active = (int)cases.size();
+    s->cv_work.notify_all();
+  }
+
+  void fail_group(Group &g, int code) {
+    const std::string msg = dg_last_error();
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (Active *a : g.m) s->fail(*a, code, msg.c_str());
+  }
+
+  void run() {
+    for (;;) {
+      bool progressed = false;
+      {
+        std::unique_lock<std::mutex> lk(s->mu);
+        if (cases.empty() && s->ready.empty()) {
+          s->cv_step.wait(lk, [&] {
+            return !s->ready.empty() || (s->stop && s->queue.empty() && s->preparing == 0);
+          });
+          if (s->ready.empty() && s->stop && s->queue.empty() && s->preparing == 0) return;
+        }
+        while (!s->ready.empty()) {
+          cases.push_back(std::make_unique<Active>(std::move(s->ready.front())));
+          s->ready.pop_front();
+          place(cases.back().get());
+          progressed = true;
+        }
+        s->n_active = (int)cases.size();
+      }
+      // groups: collect finished steps, retire members that are done,
+      // rebuild changed groups once idle, keep two steps in flight
+      for (size_t gi = 0; gi < groups.size();) {
+        Group &g = *groups[gi];
+        while (!g.inflight.empty() && cudaEventQuery(g.inflight.front().e1) == cudaSuccess) {
+          InFlight f = g.inflight.front();
+          g.inflight.pop_front();
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, f.e0, f.e1);
+          {
+            std::lock_guard<std::mutex> lk(s->mu);
+            for (Active *a : g.m) {
+              s->step_ms.push_back(ms);
+              s->steps_done++;
+              s->point_steps += pts(a);
+            }
+          }
+          for (Active *a : g.m) a->completed++;
+          g.pool.push_back(f);
+          progressed = true;
+        }
+        if (g.inflight.empty()) {
+          // members that are done (or failed) leave the group
+          for (size_t k = 0; k < g.m.size();) {
+            Active *a = g.m[k];
+            if (a->r->status != 2 || a->completed >= a->r->nsteps) {
+              g.m.erase(g.m.begin() + k);
+              g.dirty = true;
+              retire_case(a);
+              progressed = true;
+            } else {
+              k++;
+            }
+          }
+          if (g.m.empty()) {
+            destroy_group(gi);
+            continue;
+          }
+          if (g.dirty) {
+            const int code = rebuild(g);
+            if (code != DG_OK) {
+              fail_group(g, code);  // its members leave at the next pass
+              gi++;
+              continue;
+            }
+            progressed = true;
+          }
+        }
+        if (!g.dirty) {
+          int left = 1 << 30;
+          for (Active *a : g.m) left = std::min(left, a->r->nsteps - a->launched);
+          while (left > 0 && !g.pool.empty()) {
+            InFlight f = g.pool.back();
+            g.pool.pop_back();
+            cudaEventRecord(f.e0, g.gs);
+            const cudaError_t e = cudaGraphLaunch(g.exec, g.gs);
+            cudaEventRecord(f.e1, g.gs);
+            g.inflight.push_back(f);
+            dg_count_launch((int)g.gkernels);
+            for (Active *a : g.m) a->launched++;
+            left--;
+            progressed = true;
+            if (e != cudaSuccess) {
+              dg_set_error((std::string("group graph launch: ") + cudaGetErrorString(e)).c_str());
+              fail_group(g, DG_ERR_CUDA);
+              break;
+            }
+          }
+        }
+        gi++;
+      }
+      // cases that step alone: as in dg_server::loop
+      for (size_t i = 0; i < solo.size();) {
+        Active &a = *solo[i];
+        while (!a.inflight.empty() && cudaEventQuery(a.inflight.front().e1) == cudaSuccess) {
+          InFlight f = a.inflight.front();
+          a.inflight.pop_front();
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, f.e0, f.e1);
+          {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->step_ms.push_back(ms);
+            s->steps_done++;
+            s->point_steps += pts(&a);
+          }
+          a.pool.push_back(f);
+          a.completed++;
+          progressed = true;
+        }
+        if (a.r->status != 2 || a.completed >= a.r->nsteps) {
+          if (a.inflight.empty()) {
+            solo.erase(solo.begin() + i);
+            retire_case(&a);
+            progressed = true;
+            continue;
+          }
+        } else {
+          while (a.launched < a.r->nsteps && !a.pool.empty()) {
+            InFlight f = a.pool.back();
+            a.pool.pop_back();
+            cudaEventRecord(f.e0, a.st);
+            const int code = diablo_step(a.h, a.launched + 1, 1);
+            cudaEventRecord(f.e1, a.st);
+            a.inflight.push_back(f);
+            a.launched++;
+            progressed = true;
+            if (code != DG_OK) {
+              std::lock_guard<std::mutex> lk(s->mu);
+              s->fail(a, code, dg_last_error());
+              break;
+            }
+          }
+        }
+        i++;
+      }
+      if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+  }
+};
+
+void dg_server_run_grouped(dg_server *s) {
+  cudaSetDevice(s->device);
+  GroupedLoop gl(s);
+  gl.run();
+}
+
+extern "C" int dg_server_config(dg_server *s, int key, int value) {
+  if (!s) return DG_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->submitted) {
+    dg_set_error("dg_server_config must come before the first submit");
+    return DG_ERR_ARG;
+  }
+  if (key == DG_SERVER_GROUP_CASES) {
+    if (value < 0 || value > 64) return DG_ERR_ARG;
+    s->group_cases = value;
+    return DG_OK;
+  }
+  return DG_ERR_ARG;
+}
+
 extern "C" int dg_server_create(int max_active, double hbm_budget_gb, int autotune,
                                 dg_server **out) {
   if (!out || max_active < 1) return DG_ERR_ARG;
@@ -384,11 +803,13 @@ extern "C" int dg_server_submit(dg_server *s, const dg_params *p, const double *
   {
     std::lock_guard<std::mutex> lk(s->mu);
     r->id = s->next_id++;
+    s->submitted = true;
     if (s->t_first_submit < 0) s->t_first_submit = r->t_submit;
     s->all[r->id] = r;
     s->queue.push_back(r);
   }
   s->cv_work.notify_one();
+  s->cv_step.notify_all();
   *id = r->id;
   return DG_OK;
 }

@@ -207,6 +207,7 @@ extern "C" int64_t dg_state_bytes(const dg_params *p) {
     const int64_t hsz = planes * p->nz * nkxp;
     b += 16 * ns + 8 * 2 * ns;                              // gphi, rem_a, rem_rb
     b += 8 * 3 * (3 + DG_MAX_TH) * 5 * L + 8 * nf * 8 * L;  // cn_tab, cn_rows
+    b += 8 * 8 * L;                                          // rowc
     b += 16 * hsz * nf + 16 * hsz * 2 * nf;                 // H, G
     int64_t w = 8 * L * p->nz * p->nx * (nf > 3 ? nf : 3);
     if (w < 8 * 8 * L) w = 8 * 8 * L;
@@ -249,7 +250,8 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
   h->nspec = h->ss * h->nplanes;
   h->nf = 3 + h->NTH;
   h->col_mt = dg_default_col_mt(h);
-  h->cn_mt = h->col_mt;
+  h->cn_mt = 4;
+  h->zf_nlo = 1;
   h->pdl = 1;
   h->pi = 4.0 * atan(1.0);
   h->eps = (double)(float)0.000000001;  // default-real literal, for/fft.f:74
@@ -412,7 +414,7 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
   cudaStreamSynchronize(h->st);
   cudaStreamSynchronize(h->st2);
   void *dp[] = {h->gyf, h->dy, h->dyf, h->kx, h->kz, h->ky, h->kx2, h->kz2, h->ky2, h->twx, h->twz,
-                h->twy, h->twx_f, h->twz_f, h->twy_f, h->dscal, h->cp, h->cr1, h->gphi, h->rem_a, h->rem_rb, h->cn_tab, h->cn_rows, h->H, h->G, h->work, h->dmin_bits, h->dflag, h->Hy, h->P,
+                h->twy, h->twx_f, h->twz_f, h->twy_f, h->dscal, h->cp, h->cr1, h->gphi, h->rem_a, h->rem_rb, h->cn_tab, h->cn_rows, h->rowc, h->H, h->G, h->work, h->dmin_bits, h->dflag, h->Hy, h->P,
                 h->Q};
   for (void *q : dp) dg_free(h, q);
   dg_free(h, h->les_phys);
@@ -432,6 +434,7 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
   dg_graphs_free(h);
   free(h->h_ubar);
   delete h->cn_maps;
+  delete h->cs_maps;
   cudaEventDestroy(h->ev_fork);
   cudaEventDestroy(h->ev_join);
   cudaEventDestroy(h->ev_cfl0);

@@ -1,11 +1,14 @@
 // Tunable launch shapes of the channel substep and the autotuner that picks
 // them by timing.
 //
-//   DG_TUNE_COL_MT      modes per CTA of the REM_DIV column kernel (k_rd_col),
-//   DG_TUNE_CN_MT       and of the CN column kernel (k_cn_col): 4, 8 or 16.
-//                       Fewer modes per CTA means more CTAs resident per SM to
-//                       hide the column loads; more means more sweep lanes per
-//                       CTA.
+//   DG_TUNE_COL_MT      modes per CTA of the REM_DIV column kernel (k_rd_col:
+//                       REM_DIV_CHAN, and the substep that runs COURANT): 4, 8
+//                       or 16.
+//   DG_TUNE_CN_MT       modes per CTA of the substep's column kernel
+//                       (k_col_step: right-hand sides, CN solves, REM_DIV):
+//                       2, 4, 8 or 16.  Fewer modes per CTA means more CTAs
+//                       resident per SM to hide the column loads; more means
+//                       more sweep lanes per CTA.
 //   DG_TUNE_XROW_CHUNK  y-planes one CTA of the x-row product kernel marches
 //                       through (0 = automatic).  Longer marches re-read fewer
 //                       halo planes; shorter ones give more CTAs.
@@ -14,7 +17,7 @@
 //   DG_TUNE_PDL         1 (default): the substep kernels are launched with
 //                       programmatic dependent launch; 0: plain launches.
 //   DG_TUNE_WAIT_TEST   test only, not a launch shape: value > 0 makes the
-//                       next CN column launch poll its bulk-copy barrier at
+//                       next column-kernel launch poll its bulk-copy barrier at
 //                       most `value` times and expect 16 bytes more than its
 //                       copies bring, so every copy lands but the wait runs
 //                       out; the kernel then flags the failure and skips its
@@ -51,7 +54,7 @@ extern "C" int dg_tune_set(dg_handle *h, int key, int value) {
       h->col_mt = value;
       break;
     case DG_TUNE_CN_MT:
-      if (value != 4 && value != 8 && value != 16) return DG_ERR_ARG;
+      if (value != 2 && value != 4 && value != 8 && value != 16) return DG_ERR_ARG;
       h->cn_mt = value;
       break;
     case DG_TUNE_XROW_CHUNK:
@@ -172,7 +175,7 @@ extern "C" int dg_autotune(dg_handle *h, int steps_per_trial) {
   };
   std::vector<Knob> knobs = {
       {DG_TUNE_COL_MT, {4, 8, 16}},
-      {DG_TUNE_CN_MT, {4, 8, 16}},
+      {DG_TUNE_CN_MT, {2, 4, 8, 16}},
       {DG_TUNE_XROW_CHUNK, {0, 2, 4, 8, 16}},
       {DG_TUNE_YCHUNK, {0, 16, 32, 64}},
   };

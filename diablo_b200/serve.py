@@ -30,7 +30,11 @@ def state_bytes(p: Params) -> int:
 
 
 class Server:
-    def __init__(self, max_active: int = 32, budget_gb: float = 150.0, autotune: bool = True):
+    def __init__(self, max_active: int = 32, budget_gb: float = 150.0, autotune: bool = True,
+                 group_cases: int = 0):
+        """group_cases > 0: cases of similar size step together in groups of
+        up to that many, one graph per group step with one ragged column
+        launch per substep (dg_server_config DG_SERVER_GROUP_CASES)."""
         self.L = _lib.load()
         s = ctypes.c_void_p()
         _lib.check("dg_server_create",
@@ -38,6 +42,8 @@ class Server:
                                            ctypes.byref(s)))
         self.s = s
         self._params = {}
+        if group_cases:
+            _lib.check("dg_server_config", self.L.dg_server_config(self.s, 0, int(group_cases)))
 
     def submit(self, p: Params, gy: np.ndarray, state: dict, nsteps: int,
                prepare: bool = True) -> int:

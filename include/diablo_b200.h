@@ -220,7 +220,8 @@ int dg_timing_read(dg_handle *h, int i, char *name, int name_len, int64_t *launc
 
 /* -------------------------------------------------------------- tuning */
 /* No counterpart in the reference.  Launch shapes of the channel substep:
- * modes per CTA of the REM_DIV and CN y-column kernels (4, 8, 16), y-planes per CTA of the
+ * modes per CTA of the REM_DIV y-column kernel (4, 8, 16) and of the substep's
+ * column kernel (right-hand sides, CN solves, REM_DIV; 2, 4, 8, 16), y-planes per CTA of the
  * x-row product kernel (0 = automatic), planes per y-chunk of a substep
  * (0 = all).  Results do not depend on them.  dg_autotune times candidates on
  * the handle's own state (steps_per_trial eager RK3 steps each), keeps the
@@ -229,7 +230,7 @@ int dg_timing_read(dg_handle *h, int i, char *name, int name_len, int64_t *launc
 enum { DG_TUNE_COL_MT = 0, DG_TUNE_XROW_CHUNK = 1, DG_TUNE_YCHUNK = 2, DG_TUNE_CN_MT = 3,
        DG_TUNE_PDL = 4, DG_TUNE_WAIT_TEST = 5 };
 /* DG_TUNE_WAIT_TEST (test only): value > 0 makes the next Crank-Nicolson
- * column launch give up on its bulk-copy barrier after `value` polls, with
+ * column-kernel launch give up on its bulk-copy barrier after `value` polls, with
  * the barrier expecting 16 bytes more than its copies bring (every copy
  * lands; nothing faults).  The kernel skips its work and the next
  * diablo_synchronize / diablo_stats returns DG_ERR_TIMEOUT once.  The
@@ -287,6 +288,15 @@ int dg_server_submit(dg_server *s, const dg_params *p, const double *gy,
                      const double *const *state, int nsteps, int prepare, int64_t *id);
 int dg_server_wait(dg_server *s, int64_t id, double *const *state, double *times);
 int dg_server_query(dg_server *s, dg_server_stats *st);
+/* Server options, set before the first dg_server_submit.
+ * DG_SERVER_GROUP_CASES = G > 0: cases of similar size step together in
+ * groups of up to G, one CUDA graph per group step, with one ragged column
+ * launch per substep covering every member's (case, mode tile) work list;
+ * 0 (default): every case steps on its own.  Results are the same either
+ * way.  LES cases and cases with COURANT at an UPDATE_DT other than 1 always
+ * step on their own. */
+enum { DG_SERVER_GROUP_CASES = 0 };
+int dg_server_config(dg_server *s, int key, int value);
 int dg_server_destroy(dg_server *s);
 
 /* ------------------------------------------------------------ flow files */

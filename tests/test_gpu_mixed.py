@@ -195,3 +195,27 @@ def test_mixed_periodic_scalar_background_gradient():
     err = {nm: rel(g.get_field(nm), ref.get(nm)) for nm in fields(q)}
     assert all(v <= TOL_MIXED for v in err.values()), err
     g.close()
+
+
+@pytest.mark.parametrize("nx", [128, 256, 512])
+def test_mixed_error_does_not_grow_with_row_length(nx):
+    """The FP32 transforms sum along x; the row means they feed are formed
+    from exact FP64 products of the FP32 fluctuations.  KH layers of 128,
+    256 and 512 points per x-row (the 512-point rows take the two-launch
+    x-row stage), 100 steps against the FP64 oracle: all within the mixed
+    bar, and the 512-point error within 10x the 128-point one."""
+    p, gy = configs.kh_shear_layer(nx=nx, ny=33, nz=32)
+    ref, g = pair(p, gy, ics.kh_shear_layer, seed=9)
+    for s in range(1, 101):
+        ref.step(s)
+        g.steps(s, 1)
+    err = {nm: rel(g.get_field(nm), ref.get(nm)) for nm in fields(p)}
+    print(f"\nMIXED_NX {nx} " + " ".join(f"{k}={v:.3e}" for k, v in err.items()))
+    assert all(v <= TOL_MIXED for v in err.values()), err
+    _ERR_BY_NX[nx] = max(err.values())
+    if nx == 512 and 128 in _ERR_BY_NX:
+        assert _ERR_BY_NX[512] <= 10 * _ERR_BY_NX[128], _ERR_BY_NX
+    g.close()
+
+
+_ERR_BY_NX = {}

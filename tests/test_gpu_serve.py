@@ -37,10 +37,31 @@ def alone(p, gy, st, nsteps):
     return res
 
 
-def test_each_result_same_alone_and_in_the_mix():
-    cs = cases()
+def courant_cases():
+    """Small no-slip channels with variable DELTA_T: COURANT every step (can
+    join a group: the column launch of substep 3 stops after its CN solves)
+    and every other step (steps alone in grouped mode)."""
+    out = []
+    for i, upd in enumerate((1, 2)):
+        p, gy = configs.channel_re180(nx=32, ny=17, nz=32)
+        p = p.replace(update_dt=upd, precision=i)
+        u1, u2, u3, _ = ics.channel_laminar(p, gy, seed=40 + i)
+        from diablo_b200.solver import Channel
+        ch = Channel(p, gy)
+        ch.create_flow(u1, u2, u3)
+        st = {n: ch.get_field(n) for n in state_names(p)}
+        ch.close()
+        out.append((p, gy, st, 12))
+    return out
+
+
+@pytest.mark.parametrize("group", [0, 3])
+def test_each_result_same_alone_and_in_the_mix(group):
+    """group = 0: every case steps on its own stream; group = 3: cases of
+    similar size step together, one ragged column launch per substep."""
+    cs = cases() + courant_cases()
     solo = [alone(*c) for c in cs]
-    with Server(max_active=3, budget_gb=0, autotune=True) as srv:
+    with Server(max_active=5, budget_gb=0, autotune=True, group_cases=group) as srv:
         ids = [srv.submit(p, gy, st, n) for p, gy, st, n in cs]
         res = [srv.wait(i) for i in ids]
         s = srv.stats()

@@ -94,7 +94,9 @@ def load(path: str = LIB_PATH):
         "diablo_fft_xz_to_fourier_noalloc": [P, P, I, I, I, I, I, P],
         "dg_timing_enable": [P, I], "diablo_step": [P, I, I],
         "dg_tune_set": [P, I, I], "dg_tune_get": [P, I, ctypes.POINTER(I)],
-        "dg_autotune": [P, I],
+        "dg_autotune": [P, I], "dg_tune_lookup": [P, ctypes.POINTER(I)],
+        "dg_tune_cache_get": [P, I, ctypes.POINTER(I)], "dg_tune_cache_save": [ctypes.c_char_p],
+        "dg_tune_cache_load": [ctypes.c_char_p],
         "dg_server_create": [I, D, I, ctypes.POINTER(P)],
         "dg_server_submit": [P, P, P, P, I, I, ctypes.POINTER(ctypes.c_int64)],
         "dg_server_wait": [P, ctypes.c_int64, P, P],
@@ -127,3 +129,24 @@ def check(fn: str, code: int):
 
 def kernel_launches() -> int:
     return int(load().dg_kernel_launches())
+
+
+def tune_cache_save(path: str):
+    """Write the process-wide tuning cache (dg_tune_cache_save) as JSON."""
+    L = load()
+    check("dg_tune_cache_save", L.dg_tune_cache_save(os.fsencode(path)))
+
+
+def tune_cache_load(path: str):
+    """Merge a JSON tuning cache into the process-wide one."""
+    L = load()
+    check("dg_tune_cache_load", L.dg_tune_cache_load(os.fsencode(path)))
+
+
+def tune_cache_get(p, key: int):
+    """One stored tunable for the shape of params p, or None."""
+    L = load()
+    v = ctypes.c_int()
+    if L.dg_tune_cache_get(ctypes.byref(p.to_struct(DgParams)), key, ctypes.byref(v)) != 0:
+        return None
+    return v.value

@@ -1,7 +1,7 @@
 // Channel substep kernels (RK_CHAN_1, for/channel.f:62-1073) on the
 // retained-mode layout [j][kz][kx].
 //
-// One substep is five launches (six when COURANT runs):
+// One substep is four launches (five, plus COURANT's, when COURANT runs):
 //   zinv        spectral U1..U3, TH -> half-physical H (z inverse per kx)
 //   k_xrow_w    per physical z-row, marching up in y: x c2r of every field,
 //               all products/fluxes of for/channel.f:409-571,665-720, x r2c,
@@ -10,16 +10,20 @@
 //               without a warp kernel take two launches instead: k_xc2r of
 //               every plane into physical space, then k_xprod (products, x
 //               r2c and the combination, one product pair per CTA).
-//   k_zfwd_rhs  per plane: z forward of A/B, nonlinear + explicit linear
-//               terms -> CF (new), and the Crank-Nicolson right-hand side
+//   k_zfwd_w    per plane: z forward of A/B -> the nonlinear term
+//               NL = -i kz A + B of every retained mode (with LES, whose
+//               solves need them, the epilogue also forms the explicit terms,
+//               CF and the Crank-Nicolson right-hand side
 //               R = CU + zeta h CF_old - h grad P + beta h CF_new
-//                   + (nu h / 2) d2/dy2 CU           (for/channel.f:88-626)
-//   k_cn_col    per (mode tile, field): tridiagonal CN solve in Fourier space
-//               (the reference solves the same x-z independent operator per
-//               physical column, for/channel.f:767-1029; the operator is linear
-//               and identical for every column, so it commutes with the FFT)
-//   k_rd_col    per mode tile: REM_DIV_CHAN's complex tridiagonal, projection
-//               and CP += phi / h (for/channel.f:1103-1214, 1059-1065)
+//                   + (nu h / 2) d2/dy2 CU,          for/channel.f:88-626)
+//   k_col_step  per mode tile (chan_column.cu): explicit terms, CF, the CN
+//               right-hand sides and solves of every field, REM_DIV_CHAN and
+//               CP += phi / h.  The reference solves the same x-z independent
+//               CN operator per physical column (for/channel.f:767-1029); it
+//               is linear and identical for every column, so it commutes with
+//               the x-z transform.  With COURANT the kernel stops after the
+//               CN solves and k_rd_col (below) projects after COURANT's
+//               transform (for/channel.f:1037-1065, 1103-1214).
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -470,7 +474,7 @@ __host__ __device__ constexpr bool xw_supported(int n) {
   return n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 256;
 }
 
-template <int NX, int NTH, typename CX = double2>
+template <int NX, int NTH, typename CX = double2, int PV = 0>
 __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? (sizeof(CX) == 8 ? 4 : 3) : 2) k_xrow_w(
     ChanConst C, const CX *__restrict__ H, long Hfield, int chunk, int jbase, int jtop,
     const CX *__restrict__ tw, const double *__restrict__ dyf, const double *__restrict__ dy,
@@ -543,7 +547,7 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? (sizeof(CX) == 8 ? 4
       }
     }
     __syncwarp();
-    wpasses<NX, +1, 0>(buf, NPIN, SSTR, stw, lane);
+    wpasses<NX, +1, 0, PV>(buf, NPIN, SSTR, stw, lane);
 #pragma unroll
     for (int q = 0; q < NPIN; q++)
 #pragma unroll
@@ -659,7 +663,7 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? (sizeof(CX) == 8 ? 4
     }
     }
     __syncwarp();
-    wpasses<NX, -1, 0>(buf, NPP, SSTR, stw, lane);
+    wpasses<NX, -1, 0, PV>(buf, NPP, SSTR, stw, lane);
     const bool out = (j >= j0);
     const T d2 = (T)2 * dyf_j, dyj = dy[j];
     const T id2 = (T)1 / d2, idyj = (T)1 / dyj;  // per plane: multiply in the row loop
@@ -731,6 +735,14 @@ size_t xw_smem() {
   constexpr int NF = 3 + NTH, NPIN = (NF + 1) / 2, NPP = (8 + 3 * NTH + 1) / 2;
   constexpr int MAXP = NPIN > NPP ? NPIN : NPP;
   return sizeof(CX) * (NX + XW_WARPS * MAXP * padded_len(NX) + XW_WARPS * (5 + NTH) * (NX / 3 + 1));
+}
+
+// the plan variant of the handle's tuning, for lengths that have one
+template <int NX, int NTH, typename CX>
+auto xrow_kernel(int v) {
+  if constexpr (plan_has_variant(NX))
+    if (v) return k_xrow_w<NX, NTH, CX, 1>;
+  return k_xrow_w<NX, NTH, CX, 0>;
 }
 
 // ------------------------------------------------------------- zfwd + rhs
@@ -932,7 +944,7 @@ size_t zw_smem(int nz) {
 }
 
 // NLO as for k_zfwd_rhs: only -i kz A + B goes out, into rhs.
-template <int NZ, typename CX = double2, bool NLO = false>
+template <int NZ, typename CX = double2, bool NLO = false, int PV = 0>
 __global__ void __launch_bounds__(128, zw_minb(NZ, sizeof(CX))) k_zfwd_w(
     ChanConst C, const CX *__restrict__ G, long Gfield, const CX *__restrict__ tw,
     const double *__restrict__ dscal, int rk_step, const double *__restrict__ kxv,
@@ -977,7 +989,7 @@ __global__ void __launch_bounds__(128, zw_minb(NZ, sizeof(CX))) k_zfwd_w(
   }
   __syncthreads();
   CX *wb = buf + warp * 2 * KPW * SSTR;
-  wpasses_any<NZ, -1, 0>(wb, 2 * KPW, SSTR, stw, lane);
+  wpasses_any<NZ, -1, 0, PV>(wb, 2 * KPW, SSTR, stw, lane);
   __syncthreads();  // the epilogue below reads every warp's columns
 
   const double h = dscal[1 + rk_step];
@@ -1116,6 +1128,13 @@ __global__ void __launch_bounds__(128, zw_minb(NZ, sizeof(CX))) k_zfwd_w(
   }
 }
 
+template <int NZ, typename CX, bool NLO>
+auto zfwd_kernel(int v) {
+  if constexpr (plan_has_variant(NZ))
+    if (v) return k_zfwd_w<NZ, CX, NLO, 1>;
+  return k_zfwd_w<NZ, CX, NLO, 0>;
+}
+
 __host__ __device__ constexpr bool zw_supported(int n) {
   return n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 256;
 }
@@ -1237,112 +1256,15 @@ __global__ void k_remdiv_init(int NY, long ss, int nkxp, const double *__restric
 }
 
 // ------------------------------------------------------- column kernels
-// Each CTA owns MT = 16 modes and their whole y-column.  Inputs are staged
-// into shared memory with coalesced loads from all 128 threads; the
-// sequential sweeps then run with one lane per (mode, re/im) part -- the
-// operators are real, so real and imaginary parts are independent systems --
-// touching only shared memory; results leave with coalesced stores.
+// k_rd_col owns MT modes and their whole y-column (REM_DIV_CHAN on its own:
+// the entry point, and the substeps that run COURANT between the CN solves
+// and the projection).  Inputs are staged into shared memory with coalesced
+// loads from all 128 threads; the sequential sweeps then run with one lane
+// per (mode, re/im) part -- the operator is real, so real and imaginary
+// parts are independent systems -- touching only shared memory; results
+// leave with coalesced stores.  The substep's CN solves run in the column
+// kernel of chan_column.cu.
 constexpr int COL_THR = 128;
-
-// CN solve of one field for MT modes (rows 0..NY+1, tables of this substep).
-// The R tile (all planes x MT modes) arrives by bulk tensor copies, nbox
-// boxes of `by` planes, while the threads stage the CN tables.
-template <int MT>
-__global__ void __launch_bounds__(COL_THR) k_cn_col(int NY, long ss, const double *__restrict__ tab_rk,
-                                                   const __grid_constant__ CnMaps maps, int by,
-                                                   int nbox, FieldPtrs cu, int4 wlo_a,
-                                                   int4 wlo_b, int *__restrict__ err, long spin,
-                                                   unsigned extra_tx) {
-  extern __shared__ __align__(128) unsigned char csm_raw[];
-  unsigned char *sbase = csm_raw + ((128u - (dg_smem_addr(csm_raw) & 127u)) & 127u);
-  const int L = NY + 2;
-  const int f = blockIdx.y;
-  const long m0 = (long)blockIdx.x * MT;
-  double2 *X = reinterpret_cast<double2 *>(sbase);                    // [nbox * by][MT]
-  double *TB = reinterpret_cast<double *>(X + (long)nbox * by * MT);  // [5][L]
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(TB + 5 * L);
-  double2 *__restrict__ U = cu(f);
-  const int wl[8] = {wlo_a.x, wlo_a.y, wlo_a.z, wlo_a.w, wlo_b.x, wlo_b.y, wlo_b.z, wlo_b.w};
-  const int wlo = wl[f];
-  const int tid = threadIdx.x;
-  if (tid == 0) dg_mbar_init(bar, 1);
-  __syncthreads();
-  dg_pdl_wait();  // R comes from the z-forward kernel
-  if (tid == 0) {
-    // columns beyond ss and planes beyond L arrive as zeros (extra_tx is 0
-    // except in the wait test, where the barrier can then never complete)
-    dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * nbox * by * MT) + extra_tx);
-    for (int q = 0; q < nbox; q++)
-      dg_tma_load_2d(X + (long)q * by * MT, &maps.m[f], (int)(2 * m0), q * by, bar);
-  }
-  const double *T = tab_rk + (long)f * 5 * L;
-  for (int i = tid; i < 5 * L; i += COL_THR) TB[i] = T[i];
-  const bool landed = dg_mbar_wait(bar, 0, spin);
-  __syncthreads();
-  if (!landed) {
-    if (tid == 0) atomicExch(err + 1, 1);
-    dg_mbar_wait(bar, 0, spin);  // give the copies in flight one more bounded wait
-    return;
-  }
-  const int mt = (int)((ss - m0) < MT ? (ss - m0) : MT);
-  if (tid < 2 * MT) {
-    const int m = tid >> 1, part = tid & 1;
-    const double *Aa = TB, *Rb = TB + L, *Cc = TB + 2 * L, *K = TB + 3 * L, *V = TB + 4 * L;
-    double *x = (double *)X + tid;
-    constexpr int st = 2 * MT;
-    constexpr int B = 8;  // rows per register block: loads first, then the recurrence
-    const bool mean_re = (m0 + m == 0) && part == 0;
-    double g = 0.0;
-    for (int j0 = 0; j0 < L; j0 += B) {
-      double r[B], a[B];
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        const int j = j0 + q < L ? j0 + q : L - 1;
-        const double kind = K[j];
-        const double xr = x[j * st];
-        r[q] = (kind == (double)ROW_RHS) ? xr : ((kind == (double)ROW_BC && mean_re) ? V[j] : 0.0);
-        a[q] = Aa[j];
-      }
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        if (j0 + q < L) {
-          g = r[q] + a[q] * g;
-          r[q] = g;
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < B; q++)
-        if (j0 + q < L) x[(j0 + q) * st] = r[q];
-    }
-    double xv = g * Rb[L - 1];
-    x[(L - 1) * st] = xv;
-    for (int j1 = L - 2; j1 >= wlo; j1 -= B) {
-      double gq[B], cq[B], rq[B];
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        const int j = j1 - q >= wlo ? j1 - q : wlo;
-        gq[q] = x[j * st];
-        cq[q] = Cc[j];
-        rq[q] = Rb[j];
-      }
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        if (j1 - q >= wlo) {
-          xv = (gq[q] - cq[q] * xv) * rq[q];
-          gq[q] = xv;
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < B; q++)
-        if (j1 - q >= wlo) x[(j1 - q) * st] = gq[q];
-    }
-  }
-  __syncthreads();
-  for (int i = tid; i < L * MT; i += COL_THR) {
-    const int m = i % MT, j = i / MT;
-    if (m < mt && j >= wlo) U[(long)j * ss + m0 + m] = X[i];
-  }
-}
 
 // REM_DIV_CHAN for MT modes: divergence (parallel) -> forward and backward
 // sweeps (per part) -> projection, phi and CP update (parallel).
@@ -1799,52 +1721,6 @@ int dg_apply_bc_vel_dev(dg_handle *h) {
   return DG_OK;
 }
 
-int dg_cn_solve_dev(dg_handle *h, int rk_step) {
-  if (h->tables_pending) {
-    DG_CUDA(cudaStreamWaitEvent(h->st, h->ev_join, 0));
-    h->tables_pending = false;
-  }
-  FieldPtrs cu;
-  for (int f = 0; f < h->nf; f++) cu.p[f] = h->cu[f];
-  int wl[8] = {1, 1, 1, 1, 1, 1, 1, 1};
-  for (int n = 0; n < h->NTH; n++) wl[3 + n] = h->jstart_th[n] - 1;
-  const int L = h->NY + 2;
-  const double *tab = h->cn_tab + (long)(rk_step - 1) * (3 + DG_MAX_TH) * 5 * L;
-  // the column arrives in nbox boxes of `by` planes (a box is at most 256
-  // planes; a multiple of 8 planes keeps every box's shared-memory
-  // destination 128-byte aligned for any modes per CTA)
-  const int nbox = dg_cdiv(L, 256), by = (dg_cdiv(L, nbox) + 7) / 8 * 8;
-  auto cn_smem = [&](int m) {
-    return sizeof(double2) * (size_t)nbox * by * m + sizeof(double) * 5 * L + 8 + 128;
-  };
-  int mt = h->cn_mt;  // fewer modes per CTA where a tall column needs it
-  while (mt > 4 && cn_smem(mt) > 220 * 1024) mt /= 2;
-  const size_t sm = cn_smem(mt);
-  if (h->cn_maps_mt != mt) {
-    for (int f = 0; f < h->nf; f++)
-      DG_TRY(dg_tmap_planes(h->rhs[f], h->ss, L, mt, by, &h->cn_maps->m[f]));
-    h->cn_maps_mt = mt;
-  }
-  const CnMaps maps = *h->cn_maps;
-  dim3 grid(dg_cdiv(h->ss, mt), h->nf);
-  // the wait test (DG_TUNE_WAIT_TEST) applies to this one launch
-  const long spin = h->wait_test > 0 ? (long)h->wait_test : DG_ASYNC_SPIN;
-  const unsigned extra_tx = h->wait_test > 0 ? 16u : 0u;
-  h->wait_test = 0;
-#define CN_CASE(MTV)                                                                    \
-  if (mt == MTV) {                                                                      \
-    dg_big_smem((const void *)k_cn_col<MTV>);                                           \
-    dg_kt_begin(h, "k_cn_col", h->st);                                                  \
-    DG_CUDA(dg_launch(h->pdl, k_cn_col<MTV>, grid, dim3(COL_THR), sm, h->st, h->NY, h->ss, \
-                      tab, maps, by, nbox, cu, make_int4(wl[0], wl[1], wl[2], wl[3]),    \
-                      make_int4(wl[4], wl[5], wl[6], wl[7]), h->dflag, spin, extra_tx)); \
-  }
-  CN_CASE(4) CN_CASE(8) CN_CASE(16)
-#undef CN_CASE
-  DG_LAUNCHED();
-  return DG_OK;
-}
-
 int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step) {
   const int L = h->NY + 2;
   auto rd_smem = [&](int m) {
@@ -1959,8 +1835,6 @@ int dg_dt_commit(dg_handle *h) {
 }
 
 int dg_chan_init(dg_handle *h) {
-  h->cn_maps = new CnMaps();
-  h->cn_maps_mt = 0;
   h->cs_maps = new CnMaps();
   h->cs_maps_mt = 0;
   DG_TRY(dg_col_init(h));
@@ -2004,9 +1878,10 @@ static int nl_chunk_mixed(dg_handle *h, const ChanConst &C, int rk_step, int a, 
   bool done = false;
 #define XW_CASE(NXV, NTHV)                                                                      \
   if (!done && h->NX == NXV && h->NTH == NTHV) {                                                \
-    dg_big_smem((const void *)k_xrow_w<NXV, NTHV, float2>);                                     \
+    auto kern = xrow_kernel<NXV, NTHV, float2>(h->fft_plan);                                    \
+    dg_big_smem((const void *)kern);                                                            \
     dg_kt_begin(h, "k_xrow_w_f32", h->st);                                                      \
-    DG_CUDA(dg_launch(h->pdl, k_xrow_w<NXV, NTHV, float2>, grid, dim3(32 * XW_WARPS),           \
+    DG_CUDA(dg_launch(h->pdl, kern, grid, dim3(32 * XW_WARPS),                                  \
                       xw_smem<NXV, NTHV, float2>(), h->st, C, Hf, Hfield, chunk, a, b,          \
                       h->twx_f, h->dyf, h->dy, h->kx, Gf, Hfield));                             \
     done = true;                                                                                \
@@ -2025,7 +1900,8 @@ static int nl_chunk_mixed(dg_handle *h, const ChanConst &C, int rk_step, int a, 
   done = false;
 #define ZW_CASE(N)                                                                              \
   if (!done && h->NZ == N) {                                                                    \
-    auto kern = h->zf_nlo ? k_zfwd_w<N, float2, true> : k_zfwd_w<N, float2, false>;             \
+    auto kern = h->zf_nlo ? zfwd_kernel<N, float2, true>(h->fft_plan)                           \
+                          : zfwd_kernel<N, float2, false>(h->fft_plan);                         \
     dg_big_smem((const void *)kern);                                                            \
     dg_kt_begin(h, "k_zfwd_w_f32", h->st);                                                      \
     DG_CUDA(dg_launch(h->pdl, kern, zgrid, dim3(128), sm, h->st, C, Gf, Hfield,                 \
@@ -2104,7 +1980,8 @@ static int nl_generic_mixed(dg_handle *h, const ChanConst &C, int rk_step,
   const size_t sm = zw_smem<float2>(NZ);
 #define ZW_CASE(N)                                                                              \
   if (!done && NZ == N) {                                                                       \
-    auto kern = h->zf_nlo ? k_zfwd_w<N, float2, true> : k_zfwd_w<N, float2, false>;             \
+    auto kern = h->zf_nlo ? zfwd_kernel<N, float2, true>(h->fft_plan)                           \
+                          : zfwd_kernel<N, float2, false>(h->fft_plan);                         \
     dg_big_smem((const void *)kern);                                                            \
     dg_kt_begin(h, "k_zfwd_w_f32", h->st);                                                      \
     DG_CUDA(dg_launch(h->pdl, kern, zgrid, dim3(128), sm, h->st, C, Gf, Hfield,                 \
@@ -2182,9 +2059,10 @@ int dg_chan_nonlinear(dg_handle *h, int time_step, int rk_step, bool *column_nex
       dim3 grid(dg_cdiv(h->NZ, XW_WARPS), dg_cdiv(nplan, chunk));
 #define XW_CASE(NXV, NTHV)                                                                         \
   if (h->NX == NXV && h->NTH == NTHV) {                                                          \
-    dg_big_smem((const void *)k_xrow_w<NXV, NTHV>);                                              \
+    auto kern = xrow_kernel<NXV, NTHV, double2>(h->fft_plan);                                    \
+    dg_big_smem((const void *)kern);                                                             \
     dg_kt_begin(h, "k_xrow_w", h->st);                                                             \
-    DG_CUDA(dg_launch(h->pdl, k_xrow_w<NXV, NTHV>, grid, dim3(32 * XW_WARPS),                    \
+    DG_CUDA(dg_launch(h->pdl, kern, grid, dim3(32 * XW_WARPS),                                   \
                       xw_smem<NXV, NTHV>(), h->st, C, h->H, Hfield, chunk, a, b, h->twx,        \
                       h->dyf, h->dy, h->kx, h->G, Hfield));                                     \
     done = true;                                                                                 \
@@ -2230,7 +2108,8 @@ int dg_chan_nonlinear(dg_handle *h, int time_step, int rk_step, bool *column_nex
       const size_t sm = zw_smem<double2>(h->NZ);
 #define ZW_CASE(N)                                                                             \
   if (h->NZ == N) {                                                                            \
-    auto kern = h->zf_nlo ? k_zfwd_w<N, double2, true> : k_zfwd_w<N, double2, false>;          \
+    auto kern = h->zf_nlo ? zfwd_kernel<N, double2, true>(h->fft_plan)                         \
+                          : zfwd_kernel<N, double2, false>(h->fft_plan);                       \
     dg_big_smem((const void *)kern);                                                           \
     dg_kt_begin(h, "k_zfwd_w", h->st);                                                          \
     DG_CUDA(dg_launch(h->pdl, kern, grid, dim3(128), sm, h->st, C, h->G, Hfield, h->twz,       \

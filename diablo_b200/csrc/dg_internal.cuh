@@ -76,8 +76,8 @@ enum { F_U1 = 0, F_U2 = 1, F_U3 = 2, F_TH0 = 3 };
 
 struct dg_ktimer;
 
-// Tensor maps of the CN right-hand-side columns, one per field: 2-D over
-// [plane][2 ss doubles] (the CN column kernel's grid row is the field).
+// Tensor maps of the CU columns, one per field: 2-D over [plane][2 ss
+// doubles] (the column kernel stages every field's tile).
 struct CnMaps {
   CUtensorMap m[3 + DG_MAX_TH];
 };
@@ -154,8 +154,6 @@ struct dg_handle {
   // tunables (dg_tune_set / dg_autotune)
   int pdl;                      // substep kernels use programmatic dependent launch
   int pdl_zinv;                 // the next z inverse follows a kernel of the substep path
-  CnMaps *cn_maps;              // tensor maps of the CN right-hand sides (built per modes/CTA)
-  int cn_maps_mt;               // modes per CTA the maps were built for (0: none)
   int col_mt;                   // modes per CTA of the REM_DIV column kernel (4, 8, 16)
   int cn_mt;                    // modes per CTA of the column (CN) kernel (2, 4, 8, 16)
   int xrow_chunk;               // planes per CTA of the x-row product kernel (0 = auto)
@@ -163,10 +161,11 @@ struct dg_handle {
   double *rowc;                 // per-row grid factors of the column kernel [8][NY+2]
   CnMaps *cs_maps;              // tensor maps of CU for the column kernel
   int cs_maps_mt;               // modes per CTA the maps were built for (0: none)
+  int fft_plan;                 // radix-order variant of the x and z transform plans (0, 1)
   int zf_nlo;                   // the z forward writes only the nonlinear terms (the
                                 // column kernel assembles the right-hand sides)
-  int wait_test;                // test only: poll limit of the next CN launch, whose
-                                // barrier then expects 16 bytes more than it receives
+  int wait_test;                // test only: poll limit of the next column-kernel launch,
+                                // whose barrier then expects 16 bytes more than it receives
 
   // LES (dg_params.les): physical slots [nslots][NY+2][NZ][NX], spectral slots
   // [nslots][NY+2][ss], filter-width factors [2][NY+2] (DYF, DY), mean U1/U3

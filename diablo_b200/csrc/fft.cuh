@@ -218,7 +218,7 @@ __device__ inline C *run(C *buf0, C *buf1, const FftPlan &pl, int nsig,
 // ----------------------------------------------------- compile-time plans
 // radix of pass p for length N (0 = no pass).  Lengths 2^a 3^b; every pass
 // keeps N/R <= 128 so a 128-thread CTA holds whole signals per round.
-__host__ __device__ constexpr int plan_radix(int N, int p) {
+__host__ __device__ constexpr int plan_radix0(int N, int p) {
   int m = N, r = 0;
   for (int q = 0; q <= p; q++) {
     if (m == 1) return 0;
@@ -234,9 +234,32 @@ __host__ __device__ constexpr int plan_radix(int N, int p) {
   return r;
 }
 
-__host__ __device__ constexpr int plan_ns(int N, int p) {
+__host__ __device__ constexpr int plan_passes(int N) {
+  int p = 0;
+  while (p < DG_MAX_PASSES && plan_radix0(N, p) != 0) p++;
+  return p;
+}
+
+// Plan variant V: 0 as above (largest radix first), 1 the same radices in
+// reverse order.  Both are the same transform (a Stockham pass sequence is
+// valid for any order of the factors); they differ in shared-memory strides,
+// twiddle reuse and register use, so the autotuner picks per grid shape.
+__host__ __device__ constexpr int plan_radix(int N, int p, int V = 0) {
+  return V == 0 ? plan_radix0(N, p)
+                : (p < plan_passes(N) ? plan_radix0(N, plan_passes(N) - 1 - p) : 0);
+}
+
+// lengths whose two plan variants differ
+__host__ __device__ constexpr bool plan_has_variant(int N) {
+  bool differ = false;
+  for (int p = 0; p < plan_passes(N); p++)
+    if (plan_radix(N, p, 0) != plan_radix(N, p, 1)) differ = true;
+  return differ;
+}
+
+__host__ __device__ constexpr int plan_ns(int N, int p, int V = 0) {
   int ns = 1;
-  for (int q = 0; q < p; q++) ns *= plan_radix(N, q);
+  for (int q = 0; q < p; q++) ns *= plan_radix(N, q, V);
   return ns;
 }
 
@@ -271,18 +294,18 @@ __device__ __forceinline__ void cpass(const C *__restrict__ src, C *__restrict__
   }
 }
 
-template <int N, int SIGN, int P, typename C>
+template <int N, int SIGN, int P, int V = 0, typename C>
 __device__ __forceinline__ void cpasses(C *&src, C *&dst, int nsig, int sig_stride,
                                         const C *tw, int tid, int nthr) {
-  constexpr int R = plan_radix(N, P);
+  constexpr int R = plan_radix(N, P, V);
   if constexpr (R != 0) {
-    constexpr int NS = plan_ns(N, P);
+    constexpr int NS = plan_ns(N, P, V);
     cpass<N, R, NS, SIGN>(src, dst, nsig, sig_stride, tw, tid, nthr);
     __syncthreads();
     C *t = src;
     src = dst;
     dst = t;
-    cpasses<N, SIGN, P + 1>(src, dst, nsig, sig_stride, tw, tid, nthr);
+    cpasses<N, SIGN, P + 1, V>(src, dst, nsig, sig_stride, tw, tid, nthr);
   }
 }
 
@@ -325,14 +348,14 @@ __device__ __forceinline__ void ippass(C *__restrict__ buf, int nsig, int sig_st
   }
 }
 
-template <int N, int SIGN, int P, typename C>
+template <int N, int SIGN, int P, int V = 0, typename C>
 __device__ __forceinline__ void ippasses(C *buf, int nsig, int sig_stride, const C *tw,
                                          int tid, int nthr) {
-  constexpr int R = plan_radix(N, P);
+  constexpr int R = plan_radix(N, P, V);
   if constexpr (R != 0) {
-    constexpr int NS = plan_ns(N, P);
+    constexpr int NS = plan_ns(N, P, V);
     ippass<N, R, NS, SIGN>(buf, nsig, sig_stride, tw, tid, nthr);
-    ippasses<N, SIGN, P + 1>(buf, nsig, sig_stride, tw, tid, nthr);
+    ippasses<N, SIGN, P + 1, V>(buf, nsig, sig_stride, tw, tid, nthr);
   }
 }
 
@@ -391,13 +414,13 @@ __device__ __forceinline__ void wpass(C *__restrict__ buf, int nsig, int sstr,
   }
 }
 
-template <int N, int SIGN, int P, typename C>
+template <int N, int SIGN, int P, int V = 0, typename C>
 __device__ __forceinline__ void wpasses(C *buf, int nsig, int sstr, const C *tw,
                                         int lane) {
-  constexpr int R = plan_radix(N, P);
+  constexpr int R = plan_radix(N, P, V);
   if constexpr (R != 0) {
-    wpass<N, R, plan_ns(N, P), SIGN>(buf, nsig, sstr, tw, lane);
-    wpasses<N, SIGN, P + 1>(buf, nsig, sstr, tw, lane);
+    wpass<N, R, plan_ns(N, P, V), SIGN>(buf, nsig, sstr, tw, lane);
+    wpasses<N, SIGN, P + 1, V>(buf, nsig, sstr, tw, lane);
   }
 }
 
@@ -450,27 +473,27 @@ __device__ __forceinline__ void wpass_m(C *__restrict__ buf, int nsig, int sstr,
 
 // warp passes for any compile-time length: signal-parallel where N/R <= 32,
 // butterfly-parallel above
-template <int N, int SIGN, int P, typename C>
+template <int N, int SIGN, int P, int V = 0, typename C>
 __device__ __forceinline__ void wpasses_any(C *buf, int nsig, int sstr, const C *tw, int lane) {
-  constexpr int R = plan_radix(N, P);
+  constexpr int R = plan_radix(N, P, V);
   if constexpr (R != 0) {
-    if constexpr (N / R <= 32) wpass<N, R, plan_ns(N, P), SIGN>(buf, nsig, sstr, tw, lane);
-    else wpass_m<N, R, plan_ns(N, P), SIGN>(buf, nsig, sstr, tw, lane);
-    wpasses_any<N, SIGN, P + 1>(buf, nsig, sstr, tw, lane);
+    if constexpr (N / R <= 32) wpass<N, R, plan_ns(N, P, V), SIGN>(buf, nsig, sstr, tw, lane);
+    else wpass_m<N, R, plan_ns(N, P, V), SIGN>(buf, nsig, sstr, tw, lane);
+    wpasses_any<N, SIGN, P + 1, V>(buf, nsig, sstr, tw, lane);
   }
 }
 
 // Compile-time lengths run in place in buf0 (buf1 unused); the runtime plan
 // ping-pongs between buf0 and buf1.
-template <int N, typename C>
+template <int N, int V = 0, typename C>
 __device__ __forceinline__ C *fft(C *buf0, C *buf1, const FftPlan &pl, int nsig,
                                         int sig_stride, const C *tw, int sign) {
   if constexpr (N == 0) {
     return run(buf0, buf1, pl, nsig, sig_stride, tw, sign);
   } else {
     const int tid = threadIdx.x, nthr = blockDim.x;
-    if (sign < 0) ippasses<N, -1, 0>(buf0, nsig, sig_stride, tw, tid, nthr);
-    else ippasses<N, +1, 0>(buf0, nsig, sig_stride, tw, tid, nthr);
+    if (sign < 0) ippasses<N, -1, 0, V>(buf0, nsig, sig_stride, tw, tid, nthr);
+    else ippasses<N, +1, 0, V>(buf0, nsig, sig_stride, tw, tid, nthr);
     return buf0;
   }
 }
@@ -479,7 +502,7 @@ __device__ __forceinline__ C *fft(C *buf0, C *buf1, const FftPlan &pl, int nsig,
 // warps (no CTA barrier between passes), otherwise the CTA-wide passes run.
 // (For 192, 384 and 512 the CTA-wide passes measured faster here than
 // butterfly-parallel warp passes: fewer registers, more resident CTAs.)
-template <int N, typename C>
+template <int N, int V = 0, typename C>
 __device__ __forceinline__ C *fft_cta(C *buf0, C *buf1, const FftPlan &pl,
                                             int nsig, int sig_stride, const C *tw,
                                             int sign) {
@@ -489,13 +512,15 @@ __device__ __forceinline__ C *fft_cta(C *buf0, C *buf1, const FftPlan &pl,
     const int s0 = warp * per;
     const int ns = (nsig - s0) < per ? (nsig - s0) : per;
     if (ns > 0) {
-      if (sign < 0) wpasses_any<N, -1, 0>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
-      else wpasses_any<N, +1, 0>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
+      if (sign < 0)
+        wpasses_any<N, -1, 0, V>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
+      else
+        wpasses_any<N, +1, 0, V>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
     }
     __syncthreads();
     return buf0;
   } else {
-    return fft<N>(buf0, buf1, pl, nsig, sig_stride, tw, sign);
+    return fft<N, V>(buf0, buf1, pl, nsig, sig_stride, tw, sign);
   }
 }
 

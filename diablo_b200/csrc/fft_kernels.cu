@@ -37,7 +37,7 @@ __device__ __forceinline__ int packed_index(int z, int NZ, int NKZ) {
   return -1;
 }
 
-template <int NT, typename CX, typename PA = CFieldPtrs>
+template <int NT, typename CX, typename PA = CFieldPtrs, int PV = 0>
 __global__ void __launch_bounds__(NTHR) k_zinv(PA fields, int jmin, long ss, int nkxp,
                                               int NZr, int NKZ, FftPlan pl,
                                               const CX *__restrict__ tw,
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(NTHR) k_zinv(PA fields, int jmin, long ss, int
     }
   }
   __syncthreads();
-  CX *res = fft_cta<NT>(b0, b1, pl, KXG, sstr, stw, +1);
+  CX *res = fft_cta<NT, PV>(b0, b1, pl, KXG, sstr, stw, +1);
   CX *out = H + f * Hfield + (long)j * NZ * nkxp;
   for (int idx = tid; idx < KXG * NZ; idx += nthr) {
     const int c = idx % KXG, z = idx / KXG;
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(NTHR) k_xc2r(const double2 *__restrict__ H, lo
 // c2r of RPAIR row pairs followed by COURANT's per-point limit
 // min(CFL d / |u|) (for/courant.f:35-44) instead of a store: field 0 uses DX,
 // field 1 DY(j), field 2 DZ.  The minimum goes to *out as ordered bits.
-template <int NT>
+template <int NT, int PV = 0>
 __global__ void __launch_bounds__(NTHR) k_xc2r_cfl(const double2 *__restrict__ H, long Hfield,
                                                    int jmin, int nkxp, int NXr, int NZ, FftPlan pl,
                                                    const double2 *__restrict__ tw, double cfl,
@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(NTHR) k_xc2r_cfl(const double2 *__restrict__ H
     }
   }
   __syncthreads();
-  double2 *res = fft_cta<NT>(b0, b1, pl, RPAIR, sstr, stw, +1);
+  double2 *res = fft_cta<NT, PV>(b0, b1, pl, RPAIR, sstr, stw, +1);
   const double d = (f == 0) ? dxv : (f == 1 ? dy[j] : dzv);
   // min over points of CFL d / |u| is CFL d / max |u| (division is correctly
   // rounded and monotone), so only the largest |u| of the CTA is divided
@@ -333,6 +333,20 @@ void big_smem(K kern) {
   dg_big_smem((const void *)kern);
 }
 
+// the plan variant the handle's tuning chose, for lengths that have one
+template <int NN, typename CX, typename PA>
+auto zinv_kernel(int v) {
+  if constexpr (NN != 0 && plan_has_variant(NN))
+    if (v) return k_zinv<NN, CX, PA, 1>;
+  return k_zinv<NN, CX, PA, 0>;
+}
+template <int NN>
+auto xc2r_cfl_kernel(int v) {
+  if constexpr (NN != 0 && plan_has_variant(NN))
+    if (v) return k_xc2r_cfl<NN, 1>;
+  return k_xc2r_cfl<NN, 0>;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- host wrappers
@@ -353,10 +367,13 @@ static int cinv_t(dg_handle *h, const CI *const *fields, int nf, int jmin, int j
   dim3 grid(dg_cdiv(rowlen, batch_for(N)), jmax - jmin + 1, nf);
   const size_t sm = zsmem(N, sizeof(CX));
 #define KERNEL_BODY(NN)                                                                       \
-  big_smem(k_zinv<NN, CX, PA>);                                                               \
-  dg_kt_begin(h, "k_zinv", h->st);                                                            \
-  DG_CUDA(dg_launch(h->pdl_zinv, k_zinv<NN, CX, PA>, grid, dim3(NTHR), sm, h->st, fp, jmin,      \
-                    in_plane, rowlen, N, NK, pl, tw, H, out_field))
+  {                                                                                           \
+    auto kern = zinv_kernel<NN, CX, PA>(h->fft_plan);                                         \
+    big_smem(kern);                                                                           \
+    dg_kt_begin(h, "k_zinv", h->st);                                                          \
+    DG_CUDA(dg_launch(h->pdl_zinv, kern, grid, dim3(NTHR), sm, h->st, fp, jmin, in_plane,     \
+                      rowlen, N, NK, pl, tw, H, out_field));                                  \
+  }
   switch (N) {
     DG_FOR_EACH_N(DG_CASE_N)
     default: KERNEL_BODY(0); break;
@@ -479,10 +496,13 @@ int dg_xc2r_cfl(dg_handle *h, const double2 *H, int jmin, int jmax, unsigned lon
   const long Hf = (long)h->nplanes * h->NZ * h->nkxp;
   const double dxv = h->p.lx / h->NX, dzv = h->p.lz / h->NZ;
 #define KERNEL_BODY(N)                                                                          \
-  big_smem(k_xc2r_cfl<N>);                                                                      \
-  dg_kt_begin(h, "k_xc2r_cfl", h->st);                                                              \
-  DG_CUDA(dg_launch(0, k_xc2r_cfl<N>, grid, dim3(NTHR), sm, h->st, H, Hf, jmin, h->nkxp,          \
-                    h->NX, h->NZ, h->plx, h->twx, h->p.cfl, dxv, dzv, h->dy, out))
+  {                                                                                             \
+    auto kern = xc2r_cfl_kernel<N>(h->fft_plan);                                                \
+    big_smem(kern);                                                                             \
+    dg_kt_begin(h, "k_xc2r_cfl", h->st);                                                        \
+    DG_CUDA(dg_launch(0, kern, grid, dim3(NTHR), sm, h->st, H, Hf, jmin, h->nkxp, h->NX, h->NZ,  \
+                      h->plx, h->twx, h->p.cfl, dxv, dzv, h->dy, out));                        \
+  }
   switch (h->NX) {
     DG_FOR_EACH_N(DG_CASE_N)
     default: KERNEL_BODY(0); break;

@@ -13,7 +13,7 @@
 // each step is one replay of the case's captured graph (diablo_step) on the
 // case's stream, so steps of different cases overlap on the device.  Launch
 // shapes are tuned once per grid shape (dg_autotune on the first case of a
-// shape, reused for later ones).  A finished case's state is copied back to
+// shape; later cases of the shape take the tuning cache's entry).  A finished case's state is copied back to
 // host memory, its device memory is freed, and the slot goes to the next
 // request: requests that arrive while others run are admitted as soon as a
 // slot and memory free up.  Step latency is the device time between events
@@ -82,8 +82,6 @@ struct Active {
   int64_t bytes = 0;
 };
 
-using ShapeKey = std::tuple<int, int, int, int, int>;
-
 // a case can join a group: its step's launch sequence is the same every step
 bool groupable(const dg_params &p) {
   return !p.les && (!p.variable_dt || p.update_dt == 1);
@@ -137,7 +135,6 @@ struct dg_server {
   std::vector<Active> active;     // stepping thread only
   std::deque<Active> ready;       // prepared, handed to the stepping thread
   int preparing = 0;
-  std::map<ShapeKey, std::vector<int>> tuned;
   std::vector<float> step_ms;
   int64_t next_id = 1;
   int64_t bytes_active = 0, bytes_peak = 0;
@@ -187,18 +184,12 @@ struct dg_server {
       if (code == DG_OK) code = diablo_apply_bc_vel(a.h);
     }
     if (code == DG_OK && autotune) {
-      const ShapeKey key{r->p.nx, r->p.ny, r->p.nz, r->p.n_th, r->p.precision};
-      auto it = tuned.find(key);
-      if (it == tuned.end()) {
-        code = dg_autotune(a.h, 2);
-        if (code == DG_OK) {
-          std::vector<int> v(4);
-          for (int k = 0; k < 4; k++) dg_tune_get(a.h, k, &v[k]);
-          tuned[key] = v;
-        }
-      } else {
-        for (int k = 0; k < 4; k++) dg_tune_set(a.h, k, it->second[k]);
-      }
+      // the process-wide tuning cache holds one entry per grid shape: the
+      // first case of a shape is tuned, later ones (and later runs that
+      // loaded the cache file) reuse it
+      int hit = 0;
+      code = dg_tune_lookup(a.h, &hit);
+      if (code == DG_OK && !hit) code = dg_autotune(a.h, 2);
     }
     if (code != DG_OK) {
       const std::string msg = dg_last_error();

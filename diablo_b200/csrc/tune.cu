@@ -16,6 +16,11 @@
 //                       chunks keep the intermediate planes in L2.
 //   DG_TUNE_PDL         1 (default): the substep kernels are launched with
 //                       programmatic dependent launch; 0: plain launches.
+//   DG_TUNE_FFT_PLAN    radix order of the x and z transform plans: 0 the
+//                       largest radix first (128 = 16 x 8), 1 the reverse
+//                       (128 = 8 x 16).  Same transform, different shared-
+//                       memory strides, twiddle reuse and registers; lengths
+//                       whose factors are all equal have one plan.
 //   DG_TUNE_WAIT_TEST   test only, not a launch shape: value > 0 makes the
 //                       next column-kernel launch poll its bulk-copy barrier at
 //                       most `value` times and expect 16 bytes more than its
@@ -30,9 +35,46 @@
 // The choice depends only on the grid and field count, so a caller that
 // serves many cases can tune once per shape and copy the values across with
 // dg_tune_set.
+#include <stdio.h>
+#include <string.h>
+
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "dg_internal.cuh"
+
+// ------------------------------------------------------------ tuning cache
+// The autotuner's choices per grid shape, process-wide: key
+// "NXxNYxNZ_thN_fp64|mixed", value the launch-shape tunables.  dg_autotune
+// stores its result here; dg_tune_lookup applies a stored one;
+// dg_tune_cache_save / _load keep the table in a JSON file between runs:
+//   {"128x129x128_th0_fp64": {"col_mt": 8, "xrow_chunk": 0, "ychunk": 0,
+//    "cn_mt": 4, "pdl": 1, "fft_plan": 0}, ...}
+namespace {
+
+constexpr int kTuneKeys[] = {DG_TUNE_COL_MT, DG_TUNE_XROW_CHUNK, DG_TUNE_YCHUNK, DG_TUNE_CN_MT,
+                             DG_TUNE_PDL, DG_TUNE_FFT_PLAN};
+constexpr const char *kTuneNames[] = {"col_mt", "xrow_chunk", "ychunk", "cn_mt", "pdl",
+                                      "fft_plan"};
+constexpr int kNTune = 6;
+
+struct TuneRec {
+  int v[kNTune];
+};
+
+std::mutex g_tmu;
+std::map<std::string, TuneRec> g_tcache;
+
+std::string shape_key(const dg_params &p) {
+  char b[96];
+  snprintf(b, sizeof(b), "%dx%dx%d_th%d_%s", p.nx, p.ny, p.nz, p.n_th,
+           p.precision ? "mixed" : "fp64");
+  return b;
+}
+
+}  // namespace
 
 int dg_default_col_mt(const dg_handle *h) {
   // enough CTAs for about three per SM
@@ -73,6 +115,10 @@ extern "C" int dg_tune_set(dg_handle *h, int key, int value) {
       if (value < 0 || value > (1 << 20)) return DG_ERR_ARG;
       h->wait_test = value;
       break;
+    case DG_TUNE_FFT_PLAN:
+      if (value != 0 && value != 1) return DG_ERR_ARG;
+      h->fft_plan = value;
+      break;
     default:
       return DG_ERR_ARG;
   }
@@ -89,6 +135,7 @@ extern "C" int dg_tune_get(dg_handle *h, int key, int *value) {
     case DG_TUNE_YCHUNK: *value = h->ychunk; return DG_OK;
     case DG_TUNE_PDL: *value = h->pdl; return DG_OK;
     case DG_TUNE_WAIT_TEST: *value = h->wait_test; return DG_OK;
+    case DG_TUNE_FFT_PLAN: *value = h->fft_plan; return DG_OK;
     default: return DG_ERR_ARG;
   }
 }
@@ -178,6 +225,7 @@ extern "C" int dg_autotune(dg_handle *h, int steps_per_trial) {
       {DG_TUNE_CN_MT, {2, 4, 8, 16}},
       {DG_TUNE_XROW_CHUNK, {0, 2, 4, 8, 16}},
       {DG_TUNE_YCHUNK, {0, 16, 32, 64}},
+      {DG_TUNE_FFT_PLAN, {0, 1}},
   };
   for (const Knob &k : knobs) {
     int best = 0;
@@ -201,6 +249,12 @@ extern "C" int dg_autotune(dg_handle *h, int steps_per_trial) {
   free_saved(h, &sv);
   DG_TRY(s);
   DG_TRY(r);
+  {
+    TuneRec rec;
+    for (int k = 0; k < kNTune; k++) dg_tune_get(h, kTuneKeys[k], &rec.v[k]);
+    std::lock_guard<std::mutex> lk(g_tmu);
+    g_tcache[shape_key(h->p)] = rec;
+  }
   // the tables of the restored DELTA_T
   if (h->tables_pending) {
     DG_CUDA(cudaStreamWaitEvent(h->st, h->ev_join, 0));
@@ -208,5 +262,137 @@ extern "C" int dg_autotune(dg_handle *h, int steps_per_trial) {
   }
   DG_TRY(dg_cn_tables(h));
   DG_CUDA(cudaStreamSynchronize(h->st));
+  return DG_OK;
+}
+
+extern "C" int dg_tune_lookup(dg_handle *h, int *hit) {
+  if (!h || !hit) return DG_ERR_ARG;
+  *hit = 0;
+  TuneRec rec;
+  {
+    std::lock_guard<std::mutex> lk(g_tmu);
+    auto it = g_tcache.find(shape_key(h->p));
+    if (it == g_tcache.end()) return DG_OK;
+    rec = it->second;
+  }
+  for (int k = 0; k < kNTune; k++) DG_TRY(dg_tune_set(h, kTuneKeys[k], rec.v[k]));
+  *hit = 1;
+  return DG_OK;
+}
+
+extern "C" int dg_tune_cache_get(const dg_params *p, int key, int *value) {
+  if (!p || !value) return DG_ERR_ARG;
+  std::lock_guard<std::mutex> lk(g_tmu);
+  auto it = g_tcache.find(shape_key(*p));
+  if (it == g_tcache.end()) return DG_ERR_ARG;
+  for (int k = 0; k < kNTune; k++)
+    if (kTuneKeys[k] == key) {
+      *value = it->second.v[k];
+      return DG_OK;
+    }
+  return DG_ERR_ARG;
+}
+
+extern "C" int dg_tune_cache_save(const char *path) {
+  if (!path) return DG_ERR_ARG;
+  std::string out = "{";
+  {
+    std::lock_guard<std::mutex> lk(g_tmu);
+    bool first = true;
+    for (const auto &kv : g_tcache) {
+      out += first ? "\n" : ",\n";
+      first = false;
+      out += " \"" + kv.first + "\": {";
+      for (int k = 0; k < kNTune; k++) {
+        char b[48];
+        snprintf(b, sizeof(b), "%s\"%s\": %d", k ? ", " : "", kTuneNames[k], kv.second.v[k]);
+        out += b;
+      }
+      out += "}";
+    }
+  }
+  out += "\n}\n";
+  FILE *f = fopen(path, "w");
+  if (!f) {
+    dg_set_error((std::string("cannot write the tuning cache ") + path).c_str());
+    return DG_ERR_ARG;
+  }
+  const bool ok = fwrite(out.data(), 1, out.size(), f) == out.size();
+  if (fclose(f) != 0 || !ok) {
+    dg_set_error((std::string("writing the tuning cache ") + path + " failed").c_str());
+    return DG_ERR_ARG;
+  }
+  return DG_OK;
+}
+
+// Reads the file dg_tune_cache_save writes (a JSON object of objects whose
+// values are integers) and merges its entries into the table.  Unknown
+// tunable names are ignored; an entry lacking one keeps that tunable's
+// default; anything that is not this shape of JSON is an error and leaves
+// the table as it was.
+extern "C" int dg_tune_cache_load(const char *path) {
+  if (!path) return DG_ERR_ARG;
+  FILE *f = fopen(path, "r");
+  if (!f) {
+    dg_set_error((std::string("cannot read the tuning cache ") + path).c_str());
+    return DG_ERR_ARG;
+  }
+  std::string t;
+  char buf[4096];
+  size_t n;
+  while ((n = fread(buf, 1, sizeof(buf), f)) > 0) t.append(buf, n);
+  fclose(f);
+  size_t i = 0;
+  auto ws = [&] {
+    while (i < t.size() && (t[i] == ' ' || t[i] == '\n' || t[i] == '\r' || t[i] == '\t')) i++;
+  };
+  auto str = [&](std::string &o) -> bool {
+    ws();
+    if (i >= t.size() || t[i] != '"') return false;
+    size_t j = t.find('"', i + 1);
+    if (j == std::string::npos) return false;
+    o = t.substr(i + 1, j - i - 1);
+    i = j + 1;
+    return true;
+  };
+  auto ch = [&](char c) -> bool {
+    ws();
+    if (i < t.size() && t[i] == c) {
+      i++;
+      return true;
+    }
+    return false;
+  };
+  auto bad = [&]() {
+    dg_set_error((std::string("the tuning cache ") + path + " is not in the expected format").c_str());
+    return DG_ERR_ARG;
+  };
+  std::map<std::string, TuneRec> got;
+  if (!ch('{')) return bad();
+  if (!ch('}')) {
+    do {
+      std::string key;
+      if (!str(key) || !ch(':') || !ch('{')) return bad();
+      TuneRec rec = {{8, 0, 0, 4, 1, 0}};
+      if (!ch('}')) {
+        do {
+          std::string name;
+          if (!str(name) || !ch(':')) return bad();
+          ws();
+          char *end = nullptr;
+          const long v = strtol(t.c_str() + i, &end, 10);
+          if (end == t.c_str() + i) return bad();
+          i = end - t.c_str();
+          for (int k = 0; k < kNTune; k++)
+            if (name == kTuneNames[k]) rec.v[k] = (int)v;
+        } while (ch(','));
+        if (!ch('}')) return bad();
+      }
+      got[key] = rec;
+    } while (ch(','));
+    if (!ch('}')) return bad();
+  }
+  std::lock_guard<std::mutex> lk(g_tmu);
+  for (const auto &kv : got) g_tcache[kv.first] = kv.second;
   return DG_OK;
 }

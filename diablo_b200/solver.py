@@ -76,7 +76,7 @@ class _Solver:
     def _call(self, name, *args):
         _lib.check(name, getattr(self.L, name)(self.h, *args))
 
-    TUNE_KEYS = {"col_mt": 0, "xrow_chunk": 1, "ychunk": 2, "cn_mt": 3, "pdl": 4}
+    TUNE_KEYS = {"col_mt": 0, "xrow_chunk": 1, "ychunk": 2, "cn_mt": 3, "pdl": 4, "fft_plan": 6}
 
     def tune_set(self, **kw):
         """Launch-shape tunables (results do not depend on them)."""
@@ -101,9 +101,16 @@ class _Solver:
 
     def autotune(self, steps_per_trial: int = 3) -> dict:
         """Time candidate launch shapes on this state, keep the fastest; the
-        state, TIME and DELTA_T are restored afterwards."""
+        state, TIME and DELTA_T are restored afterwards.  The choice also goes
+        into the process-wide tuning cache (tune_cache_save / _load)."""
         self._call("dg_autotune", steps_per_trial)
         return self.tune_get()
+
+    def tune_lookup(self) -> bool:
+        """Apply the tuning cache's entry for this grid shape, if any."""
+        hit = ctypes.c_int()
+        self._call("dg_tune_lookup", ctypes.byref(hit))
+        return bool(hit.value)
 
     def steps(self, time_step: int, nsteps: int):
         """nsteps full RK3 steps from time_step (the driver loop body,

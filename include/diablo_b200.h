@@ -223,12 +223,19 @@ int dg_timing_read(dg_handle *h, int i, char *name, int name_len, int64_t *launc
  * modes per CTA of the REM_DIV y-column kernel (4, 8, 16) and of the substep's
  * column kernel (right-hand sides, CN solves, REM_DIV; 2, 4, 8, 16), y-planes per CTA of the
  * x-row product kernel (0 = automatic), planes per y-chunk of a substep
- * (0 = all).  Results do not depend on them.  dg_autotune times candidates on
+ * (0 = all).  Results do not depend on them (DG_TUNE_FFT_PLAN below: at
+ * round-off level only).  dg_autotune times candidates on
  * the handle's own state (steps_per_trial eager RK3 steps each), keeps the
  * fastest and restores the state, TIME and DELTA_T; it allocates temporary
  * device copies of the state while it runs. */
 enum { DG_TUNE_COL_MT = 0, DG_TUNE_XROW_CHUNK = 1, DG_TUNE_YCHUNK = 2, DG_TUNE_CN_MT = 3,
-       DG_TUNE_PDL = 4, DG_TUNE_WAIT_TEST = 5 };
+       DG_TUNE_PDL = 4, DG_TUNE_WAIT_TEST = 5, DG_TUNE_FFT_PLAN = 6 };
+/* DG_TUNE_FFT_PLAN: radix order of the x and z transform plans of the
+ * substep (0: largest radix first, 128 = 16 x 8; 1: the reverse, 8 x 16).
+ * The same transform either way; the autotuner times both per grid shape.
+ * Unlike the other tunables it changes the order of the transforms'
+ * arithmetic, so results differ between the two at round-off level (both
+ * are held to the same parity tolerance). */
 /* DG_TUNE_WAIT_TEST (test only): value > 0 makes the next Crank-Nicolson
  * column-kernel launch give up on its bulk-copy barrier after `value` polls, with
  * the barrier expecting 16 bytes more than its copies bring (every copy
@@ -238,6 +245,19 @@ enum { DG_TUNE_COL_MT = 0, DG_TUNE_XROW_CHUNK = 1, DG_TUNE_YCHUNK = 2, DG_TUNE_C
 int dg_tune_set(dg_handle *h, int key, int value);
 int dg_tune_get(dg_handle *h, int key, int *value);
 int dg_autotune(dg_handle *h, int steps_per_trial);
+/* The autotuner's choices per grid shape (NX, NY, NZ, N_TH, precision) in a
+ * process-wide table (no counterpart in the reference; FFTW_MEASURE planning,
+ * for/fft.f:77-94, is the reference's own per-size tuning).  dg_autotune
+ * stores its result in it; dg_tune_lookup applies the stored values for h's
+ * shape (*hit = 1) or leaves h as it is (*hit = 0); dg_tune_cache_get reads
+ * one stored value for a shape (DG_ERR_ARG when absent).  The table persists
+ * in a JSON file, {"NXxNYxNZ_thN_fp64|mixed": {"col_mt": .., "xrow_chunk": ..,
+ * "ychunk": .., "cn_mt": .., "pdl": .., "fft_plan": ..}, ...}: _save writes
+ * the whole table, _load merges a file's entries into it. */
+int dg_tune_lookup(dg_handle *h, int *hit);
+int dg_tune_cache_get(const dg_params *p, int key, int *value);
+int dg_tune_cache_save(const char *path);
+int dg_tune_cache_load(const char *path);
 
 /* ------------------------------------------- allocation-free transform */
 /* No counterpart in the reference.  FFT_XZ_TO_FOURIER(V,VV,JMIN,JMAX) on

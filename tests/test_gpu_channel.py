@@ -324,7 +324,9 @@ def test_graph_steps_match_substep_calls(case):
 
 def test_autotune_restores_state_and_keeps_results():
     """dg_autotune leaves the state, TIME and DELTA_T as it found them, and
-    the launch shapes it picks do not change results (bit for bit)."""
+    the launch shapes it picks do not change results (bit for bit; the
+    transform plan variant, which changes them at round-off level, is set the
+    same on both sides)."""
     p, gy = configs.channel_re180(nx=64, ny=65, nz=48)
     ref, a, _ = start_pair(p, gy, ics.channel_laminar, seed=8)
     b = channel(p, gy)
@@ -337,6 +339,7 @@ def test_autotune_restores_state_and_keeps_results():
     for nm, v in before.items():
         assert np.array_equal(b.get_field(nm), v), nm
     assert b.get_time() == t0
+    a.tune_set(fft_plan=chosen["fft_plan"])
     for s in range(1, 6):
         a.step(s)
     b.steps(1, 5)
@@ -345,6 +348,7 @@ def test_autotune_restores_state_and_keeps_results():
     for mt in (4, 16):
         b.tune_set(col_mt=mt, cn_mt=20 - mt, xrow_chunk=3, ychunk=20)
         c = channel(p, gy)
+        c.tune_set(fft_plan=chosen["fft_plan"])
         c.set_state(ref.state())
         c.set_time(0.0, p.delta_t)
         b.set_state(ref.state())
@@ -401,3 +405,32 @@ def test_reference_layout_round_trip(periodic):
         assert np.array_equal(out[n][:, :nkzt, :nkxp], a[:, :nkzt, :nkxp]), n
         assert np.all(out[n][:, nkzt:, :] == 5.0) and np.all(out[n][:, :, nkxp:] == 5.0), n
     s.close()
+
+
+def test_fft_plan_variant_parity_and_tuning_cache(tmp_path):
+    """The reversed-radix transform plan (DG_TUNE_FFT_PLAN = 1) against the
+    oracle, and the autotuner's per-shape cache: dg_autotune stores its
+    choice, a new handle of the same shape takes it with dg_tune_lookup, and
+    the JSON file written by dg_tune_cache_save holds it."""
+    import json
+    from diablo_b200 import _lib
+    p, gy = configs.kh_shear_layer(nx=128, ny=33, nz=32)
+    ref, ch, _ = start_pair(p, gy, ics.kh_shear_layer, seed=5)
+    ch.tune_set(fft_plan=1)
+    for s in range(1, 21):
+        ref.step(s)
+        ch.step(s)
+    compare(ref, ch, fields(p))
+    ch.set_state(ref.state())
+    tuned = ch.autotune(1)
+    ch.close()
+    other = channel(p, gy)
+    assert other.tune_lookup()
+    assert other.tune_get() == tuned
+    other.close()
+    path = tmp_path / "tune.json"
+    _lib.tune_cache_save(str(path))
+    key = f"{p.nx}x{p.ny}x{p.nz}_th{p.n_th}_fp64"
+    assert json.loads(path.read_text())[key] == {k: tuned[k] for k in
+                                                 ("col_mt", "xrow_chunk", "ychunk", "cn_mt",
+                                                  "pdl", "fft_plan")}

@@ -162,6 +162,7 @@ struct dg_handle {
   CnMaps *cs_maps;              // tensor maps of CU for the column kernel
   int cs_maps_mt;               // modes per CTA the maps were built for (0: none)
   int fft_plan;                 // radix-order variant of the x and z transform plans (0, 1)
+  int col_fused;                // column stage: 0 split (per field, REM_DIV apart), 1 fused
   int zf_nlo;                   // the z forward writes only the nonlinear terms (the
                                 // column kernel assembles the right-hand sides)
   int wait_test;                // test only: poll limit of the next column-kernel launch,
@@ -243,13 +244,13 @@ bool dg_chan_cfl(const dg_handle *h, int time_step, int rk_step);
 int dg_chan_cfl_tail(dg_handle *h, int rk_step);
 int dg_col_init(dg_handle *h);
 int dg_col_step_dev(dg_handle *h, int rk_step, bool rd);
-size_t dg_col_smem(const dg_handle *h, int mt, int *by_out, int *nbox_out);
+size_t dg_col_smem(const dg_handle *h, int mt, bool fused);
 size_t dg_col_case_bytes();
-int dg_col_batch_build(dg_handle *const *hs, const int *rd, int n, int want_mt,
-                       std::vector<unsigned char> &cases, std::vector<int2> &work, int *mt_out,
+int dg_col_batch_build(dg_handle *const *hs, const int *rd, int n, int want_mt, int fused,
+                       std::vector<unsigned char> &cases, std::vector<int4> &work, int *mt_out,
                        size_t *smem_out);
 int dg_col_batch_launch(cudaStream_t st, int mt, size_t smem, const void *dev_cases,
-                        const int2 *dev_work, int nwork, int rk_step);
+                        const int4 *dev_work, int nwork, int rk_step, int fused);
 
 #define DG_CASE_N(N) \
   case N:            \

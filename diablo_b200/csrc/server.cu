@@ -24,9 +24,12 @@
 // step of a group is one CUDA graph: per substep, every member's transform
 // stage (z inverse, x-row products, z forward) runs on the member's own
 // stream, the members join, and ONE ragged column launch (k_col_step_ragged)
-// does the right-hand sides, CN solves and REM_DIV of every member's modes
-// -- a (case, mode tile) work list over all members -- before the members'
-// streams fork again.  Groups run concurrently on their own streams.  A
+// does the right-hand sides and CN solves (and, in the fused column form,
+// REM_DIV) of every member's modes -- a (case, mode tile, field) work list
+// over all members -- before the members' streams fork again (in the split
+// form each member's REM_DIV then runs on its own stream).  A group's
+// members share the column form their tuning chose.  Groups run
+// concurrently on their own streams.  A
 // group is re-captured when a member joins or leaves (at step boundaries,
 // after the group's steps in flight have finished).  Results are the same
 // as per-case stepping: every mode's arithmetic is the single-case kernels'.
@@ -94,7 +97,8 @@ struct Group {
   std::vector<cudaEvent_t> ev_m;   // one per member: joins into gs
   cudaEvent_t ev_col = nullptr;    // column launch done: members fork from it
   void *d_cases[3] = {nullptr, nullptr, nullptr};  // case tables per substep (rd differs at 3)
-  int2 *d_work = nullptr;
+  int4 *d_work = nullptr;
+  int fused = 0;                   // the members' column-stage form (all the same)
   int nwork = 0, mt = 0;
   size_t smem = 0;
   cudaGraphExec_t exec = nullptr;
@@ -447,17 +451,23 @@ struct GroupedLoop {
       solo.push_back(a);
       return;
     }
+    // a group's members share one ragged column launch, so they share the
+    // column-stage form their tuning chose (it changes results at round-off)
+    const int fused = a->h->col_fused;
     Group *best = nullptr;
     double bd = 1e30;
     for (auto &g : groups) {
-      if ((int)g->m.size() >= s->group_cases) continue;
+      if ((int)g->m.size() >= s->group_cases || g->fused != fused) continue;
       const double d = fabs(log(pts(a) / g->points));
       if (d < log(4.0) && d < bd) {
         bd = d;
         best = g.get();
       }
     }
-    if (!best) best = new_group();
+    if (!best) {
+      best = new_group();
+      best->fused = fused;
+    }
     best->m.push_back(a);
     double sum = 0;
     for (Active *x : best->m) sum += pts(x);
@@ -498,12 +508,14 @@ struct GroupedLoop {
         DG_CUDA(cudaEventRecord(g.ev_m[c], h->st));
         DG_CUDA(cudaStreamWaitEvent(g.gs, g.ev_m[c], 0));
       }
-      DG_TRY(dg_col_batch_launch(g.gs, g.mt, g.smem, g.d_cases[rk - 1], g.d_work, g.nwork, rk));
+      DG_TRY(dg_col_batch_launch(g.gs, g.mt, g.smem, g.d_cases[rk - 1], g.d_work, g.nwork, rk,
+                                 g.fused));
       DG_CUDA(cudaEventRecord(g.ev_col, g.gs));
       for (Active *a : g.m) {
         dg_handle *h = a->h;
         DG_CUDA(cudaStreamWaitEvent(h->st, g.ev_col, 0));
         if (dg_chan_cfl(h, 2, rk)) DG_TRY(dg_chan_cfl_tail(h, rk));
+        else if (!g.fused) DG_TRY(dg_rem_div_dev(h, 1, rk));  // the split form's REM_DIV
       }
     }
     for (int c = 0; c < n; c++) {
@@ -537,15 +549,15 @@ struct GroupedLoop {
       std::vector<int> rd;
       for (dg_handle *h : hs) rd.push_back(dg_chan_cfl(h, 2, rk) ? 0 : 1);
       std::vector<unsigned char> tab;
-      std::vector<int2> work;
-      DG_TRY(dg_col_batch_build(hs.data(), rd.data(), (int)hs.size(), want, tab, work, &g.mt,
-                                &g.smem));
+      std::vector<int4> work;
+      DG_TRY(dg_col_batch_build(hs.data(), rd.data(), (int)hs.size(), want, g.fused, tab, work,
+                                &g.mt, &g.smem));
       DG_CUDA(cudaMalloc(&g.d_cases[rk - 1], tab.size()));
       DG_CUDA(cudaMemcpy(g.d_cases[rk - 1], tab.data(), tab.size(), cudaMemcpyHostToDevice));
       if (rk == 1) {
         g.nwork = (int)work.size();
-        DG_CUDA(cudaMalloc((void **)&g.d_work, sizeof(int2) * work.size()));
-        DG_CUDA(cudaMemcpy(g.d_work, work.data(), sizeof(int2) * work.size(),
+        DG_CUDA(cudaMalloc((void **)&g.d_work, sizeof(int4) * work.size()));
+        DG_CUDA(cudaMemcpy(g.d_work, work.data(), sizeof(int4) * work.size(),
                            cudaMemcpyHostToDevice));
       }
     }

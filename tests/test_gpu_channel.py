@@ -325,8 +325,8 @@ def test_graph_steps_match_substep_calls(case):
 def test_autotune_restores_state_and_keeps_results():
     """dg_autotune leaves the state, TIME and DELTA_T as it found them, and
     the launch shapes it picks do not change results (bit for bit; the
-    transform plan variant, which changes them at round-off level, is set the
-    same on both sides)."""
+    transform plan variant and the column-stage form, which change them at
+    round-off level, are set the same on both sides)."""
     p, gy = configs.channel_re180(nx=64, ny=65, nz=48)
     ref, a, _ = start_pair(p, gy, ics.channel_laminar, seed=8)
     b = channel(p, gy)
@@ -339,7 +339,7 @@ def test_autotune_restores_state_and_keeps_results():
     for nm, v in before.items():
         assert np.array_equal(b.get_field(nm), v), nm
     assert b.get_time() == t0
-    a.tune_set(fft_plan=chosen["fft_plan"])
+    a.tune_set(fft_plan=chosen["fft_plan"], col_fused=chosen["col_fused"])
     for s in range(1, 6):
         a.step(s)
     b.steps(1, 5)
@@ -348,7 +348,7 @@ def test_autotune_restores_state_and_keeps_results():
     for mt in (4, 16):
         b.tune_set(col_mt=mt, cn_mt=20 - mt, xrow_chunk=3, ychunk=20)
         c = channel(p, gy)
-        c.tune_set(fft_plan=chosen["fft_plan"])
+        c.tune_set(fft_plan=chosen["fft_plan"], col_fused=chosen["col_fused"])
         c.set_state(ref.state())
         c.set_time(0.0, p.delta_t)
         b.set_state(ref.state())
@@ -433,4 +433,32 @@ def test_fft_plan_variant_parity_and_tuning_cache(tmp_path):
     key = f"{p.nx}x{p.ny}x{p.nz}_th{p.n_th}_fp64"
     assert json.loads(path.read_text())[key] == {k: tuned[k] for k in
                                                  ("col_mt", "xrow_chunk", "ychunk", "cn_mt",
-                                                  "pdl", "fft_plan")}
+                                                  "pdl", "fft_plan", "col_fused")}
+
+
+@pytest.mark.parametrize("fused,mt", [(0, 2), (0, 16), (1, 4), (1, 16)])
+def test_column_forms_match_oracle(fused, mt):
+    """The split and the fused column stage (DG_TUNE_COL_FUSED), at small and
+    large tiles, against the oracle: a stratified KH layer with rotation,
+    gravity in x and z, a Neumann scalar with DRHODX/Z, and COURANT every
+    step (substep 3 stops after the CN solves and projects after COURANT)."""
+    p, gy = configs.kh_shear_layer(nx=32, ny=33, nz=16)
+    p = p.replace(i_ro=0.3, grav_x=0.2, grav_z=-0.1, variable_dt=1, update_dt=1, cfl=0.4, n_th=2)
+    p.ri = [0.1, 0.05, 0, 0]
+    p.pr = [1.0, 0.7, 1, 1]
+    p.th_bc_ymin = [0, 1, 0, 0]
+    p.th_bc_ymax = [0, 1, 0, 0]
+    p.th_bc_ymin_c1 = [-1.0, 0.1, 0, 0]
+    p.th_bc_ymax_c1 = [1.0, -0.2, 0, 0]
+    p.drhodx = [0.0, 0.3, 0, 0]
+    p.drhodz = [0.0, -0.2, 0, 0]
+    ref, ch, _ = start_pair(p, gy, ics.kh_shear_layer, seed=12)
+    ch.tune_set(col_fused=fused, cn_mt=mt)
+    for s in range(1, 11):
+        ref.step(s)
+        ch.step(s)
+    compare(ref, ch, fields(p) + ["CP"], tol=1e-10)
+    t_o, dt_o = ref.get_time()
+    t_g, dt_g = ch.get_time()
+    assert abs(dt_g - dt_o) <= 1e-12 * dt_o
+    ch.close()

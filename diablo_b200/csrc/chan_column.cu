@@ -24,7 +24,11 @@
 //              and the REM_DIV recurrences one after the other.
 // The autotuner picks per grid shape.  Both do the same arithmetic per mode
 // except for the REM_DIV divergence, which each compiles on its own (results
-// agree to round-off).
+// agree to round-off).  The split form writes each field as soon as its CTA
+// has solved it, so it is used only when no field's right-hand side reads
+// another field (no rotation, no buoyancy or GRAV terms, no DRHODX/Z);
+// otherwise the fused form runs, which stages every field before it writes
+// any.
 //
 // Layout: every field is [NY+2][ss] complex, modes kx fastest; a CTA owns
 // modes m0 .. m0+MT-1.  The CU tiles (all planes x MT modes) arrive by bulk
@@ -599,6 +603,20 @@ static int fill_case(dg_handle *h, int mt, bool rd, ColCase *cc) {
   return DG_OK;
 }
 
+// The column form that runs for h: the split form only when no field's
+// right-hand side reads another field (see above).
+bool dg_col_fused(const dg_handle *h) {
+  if (h->col_fused) return true;
+  if (h->p.i_ro != 0.0) return true;
+  for (int n = 0; n < h->NTH; n++) {
+    const double ri = h->p.ri[n];
+    if (ri * h->p.grav_x != 0.0 || ri * h->p.grav_y != 0.0 || ri * h->p.grav_z != 0.0 ||
+        h->p.drhodx[n] != 0.0 || h->p.drhodz[n] != 0.0)
+      return true;
+  }
+  return false;
+}
+
 // modes per CTA for handle h: the tuned value, halved until the tiles fit
 static int col_mt(const dg_handle *h, int want, bool fused) {
   int mt = want;
@@ -614,7 +632,7 @@ int dg_col_step_dev(dg_handle *h, int rk_step, bool rd) {
     DG_CUDA(cudaStreamWaitEvent(h->st, h->ev_join, 0));
     h->tables_pending = false;
   }
-  const bool fused = h->col_fused != 0;
+  const bool fused = dg_col_fused(h);
   const int mt = col_mt(h, h->cn_mt, fused);
   const size_t sm = dg_col_smem(h, mt, fused);
   if (sm > 220 * 1024) {

@@ -27,6 +27,10 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+
+#include <map>
+#include <mutex>
+#include <utility>
 #include "dg_internal.cuh"
 #include "fft.cuh"
 
@@ -735,6 +739,42 @@ size_t xw_smem() {
   constexpr int NF = 3 + NTH, NPIN = (NF + 1) / 2, NPP = (8 + 3 * NTH + 1) / 2;
   constexpr int MAXP = NPIN > NPP ? NPIN : NPP;
   return sizeof(CX) * (NX + XW_WARPS * MAXP * padded_len(NX) + XW_WARPS * (5 + NTH) * (NX / 3 + 1));
+}
+
+// Planes one x-row CTA marches through when the tuning leaves it automatic
+// (DG_TUNE_XROW_CHUNK = 0): the fewest (at least 3) that fit the whole grid
+// into one wave of resident CTAs, so no SM waits out a partial last wave;
+// grids too large for that take 32 planes per CTA.
+int xrow_auto_chunk(int nplan, int NZ, const void *kern, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, size_t>, int> per_sm_cache;
+  static int nsm = 0;
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!nsm) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        nsm = 148;
+    }
+    auto it = per_sm_cache.find({kern, smem});
+    if (it != per_sm_cache.end()) {
+      per_sm = it->second;
+    } else {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * XW_WARPS, smem) !=
+          cudaSuccess)
+        per_sm = 1;
+      per_sm_cache[{kern, smem}] = per_sm;
+    }
+  }
+  const long slots = (long)(per_sm > 0 ? per_sm : 1) * nsm;
+  const long zb = dg_cdiv(NZ, XW_WARPS);
+  const long per_col = slots / zb > 0 ? slots / zb : 1;  // CTAs per z-block column in one wave
+  int chunk = dg_cdiv(nplan, per_col);
+  if (chunk < 3) chunk = 3;
+  if (chunk > 32) chunk = 32;
+  return chunk < nplan ? chunk : nplan;
 }
 
 // the plan variant of the handle's tuning, for lengths that have one
@@ -1868,18 +1908,15 @@ static int nl_chunk_mixed(dg_handle *h, const ChanConst &C, int rk_step, int a, 
   DG_TRY(zs);
   hdone = b + 1;
   const int nplan = b - a + 1;
-  int chunk = h->xrow_chunk;
-  if (chunk <= 0) {
-    chunk = (int)((long)nplan * h->NZ / (148L * 16));
-    if (chunk < 4) chunk = 4;
-  }
-  if (chunk > nplan) chunk = nplan;
-  dim3 grid(dg_cdiv(h->NZ, XW_WARPS), dg_cdiv(nplan, chunk));
   bool done = false;
 #define XW_CASE(NXV, NTHV)                                                                      \
   if (!done && h->NX == NXV && h->NTH == NTHV) {                                                \
     auto kern = xrow_kernel<NXV, NTHV, float2>(h->fft_plan);                                    \
     dg_big_smem((const void *)kern);                                                            \
+    int chunk = h->xrow_chunk > 0 ? (h->xrow_chunk < nplan ? h->xrow_chunk : nplan)            \
+                                  : xrow_auto_chunk(nplan, h->NZ, (const void *)kern,          \
+                                                    xw_smem<NXV, NTHV, float2>());              \
+    dim3 grid(dg_cdiv(h->NZ, XW_WARPS), dg_cdiv(nplan, chunk));                                 \
     dg_kt_begin(h, "k_xrow_w_f32", h->st);                                                      \
     DG_CUDA(dg_launch(h->pdl, kern, grid, dim3(32 * XW_WARPS),                                  \
                       xw_smem<NXV, NTHV, float2>(), h->st, C, Hf, Hfield, chunk, a, b,          \
@@ -2048,19 +2085,16 @@ int dg_chan_nonlinear(dg_handle *h, int time_step, int rk_step, bool *column_nex
     bool done = false;
     if (xw_supported(h->NX) && h->NTH <= 2) {
       const int nplan = b - a + 1;
-      // planes marched by one CTA (tunable DG_TUNE_XROW_CHUNK; 0 = about 16
-      // x-rows of work per SM-slot)
-      int chunk = h->xrow_chunk;
-      if (chunk <= 0) {
-        chunk = (int)((long)nplan * h->NZ / (148L * 16));
-        if (chunk < 4) chunk = 4;
-      }
-      if (chunk > nplan) chunk = nplan;
-      dim3 grid(dg_cdiv(h->NZ, XW_WARPS), dg_cdiv(nplan, chunk));
+      // planes marched by one CTA (tunable DG_TUNE_XROW_CHUNK; 0 = the one-wave
+      // choice of xrow_auto_chunk)
 #define XW_CASE(NXV, NTHV)                                                                         \
   if (h->NX == NXV && h->NTH == NTHV) {                                                          \
     auto kern = xrow_kernel<NXV, NTHV, double2>(h->fft_plan);                                    \
     dg_big_smem((const void *)kern);                                                             \
+    int chunk = h->xrow_chunk > 0 ? (h->xrow_chunk < nplan ? h->xrow_chunk : nplan)             \
+                                  : xrow_auto_chunk(nplan, h->NZ, (const void *)kern,           \
+                                                    xw_smem<NXV, NTHV>());                       \
+    dim3 grid(dg_cdiv(h->NZ, XW_WARPS), dg_cdiv(nplan, chunk));                                  \
     dg_kt_begin(h, "k_xrow_w", h->st);                                                             \
     DG_CUDA(dg_launch(h->pdl, kern, grid, dim3(32 * XW_WARPS),                                   \
                       xw_smem<NXV, NTHV>(), h->st, C, h->H, Hfield, chunk, a, b, h->twx,        \

@@ -245,6 +245,7 @@ int dg_chan_cfl_tail(dg_handle *h, int rk_step);
 int dg_col_init(dg_handle *h);
 int dg_col_step_dev(dg_handle *h, int rk_step, bool rd);
 size_t dg_col_smem(const dg_handle *h, int mt, bool fused);
+bool dg_col_fused(const dg_handle *h);
 size_t dg_col_case_bytes();
 int dg_col_batch_build(dg_handle *const *hs, const int *rd, int n, int want_mt, int fused,
                        std::vector<unsigned char> &cases, std::vector<int4> &work, int *mt_out,

@@ -453,7 +453,7 @@ struct GroupedLoop {
     }
     // a group's members share one ragged column launch, so they share the
     // column-stage form their tuning chose (it changes results at round-off)
-    const int fused = a->h->col_fused;
+    const int fused = dg_col_fused(a->h) ? 1 : 0;
     Group *best = nullptr;
     double bd = 1e30;
     for (auto &g : groups) {

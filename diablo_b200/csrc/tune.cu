@@ -20,7 +20,8 @@
 //                       with REM_DIV as its own launch (0), or one CTA per
 //                       mode tile doing every field and REM_DIV (1).  Results
 //                       agree to round-off (the REM_DIV divergence is
-//                       compiled separately in each).
+//                       compiled separately in each).  Cases whose fields
+//                       couple in the right-hand sides always run fused.
 //   DG_TUNE_FFT_PLAN    radix order of the x and z transform plans: 0 the
 //                       largest radix first (128 = 16 x 8), 1 the reverse
 //                       (128 = 8 x 16).  Same transform, different shared-
@@ -244,6 +245,8 @@ extern "C" int dg_autotune(dg_handle *h, int steps_per_trial) {
     float best_ms = 1e30f;
     for (int v : k.vals) {
       if (k.key == DG_TUNE_YCHUNK && v != 0 && v >= h->NY) continue;
+      // a coupled case runs fused whatever the setting: nothing to time
+      if (k.key == DG_TUNE_COL_FUSED && v == 0 && dg_col_fused(h) && h->col_fused == 0) continue;
       if ((s = dg_tune_set(h, k.key, v)) != DG_OK) break;
       float ms = 0.f;
       if ((s = time_steps(h, steps_per_trial, &ms)) != DG_OK) break;

@@ -234,7 +234,9 @@ enum { DG_TUNE_COL_MT = 0, DG_TUNE_XROW_CHUNK = 1, DG_TUNE_YCHUNK = 2, DG_TUNE_C
 /* DG_TUNE_COL_FUSED: the substep's column stage as one CTA per (mode tile,
  * field) with REM_DIV as its own launch (0, default), or one CTA per mode
  * tile doing every field's right-hand side and CN solve and then REM_DIV
- * (1).  Results agree to round-off. */
+ * (1).  Results agree to round-off.  A case whose fields couple in the
+ * right-hand sides (rotation, buoyancy or GRAV terms, DRHODX/Z) always runs
+ * the fused form. */
 /* DG_TUNE_FFT_PLAN: radix order of the x and z transform plans of the
  * substep (0: largest radix first, 128 = 16 x 8; 1: the reverse, 8 x 16).
  * The same transform either way; the autotuner times both per grid shape.

@@ -436,23 +436,33 @@ def test_fft_plan_variant_parity_and_tuning_cache(tmp_path):
                                                   "pdl", "fft_plan", "col_fused")}
 
 
+@pytest.mark.parametrize("case", ["coupled", "uncoupled"])
 @pytest.mark.parametrize("fused,mt", [(0, 2), (0, 16), (1, 4), (1, 16)])
-def test_column_forms_match_oracle(fused, mt):
+def test_column_forms_match_oracle(case, fused, mt):
     """The split and the fused column stage (DG_TUNE_COL_FUSED), at small and
-    large tiles, against the oracle: a stratified KH layer with rotation,
-    gravity in x and z, a Neumann scalar with DRHODX/Z, and COURANT every
-    step (substep 3 stops after the CN solves and projects after COURANT)."""
-    p, gy = configs.kh_shear_layer(nx=32, ny=33, nz=16)
-    p = p.replace(i_ro=0.3, grav_x=0.2, grav_z=-0.1, variable_dt=1, update_dt=1, cfl=0.4, n_th=2)
-    p.ri = [0.1, 0.05, 0, 0]
-    p.pr = [1.0, 0.7, 1, 1]
-    p.th_bc_ymin = [0, 1, 0, 0]
-    p.th_bc_ymax = [0, 1, 0, 0]
-    p.th_bc_ymin_c1 = [-1.0, 0.1, 0, 0]
-    p.th_bc_ymax_c1 = [1.0, -0.2, 0, 0]
-    p.drhodx = [0.0, 0.3, 0, 0]
-    p.drhodz = [0.0, -0.2, 0, 0]
-    ref, ch, _ = start_pair(p, gy, ics.kh_shear_layer, seed=12)
+    large tiles, against the oracle, with COURANT every step (substep 3 stops
+    after the CN solves and projects after COURANT).  "coupled": a stratified
+    KH layer with rotation, gravity in x and z, and a Neumann scalar with
+    DRHODX/Z -- every field's right-hand side reads others, so the split
+    setting runs the fused form; "uncoupled": a small no-slip channel, where
+    the split form runs."""
+    if case == "coupled":
+        p, gy = configs.kh_shear_layer(nx=32, ny=33, nz=16)
+        p = p.replace(i_ro=0.3, grav_x=0.2, grav_z=-0.1, variable_dt=1, update_dt=1, cfl=0.4,
+                      n_th=2)
+        p.ri = [0.1, 0.05, 0, 0]
+        p.pr = [1.0, 0.7, 1, 1]
+        p.th_bc_ymin = [0, 1, 0, 0]
+        p.th_bc_ymax = [0, 1, 0, 0]
+        p.th_bc_ymin_c1 = [-1.0, 0.1, 0, 0]
+        p.th_bc_ymax_c1 = [1.0, -0.2, 0, 0]
+        p.drhodx = [0.0, 0.3, 0, 0]
+        p.drhodz = [0.0, -0.2, 0, 0]
+        maker = ics.kh_shear_layer
+    else:
+        p, gy = configs.channel_re180(nx=48, ny=33, nz=32)
+        maker = ics.channel_laminar
+    ref, ch, _ = start_pair(p, gy, maker, seed=12)
     ch.tune_set(col_fused=fused, cn_mt=mt)
     for s in range(1, 11):
         ref.step(s)

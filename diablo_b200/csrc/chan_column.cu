@@ -288,61 +288,70 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   }
   __syncthreads();
 
-  // ---- 2. CN solves, one lane per (field, mode, re/im part), rows 0..NY+1
-  for (int t = tid; t < 2 * MT * F; t += CS_THR) {
-    const int fl = t / (2 * MT);
+  // ---- 2. CN solves, one lane per (field, mode), rows 0..NY+1.  The operator
+  // is real, so the real and imaginary parts are two independent recurrences;
+  // one lane runs both, interleaved, which hides half of each one's latency.
+  for (int t = tid; t < MT * F; t += CS_THR) {
+    const int fl = t / MT;
     const int f = f0 + fl;
-    const int m = (t >> 1) % MT, part = t & 1;
+    const int m = t - fl * MT;
     const double *T = TB + (long)fl * 5 * L;
     const double *Aa = T, *Rb = T + L, *Cc = T + 2 * L, *K = T + 3 * L, *V = T + 4 * L;
-    double *x = reinterpret_cast<double *>(R + (long)fl * L * MT) + 2 * m + part;
-    constexpr int st = 2 * MT;
-    constexpr int B = 8;  // rows per register block: loads first, then the recurrence
-    const bool mean_re = (m0 + m == 0) && part == 0;
+    double2 *x = R + (long)fl * L * MT + m;
+    constexpr int B = 8;  // rows per register block: loads first, then the recurrences
+    const bool mean = (m0 + m == 0);
     const int wlo = (f >= 3) ? pick(C.JSt, f - 3) - 1 : 1;
-    double g = 0.0;
+    double2 g = make_double2(0.0, 0.0);
     for (int j0 = 0; j0 < L; j0 += B) {
-      double r[B], a[B];
+      double2 r[B];
+      double a[B];
 #pragma unroll
       for (int q = 0; q < B; q++) {
         const int j = j0 + q < L ? j0 + q : L - 1;
         const double kind = K[j];
-        const double xr = x[j * st];
-        r[q] = (kind == (double)ROW_RHS) ? xr : ((kind == (double)ROW_BC && mean_re) ? V[j] : 0.0);
+        const double2 xr = x[j * MT];
+        // a BC row's value goes to the real part of the (0,0) mode only
+        r[q] = (kind == (double)ROW_RHS)
+                   ? xr
+                   : make_double2((kind == (double)ROW_BC && mean) ? V[j] : 0.0, 0.0);
         a[q] = Aa[j];
       }
 #pragma unroll
       for (int q = 0; q < B; q++) {
         if (j0 + q < L) {
-          g = r[q] + a[q] * g;
+          g.x = r[q].x + a[q] * g.x;
+          g.y = r[q].y + a[q] * g.y;
           r[q] = g;
         }
       }
 #pragma unroll
       for (int q = 0; q < B; q++)
-        if (j0 + q < L) x[(j0 + q) * st] = r[q];
+        if (j0 + q < L) x[(j0 + q) * MT] = r[q];
     }
-    double xv = g * Rb[L - 1];
-    x[(L - 1) * st] = xv;
+    const double rbl = Rb[L - 1];
+    double2 xv = make_double2(g.x * rbl, g.y * rbl);
+    x[(L - 1) * MT] = xv;
     for (int j1 = L - 2; j1 >= wlo; j1 -= B) {
-      double gq[B], cq[B], rq[B];
+      double2 gq[B];
+      double cq[B], rq[B];
 #pragma unroll
       for (int q = 0; q < B; q++) {
         const int j = j1 - q >= wlo ? j1 - q : wlo;
-        gq[q] = x[j * st];
+        gq[q] = x[j * MT];
         cq[q] = Cc[j];
         rq[q] = Rb[j];
       }
 #pragma unroll
       for (int q = 0; q < B; q++) {
         if (j1 - q >= wlo) {
-          xv = (gq[q] - cq[q] * xv) * rq[q];
+          xv.x = (gq[q].x - cq[q] * xv.x) * rq[q];
+          xv.y = (gq[q].y - cq[q] * xv.y) * rq[q];
           gq[q] = xv;
         }
       }
 #pragma unroll
       for (int q = 0; q < B; q++)
-        if (j1 - q >= wlo) x[(j1 - q) * st] = gq[q];
+        if (j1 - q >= wlo) x[(j1 - q) * MT] = gq[q];
     }
   }
   __syncthreads();
@@ -382,59 +391,66 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
     RAB[i] = ok ? make_double2(cc.ra[o], cc.rrb[o]) : make_double2(0.0, 0.0);
   }
   __syncthreads();
-  if (tid < 2 * MT) {
-    const int m = tid >> 1;
+  if (tid < MT) {
+    // one lane per mode: the real and imaginary recurrences interleaved
+    const int m = tid;
     const bool mean = (m0 + m == 0);
-    double *x = reinterpret_cast<double *>(GX) + tid;
-    const double *RAd = reinterpret_cast<const double *>(RAB) + 2 * m;  // .x of [j][m]
-    constexpr int st = 2 * MT;
+    double2 *x = GX + m;
+    const double2 *AB = RAB + m;  // (multiplier, reciprocal pivot) of [j][m]
     constexpr int B = 8;
-    double g = 0.0;  // row 1 has a zero right-hand side
-    x[1 * st] = 0.0;
+    double2 g = make_double2(0.0, 0.0);  // row 1 has a zero right-hand side
+    x[1 * MT] = g;
     for (int j0 = 2; j0 <= NY; j0 += B) {
-      double r[B], a[B];
+      double2 r[B];
+      double a[B];
 #pragma unroll
       for (int q = 0; q < B; q++) {
         const int j = j0 + q <= NY ? j0 + q : NY;
-        r[q] = x[j * st];
-        a[q] = RAd[j * st];
+        r[q] = x[j * MT];
+        a[q] = AB[j * MT].x;
       }
 #pragma unroll
       for (int q = 0; q < B; q++) {
         if (j0 + q <= NY) {
-          g = r[q] + a[q] * g;
+          g.x = r[q].x + a[q] * g.x;
+          g.y = r[q].y + a[q] * g.y;
           r[q] = g;
         }
       }
 #pragma unroll
       for (int q = 0; q < B; q++)
-        if (j0 + q <= NY) x[(j0 + q) * st] = r[q];
+        if (j0 + q <= NY) x[(j0 + q) * MT] = r[q];
     }
-    double ph = g * RAd[NY * st + 1];
-    x[NY * st] = ph;
+    const double rbn = AB[NY * MT].y;
+    double2 ph = make_double2(g.x * rbn, g.y * rbn);
+    x[NY * MT] = ph;
     for (int j1 = NY - 1; j1 >= 2; j1 -= B) {
-      double gq[B], uq[B], bq[B];
+      double2 gq[B];
+      double uq[B], bq[B];
 #pragma unroll
       for (int q = 0; q < B; q++) {
         const int j = j1 - q >= 2 ? j1 - q : 2;
-        gq[q] = x[j * st];
+        gq[q] = x[j * MT];
         uq[q] = UU[j];
-        bq[q] = RAd[j * st + 1];
+        bq[q] = AB[j * MT].y;
       }
 #pragma unroll
       for (int q = 0; q < B; q++) {
         if (j1 - q >= 2) {
-          ph = (gq[q] - uq[q] * ph) * bq[q];
+          ph.x = (gq[q].x - uq[q] * ph.x) * bq[q];
+          ph.y = (gq[q].y - uq[q] * ph.y) * bq[q];
           gq[q] = ph;
         }
       }
 #pragma unroll
       for (int q = 0; q < B; q++)
-        if (j1 - q >= 2) x[(j1 - q) * st] = gq[q];
+        if (j1 - q >= 2) x[(j1 - q) * MT] = gq[q];
     }
     const double u1r = mean ? 0.0 : -1.0;
-    ph = (x[1 * st] - u1r * ph) * RAd[1 * st + 1];
-    x[1 * st] = ph;
+    const double2 x1 = x[1 * MT];
+    const double rb1 = AB[1 * MT].y;
+    ph = make_double2((x1.x - u1r * ph.x) * rb1, (x1.y - u1r * ph.y) * rb1);
+    x[1 * MT] = ph;
   }
   __syncthreads();
 

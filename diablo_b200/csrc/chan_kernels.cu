@@ -1307,7 +1307,8 @@ __global__ void k_remdiv_init(int NY, long ss, int nkxp, const double *__restric
 constexpr int COL_THR = 128;
 
 // REM_DIV_CHAN for MT modes: divergence (parallel) -> forward and backward
-// sweeps (per part) -> projection, phi and CP update (parallel).
+// sweeps (one lane per mode, both parts) -> projection, phi and CP update
+// (parallel).
 template <int MT>
 __global__ void __launch_bounds__(COL_THR) k_rd_col(
     int NY, long ss, int nkxp, int JS, int JE, int rk_step, const double *__restrict__ kxv,
@@ -1375,58 +1376,65 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
     }
   }
   __syncthreads();
-  if (tid < 2 * MT) {
-    const int m = tid >> 1;
+  if (tid < MT) {
+    // one lane per mode: the real and imaginary recurrences interleaved
+    const int m = tid;
     const bool mean = (m0 + m == 0);
-    double *x = (double *)GX + tid;
-    constexpr int st = 2 * MT;
+    double2 *x = GX + m;
     constexpr int B = 8;
-    double g = 0.0;  // row 1 has a zero right-hand side
-    x[1 * st] = 0.0;
+    double2 g = make_double2(0.0, 0.0);  // row 1 has a zero right-hand side
+    x[1 * MT] = g;
     for (int j0 = 2; j0 <= NY; j0 += B) {
-      double r[B], a[B];
+      double2 r[B];
+      double a[B];
 #pragma unroll
       for (int q = 0; q < B; q++) {
         const int j = j0 + q <= NY ? j0 + q : NY;
-        r[q] = x[j * st];
+        r[q] = x[j * MT];
         a[q] = RA[j * MT + m];
       }
 #pragma unroll
       for (int q = 0; q < B; q++) {
         if (j0 + q <= NY) {
-          g = r[q] + a[q] * g;
+          g.x = r[q].x + a[q] * g.x;
+          g.y = r[q].y + a[q] * g.y;
           r[q] = g;
         }
       }
 #pragma unroll
       for (int q = 0; q < B; q++)
-        if (j0 + q <= NY) x[(j0 + q) * st] = r[q];
+        if (j0 + q <= NY) x[(j0 + q) * MT] = r[q];
     }
-    double ph = g * RB[NY * MT + m];
-    x[NY * st] = ph;
+    const double rbn = RB[NY * MT + m];
+    double2 ph = make_double2(g.x * rbn, g.y * rbn);
+    x[NY * MT] = ph;
     for (int j1 = NY - 1; j1 >= 2; j1 -= B) {
-      double gq[B], uq[B], bq[B];
+      double2 gq[B];
+      double uq[B], bq[B];
 #pragma unroll
       for (int q = 0; q < B; q++) {
         const int j = j1 - q >= 2 ? j1 - q : 2;
-        gq[q] = x[j * st];
+        gq[q] = x[j * MT];
         uq[q] = UU[j];
         bq[q] = RB[j * MT + m];
       }
 #pragma unroll
       for (int q = 0; q < B; q++) {
         if (j1 - q >= 2) {
-          ph = (gq[q] - uq[q] * ph) * bq[q];
+          ph.x = (gq[q].x - uq[q] * ph.x) * bq[q];
+          ph.y = (gq[q].y - uq[q] * ph.y) * bq[q];
           gq[q] = ph;
         }
       }
 #pragma unroll
       for (int q = 0; q < B; q++)
-        if (j1 - q >= 2) x[(j1 - q) * st] = gq[q];
+        if (j1 - q >= 2) x[(j1 - q) * MT] = gq[q];
     }
     const double u1r = mean ? 0.0 : -1.0;
-    ph = (x[1 * st] - u1r * ph) * RB[1 * MT + m];
-    x[1 * st] = ph;
+    const double2 x1 = x[1 * MT];
+    const double rb1 = RB[1 * MT + m];
+    ph = make_double2((x1.x - u1r * ph.x) * rb1, (x1.y - u1r * ph.y) * rb1);
+    x[1 * MT] = ph;
   }
   __syncthreads();
   const double ihh = (rk_step > 0) ? 1.0 / dscal[1 + rk_step] : 1.0;

@@ -1203,10 +1203,13 @@ struct CnRows {
 };
 
 // blockIdx.x = rk * nfld + field.  The CTA stages the field's row templates
-// into shared memory with coalesced loads, one thread runs the elimination
-// recurrence out of shared memory (the recurrence is sequential in j; only
-// its division and multiply-add are on the critical path), and the CTA
-// writes the table back with coalesced stores.
+// into shared memory with coalesced loads and forms every row's (l, d, u) in
+// parallel; one thread then runs the elimination recurrence, whose critical
+// path per row is a multiply, a multiply-add and a reciprocal: the
+// multiplier is -l times the previous reciprocal pivot, the value the table
+// stores and the solves use (a division there would add a second long
+// operation to every row); the CTA writes the table back with coalesced
+// stores.
 constexpr int CT_THR = 128;
 
 __global__ void __launch_bounds__(CT_THR) k_cn_tables(CnRows P, const double *__restrict__ dscal,
@@ -1216,46 +1219,53 @@ __global__ void __launch_bounds__(CT_THR) k_cn_tables(CnRows P, const double *__
   extern __shared__ double ct_sm[];
   const int L = P.NY + 2;
   const int rk = blockIdx.x / P.nfld, f = blockIdx.x % P.nfld;
-  double *R = ct_sm;          // [8][L]
-  double *T = ct_sm + 8 * L;  // [5][L]
+  double *R = ct_sm;           // [8][L] templates
+  double *T = ct_sm + 8 * L;   // [5][L] the table
+  double *W = T + 5 * L;       // [2][L] l, d of every row
   const double *Rg = rows + (long)f * 8 * L;
   for (int i = threadIdx.x; i < 8 * L; i += CT_THR) R[i] = Rg[i];
   __syncthreads();
+  const double h = dscal[2 + rk];
+  const double s = (P.nu * h / 2.0) / P.pr[f] * P.nuv;
+  for (int j = threadIdx.x; j < L; j += CT_THR) {
+    const bool cn = R[j] == (double)ROW_RHS;
+    W[j] = cn ? s * R[1 * L + j] : R[4 * L + j];               // l
+    W[L + j] = cn ? 1.0 + s * R[2 * L + j] : R[5 * L + j];     // d
+    T[2 * L + j] = cn ? s * R[3 * L + j] : R[6 * L + j];       // u
+    T[3 * L + j] = R[j];                                       // kind
+    T[4 * L + j] = R[7 * L + j];                               // bc value
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
-    const double h = dscal[2 + rk];
-    const double s = (P.nu * h / 2.0) / P.pr[f] * P.nuv;
-    double bprev = 1.0, cprev = 0.0;
-    for (int j = 0; j < L; j++) {
-      const double kind = R[j];
-      double l, d, u;
-      if (kind == (double)ROW_RHS) {
-        l = s * R[1 * L + j];
-        d = 1.0 + s * R[2 * L + j];
-        u = s * R[3 * L + j];
-      } else {
-        l = R[4 * L + j];
-        d = R[5 * L + j];
-        u = R[6 * L + j];
+    constexpr int B = 8;
+    const double *U = T + 2 * L;
+    double rbp = 0.0;  // reciprocal pivot of the previous row
+    for (int j0 = 0; j0 < L; j0 += B) {
+      double l[B], d[B], c[B];
+#pragma unroll
+      for (int q = 0; q < B; q++) {
+        const int j = j0 + q < L ? j0 + q : L - 1;
+        l[q] = W[j];
+        d[q] = W[L + j];
+        c[q] = j > 0 ? U[j - 1] : 0.0;
       }
-      double a = 0.0, b = d;
-      if (j > 0) {
-        a = -l / bprev;
-        b = d + a * cprev;
+#pragma unroll
+      for (int q = 0; q < B; q++) {
+        const int j = j0 + q;
+        if (j < L) {
+          const double a = (j > 0) ? -l[q] * rbp : 0.0;
+          const double b = (j > 0) ? d[q] + a * c[q] : d[q];
+          const double rb = (b != 0.0) ? 1.0 / b : 0.0;
+          T[j] = a;
+          T[L + j] = rb;
+          rbp = rb;
+        }
       }
-      T[0 * L + j] = a;
-      T[1 * L + j] = (b != 0.0) ? 1.0 / b : 0.0;
-      T[2 * L + j] = u;
-      bprev = b;
-      cprev = u;
     }
   }
   __syncthreads();
   double *Tg = tab + (long)(rk * (3 + DG_MAX_TH) + f) * 5 * L;
-  for (int i = threadIdx.x; i < 3 * L; i += CT_THR) Tg[i] = T[i];
-  for (int i = threadIdx.x; i < L; i += CT_THR) {
-    Tg[3 * L + i] = R[i];          // kind
-    Tg[4 * L + i] = R[7 * L + i];  // bc value
-  }
+  for (int i = threadIdx.x; i < 5 * L; i += CT_THR) Tg[i] = T[i];
 }
 
 // ------------------------------------------------------------- REM_DIV
@@ -1743,9 +1753,9 @@ int dg_cn_tables(dg_handle *h) {
   CnRows P;
   P.NY = h->NY; P.nfld = h->nf; P.nu = h->p.nu; P.nuv = h->p.nu_v_scale;
   for (int f = 0; f < 3 + DG_MAX_TH; f++) P.pr[f] = (f >= 3 && f - 3 < h->NTH) ? h->p.pr[f - 3] : 1.0;
-  const size_t sm = sizeof(double) * 13 * (size_t)L;
+  const size_t sm = sizeof(double) * 15 * (size_t)L;
   if (sm > 220 * 1024) {
-    dg_set_error("NY too large for the Crank-Nicolson table kernel (NY + 2 <= 2166)");
+    dg_set_error("NY too large for the Crank-Nicolson table kernel (NY + 2 <= 1877)");
     return DG_ERR_DIMS;
   }
   if (sm > 48 * 1024) dg_big_smem((const void *)k_cn_tables);

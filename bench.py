@@ -59,7 +59,9 @@ def kernel_bytes_per_launch(p, name):
     """Algorithmic HBM bytes of one launch of a channel-substep kernel: each
     array the kernel must read or write, once (stencil neighbours and halo
     rows are free).  Fields are FP64 complex (16 B); the REM_DIV factors are
-    FP64 real.  CF_old is read in substeps 2 and 3 only: counted at 2/3."""
+    FP64 real.  CF_old is read in substeps 2 and 3 only: counted at 2/3.
+    M: retained modes x all planes; Si: x interior planes; Mh, Mi: half-
+    physical values (NZ x (NKX+1) per plane) on all / interior planes."""
     nf = 3 + p.n_th
     nkxp, nkzt = p.nkx + 1, 2 * p.nkz + 1
     L, NY, NZ = p.ny + 2, p.ny, p.nz
@@ -70,11 +72,17 @@ def kernel_bytes_per_launch(p, name):
     table = {
         "k_zinv": c * nf * (M + Mh),
         "k_xrow_w": c * (nf * Mh + 2 * nf * Mi),
-        "k_zfwd_w": c * (2 * nf * Mi + Si * (nf + 1 + nf * 2 / 3) + 2 * nf * Si),
-        "k_cn_col": c * 2 * nf * M,
+        # z forward of the 2 Nf product arrays; writes NL of every field
+        "k_zfwd_w": c * (2 * nf * Mi + nf * Si),
+        # split column form, all fields: read CU, NL, CF_old, CP; write CF, CU
+        "k_col_cn": c * (2 * nf * M + nf * Si * (1 + 2 / 3 + 1) + Si),
+        # fused column form: the same plus REM_DIV's factors, CP and phi
+        "k_col_step": c * (2 * nf * M + nf * Si * (1 + 2 / 3 + 1) + 3 * M) + 8 * 2 * M,
         "k_rd_col": c * (4 * M + 5 * M) + 8 * 2 * M,
         "k_xc2r_cfl": c * 3 * Mh,
     }
+    # the fused form stopping after the CN solves (the substep that runs COURANT)
+    table["k_col_step_cn"] = table["k_col_cn"]
     return table.get(name)
 
 

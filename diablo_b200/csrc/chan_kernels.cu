@@ -535,23 +535,22 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? (sizeof(CX) == 8 ? 4
 #pragma unroll
       for (int i = 0; i < (NX + 31) / 32; i++) {
         const int k = lane + 32 * i;
-        if (k < NX) {
-          const int kk = (k <= NX / 2) ? k : NX - k;
-          CX v = CT<CX>::mk(0, 0);
-          if (kk < NKXP && kk < NX / 2) {
-            CX a = row[fa * Hfield + kk];
-            CX bb = (fb < NF) ? row[fb * Hfield + kk] : CT<CX>::mk(0, 0);
-            if (kk == 0) { a.y = 0.0; bb.y = 0.0; }
-            if (F32 && kk == 0) { a.x = 0.0; bb.x = 0.0; }
-            v = (k == kk) ? CT<CX>::mk(a.x - bb.y, a.y + bb.x)
-                          : CT<CX>::mk(a.x + bb.y, -a.y + bb.x);
-          }
-          buf[q * SSTR + pad(k)] = v;
+        const int kk = (k <= NX / 2) ? k : NX - k;
+        // bins above NKX (the truncated band, the x-Nyquist bin among them)
+        // are zero: the pruned first pass below does not read them
+        if (k < NX && kk < NKXP && kk < NX / 2) {
+          CX a = row[fa * Hfield + kk];
+          CX bb = (fb < NF) ? row[fb * Hfield + kk] : CT<CX>::mk(0, 0);
+          if (kk == 0) { a.y = 0.0; bb.y = 0.0; }
+          if (F32 && kk == 0) { a.x = 0.0; bb.x = 0.0; }
+          buf[q * SSTR + pad(k)] = (k == kk) ? CT<CX>::mk(a.x - bb.y, a.y + bb.x)
+                                             : CT<CX>::mk(a.x + bb.y, -a.y + bb.x);
         }
       }
     }
     __syncwarp();
-    wpasses<NX, +1, 0, PV>(buf, NPIN, SSTR, stw, lane);
+    static_assert(NKXP - 1 == NX / 3, "the truncated band of the pruned pass is NX/3 + 1 ..");
+    wpasses_pz<NX, +1, PV>(buf, NPIN, SSTR, stw, lane);
 #pragma unroll
     for (int q = 0; q < NPIN; q++)
 #pragma unroll

@@ -483,6 +483,55 @@ __device__ __forceinline__ void wpasses_any(C *buf, int nsig, int sstr, const C 
   }
 }
 
+// First pass of an inverse transform whose input is zero in the truncated
+// band [N/3 + 1, N - N/3 - 1] (the 2/3-rule modes the reference zeroes
+// before FFT_XZ_TO_PHYSICAL, for/mpi.f:1640-1655): the pass reads nothing
+// there, so the band of the buffer need not be written beforehand.  NS = 1:
+// no twiddles; the output index of butterfly b is b R + r.
+template <int N, int R, int SIGN, typename C>
+__device__ __forceinline__ void wpass_first_pz(C *__restrict__ buf, int nsig, int sstr,
+                                               int lane) {
+  constexpr int NB = N / R;
+  static_assert(NB <= 32, "warp pass needs N/R <= 32");
+  constexpr int SPR = 32 / NB;
+  constexpr int ZLO = N / 3 + 1, ZHI = N - N / 3 - 1;
+  const int sl = lane / NB, b = lane % NB;
+  for (int s0 = 0; s0 < nsig; s0 += SPR) {
+    const int s = s0 + sl;
+    const bool act = (sl < SPR) && (s < nsig);
+    C v[R];
+    if (act) {
+      const C *in = buf + s * sstr;
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        const int e = b + r * NB;
+        v[r] = (e >= ZLO && e <= ZHI) ? CT<C>::mk(0, 0) : in[pad(e)];
+      }
+      dft<R>(v, SIGN);
+    }
+    __syncwarp();
+    if (act) {
+      C *out = buf + s * sstr;
+#pragma unroll
+      for (int r = 0; r < R; r++) out[pad(b * R + r)] = v[r];
+    }
+    __syncwarp();
+  }
+}
+
+// whole transform with the pruned first pass (lengths whose first pass has
+// at most 32 butterflies; others take wpasses_any)
+template <int N, int SIGN, int V = 0, typename C>
+__device__ __forceinline__ void wpasses_pz(C *buf, int nsig, int sstr, const C *tw, int lane) {
+  constexpr int R0 = plan_radix(N, 0, V);
+  if constexpr (N / R0 <= 32) {
+    wpass_first_pz<N, R0, SIGN>(buf, nsig, sstr, lane);
+    wpasses_any<N, SIGN, 1, V>(buf, nsig, sstr, tw, lane);
+  } else {
+    wpasses_any<N, SIGN, 0, V>(buf, nsig, sstr, tw, lane);
+  }
+}
+
 // Compile-time lengths run in place in buf0 (buf1 unused); the runtime plan
 // ping-pongs between buf0 and buf1.
 template <int N, int V = 0, typename C>
@@ -522,6 +571,20 @@ __device__ __forceinline__ C *fft_cta(C *buf0, C *buf1, const FftPlan &pl,
   } else {
     return fft<N, V>(buf0, buf1, pl, nsig, sig_stride, tw, sign);
   }
+}
+
+// CTA front end of an inverse transform with the truncated band unread
+// (wpass_first_pz); warp-capable lengths only
+template <int N, int V = 0, typename C>
+__device__ __forceinline__ C *fft_cta_inv_pz(C *buf0, int nsig, int sig_stride, const C *tw) {
+  static_assert(N != 0 && warp_fft_ok(N), "pruned transforms need a warp-capable length");
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int per = (nsig + nw - 1) / nw;
+  const int s0 = warp * per;
+  const int ns = (nsig - s0) < per ? (nsig - s0) : per;
+  if (ns > 0) wpasses_pz<N, +1, V>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
+  __syncthreads();
+  return buf0;
 }
 
 // shared buffers a transform of length n needs (1 in place, 2 ping-pong)

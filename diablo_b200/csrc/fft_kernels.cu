@@ -68,16 +68,27 @@ __global__ void __launch_bounds__(NTHR) k_zinv(PA fields, int jmin, long ss, int
       const int kp = packed_index(z, NZ, NKZ);
       v[u] = (idx < KXG * NZ && kp >= 0 && kx0 + c < nkxp) ? in[(long)kp * nkxp + kx0 + c] : zero;
     }
+    // with a compile-time length the first pass skips the truncated band
+    // (NK = N/3), so its zeros are not stored
+    constexpr bool PRUNED = NT != 0 && warp_fft_ok(NT);
+    const bool pz = PRUNED && NKZ == NZ / 3;
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       const int idx = base + u * nthr + tid;
-      if (idx < KXG * NZ)
-        b0[(idx % KXG) * sstr + pad(idx / KXG)] =
+      const int z = idx / KXG;
+      if (idx < KXG * NZ && !(pz && z > NKZ && z < NZ - NKZ))
+        b0[(idx % KXG) * sstr + pad(z)] =
             CT<CX>::mk((typename CT<CX>::T)v[u].x, (typename CT<CX>::T)v[u].y);
     }
   }
   __syncthreads();
-  CX *res = fft_cta<NT, PV>(b0, b1, pl, KXG, sstr, stw, +1);
+  CX *res;
+  if constexpr (NT != 0 && warp_fft_ok(NT)) {
+    if (NKZ == NZ / 3) res = fft_cta_inv_pz<NT, PV>(b0, KXG, sstr, stw);
+    else res = fft_cta<NT, PV>(b0, b1, pl, KXG, sstr, stw, +1);
+  } else {
+    res = fft_cta<NT, PV>(b0, b1, pl, KXG, sstr, stw, +1);
+  }
   CX *out = H + f * Hfield + (long)j * NZ * nkxp;
   for (int idx = tid; idx < KXG * NZ; idx += nthr) {
     const int c = idx % KXG, z = idx / KXG;

@@ -499,30 +499,20 @@ size_t col_smem_f(int L, int F, int mt, int by, int nbox) {
          sizeof(double) * ((size_t)F * 5 * L + 3 * L + 3 * mt) + sizeof(Hdr) + 8 + 128;
 }
 
+// The column kernel: CTA b takes work[b] = (case, mode tile, first field,
+// fields) from the case table (fields = the case's nf in the fused form, 1
+// in the split form; every case at substep rk_step with MT modes per CTA).
+// A single case runs it with a one-case table, so a case computes with the
+// same machine code alone and in an ensemble group (whose launch covers
+// every member's tiles), and its results are bit-identical either way.
 template <int MT>
-__global__ void __launch_bounds__(CS_THR) k_col_step(const __grid_constant__ ColCase cc,
-                                                    int rk_step, int fused, long spin,
-                                                    unsigned extra_tx) {
-  extern __shared__ __align__(128) unsigned char cs_raw[];
-  unsigned char *sbase = cs_raw + ((128u - (dg_smem_addr(cs_raw) & 127u)) & 127u);
-  // fused: grid (tiles); split: grid (tiles, fields)
-  if (fused)
-    col_body<MT>(cc, rk_step, (long)blockIdx.x * MT, 0, cc.C.nf, true, spin, extra_tx, sbase);
-  else
-    col_body<MT>(cc, rk_step, (long)blockIdx.x * MT, blockIdx.y, 1, false, spin, extra_tx, sbase);
-}
-
-// Ragged launch over several cases: CTA b takes work[b] = (case, tile,
-// first field, fields) (every case at substep rk_step, all with MT modes
-// per CTA; fields = the case's nf in the fused form, 1 in the split form).
-template <int MT>
-__global__ void __launch_bounds__(CS_THR) k_col_step_ragged(const ColCase *__restrict__ cases,
-                                                           const int4 *__restrict__ work,
-                                                           int rk_step, int fused) {
+__global__ void __launch_bounds__(CS_THR) k_col_step(const ColCase *__restrict__ cases,
+                                                    const int4 *__restrict__ work, int rk_step,
+                                                    int fused, long spin, unsigned extra_tx) {
   extern __shared__ __align__(128) unsigned char cs_raw[];
   unsigned char *sbase = cs_raw + ((128u - (dg_smem_addr(cs_raw) & 127u)) & 127u);
   const int4 w = work[blockIdx.x];
-  col_body<MT>(cases[w.x], rk_step, (long)w.y * MT, w.z, w.w, fused != 0, DG_ASYNC_SPIN, 0u,
+  col_body<MT>(cases[w.x], rk_step, (long)w.y * MT, w.z, w.w, fused != 0, spin, extra_tx,
                sbase);
 }
 
@@ -640,6 +630,51 @@ static int col_mt(const dg_handle *h, int want, bool fused) {
   return mt;
 }
 
+// the work list of one case: (case 0, tile, first field, fields) per CTA
+static void case_work(const dg_handle *h, int c, int mt, bool fused, std::vector<int4> &work) {
+  const int tiles = dg_cdiv(h->ss, mt);
+  if (fused) {
+    for (int t = 0; t < tiles; t++) work.push_back(make_int4(c, t, 0, h->nf));
+  } else {
+    for (int f = 0; f < h->nf; f++)
+      for (int t = 0; t < tiles; t++) work.push_back(make_int4(c, t, f, 1));
+  }
+}
+
+// The handle's device copies of its case table (rd = 0 and 1) and work list
+// for (mt, fused), rebuilt when either changes.  The copies are synchronous,
+// so they cannot run inside a stream capture: diablo_step's first step of a
+// kind, which runs eagerly, builds them before any capture.
+static int col_tables(dg_handle *h, int mt, bool fused) {
+  if (h->col_dcase && h->col_dmt == mt && h->col_dfused == (int)fused) return DG_OK;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(h->st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+    dg_set_error("the column kernel's case table must be built before a stream capture "
+                 "(run one substep eagerly after changing the tuning)");
+    return DG_ERR_ARG;
+  }
+  ColCase cc[2];
+  DG_TRY(fill_case(h, mt, false, &cc[0]));
+  DG_TRY(fill_case(h, mt, true, &cc[1]));
+  std::vector<int4> work;
+  case_work(h, 0, mt, fused, work);
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  if (h->col_dcase) dg_free(h, h->col_dcase);
+  if (h->col_dwork) dg_free(h, h->col_dwork);
+  h->col_dcase = nullptr;
+  h->col_dwork = nullptr;
+  DG_CUDA(dg_malloc(h, &h->col_dcase, sizeof(cc)));
+  DG_CUDA(dg_malloc(h, (void **)&h->col_dwork, sizeof(int4) * work.size()));
+  DG_CUDA(cudaMemcpyAsync(h->col_dcase, cc, sizeof(cc), cudaMemcpyHostToDevice, h->st));
+  DG_CUDA(cudaMemcpyAsync(h->col_dwork, work.data(), sizeof(int4) * work.size(),
+                          cudaMemcpyHostToDevice, h->st));
+  DG_CUDA(cudaStreamSynchronize(h->st));
+  h->col_dmt = mt;
+  h->col_dfused = fused ? 1 : 0;
+  h->col_dnwork = (int)work.size();
+  return DG_OK;
+}
+
 // The column stage of substep rk_step.  rd = false: stop after the CN
 // solves (the velocity goes out unprojected; COURANT and REM_DIV follow).
 // The split form always stops there, and REM_DIV runs here after it when rd.
@@ -655,20 +690,20 @@ int dg_col_step_dev(dg_handle *h, int rk_step, bool rd) {
     dg_set_error("column kernel: the y-columns of two modes do not fit in shared memory");
     return DG_ERR_DIMS;
   }
-  ColCase cc;
-  DG_TRY(fill_case(h, mt, rd, &cc));
+  DG_TRY(col_tables(h, mt, fused));
+  const ColCase *dcase = reinterpret_cast<const ColCase *>(h->col_dcase) + ((fused && rd) ? 1 : 0);
   // the wait test (DG_TUNE_WAIT_TEST) applies to this one launch
   const long spin = h->wait_test > 0 ? (long)h->wait_test : DG_ASYNC_SPIN;
   const unsigned extra_tx = h->wait_test > 0 ? 16u : 0u;
   h->wait_test = 0;
-  const dim3 grid(dg_cdiv(h->ss, mt), fused ? 1 : h->nf);
   const char *name = fused ? (rd ? "k_col_step" : "k_col_step_cn") : "k_col_cn";
-#define CS_CASE(MTV)                                                                          \
-  if (mt == MTV) {                                                                            \
-    dg_big_smem((const void *)k_col_step<MTV>);                                               \
-    dg_kt_begin(h, name, h->st);                                                              \
-    DG_CUDA(dg_launch(h->pdl, k_col_step<MTV>, grid, dim3(CS_THR), sm, h->st, cc, rk_step,    \
-                      fused ? 1 : 0, spin, extra_tx));                                        \
+#define CS_CASE(MTV)                                                                           \
+  if (mt == MTV) {                                                                             \
+    dg_big_smem((const void *)k_col_step<MTV>);                                                \
+    dg_kt_begin(h, name, h->st);                                                               \
+    DG_CUDA(dg_launch(h->pdl, k_col_step<MTV>, dim3(h->col_dnwork), dim3(CS_THR), sm, h->st,   \
+                      dcase, (const int4 *)h->col_dwork, rk_step, fused ? 1 : 0, spin,         \
+                      extra_tx));                                                              \
   }
   CS_CASE(2) CS_CASE(4) CS_CASE(8) CS_CASE(16)
 #undef CS_CASE
@@ -706,13 +741,7 @@ int dg_col_batch_build(dg_handle *const *hs, const int *rd, int n, int want_mt, 
     ColCase cc;
     DG_TRY(fill_case(hs[c], mt, fused && rd[c] != 0, &cc));
     memcpy(cases.data() + sizeof(ColCase) * c, &cc, sizeof(ColCase));
-    const int tiles = dg_cdiv(hs[c]->ss, mt);
-    if (fused) {
-      for (int t = 0; t < tiles; t++) work.push_back(make_int4(c, t, 0, hs[c]->nf));
-    } else {
-      for (int f = 0; f < hs[c]->nf; f++)
-        for (int t = 0; t < tiles; t++) work.push_back(make_int4(c, t, f, 1));
-    }
+    case_work(hs[c], c, mt, fused != 0, work);
   }
   *mt_out = mt;
   *smem_out = sm;
@@ -723,9 +752,9 @@ int dg_col_batch_launch(cudaStream_t st, int mt, size_t smem, const void *dev_ca
                         const int4 *dev_work, int nwork, int rk_step, int fused) {
 #define CR_CASE(MTV)                                                                              \
   if (mt == MTV) {                                                                                \
-    dg_big_smem((const void *)k_col_step_ragged<MTV>);                                            \
-    k_col_step_ragged<MTV><<<nwork, CS_THR, smem, st>>>((const ColCase *)dev_cases, dev_work,     \
-                                                       rk_step, fused);                           \
+    dg_big_smem((const void *)k_col_step<MTV>);                                                   \
+    k_col_step<MTV><<<nwork, CS_THR, smem, st>>>((const ColCase *)dev_cases, dev_work, rk_step,   \
+                                                fused, (long)DG_ASYNC_SPIN, 0u);                  \
   }
   CR_CASE(2) CR_CASE(4) CR_CASE(8) CR_CASE(16)
 #undef CR_CASE

@@ -160,6 +160,9 @@ struct dg_handle {
   int ychunk;                   // planes per y-chunk of a substep (0 = all)
   double *rowc;                 // per-row grid factors of the column kernel [8][NY+2]
   CnMaps *cs_maps;              // tensor maps of CU for the column kernel
+  void *col_dcase;              // device case table of the column kernel (rd = 0, 1)
+  int4 *col_dwork;              // and its work list
+  int col_dmt, col_dfused, col_dnwork;  // what they were built for
   int cs_maps_mt;               // modes per CTA the maps were built for (0: none)
   int fft_plan;                 // radix-order variant of the x and z transform plans (0, 1)
   int col_fused;                // column stage: 0 split (per field, REM_DIV apart), 1 fused

@@ -23,7 +23,7 @@
 // cases of similar size advance together in groups of up to G.  One RK3
 // step of a group is one CUDA graph: per substep, every member's transform
 // stage (z inverse, x-row products, z forward) runs on the member's own
-// stream, the members join, and ONE ragged column launch (k_col_step_ragged)
+// stream, the members join, and ONE ragged column launch (k_col_step)
 // does the right-hand sides and CN solves (and, in the fused column form,
 // REM_DIV) of every member's modes -- a (case, mode tile, field) work list
 // over all members -- before the members' streams fork again (in the split

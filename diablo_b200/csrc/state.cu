@@ -414,7 +414,7 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
   cudaStreamSynchronize(h->st);
   cudaStreamSynchronize(h->st2);
   void *dp[] = {h->gyf, h->dy, h->dyf, h->kx, h->kz, h->ky, h->kx2, h->kz2, h->ky2, h->twx, h->twz,
-                h->twy, h->twx_f, h->twz_f, h->twy_f, h->dscal, h->cp, h->cr1, h->gphi, h->rem_a, h->rem_rb, h->cn_tab, h->cn_rows, h->rowc, h->H, h->G, h->work, h->dmin_bits, h->dflag, h->Hy, h->P,
+                h->twy, h->twx_f, h->twz_f, h->twy_f, h->dscal, h->cp, h->cr1, h->gphi, h->rem_a, h->rem_rb, h->cn_tab, h->cn_rows, h->rowc, h->col_dcase, h->col_dwork, h->H, h->G, h->work, h->dmin_bits, h->dflag, h->Hy, h->P,
                 h->Q};
   for (void *q : dp) dg_free(h, q);
   dg_free(h, h->les_phys);

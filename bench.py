@@ -63,6 +63,9 @@ def kernel_bytes_per_launch(p, name):
     M: retained modes x all planes; Si: x interior planes; Mh, Mi: half-
     physical values (NZ x (NKX+1) per plane) on all / interior planes."""
     nf = 3 + p.n_th
+    th_copies = sum(1 for n in range(p.n_th)
+                    if p.ri[n] * p.grav_x != 0 or p.ri[n] * p.grav_y != 0
+                    or p.ri[n] * p.grav_z != 0)
     nkxp, nkzt = p.nkx + 1, 2 * p.nkz + 1
     L, NY, NZ = p.ny + 2, p.ny, p.nz
     ss = nkxp * nkzt
@@ -74,15 +77,15 @@ def kernel_bytes_per_launch(p, name):
         "k_xrow_w": c * (nf * Mh + 2 * nf * Mi),
         # z forward of the 2 Nf product arrays; writes NL of every field
         "k_zfwd_w": c * (2 * nf * Mi + nf * Si),
-        # split column form, all fields: read CU, NL, CF_old, CP; write CF, CU
-        "k_col_cn": c * (2 * nf * M + nf * Si * (1 + 2 / 3 + 1) + Si),
-        # fused column form: the same plus REM_DIV's factors, CP and phi
-        "k_col_step": c * (2 * nf * M + nf * Si * (1 + 2 / 3 + 1) + 3 * M) + 8 * 2 * M,
-        "k_rd_col": c * (4 * M + 5 * M) + 8 * 2 * M,
+        # column stage, all fields: read CU, NL, CF_old and CP (once); write
+        # CF and the post-CN field
+        "k_col_cn": c * (2 * nf * M + nf * Si * (1 + 2 / 3 + 1) + M),
+        # REM_DIV from the post-CN velocity: read U and CP, write U, phi and
+        # CP, read the two factor arrays; copy the scalars that a velocity
+        # right-hand side reads (left in the rhs arrays) into CU
+        "k_rd_col": c * (4 * M + 5 * M) + 8 * 2 * M + c * 2 * M * th_copies,
         "k_xc2r_cfl": c * 3 * Mh,
     }
-    # the fused form stopping after the CN solves (the substep that runs COURANT)
-    table["k_col_step_cn"] = table["k_col_cn"]
     return table.get(name)
 
 

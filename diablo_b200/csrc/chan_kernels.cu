@@ -1318,13 +1318,26 @@ constexpr int COL_THR = 128;
 // REM_DIV_CHAN for MT modes: divergence (parallel) -> forward and backward
 // sweeps (one lane per mode, both parts) -> projection, phi and CP update
 // (parallel).
+// The velocity is read from s1..s3 and written to u1..u3: the same arrays for
+// REM_DIV_CHAN on its own (in place), the rhs arrays holding the column
+// stage's post-CN velocity inside a substep.  In that case the rows the
+// projection leaves alone (U1, U3 at NY+1; U2 at 1 and NY+1) and the scalars
+// the column stage also left in the rhs arrays (RdCopy) are copied over too.
+struct RdCopy {
+  const double2 *src[DG_MAX_TH];
+  double2 *dst[DG_MAX_TH];
+  int lo[DG_MAX_TH];  // first row the column stage wrote
+  int n;
+};
+
 template <int MT>
 __global__ void __launch_bounds__(COL_THR) k_rd_col(
     int NY, long ss, int nkxp, int JS, int JE, int rk_step, const double *__restrict__ kxv,
     const double *__restrict__ kzv, const double *__restrict__ dy, const double *__restrict__ dyf,
-    const double *__restrict__ ra, const double *__restrict__ rrb, double2 *__restrict__ u1,
-    double2 *__restrict__ u2, double2 *__restrict__ u3, double2 *__restrict__ cp,
-    double2 *__restrict__ phi_out, const double *__restrict__ dscal) {
+    const double *__restrict__ ra, const double *__restrict__ rrb, const double2 *s1,
+    const double2 *s2, const double2 *s3, double2 *u1, double2 *u2, double2 *u3,
+    double2 *__restrict__ cp, double2 *__restrict__ phi_out, const double *__restrict__ dscal,
+    RdCopy cpy) {
   extern __shared__ double2 csm[];
   const int L = NY + 2;
   const long m0 = (long)blockIdx.x * MT;
@@ -1361,10 +1374,10 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
       const long o = (long)j * ss + m0 + m;
       av[u] = ok ? ra[o] : 0.0;
       bv[u] = ok ? rrb[o] : 0.0;
-      a1[u] = in ? u1[o] : make_double2(0.0, 0.0);
-      a3[u] = in ? u3[o] : make_double2(0.0, 0.0);
-      b2[u] = in ? u2[o] : make_double2(0.0, 0.0);
-      b2p[u] = in ? u2[o + ss] : make_double2(0.0, 0.0);
+      a1[u] = in ? s1[o] : make_double2(0.0, 0.0);
+      a3[u] = in ? s3[o] : make_double2(0.0, 0.0);
+      b2[u] = in ? s2[o] : make_double2(0.0, 0.0);
+      b2p[u] = in ? s2[o + ss] : make_double2(0.0, 0.0);
     }
 #pragma unroll
     for (int u = 0; u < 4; u++) {
@@ -1455,9 +1468,9 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
       const int m = i % MT, j = i / MT;
       const bool ok = i < L * MT && m < mt && j >= 1 && j <= NY;
       const long o = (long)j * ss + m0 + m;
-      a1[u] = ok ? u1[o] : make_double2(0.0, 0.0);
-      a3[u] = ok ? u3[o] : make_double2(0.0, 0.0);
-      b2[u] = (ok && j >= 2) ? u2[o] : make_double2(0.0, 0.0);
+      a1[u] = ok ? s1[o] : make_double2(0.0, 0.0);
+      a3[u] = ok ? s3[o] : make_double2(0.0, 0.0);
+      b2[u] = (ok && j >= 2) ? s2[o] : make_double2(0.0, 0.0);
       pc[u] = (ok && rk_step > 0 && j >= JS && j <= JE) ? cp[o] : make_double2(0.0, 0.0);
     }
 #pragma unroll
@@ -1486,6 +1499,24 @@ __global__ void __launch_bounds__(COL_THR) k_rd_col(
         pc[u].y = pc[u].y + ph.y * ihh;
         cp[o] = pc[u];
       }
+    }
+  }
+  if (s1 == u1) return;
+  // rows the projection does not touch, and the scalars, from the rhs arrays
+  for (int i = tid; i < 3 * MT; i += COL_THR) {
+    const int q = i / MT, m = i - q * MT;
+    if (m >= mt) continue;
+    const long top = (long)(NY + 1) * ss + m0 + m;
+    if (q == 0) { u1[top] = s1[top]; u3[top] = s3[top]; }
+    else if (q == 1) u2[top] = s2[top];
+    else u2[ss + m0 + m] = s2[ss + m0 + m];
+  }
+  for (int c = 0; c < cpy.n; c++) {
+    const double2 *src = cpy.src[c];
+    double2 *dst = cpy.dst[c];
+    for (int i = cpy.lo[c] * MT + tid; i < L * MT; i += COL_THR) {
+      const int j = i / MT, m = i - j * MT;
+      if (m < mt) dst[(long)j * ss + m0 + m] = src[(long)j * ss + m0 + m];
     }
   }
 }
@@ -1778,7 +1809,7 @@ int dg_apply_bc_vel_dev(dg_handle *h) {
   return DG_OK;
 }
 
-int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step) {
+int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step, bool from_rhs) {
   const int L = h->NY + 2;
   auto rd_smem = [&](int m) {
     return sizeof(double2) * L * m + sizeof(double) * (2 * L * m + 3 * L + 2 * m);
@@ -1786,6 +1817,19 @@ int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step) {
   int mt = h->col_mt;  // fewer modes per CTA where a tall column needs it
   while (mt > 4 && rd_smem(mt) > 220 * 1024) mt /= 2;
   const size_t sm = rd_smem(mt);
+  // from_rhs: the column stage left the post-CN velocity (and the scalars a
+  // velocity right-hand side reads) in the rhs arrays
+  const double2 *const *src = from_rhs ? h->rhs : h->cu;
+  RdCopy cpy;
+  memset(&cpy, 0, sizeof(cpy));
+  if (from_rhs)
+    for (int n = 0; n < h->NTH; n++)
+      if (dg_col_th_to_rhs(h, n)) {
+        cpy.src[cpy.n] = h->rhs[3 + n];
+        cpy.dst[cpy.n] = h->cu[3 + n];
+        cpy.lo[cpy.n] = h->jstart_th[n] - 1;
+        cpy.n++;
+      }
 #define RD_CASE(MTV)                                                                          \
   if (mt == MTV) {                                                                            \
     dg_big_smem((const void *)k_rd_col<MTV>);                                                 \
@@ -1793,7 +1837,8 @@ int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step) {
     DG_CUDA(dg_launch(h->pdl && update_cp, k_rd_col<MTV>, dim3(dg_cdiv(h->ss, MTV)),           \
                       dim3(COL_THR), sm, h->st, h->NY, h->ss, h->nkxp, h->jstart, h->jend,    \
                       update_cp ? rk_step : 0, h->kx, h->kz, h->dy, h->dyf, h->rem_a,         \
-                      h->rem_rb, h->cu[0], h->cu[1], h->cu[2], h->cp, h->cr1, h->dscal));     \
+                      h->rem_rb, src[0], src[1], src[2], h->cu[0], h->cu[1], h->cu[2], h->cp, \
+                      h->cr1, h->dscal, cpy));                                                \
   }
   RD_CASE(4) RD_CASE(8) RD_CASE(16)
 #undef RD_CASE
@@ -1892,8 +1937,6 @@ int dg_dt_commit(dg_handle *h) {
 }
 
 int dg_chan_init(dg_handle *h) {
-  h->cs_maps = new CnMaps();
-  h->cs_maps_mt = 0;
   DG_TRY(dg_col_init(h));
   dg_kt_begin(h, "k_remdiv_init", h->st);
   k_remdiv_init<<<dg_cdiv(h->ss, 128), 128, 0, h->st>>>(h->NY, h->ss, h->nkxp, h->kx, h->kz, h->dy,
@@ -2209,9 +2252,10 @@ bool dg_chan_cfl(const dg_handle *h, int time_step, int rk_step) {
 // while COURANT's reduction finishes on the side stream, then the new
 // DELTA_T is committed.
 int dg_chan_cfl_tail(dg_handle *h, int rk_step) {
-  const double2 *u[3] = {h->cu[0], h->cu[1], h->cu[2]};
+  // the column stage left the post-CN velocity in the rhs arrays
+  const double2 *u[3] = {h->rhs[0], h->rhs[1], h->rhs[2]};
   DG_TRY(dg_courant_dev(h, u, true));
-  DG_TRY(dg_rem_div_dev(h, 1, rk_step));
+  DG_TRY(dg_rem_div_dev(h, 1, rk_step, true));
   DG_CUDA(cudaStreamWaitEvent(h->st, h->ev_cfl1, 0));
   return dg_dt_commit(h);
 }
@@ -2232,7 +2276,7 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
 
 extern "C" int diablo_rem_div_chan(dg_handle *h) {
   if (!h || h->periodic) return DG_ERR_ARG;
-  return dg_rem_div_dev(h, 0, 0);
+  return dg_rem_div_dev(h, 0, 0, false);
 }
 
 extern "C" int diablo_apply_bc_vel(dg_handle *h) {

@@ -76,12 +76,6 @@ enum { F_U1 = 0, F_U2 = 1, F_U3 = 2, F_TH0 = 3 };
 
 struct dg_ktimer;
 
-// Tensor maps of the CU columns, one per field: 2-D over [plane][2 ss
-// doubles] (the column kernel stages every field's tile).
-struct CnMaps {
-  CUtensorMap m[3 + DG_MAX_TH];
-};
-
 struct dg_handle {
   dg_params p;
   int NX, NY, NZ, NTH, NKX, NKZ, TNKZ, NKY, TNKY;
@@ -159,13 +153,10 @@ struct dg_handle {
   int xrow_chunk;               // planes per CTA of the x-row product kernel (0 = auto)
   int ychunk;                   // planes per y-chunk of a substep (0 = all)
   double *rowc;                 // per-row grid factors of the column kernel [8][NY+2]
-  CnMaps *cs_maps;              // tensor maps of CU for the column kernel
-  void *col_dcase;              // device case table of the column kernel (rd = 0, 1)
+  void *col_dcase;              // device case table of the column kernel (one case)
   int4 *col_dwork;              // and its work list
-  int col_dmt, col_dfused, col_dnwork;  // what they were built for
-  int cs_maps_mt;               // modes per CTA the maps were built for (0: none)
+  int col_dmt, col_dnwork;      // the modes per CTA they were built for; CTAs
   int fft_plan;                 // radix-order variant of the x and z transform plans (0, 1)
-  int col_fused;                // column stage: 0 split (per field, REM_DIV apart), 1 fused
   int zf_nlo;                   // the z forward writes only the nonlinear terms (the
                                 // column kernel assembles the right-hand sides)
   int wait_test;                // test only: poll limit of the next column-kernel launch,
@@ -231,7 +222,7 @@ int dg_zfwd_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax,
 int dg_chan_init(dg_handle *h);
 int dg_per_init(dg_handle *h);
 int dg_apply_bc_vel_dev(dg_handle *h);
-int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step);
+int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step, bool from_rhs);
 int dg_courant_dev(dg_handle *h, const double2 *const *u, bool side = false);
 int dg_stats_dev(dg_handle *h, dg_stats *s);
 int dg_per_stats(dg_handle *h, dg_stats *s);
@@ -247,14 +238,12 @@ bool dg_chan_cfl(const dg_handle *h, int time_step, int rk_step);
 int dg_chan_cfl_tail(dg_handle *h, int rk_step);
 int dg_col_init(dg_handle *h);
 int dg_col_step_dev(dg_handle *h, int rk_step, bool rd);
-size_t dg_col_smem(const dg_handle *h, int mt, bool fused);
-bool dg_col_fused(const dg_handle *h);
-size_t dg_col_case_bytes();
-int dg_col_batch_build(dg_handle *const *hs, const int *rd, int n, int want_mt, int fused,
-                       std::vector<unsigned char> &cases, std::vector<int4> &work, int *mt_out,
-                       size_t *smem_out);
+size_t dg_col_smem(const dg_handle *h, int mt);
+bool dg_col_th_to_rhs(const dg_handle *h, int n);
+int dg_col_batch_build(dg_handle *const *hs, int n, int want_mt, std::vector<unsigned char> &cases,
+                       std::vector<int4> &work, int *mt_out, size_t *smem_out);
 int dg_col_batch_launch(cudaStream_t st, int mt, size_t smem, const void *dev_cases,
-                        const int4 *dev_work, int nwork, int rk_step, int fused);
+                        const int4 *dev_work, int nwork, int rk_step);
 
 #define DG_CASE_N(N) \
   case N:            \

@@ -866,7 +866,7 @@ int dg_les_post(dg_handle *h, int time_step, int rk_step, bool sgs) {
   double2 *v[3 + DG_MAX_TH];
   for (int f = 0; f < h->nf; f++) v[f] = h->cu[f];
   DG_TRY(to_fourier(h, pslot(h, PS_U), h->nf, 0, NY + 1, v));
-  DG_TRY(dg_rem_div_dev(h, 1, rk_step));
+  DG_TRY(dg_rem_div_dev(h, 1, rk_step, false));
   if (cfl) DG_TRY(dg_dt_commit(h));
   return DG_OK;
 }

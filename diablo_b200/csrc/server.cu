@@ -23,12 +23,10 @@
 // cases of similar size advance together in groups of up to G.  One RK3
 // step of a group is one CUDA graph: per substep, every member's transform
 // stage (z inverse, x-row products, z forward) runs on the member's own
-// stream, the members join, and ONE ragged column launch (k_col_step)
-// does the right-hand sides and CN solves (and, in the fused column form,
-// REM_DIV) of every member's modes -- a (case, mode tile, field) work list
-// over all members -- before the members' streams fork again (in the split
-// form each member's REM_DIV then runs on its own stream).  A group's
-// members share the column form their tuning chose.  Groups run
+// stream, the members join, and ONE ragged column launch (k_col_cn) does
+// the right-hand sides and CN solves of every member's modes -- a (case,
+// mode tile, field) work list over all members -- before the members'
+// streams fork again for their REM_DIV (and COURANT) kernels.  Groups run
 // concurrently on their own streams.  A
 // group is re-captured when a member joins or leaves (at step boundaries,
 // after the group's steps in flight have finished).  Results are the same
@@ -96,9 +94,8 @@ struct Group {
   cudaEvent_t ev_fork = nullptr;
   std::vector<cudaEvent_t> ev_m;   // one per member: joins into gs
   cudaEvent_t ev_col = nullptr;    // column launch done: members fork from it
-  void *d_cases[3] = {nullptr, nullptr, nullptr};  // case tables per substep (rd differs at 3)
-  int4 *d_work = nullptr;
-  int fused = 0;                   // the members' column-stage form (all the same)
+  void *d_cases = nullptr;         // the column kernel's case table
+  int4 *d_work = nullptr;          // and its work list
   int nwork = 0, mt = 0;
   size_t smem = 0;
   cudaGraphExec_t exec = nullptr;
@@ -407,10 +404,8 @@ struct GroupedLoop {
   void free_graph(Group &g) {
     if (g.exec) cudaGraphExecDestroy(g.exec);
     g.exec = nullptr;
-    for (void *&d : g.d_cases) {
-      if (d) cudaFree(d);
-      d = nullptr;
-    }
+    if (g.d_cases) cudaFree(g.d_cases);
+    g.d_cases = nullptr;
     if (g.d_work) cudaFree(g.d_work);
     g.d_work = nullptr;
   }
@@ -451,23 +446,17 @@ struct GroupedLoop {
       solo.push_back(a);
       return;
     }
-    // a group's members share one ragged column launch, so they share the
-    // column-stage form their tuning chose (it changes results at round-off)
-    const int fused = dg_col_fused(a->h) ? 1 : 0;
     Group *best = nullptr;
     double bd = 1e30;
     for (auto &g : groups) {
-      if ((int)g->m.size() >= s->group_cases || g->fused != fused) continue;
+      if ((int)g->m.size() >= s->group_cases) continue;
       const double d = fabs(log(pts(a) / g->points));
       if (d < log(4.0) && d < bd) {
         bd = d;
         best = g.get();
       }
     }
-    if (!best) {
-      best = new_group();
-      best->fused = fused;
-    }
+    if (!best) best = new_group();
     best->m.push_back(a);
     double sum = 0;
     for (Active *x : best->m) sum += pts(x);
@@ -508,14 +497,13 @@ struct GroupedLoop {
         DG_CUDA(cudaEventRecord(g.ev_m[c], h->st));
         DG_CUDA(cudaStreamWaitEvent(g.gs, g.ev_m[c], 0));
       }
-      DG_TRY(dg_col_batch_launch(g.gs, g.mt, g.smem, g.d_cases[rk - 1], g.d_work, g.nwork, rk,
-                                 g.fused));
+      DG_TRY(dg_col_batch_launch(g.gs, g.mt, g.smem, g.d_cases, g.d_work, g.nwork, rk));
       DG_CUDA(cudaEventRecord(g.ev_col, g.gs));
       for (Active *a : g.m) {
         dg_handle *h = a->h;
         DG_CUDA(cudaStreamWaitEvent(h->st, g.ev_col, 0));
         if (dg_chan_cfl(h, 2, rk)) DG_TRY(dg_chan_cfl_tail(h, rk));
-        else if (!g.fused) DG_TRY(dg_rem_div_dev(h, 1, rk));  // the split form's REM_DIV
+        else DG_TRY(dg_rem_div_dev(h, 1, rk, true));
       }
     }
     for (int c = 0; c < n; c++) {
@@ -545,21 +533,16 @@ struct GroupedLoop {
     }
     int want = 16;
     for (dg_handle *h : hs) want = std::min(want, h->cn_mt);
-    for (int rk = 1; rk <= 3; rk++) {
-      std::vector<int> rd;
-      for (dg_handle *h : hs) rd.push_back(dg_chan_cfl(h, 2, rk) ? 0 : 1);
+    {
       std::vector<unsigned char> tab;
       std::vector<int4> work;
-      DG_TRY(dg_col_batch_build(hs.data(), rd.data(), (int)hs.size(), want, g.fused, tab, work,
-                                &g.mt, &g.smem));
-      DG_CUDA(cudaMalloc(&g.d_cases[rk - 1], tab.size()));
-      DG_CUDA(cudaMemcpy(g.d_cases[rk - 1], tab.data(), tab.size(), cudaMemcpyHostToDevice));
-      if (rk == 1) {
-        g.nwork = (int)work.size();
-        DG_CUDA(cudaMalloc((void **)&g.d_work, sizeof(int4) * work.size()));
-        DG_CUDA(cudaMemcpy(g.d_work, work.data(), sizeof(int4) * work.size(),
-                           cudaMemcpyHostToDevice));
-      }
+      DG_TRY(dg_col_batch_build(hs.data(), (int)hs.size(), want, tab, work, &g.mt, &g.smem));
+      DG_CUDA(cudaMalloc(&g.d_cases, tab.size()));
+      DG_CUDA(cudaMemcpy(g.d_cases, tab.data(), tab.size(), cudaMemcpyHostToDevice));
+      g.nwork = (int)work.size();
+      DG_CUDA(cudaMalloc((void **)&g.d_work, sizeof(int4) * work.size()));
+      DG_CUDA(cudaMemcpy(g.d_work, work.data(), sizeof(int4) * work.size(),
+                         cudaMemcpyHostToDevice));
     }
     DG_CUDA(cudaStreamBeginCapture(g.gs, cudaStreamCaptureModeThreadLocal));
     for (dg_handle *h : hs) h->capturing = true;

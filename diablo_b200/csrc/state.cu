@@ -433,7 +433,6 @@ extern "C" int diablo_gpu_finalize(dg_handle *h) {
   dg_kt_free(h);
   dg_graphs_free(h);
   free(h->h_ubar);
-  delete h->cs_maps;
   cudaEventDestroy(h->ev_fork);
   cudaEventDestroy(h->ev_join);
   cudaEventDestroy(h->ev_cfl0);

@@ -5,10 +5,10 @@
 //                       REM_DIV_CHAN, and the substep that runs COURANT): 4, 8
 //                       or 16.
 //   DG_TUNE_CN_MT       modes per CTA of the substep's column kernel
-//                       (k_col_step: right-hand sides, CN solves and, fused,
-//                       REM_DIV): 2, 4, 8 or 16.  Fewer modes per CTA means more CTAs
-//                       resident per SM to hide the column loads; more means
-//                       more sweep lanes per CTA.
+//                       (k_col_cn: right-hand side and CN solve of one field):
+//                       2, 4, 8 or 16.  Fewer modes per CTA means more CTAs
+//                       and smaller tiles to stage; more means more sweep
+//                       lanes per CTA.
 //   DG_TUNE_XROW_CHUNK  y-planes one CTA of the x-row product kernel marches
 //                       through (0 = automatic).  Longer marches re-read fewer
 //                       halo planes; shorter ones give more CTAs.
@@ -16,12 +16,6 @@
 //                       chunks keep the intermediate planes in L2.
 //   DG_TUNE_PDL         1 (default): the substep kernels are launched with
 //                       programmatic dependent launch; 0: plain launches.
-//   DG_TUNE_COL_FUSED   the column stage as one CTA per (mode tile, field)
-//                       with REM_DIV as its own launch (0), or one CTA per
-//                       mode tile doing every field and REM_DIV (1).  Results
-//                       agree to round-off (the REM_DIV divergence is
-//                       compiled separately in each).  Cases whose fields
-//                       couple in the right-hand sides always run fused.
 //   DG_TUNE_FFT_PLAN    radix order of the x and z transform plans: 0 the
 //                       largest radix first (128 = 16 x 8), 1 the reverse
 //                       (128 = 8 x 16).  Same transform, different shared-
@@ -61,10 +55,10 @@
 namespace {
 
 constexpr int kTuneKeys[] = {DG_TUNE_COL_MT, DG_TUNE_XROW_CHUNK, DG_TUNE_YCHUNK, DG_TUNE_CN_MT,
-                             DG_TUNE_PDL, DG_TUNE_FFT_PLAN, DG_TUNE_COL_FUSED};
+                             DG_TUNE_PDL, DG_TUNE_FFT_PLAN};
 constexpr const char *kTuneNames[] = {"col_mt", "xrow_chunk", "ychunk", "cn_mt", "pdl",
-                                      "fft_plan", "col_fused"};
-constexpr int kNTune = 7;
+                                      "fft_plan"};
+constexpr int kNTune = 6;
 
 struct TuneRec {
   int v[kNTune];
@@ -125,10 +119,6 @@ extern "C" int dg_tune_set(dg_handle *h, int key, int value) {
       if (value != 0 && value != 1) return DG_ERR_ARG;
       h->fft_plan = value;
       break;
-    case DG_TUNE_COL_FUSED:
-      if (value != 0 && value != 1) return DG_ERR_ARG;
-      h->col_fused = value;
-      break;
     default:
       return DG_ERR_ARG;
   }
@@ -146,7 +136,6 @@ extern "C" int dg_tune_get(dg_handle *h, int key, int *value) {
     case DG_TUNE_PDL: *value = h->pdl; return DG_OK;
     case DG_TUNE_WAIT_TEST: *value = h->wait_test; return DG_OK;
     case DG_TUNE_FFT_PLAN: *value = h->fft_plan; return DG_OK;
-    case DG_TUNE_COL_FUSED: *value = h->col_fused; return DG_OK;
     default: return DG_ERR_ARG;
   }
 }
@@ -232,7 +221,6 @@ extern "C" int dg_autotune(dg_handle *h, int steps_per_trial) {
     std::vector<int> vals;
   };
   std::vector<Knob> knobs = {
-      {DG_TUNE_COL_FUSED, {0, 1}},
       {DG_TUNE_CN_MT, {2, 4, 8, 16}},
       {DG_TUNE_COL_MT, {4, 8, 16}},
       {DG_TUNE_XROW_CHUNK, {0, 2, 4, 8, 16}},
@@ -245,8 +233,6 @@ extern "C" int dg_autotune(dg_handle *h, int steps_per_trial) {
     float best_ms = 1e30f;
     for (int v : k.vals) {
       if (k.key == DG_TUNE_YCHUNK && v != 0 && v >= h->NY) continue;
-      // a coupled case runs fused whatever the setting: nothing to time
-      if (k.key == DG_TUNE_COL_FUSED && v == 0 && dg_col_fused(h) && h->col_fused == 0) continue;
       if ((s = dg_tune_set(h, k.key, v)) != DG_OK) break;
       float ms = 0.f;
       if ((s = time_steps(h, steps_per_trial, &ms)) != DG_OK) break;
@@ -387,7 +373,7 @@ extern "C" int dg_tune_cache_load(const char *path) {
     do {
       std::string key;
       if (!str(key) || !ch(':') || !ch('{')) return bad();
-      TuneRec rec = {{8, 0, 0, 4, 1, 0, 0}};
+      TuneRec rec = {{8, 0, 0, 4, 1, 0}};
       if (!ch('}')) {
         do {
           std::string name;

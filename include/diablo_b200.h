@@ -221,22 +221,15 @@ int dg_timing_read(dg_handle *h, int i, char *name, int name_len, int64_t *launc
 /* -------------------------------------------------------------- tuning */
 /* No counterpart in the reference.  Launch shapes of the channel substep:
  * modes per CTA of the REM_DIV y-column kernel (4, 8, 16) and of the substep's
- * column kernel (right-hand sides, CN solves, REM_DIV; 2, 4, 8, 16), y-planes per CTA of the
- * x-row product kernel (0 = automatic), planes per y-chunk of a substep
- * (0 = all).  Results do not depend on them (DG_TUNE_FFT_PLAN and
- * DG_TUNE_COL_FUSED below: at round-off level only).  dg_autotune times
- * candidates on
- * the handle's own state (steps_per_trial eager RK3 steps each), keeps the
+ * column kernel (one field's right-hand side and CN solve; 2, 4, 8, 16),
+ * y-planes per CTA of the x-row product kernel (0 = automatic), planes per
+ * y-chunk of a substep (0 = all).  Results do not depend on them
+ * (DG_TUNE_FFT_PLAN below: at round-off level only).  dg_autotune times
+ * candidates on the handle's own state (steps_per_trial eager RK3 steps each), keeps the
  * fastest and restores the state, TIME and DELTA_T; it allocates temporary
  * device copies of the state while it runs. */
 enum { DG_TUNE_COL_MT = 0, DG_TUNE_XROW_CHUNK = 1, DG_TUNE_YCHUNK = 2, DG_TUNE_CN_MT = 3,
-       DG_TUNE_PDL = 4, DG_TUNE_WAIT_TEST = 5, DG_TUNE_FFT_PLAN = 6, DG_TUNE_COL_FUSED = 7 };
-/* DG_TUNE_COL_FUSED: the substep's column stage as one CTA per (mode tile,
- * field) with REM_DIV as its own launch (0, default), or one CTA per mode
- * tile doing every field's right-hand side and CN solve and then REM_DIV
- * (1).  Results agree to round-off.  A case whose fields couple in the
- * right-hand sides (rotation, buoyancy or GRAV terms, DRHODX/Z) always runs
- * the fused form. */
+       DG_TUNE_PDL = 4, DG_TUNE_WAIT_TEST = 5, DG_TUNE_FFT_PLAN = 6 };
 /* DG_TUNE_FFT_PLAN: radix order of the x and z transform plans of the
  * substep (0: largest radix first, 128 = 16 x 8; 1: the reverse, 8 x 16).
  * The same transform either way; the autotuner times both per grid shape.
@@ -259,7 +252,7 @@ int dg_autotune(dg_handle *h, int steps_per_trial);
  * shape (*hit = 1) or leaves h as it is (*hit = 0); dg_tune_cache_get reads
  * one stored value for a shape (DG_ERR_ARG when absent).  The table persists
  * in a JSON file, {"NXxNYxNZ_thN_fp64|mixed": {"col_mt": .., "xrow_chunk": ..,
- * "ychunk": .., "cn_mt": .., "pdl": .., "fft_plan": .., "col_fused": ..},
+ * "ychunk": .., "cn_mt": .., "pdl": .., "fft_plan": ..},
  * ...}: _save writes the whole table, _load merges a file's entries into it. */
 int dg_tune_lookup(dg_handle *h, int *hit);
 int dg_tune_cache_get(const dg_params *p, int key, int *value);

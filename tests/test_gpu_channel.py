@@ -339,7 +339,7 @@ def test_autotune_restores_state_and_keeps_results():
     for nm, v in before.items():
         assert np.array_equal(b.get_field(nm), v), nm
     assert b.get_time() == t0
-    a.tune_set(fft_plan=chosen["fft_plan"], col_fused=chosen["col_fused"])
+    a.tune_set(fft_plan=chosen["fft_plan"])
     for s in range(1, 6):
         a.step(s)
     b.steps(1, 5)
@@ -348,7 +348,7 @@ def test_autotune_restores_state_and_keeps_results():
     for mt in (4, 16):
         b.tune_set(col_mt=mt, cn_mt=20 - mt, xrow_chunk=3, ychunk=20)
         c = channel(p, gy)
-        c.tune_set(fft_plan=chosen["fft_plan"], col_fused=chosen["col_fused"])
+        c.tune_set(fft_plan=chosen["fft_plan"])
         c.set_state(ref.state())
         c.set_time(0.0, p.delta_t)
         b.set_state(ref.state())
@@ -433,19 +433,19 @@ def test_fft_plan_variant_parity_and_tuning_cache(tmp_path):
     key = f"{p.nx}x{p.ny}x{p.nz}_th{p.n_th}_fp64"
     assert json.loads(path.read_text())[key] == {k: tuned[k] for k in
                                                  ("col_mt", "xrow_chunk", "ychunk", "cn_mt",
-                                                  "pdl", "fft_plan", "col_fused")}
+                                                  "pdl", "fft_plan")}
 
 
 @pytest.mark.parametrize("case", ["coupled", "uncoupled"])
-@pytest.mark.parametrize("fused,mt", [(0, 2), (0, 16), (1, 4), (1, 16)])
-def test_column_forms_match_oracle(case, fused, mt):
-    """The split and the fused column stage (DG_TUNE_COL_FUSED), at small and
-    large tiles, against the oracle, with COURANT every step (substep 3 stops
-    after the CN solves and projects after COURANT).  "coupled": a stratified
-    KH layer with rotation, gravity in x and z, and a Neumann scalar with
-    DRHODX/Z -- every field's right-hand side reads others, so the split
-    setting runs the fused form; "uncoupled": a small no-slip channel, where
-    the split form runs."""
+@pytest.mark.parametrize("mt", [2, 4, 16])
+def test_column_stage_tiles_match_oracle(case, mt):
+    """The column stage at small and large tiles (DG_TUNE_CN_MT) against the
+    oracle, with COURANT every step (substep 3 runs COURANT on the post-CN
+    velocity before the projection).  "coupled": a stratified KH layer with
+    rotation, gravity in x and z, and a Neumann scalar with DRHODX/Z -- every
+    field's right-hand side reads others, and both scalars go through the
+    rhs arrays; "uncoupled": a small no-slip channel with a passive scalar
+    written in place."""
     if case == "coupled":
         p, gy = configs.kh_shear_layer(nx=32, ny=33, nz=16)
         p = p.replace(i_ro=0.3, grav_x=0.2, grav_z=-0.1, variable_dt=1, update_dt=1, cfl=0.4,
@@ -461,9 +461,16 @@ def test_column_forms_match_oracle(case, fused, mt):
         maker = ics.kh_shear_layer
     else:
         p, gy = configs.channel_re180(nx=48, ny=33, nz=32)
+        p = p.replace(n_th=1)
+        p.pr = [0.71, 1, 1, 1]
+        p.ri = [0.0, 0, 0, 0]
+        p.th_bc_ymin = [0, 0, 0, 0]
+        p.th_bc_ymax = [0, 0, 0, 0]
+        p.th_bc_ymin_c1 = [-1.0, 0, 0, 0]
+        p.th_bc_ymax_c1 = [1.0, 0, 0, 0]
         maker = ics.channel_laminar
     ref, ch, _ = start_pair(p, gy, maker, seed=12)
-    ch.tune_set(col_fused=fused, cn_mt=mt)
+    ch.tune_set(cn_mt=mt)
     for s in range(1, 11):
         ref.step(s)
         ch.step(s)

@@ -22,7 +22,7 @@ def test_cache_round_trip(tmp_path):
     _lib.tune_cache_save(str(out))
     table = json.loads(out.read_text())
     assert table[key] == {"col_mt": 16, "xrow_chunk": 8, "ychunk": 0, "cn_mt": 2, "pdl": 1,
-                          "fft_plan": 1, "col_fused": 0}
+                          "fft_plan": 1}
 
 
 def test_cache_rejects_malformed_file(tmp_path):

@@ -12,19 +12,30 @@
 //   CN solves        for/channel.f:771-1029 (THOMAS_*_MPI, for/mpi.f:630-866)
 // REM_DIV_CHAN and the pressure update follow as their own launch (k_rd_col).
 //
-// One CTA per (mode tile, field).  Every input tile of the field -- CU, the
-// nonlinear term NL that the z-forward kernel left in the field's rhs array,
-// CF_old (substeps 2, 3) and CP (velocity fields) -- arrives in shared
-// memory by bulk tensor copies (TMA, no multicast), all issued at once by one
-// thread and completed on one mbarrier with a bounded wait, so the CTA has
-// its whole column in flight before it computes anything.  The right-hand
-// side is formed in place of NL, the CN recurrences (one lane per mode, the
-// real and imaginary parts interleaved) run in shared memory with the row
-// tables staged there too, and the post-CN field goes to the field's rhs
-// array: CU is read-only in this kernel, so a field's right-hand side may
-// read another field (rotation, buoyancy, GRAV, DRHODX/Z) without a race.
-// REM_DIV then reads the post-CN velocity from the rhs arrays and writes CU.
-// A scalar that no velocity right-hand side reads is written in place.
+// One CTA per (mode tile, field); one thread per (mode, segment of SEG_K
+// consecutive rows).  The CN system of a field is the same for every mode,
+// and its elimination (the substep's table: multipliers a, reciprocal pivots
+// 1/b, upper diagonal c) turns the solve into two first-order linear
+// recurrences, forward g(j) = r(j) + a(j) g(j-1) and backward
+// x(j) = e(j) + f(j) x(j+1) with e = g/b, f = -c/b.  A linear recurrence
+// splits exactly over segments: each thread runs its segment from a zero
+// start, keeping the product of the coefficients; one lane per mode then
+// carries the segment ends across the column (NSEG steps instead of NY + 2),
+// and each thread adds carry x product to its rows.  The same algebra as
+// THOMAS_FORWARD / THOMAS_BACKWARD, with the rounding of a different order
+// of the same operations.  Segment boundaries depend only on NY, so a mode's
+// arithmetic does not depend on the tile width.
+//
+// CU arrives in shared memory by one bulk tensor copy per box (TMA, no
+// multicast) completed on an mbarrier with a bounded wait; each thread's NL,
+// CF_old and CP rows are plain loads issued before that wait.  The right-
+// hand side is formed in registers, the post-CN field goes to the field's
+// rhs array (which held the NL term the kernel consumes: every element is
+// read and written by the same thread).  CU is read-only in this kernel, so
+// a field's right-hand side may read another field (rotation, buoyancy,
+// GRAV, DRHODX/Z) without a race.  REM_DIV then reads the post-CN velocity
+// from the rhs arrays and writes CU.  A scalar that no velocity right-hand
+// side reads is written in place.
 //
 // The same kernel serves one case (a one-case table) and the ensemble
 // server's groups (a ragged (case, tile, field) work list over every member),
@@ -38,7 +49,8 @@
 
 namespace {
 
-constexpr int CS_THR = 128;
+constexpr int SEG_K = 8;         // rows per segment of the CN recurrences
+constexpr int COL_MAX_THR = 256; // threads per CTA: MT x segments, rounded up to warps
 
 struct ColConst {
   int NY, nf, nth, nkxp, JS, JE;
@@ -52,14 +64,15 @@ struct ColConst {
 // Everything the column stage of one case needs, in device memory (tensor
 // maps first: 64-byte aligned).  Maps are 2-D over [plane][2 ss doubles].
 struct ColCase {
-  CUtensorMap map_cu[3 + DG_MAX_TH], map_nl[3 + DG_MAX_TH], map_cf[3 + DG_MAX_TH];
-  CUtensorMap map_cp;
+  CUtensorMap map_cu[3 + DG_MAX_TH];
   ColConst C;
   const double *dscal, *tab, *kxv, *kzv, *rowc;
+  const double2 *cp;
   const double2 *cu[3 + DG_MAX_TH];
-  double2 *cf[3 + DG_MAX_TH], *out[3 + DG_MAX_TH];  // out: the rhs arrays
+  const double2 *nl[3 + DG_MAX_TH];  // the z forward's NL terms (rhs arrays)
+  double2 *cf[3 + DG_MAX_TH], *out[3 + DG_MAX_TH];
   int *err;
-  int by, nbox;
+  int by, nbox, nseg;
 };
 
 template <typename T>
@@ -70,267 +83,329 @@ __device__ __forceinline__ T pick(const T (&a)[DG_MAX_TH], int i) {
   return r;
 }
 
+__device__ __forceinline__ double2 z2() { return make_double2(0.0, 0.0); }
+
 // rowc: per-row grid factors [8][NY+2]
 //   0 1/(DY(j+1) DYF(j))  1 1/(DY(j) DYF(j))       (GYF rows: U1, U3, TH)
 //   2 1/(DYF(j) DY(j))    3 1/(DYF(j-1) DY(j))     (GY rows: U2)
 //   4 1/DY(j)             5 1/DYF(j)               6 REM_DIV upper diagonal
 //   7 DYF(j)
-//
-// The column stage of field f for modes m0 .. m0+MT-1 of one case.  sbase:
-// the CTA's 128-byte aligned dynamic shared memory.
+
+// The field's coefficients that do not change along the column.
+struct FieldCoef {
+  double T3, T4, T5, aaU, NU, nup, ipr, ddx, ddz, sgn, gr, time;
+  int lo, hi;
+};
+
+__device__ __forceinline__ FieldCoef field_coef(const ColConst &C, const double *dscal,
+                                                int rk_step, int f) {
+  FieldCoef k;
+  const double h = dscal[1 + rk_step];
+  const double zeta = (rk_step == 2) ? -17.0 / 8.0 : (rk_step == 3) ? -5.0 / 4.0 : 0.0;
+  const double bbar = (rk_step == 2) ? 25.0 / 8.0 : (rk_step == 3) ? 9.0 / 4.0 : 1.0;
+  const double T1 = C.nu * h / 2.0;
+  k.T3 = zeta * h;
+  k.T4 = h;
+  k.T5 = bbar * h;
+  k.aaU = T1 * C.nuv;
+  k.NU = C.nu;
+  k.time = dscal[0];
+  const int n = f - 3;
+  k.nup = (f >= 3) ? C.nu / pick(C.pr, n) : C.nu;
+  k.ipr = (f >= 3) ? 1.0 / pick(C.pr, n) : 1.0;
+  k.ddx = (f >= 3) ? pick(C.drhodx, n) : 0.0;
+  k.ddz = (f >= 3) ? pick(C.drhodz, n) : 0.0;
+  k.sgn = (f == 0) ? 1.0 : -1.0;
+  k.gr = (f == 0) ? C.grav_x : C.grav_z;
+  if (f == 0 || f == 2) { k.lo = C.JS; k.hi = C.JE; }
+  else if (f == 1) { k.lo = 2; k.hi = C.NY; }
+  else { k.lo = pick(C.JSt, n); k.hi = pick(C.JEt, n); }
+  return k;
+}
+
+// The explicit terms fv (the new CF) and the CN right-hand side r of field f
+// at row j, mode mg (offset o): u, um, up = CU at j, j-1, j+1; nlv = NL;
+// old = CF_old; p0, pm = CP at j, j-1.  RC: the rowc rows in shared memory.
+__device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, int f, int j,
+                                        long o, bool mean, double KX, double KZ, double kk,
+                                        const double *RC, double2 u, double2 um, double2 up,
+                                        double2 nlv, double2 old, double2 p0, double2 pm,
+                                        double2 &fv, double2 &r) {
+  const ColConst &C = cc.C;
+  const int L = C.NY + 2, nth = C.nth;
+  const long ss = C.ss;
+  if (f == 0 || f == 2) {
+    fv = make_double2(-k.NU * kk * u.x, -k.NU * kk * u.y);
+    if (C.i_ro != 0.0) {
+      const double2 uo = cc.cu[2 - f][o];
+      fv.x += k.sgn * C.i_ro * uo.x;
+      fv.y += k.sgn * C.i_ro * uo.y;
+    }
+    for (int q = 0; q < nth; q++) {
+      const double w = C.ri[q] * k.gr;
+      if (w == 0.0) continue;
+      const double2 t = cc.cu[3 + q][o];
+      fv.x += w * t.x;
+      fv.y += w * t.y;
+    }
+    fv.x += nlv.x;
+    fv.y += nlv.y;
+    r = u;
+    r.x += k.T3 * old.x;
+    r.y += k.T3 * old.y;
+    const double K = (f == 0) ? KX : KZ;
+    r.x -= k.T4 * (-K * p0.y);
+    r.y -= k.T4 * (K * p0.x);
+    if (f == 0 && mean) {
+      if (C.f_type == 1) r.x -= k.T4 * C.px0;
+      else if (C.f_type == 2) r.x -= k.T4 * (C.px0 + C.amp_omega0 * cos(C.omega0 * k.time));
+    }
+    r.x += k.T5 * fv.x;
+    r.y += k.T5 * fv.y;
+    const double cup = k.aaU * RC[0 * L + j], cdn = k.aaU * RC[1 * L + j];
+    r.x += cup * (up.x - u.x) - cdn * (u.x - um.x);
+    r.y += cup * (up.y - u.y) - cdn * (u.y - um.y);
+  } else if (f == 1) {
+    fv = make_double2(-k.NU * kk * u.x, -k.NU * kk * u.y);
+    if (!mean) {
+      const double dyfj = RC[7 * L + j], dyfm = RC[7 * L + j - 1];
+      const double bw2 = 0.5 * RC[4 * L + j];
+      for (int q = 0; q < nth; q++) {
+        if (C.ri[q] * C.grav_y == 0.0) continue;
+        const double w = C.ri[q] * C.grav_y * bw2;
+        const double2 t = cc.cu[3 + q][o], tm = cc.cu[3 + q][o - ss];
+        fv.x += w * (t.x * dyfm + tm.x * dyfj);
+        fv.y += w * (t.y * dyfm + tm.y * dyfj);
+      }
+    }
+    fv.x += nlv.x;
+    fv.y += nlv.y;
+    r = u;
+    r.x += k.T3 * old.x;
+    r.y += k.T3 * old.y;
+    const double idy = RC[4 * L + j];
+    r.x -= k.T4 * ((p0.x - pm.x) * idy);
+    r.y -= k.T4 * ((p0.y - pm.y) * idy);
+    r.x += k.T5 * fv.x;
+    r.y += k.T5 * fv.y;
+    const double cup2 = k.aaU * RC[2 * L + j], cdn2 = k.aaU * RC[3 * L + j];
+    r.x += cup2 * (up.x - u.x) - cdn2 * (u.x - um.x);
+    r.y += cup2 * (up.y - u.y) - cdn2 * (u.y - um.y);
+  } else {
+    fv = make_double2(-k.nup * kk * u.x, -k.nup * kk * u.y);
+    if (k.ddx != 0.0 || k.ddz != 0.0) {
+      const double2 u1 = cc.cu[0][o], u3 = cc.cu[2][o];
+      fv.x = fv.x - u1.x * k.ddx - u3.x * k.ddz;
+      fv.y = fv.y - u1.y * k.ddx - u3.y * k.ddz;
+    }
+    fv.x += nlv.x;
+    fv.y += nlv.y;
+    r = u;
+    r.x += k.T3 * old.x;
+    r.y += k.T3 * old.y;
+    r.x += k.T5 * fv.x;
+    r.y += k.T5 * fv.y;
+    const double cup = k.aaU * RC[0 * L + j], cdn = k.aaU * RC[1 * L + j];
+    r.x += k.ipr * (cup * (up.x - u.x) - cdn * (u.x - um.x));
+    r.y += k.ipr * (cup * (up.y - u.y) - cdn * (u.y - um.y));
+  }
+}
+
+// Shared memory of one CTA (128-byte aligned base): the CU tile
+// [nbox * by][MT]; per (segment, mode) values SV [nseg][MT]; per segment
+// products SP [nseg]; the CN table rows TB [6][L] (a, 1/b, c, kind, BC value,
+// f = -c/b); the grid factors RC [8][L]; the mbarrier.
+size_t col_smem_l(int L, int mt, int by, int nbox, int nseg) {
+  return sizeof(double2) * ((size_t)nbox * by * mt + (size_t)nseg * mt) +
+         sizeof(double) * ((size_t)nseg + 14 * (size_t)L) + 8 + 128;
+}
+
+// The column stage of field f for modes m0 .. m0+MT-1 of one case.
 template <int MT>
 __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0, int f,
                                          long spin, unsigned extra_tx, unsigned char *sbase) {
   const ColConst &C = cc.C;
-  const int NY = C.NY, L = NY + 2, nth = C.nth;
-  const int by = cc.by, nbox = cc.nbox;
+  const int NY = C.NY, L = NY + 2;
+  const int nseg = cc.nseg;
   const long ss = C.ss;
   const int mt = (int)((ss - m0) < MT ? (ss - m0) : MT);
   const bool vel = f < 3;
   const bool old_cf = rk_step > 1;
-  const int tile = nbox * by * MT;                                 // double2 per tile
-  double2 *CUt = reinterpret_cast<double2 *>(sbase);               // CU
-  double2 *NLt = CUt + tile;                                       // NL -> R -> solution
-  double2 *CFt = NLt + tile;                                       // CF_old
-  double2 *CPt = CFt + tile;                                       // CP
-  double *TB = reinterpret_cast<double *>(CPt + tile);             // [5][L] CN tables
-  double *KXS = TB + 5 * L, *KZS = KXS + MT, *KKS = KZS + MT;      // [MT]
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(KKS + MT);
-  const int tid = threadIdx.x;
+  const int tile = cc.nbox * cc.by * MT;
+  double2 *CUt = reinterpret_cast<double2 *>(sbase);
+  double2 *SV = CUt + tile;
+  double *SP = reinterpret_cast<double *>(SV + nseg * MT);
+  double *TB = SP + nseg;
+  double *RC = TB + 6 * L;
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(RC + 8 * L);
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int m = tid % MT, s = tid / MT;
+  const int j0 = s * SEG_K;
+  const int nr = (s < nseg) ? min(SEG_K, L - j0) : 0;  // rows of this thread's segment
+  const long mg = m0 + m;
+  const bool live = m < mt;
+  const bool mean = (mg == 0);
 
-  // constant tables first: they do not depend on the preceding kernel
+  // ---- 0. tables (they do not depend on the preceding kernel)
   if (tid == 0) dg_mbar_init(bar, 1);
-  if (tid < MT) {
-    const long mg = (m0 + tid < ss) ? m0 + tid : 0;
-    const double KX = cc.kxv[mg % C.nkxp], KZ = cc.kzv[mg / C.nkxp];
-    const double k2 = KX * KX + KZ * KZ;
-    KXS[tid] = KX;
-    KZS[tid] = KZ;
-    KKS[tid] = (C.beta == 1.0) ? k2 : pow(k2, C.beta);
-  }
-  const double *tab_f = cc.tab + ((long)(rk_step - 1) * (3 + DG_MAX_TH) + f) * 5 * L;
-  for (int i = tid; i < 5 * L; i += CS_THR) TB[i] = tab_f[i];
+  const double *tb = cc.tab + ((long)(rk_step - 1) * (3 + DG_MAX_TH) + f) * 5 * L;
+  for (int i = tid; i < 5 * L; i += nthr) TB[i] = tb[i];
+  for (int j = tid; j < L; j += nthr) TB[5 * L + j] = (j < L - 1) ? -tb[2 * L + j] * tb[L + j] : 0.0;
+  for (int i = tid; i < 8 * L; i += nthr) RC[i] = cc.rowc[i];
+  const long mgc = live ? mg : 0;
+  const double KX = cc.kxv[mgc % C.nkxp], KZ = cc.kzv[mgc / C.nkxp];
+  const double k2 = KX * KX + KZ * KZ;
+  const double kk = (C.beta == 1.0) ? k2 : pow(k2, C.beta);
   __syncthreads();
+
+  // ---- 1. loads: CU by bulk tensor copy, this thread's NL, CF_old, CP rows
   dg_pdl_wait();  // NL comes from the z-forward kernel
   if (tid == 0) {
     // columns beyond ss and planes beyond L arrive as zeros (extra_tx is 0
     // except in the wait test, where the barrier can then never complete)
-    const unsigned ntiles = 2u + (old_cf ? 1u : 0u) + (vel ? 1u : 0u);
-    dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * tile) * ntiles + extra_tx);
-    for (int q = 0; q < nbox; q++) {
-      const long d = (long)q * by * MT;
-      dg_tma_load_2d(CUt + d, &cc.map_cu[f], (int)(2 * m0), q * by, bar);
-      dg_tma_load_2d(NLt + d, &cc.map_nl[f], (int)(2 * m0), q * by, bar);
-      if (old_cf) dg_tma_load_2d(CFt + d, &cc.map_cf[f], (int)(2 * m0), q * by, bar);
-      if (vel) dg_tma_load_2d(CPt + d, &cc.map_cp, (int)(2 * m0), q * by, bar);
-    }
+    dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * tile) + extra_tx);
+    for (int q = 0; q < cc.nbox; q++)
+      dg_tma_load_2d(CUt + (long)q * cc.by * MT, &cc.map_cu[f], (int)(2 * m0), q * cc.by, bar);
   }
+  const double2 *nlp = cc.nl[f];
+  const double2 *cfo = cc.cf[f];
   const bool landed = dg_mbar_wait(bar, 0, spin);
-  __syncthreads();
-  if (!landed) {
-    if (tid == 0) atomicExch(cc.err + 1, 1);
-    dg_mbar_wait(bar, 0, spin);  // give the copies in flight one more bounded wait
+  if (__syncthreads_or(!landed)) {
+    if (tid == 0) {
+      atomicExch(cc.err + 1, 1);
+      dg_mbar_wait(bar, 0, spin);  // the copies in flight get one more bounded wait
+    }
     return;
   }
 
-  // ---- 1. explicit terms, CF and the CN right-hand side (in place of NL)
-  const double h = cc.dscal[1 + rk_step];
-  const double time = cc.dscal[0];
-  const double zeta = (rk_step == 2) ? -17.0 / 8.0 : (rk_step == 3) ? -5.0 / 4.0 : 0.0;
-  const double bbar = (rk_step == 2) ? 25.0 / 8.0 : (rk_step == 3) ? 9.0 / 4.0 : 1.0;
-  const double T1 = C.nu * h / 2.0, T3 = zeta * h, T4 = h, T5 = bbar * h;
-  const double aaU = T1 * C.nuv;
-  const double NU = C.nu;
-  const double *__restrict__ rowc = cc.rowc;
-  double2 *__restrict__ cff = cc.cf[f];
-  int lo, hi;
-  if (f == 0 || f == 2) { lo = C.JS; hi = C.JE; }
-  else if (f == 1) { lo = 2; hi = NY; }
-  else { lo = pick(C.JSt, f - 3); hi = pick(C.JEt, f - 3); }
-  // the field's uniform coefficients
-  const double sgn = (f == 0) ? 1.0 : -1.0;
-  const double gr = (f == 0) ? C.grav_x : C.grav_z;
-  const int n = f - 3;
-  const double nup = (f >= 3) ? NU / pick(C.pr, n) : NU;
-  const double ipr = (f >= 3) ? 1.0 / pick(C.pr, n) : 1.0;
-  const double ddx = (f >= 3) ? pick(C.drhodx, n) : 0.0;
-  const double ddz = (f >= 3) ? pick(C.drhodz, n) : 0.0;
-  for (int i = lo * MT + tid; i < (hi + 1) * MT; i += CS_THR) {
-    const int j = i / MT, m = i - j * MT;
-    if (m >= mt) continue;
-    const long o = (long)j * ss + m0 + m;
-    const double2 u = CUt[i], um = CUt[i - MT], up = CUt[i + MT];
-    const double2 nlv = NLt[i];
-    const double2 old = old_cf ? CFt[i] : make_double2(0.0, 0.0);
-    const double kk = KKS[m];
-    double2 fv, r;
-    if (f == 0 || f == 2) {
-      fv = make_double2(-NU * kk * u.x, -NU * kk * u.y);
-      if (C.i_ro != 0.0) {
-        const double2 uo = cc.cu[2 - f][o];
-        fv.x += sgn * C.i_ro * uo.x;
-        fv.y += sgn * C.i_ro * uo.y;
+  // ---- 2. explicit terms, CF and the right-hand side row by row, and the
+  // forward recurrence g(j) = r(j) + a(j) g(j-1) over the segment from zero
+  const FieldCoef k = field_coef(C, cc.dscal, rk_step, f);
+  double2 *cff = cc.cf[f];
+  double2 g = z2();
+  double2 gl[SEG_K];
+  double pa = 1.0;
+  // CP one row below the segment (the U2 pressure gradient)
+  double2 pprev = (live && f == 1 && nr > 0 && j0 >= 1) ? cc.cp[(long)(j0 - 1) * ss + mg] : z2();
+#pragma unroll
+  for (int q = 0; q < SEG_K; q++) {
+    gl[q] = z2();
+    if (q < nr) {
+      const int j = j0 + q;
+      const long o = (long)j * ss + mg;
+      const double2 p0 = (live && vel) ? cc.cp[o] : z2();
+      const double kind = TB[3 * L + j];
+      // a BC row's value goes to the real part of the (0,0) mode only
+      double2 r = make_double2((kind == (double)ROW_BC && mean) ? TB[4 * L + j] : 0.0, 0.0);
+      if (j >= k.lo && j <= k.hi) {
+        const double2 nlv = live ? nlp[o] : z2();
+        const double2 old = (live && old_cf) ? cfo[o] : z2();
+        double2 fv, rr;
+        rhs_row(cc, k, f, j, o, mean, KX, KZ, kk, RC, CUt[j * MT + m], CUt[(j - 1) * MT + m],
+                CUt[(j + 1) * MT + m], nlv, old, p0, pprev, fv, rr);
+        if (live) cff[o] = fv;
+        if (kind == (double)ROW_RHS) r = rr;
       }
-      for (int q = 0; q < nth; q++) {
-        const double w = C.ri[q] * gr;
-        if (w == 0.0) continue;
-        const double2 t = cc.cu[3 + q][o];
-        fv.x += w * t.x;
-        fv.y += w * t.y;
-      }
-      fv.x += nlv.x;
-      fv.y += nlv.y;
-      r = u;
-      r.x += T3 * old.x;
-      r.y += T3 * old.y;
-      const double2 p0 = CPt[i];
-      const double K = (f == 0) ? KXS[m] : KZS[m];
-      r.x -= T4 * (-K * p0.y);
-      r.y -= T4 * (K * p0.x);
-      if (f == 0 && m0 + m == 0) {
-        if (C.f_type == 1) r.x -= T4 * C.px0;
-        else if (C.f_type == 2) r.x -= T4 * (C.px0 + C.amp_omega0 * cos(C.omega0 * time));
-      }
-      r.x += T5 * fv.x;
-      r.y += T5 * fv.y;
-      const double cup = aaU * rowc[0 * L + j], cdn = aaU * rowc[1 * L + j];
-      r.x += cup * (up.x - u.x) - cdn * (u.x - um.x);
-      r.y += cup * (up.y - u.y) - cdn * (u.y - um.y);
-    } else if (f == 1) {
-      fv = make_double2(-NU * kk * u.x, -NU * kk * u.y);
-      if (m0 + m != 0) {
-        const double dyfj = rowc[7 * L + j], dyfm = rowc[7 * L + j - 1];
-        const double bw2 = 0.5 * rowc[4 * L + j];
-        for (int q = 0; q < nth; q++) {
-          if (C.ri[q] * C.grav_y == 0.0) continue;
-          const double w = C.ri[q] * C.grav_y * bw2;
-          const double2 t = cc.cu[3 + q][o], tm = cc.cu[3 + q][o - ss];
-          fv.x += w * (t.x * dyfm + tm.x * dyfj);
-          fv.y += w * (t.y * dyfm + tm.y * dyfj);
-        }
-      }
-      fv.x += nlv.x;
-      fv.y += nlv.y;
-      r = u;
-      r.x += T3 * old.x;
-      r.y += T3 * old.y;
-      const double2 p0 = CPt[i], pm = CPt[i - MT];
-      const double idy = rowc[4 * L + j];
-      r.x -= T4 * ((p0.x - pm.x) * idy);
-      r.y -= T4 * ((p0.y - pm.y) * idy);
-      r.x += T5 * fv.x;
-      r.y += T5 * fv.y;
-      const double cup2 = aaU * rowc[2 * L + j], cdn2 = aaU * rowc[3 * L + j];
-      r.x += cup2 * (up.x - u.x) - cdn2 * (u.x - um.x);
-      r.y += cup2 * (up.y - u.y) - cdn2 * (u.y - um.y);
-    } else {
-      fv = make_double2(-nup * kk * u.x, -nup * kk * u.y);
-      if (ddx != 0.0 || ddz != 0.0) {
-        const double2 u1 = cc.cu[0][o], u3 = cc.cu[2][o];
-        fv.x = fv.x - u1.x * ddx - u3.x * ddz;
-        fv.y = fv.y - u1.y * ddx - u3.y * ddz;
-      }
-      fv.x += nlv.x;
-      fv.y += nlv.y;
-      r = u;
-      r.x += T3 * old.x;
-      r.y += T3 * old.y;
-      r.x += T5 * fv.x;
-      r.y += T5 * fv.y;
-      const double cup = aaU * rowc[0 * L + j], cdn = aaU * rowc[1 * L + j];
-      r.x += ipr * (cup * (up.x - u.x) - cdn * (u.x - um.x));
-      r.y += ipr * (cup * (up.y - u.y) - cdn * (u.y - um.y));
+      const double a = TB[j];
+      g.x = r.x + a * g.x;
+      g.y = r.y + a * g.y;
+      pa = a * pa;
+      gl[q] = g;
+      pprev = p0;
     }
-    cff[o] = fv;
-    NLt[i] = r;
+  }
+  if (nr > 0) {
+    SV[s * MT + m] = g;
+    if (m == 0) SP[s] = pa;
   }
   __syncthreads();
-
-  // ---- 2. CN solve, one lane per mode, rows 0..NY+1.  The operator is real,
-  // so the real and imaginary parts are two independent recurrences; one
-  // lane runs both, interleaved, which hides half of each one's latency.
-  const int wlo = (f >= 3) ? pick(C.JSt, f - 3) - 1 : 1;
+  // ---- 3. the segment ends carried down the column, one lane per mode
   if (tid < MT) {
-    const int m = tid;
-    const double *Aa = TB, *Rb = TB + L, *Cc = TB + 2 * L, *K = TB + 3 * L, *V = TB + 4 * L;
-    double2 *x = NLt + m;
-    constexpr int B = 8;  // rows per register block: loads first, then the recurrences
-    const bool mean = (m0 + m == 0);
-    double2 g = make_double2(0.0, 0.0);
-    for (int j0 = 0; j0 < L; j0 += B) {
-      double2 r[B];
-      double a[B];
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        const int j = j0 + q < L ? j0 + q : L - 1;
-        const double kind = K[j];
-        const double2 xr = x[j * MT];
-        // a BC row's value goes to the real part of the (0,0) mode only
-        r[q] = (kind == (double)ROW_RHS)
-                   ? xr
-                   : make_double2((kind == (double)ROW_BC && mean) ? V[j] : 0.0, 0.0);
-        a[q] = Aa[j];
-      }
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        if (j0 + q < L) {
-          g.x = r[q].x + a[q] * g.x;
-          g.y = r[q].y + a[q] * g.y;
-          r[q] = g;
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < B; q++)
-        if (j0 + q < L) x[(j0 + q) * MT] = r[q];
-    }
-    const double rbl = Rb[L - 1];
-    double2 xv = make_double2(g.x * rbl, g.y * rbl);
-    x[(L - 1) * MT] = xv;
-    for (int j1 = L - 2; j1 >= wlo; j1 -= B) {
-      double2 gq[B];
-      double cq[B], rq[B];
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        const int j = j1 - q >= wlo ? j1 - q : wlo;
-        gq[q] = x[j * MT];
-        cq[q] = Cc[j];
-        rq[q] = Rb[j];
-      }
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        if (j1 - q >= wlo) {
-          xv.x = (gq[q].x - cq[q] * xv.x) * rq[q];
-          xv.y = (gq[q].y - cq[q] * xv.y) * rq[q];
-          gq[q] = xv;
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < B; q++)
-        if (j1 - q >= wlo) x[(j1 - q) * MT] = gq[q];
+    double2 G = z2();
+    for (int t = 0; t < nseg; t++) {
+      const double2 e = SV[t * MT + tid];
+      const double p = SP[t];
+      SV[t * MT + tid] = G;
+      G = make_double2(e.x + p * G.x, e.y + p * G.y);
     }
   }
   __syncthreads();
-
-  // ---- 3. the post-CN field goes to the field's rhs array (rows >= wlo)
-  double2 *__restrict__ dst = cc.out[f];
-  for (int i = wlo * MT + tid; i < L * MT; i += CS_THR) {
-    const int j = i / MT, m = i - j * MT;
-    if (m < mt) dst[(long)j * ss + m0 + m] = NLt[i];
+  // ---- 4. g = local + product x carry; e = g / b; the backward recurrence
+  // x(j) = e(j) + f(j) x(j+1) over the segment (rows >= wlo) from zero
+  const int wlo = (f >= 3) ? pick(C.JSt, f - 3) - 1 : 1;
+  const int qb = wlo > j0 ? wlo - j0 : 0;  // first row of the segment to solve
+  double2 xv[SEG_K];
+  double2 xl = z2();
+  double ps = 1.0;
+  {
+    const double2 c = (nr > 0) ? SV[s * MT + m] : z2();
+    double pi = 1.0;
+    double2 ev[SEG_K];
+#pragma unroll
+    for (int q = 0; q < SEG_K; q++) {
+      ev[q] = z2();
+      if (q < nr) {
+        const int j = j0 + q;
+        pi = TB[j] * pi;
+        const double2 gv = make_double2(gl[q].x + pi * c.x, gl[q].y + pi * c.y);
+        const double rb = TB[L + j];
+        ev[q] = make_double2(gv.x * rb, gv.y * rb);
+      }
+    }
+#pragma unroll
+    for (int q = SEG_K - 1; q >= 0; q--) {
+      xv[q] = z2();
+      if (q < nr && q >= qb) {
+        const double fj = TB[5 * L + j0 + q];
+        xl = make_double2(ev[q].x + fj * xl.x, ev[q].y + fj * xl.y);
+        ps = fj * ps;
+        xv[q] = xl;
+      }
+    }
   }
-}
-
-// dynamic shared memory of one CTA
-size_t col_smem_l(int L, int mt, int by, int nbox) {
-  return sizeof(double2) * 4 * (size_t)nbox * by * mt + sizeof(double) * (5 * (size_t)L + 3 * mt) +
-         8 + 128;
+  // each thread overwrites only its own SV entry, read above by itself;
+  // SP was last read in step 3, before the barrier
+  const bool solves = nr > 0 && qb < nr;
+  if (solves) {
+    SV[s * MT + m] = xl;
+    if (m == 0) SP[s] = ps;
+  }
+  __syncthreads();
+  // ---- 5. the segment starts carried up the column, one lane per mode
+  const int sw = wlo / SEG_K;  // lowest segment with rows to solve
+  if (tid < MT) {
+    double2 X = z2();
+    for (int t = nseg - 1; t >= sw; t--) {
+      const double2 e = SV[t * MT + tid];
+      const double p = SP[t];
+      SV[t * MT + tid] = X;
+      X = make_double2(e.x + p * X.x, e.y + p * X.y);
+    }
+  }
+  __syncthreads();
+  // ---- 6. x = local + product x carry: the post-CN field, rows >= wlo
+  if (solves && live) {
+    const double2 c = SV[s * MT + m];
+    double2 *dst = cc.out[f];
+    double p2 = 1.0;
+#pragma unroll
+    for (int q = SEG_K - 1; q >= 0; q--) {
+      if (q < nr && q >= qb) {
+        const int j = j0 + q;
+        p2 = TB[5 * L + j] * p2;
+        dst[(long)j * ss + mg] = make_double2(xv[q].x + p2 * c.x, xv[q].y + p2 * c.y);
+      }
+    }
+  }
 }
 
 // The column kernel: CTA b takes work[b] = (case, mode tile, field) from
 // the case table (every case at substep rk_step with MT modes per CTA).
 template <int MT>
-__global__ void __launch_bounds__(CS_THR) k_col_cn(const ColCase *__restrict__ cases,
-                                                  const int4 *__restrict__ work, int rk_step,
-                                                  long spin, unsigned extra_tx) {
+__global__ void __launch_bounds__(COL_MAX_THR) k_col_cn(const ColCase *__restrict__ cases,
+                                                       const int4 *__restrict__ work,
+                                                       int rk_step, long spin,
+                                                       unsigned extra_tx) {
   extern __shared__ __align__(128) unsigned char cs_raw[];
   unsigned char *sbase = cs_raw + ((128u - (dg_smem_addr(cs_raw) & 127u)) & 127u);
   const int4 w = work[blockIdx.x];
@@ -388,56 +463,74 @@ int dg_col_init(dg_handle *h) {
   return DG_OK;
 }
 
-static void col_geometry(const dg_handle *h, int *by, int *nbox) {
+static void col_geometry(const dg_handle *h, int *by, int *nbox, int *nseg) {
   const int L = h->NY + 2;
   // boxes of at most 256 planes; a multiple of 8 planes keeps every box's
   // shared-memory destination 128-byte aligned for any modes per CTA
   *nbox = dg_cdiv(L, 256);
   *by = (dg_cdiv(L, *nbox) + 7) / 8 * 8;
+  *nseg = dg_cdiv(L, SEG_K);
 }
 
 size_t dg_col_smem(const dg_handle *h, int mt) {
-  int by, nbox;
-  col_geometry(h, &by, &nbox);
-  return col_smem_l(h->NY + 2, mt, by, nbox);
+  int by, nbox, nseg;
+  col_geometry(h, &by, &nbox, &nseg);
+  return col_smem_l(h->NY + 2, mt, by, nbox, nseg);
+}
+
+// threads of one CTA for handle h at mt modes: one per (mode, segment)
+static int col_threads(const dg_handle *h, int mt) {
+  int by, nbox, nseg;
+  col_geometry(h, &by, &nbox, &nseg);
+  return (mt * nseg + 31) / 32 * 32;
 }
 
 // The case description of handle h for `mt` modes per CTA (builds the
-// tensor maps of its CU, rhs and CF arrays and CP for that tile width).
+// tensor maps of its CU arrays for that tile width).
 static int fill_case(dg_handle *h, int mt, ColCase *cc) {
   const int L = h->NY + 2;
-  int by = 0, nbox = 0;
-  col_geometry(h, &by, &nbox);
+  int by = 0, nbox = 0, nseg = 0;
+  col_geometry(h, &by, &nbox, &nseg);
   memset(cc, 0, sizeof(*cc));
-  for (int f = 0; f < h->nf; f++) {
+  for (int f = 0; f < h->nf; f++)
     DG_TRY(dg_tmap_planes(h->cu[f], h->ss, L, mt, by, &cc->map_cu[f]));
-    DG_TRY(dg_tmap_planes(h->rhs[f], h->ss, L, mt, by, &cc->map_nl[f]));
-    DG_TRY(dg_tmap_planes(h->cf[f], h->ss, L, mt, by, &cc->map_cf[f]));
-  }
-  DG_TRY(dg_tmap_planes(h->cp, h->ss, L, mt, by, &cc->map_cp));
   cc->C = make_col_const(h);
   cc->dscal = h->dscal;
   cc->tab = h->cn_tab;
   cc->kxv = h->kx;
   cc->kzv = h->kz;
   cc->rowc = h->rowc;
+  cc->cp = h->cp;
   for (int f = 0; f < h->nf; f++) {
     cc->cu[f] = h->cu[f];
+    cc->nl[f] = h->rhs[f];
     cc->cf[f] = h->cf[f];
     cc->out[f] = (f < 3 || dg_col_th_to_rhs(h, f - 3)) ? h->rhs[f] : h->cu[f];
   }
   cc->err = h->dflag;
   cc->by = by;
   cc->nbox = nbox;
+  cc->nseg = nseg;
   return DG_OK;
 }
 
-// modes per CTA for handle h: the tuned value, halved until the tiles fit
+// modes per CTA for handle h: the tuned value, halved until the CTA fits
+// (shared memory, and one thread per mode and segment)
 static int col_mt(const dg_handle *h, int want) {
   int mt = want;
-  while (mt > 2 && dg_col_smem(h, mt) > 220 * 1024) mt /= 2;
+  while (mt > 2 && (dg_col_smem(h, mt) > 220 * 1024 || col_threads(h, mt) > COL_MAX_THR)) mt /= 2;
   return mt;
 }
+
+static int col_fits(const dg_handle *h, int mt) {
+  if (dg_col_smem(h, mt) > 220 * 1024 || col_threads(h, mt) > COL_MAX_THR) {
+    dg_set_error("column kernel: NY too large for two modes per CTA (NY + 2 <= 1024)");
+    return DG_ERR_DIMS;
+  }
+  return DG_OK;
+}
+
+int dg_col_mt_eff(const dg_handle *h) { return col_mt(h, h->cn_mt); }
 
 // the work list of one case: (case c, tile, field, 0) per CTA
 static void case_work(const dg_handle *h, int c, int mt, std::vector<int4> &work) {
@@ -478,13 +571,13 @@ static int col_tables(dg_handle *h, int mt) {
   return DG_OK;
 }
 
-static int launch_col(cudaStream_t st, int pdl, int mt, size_t smem, const void *dev_cases,
-                      const int4 *dev_work, int nwork, int rk_step, long spin,
-                      unsigned extra_tx) {
+static int launch_col(cudaStream_t st, int pdl, int mt, int thr, size_t smem,
+                      const void *dev_cases, const int4 *dev_work, int nwork, int rk_step,
+                      long spin, unsigned extra_tx) {
 #define CS_CASE(MTV)                                                                            \
   if (mt == MTV) {                                                                              \
     dg_big_smem((const void *)k_col_cn<MTV>);                                                   \
-    DG_CUDA(dg_launch(pdl, k_col_cn<MTV>, dim3(nwork), dim3(CS_THR), smem, st,                  \
+    DG_CUDA(dg_launch(pdl, k_col_cn<MTV>, dim3(nwork), dim3(thr), smem, st,                     \
                       (const ColCase *)dev_cases, dev_work, rk_step, spin, extra_tx));          \
   }
   CS_CASE(2) CS_CASE(4) CS_CASE(8) CS_CASE(16)
@@ -503,19 +596,15 @@ int dg_col_step_dev(dg_handle *h, int rk_step, bool rd) {
     h->tables_pending = false;
   }
   const int mt = col_mt(h, h->cn_mt);
-  const size_t sm = dg_col_smem(h, mt);
-  if (sm > 220 * 1024) {
-    dg_set_error("column kernel: the y-columns of two modes do not fit in shared memory");
-    return DG_ERR_DIMS;
-  }
+  DG_TRY(col_fits(h, mt));
   DG_TRY(col_tables(h, mt));
   // the wait test (DG_TUNE_WAIT_TEST) applies to this one launch
   const long spin = h->wait_test > 0 ? (long)h->wait_test : DG_ASYNC_SPIN;
   const unsigned extra_tx = h->wait_test > 0 ? 16u : 0u;
   h->wait_test = 0;
   dg_kt_begin(h, "k_col_cn", h->st);
-  DG_TRY(launch_col(h->st, h->pdl, mt, sm, h->col_dcase, h->col_dwork, h->col_dnwork, rk_step,
-                    spin, extra_tx));
+  DG_TRY(launch_col(h->st, h->pdl, mt, col_threads(h, mt), dg_col_smem(h, mt), h->col_dcase,
+                    h->col_dwork, h->col_dnwork, rk_step, spin, extra_tx));
   if (rd) DG_TRY(dg_rem_div_dev(h, 1, rk_step, true));
   return DG_OK;
 }
@@ -524,20 +613,23 @@ int dg_col_step_dev(dg_handle *h, int rk_step, bool rd) {
 // The column stage of several cases at the same substep in one launch (the
 // ensemble server's groups).  dg_col_batch_build fills, for the handles, the
 // host images of the case table and the work list (one (case, tile, field)
-// entry per CTA) with one MT for all, and returns the launch's shared
-// memory; the caller copies them to device memory it owns and launches with
-// dg_col_batch_launch.  Each case's REM_DIV follows on its own stream.
-// Results do not depend on the batch: each mode's arithmetic is the
-// single-case launch's, with the same kernel.
+// entry per CTA) with one MT for all, and returns the launch's threads per
+// CTA and shared memory (the largest any case needs; a case's CTAs leave
+// the threads beyond its own segments idle); the caller copies the images
+// to device memory it owns and launches with dg_col_batch_launch.  Each
+// case's REM_DIV follows on its own stream.  Results do not depend on the
+// batch: each mode's arithmetic is the single-case launch's, with the same
+// kernel.
 int dg_col_batch_build(dg_handle *const *hs, int n, int want_mt, std::vector<unsigned char> &cases,
-                       std::vector<int4> &work, int *mt_out, size_t *smem_out) {
+                       std::vector<int4> &work, int *mt_out, int *thr_out, size_t *smem_out) {
   int mt = want_mt;
   for (int c = 0; c < n; c++) mt = std::min(mt, col_mt(hs[c], want_mt));
   size_t sm = 0;
-  for (int c = 0; c < n; c++) sm = std::max(sm, dg_col_smem(hs[c], mt));
-  if (sm > 220 * 1024) {
-    dg_set_error("column kernel: the y-columns of two modes do not fit in shared memory");
-    return DG_ERR_DIMS;
+  int thr = 0;
+  for (int c = 0; c < n; c++) {
+    DG_TRY(col_fits(hs[c], mt));
+    sm = std::max(sm, dg_col_smem(hs[c], mt));
+    thr = std::max(thr, col_threads(hs[c], mt));
   }
   cases.assign(sizeof(ColCase) * n, 0);
   work.clear();
@@ -548,11 +640,13 @@ int dg_col_batch_build(dg_handle *const *hs, int n, int want_mt, std::vector<uns
     case_work(hs[c], c, mt, work);
   }
   *mt_out = mt;
+  *thr_out = thr;
   *smem_out = sm;
   return DG_OK;
 }
 
-int dg_col_batch_launch(cudaStream_t st, int mt, size_t smem, const void *dev_cases,
+int dg_col_batch_launch(cudaStream_t st, int mt, int thr, size_t smem, const void *dev_cases,
                         const int4 *dev_work, int nwork, int rk_step) {
-  return launch_col(st, 0, mt, smem, dev_cases, dev_work, nwork, rk_step, DG_ASYNC_SPIN, 0u);
+  return launch_col(st, 0, mt, thr, smem, dev_cases, dev_work, nwork, rk_step, DG_ASYNC_SPIN,
+                    0u);
 }

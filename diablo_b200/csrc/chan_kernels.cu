@@ -2326,10 +2326,18 @@ int dg_stats_dev(dg_handle *h, dg_stats *s) {
   double *ume = (double *)calloc(NY + 2, sizeof(double));
   double *tmp = (double *)calloc(4 * (NY + 2), sizeof(double));
   double *urms = tmp, *vrms = tmp + (NY + 2), *wrms = tmp + 2 * (NY + 2), *ke = tmp + 3 * (NY + 2);
-  double2 c0;
-  for (int j = 0; j <= NY + 1; j++) {
-    cudaMemcpy(&c0, h->cu[0] + (long)j * h->ss, sizeof(double2), cudaMemcpyDeviceToHost);
-    ume[j] = c0.x;
+  // the mean U1 of every plane: one strided copy on the handle's stream
+  double2 *c0 = (double2 *)malloc(sizeof(double2) * (NY + 2));
+  cudaError_t ce = cudaMemcpy2DAsync(c0, sizeof(double2), h->cu[0], sizeof(double2) * h->ss,
+                                     sizeof(double2), NY + 2, cudaMemcpyDeviceToHost, h->st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->st);
+  for (int j = 0; j <= NY + 1; j++) ume[j] = (ce == cudaSuccess) ? c0[j].x : 0.0;
+  free(c0);
+  if (ce != cudaSuccess) {
+    free(ume);
+    free(tmp);
+    free(hs);
+    DG_CUDA(ce);
   }
   s->ubulk = integ(ume);
   for (int j = 1; j <= NY; j++) {

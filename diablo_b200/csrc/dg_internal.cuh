@@ -240,9 +240,10 @@ int dg_col_init(dg_handle *h);
 int dg_col_step_dev(dg_handle *h, int rk_step, bool rd);
 size_t dg_col_smem(const dg_handle *h, int mt);
 bool dg_col_th_to_rhs(const dg_handle *h, int n);
+int dg_col_mt_eff(const dg_handle *h);  // modes per CTA the column kernel runs h with
 int dg_col_batch_build(dg_handle *const *hs, int n, int want_mt, std::vector<unsigned char> &cases,
-                       std::vector<int4> &work, int *mt_out, size_t *smem_out);
-int dg_col_batch_launch(cudaStream_t st, int mt, size_t smem, const void *dev_cases,
+                       std::vector<int4> &work, int *mt_out, int *thr_out, size_t *smem_out);
+int dg_col_batch_launch(cudaStream_t st, int mt, int thr, size_t smem, const void *dev_cases,
                         const int4 *dev_work, int nwork, int rk_step);
 
 #define DG_CASE_N(N) \

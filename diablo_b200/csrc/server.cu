@@ -94,9 +94,10 @@ struct Group {
   cudaEvent_t ev_fork = nullptr;
   std::vector<cudaEvent_t> ev_m;   // one per member: joins into gs
   cudaEvent_t ev_col = nullptr;    // column launch done: members fork from it
+  int cmt = 0;                     // the members' modes per column CTA (all the same)
   void *d_cases = nullptr;         // the column kernel's case table
   int4 *d_work = nullptr;          // and its work list
-  int nwork = 0, mt = 0;
+  int nwork = 0, mt = 0, thr = 0;
   size_t smem = 0;
   cudaGraphExec_t exec = nullptr;
   long long gkernels = 0;
@@ -446,17 +447,23 @@ struct GroupedLoop {
       solo.push_back(a);
       return;
     }
+    // a group's members share one column launch, so they share its modes per
+    // CTA: the width each one runs alone (same kernel instance, same results)
+    const int cmt = dg_col_mt_eff(a->h);
     Group *best = nullptr;
     double bd = 1e30;
     for (auto &g : groups) {
-      if ((int)g->m.size() >= s->group_cases) continue;
+      if ((int)g->m.size() >= s->group_cases || g->cmt != cmt) continue;
       const double d = fabs(log(pts(a) / g->points));
       if (d < log(4.0) && d < bd) {
         bd = d;
         best = g.get();
       }
     }
-    if (!best) best = new_group();
+    if (!best) {
+      best = new_group();
+      best->cmt = cmt;
+    }
     best->m.push_back(a);
     double sum = 0;
     for (Active *x : best->m) sum += pts(x);
@@ -497,7 +504,7 @@ struct GroupedLoop {
         DG_CUDA(cudaEventRecord(g.ev_m[c], h->st));
         DG_CUDA(cudaStreamWaitEvent(g.gs, g.ev_m[c], 0));
       }
-      DG_TRY(dg_col_batch_launch(g.gs, g.mt, g.smem, g.d_cases, g.d_work, g.nwork, rk));
+      DG_TRY(dg_col_batch_launch(g.gs, g.mt, g.thr, g.smem, g.d_cases, g.d_work, g.nwork, rk));
       DG_CUDA(cudaEventRecord(g.ev_col, g.gs));
       for (Active *a : g.m) {
         dg_handle *h = a->h;
@@ -531,18 +538,21 @@ struct GroupedLoop {
       }
       DG_CUDA(cudaStreamSynchronize(a->h->st));
     }
-    int want = 16;
-    for (dg_handle *h : hs) want = std::min(want, h->cn_mt);
+    const int want = g.cmt;  // every member's own width (place() groups by it)
     {
       std::vector<unsigned char> tab;
       std::vector<int4> work;
-      DG_TRY(dg_col_batch_build(hs.data(), (int)hs.size(), want, tab, work, &g.mt, &g.smem));
+      DG_TRY(dg_col_batch_build(hs.data(), (int)hs.size(), want, tab, work, &g.mt, &g.thr,
+                                &g.smem));
       DG_CUDA(cudaMalloc(&g.d_cases, tab.size()));
-      DG_CUDA(cudaMemcpy(g.d_cases, tab.data(), tab.size(), cudaMemcpyHostToDevice));
+      // on the group's stream (non-blocking: a legacy-stream copy would not be
+      // ordered before the graph launches), finished before tab goes away
+      DG_CUDA(cudaMemcpyAsync(g.d_cases, tab.data(), tab.size(), cudaMemcpyHostToDevice, g.gs));
       g.nwork = (int)work.size();
       DG_CUDA(cudaMalloc((void **)&g.d_work, sizeof(int4) * work.size()));
-      DG_CUDA(cudaMemcpy(g.d_work, work.data(), sizeof(int4) * work.size(),
-                         cudaMemcpyHostToDevice));
+      DG_CUDA(cudaMemcpyAsync(g.d_work, work.data(), sizeof(int4) * work.size(),
+                              cudaMemcpyHostToDevice, g.gs));
+      DG_CUDA(cudaStreamSynchronize(g.gs));
     }
     DG_CUDA(cudaStreamBeginCapture(g.gs, cudaStreamCaptureModeThreadLocal));
     for (dg_handle *h : hs) h->capturing = true;

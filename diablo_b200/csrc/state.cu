@@ -378,14 +378,16 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
     DG_TRY(dalloc(h, &h->cu[f], ns));
     DG_TRY(dalloc(h, &h->cf[f], ns));
     DG_TRY(dalloc(h, &h->rhs[f], ns));
-    DG_CUDA(cudaMemset(h->cu[f], 0, ns * sizeof(double2)));
-    DG_CUDA(cudaMemset(h->cf[f], 0, ns * sizeof(double2)));
-    DG_CUDA(cudaMemset(h->rhs[f], 0, ns * sizeof(double2)));
+    // on the handle's stream: a legacy-stream memset is not ordered with the
+    // handle's non-blocking stream, and could land after the first state upload
+    DG_CUDA(cudaMemsetAsync(h->cu[f], 0, ns * sizeof(double2), h->st));
+    DG_CUDA(cudaMemsetAsync(h->cf[f], 0, ns * sizeof(double2), h->st));
+    DG_CUDA(cudaMemsetAsync(h->rhs[f], 0, ns * sizeof(double2), h->st));
   }
   DG_TRY(dalloc(h, &h->cp, ns));
   DG_TRY(dalloc(h, &h->cr1, ns));
-  DG_CUDA(cudaMemset(h->cp, 0, ns * sizeof(double2)));
-  DG_CUDA(cudaMemset(h->cr1, 0, ns * sizeof(double2)));
+  DG_CUDA(cudaMemsetAsync(h->cp, 0, ns * sizeof(double2), h->st));
+  DG_CUDA(cudaMemsetAsync(h->cr1, 0, ns * sizeof(double2), h->st));
 
   if (!h->periodic) {
     DG_TRY(dalloc(h, &h->gphi, ns));

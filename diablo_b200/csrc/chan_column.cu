@@ -26,12 +26,13 @@
 // of the same operations.  Segment boundaries depend only on NY, so a mode's
 // arithmetic does not depend on the tile width.
 //
-// CU arrives in shared memory by one bulk tensor copy per box (TMA, no
-// multicast) completed on an mbarrier with a bounded wait; each thread's NL,
-// CF_old and CP rows are plain loads issued before that wait.  The right-
-// hand side is formed in registers, the post-CN field goes to the field's
-// rhs array (which held the NL term the kernel consumes: every element is
-// read and written by the same thread).  CU is read-only in this kernel, so
+// The field's input tiles -- CU, the NL term the z-forward kernel left in
+// the field's rhs array, CF_old (substeps 2, 3) and CP (velocity fields) --
+// arrive in shared memory by bulk tensor copies (TMA, no multicast), all
+// issued at once by one thread and completed on one mbarrier with a bounded
+// wait; the table rows are staged meanwhile.  The right-hand side replaces
+// NL in shared memory, the recurrences run there, and the post-CN field goes
+// to the field's rhs array.  CU is read-only in this kernel, so
 // a field's right-hand side may read another field (rotation, buoyancy,
 // GRAV, DRHODX/Z) without a race.  REM_DIV then reads the post-CN velocity
 // from the rhs arrays and writes CU.  A scalar that no velocity right-hand
@@ -64,13 +65,12 @@ struct ColConst {
 // Everything the column stage of one case needs, in device memory (tensor
 // maps first: 64-byte aligned).  Maps are 2-D over [plane][2 ss doubles].
 struct ColCase {
-  CUtensorMap map_cu[3 + DG_MAX_TH];
+  CUtensorMap map_cu[3 + DG_MAX_TH], map_nl[3 + DG_MAX_TH], map_cf[3 + DG_MAX_TH];
+  CUtensorMap map_cp;
   ColConst C;
   const double *dscal, *tab, *kxv, *kzv, *rowc;
-  const double2 *cp;
   const double2 *cu[3 + DG_MAX_TH];
-  const double2 *nl[3 + DG_MAX_TH];  // the z forward's NL terms (rhs arrays)
-  double2 *cf[3 + DG_MAX_TH], *out[3 + DG_MAX_TH];
+  double2 *cf[3 + DG_MAX_TH], *out[3 + DG_MAX_TH];  // out: the rhs arrays
   int *err;
   int by, nbox, nseg;
 };
@@ -125,7 +125,8 @@ __device__ __forceinline__ FieldCoef field_coef(const ColConst &C, const double 
 
 // The explicit terms fv (the new CF) and the CN right-hand side r of field f
 // at row j, mode mg (offset o): u, um, up = CU at j, j-1, j+1; nlv = NL;
-// old = CF_old; p0, pm = CP at j, j-1.  RC: the rowc rows in shared memory.
+// old = CF_old; p0, pm = CP at j, j-1.  RC: the field's rowc rows in shared
+// memory, [4][L]: rows 0, 1 (U1, U3, TH) or 2, 3, 4, 7 (U2).
 __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, int f, int j,
                                         long o, bool mean, double KX, double KZ, double kk,
                                         const double *RC, double2 u, double2 um, double2 up,
@@ -168,8 +169,8 @@ __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, i
   } else if (f == 1) {
     fv = make_double2(-k.NU * kk * u.x, -k.NU * kk * u.y);
     if (!mean) {
-      const double dyfj = RC[7 * L + j], dyfm = RC[7 * L + j - 1];
-      const double bw2 = 0.5 * RC[4 * L + j];
+      const double dyfj = RC[3 * L + j], dyfm = RC[3 * L + j - 1];
+      const double bw2 = 0.5 * RC[2 * L + j];
       for (int q = 0; q < nth; q++) {
         if (C.ri[q] * C.grav_y == 0.0) continue;
         const double w = C.ri[q] * C.grav_y * bw2;
@@ -183,12 +184,12 @@ __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, i
     r = u;
     r.x += k.T3 * old.x;
     r.y += k.T3 * old.y;
-    const double idy = RC[4 * L + j];
+    const double idy = RC[2 * L + j];
     r.x -= k.T4 * ((p0.x - pm.x) * idy);
     r.y -= k.T4 * ((p0.y - pm.y) * idy);
     r.x += k.T5 * fv.x;
     r.y += k.T5 * fv.y;
-    const double cup2 = k.aaU * RC[2 * L + j], cdn2 = k.aaU * RC[3 * L + j];
+    const double cup2 = k.aaU * RC[0 * L + j], cdn2 = k.aaU * RC[1 * L + j];
     r.x += cup2 * (up.x - u.x) - cdn2 * (u.x - um.x);
     r.y += cup2 * (up.y - u.y) - cdn2 * (u.y - um.y);
   } else {
@@ -211,13 +212,14 @@ __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, i
   }
 }
 
-// Shared memory of one CTA (128-byte aligned base): the CU tile
-// [nbox * by][MT]; per (segment, mode) values SV [nseg][MT]; per segment
-// products SP [nseg]; the CN table rows TB [6][L] (a, 1/b, c, kind, BC value,
-// f = -c/b); the grid factors RC [8][L]; the mbarrier.
+// Shared memory of one CTA (128-byte aligned base): four tiles [nbox * by][MT]
+// -- CU, NL (which then holds g, e and x of the recurrences), CF_old, CP --;
+// per (segment, mode) values SV [nseg][MT]; per segment products SP [nseg];
+// the CN table rows TB [5][L] (a, 1/b, f = -c/b, kind, BC value); the
+// field's grid factors RC [4][L]; the mbarrier.
 size_t col_smem_l(int L, int mt, int by, int nbox, int nseg) {
-  return sizeof(double2) * ((size_t)nbox * by * mt + (size_t)nseg * mt) +
-         sizeof(double) * ((size_t)nseg + 14 * (size_t)L) + 8 + 128;
+  return sizeof(double2) * (4 * (size_t)nbox * by * mt + (size_t)nseg * mt) +
+         sizeof(double) * ((size_t)nseg + 9 * (size_t)L) + 8 + 128;
 }
 
 // The column stage of field f for modes m0 .. m0+MT-1 of one case.
@@ -233,11 +235,14 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   const bool old_cf = rk_step > 1;
   const int tile = cc.nbox * cc.by * MT;
   double2 *CUt = reinterpret_cast<double2 *>(sbase);
-  double2 *SV = CUt + tile;
+  double2 *NLt = CUt + tile;
+  double2 *CFt = NLt + tile;
+  double2 *CPt = CFt + tile;
+  double2 *SV = CPt + tile;
   double *SP = reinterpret_cast<double *>(SV + nseg * MT);
   double *TB = SP + nseg;
-  double *RC = TB + 6 * L;
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(RC + 8 * L);
+  double *RC = TB + 5 * L;
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(RC + 4 * L);
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int m = tid % MT, s = tid / MT;
   const int j0 = s * SEG_K;
@@ -246,29 +251,61 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   const bool live = m < mt;
   const bool mean = (mg == 0);
 
-  // ---- 0. tables (they do not depend on the preceding kernel)
+  // ---- 0. tables (they do not depend on the preceding kernel), loads
+  // issued in batches before their stores so their latencies overlap
   if (tid == 0) dg_mbar_init(bar, 1);
-  const double *tb = cc.tab + ((long)(rk_step - 1) * (3 + DG_MAX_TH) + f) * 5 * L;
-  for (int i = tid; i < 5 * L; i += nthr) TB[i] = tb[i];
-  for (int j = tid; j < L; j += nthr) TB[5 * L + j] = (j < L - 1) ? -tb[2 * L + j] * tb[L + j] : 0.0;
-  for (int i = tid; i < 8 * L; i += nthr) RC[i] = cc.rowc[i];
+  {
+    const double *tb = cc.tab + ((long)(rk_step - 1) * (3 + DG_MAX_TH) + f) * 5 * L;
+    // the field's rowc rows: 0, 1 (GYF fields) or 2, 3, 4, 7 (U2)
+    const int r0 = (f == 1) ? 2 : 0, r1 = (f == 1) ? 3 : 1, r2 = (f == 1) ? 4 : 0,
+              r3 = (f == 1) ? 7 : 1;
+    constexpr int SU = 8;
+    for (int base = 0; base < 9 * L; base += SU * nthr) {
+      double v[SU];
+#pragma unroll
+      for (int u = 0; u < SU; u++) {
+        const int i = base + u * nthr + tid;
+        v[u] = 0.0;
+        if (i < 5 * L) {
+          // table rows a, 1/b, c, kind, BC value in that order
+          v[u] = tb[i];
+        } else if (i < 9 * L) {
+          const int r = (i - 5 * L) / L, j = (i - 5 * L) - r * L;
+          const int rr = r == 0 ? r0 : r == 1 ? r1 : r == 2 ? r2 : r3;
+          v[u] = cc.rowc[rr * L + j];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < SU; u++) {
+        const int i = base + u * nthr + tid;
+        if (i < 9 * L) TB[i] = v[u];  // RC follows TB contiguously
+      }
+    }
+  }
   const long mgc = live ? mg : 0;
   const double KX = cc.kxv[mgc % C.nkxp], KZ = cc.kzv[mgc / C.nkxp];
   const double k2 = KX * KX + KZ * KZ;
   const double kk = (C.beta == 1.0) ? k2 : pow(k2, C.beta);
   __syncthreads();
+  // row 2 of TB becomes f = -c / b (the backward recurrence's coefficient)
+  for (int j = tid; j < L; j += nthr) TB[2 * L + j] = (j < L - 1) ? -TB[2 * L + j] * TB[L + j] : 0.0;
 
-  // ---- 1. loads: CU by bulk tensor copy, this thread's NL, CF_old, CP rows
+  // ---- 1. the four tiles by bulk tensor copies, all in flight at once
   dg_pdl_wait();  // NL comes from the z-forward kernel
   if (tid == 0) {
     // columns beyond ss and planes beyond L arrive as zeros (extra_tx is 0
     // except in the wait test, where the barrier can then never complete)
-    dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * tile) + extra_tx);
-    for (int q = 0; q < cc.nbox; q++)
-      dg_tma_load_2d(CUt + (long)q * cc.by * MT, &cc.map_cu[f], (int)(2 * m0), q * cc.by, bar);
+    const unsigned ntiles = 2u + (old_cf ? 1u : 0u) + (vel ? 1u : 0u);
+    dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * tile) * ntiles + extra_tx);
+    for (int q = 0; q < cc.nbox; q++) {
+      const long d = (long)q * cc.by * MT;
+      const int x = (int)(2 * m0), y = q * cc.by;
+      dg_tma_load_2d(CUt + d, &cc.map_cu[f], x, y, bar);
+      dg_tma_load_2d(NLt + d, &cc.map_nl[f], x, y, bar);
+      if (old_cf) dg_tma_load_2d(CFt + d, &cc.map_cf[f], x, y, bar);
+      if (vel) dg_tma_load_2d(CPt + d, &cc.map_cp, x, y, bar);
+    }
   }
-  const double2 *nlp = cc.nl[f];
-  const double2 *cfo = cc.cf[f];
   const bool landed = dg_mbar_wait(bar, 0, spin);
   if (__syncthreads_or(!landed)) {
     if (tid == 0) {
@@ -279,30 +316,25 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   }
 
   // ---- 2. explicit terms, CF and the right-hand side row by row, and the
-  // forward recurrence g(j) = r(j) + a(j) g(j-1) over the segment from zero
+  // forward recurrence g(j) = r(j) + a(j) g(j-1) over the segment from zero;
+  // g replaces NL (each (row, mode) element belongs to one thread)
   const FieldCoef k = field_coef(C, cc.dscal, rk_step, f);
   double2 *cff = cc.cf[f];
   double2 g = z2();
-  double2 gl[SEG_K];
   double pa = 1.0;
-  // CP one row below the segment (the U2 pressure gradient)
-  double2 pprev = (live && f == 1 && nr > 0 && j0 >= 1) ? cc.cp[(long)(j0 - 1) * ss + mg] : z2();
 #pragma unroll
   for (int q = 0; q < SEG_K; q++) {
-    gl[q] = z2();
     if (q < nr) {
       const int j = j0 + q;
-      const long o = (long)j * ss + mg;
-      const double2 p0 = (live && vel) ? cc.cp[o] : z2();
+      const int i = j * MT + m;
       const double kind = TB[3 * L + j];
       // a BC row's value goes to the real part of the (0,0) mode only
       double2 r = make_double2((kind == (double)ROW_BC && mean) ? TB[4 * L + j] : 0.0, 0.0);
       if (j >= k.lo && j <= k.hi) {
-        const double2 nlv = live ? nlp[o] : z2();
-        const double2 old = (live && old_cf) ? cfo[o] : z2();
+        const long o = (long)j * ss + mg;
         double2 fv, rr;
-        rhs_row(cc, k, f, j, o, mean, KX, KZ, kk, RC, CUt[j * MT + m], CUt[(j - 1) * MT + m],
-                CUt[(j + 1) * MT + m], nlv, old, p0, pprev, fv, rr);
+        rhs_row(cc, k, f, j, o, mean, KX, KZ, kk, RC, CUt[i], CUt[i - MT], CUt[i + MT], NLt[i],
+                old_cf ? CFt[i] : z2(), CPt[i], CPt[i - MT], fv, rr);
         if (live) cff[o] = fv;
         if (kind == (double)ROW_RHS) r = rr;
       }
@@ -310,8 +342,7 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
       g.x = r.x + a * g.x;
       g.y = r.y + a * g.y;
       pa = a * pa;
-      gl[q] = g;
-      pprev = p0;
+      NLt[i] = g;
     }
   }
   if (nr > 0) {
@@ -330,45 +361,43 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
     }
   }
   __syncthreads();
-  // ---- 4. g = local + product x carry; e = g / b; the backward recurrence
-  // x(j) = e(j) + f(j) x(j+1) over the segment (rows >= wlo) from zero
+  // ---- 4. g = local + product x carry, e = g / b; then the backward
+  // recurrence x(j) = e(j) + f(j) x(j+1) over the segment (rows >= wlo)
   const int wlo = (f >= 3) ? pick(C.JSt, f - 3) - 1 : 1;
   const int qb = wlo > j0 ? wlo - j0 : 0;  // first row of the segment to solve
-  double2 xv[SEG_K];
-  double2 xl = z2();
-  double ps = 1.0;
+  const bool solves = nr > 0 && qb < nr;
   {
     const double2 c = (nr > 0) ? SV[s * MT + m] : z2();
     double pi = 1.0;
-    double2 ev[SEG_K];
 #pragma unroll
     for (int q = 0; q < SEG_K; q++) {
-      ev[q] = z2();
       if (q < nr) {
         const int j = j0 + q;
         pi = TB[j] * pi;
-        const double2 gv = make_double2(gl[q].x + pi * c.x, gl[q].y + pi * c.y);
+        const double2 gv = NLt[j * MT + m];
         const double rb = TB[L + j];
-        ev[q] = make_double2(gv.x * rb, gv.y * rb);
+        NLt[j * MT + m] = make_double2((gv.x + pi * c.x) * rb, (gv.y + pi * c.y) * rb);
       }
     }
+    double2 xl = z2();
+    double ps = 1.0;
 #pragma unroll
     for (int q = SEG_K - 1; q >= 0; q--) {
-      xv[q] = z2();
       if (q < nr && q >= qb) {
-        const double fj = TB[5 * L + j0 + q];
-        xl = make_double2(ev[q].x + fj * xl.x, ev[q].y + fj * xl.y);
+        const int j = j0 + q;
+        const double fj = TB[2 * L + j];
+        const double2 e = NLt[j * MT + m];
+        xl = make_double2(e.x + fj * xl.x, e.y + fj * xl.y);
         ps = fj * ps;
-        xv[q] = xl;
+        NLt[j * MT + m] = xl;
       }
     }
-  }
-  // each thread overwrites only its own SV entry, read above by itself;
-  // SP was last read in step 3, before the barrier
-  const bool solves = nr > 0 && qb < nr;
-  if (solves) {
-    SV[s * MT + m] = xl;
-    if (m == 0) SP[s] = ps;
+    // each thread overwrites only its own SV entry, read above by itself;
+    // SP was last read in step 3, before the barrier
+    if (solves) {
+      SV[s * MT + m] = xl;
+      if (m == 0) SP[s] = ps;
+    }
   }
   __syncthreads();
   // ---- 5. the segment starts carried up the column, one lane per mode
@@ -392,8 +421,9 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
     for (int q = SEG_K - 1; q >= 0; q--) {
       if (q < nr && q >= qb) {
         const int j = j0 + q;
-        p2 = TB[5 * L + j] * p2;
-        dst[(long)j * ss + mg] = make_double2(xv[q].x + p2 * c.x, xv[q].y + p2 * c.y);
+        p2 = TB[2 * L + j] * p2;
+        const double2 xl = NLt[j * MT + m];
+        dst[(long)j * ss + mg] = make_double2(xl.x + p2 * c.x, xl.y + p2 * c.y);
       }
     }
   }
@@ -486,24 +516,26 @@ static int col_threads(const dg_handle *h, int mt) {
 }
 
 // The case description of handle h for `mt` modes per CTA (builds the
-// tensor maps of its CU arrays for that tile width).
+// tensor maps of its CU, rhs and CF arrays and CP for that tile width).
 static int fill_case(dg_handle *h, int mt, ColCase *cc) {
   const int L = h->NY + 2;
   int by = 0, nbox = 0, nseg = 0;
   col_geometry(h, &by, &nbox, &nseg);
   memset(cc, 0, sizeof(*cc));
-  for (int f = 0; f < h->nf; f++)
+  for (int f = 0; f < h->nf; f++) {
     DG_TRY(dg_tmap_planes(h->cu[f], h->ss, L, mt, by, &cc->map_cu[f]));
+    DG_TRY(dg_tmap_planes(h->rhs[f], h->ss, L, mt, by, &cc->map_nl[f]));
+    DG_TRY(dg_tmap_planes(h->cf[f], h->ss, L, mt, by, &cc->map_cf[f]));
+  }
+  DG_TRY(dg_tmap_planes(h->cp, h->ss, L, mt, by, &cc->map_cp));
   cc->C = make_col_const(h);
   cc->dscal = h->dscal;
   cc->tab = h->cn_tab;
   cc->kxv = h->kx;
   cc->kzv = h->kz;
   cc->rowc = h->rowc;
-  cc->cp = h->cp;
   for (int f = 0; f < h->nf; f++) {
     cc->cu[f] = h->cu[f];
-    cc->nl[f] = h->rhs[f];
     cc->cf[f] = h->cf[f];
     cc->out[f] = (f < 3 || dg_col_th_to_rhs(h, f - 3)) ? h->rhs[f] : h->cu[f];
   }

@@ -12,38 +12,44 @@
 //   CN solves        for/channel.f:771-1029 (THOMAS_*_MPI, for/mpi.f:630-866)
 // REM_DIV_CHAN and the pressure update follow as their own launch (k_rd_col).
 //
-// One CTA per (mode tile, field); one thread per (mode, segment of SEG_K
-// consecutive rows).  The CN system of a field is the same for every mode,
-// and its elimination (the substep's table: multipliers a, reciprocal pivots
-// 1/b, upper diagonal c) turns the solve into two first-order linear
+// A work item is (case, mode tile, field); one thread per (mode, segment of
+// SEG_K consecutive rows).  The CN system of a field is the same for every
+// mode, and its elimination (the substep's table: multipliers a, reciprocal
+// pivots 1/b, f = -c/b) turns the solve into two first-order linear
 // recurrences, forward g(j) = r(j) + a(j) g(j-1) and backward
-// x(j) = e(j) + f(j) x(j+1) with e = g/b, f = -c/b.  A linear recurrence
-// splits exactly over segments: each thread runs its segment from a zero
-// start, keeping the product of the coefficients; one lane per mode then
-// carries the segment ends across the column (NSEG steps instead of NY + 2),
-// and each thread adds carry x product to its rows.  The same algebra as
+// x(j) = e(j) + f(j) x(j+1) with e = g/b.  A linear recurrence splits exactly
+// over segments: each thread runs its segment from a zero start, keeping the
+// product of the coefficients; one lane per mode then carries the segment
+// ends across the column (one step per segment instead of one per row), and
+// each thread adds carry x product to its rows.  The same algebra as
 // THOMAS_FORWARD / THOMAS_BACKWARD, with the rounding of a different order
 // of the same operations.  Segment boundaries depend only on NY, so a mode's
 // arithmetic does not depend on the tile width.
 //
-// The field's input tiles -- CU, the NL term the z-forward kernel left in
-// the field's rhs array, CF_old (substeps 2, 3) and CP (velocity fields) --
-// arrive in shared memory by bulk tensor copies (TMA, no multicast), all
-// issued at once by one thread and completed on one mbarrier with a bounded
-// wait; the table rows are staged meanwhile.  The right-hand side replaces
-// NL in shared memory, the recurrences run there, and the post-CN field goes
-// to the field's rhs array.  CU is read-only in this kernel, so
+// The kernel is persistent: each CTA takes work items in a grid-stride loop
+// through two shared-memory stages.  One thread fetches an item's inputs --
+// the field's CU tile, the NL term the z-forward kernel left in the field's
+// rhs array, CF_old (substeps 2, 3), CP (velocity fields), by bulk tensor
+// copies (TMA, no multicast), and its table and grid-factor rows by bulk
+// copies -- into a stage, all on the stage's mbarrier; the CTA computes the
+// item in the other stage meanwhile, so the loads of item i + 1 overlap the
+// arithmetic of item i.  Every wait is bounded.  The right-hand side
+// replaces NL in shared memory, the recurrences run there, and the post-CN
+// field goes to the field's rhs array.  CU is read-only in this kernel, so
 // a field's right-hand side may read another field (rotation, buoyancy,
 // GRAV, DRHODX/Z) without a race.  REM_DIV then reads the post-CN velocity
 // from the rhs arrays and writes CU.  A scalar that no velocity right-hand
 // side reads is written in place.
 //
 // The same kernel serves one case (a one-case table) and the ensemble
-// server's groups (a ragged (case, tile, field) work list over every member),
-// so a case computes with the same machine code either way.
+// server's groups (a ragged work list over every member), so a case
+// computes with the same machine code either way.
 #include <string.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "dg_internal.cuh"
@@ -85,11 +91,12 @@ __device__ __forceinline__ T pick(const T (&a)[DG_MAX_TH], int i) {
 
 __device__ __forceinline__ double2 z2() { return make_double2(0.0, 0.0); }
 
-// rowc: per-row grid factors [8][NY+2]
+// rowc: per-row grid factors [8][LP] (LP = NY + 2 rounded up to even, so
+// rows start on 16-byte boundaries for the bulk copies)
 //   0 1/(DY(j+1) DYF(j))  1 1/(DY(j) DYF(j))       (GYF rows: U1, U3, TH)
 //   2 1/(DYF(j) DY(j))    3 1/(DYF(j-1) DY(j))     (GY rows: U2)
-//   4 1/DY(j)             5 1/DYF(j)               6 REM_DIV upper diagonal
-//   7 DYF(j)
+//   4 1/DY(j)             5 DYF(j)                 (U2)
+//   6 1/DYF(j)            7 REM_DIV upper diagonal
 
 // The field's coefficients that do not change along the column.
 struct FieldCoef {
@@ -125,15 +132,15 @@ __device__ __forceinline__ FieldCoef field_coef(const ColConst &C, const double 
 
 // The explicit terms fv (the new CF) and the CN right-hand side r of field f
 // at row j, mode mg (offset o): u, um, up = CU at j, j-1, j+1; nlv = NL;
-// old = CF_old; p0, pm = CP at j, j-1.  RC: the field's rowc rows in shared
-// memory, [4][L]: rows 0, 1 (U1, U3, TH) or 2, 3, 4, 7 (U2).
+// old = CF_old; p0, pm = CP at j, j-1.  RC: the field's grid-factor rows in
+// shared memory, row stride ld: rows 0, 1 (U1, U3, TH) or 2, 3, 4, 5 (U2).
 __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, int f, int j,
                                         long o, bool mean, double KX, double KZ, double kk,
-                                        const double *RC, double2 u, double2 um, double2 up,
+                                        const double *RC, int ld, double2 u, double2 um, double2 up,
                                         double2 nlv, double2 old, double2 p0, double2 pm,
                                         double2 &fv, double2 &r) {
   const ColConst &C = cc.C;
-  const int L = C.NY + 2, nth = C.nth;
+  const int nth = C.nth;
   const long ss = C.ss;
   if (f == 0 || f == 2) {
     fv = make_double2(-k.NU * kk * u.x, -k.NU * kk * u.y);
@@ -163,14 +170,14 @@ __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, i
     }
     r.x += k.T5 * fv.x;
     r.y += k.T5 * fv.y;
-    const double cup = k.aaU * RC[0 * L + j], cdn = k.aaU * RC[1 * L + j];
+    const double cup = k.aaU * RC[0 * ld + j], cdn = k.aaU * RC[1 * ld + j];
     r.x += cup * (up.x - u.x) - cdn * (u.x - um.x);
     r.y += cup * (up.y - u.y) - cdn * (u.y - um.y);
   } else if (f == 1) {
     fv = make_double2(-k.NU * kk * u.x, -k.NU * kk * u.y);
     if (!mean) {
-      const double dyfj = RC[3 * L + j], dyfm = RC[3 * L + j - 1];
-      const double bw2 = 0.5 * RC[2 * L + j];
+      const double dyfj = RC[3 * ld + j], dyfm = RC[3 * ld + j - 1];
+      const double bw2 = 0.5 * RC[2 * ld + j];
       for (int q = 0; q < nth; q++) {
         if (C.ri[q] * C.grav_y == 0.0) continue;
         const double w = C.ri[q] * C.grav_y * bw2;
@@ -184,12 +191,12 @@ __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, i
     r = u;
     r.x += k.T3 * old.x;
     r.y += k.T3 * old.y;
-    const double idy = RC[2 * L + j];
+    const double idy = RC[2 * ld + j];
     r.x -= k.T4 * ((p0.x - pm.x) * idy);
     r.y -= k.T4 * ((p0.y - pm.y) * idy);
     r.x += k.T5 * fv.x;
     r.y += k.T5 * fv.y;
-    const double cup2 = k.aaU * RC[0 * L + j], cdn2 = k.aaU * RC[1 * L + j];
+    const double cup2 = k.aaU * RC[0 * ld + j], cdn2 = k.aaU * RC[1 * ld + j];
     r.x += cup2 * (up.x - u.x) - cdn2 * (u.x - um.x);
     r.y += cup2 * (up.y - u.y) - cdn2 * (u.y - um.y);
   } else {
@@ -206,116 +213,100 @@ __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, i
     r.y += k.T3 * old.y;
     r.x += k.T5 * fv.x;
     r.y += k.T5 * fv.y;
-    const double cup = k.aaU * RC[0 * L + j], cdn = k.aaU * RC[1 * L + j];
+    const double cup = k.aaU * RC[0 * ld + j], cdn = k.aaU * RC[1 * ld + j];
     r.x += k.ipr * (cup * (up.x - u.x) - cdn * (u.x - um.x));
     r.y += k.ipr * (cup * (up.y - u.y) - cdn * (u.y - um.y));
   }
 }
 
-// Shared memory of one CTA (128-byte aligned base): four tiles [nbox * by][MT]
-// -- CU, NL (which then holds g, e and x of the recurrences), CF_old, CP --;
-// per (segment, mode) values SV [nseg][MT]; per segment products SP [nseg];
-// the CN table rows TB [5][L] (a, 1/b, f = -c/b, kind, BC value); the
-// field's grid factors RC [4][L]; the mbarrier.
-size_t col_smem_l(int L, int mt, int by, int nbox, int nseg) {
-  return sizeof(double2) * (4 * (size_t)nbox * by * mt + (size_t)nseg * mt) +
-         sizeof(double) * ((size_t)nseg + 9 * (size_t)L) + 8 + 128;
+// Launch-wide sizes: a stage holds the largest item of the work list.
+struct ColLaunch {
+  int tile;   // double2 per input tile (nbox * by * MT of the largest case)
+  int lp;     // table row length (the largest case's NY + 2, rounded up to even)
+  int nseg;   // segments per column (the largest case)
+  int nwork;  // work items
+};
+
+// A stage (128-byte aligned): the tiles CU, NL (which then holds g, e and x
+// of the recurrences), CF_old, CP [tile] double2; the CN table rows TB
+// [5][lp] (a, 1/b, f = -c/b, kind, BC value); the field's grid factors RC
+// [4][lp].  After the two stages, once per CTA: SV [nseg][MT] double2 (per
+// segment and mode values, then carries), SP [nseg] (per segment products),
+// the stages' two mbarriers.
+__host__ __device__ inline size_t col_stage_bytes(int tile, int lp) {
+  const size_t b = sizeof(double2) * 4 * (size_t)tile + sizeof(double) * 9 * (size_t)lp;
+  return (b + 127) / 128 * 128;
 }
 
-// The column stage of field f for modes m0 .. m0+MT-1 of one case.
+size_t col_smem_l(const ColLaunch &P, int mt) {
+  return 2 * col_stage_bytes(P.tile, P.lp) + sizeof(double2) * (size_t)P.nseg * mt +
+         sizeof(double) * (size_t)P.nseg + 16 + 128;
+}
+
+// One thread fetches work item w into a stage: the field's tiles by bulk
+// tensor copies, its table and grid-factor rows by bulk copies, all on the
+// stage's mbarrier (extra_tx: 0, or 16 in the wait test, where the barrier
+// then never completes).
 template <int MT>
-__device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0, int f,
-                                         long spin, unsigned extra_tx, unsigned char *sbase) {
+__device__ __forceinline__ void col_issue(const ColCase &cc, int4 w, int rk_step,
+                                          const ColLaunch &P, unsigned char *stage,
+                                          unsigned long long *bar, unsigned extra_tx) {
+  const int f = w.z;
+  const int L = cc.C.NY + 2, LP = (L + 1) & ~1;
+  const int ctile = cc.nbox * cc.by * MT;
+  const bool vel = f < 3, old_cf = rk_step > 1;
+  double2 *CUt = reinterpret_cast<double2 *>(stage);
+  double2 *NLt = CUt + P.tile, *CFt = NLt + P.tile, *CPt = CFt + P.tile;
+  double *TB = reinterpret_cast<double *>(CPt + P.tile);
+  double *RC = TB + 5 * P.lp;
+  const unsigned ntiles = 2u + (old_cf ? 1u : 0u) + (vel ? 1u : 0u);
+  const int nrc = (f == 1) ? 4 : 2;  // grid-factor rows 2..5 (U2) or 0..1
+  dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * ctile) * ntiles +
+                             (unsigned)(sizeof(double) * (5 + nrc) * LP) + extra_tx);
+  // columns beyond ss and planes beyond L arrive as zeros
+  for (int q = 0; q < cc.nbox; q++) {
+    const long d = (long)q * cc.by * MT;
+    const int x = 2 * w.y * MT, y = q * cc.by;
+    dg_tma_load_2d(CUt + d, &cc.map_cu[f], x, y, bar);
+    dg_tma_load_2d(NLt + d, &cc.map_nl[f], x, y, bar);
+    if (old_cf) dg_tma_load_2d(CFt + d, &cc.map_cf[f], x, y, bar);
+    if (vel) dg_tma_load_2d(CPt + d, &cc.map_cp, x, y, bar);
+  }
+  dg_bulk_load(TB, cc.tab + ((long)(rk_step - 1) * (3 + DG_MAX_TH) + f) * 5 * LP,
+               (unsigned)(sizeof(double) * 5 * LP), bar);
+  dg_bulk_load(RC, cc.rowc + (long)(f == 1 ? 2 : 0) * LP, (unsigned)(sizeof(double) * nrc * LP),
+               bar);
+}
+
+// The column stage of field f for modes m0 .. m0+MT-1 of one case, from a
+// stage whose copies have landed.
+template <int MT>
+__device__ __forceinline__ void col_item(const ColCase &cc, int rk_step, long m0, int f,
+                                         const ColLaunch &P, unsigned char *stage, double2 *SV,
+                                         double *SP) {
   const ColConst &C = cc.C;
-  const int NY = C.NY, L = NY + 2;
+  const int NY = C.NY, L = NY + 2, LP = (L + 1) & ~1;  // the case's own row length
   const int nseg = cc.nseg;
   const long ss = C.ss;
   const int mt = (int)((ss - m0) < MT ? (ss - m0) : MT);
-  const bool vel = f < 3;
   const bool old_cf = rk_step > 1;
-  const int tile = cc.nbox * cc.by * MT;
-  double2 *CUt = reinterpret_cast<double2 *>(sbase);
-  double2 *NLt = CUt + tile;
-  double2 *CFt = NLt + tile;
-  double2 *CPt = CFt + tile;
-  double2 *SV = CPt + tile;
-  double *SP = reinterpret_cast<double *>(SV + nseg * MT);
-  double *TB = SP + nseg;
-  double *RC = TB + 5 * L;
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(RC + 4 * L);
-  const int tid = threadIdx.x, nthr = blockDim.x;
+  double2 *CUt = reinterpret_cast<double2 *>(stage);
+  double2 *NLt = CUt + P.tile, *CFt = NLt + P.tile, *CPt = CFt + P.tile;
+  const double *TB = reinterpret_cast<const double *>(CPt + P.tile);
+  const double *RC = TB + 5 * P.lp;  // the slots are sized for the largest case
+  const int tid = threadIdx.x;
   const int m = tid % MT, s = tid / MT;
   const int j0 = s * SEG_K;
   const int nr = (s < nseg) ? min(SEG_K, L - j0) : 0;  // rows of this thread's segment
   const long mg = m0 + m;
   const bool live = m < mt;
   const bool mean = (mg == 0);
-
-  // ---- 0. tables (they do not depend on the preceding kernel), loads
-  // issued in batches before their stores so their latencies overlap
-  if (tid == 0) dg_mbar_init(bar, 1);
-  {
-    const double *tb = cc.tab + ((long)(rk_step - 1) * (3 + DG_MAX_TH) + f) * 5 * L;
-    // the field's rowc rows: 0, 1 (GYF fields) or 2, 3, 4, 7 (U2)
-    const int r0 = (f == 1) ? 2 : 0, r1 = (f == 1) ? 3 : 1, r2 = (f == 1) ? 4 : 0,
-              r3 = (f == 1) ? 7 : 1;
-    constexpr int SU = 8;
-    for (int base = 0; base < 9 * L; base += SU * nthr) {
-      double v[SU];
-#pragma unroll
-      for (int u = 0; u < SU; u++) {
-        const int i = base + u * nthr + tid;
-        v[u] = 0.0;
-        if (i < 5 * L) {
-          // table rows a, 1/b, c, kind, BC value in that order
-          v[u] = tb[i];
-        } else if (i < 9 * L) {
-          const int r = (i - 5 * L) / L, j = (i - 5 * L) - r * L;
-          const int rr = r == 0 ? r0 : r == 1 ? r1 : r == 2 ? r2 : r3;
-          v[u] = cc.rowc[rr * L + j];
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < SU; u++) {
-        const int i = base + u * nthr + tid;
-        if (i < 9 * L) TB[i] = v[u];  // RC follows TB contiguously
-      }
-    }
-  }
   const long mgc = live ? mg : 0;
   const double KX = cc.kxv[mgc % C.nkxp], KZ = cc.kzv[mgc / C.nkxp];
   const double k2 = KX * KX + KZ * KZ;
   const double kk = (C.beta == 1.0) ? k2 : pow(k2, C.beta);
-  __syncthreads();
-  // row 2 of TB becomes f = -c / b (the backward recurrence's coefficient)
-  for (int j = tid; j < L; j += nthr) TB[2 * L + j] = (j < L - 1) ? -TB[2 * L + j] * TB[L + j] : 0.0;
 
-  // ---- 1. the four tiles by bulk tensor copies, all in flight at once
-  dg_pdl_wait();  // NL comes from the z-forward kernel
-  if (tid == 0) {
-    // columns beyond ss and planes beyond L arrive as zeros (extra_tx is 0
-    // except in the wait test, where the barrier can then never complete)
-    const unsigned ntiles = 2u + (old_cf ? 1u : 0u) + (vel ? 1u : 0u);
-    dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * tile) * ntiles + extra_tx);
-    for (int q = 0; q < cc.nbox; q++) {
-      const long d = (long)q * cc.by * MT;
-      const int x = (int)(2 * m0), y = q * cc.by;
-      dg_tma_load_2d(CUt + d, &cc.map_cu[f], x, y, bar);
-      dg_tma_load_2d(NLt + d, &cc.map_nl[f], x, y, bar);
-      if (old_cf) dg_tma_load_2d(CFt + d, &cc.map_cf[f], x, y, bar);
-      if (vel) dg_tma_load_2d(CPt + d, &cc.map_cp, x, y, bar);
-    }
-  }
-  const bool landed = dg_mbar_wait(bar, 0, spin);
-  if (__syncthreads_or(!landed)) {
-    if (tid == 0) {
-      atomicExch(cc.err + 1, 1);
-      dg_mbar_wait(bar, 0, spin);  // the copies in flight get one more bounded wait
-    }
-    return;
-  }
-
-  // ---- 2. explicit terms, CF and the right-hand side row by row, and the
+  // ---- 1. explicit terms, CF and the right-hand side row by row, and the
   // forward recurrence g(j) = r(j) + a(j) g(j-1) over the segment from zero;
   // g replaces NL (each (row, mode) element belongs to one thread)
   const FieldCoef k = field_coef(C, cc.dscal, rk_step, f);
@@ -327,14 +318,14 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
     if (q < nr) {
       const int j = j0 + q;
       const int i = j * MT + m;
-      const double kind = TB[3 * L + j];
+      const double kind = TB[3 * LP + j];
       // a BC row's value goes to the real part of the (0,0) mode only
-      double2 r = make_double2((kind == (double)ROW_BC && mean) ? TB[4 * L + j] : 0.0, 0.0);
+      double2 r = make_double2((kind == (double)ROW_BC && mean) ? TB[4 * LP + j] : 0.0, 0.0);
       if (j >= k.lo && j <= k.hi) {
         const long o = (long)j * ss + mg;
         double2 fv, rr;
-        rhs_row(cc, k, f, j, o, mean, KX, KZ, kk, RC, CUt[i], CUt[i - MT], CUt[i + MT], NLt[i],
-                old_cf ? CFt[i] : z2(), CPt[i], CPt[i - MT], fv, rr);
+        rhs_row(cc, k, f, j, o, mean, KX, KZ, kk, RC, LP, CUt[i], CUt[i - MT], CUt[i + MT],
+                NLt[i], old_cf ? CFt[i] : z2(), CPt[i], CPt[i - MT], fv, rr);
         if (live) cff[o] = fv;
         if (kind == (double)ROW_RHS) r = rr;
       }
@@ -350,7 +341,7 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
     if (m == 0) SP[s] = pa;
   }
   __syncthreads();
-  // ---- 3. the segment ends carried down the column, one lane per mode
+  // ---- 2. the segment ends carried down the column, one lane per mode
   if (tid < MT) {
     double2 G = z2();
     for (int t = 0; t < nseg; t++) {
@@ -361,7 +352,7 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
     }
   }
   __syncthreads();
-  // ---- 4. g = local + product x carry, e = g / b; then the backward
+  // ---- 3. g = local + product x carry, e = g / b; then the backward
   // recurrence x(j) = e(j) + f(j) x(j+1) over the segment (rows >= wlo)
   const int wlo = (f >= 3) ? pick(C.JSt, f - 3) - 1 : 1;
   const int qb = wlo > j0 ? wlo - j0 : 0;  // first row of the segment to solve
@@ -375,7 +366,7 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
         const int j = j0 + q;
         pi = TB[j] * pi;
         const double2 gv = NLt[j * MT + m];
-        const double rb = TB[L + j];
+        const double rb = TB[LP + j];
         NLt[j * MT + m] = make_double2((gv.x + pi * c.x) * rb, (gv.y + pi * c.y) * rb);
       }
     }
@@ -385,7 +376,7 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
     for (int q = SEG_K - 1; q >= 0; q--) {
       if (q < nr && q >= qb) {
         const int j = j0 + q;
-        const double fj = TB[2 * L + j];
+        const double fj = TB[2 * LP + j];
         const double2 e = NLt[j * MT + m];
         xl = make_double2(e.x + fj * xl.x, e.y + fj * xl.y);
         ps = fj * ps;
@@ -393,14 +384,14 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
       }
     }
     // each thread overwrites only its own SV entry, read above by itself;
-    // SP was last read in step 3, before the barrier
+    // SP was last read in step 2, before the barrier
     if (solves) {
       SV[s * MT + m] = xl;
       if (m == 0) SP[s] = ps;
     }
   }
   __syncthreads();
-  // ---- 5. the segment starts carried up the column, one lane per mode
+  // ---- 4. the segment starts carried up the column, one lane per mode
   const int sw = wlo / SEG_K;  // lowest segment with rows to solve
   if (tid < MT) {
     double2 X = z2();
@@ -412,7 +403,7 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
     }
   }
   __syncthreads();
-  // ---- 6. x = local + product x carry: the post-CN field, rows >= wlo
+  // ---- 5. x = local + product x carry: the post-CN field, rows >= wlo
   if (solves && live) {
     const double2 c = SV[s * MT + m];
     double2 *dst = cc.out[f];
@@ -421,7 +412,7 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
     for (int q = SEG_K - 1; q >= 0; q--) {
       if (q < nr && q >= qb) {
         const int j = j0 + q;
-        p2 = TB[2 * L + j] * p2;
+        p2 = TB[2 * LP + j] * p2;
         const double2 xl = NLt[j * MT + m];
         dst[(long)j * ss + mg] = make_double2(xl.x + p2 * c.x, xl.y + p2 * c.y);
       }
@@ -429,17 +420,64 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   }
 }
 
-// The column kernel: CTA b takes work[b] = (case, mode tile, field) from
-// the case table (every case at substep rk_step with MT modes per CTA).
+// The column kernel, persistent: CTA b takes work items b, b + G, b + 2G, ...
+// (G = gridDim.x) of the case table (every case at substep rk_step with MT
+// modes per CTA), through two stages: item i + 1's copies are in flight
+// while item i is computed.
 template <int MT>
-__global__ void __launch_bounds__(COL_MAX_THR) k_col_cn(const ColCase *__restrict__ cases,
+__global__ void __launch_bounds__(COL_MAX_THR, 2) k_col_cn(const ColCase *__restrict__ cases,
                                                        const int4 *__restrict__ work,
-                                                       int rk_step, long spin,
+                                                       ColLaunch P, int rk_step, long spin,
                                                        unsigned extra_tx) {
   extern __shared__ __align__(128) unsigned char cs_raw[];
-  unsigned char *sbase = cs_raw + ((128u - (dg_smem_addr(cs_raw) & 127u)) & 127u);
-  const int4 w = work[blockIdx.x];
-  col_body<MT>(cases[w.x], rk_step, (long)w.y * MT, w.z, spin, extra_tx, sbase);
+  unsigned char *base = cs_raw + ((128u - (dg_smem_addr(cs_raw) & 127u)) & 127u);
+  const size_t sb = col_stage_bytes(P.tile, P.lp);
+  unsigned char *stg[2] = {base, base + sb};
+  double2 *SV = reinterpret_cast<double2 *>(base + 2 * sb);
+  double *SP = reinterpret_cast<double *>(SV + P.nseg * MT);
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(SP + P.nseg);
+  const int tid = threadIdx.x;
+  const int G = gridDim.x;
+  if (tid == 0) {
+    dg_mbar_init(bar, 1);
+    dg_mbar_init(bar + 1, 1);
+  }
+  __syncthreads();
+  dg_pdl_wait();  // NL comes from the z-forward kernel
+  if (tid == 0) {
+    for (int q = 0; q < 2; q++) {
+      const int w = blockIdx.x + q * G;
+      if (w < P.nwork) {
+        const int4 wi = work[w];
+        col_issue<MT>(cases[wi.x], wi, rk_step, P, stg[q], bar + q, extra_tx);
+      }
+    }
+  }
+  int it = 0;
+  for (int w = blockIdx.x; w < P.nwork; w += G, it++) {
+    const int st = it & 1;
+    const unsigned par = (unsigned)(it >> 1) & 1u;
+    const int4 wi = work[w];
+    const bool landed = dg_mbar_wait(bar + st, par, spin);
+    if (__syncthreads_or(!landed)) {
+      if (tid == 0) {
+        atomicExch(cases[wi.x].err + 1, 1);
+        // the copies in flight get one more bounded wait each
+        dg_mbar_wait(bar + st, par, spin);
+        if (w + G < P.nwork) dg_mbar_wait(bar + (st ^ 1), (unsigned)((it + 1) >> 1) & 1u, spin);
+      }
+      return;
+    }
+    col_item<MT>(cases[wi.x], rk_step, (long)wi.y * MT, wi.z, P, stg[st], SV, SP);
+    // the stage is free again: order this thread's accesses to it before the
+    // copies of the item after next
+    dg_fence_proxy_async();
+    __syncthreads();
+    if (tid == 0 && w + 2 * G < P.nwork) {
+      const int4 wn = work[w + 2 * G];
+      col_issue<MT>(cases[wn.x], wn, rk_step, P, stg[st], bar + st, extra_tx);
+    }
+  }
 }
 
 ColConst make_col_const(const dg_handle *h) {
@@ -468,25 +506,25 @@ bool dg_col_th_to_rhs(const dg_handle *h, int n) {
   return ri * h->p.grav_x != 0.0 || ri * h->p.grav_y != 0.0 || ri * h->p.grav_z != 0.0;
 }
 
-// Per-row grid factors of the column kernels (once per handle, host side).
+// Per-row grid factors of the column kernel (once per handle, host side).
 int dg_col_init(dg_handle *h) {
-  const int L = h->NY + 2;
-  double *t = (double *)calloc((size_t)8 * L, sizeof(double));
+  const int L = h->NY + 2, LP = (L + 1) / 2 * 2;
+  double *t = (double *)calloc((size_t)8 * LP, sizeof(double));
   if (!t) return DG_ERR_OOM;
   const double *dy = h->h_dy, *dyf = h->h_dyf;
   for (int j = 1; j <= h->NY; j++) {
-    t[0 * L + j] = 1.0 / (dy[j + 1] * dyf[j]);
-    t[1 * L + j] = 1.0 / (dy[j] * dyf[j]);
-    t[2 * L + j] = 1.0 / (dyf[j] * dy[j]);
-    t[3 * L + j] = 1.0 / (dyf[j - 1] * dy[j]);
-    t[5 * L + j] = 1.0 / dyf[j];
-    t[6 * L + j] = (j >= 2 && j < h->NY) ? 1.0 / (dy[j + 1] * dyf[j]) : 0.0;
+    t[0 * LP + j] = 1.0 / (dy[j + 1] * dyf[j]);
+    t[1 * LP + j] = 1.0 / (dy[j] * dyf[j]);
+    t[2 * LP + j] = 1.0 / (dyf[j] * dy[j]);
+    t[3 * LP + j] = 1.0 / (dyf[j - 1] * dy[j]);
+    t[6 * LP + j] = 1.0 / dyf[j];
+    t[7 * LP + j] = (j >= 2 && j < h->NY) ? 1.0 / (dy[j + 1] * dyf[j]) : 0.0;
   }
-  for (int j = 1; j < L; j++) t[4 * L + j] = 1.0 / dy[j];
-  for (int j = 0; j < L; j++) t[7 * L + j] = dyf[j];
-  cudaError_t e = dg_malloc(h, (void **)&h->rowc, sizeof(double) * 8 * L);
+  for (int j = 1; j < L; j++) t[4 * LP + j] = 1.0 / dy[j];
+  for (int j = 0; j < L; j++) t[5 * LP + j] = dyf[j];
+  cudaError_t e = dg_malloc(h, (void **)&h->rowc, sizeof(double) * 8 * LP);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(h->rowc, t, sizeof(double) * 8 * L, cudaMemcpyHostToDevice, h->st);
+    e = cudaMemcpyAsync(h->rowc, t, sizeof(double) * 8 * LP, cudaMemcpyHostToDevice, h->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
   free(t);
   DG_CUDA(e);
@@ -502,18 +540,24 @@ static void col_geometry(const dg_handle *h, int *by, int *nbox, int *nseg) {
   *nseg = dg_cdiv(L, SEG_K);
 }
 
-size_t dg_col_smem(const dg_handle *h, int mt) {
+// launch sizes of handle h alone at mt modes per CTA (nwork left 0)
+static ColLaunch col_sizes(const dg_handle *h, int mt) {
   int by, nbox, nseg;
   col_geometry(h, &by, &nbox, &nseg);
-  return col_smem_l(h->NY + 2, mt, by, nbox, nseg);
+  ColLaunch P;
+  P.tile = nbox * by * mt;
+  P.lp = (h->NY + 2 + 1) / 2 * 2;
+  P.nseg = nseg;
+  P.nwork = 0;
+  return P;
 }
 
 // threads of one CTA for handle h at mt modes: one per (mode, segment)
 static int col_threads(const dg_handle *h, int mt) {
-  int by, nbox, nseg;
-  col_geometry(h, &by, &nbox, &nseg);
-  return (mt * nseg + 31) / 32 * 32;
+  return (mt * col_sizes(h, mt).nseg + 31) / 32 * 32;
 }
+
+size_t dg_col_smem(const dg_handle *h, int mt) { return col_smem_l(col_sizes(h, mt), mt); }
 
 // The case description of handle h for `mt` modes per CTA (builds the
 // tensor maps of its CU, rhs and CF arrays and CP for that tile width).
@@ -547,7 +591,7 @@ static int fill_case(dg_handle *h, int mt, ColCase *cc) {
 }
 
 // modes per CTA for handle h: the tuned value, halved until the CTA fits
-// (shared memory, and one thread per mode and segment)
+// (two stages in shared memory, one thread per mode and segment)
 static int col_mt(const dg_handle *h, int want) {
   int mt = want;
   while (mt > 2 && (dg_col_smem(h, mt) > 220 * 1024 || col_threads(h, mt) > COL_MAX_THR)) mt /= 2;
@@ -564,11 +608,41 @@ static int col_fits(const dg_handle *h, int mt) {
 
 int dg_col_mt_eff(const dg_handle *h) { return col_mt(h, h->cn_mt); }
 
-// the work list of one case: (case c, tile, field, 0) per CTA
+// the work list of one case: (case c, tile, field, 0) per item
 static void case_work(const dg_handle *h, int c, int mt, std::vector<int4> &work) {
   const int tiles = dg_cdiv(h->ss, mt);
   for (int f = 0; f < h->nf; f++)
     for (int t = 0; t < tiles; t++) work.push_back(make_int4(c, t, f, 0));
+}
+
+// CTAs of the persistent launch: as many as fit on the device at once (at
+// most one per work item)
+static int col_grid(int mt, int thr, size_t smem, int nwork) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, size_t>, int> cache;
+  int per_sm = 0, nsm = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(std::make_tuple(mt, thr, smem));
+    if (it != cache.end()) {
+      per_sm = it->second;
+    } else {
+      const void *kern = mt == 2 ? (const void *)k_col_cn<2>
+                       : mt == 4 ? (const void *)k_col_cn<4>
+                       : mt == 8 ? (const void *)k_col_cn<8>
+                                 : (const void *)k_col_cn<16>;
+      dg_big_smem(kern);
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, thr, smem) != cudaSuccess ||
+          per_sm < 1)
+        per_sm = 1;
+      cache[std::make_tuple(mt, thr, smem)] = per_sm;
+    }
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) nsm = 148;
+  const long g = (long)per_sm * nsm;
+  return (int)(g < nwork ? g : nwork);
 }
 
 // The handle's device copy of its one-case table and work list for mt,
@@ -603,18 +677,53 @@ static int col_tables(dg_handle *h, int mt) {
   return DG_OK;
 }
 
-static int launch_col(cudaStream_t st, int pdl, int mt, int thr, size_t smem,
-                      const void *dev_cases, const int4 *dev_work, int nwork, int rk_step,
-                      long spin, unsigned extra_tx) {
+static int launch_col(cudaStream_t st, int pdl, const dg_col_launch &cl, const void *dev_cases,
+                      const int4 *dev_work, int rk_step, long spin, unsigned extra_tx) {
+  ColLaunch P;
+  P.tile = cl.tile;
+  P.lp = cl.lp;
+  P.nseg = cl.nseg;
+  P.nwork = cl.nwork;
 #define CS_CASE(MTV)                                                                            \
-  if (mt == MTV) {                                                                              \
+  if (cl.mt == MTV) {                                                                           \
     dg_big_smem((const void *)k_col_cn<MTV>);                                                   \
-    DG_CUDA(dg_launch(pdl, k_col_cn<MTV>, dim3(nwork), dim3(thr), smem, st,                     \
-                      (const ColCase *)dev_cases, dev_work, rk_step, spin, extra_tx));          \
+    DG_CUDA(dg_launch(pdl, k_col_cn<MTV>, dim3(cl.grid), dim3(cl.thr), cl.smem, st,             \
+                      (const ColCase *)dev_cases, dev_work, P, rk_step, spin, extra_tx));       \
   }
   CS_CASE(2) CS_CASE(4) CS_CASE(8) CS_CASE(16)
 #undef CS_CASE
   DG_LAUNCHED();
+  return DG_OK;
+}
+
+// launch sizes of handles hs together at `want` modes per CTA: the largest
+// any of them needs (a case's CTAs leave threads beyond its own segments idle)
+static int col_plan(dg_handle *const *hs, int n, int want, int nwork, dg_col_launch *cl) {
+  int mt = want;
+  for (int c = 0; c < n; c++) mt = std::min(mt, col_mt(hs[c], want));
+  dg_col_launch r = {};
+  r.mt = mt;
+  for (int c = 0; c < n; c++) {
+    DG_TRY(col_fits(hs[c], mt));
+    const ColLaunch P = col_sizes(hs[c], mt);
+    r.tile = std::max(r.tile, P.tile);
+    r.lp = std::max(r.lp, P.lp);
+    r.nseg = std::max(r.nseg, P.nseg);
+    r.thr = std::max(r.thr, col_threads(hs[c], mt));
+  }
+  ColLaunch P;
+  P.tile = r.tile;
+  P.lp = r.lp;
+  P.nseg = r.nseg;
+  P.nwork = nwork;
+  r.smem = col_smem_l(P, mt);
+  if (r.smem > 220 * 1024) {
+    dg_set_error("column kernel: the cases' tiles do not fit in shared memory together");
+    return DG_ERR_DIMS;
+  }
+  r.nwork = nwork;
+  r.grid = col_grid(mt, r.thr, r.smem, nwork);
+  *cl = r;
   return DG_OK;
 }
 
@@ -630,13 +739,15 @@ int dg_col_step_dev(dg_handle *h, int rk_step, bool rd) {
   const int mt = col_mt(h, h->cn_mt);
   DG_TRY(col_fits(h, mt));
   DG_TRY(col_tables(h, mt));
+  dg_col_launch cl;
+  dg_handle *hs[1] = {h};
+  DG_TRY(col_plan(hs, 1, mt, h->col_dnwork, &cl));
   // the wait test (DG_TUNE_WAIT_TEST) applies to this one launch
   const long spin = h->wait_test > 0 ? (long)h->wait_test : DG_ASYNC_SPIN;
   const unsigned extra_tx = h->wait_test > 0 ? 16u : 0u;
   h->wait_test = 0;
   dg_kt_begin(h, "k_col_cn", h->st);
-  DG_TRY(launch_col(h->st, h->pdl, mt, col_threads(h, mt), dg_col_smem(h, mt), h->col_dcase,
-                    h->col_dwork, h->col_dnwork, rk_step, spin, extra_tx));
+  DG_TRY(launch_col(h->st, h->pdl, cl, h->col_dcase, h->col_dwork, rk_step, spin, extra_tx));
   if (rd) DG_TRY(dg_rem_div_dev(h, 1, rk_step, true));
   return DG_OK;
 }
@@ -645,24 +756,15 @@ int dg_col_step_dev(dg_handle *h, int rk_step, bool rd) {
 // The column stage of several cases at the same substep in one launch (the
 // ensemble server's groups).  dg_col_batch_build fills, for the handles, the
 // host images of the case table and the work list (one (case, tile, field)
-// entry per CTA) with one MT for all, and returns the launch's threads per
-// CTA and shared memory (the largest any case needs; a case's CTAs leave
-// the threads beyond its own segments idle); the caller copies the images
-// to device memory it owns and launches with dg_col_batch_launch.  Each
-// case's REM_DIV follows on its own stream.  Results do not depend on the
-// batch: each mode's arithmetic is the single-case launch's, with the same
-// kernel.
+// entry per item) with one MT for all, and the launch sizes; the caller
+// copies the images to device memory it owns and launches with
+// dg_col_batch_launch.  Each case's REM_DIV follows on its own stream.
+// Results do not depend on the batch: each mode's arithmetic is the
+// single-case launch's, with the same kernel.
 int dg_col_batch_build(dg_handle *const *hs, int n, int want_mt, std::vector<unsigned char> &cases,
-                       std::vector<int4> &work, int *mt_out, int *thr_out, size_t *smem_out) {
+                       std::vector<int4> &work, dg_col_launch *cl) {
   int mt = want_mt;
   for (int c = 0; c < n; c++) mt = std::min(mt, col_mt(hs[c], want_mt));
-  size_t sm = 0;
-  int thr = 0;
-  for (int c = 0; c < n; c++) {
-    DG_TRY(col_fits(hs[c], mt));
-    sm = std::max(sm, dg_col_smem(hs[c], mt));
-    thr = std::max(thr, col_threads(hs[c], mt));
-  }
   cases.assign(sizeof(ColCase) * n, 0);
   work.clear();
   for (int c = 0; c < n; c++) {
@@ -671,14 +773,10 @@ int dg_col_batch_build(dg_handle *const *hs, int n, int want_mt, std::vector<uns
     memcpy(cases.data() + sizeof(ColCase) * c, &cc, sizeof(ColCase));
     case_work(hs[c], c, mt, work);
   }
-  *mt_out = mt;
-  *thr_out = thr;
-  *smem_out = sm;
-  return DG_OK;
+  return col_plan(hs, n, mt, (int)work.size(), cl);
 }
 
-int dg_col_batch_launch(cudaStream_t st, int mt, int thr, size_t smem, const void *dev_cases,
-                        const int4 *dev_work, int nwork, int rk_step) {
-  return launch_col(st, 0, mt, thr, smem, dev_cases, dev_work, nwork, rk_step, DG_ASYNC_SPIN,
-                    0u);
+int dg_col_batch_launch(cudaStream_t st, const dg_col_launch &cl, const void *dev_cases,
+                        const int4 *dev_work, int rk_step) {
+  return launch_col(st, 0, cl, dev_cases, dev_work, rk_step, DG_ASYNC_SPIN, 0u);
 }

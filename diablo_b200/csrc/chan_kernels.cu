@@ -1195,7 +1195,8 @@ size_t zfwd_smem(const dg_handle *h) {
 //   CN row : l = t l1, d = 1 + t d1, u = t u1   with t = TEMP1 (or TEMP1/PR)
 //   fixed  : l0, d0, u0 and the BC value
 // and one CTA per (substep, field) runs the elimination whenever DELTA_T
-// changes.  Output per (rk, field): [5][NY+2] = a', 1/b', c, kind, bc value.
+// changes.  Output per (rk, field): [5][LP] = a', 1/b', -c/b', kind, bc value
+// (LP = NY + 2 rounded up to even).
 struct CnRows {
   int NY, nfld;
   double nu, nuv, pr[3 + DG_MAX_TH];  // pr = 1 for velocity
@@ -1263,8 +1264,20 @@ __global__ void __launch_bounds__(CT_THR) k_cn_tables(CnRows P, const double *__
     }
   }
   __syncthreads();
-  double *Tg = tab + (long)(rk * (3 + DG_MAX_TH) + f) * 5 * L;
-  for (int i = threadIdx.x; i < 5 * L; i += CT_THR) Tg[i] = T[i];
+  // rows of LP = L rounded up to even doubles, so every row starts on a
+  // 16-byte boundary (the column kernel fetches them by bulk copies)
+  const int LP = (L + 1) & ~1;
+  double *Tg = tab + (long)(rk * (3 + DG_MAX_TH) + f) * 5 * LP;
+  for (int i = threadIdx.x; i < 5 * LP; i += CT_THR) {
+    const int r = i / LP, j = i - r * LP;
+    double v = 0.0;
+    if (j < L) {
+      // row 2: the backward recurrence's coefficient -c / b (0 on the last row)
+      if (r == 2) v = (j < L - 1) ? -T[2 * L + j] * T[L + j] : 0.0;
+      else v = T[r * L + j];
+    }
+    Tg[i] = v;
+  }
 }
 
 // ------------------------------------------------------------- REM_DIV

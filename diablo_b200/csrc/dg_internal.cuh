@@ -116,7 +116,7 @@ struct dg_handle {
   double2 *rhs[3 + DG_MAX_TH];  // CN right-hand sides
   double2 *gphi;                // REM_DIV forward-sweep scratch
   double *rem_a, *rem_rb;       // REM_DIV multipliers and reciprocal pivots [NY+2][ss]
-  double *cn_tab;               // CN tables [rk][field][5][NY+2]
+  double *cn_tab;               // CN tables [rk][field][5][LP] (LP: NY+2 rounded up to even)
   double *cn_rows;              // CN row templates [field][8][NY+2]
 
   // work arrays
@@ -152,10 +152,10 @@ struct dg_handle {
   int cn_mt;                    // modes per CTA of the column (CN) kernel (2, 4, 8, 16)
   int xrow_chunk;               // planes per CTA of the x-row product kernel (0 = auto)
   int ychunk;                   // planes per y-chunk of a substep (0 = all)
-  double *rowc;                 // per-row grid factors of the column kernel [8][NY+2]
+  double *rowc;                 // per-row grid factors of the column kernel [8][LP]
   void *col_dcase;              // device case table of the column kernel (one case)
   int4 *col_dwork;              // and its work list
-  int col_dmt, col_dnwork;      // the modes per CTA they were built for; CTAs
+  int col_dmt, col_dnwork;      // the modes per item they were built for; items
   int fft_plan;                 // radix-order variant of the x and z transform plans (0, 1)
   int zf_nlo;                   // the z forward writes only the nonlinear terms (the
                                 // column kernel assembles the right-hand sides)
@@ -241,10 +241,17 @@ int dg_col_step_dev(dg_handle *h, int rk_step, bool rd);
 size_t dg_col_smem(const dg_handle *h, int mt);
 bool dg_col_th_to_rhs(const dg_handle *h, int n);
 int dg_col_mt_eff(const dg_handle *h);  // modes per CTA the column kernel runs h with
+// launch sizes of a column-kernel launch (one case or a server group)
+struct dg_col_launch {
+  int mt, thr, grid;      // modes per item, threads per CTA, CTAs (persistent)
+  int tile, lp, nseg;     // stage sizes: the largest case's
+  int nwork;              // work items
+  size_t smem;
+};
 int dg_col_batch_build(dg_handle *const *hs, int n, int want_mt, std::vector<unsigned char> &cases,
-                       std::vector<int4> &work, int *mt_out, int *thr_out, size_t *smem_out);
-int dg_col_batch_launch(cudaStream_t st, int mt, int thr, size_t smem, const void *dev_cases,
-                        const int4 *dev_work, int nwork, int rk_step);
+                       std::vector<int4> &work, dg_col_launch *cl);
+int dg_col_batch_launch(cudaStream_t st, const dg_col_launch &cl, const void *dev_cases,
+                        const int4 *dev_work, int rk_step);
 
 #define DG_CASE_N(N) \
   case N:            \
@@ -293,6 +300,21 @@ __device__ __forceinline__ void dg_tma_load_2d(void *dst, const CUtensorMap *map
       " [%0], [%1, {%2, %3}], [%4];" ::"r"(dg_smem_addr(dst)),
       "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(dg_smem_addr(bar))
       : "memory");
+}
+// 1-D bulk copy (no multicast) of `bytes` from global to shared memory:
+// both addresses 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void dg_bulk_load(void *dst, const void *src, unsigned bytes,
+                                             unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          dg_smem_addr(dst)),
+      "l"(reinterpret_cast<unsigned long long>(src)), "r"(bytes), "r"(dg_smem_addr(bar))
+      : "memory");
+}
+// orders this thread's generic-proxy shared-memory accesses before later
+// bulk copies (async proxy) into the same shared memory
+__device__ __forceinline__ void dg_fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 // true once phase `parity` of the barrier completed; false after `spin` polls
 __device__ __forceinline__ bool dg_mbar_wait(unsigned long long *bar, unsigned parity,

@@ -97,8 +97,7 @@ struct Group {
   int cmt = 0;                     // the members' modes per column CTA (all the same)
   void *d_cases = nullptr;         // the column kernel's case table
   int4 *d_work = nullptr;          // and its work list
-  int nwork = 0, mt = 0, thr = 0;
-  size_t smem = 0;
+  dg_col_launch cl = {};           // the column launch's sizes
   cudaGraphExec_t exec = nullptr;
   long long gkernels = 0;
   std::deque<InFlight> inflight;
@@ -504,7 +503,7 @@ struct GroupedLoop {
         DG_CUDA(cudaEventRecord(g.ev_m[c], h->st));
         DG_CUDA(cudaStreamWaitEvent(g.gs, g.ev_m[c], 0));
       }
-      DG_TRY(dg_col_batch_launch(g.gs, g.mt, g.thr, g.smem, g.d_cases, g.d_work, g.nwork, rk));
+      DG_TRY(dg_col_batch_launch(g.gs, g.cl, g.d_cases, g.d_work, rk));
       DG_CUDA(cudaEventRecord(g.ev_col, g.gs));
       for (Active *a : g.m) {
         dg_handle *h = a->h;
@@ -542,13 +541,11 @@ struct GroupedLoop {
     {
       std::vector<unsigned char> tab;
       std::vector<int4> work;
-      DG_TRY(dg_col_batch_build(hs.data(), (int)hs.size(), want, tab, work, &g.mt, &g.thr,
-                                &g.smem));
+      DG_TRY(dg_col_batch_build(hs.data(), (int)hs.size(), want, tab, work, &g.cl));
       DG_CUDA(cudaMalloc(&g.d_cases, tab.size()));
       // on the group's stream (non-blocking: a legacy-stream copy would not be
       // ordered before the graph launches), finished before tab goes away
       DG_CUDA(cudaMemcpyAsync(g.d_cases, tab.data(), tab.size(), cudaMemcpyHostToDevice, g.gs));
-      g.nwork = (int)work.size();
       DG_CUDA(cudaMalloc((void **)&g.d_work, sizeof(int4) * work.size()));
       DG_CUDA(cudaMemcpyAsync(g.d_work, work.data(), sizeof(int4) * work.size(),
                               cudaMemcpyHostToDevice, g.gs));

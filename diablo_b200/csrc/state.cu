@@ -206,8 +206,9 @@ extern "C" int64_t dg_state_bytes(const dg_params *p) {
   if (!per) {
     const int64_t hsz = planes * p->nz * nkxp;
     b += 16 * ns + 8 * 2 * ns;                              // gphi, rem_a, rem_rb
-    b += 8 * 3 * (3 + DG_MAX_TH) * 5 * L + 8 * nf * 8 * L;  // cn_tab, cn_rows
-    b += 8 * 8 * L;                                          // rowc
+    const int64_t LP = (L + 1) / 2 * 2;                     // 16-byte table rows
+    b += 8 * 3 * (3 + DG_MAX_TH) * 5 * LP + 8 * nf * 8 * L; // cn_tab, cn_rows
+    b += 8 * 8 * LP;                                         // rowc
     b += 16 * hsz * nf + 16 * hsz * 2 * nf;                 // H, G
     int64_t w = 8 * L * p->nz * p->nx * (nf > 3 ? nf : 3);
     if (w < 8 * 8 * L) w = 8 * 8 * L;
@@ -393,7 +394,7 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
     DG_TRY(dalloc(h, &h->gphi, ns));
     DG_TRY(dalloc(h, &h->rem_a, ns));
     DG_TRY(dalloc(h, &h->rem_rb, ns));
-    DG_TRY(dalloc(h, &h->cn_tab, (size_t)3 * (3 + DG_MAX_TH) * 5 * L));
+    DG_TRY(dalloc(h, &h->cn_tab, (size_t)3 * (3 + DG_MAX_TH) * 5 * ((L + 1) / 2 * 2)));
     const size_t hsz = (size_t)h->nplanes * h->NZ * h->nkxp;
     DG_TRY(dalloc(h, &h->H, hsz * h->nf));
     DG_TRY(dalloc(h, &h->G, hsz * 2 * h->nf));

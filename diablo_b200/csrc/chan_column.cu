@@ -47,9 +47,6 @@
 #include <string.h>
 
 #include <algorithm>
-#include <map>
-#include <mutex>
-#include <tuple>
 #include <vector>
 
 #include "dg_internal.cuh"
@@ -71,12 +68,13 @@ struct ColConst {
 // Everything the column stage of one case needs, in device memory (tensor
 // maps first: 64-byte aligned).  Maps are 2-D over [plane][2 ss doubles].
 struct ColCase {
-  CUtensorMap map_cu[3 + DG_MAX_TH], map_nl[3 + DG_MAX_TH], map_cf[3 + DG_MAX_TH];
-  CUtensorMap map_cp;
+  CUtensorMap map_cu[3 + DG_MAX_TH];
   ColConst C;
   const double *dscal, *tab, *kxv, *kzv, *rowc;
+  const double2 *cp;
   const double2 *cu[3 + DG_MAX_TH];
-  double2 *cf[3 + DG_MAX_TH], *out[3 + DG_MAX_TH];  // out: the rhs arrays
+  const double2 *nl[3 + DG_MAX_TH];  // the z forward's NL terms (the rhs arrays)
+  double2 *cf[3 + DG_MAX_TH], *out[3 + DG_MAX_TH];
   int *err;
   int by, nbox, nseg;
 };
@@ -134,6 +132,7 @@ __device__ __forceinline__ FieldCoef field_coef(const ColConst &C, const double 
 // at row j, mode mg (offset o): u, um, up = CU at j, j-1, j+1; nlv = NL;
 // old = CF_old; p0, pm = CP at j, j-1.  RC: the field's grid-factor rows in
 // shared memory, row stride ld: rows 0, 1 (U1, U3, TH) or 2, 3, 4, 5 (U2).
+template <int FK>
 __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, int f, int j,
                                         long o, bool mean, double KX, double KZ, double kk,
                                         const double *RC, int ld, double2 u, double2 um, double2 up,
@@ -142,7 +141,7 @@ __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, i
   const ColConst &C = cc.C;
   const int nth = C.nth;
   const long ss = C.ss;
-  if (f == 0 || f == 2) {
+  if constexpr (FK == 0) {
     fv = make_double2(-k.NU * kk * u.x, -k.NU * kk * u.y);
     if (C.i_ro != 0.0) {
       const double2 uo = cc.cu[2 - f][o];
@@ -173,7 +172,7 @@ __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, i
     const double cup = k.aaU * RC[0 * ld + j], cdn = k.aaU * RC[1 * ld + j];
     r.x += cup * (up.x - u.x) - cdn * (u.x - um.x);
     r.y += cup * (up.y - u.y) - cdn * (u.y - um.y);
-  } else if (f == 1) {
+  } else if constexpr (FK == 1) {
     fv = make_double2(-k.NU * kk * u.x, -k.NU * kk * u.y);
     if (!mean) {
       const double dyfj = RC[3 * ld + j], dyfm = RC[3 * ld + j - 1];
@@ -219,129 +218,158 @@ __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, i
   }
 }
 
-// Launch-wide sizes: a stage holds the largest item of the work list.
+// Launch-wide sizes: the largest item of the work list sets the layout.
 struct ColLaunch {
-  int tile;   // double2 per input tile (nbox * by * MT of the largest case)
+  int tile;   // double2 per tile (nbox * by * MT of the largest case)
   int lp;     // table row length (the largest case's NY + 2, rounded up to even)
   int nseg;   // segments per column (the largest case)
-  int nwork;  // work items
+  int nwork;  // work items (CTAs)
 };
 
-// A stage (128-byte aligned): the tiles CU, NL (which then holds g, e and x
-// of the recurrences), CF_old, CP [tile] double2; the CN table rows TB
-// [5][lp] (a, 1/b, f = -c/b, kind, BC value); the field's grid factors RC
-// [4][lp].  After the two stages, once per CTA: SV [nseg][MT] double2 (per
-// segment and mode values, then carries), SP [nseg] (per segment products),
-// the stages' two mbarriers.
-__host__ __device__ inline size_t col_stage_bytes(int tile, int lp) {
-  const size_t b = sizeof(double2) * 4 * (size_t)tile + sizeof(double) * 9 * (size_t)lp;
-  return (b + 127) / 128 * 128;
-}
-
+// Shared memory of one CTA (128-byte aligned): the CU tile and the R tile
+// (the right-hand side, then g, e and x of the recurrences) [tile] double2;
+// the CN table rows TB [5][lp] (a, 1/b, f = -c/b, kind, BC value); the
+// field's grid factors RC [4][lp]; per (segment, mode) values SV [nseg][MT]
+// double2 (then carries); per segment products SP [nseg]; the modes'
+// wavenumbers and k^2 (to the power BETA) KW [3][MT]; the mbarrier.
 size_t col_smem_l(const ColLaunch &P, int mt) {
-  return 2 * col_stage_bytes(P.tile, P.lp) + sizeof(double2) * (size_t)P.nseg * mt +
-         sizeof(double) * (size_t)P.nseg + 16 + 128;
+  return sizeof(double2) * (2 * (size_t)P.tile + (size_t)P.nseg * mt) +
+         sizeof(double) * (9 * (size_t)P.lp + (size_t)P.nseg + 3 * (size_t)mt) + 8 + 128;
 }
 
-// One thread fetches work item w into a stage: the field's tiles by bulk
-// tensor copies, its table and grid-factor rows by bulk copies, all on the
-// stage's mbarrier (extra_tx: 0, or 16 in the wait test, where the barrier
-// then never completes).
-template <int MT>
-__device__ __forceinline__ void col_issue(const ColCase &cc, int4 w, int rk_step,
-                                          const ColLaunch &P, unsigned char *stage,
-                                          unsigned long long *bar, unsigned extra_tx) {
-  const int f = w.z;
-  const int L = cc.C.NY + 2, LP = (L + 1) & ~1;
-  const int ctile = cc.nbox * cc.by * MT;
-  const bool vel = f < 3, old_cf = rk_step > 1;
-  double2 *CUt = reinterpret_cast<double2 *>(stage);
-  double2 *NLt = CUt + P.tile, *CFt = NLt + P.tile, *CPt = CFt + P.tile;
-  double *TB = reinterpret_cast<double *>(CPt + P.tile);
-  double *RC = TB + 5 * P.lp;
-  const unsigned ntiles = 2u + (old_cf ? 1u : 0u) + (vel ? 1u : 0u);
-  const int nrc = (f == 1) ? 4 : 2;  // grid-factor rows 2..5 (U2) or 0..1
-  dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * ctile) * ntiles +
-                             (unsigned)(sizeof(double) * (5 + nrc) * LP) + extra_tx);
-  // columns beyond ss and planes beyond L arrive as zeros
-  for (int q = 0; q < cc.nbox; q++) {
-    const long d = (long)q * cc.by * MT;
-    const int x = 2 * w.y * MT, y = q * cc.by;
-    dg_tma_load_2d(CUt + d, &cc.map_cu[f], x, y, bar);
-    dg_tma_load_2d(NLt + d, &cc.map_nl[f], x, y, bar);
-    if (old_cf) dg_tma_load_2d(CFt + d, &cc.map_cf[f], x, y, bar);
-    if (vel) dg_tma_load_2d(CPt + d, &cc.map_cp, x, y, bar);
+// The right-hand side of field f (kind FK: 0 U1/U3, 1 U2, 2 scalar) for the
+// CTA's rows lo..hi: one element (row, mode) per step of a flat loop over
+// all threads; NL, CF_old and CP are read from global memory (each element
+// once, coalesced), CU from the staged tile (its neighbours in y too).
+template <int MT, int FK>
+__device__ __forceinline__ void rhs_tile(const ColCase &cc, const FieldCoef &k, int rk_step,
+                                         long m0, int f, int mt, const double2 *CUt,
+                                         double2 *Rt, const double *RC, int LP,
+                                         const double *KW) {
+  const ColConst &C = cc.C;
+  const long ss = C.ss;
+  const bool old_cf = rk_step > 1;
+  const double2 *nlp = cc.nl[f];
+  const double2 *cfo = cc.cf[f];
+  double2 *cff = cc.cf[f];
+  const int nthr = blockDim.x;
+#pragma unroll 2
+  for (int i = k.lo * MT + (int)threadIdx.x; i < (k.hi + 1) * MT; i += nthr) {
+    const int j = i / MT, m = i - j * MT;
+    if (m >= mt) continue;
+    const long mg = m0 + m;
+    const long o = (long)j * ss + mg;
+    const double2 nlv = nlp[o];
+    const double2 old = old_cf ? cfo[o] : z2();
+    const double2 p0 = (FK < 2) ? cc.cp[o] : z2();
+    const double2 pm = (FK == 1) ? cc.cp[o - ss] : z2();
+    const double KX = KW[m], KZ = KW[MT + m], kk = KW[2 * MT + m];
+    double2 fv, rr;
+    rhs_row<FK>(cc, k, f, j, o, mg == 0, KX, KZ, kk, RC, LP, CUt[i], CUt[i - MT], CUt[i + MT],
+                nlv, old, p0, pm, fv, rr);
+    cff[o] = fv;
+    Rt[i] = rr;
   }
-  dg_bulk_load(TB, cc.tab + ((long)(rk_step - 1) * (3 + DG_MAX_TH) + f) * 5 * LP,
-               (unsigned)(sizeof(double) * 5 * LP), bar);
-  dg_bulk_load(RC, cc.rowc + (long)(f == 1 ? 2 : 0) * LP, (unsigned)(sizeof(double) * nrc * LP),
-               bar);
 }
 
-// The column stage of field f for modes m0 .. m0+MT-1 of one case, from a
-// stage whose copies have landed.
+// The column stage of field f for modes m0 .. m0+MT-1 of one case.
 template <int MT>
-__device__ __forceinline__ void col_item(const ColCase &cc, int rk_step, long m0, int f,
-                                         const ColLaunch &P, unsigned char *stage, double2 *SV,
-                                         double *SP) {
+__device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0, int f,
+                                         const ColLaunch &P, long spin, unsigned extra_tx,
+                                         unsigned char *sbase) {
   const ColConst &C = cc.C;
   const int NY = C.NY, L = NY + 2, LP = (L + 1) & ~1;  // the case's own row length
   const int nseg = cc.nseg;
   const long ss = C.ss;
   const int mt = (int)((ss - m0) < MT ? (ss - m0) : MT);
-  const bool old_cf = rk_step > 1;
-  double2 *CUt = reinterpret_cast<double2 *>(stage);
-  double2 *NLt = CUt + P.tile, *CFt = NLt + P.tile, *CPt = CFt + P.tile;
-  const double *TB = reinterpret_cast<const double *>(CPt + P.tile);
-  const double *RC = TB + 5 * P.lp;  // the slots are sized for the largest case
+  double2 *CUt = reinterpret_cast<double2 *>(sbase);
+  double2 *Rt = CUt + P.tile;
+  double *TB = reinterpret_cast<double *>(Rt + P.tile);
+  double *RC = TB + 5 * P.lp;  // the slots are sized for the largest case
+  double2 *SV = reinterpret_cast<double2 *>(RC + 4 * P.lp);
+  double *SP = reinterpret_cast<double *>(SV + P.nseg * MT);
+  double *KW = SP + P.nseg;
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(KW + 3 * MT);
   const int tid = threadIdx.x;
+  if (tid < MT) {
+    const long mg = (m0 + tid < ss) ? m0 + tid : 0;
+    const double KX = cc.kxv[mg % C.nkxp], KZ = cc.kzv[mg / C.nkxp];
+    const double k2 = KX * KX + KZ * KZ;
+    KW[tid] = KX;
+    KW[MT + tid] = KZ;
+    KW[2 * MT + tid] = (C.beta == 1.0) ? k2 : pow(k2, C.beta);
+  }
+
+  // ---- 0. the CU tile by bulk tensor copies, the table and grid-factor rows
+  // by bulk copies, all on one mbarrier with a bounded wait
+  if (tid == 0) dg_mbar_init(bar, 1);
+  __syncthreads();
+  dg_pdl_wait();  // NL comes from the z-forward kernel
+  if (tid == 0) {
+    const int ctile = cc.nbox * cc.by * MT;
+    const int nrc = (f == 1) ? 4 : 2;  // grid-factor rows 2..5 (U2) or 0..1
+    // extra_tx is 0 except in the wait test, where the barrier then never completes
+    dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * ctile) +
+                               (unsigned)(sizeof(double) * (5 + nrc) * LP) + extra_tx);
+    // columns beyond ss and planes beyond L arrive as zeros
+    for (int q = 0; q < cc.nbox; q++)
+      dg_tma_load_2d(CUt + (long)q * cc.by * MT, &cc.map_cu[f], (int)(2 * m0), q * cc.by, bar);
+    dg_bulk_load(TB, cc.tab + ((long)(rk_step - 1) * (3 + DG_MAX_TH) + f) * 5 * LP,
+                 (unsigned)(sizeof(double) * 5 * LP), bar);
+    dg_bulk_load(RC, cc.rowc + (long)(f == 1 ? 2 : 0) * LP,
+                 (unsigned)(sizeof(double) * nrc * LP), bar);
+  }
+  const bool landed = dg_mbar_wait(bar, 0, spin);
+  if (__syncthreads_or(!landed)) {
+    if (tid == 0) {
+      atomicExch(cc.err + 1, 1);
+      dg_mbar_wait(bar, 0, spin);  // the copies in flight get one more bounded wait
+    }
+    return;
+  }
+
+  // ---- 1. explicit terms, CF and the right-hand side of rows lo..hi
+  const FieldCoef k = field_coef(C, cc.dscal, rk_step, f);
+  if (f == 1) rhs_tile<MT, 1>(cc, k, rk_step, m0, f, mt, CUt, Rt, RC, LP, KW);
+  else if (f < 3) rhs_tile<MT, 0>(cc, k, rk_step, m0, f, mt, CUt, Rt, RC, LP, KW);
+  else rhs_tile<MT, 2>(cc, k, rk_step, m0, f, mt, CUt, Rt, RC, LP, KW);
+  __syncthreads();
+
+  // ---- 2. forward recurrence g(j) = r(j) + a(j) g(j-1) over each segment
+  // from zero (one thread per mode and segment); r is R on CN rows, the BC
+  // value (the (0,0) mode's real part) or zero elsewhere; g replaces R
   const int m = tid % MT, s = tid / MT;
   const int j0 = s * SEG_K;
   const int nr = (s < nseg) ? min(SEG_K, L - j0) : 0;  // rows of this thread's segment
   const long mg = m0 + m;
   const bool live = m < mt;
   const bool mean = (mg == 0);
-  const long mgc = live ? mg : 0;
-  const double KX = cc.kxv[mgc % C.nkxp], KZ = cc.kzv[mgc / C.nkxp];
-  const double k2 = KX * KX + KZ * KZ;
-  const double kk = (C.beta == 1.0) ? k2 : pow(k2, C.beta);
-
-  // ---- 1. explicit terms, CF and the right-hand side row by row, and the
-  // forward recurrence g(j) = r(j) + a(j) g(j-1) over the segment from zero;
-  // g replaces NL (each (row, mode) element belongs to one thread)
-  const FieldCoef k = field_coef(C, cc.dscal, rk_step, f);
-  double2 *cff = cc.cf[f];
-  double2 g = z2();
-  double pa = 1.0;
+  {
+    double2 g = z2();
+    double pa = 1.0;
 #pragma unroll
-  for (int q = 0; q < SEG_K; q++) {
-    if (q < nr) {
-      const int j = j0 + q;
-      const int i = j * MT + m;
-      const double kind = TB[3 * LP + j];
-      // a BC row's value goes to the real part of the (0,0) mode only
-      double2 r = make_double2((kind == (double)ROW_BC && mean) ? TB[4 * LP + j] : 0.0, 0.0);
-      if (j >= k.lo && j <= k.hi) {
-        const long o = (long)j * ss + mg;
-        double2 fv, rr;
-        rhs_row(cc, k, f, j, o, mean, KX, KZ, kk, RC, LP, CUt[i], CUt[i - MT], CUt[i + MT],
-                NLt[i], old_cf ? CFt[i] : z2(), CPt[i], CPt[i - MT], fv, rr);
-        if (live) cff[o] = fv;
-        if (kind == (double)ROW_RHS) r = rr;
+    for (int q = 0; q < SEG_K; q++) {
+      if (q < nr) {
+        const int j = j0 + q;
+        const double kind = TB[3 * LP + j];
+        const double2 r = (kind == (double)ROW_RHS)
+                              ? Rt[j * MT + m]
+                              : make_double2((kind == (double)ROW_BC && mean) ? TB[4 * LP + j] : 0.0,
+                                             0.0);
+        const double a = TB[j];
+        g.x = r.x + a * g.x;
+        g.y = r.y + a * g.y;
+        pa = a * pa;
+        Rt[j * MT + m] = g;
       }
-      const double a = TB[j];
-      g.x = r.x + a * g.x;
-      g.y = r.y + a * g.y;
-      pa = a * pa;
-      NLt[i] = g;
+    }
+    if (nr > 0) {
+      SV[s * MT + m] = g;
+      if (m == 0) SP[s] = pa;
     }
   }
-  if (nr > 0) {
-    SV[s * MT + m] = g;
-    if (m == 0) SP[s] = pa;
-  }
   __syncthreads();
-  // ---- 2. the segment ends carried down the column, one lane per mode
+  // ---- 3. the segment ends carried down the column, one lane per mode
   if (tid < MT) {
     double2 G = z2();
     for (int t = 0; t < nseg; t++) {
@@ -352,7 +380,7 @@ __device__ __forceinline__ void col_item(const ColCase &cc, int rk_step, long m0
     }
   }
   __syncthreads();
-  // ---- 3. g = local + product x carry, e = g / b; then the backward
+  // ---- 4. g = local + product x carry, e = g / b; then the backward
   // recurrence x(j) = e(j) + f(j) x(j+1) over the segment (rows >= wlo)
   const int wlo = (f >= 3) ? pick(C.JSt, f - 3) - 1 : 1;
   const int qb = wlo > j0 ? wlo - j0 : 0;  // first row of the segment to solve
@@ -365,9 +393,9 @@ __device__ __forceinline__ void col_item(const ColCase &cc, int rk_step, long m0
       if (q < nr) {
         const int j = j0 + q;
         pi = TB[j] * pi;
-        const double2 gv = NLt[j * MT + m];
+        const double2 gv = Rt[j * MT + m];
         const double rb = TB[LP + j];
-        NLt[j * MT + m] = make_double2((gv.x + pi * c.x) * rb, (gv.y + pi * c.y) * rb);
+        Rt[j * MT + m] = make_double2((gv.x + pi * c.x) * rb, (gv.y + pi * c.y) * rb);
       }
     }
     double2 xl = z2();
@@ -377,21 +405,21 @@ __device__ __forceinline__ void col_item(const ColCase &cc, int rk_step, long m0
       if (q < nr && q >= qb) {
         const int j = j0 + q;
         const double fj = TB[2 * LP + j];
-        const double2 e = NLt[j * MT + m];
+        const double2 e = Rt[j * MT + m];
         xl = make_double2(e.x + fj * xl.x, e.y + fj * xl.y);
         ps = fj * ps;
-        NLt[j * MT + m] = xl;
+        Rt[j * MT + m] = xl;
       }
     }
     // each thread overwrites only its own SV entry, read above by itself;
-    // SP was last read in step 2, before the barrier
+    // SP was last read in step 3, before the barrier
     if (solves) {
       SV[s * MT + m] = xl;
       if (m == 0) SP[s] = ps;
     }
   }
   __syncthreads();
-  // ---- 4. the segment starts carried up the column, one lane per mode
+  // ---- 5. the segment starts carried up the column, one lane per mode
   const int sw = wlo / SEG_K;  // lowest segment with rows to solve
   if (tid < MT) {
     double2 X = z2();
@@ -403,7 +431,7 @@ __device__ __forceinline__ void col_item(const ColCase &cc, int rk_step, long m0
     }
   }
   __syncthreads();
-  // ---- 5. x = local + product x carry: the post-CN field, rows >= wlo
+  // ---- 6. x = local + product x carry: the post-CN field, rows >= wlo
   if (solves && live) {
     const double2 c = SV[s * MT + m];
     double2 *dst = cc.out[f];
@@ -413,71 +441,24 @@ __device__ __forceinline__ void col_item(const ColCase &cc, int rk_step, long m0
       if (q < nr && q >= qb) {
         const int j = j0 + q;
         p2 = TB[2 * LP + j] * p2;
-        const double2 xl = NLt[j * MT + m];
+        const double2 xl = Rt[j * MT + m];
         dst[(long)j * ss + mg] = make_double2(xl.x + p2 * c.x, xl.y + p2 * c.y);
       }
     }
   }
 }
 
-// The column kernel, persistent: CTA b takes work items b, b + G, b + 2G, ...
-// (G = gridDim.x) of the case table (every case at substep rk_step with MT
-// modes per CTA), through two stages: item i + 1's copies are in flight
-// while item i is computed.
+// The column kernel: CTA b takes work[b] = (case, mode tile, field) from
+// the case table (every case at substep rk_step with MT modes per CTA).
 template <int MT>
-__global__ void __launch_bounds__(COL_MAX_THR, 2) k_col_cn(const ColCase *__restrict__ cases,
+__global__ void __launch_bounds__(COL_MAX_THR, 3) k_col_cn(const ColCase *__restrict__ cases,
                                                        const int4 *__restrict__ work,
                                                        ColLaunch P, int rk_step, long spin,
                                                        unsigned extra_tx) {
   extern __shared__ __align__(128) unsigned char cs_raw[];
-  unsigned char *base = cs_raw + ((128u - (dg_smem_addr(cs_raw) & 127u)) & 127u);
-  const size_t sb = col_stage_bytes(P.tile, P.lp);
-  unsigned char *stg[2] = {base, base + sb};
-  double2 *SV = reinterpret_cast<double2 *>(base + 2 * sb);
-  double *SP = reinterpret_cast<double *>(SV + P.nseg * MT);
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(SP + P.nseg);
-  const int tid = threadIdx.x;
-  const int G = gridDim.x;
-  if (tid == 0) {
-    dg_mbar_init(bar, 1);
-    dg_mbar_init(bar + 1, 1);
-  }
-  __syncthreads();
-  dg_pdl_wait();  // NL comes from the z-forward kernel
-  if (tid == 0) {
-    for (int q = 0; q < 2; q++) {
-      const int w = blockIdx.x + q * G;
-      if (w < P.nwork) {
-        const int4 wi = work[w];
-        col_issue<MT>(cases[wi.x], wi, rk_step, P, stg[q], bar + q, extra_tx);
-      }
-    }
-  }
-  int it = 0;
-  for (int w = blockIdx.x; w < P.nwork; w += G, it++) {
-    const int st = it & 1;
-    const unsigned par = (unsigned)(it >> 1) & 1u;
-    const int4 wi = work[w];
-    const bool landed = dg_mbar_wait(bar + st, par, spin);
-    if (__syncthreads_or(!landed)) {
-      if (tid == 0) {
-        atomicExch(cases[wi.x].err + 1, 1);
-        // the copies in flight get one more bounded wait each
-        dg_mbar_wait(bar + st, par, spin);
-        if (w + G < P.nwork) dg_mbar_wait(bar + (st ^ 1), (unsigned)((it + 1) >> 1) & 1u, spin);
-      }
-      return;
-    }
-    col_item<MT>(cases[wi.x], rk_step, (long)wi.y * MT, wi.z, P, stg[st], SV, SP);
-    // the stage is free again: order this thread's accesses to it before the
-    // copies of the item after next
-    dg_fence_proxy_async();
-    __syncthreads();
-    if (tid == 0 && w + 2 * G < P.nwork) {
-      const int4 wn = work[w + 2 * G];
-      col_issue<MT>(cases[wn.x], wn, rk_step, P, stg[st], bar + st, extra_tx);
-    }
-  }
+  unsigned char *sbase = cs_raw + ((128u - (dg_smem_addr(cs_raw) & 127u)) & 127u);
+  const int4 w = work[blockIdx.x];
+  col_body<MT>(cases[w.x], rk_step, (long)w.y * MT, w.z, P, spin, extra_tx, sbase);
 }
 
 ColConst make_col_const(const dg_handle *h) {
@@ -560,26 +541,24 @@ static int col_threads(const dg_handle *h, int mt) {
 size_t dg_col_smem(const dg_handle *h, int mt) { return col_smem_l(col_sizes(h, mt), mt); }
 
 // The case description of handle h for `mt` modes per CTA (builds the
-// tensor maps of its CU, rhs and CF arrays and CP for that tile width).
+// tensor maps of its CU arrays for that tile width).
 static int fill_case(dg_handle *h, int mt, ColCase *cc) {
   const int L = h->NY + 2;
   int by = 0, nbox = 0, nseg = 0;
   col_geometry(h, &by, &nbox, &nseg);
   memset(cc, 0, sizeof(*cc));
-  for (int f = 0; f < h->nf; f++) {
+  for (int f = 0; f < h->nf; f++)
     DG_TRY(dg_tmap_planes(h->cu[f], h->ss, L, mt, by, &cc->map_cu[f]));
-    DG_TRY(dg_tmap_planes(h->rhs[f], h->ss, L, mt, by, &cc->map_nl[f]));
-    DG_TRY(dg_tmap_planes(h->cf[f], h->ss, L, mt, by, &cc->map_cf[f]));
-  }
-  DG_TRY(dg_tmap_planes(h->cp, h->ss, L, mt, by, &cc->map_cp));
   cc->C = make_col_const(h);
   cc->dscal = h->dscal;
   cc->tab = h->cn_tab;
   cc->kxv = h->kx;
   cc->kzv = h->kz;
   cc->rowc = h->rowc;
+  cc->cp = h->cp;
   for (int f = 0; f < h->nf; f++) {
     cc->cu[f] = h->cu[f];
+    cc->nl[f] = h->rhs[f];
     cc->cf[f] = h->cf[f];
     cc->out[f] = (f < 3 || dg_col_th_to_rhs(h, f - 3)) ? h->rhs[f] : h->cu[f];
   }
@@ -613,36 +592,6 @@ static void case_work(const dg_handle *h, int c, int mt, std::vector<int4> &work
   const int tiles = dg_cdiv(h->ss, mt);
   for (int f = 0; f < h->nf; f++)
     for (int t = 0; t < tiles; t++) work.push_back(make_int4(c, t, f, 0));
-}
-
-// CTAs of the persistent launch: as many as fit on the device at once (at
-// most one per work item)
-static int col_grid(int mt, int thr, size_t smem, int nwork) {
-  static std::mutex mu;
-  static std::map<std::tuple<int, int, size_t>, int> cache;
-  int per_sm = 0, nsm = 0;
-  {
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = cache.find(std::make_tuple(mt, thr, smem));
-    if (it != cache.end()) {
-      per_sm = it->second;
-    } else {
-      const void *kern = mt == 2 ? (const void *)k_col_cn<2>
-                       : mt == 4 ? (const void *)k_col_cn<4>
-                       : mt == 8 ? (const void *)k_col_cn<8>
-                                 : (const void *)k_col_cn<16>;
-      dg_big_smem(kern);
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, thr, smem) != cudaSuccess ||
-          per_sm < 1)
-        per_sm = 1;
-      cache[std::make_tuple(mt, thr, smem)] = per_sm;
-    }
-  }
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) nsm = 148;
-  const long g = (long)per_sm * nsm;
-  return (int)(g < nwork ? g : nwork);
 }
 
 // The handle's device copy of its one-case table and work list for mt,
@@ -722,7 +671,7 @@ static int col_plan(dg_handle *const *hs, int n, int want, int nwork, dg_col_lau
     return DG_ERR_DIMS;
   }
   r.nwork = nwork;
-  r.grid = col_grid(mt, r.thr, r.smem, nwork);
+  r.grid = nwork;  // one CTA per work item
   *cl = r;
   return DG_OK;
 }

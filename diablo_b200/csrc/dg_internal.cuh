@@ -243,8 +243,8 @@ bool dg_col_th_to_rhs(const dg_handle *h, int n);
 int dg_col_mt_eff(const dg_handle *h);  // modes per CTA the column kernel runs h with
 // launch sizes of a column-kernel launch (one case or a server group)
 struct dg_col_launch {
-  int mt, thr, grid;      // modes per item, threads per CTA, CTAs (persistent)
-  int tile, lp, nseg;     // stage sizes: the largest case's
+  int mt, thr, grid;      // modes per item, threads per CTA, CTAs (one per item)
+  int tile, lp, nseg;     // shared-memory layout: the largest case's
   int nwork;              // work items
   size_t smem;
 };

@@ -102,6 +102,10 @@ struct Group {
   long long gkernels = 0;
   std::deque<InFlight> inflight;
   std::vector<InFlight> pool;
+  // cases placed in the group while its steps were in flight: they join the
+  // members (and the graph) at the next rebuild, so completions of steps
+  // launched before they joined are not counted for them
+  std::vector<Active *> joining;
   bool dirty = true;               // membership changed: rebuild before the next step
   double points = 0;               // mean points per member (grouping by size)
 };
@@ -452,7 +456,7 @@ struct GroupedLoop {
     Group *best = nullptr;
     double bd = 1e30;
     for (auto &g : groups) {
-      if ((int)g->m.size() >= s->group_cases || g->cmt != cmt) continue;
+      if ((int)(g->m.size() + g->joining.size()) >= s->group_cases || g->cmt != cmt) continue;
       const double d = fabs(log(pts(a) / g->points));
       if (d < log(4.0) && d < bd) {
         bd = d;
@@ -463,10 +467,11 @@ struct GroupedLoop {
       best = new_group();
       best->cmt = cmt;
     }
-    best->m.push_back(a);
+    best->joining.push_back(a);
     double sum = 0;
     for (Active *x : best->m) sum += pts(x);
-    best->points = sum / best->m.size();
+    for (Active *x : best->joining) sum += pts(x);
+    best->points = sum / (best->m.size() + best->joining.size());
     best->dirty = true;
   }
 
@@ -651,6 +656,9 @@ struct GroupedLoop {
               k++;
             }
           }
+          // cases placed meanwhile join now, before the rebuild
+          for (Active *a : g.joining) g.m.push_back(a);
+          g.joining.clear();
           if (g.m.empty()) {
             destroy_group(gi);
             continue;

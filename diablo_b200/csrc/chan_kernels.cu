@@ -1318,19 +1318,24 @@ __global__ void k_remdiv_init(int NY, long ss, int nkxp, const double *__restric
 }
 
 // ------------------------------------------------------- column kernels
-// k_rd_col owns MT modes and their whole y-column (REM_DIV_CHAN on its own:
-// the entry point, and the substeps that run COURANT between the CN solves
-// and the projection).  Inputs are staged into shared memory with coalesced
-// loads from all 128 threads; the sequential sweeps then run with one lane
-// per (mode, re/im) part -- the operator is real, so real and imaginary
-// parts are independent systems -- touching only shared memory; results
-// leave with coalesced stores.  The substep's CN solves run in the column
-// kernel of chan_column.cu.
-constexpr int COL_THR = 128;
+// k_rd_col: REM_DIV_CHAN for MT modes and their whole y-columns -- the
+// divergence of the velocity, the solve of the Poisson system for phi
+// (multipliers and reciprocal pivots per mode from k_remdiv_init), the
+// projection and CP += phi / H_BAR.  The solve is the two recurrences of
+// THOMAS_FORWARD / THOMAS_BACKWARD, forward g(j) = r(j) + a(j) g(j-1) and
+// backward phi(j) = e(j) + f(j) phi(j+1) with e = g / b and f = -c / b,
+// split over segments of RD_K rows: one thread per (mode, segment) runs its
+// segment from a zero start keeping the product of the coefficients, one
+// lane per mode carries the segment ends across the column, and each thread
+// adds carry x product to its rows (the same algebra as the sequential
+// sweeps, with the rounding of a different order of the same operations;
+// the segment boundaries depend only on NY).  The divergence and the
+// projection are flat loops over (row, mode) across the CTA; the velocity
+// and CP are read from global memory there (coalesced), the factors by the
+// segment threads.
+constexpr int RD_K = 8;        // rows per segment
+constexpr int RD_MAX_THR = 256;
 
-// REM_DIV_CHAN for MT modes: divergence (parallel) -> forward and backward
-// sweeps (one lane per mode, both parts) -> projection, phi and CP update
-// (parallel).
 // The velocity is read from s1..s3 and written to u1..u3: the same arrays for
 // REM_DIV_CHAN on its own (in place), the rhs arrays holding the column
 // stage's post-CN velocity inside a substep.  In that case the rows the
@@ -1343,193 +1348,216 @@ struct RdCopy {
   int n;
 };
 
+struct RdArgs {
+  int NY, nkxp, JS, JE, rk_step, nseg;
+  long ss;
+  const double *kxv, *kzv, *dy, *dyf, *ra, *rrb, *dscal;
+  const double2 *s1, *s2, *s3;
+  double2 *u1, *u2, *u3, *cp, *phi;
+  RdCopy cpy;
+};
+
+// shared memory: PH [L][MT] double2 (r, g, e, phi), SV [nseg][MT] double2,
+// SP [nseg][MT], UU, IDY, IDYF [L], KXS, KZS [MT]
+size_t rd_smem(int L, int nseg, int mt) {
+  return sizeof(double2) * ((size_t)L * mt + (size_t)nseg * mt) +
+         sizeof(double) * ((size_t)nseg * mt + 3 * (size_t)L + 2 * (size_t)mt);
+}
+
 template <int MT>
-__global__ void __launch_bounds__(COL_THR) k_rd_col(
-    int NY, long ss, int nkxp, int JS, int JE, int rk_step, const double *__restrict__ kxv,
-    const double *__restrict__ kzv, const double *__restrict__ dy, const double *__restrict__ dyf,
-    const double *__restrict__ ra, const double *__restrict__ rrb, const double2 *s1,
-    const double2 *s2, const double2 *s3, double2 *u1, double2 *u2, double2 *u3,
-    double2 *__restrict__ cp, double2 *__restrict__ phi_out, const double *__restrict__ dscal,
-    RdCopy cpy) {
-  extern __shared__ double2 csm[];
-  const int L = NY + 2;
+__global__ void __launch_bounds__(RD_MAX_THR, 3) k_rd_col(RdArgs A) {
+  extern __shared__ double2 rsm[];
+  const int NY = A.NY, L = NY + 2, nseg = A.nseg;
+  const long ss = A.ss;
   const long m0 = (long)blockIdx.x * MT;
   const int mt = (int)((ss - m0) < MT ? (ss - m0) : MT);
-  double2 *GX = csm;                                // [j][MT]: rhs -> g -> phi
-  double *RA = (double *)(GX + (long)L * MT);   // [j][MT]
-  double *RB = RA + (long)L * MT;               // [j][MT]
-  double *UU = RB + (long)L * MT;               // [j] upper diagonal rows 2..NY-1
-  double *IDY = UU + L;                         // [j] 1 / DY(j)
-  double *IDYF = IDY + L;                       // [j] 1 / DYF(j)
-  double *KXS = IDYF + L, *KZS = KXS + MT;      // wavenumbers of the CTA's modes
-  const int tid = threadIdx.x;
+  double2 *PH = rsm;                                // [j][MT]
+  double2 *SV = PH + (long)L * MT;                  // [seg][MT]
+  double *SP = reinterpret_cast<double *>(SV + (long)nseg * MT);  // [seg][MT]
+  double *UU = SP + (long)nseg * MT;                // [j] upper diagonal rows 2..NY-1
+  double *IDY = UU + L;                             // [j] 1 / DY(j)
+  double *IDYF = IDY + L;                           // [j] 1 / DYF(j)
+  double *KXS = IDYF + L, *KZS = KXS + MT;          // wavenumbers of the CTA's modes
+  const int tid = threadIdx.x, nthr = blockDim.x;
   if (tid < MT) {
     const int mi = (int)(m0 + tid) < (int)ss ? (int)(m0 + tid) : 0;
-    KXS[tid] = kxv[mi % nkxp];
-    KZS[tid] = kzv[mi / nkxp];
+    KXS[tid] = A.kxv[mi % A.nkxp];
+    KZS[tid] = A.kzv[mi / A.nkxp];
   }
-  for (int j = tid; j < L; j += COL_THR) {
-    UU[j] = (j >= 2 && j < NY) ? 1. / (dy[j + 1] * dyf[j]) : 0.0;
-    IDY[j] = (j >= 1) ? 1. / dy[j] : 0.0;
-    IDYF[j] = (j >= 1 && j <= NY) ? 1. / dyf[j] : 0.0;
+  for (int j = tid; j < L; j += nthr) {
+    UU[j] = (j >= 2 && j < NY) ? 1. / (A.dy[j + 1] * A.dyf[j]) : 0.0;
+    IDY[j] = (j >= 1) ? 1. / A.dy[j] : 0.0;
+    IDYF[j] = (j >= 1 && j <= NY) ? 1. / A.dyf[j] : 0.0;
   }
   dg_pdl_wait();  // the velocity comes from the CN solve
   __syncthreads();
-  for (int base = 0; base < L * MT; base += 4 * COL_THR) {
-    double2 a1[4], a3[4], b2[4], b2p[4];
-    double av[4], bv[4];
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const int i = base + u * COL_THR + tid;
-      const int m = i % MT, j = i / MT;
-      const bool ok = i < L * MT && m < mt && j >= 1 && j <= NY;
-      const bool in = ok && j >= 2 && j < NY;
+  // ---- 1. the divergence (rows 2..NY-1; rows 1 and NY have a zero
+  // right-hand side)
+  for (int i = MT + tid; i < (NY + 1) * MT; i += nthr) {
+    const int j = i / MT, m = i - j * MT;
+    double2 r = make_double2(0.0, 0.0);
+    if (m < mt && j >= 2 && j < NY) {
       const long o = (long)j * ss + m0 + m;
-      av[u] = ok ? ra[o] : 0.0;
-      bv[u] = ok ? rrb[o] : 0.0;
-      a1[u] = in ? s1[o] : make_double2(0.0, 0.0);
-      a3[u] = in ? s3[o] : make_double2(0.0, 0.0);
-      b2[u] = in ? s2[o] : make_double2(0.0, 0.0);
-      b2p[u] = in ? s2[o + ss] : make_double2(0.0, 0.0);
+      const double2 a1 = A.s1[o], a3 = A.s3[o], b2 = A.s2[o], b2p = A.s2[o + ss];
+      const double KX = KXS[m], KZ = KZS[m];
+      const double id = IDYF[j];
+      r.x = (-KX * a1.y) + (b2p.x - b2.x) * id + (-KZ * a3.y);
+      r.y = (KX * a1.x) + (b2p.y - b2.y) * id + (KZ * a3.x);
     }
+    PH[i] = r;
+  }
+  __syncthreads();
+  // ---- 2. forward recurrence over each segment of rows 1..NY from zero
+  // (g(1) = 0: the multiplier of row 1 is taken as 0)
+  const int m = tid % MT, s = tid / MT;
+  const int j0 = 1 + s * RD_K;
+  const int nr = (s < nseg) ? min(RD_K, NY + 1 - j0) : 0;
+  const bool live = m < mt;
+  const long mg = live ? m0 + m : m0;
+  double a[RD_K], rb[RD_K];
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const int i = base + u * COL_THR + tid;
-      if (i >= L * MT) continue;
-      const int m = i % MT, j = i / MT;
-      const long mg = m0 + m;
-      double2 r = make_double2(0.0, 0.0);
-      if (m < mt && j >= 2 && j < NY) {
-        const double KX = KXS[m], KZ = KZS[m];
-        const double id = IDYF[j];
-        r.x = (-KX * a1[u].y) + (b2p[u].x - b2[u].x) * id + (-KZ * a3[u].y);
-        r.y = (KX * a1[u].x) + (b2p[u].y - b2[u].y) * id + (KZ * a3[u].x);
+  for (int q = 0; q < RD_K; q++) {
+    const long o = (long)(j0 + q) * ss + mg;
+    a[q] = (q < nr && j0 + q >= 2) ? A.ra[o] : 0.0;
+    rb[q] = (q < nr) ? A.rrb[o] : 0.0;
+  }
+  {
+    double2 g = make_double2(0.0, 0.0);
+    double pa = 1.0;
+#pragma unroll
+    for (int q = 0; q < RD_K; q++) {
+      if (q < nr) {
+        const double2 r = PH[(j0 + q) * MT + m];
+        g.x = r.x + a[q] * g.x;
+        g.y = r.y + a[q] * g.y;
+        pa = a[q] * pa;
+        PH[(j0 + q) * MT + m] = g;
       }
-      GX[i] = r;
-      RA[i] = av[u];
-      RB[i] = bv[u];
+    }
+    if (nr > 0) {
+      SV[s * MT + m] = g;
+      SP[s * MT + m] = pa;
     }
   }
   __syncthreads();
   if (tid < MT) {
-    // one lane per mode: the real and imaginary recurrences interleaved
-    const int m = tid;
-    const bool mean = (m0 + m == 0);
-    double2 *x = GX + m;
-    constexpr int B = 8;
-    double2 g = make_double2(0.0, 0.0);  // row 1 has a zero right-hand side
-    x[1 * MT] = g;
-    for (int j0 = 2; j0 <= NY; j0 += B) {
-      double2 r[B];
-      double a[B];
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        const int j = j0 + q <= NY ? j0 + q : NY;
-        r[q] = x[j * MT];
-        a[q] = RA[j * MT + m];
-      }
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        if (j0 + q <= NY) {
-          g.x = r[q].x + a[q] * g.x;
-          g.y = r[q].y + a[q] * g.y;
-          r[q] = g;
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < B; q++)
-        if (j0 + q <= NY) x[(j0 + q) * MT] = r[q];
+    double2 G = make_double2(0.0, 0.0);
+    for (int t = 0; t < nseg; t++) {
+      const double2 e = SV[t * MT + tid];
+      const double p = SP[t * MT + tid];
+      SV[t * MT + tid] = G;
+      G = make_double2(e.x + p * G.x, e.y + p * G.y);
     }
-    const double rbn = RB[NY * MT + m];
-    double2 ph = make_double2(g.x * rbn, g.y * rbn);
-    x[NY * MT] = ph;
-    for (int j1 = NY - 1; j1 >= 2; j1 -= B) {
-      double2 gq[B];
-      double uq[B], bq[B];
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        const int j = j1 - q >= 2 ? j1 - q : 2;
-        gq[q] = x[j * MT];
-        uq[q] = UU[j];
-        bq[q] = RB[j * MT + m];
-      }
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        if (j1 - q >= 2) {
-          ph.x = (gq[q].x - uq[q] * ph.x) * bq[q];
-          ph.y = (gq[q].y - uq[q] * ph.y) * bq[q];
-          gq[q] = ph;
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < B; q++)
-        if (j1 - q >= 2) x[(j1 - q) * MT] = gq[q];
-    }
-    const double u1r = mean ? 0.0 : -1.0;
-    const double2 x1 = x[1 * MT];
-    const double rb1 = RB[1 * MT + m];
-    ph = make_double2((x1.x - u1r * ph.x) * rb1, (x1.y - u1r * ph.y) * rb1);
-    x[1 * MT] = ph;
   }
   __syncthreads();
-  const double ihh = (rk_step > 0) ? 1.0 / dscal[1 + rk_step] : 1.0;
-  for (int base = 0; base < L * MT; base += 4 * COL_THR) {
-    double2 a1[4], a3[4], b2[4], pc[4];
+  // ---- 3. g = local + product x carry, e = g / b; the backward recurrence
+  // phi(j) = e(j) + f(j) phi(j+1), f = -c / b (row NY: f = 0; row 1: the
+  // upper coefficient of APPLY_BC_REM_DIV_MPI, 0 for the mean mode, -1
+  // otherwise)
+  const bool mean = live && (m0 + m == 0);
+  {
+    const double2 c = (nr > 0) ? SV[s * MT + m] : make_double2(0.0, 0.0);
+    double pi = 1.0;
+    double2 e[RD_K];
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const int i = base + u * COL_THR + tid;
-      const int m = i % MT, j = i / MT;
-      const bool ok = i < L * MT && m < mt && j >= 1 && j <= NY;
-      const long o = (long)j * ss + m0 + m;
-      a1[u] = ok ? s1[o] : make_double2(0.0, 0.0);
-      a3[u] = ok ? s3[o] : make_double2(0.0, 0.0);
-      b2[u] = (ok && j >= 2) ? s2[o] : make_double2(0.0, 0.0);
-      pc[u] = (ok && rk_step > 0 && j >= JS && j <= JE) ? cp[o] : make_double2(0.0, 0.0);
-    }
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const int i = base + u * COL_THR + tid;
-      const int m = i % MT, j = i / MT;
-      if (i >= L * MT || m >= mt || j < 1 || j > NY) continue;
-      const long mg = m0 + m, o = (long)j * ss + mg;
-      const double KX = KXS[m], KZ = KZS[m];
-      const double2 ph = GX[i];
-      // U1 -= i kx phi, U3 -= i kz phi
-      a1[u].x -= -KX * ph.y; a1[u].y -= KX * ph.x;
-      a3[u].x -= -KZ * ph.y; a3[u].y -= KZ * ph.x;
-      u1[o] = a1[u];
-      u3[o] = a3[u];
-      if (j >= 2) {
-        // U2(j) -= (phi(j) - phi(j-1)) / DY(j)
-        const double2 pm = GX[i - MT];
-        b2[u].x -= (ph.x - pm.x) * IDY[j];
-        b2[u].y -= (ph.y - pm.y) * IDY[j];
-        u2[o] = b2[u];
+    for (int q = 0; q < RD_K; q++) {
+      e[q] = make_double2(0.0, 0.0);
+      if (q < nr) {
+        pi = a[q] * pi;
+        const double2 gv = PH[(j0 + q) * MT + m];
+        e[q] = make_double2((gv.x + pi * c.x) * rb[q], (gv.y + pi * c.y) * rb[q]);
       }
-      phi_out[o] = ph;
-      if (rk_step > 0 && j >= JS && j <= JE) {
-        pc[u].x = pc[u].x + ph.x * ihh;
-        pc[u].y = pc[u].y + ph.y * ihh;
-        cp[o] = pc[u];
+    }
+    double2 xl = make_double2(0.0, 0.0);
+    double ps = 1.0;
+#pragma unroll
+    for (int q = RD_K - 1; q >= 0; q--) {
+      if (q < nr) {
+        const int j = j0 + q;
+        const double up = (j == NY) ? 0.0 : (j == 1) ? (mean ? 0.0 : -1.0) : UU[j];
+        const double fj = -up * rb[q];
+        xl = make_double2(e[q].x + fj * xl.x, e[q].y + fj * xl.y);
+        ps = fj * ps;
+        PH[j * MT + m] = xl;
+      }
+    }
+    if (nr > 0) {
+      SV[s * MT + m] = xl;
+      SP[s * MT + m] = ps;
+    }
+  }
+  __syncthreads();
+  if (tid < MT) {
+    double2 X = make_double2(0.0, 0.0);
+    for (int t = nseg - 1; t >= 0; t--) {
+      const double2 e = SV[t * MT + tid];
+      const double p = SP[t * MT + tid];
+      SV[t * MT + tid] = X;
+      X = make_double2(e.x + p * X.x, e.y + p * X.y);
+    }
+  }
+  __syncthreads();
+  if (nr > 0) {
+    const double2 c = SV[s * MT + m];
+    double p2 = 1.0;
+#pragma unroll
+    for (int q = RD_K - 1; q >= 0; q--) {
+      if (q < nr) {
+        const int j = j0 + q;
+        const double up = (j == NY) ? 0.0 : (j == 1) ? (mean ? 0.0 : -1.0) : UU[j];
+        p2 = (-up * rb[q]) * p2;
+        const double2 xl = PH[j * MT + m];
+        PH[j * MT + m] = make_double2(xl.x + p2 * c.x, xl.y + p2 * c.y);
       }
     }
   }
-  if (s1 == u1) return;
+  __syncthreads();
+  // ---- 4. the projection, phi and CP += phi / H_BAR (rows 1..NY)
+  const double ihh = (A.rk_step > 0) ? 1.0 / A.dscal[1 + A.rk_step] : 1.0;
+  for (int i = MT + tid; i < (NY + 1) * MT; i += nthr) {
+    const int j = i / MT, mm = i - j * MT;
+    if (mm >= mt) continue;
+    const long o = (long)j * ss + m0 + mm;
+    const double KX = KXS[mm], KZ = KZS[mm];
+    const double2 ph = PH[i];
+    double2 a1 = A.s1[o], a3 = A.s3[o];
+    // U1 -= i kx phi, U3 -= i kz phi
+    a1.x -= -KX * ph.y; a1.y -= KX * ph.x;
+    a3.x -= -KZ * ph.y; a3.y -= KZ * ph.x;
+    A.u1[o] = a1;
+    A.u3[o] = a3;
+    if (j >= 2) {
+      // U2(j) -= (phi(j) - phi(j-1)) / DY(j)
+      double2 b2 = A.s2[o];
+      const double2 pm = PH[i - MT];
+      b2.x -= (ph.x - pm.x) * IDY[j];
+      b2.y -= (ph.y - pm.y) * IDY[j];
+      A.u2[o] = b2;
+    }
+    A.phi[o] = ph;
+    if (A.rk_step > 0 && j >= A.JS && j <= A.JE) {
+      double2 pc = A.cp[o];
+      pc.x = pc.x + ph.x * ihh;
+      pc.y = pc.y + ph.y * ihh;
+      A.cp[o] = pc;
+    }
+  }
+  if (A.s1 == A.u1) return;
   // rows the projection does not touch, and the scalars, from the rhs arrays
-  for (int i = tid; i < 3 * MT; i += COL_THR) {
-    const int q = i / MT, m = i - q * MT;
-    if (m >= mt) continue;
-    const long top = (long)(NY + 1) * ss + m0 + m;
-    if (q == 0) { u1[top] = s1[top]; u3[top] = s3[top]; }
-    else if (q == 1) u2[top] = s2[top];
-    else u2[ss + m0 + m] = s2[ss + m0 + m];
+  for (int i = tid; i < 3 * MT; i += nthr) {
+    const int q = i / MT, mm = i - q * MT;
+    if (mm >= mt) continue;
+    const long top = (long)(NY + 1) * ss + m0 + mm;
+    if (q == 0) { A.u1[top] = A.s1[top]; A.u3[top] = A.s3[top]; }
+    else if (q == 1) A.u2[top] = A.s2[top];
+    else A.u2[ss + m0 + mm] = A.s2[ss + m0 + mm];
   }
-  for (int c = 0; c < cpy.n; c++) {
-    const double2 *src = cpy.src[c];
-    double2 *dst = cpy.dst[c];
-    for (int i = cpy.lo[c] * MT + tid; i < L * MT; i += COL_THR) {
-      const int j = i / MT, m = i - j * MT;
-      if (m < mt) dst[(long)j * ss + m0 + m] = src[(long)j * ss + m0 + m];
+  for (int c = 0; c < A.cpy.n; c++) {
+    const double2 *src = A.cpy.src[c];
+    double2 *dst = A.cpy.dst[c];
+    for (int i = A.cpy.lo[c] * MT + tid; i < L * MT; i += nthr) {
+      const int j = i / MT, mm = i - j * MT;
+      if (mm < mt) dst[(long)j * ss + m0 + mm] = src[(long)j * ss + m0 + mm];
     }
   }
 }
@@ -1824,36 +1852,47 @@ int dg_apply_bc_vel_dev(dg_handle *h) {
 
 int dg_rem_div_dev(dg_handle *h, int update_cp, int rk_step, bool from_rhs) {
   const int L = h->NY + 2;
-  auto rd_smem = [&](int m) {
-    return sizeof(double2) * L * m + sizeof(double) * (2 * L * m + 3 * L + 2 * m);
-  };
-  int mt = h->col_mt;  // fewer modes per CTA where a tall column needs it
-  while (mt > 4 && rd_smem(mt) > 220 * 1024) mt /= 2;
-  const size_t sm = rd_smem(mt);
+  const int nseg = dg_cdiv(h->NY, RD_K);
+  // fewer modes per CTA where a tall column needs it
+  int mt = h->col_mt;
+  while (mt > 2 && ((mt * nseg + 31) / 32 * 32 > RD_MAX_THR || rd_smem(L, nseg, mt) > 220 * 1024))
+    mt /= 2;
+  const int thr = (mt * nseg + 31) / 32 * 32;
+  const size_t sm = rd_smem(L, nseg, mt);
+  if (thr > RD_MAX_THR || sm > 220 * 1024) {
+    dg_set_error("REM_DIV column kernel: NY too large (NY <= 1016)");
+    return DG_ERR_DIMS;
+  }
+  RdArgs A;
+  memset(&A, 0, sizeof(A));
+  A.NY = h->NY; A.nkxp = h->nkxp; A.JS = h->jstart; A.JE = h->jend;
+  A.rk_step = update_cp ? rk_step : 0;
+  A.nseg = nseg;
+  A.ss = h->ss;
+  A.kxv = h->kx; A.kzv = h->kz; A.dy = h->dy; A.dyf = h->dyf;
+  A.ra = h->rem_a; A.rrb = h->rem_rb; A.dscal = h->dscal;
   // from_rhs: the column stage left the post-CN velocity (and the scalars a
   // velocity right-hand side reads) in the rhs arrays
   const double2 *const *src = from_rhs ? h->rhs : h->cu;
-  RdCopy cpy;
-  memset(&cpy, 0, sizeof(cpy));
+  A.s1 = src[0]; A.s2 = src[1]; A.s3 = src[2];
+  A.u1 = h->cu[0]; A.u2 = h->cu[1]; A.u3 = h->cu[2];
+  A.cp = h->cp; A.phi = h->cr1;
   if (from_rhs)
     for (int n = 0; n < h->NTH; n++)
       if (dg_col_th_to_rhs(h, n)) {
-        cpy.src[cpy.n] = h->rhs[3 + n];
-        cpy.dst[cpy.n] = h->cu[3 + n];
-        cpy.lo[cpy.n] = h->jstart_th[n] - 1;
-        cpy.n++;
+        A.cpy.src[A.cpy.n] = h->rhs[3 + n];
+        A.cpy.dst[A.cpy.n] = h->cu[3 + n];
+        A.cpy.lo[A.cpy.n] = h->jstart_th[n] - 1;
+        A.cpy.n++;
       }
 #define RD_CASE(MTV)                                                                          \
   if (mt == MTV) {                                                                            \
     dg_big_smem((const void *)k_rd_col<MTV>);                                                 \
     dg_kt_begin(h, "k_rd_col", h->st);                                                        \
     DG_CUDA(dg_launch(h->pdl && update_cp, k_rd_col<MTV>, dim3(dg_cdiv(h->ss, MTV)),           \
-                      dim3(COL_THR), sm, h->st, h->NY, h->ss, h->nkxp, h->jstart, h->jend,    \
-                      update_cp ? rk_step : 0, h->kx, h->kz, h->dy, h->dyf, h->rem_a,         \
-                      h->rem_rb, src[0], src[1], src[2], h->cu[0], h->cu[1], h->cu[2], h->cp, \
-                      h->cr1, h->dscal, cpy));                                                \
+                      dim3(thr), sm, h->st, A));                                              \
   }
-  RD_CASE(4) RD_CASE(8) RD_CASE(16)
+  RD_CASE(2) RD_CASE(4) RD_CASE(8) RD_CASE(16)
 #undef RD_CASE
   DG_LAUNCHED();
   return DG_OK;

@@ -26,20 +26,18 @@
 // of the same operations.  Segment boundaries depend only on NY, so a mode's
 // arithmetic does not depend on the tile width.
 //
-// The kernel is persistent: each CTA takes work items in a grid-stride loop
-// through two shared-memory stages.  One thread fetches an item's inputs --
-// the field's CU tile, the NL term the z-forward kernel left in the field's
-// rhs array, CF_old (substeps 2, 3), CP (velocity fields), by bulk tensor
-// copies (TMA, no multicast), and its table and grid-factor rows by bulk
-// copies -- into a stage, all on the stage's mbarrier; the CTA computes the
-// item in the other stage meanwhile, so the loads of item i + 1 overlap the
-// arithmetic of item i.  Every wait is bounded.  The right-hand side
-// replaces NL in shared memory, the recurrences run there, and the post-CN
-// field goes to the field's rhs array.  CU is read-only in this kernel, so
-// a field's right-hand side may read another field (rotation, buoyancy,
-// GRAV, DRHODX/Z) without a race.  REM_DIV then reads the post-CN velocity
-// from the rhs arrays and writes CU.  A scalar that no velocity right-hand
-// side reads is written in place.
+// One CTA per work item.  One thread fetches the item's inputs -- the
+// field's CU tile, the NL term the z-forward kernel left in the field's rhs
+// array, CF_old (substeps 2, 3), CP (velocity fields), by bulk tensor copies
+// (TMA, no multicast), and its table and grid-factor rows by bulk copies --
+// all at once on one mbarrier with a bounded wait.  The right-hand side is
+// formed in a flat loop over (row, mode) and replaces NL in shared memory,
+// the recurrences run there (each phase loads its rows before its chain),
+// and the post-CN field goes to the field's rhs array.  CU is read-only in
+// this kernel, so a field's right-hand side may read another field
+// (rotation, buoyancy, GRAV, DRHODX/Z) without a race.  REM_DIV then reads
+// the post-CN velocity from the rhs arrays and writes CU.  A scalar that no
+// velocity right-hand side reads is written in place.
 //
 // The same kernel serves one case (a one-case table) and the ensemble
 // server's groups (a ragged work list over every member), so a case
@@ -68,13 +66,12 @@ struct ColConst {
 // Everything the column stage of one case needs, in device memory (tensor
 // maps first: 64-byte aligned).  Maps are 2-D over [plane][2 ss doubles].
 struct ColCase {
-  CUtensorMap map_cu[3 + DG_MAX_TH];
+  CUtensorMap map_cu[3 + DG_MAX_TH], map_nl[3 + DG_MAX_TH], map_cf[3 + DG_MAX_TH];
+  CUtensorMap map_cp;
   ColConst C;
   const double *dscal, *tab, *kxv, *kzv, *rowc;
-  const double2 *cp;
   const double2 *cu[3 + DG_MAX_TH];
-  const double2 *nl[3 + DG_MAX_TH];  // the z forward's NL terms (the rhs arrays)
-  double2 *cf[3 + DG_MAX_TH], *out[3 + DG_MAX_TH];
+  double2 *cf[3 + DG_MAX_TH], *out[3 + DG_MAX_TH];  // out: the rhs arrays
   int *err;
   int by, nbox, nseg;
 };
@@ -226,49 +223,70 @@ struct ColLaunch {
   int nwork;  // work items (CTAs)
 };
 
-// Shared memory of one CTA (128-byte aligned): the CU tile and the R tile
-// (the right-hand side, then g, e and x of the recurrences) [tile] double2;
-// the CN table rows TB [5][lp] (a, 1/b, f = -c/b, kind, BC value); the
-// field's grid factors RC [4][lp]; per (segment, mode) values SV [nseg][MT]
-// double2 (then carries); per segment products SP [nseg]; the modes'
-// wavenumbers and k^2 (to the power BETA) KW [3][MT]; the mbarrier.
+// Shared memory of one CTA (128-byte aligned): the tiles CU, NL (then R, g,
+// e and x of the recurrences), CF_old and CP [tile] double2; the CN table
+// rows TB [5][lp] (a, 1/b, f = -c/b, kind, BC value); the field's grid
+// factors RC [4][lp]; per (segment, mode) values SV [nseg][MT] double2
+// (then carries); per segment products SP [nseg]; the modes' wavenumbers
+// and k^2 (to the power BETA) KW [3][MT]; the mbarrier.
 size_t col_smem_l(const ColLaunch &P, int mt) {
-  return sizeof(double2) * (2 * (size_t)P.tile + (size_t)P.nseg * mt) +
+  return sizeof(double2) * (4 * (size_t)P.tile + (size_t)P.nseg * mt) +
          sizeof(double) * (9 * (size_t)P.lp + (size_t)P.nseg + 3 * (size_t)mt) + 8 + 128;
 }
 
 // The right-hand side of field f (kind FK: 0 U1/U3, 1 U2, 2 scalar) for the
-// CTA's rows lo..hi: one element (row, mode) per step of a flat loop over
-// all threads; NL, CF_old and CP are read from global memory (each element
-// once, coalesced), CU from the staged tile (its neighbours in y too).
+// CTA's rows lo..hi, all from the staged tiles: one element (row, mode) per
+// step of a flat loop over the CTA's threads; R replaces NL.
 template <int MT, int FK>
 __device__ __forceinline__ void rhs_tile(const ColCase &cc, const FieldCoef &k, int rk_step,
                                          long m0, int f, int mt, const double2 *CUt,
-                                         double2 *Rt, const double *RC, int LP,
-                                         const double *KW) {
-  const ColConst &C = cc.C;
-  const long ss = C.ss;
+                                         double2 *NLt, const double2 *CFt, const double2 *CPt,
+                                         const double *RC, int LP, const double *KW) {
+  const long ss = cc.C.ss;
   const bool old_cf = rk_step > 1;
-  const double2 *nlp = cc.nl[f];
-  const double2 *cfo = cc.cf[f];
   double2 *cff = cc.cf[f];
   const int nthr = blockDim.x;
-#pragma unroll 2
+#pragma unroll 4
   for (int i = k.lo * MT + (int)threadIdx.x; i < (k.hi + 1) * MT; i += nthr) {
     const int j = i / MT, m = i - j * MT;
     if (m >= mt) continue;
     const long mg = m0 + m;
     const long o = (long)j * ss + mg;
-    const double2 nlv = nlp[o];
-    const double2 old = old_cf ? cfo[o] : z2();
-    const double2 p0 = (FK < 2) ? cc.cp[o] : z2();
-    const double2 pm = (FK == 1) ? cc.cp[o - ss] : z2();
-    const double KX = KW[m], KZ = KW[MT + m], kk = KW[2 * MT + m];
     double2 fv, rr;
-    rhs_row<FK>(cc, k, f, j, o, mg == 0, KX, KZ, kk, RC, LP, CUt[i], CUt[i - MT], CUt[i + MT],
-                nlv, old, p0, pm, fv, rr);
+    rhs_row<FK>(cc, k, f, j, o, mg == 0, KW[m], KW[MT + m], KW[2 * MT + m], RC, LP, CUt[i],
+                CUt[i - MT], CUt[i + MT], NLt[i], old_cf ? CFt[i] : z2(),
+                (FK < 2) ? CPt[i] : z2(), (FK == 1) ? CPt[i - MT] : z2(), fv, rr);
     cff[o] = fv;
-    Rt[i] = rr;
+    NLt[i] = rr;
+  }
+}
+
+// Carry the per-segment values e(t) through the segments in order
+// t = t0, t0 + dt, ..., n steps: X(t) = e(t) + p(t) X(previous), storing the
+// carry into each segment (its value before the segment) in place of e(t).
+// The loads of a batch are issued before its chain.
+template <int MT>
+__device__ __forceinline__ void carry_chain(double2 *SV, const double *SP, int t0, int dt, int n,
+                                            int m) {
+  double2 X = z2();
+  constexpr int B = 8;
+  for (int b = 0; b < n; b += B) {
+    double2 e[B];
+    double p[B];
+#pragma unroll
+    for (int q = 0; q < B; q++) {
+      const int t = t0 + dt * (b + q < n ? b + q : n - 1);
+      e[q] = SV[t * MT + m];
+      p[q] = SP[t];
+    }
+#pragma unroll
+    for (int q = 0; q < B; q++) {
+      if (b + q < n) {
+        const int t = t0 + dt * (b + q);
+        SV[t * MT + m] = X;
+        X = make_double2(e[q].x + p[q] * X.x, e[q].y + p[q] * X.y);
+      }
+    }
   }
 }
 
@@ -282,9 +300,10 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   const int nseg = cc.nseg;
   const long ss = C.ss;
   const int mt = (int)((ss - m0) < MT ? (ss - m0) : MT);
+  const bool vel = f < 3, old_cf = rk_step > 1;
   double2 *CUt = reinterpret_cast<double2 *>(sbase);
-  double2 *Rt = CUt + P.tile;
-  double *TB = reinterpret_cast<double *>(Rt + P.tile);
+  double2 *NLt = CUt + P.tile, *CFt = NLt + P.tile, *CPt = CFt + P.tile;
+  double *TB = reinterpret_cast<double *>(CPt + P.tile);
   double *RC = TB + 5 * P.lp;  // the slots are sized for the largest case
   double2 *SV = reinterpret_cast<double2 *>(RC + 4 * P.lp);
   double *SP = reinterpret_cast<double *>(SV + P.nseg * MT);
@@ -300,20 +319,27 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
     KW[2 * MT + tid] = (C.beta == 1.0) ? k2 : pow(k2, C.beta);
   }
 
-  // ---- 0. the CU tile by bulk tensor copies, the table and grid-factor rows
-  // by bulk copies, all on one mbarrier with a bounded wait
+  // ---- 0. the field's tiles by bulk tensor copies, the table and grid-
+  // factor rows by bulk copies, all in flight at once on one mbarrier
   if (tid == 0) dg_mbar_init(bar, 1);
   __syncthreads();
   dg_pdl_wait();  // NL comes from the z-forward kernel
   if (tid == 0) {
     const int ctile = cc.nbox * cc.by * MT;
+    const unsigned ntiles = 2u + (old_cf ? 1u : 0u) + (vel ? 1u : 0u);
     const int nrc = (f == 1) ? 4 : 2;  // grid-factor rows 2..5 (U2) or 0..1
     // extra_tx is 0 except in the wait test, where the barrier then never completes
-    dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * ctile) +
+    dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * ctile) * ntiles +
                                (unsigned)(sizeof(double) * (5 + nrc) * LP) + extra_tx);
     // columns beyond ss and planes beyond L arrive as zeros
-    for (int q = 0; q < cc.nbox; q++)
-      dg_tma_load_2d(CUt + (long)q * cc.by * MT, &cc.map_cu[f], (int)(2 * m0), q * cc.by, bar);
+    for (int q = 0; q < cc.nbox; q++) {
+      const long d = (long)q * cc.by * MT;
+      const int x = (int)(2 * m0), y = q * cc.by;
+      dg_tma_load_2d(CUt + d, &cc.map_cu[f], x, y, bar);
+      dg_tma_load_2d(NLt + d, &cc.map_nl[f], x, y, bar);
+      if (old_cf) dg_tma_load_2d(CFt + d, &cc.map_cf[f], x, y, bar);
+      if (vel) dg_tma_load_2d(CPt + d, &cc.map_cp, x, y, bar);
+    }
     dg_bulk_load(TB, cc.tab + ((long)(rk_step - 1) * (3 + DG_MAX_TH) + f) * 5 * LP,
                  (unsigned)(sizeof(double) * 5 * LP), bar);
     dg_bulk_load(RC, cc.rowc + (long)(f == 1 ? 2 : 0) * LP,
@@ -330,37 +356,44 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
 
   // ---- 1. explicit terms, CF and the right-hand side of rows lo..hi
   const FieldCoef k = field_coef(C, cc.dscal, rk_step, f);
-  if (f == 1) rhs_tile<MT, 1>(cc, k, rk_step, m0, f, mt, CUt, Rt, RC, LP, KW);
-  else if (f < 3) rhs_tile<MT, 0>(cc, k, rk_step, m0, f, mt, CUt, Rt, RC, LP, KW);
-  else rhs_tile<MT, 2>(cc, k, rk_step, m0, f, mt, CUt, Rt, RC, LP, KW);
+  if (f == 1) rhs_tile<MT, 1>(cc, k, rk_step, m0, f, mt, CUt, NLt, CFt, CPt, RC, LP, KW);
+  else if (f < 3) rhs_tile<MT, 0>(cc, k, rk_step, m0, f, mt, CUt, NLt, CFt, CPt, RC, LP, KW);
+  else rhs_tile<MT, 2>(cc, k, rk_step, m0, f, mt, CUt, NLt, CFt, CPt, RC, LP, KW);
   __syncthreads();
 
   // ---- 2. forward recurrence g(j) = r(j) + a(j) g(j-1) over each segment
   // from zero (one thread per mode and segment); r is R on CN rows, the BC
-  // value (the (0,0) mode's real part) or zero elsewhere; g replaces R
+  // value (the (0,0) mode's real part) or zero elsewhere; g replaces R.
+  // Each phase loads its rows first, then runs its chain.
   const int m = tid % MT, s = tid / MT;
   const int j0 = s * SEG_K;
   const int nr = (s < nseg) ? min(SEG_K, L - j0) : 0;  // rows of this thread's segment
   const long mg = m0 + m;
   const bool live = m < mt;
   const bool mean = (mg == 0);
+  double a[SEG_K];
   {
+    double2 r[SEG_K];
+#pragma unroll
+    for (int q = 0; q < SEG_K; q++) {
+      const int j = (q < nr) ? j0 + q : 0;
+      const double kind = TB[3 * LP + j];
+      const double2 rv = NLt[j * MT + m];
+      const double bc = TB[4 * LP + j];
+      r[q] = (kind == (double)ROW_RHS)
+                 ? rv
+                 : make_double2((kind == (double)ROW_BC && mean) ? bc : 0.0, 0.0);
+      a[q] = TB[j];
+    }
     double2 g = z2();
     double pa = 1.0;
 #pragma unroll
     for (int q = 0; q < SEG_K; q++) {
       if (q < nr) {
-        const int j = j0 + q;
-        const double kind = TB[3 * LP + j];
-        const double2 r = (kind == (double)ROW_RHS)
-                              ? Rt[j * MT + m]
-                              : make_double2((kind == (double)ROW_BC && mean) ? TB[4 * LP + j] : 0.0,
-                                             0.0);
-        const double a = TB[j];
-        g.x = r.x + a * g.x;
-        g.y = r.y + a * g.y;
-        pa = a * pa;
-        Rt[j * MT + m] = g;
+        g.x = r[q].x + a[q] * g.x;
+        g.y = r[q].y + a[q] * g.y;
+        pa = a[q] * pa;
+        NLt[(j0 + q) * MT + m] = g;
       }
     }
     if (nr > 0) {
@@ -370,45 +403,39 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   }
   __syncthreads();
   // ---- 3. the segment ends carried down the column, one lane per mode
-  if (tid < MT) {
-    double2 G = z2();
-    for (int t = 0; t < nseg; t++) {
-      const double2 e = SV[t * MT + tid];
-      const double p = SP[t];
-      SV[t * MT + tid] = G;
-      G = make_double2(e.x + p * G.x, e.y + p * G.y);
-    }
-  }
+  if (tid < MT) carry_chain<MT>(SV, SP, 0, 1, nseg, tid);
   __syncthreads();
   // ---- 4. g = local + product x carry, e = g / b; then the backward
   // recurrence x(j) = e(j) + f(j) x(j+1) over the segment (rows >= wlo)
   const int wlo = (f >= 3) ? pick(C.JSt, f - 3) - 1 : 1;
   const int qb = wlo > j0 ? wlo - j0 : 0;  // first row of the segment to solve
   const bool solves = nr > 0 && qb < nr;
+  double fc[SEG_K];
   {
     const double2 c = (nr > 0) ? SV[s * MT + m] : z2();
+    double2 e[SEG_K];
+    double rb[SEG_K];
+#pragma unroll
+    for (int q = 0; q < SEG_K; q++) {
+      const int j = (q < nr) ? j0 + q : 0;
+      e[q] = NLt[j * MT + m];
+      rb[q] = TB[LP + j];
+      fc[q] = TB[2 * LP + j];
+    }
     double pi = 1.0;
 #pragma unroll
     for (int q = 0; q < SEG_K; q++) {
-      if (q < nr) {
-        const int j = j0 + q;
-        pi = TB[j] * pi;
-        const double2 gv = Rt[j * MT + m];
-        const double rb = TB[LP + j];
-        Rt[j * MT + m] = make_double2((gv.x + pi * c.x) * rb, (gv.y + pi * c.y) * rb);
-      }
+      pi = a[q] * pi;
+      e[q] = make_double2((e[q].x + pi * c.x) * rb[q], (e[q].y + pi * c.y) * rb[q]);
     }
     double2 xl = z2();
     double ps = 1.0;
 #pragma unroll
     for (int q = SEG_K - 1; q >= 0; q--) {
       if (q < nr && q >= qb) {
-        const int j = j0 + q;
-        const double fj = TB[2 * LP + j];
-        const double2 e = Rt[j * MT + m];
-        xl = make_double2(e.x + fj * xl.x, e.y + fj * xl.y);
-        ps = fj * ps;
-        Rt[j * MT + m] = xl;
+        xl = make_double2(e[q].x + fc[q] * xl.x, e[q].y + fc[q] * xl.y);
+        ps = fc[q] * ps;
+        NLt[(j0 + q) * MT + m] = xl;
       }
     }
     // each thread overwrites only its own SV entry, read above by itself;
@@ -421,28 +448,21 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   __syncthreads();
   // ---- 5. the segment starts carried up the column, one lane per mode
   const int sw = wlo / SEG_K;  // lowest segment with rows to solve
-  if (tid < MT) {
-    double2 X = z2();
-    for (int t = nseg - 1; t >= sw; t--) {
-      const double2 e = SV[t * MT + tid];
-      const double p = SP[t];
-      SV[t * MT + tid] = X;
-      X = make_double2(e.x + p * X.x, e.y + p * X.y);
-    }
-  }
+  if (tid < MT) carry_chain<MT>(SV, SP, nseg - 1, -1, nseg - sw, tid);
   __syncthreads();
   // ---- 6. x = local + product x carry: the post-CN field, rows >= wlo
   if (solves && live) {
     const double2 c = SV[s * MT + m];
+    double2 xl[SEG_K];
+#pragma unroll
+    for (int q = 0; q < SEG_K; q++) xl[q] = NLt[((q < nr) ? j0 + q : 0) * MT + m];
     double2 *dst = cc.out[f];
     double p2 = 1.0;
 #pragma unroll
     for (int q = SEG_K - 1; q >= 0; q--) {
       if (q < nr && q >= qb) {
-        const int j = j0 + q;
-        p2 = TB[2 * LP + j] * p2;
-        const double2 xl = Rt[j * MT + m];
-        dst[(long)j * ss + mg] = make_double2(xl.x + p2 * c.x, xl.y + p2 * c.y);
+        p2 = fc[q] * p2;
+        dst[(long)(j0 + q) * ss + mg] = make_double2(xl[q].x + p2 * c.x, xl[q].y + p2 * c.y);
       }
     }
   }
@@ -533,32 +553,35 @@ static ColLaunch col_sizes(const dg_handle *h, int mt) {
   return P;
 }
 
-// threads of one CTA for handle h at mt modes: one per (mode, segment)
+// threads of one CTA for handle h at mt modes: one per (mode, segment), and
+// at least 128 for the flat right-hand-side loop
 static int col_threads(const dg_handle *h, int mt) {
-  return (mt * col_sizes(h, mt).nseg + 31) / 32 * 32;
+  return std::max(128, (mt * col_sizes(h, mt).nseg + 31) / 32 * 32);
 }
 
 size_t dg_col_smem(const dg_handle *h, int mt) { return col_smem_l(col_sizes(h, mt), mt); }
 
 // The case description of handle h for `mt` modes per CTA (builds the
-// tensor maps of its CU arrays for that tile width).
+// tensor maps of its CU, rhs and CF arrays and CP for that tile width).
 static int fill_case(dg_handle *h, int mt, ColCase *cc) {
   const int L = h->NY + 2;
   int by = 0, nbox = 0, nseg = 0;
   col_geometry(h, &by, &nbox, &nseg);
   memset(cc, 0, sizeof(*cc));
-  for (int f = 0; f < h->nf; f++)
+  for (int f = 0; f < h->nf; f++) {
     DG_TRY(dg_tmap_planes(h->cu[f], h->ss, L, mt, by, &cc->map_cu[f]));
+    DG_TRY(dg_tmap_planes(h->rhs[f], h->ss, L, mt, by, &cc->map_nl[f]));
+    DG_TRY(dg_tmap_planes(h->cf[f], h->ss, L, mt, by, &cc->map_cf[f]));
+  }
+  DG_TRY(dg_tmap_planes(h->cp, h->ss, L, mt, by, &cc->map_cp));
   cc->C = make_col_const(h);
   cc->dscal = h->dscal;
   cc->tab = h->cn_tab;
   cc->kxv = h->kx;
   cc->kzv = h->kz;
   cc->rowc = h->rowc;
-  cc->cp = h->cp;
   for (int f = 0; f < h->nf; f++) {
     cc->cu[f] = h->cu[f];
-    cc->nl[f] = h->rhs[f];
     cc->cf[f] = h->cf[f];
     cc->out[f] = (f < 3 || dg_col_th_to_rhs(h, f - 3)) ? h->rhs[f] : h->cu[f];
   }

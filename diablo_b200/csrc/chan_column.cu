@@ -26,12 +26,12 @@
 // of the same operations.  Segment boundaries depend only on NY, so a mode's
 // arithmetic does not depend on the tile width.
 //
-// One CTA per work item.  One thread fetches the item's inputs -- the
-// field's CU tile, the NL term the z-forward kernel left in the field's rhs
-// array, CF_old (substeps 2, 3), CP (velocity fields), by bulk tensor copies
-// (TMA, no multicast), and its table and grid-factor rows by bulk copies --
-// all at once on one mbarrier with a bounded wait.  The right-hand side is
-// formed in a flat loop over (row, mode) and replaces NL in shared memory,
+// One CTA per work item.  One thread fetches the field's CU tile and the NL
+// term the z-forward kernel left in the field's rhs array by bulk tensor
+// copies (TMA, no multicast), and the table and grid-factor rows by bulk
+// copies, all at once on one mbarrier with a bounded wait.  The right-hand
+// side is formed in a flat loop over (row, mode), CF_old and CP read there
+// directly, and replaces NL in shared memory,
 // the recurrences run there (each phase loads its rows before its chain),
 // and the post-CN field goes to the field's rhs array.  CU is read-only in
 // this kernel, so a field's right-hand side may read another field
@@ -66,10 +66,10 @@ struct ColConst {
 // Everything the column stage of one case needs, in device memory (tensor
 // maps first: 64-byte aligned).  Maps are 2-D over [plane][2 ss doubles].
 struct ColCase {
-  CUtensorMap map_cu[3 + DG_MAX_TH], map_nl[3 + DG_MAX_TH], map_cf[3 + DG_MAX_TH];
-  CUtensorMap map_cp;
+  CUtensorMap map_cu[3 + DG_MAX_TH], map_nl[3 + DG_MAX_TH];
   ColConst C;
   const double *dscal, *tab, *kxv, *kzv, *rowc;
+  const double2 *cp;
   const double2 *cu[3 + DG_MAX_TH];
   double2 *cf[3 + DG_MAX_TH], *out[3 + DG_MAX_TH];  // out: the rhs arrays
   int *err;
@@ -223,27 +223,29 @@ struct ColLaunch {
   int nwork;  // work items (CTAs)
 };
 
-// Shared memory of one CTA (128-byte aligned): the tiles CU, NL (then R, g,
-// e and x of the recurrences), CF_old and CP [tile] double2; the CN table
+// Shared memory of one CTA (128-byte aligned): the tiles CU and NL (then R,
+// g, e and x of the recurrences) [tile] double2; the CN table
 // rows TB [5][lp] (a, 1/b, f = -c/b, kind, BC value); the field's grid
 // factors RC [4][lp]; per (segment, mode) values SV [nseg][MT] double2
 // (then carries); per segment products SP [nseg]; the modes' wavenumbers
 // and k^2 (to the power BETA) KW [3][MT]; the mbarrier.
 size_t col_smem_l(const ColLaunch &P, int mt) {
-  return sizeof(double2) * (4 * (size_t)P.tile + (size_t)P.nseg * mt) +
+  return sizeof(double2) * (2 * (size_t)P.tile + (size_t)P.nseg * mt) +
          sizeof(double) * (9 * (size_t)P.lp + (size_t)P.nseg + 3 * (size_t)mt) + 8 + 128;
 }
 
 // The right-hand side of field f (kind FK: 0 U1/U3, 1 U2, 2 scalar) for the
-// CTA's rows lo..hi, all from the staged tiles: one element (row, mode) per
-// step of a flat loop over the CTA's threads; R replaces NL.
+// CTA's rows lo..hi: one element (row, mode) per step of a flat loop over
+// the CTA's threads, CU and NL from the staged tiles, CF_old and CP read
+// directly (each element once, coalesced); R replaces NL.
 template <int MT, int FK>
 __device__ __forceinline__ void rhs_tile(const ColCase &cc, const FieldCoef &k, int rk_step,
                                          long m0, int f, int mt, const double2 *CUt,
-                                         double2 *NLt, const double2 *CFt, const double2 *CPt,
-                                         const double *RC, int LP, const double *KW) {
+                                         double2 *NLt, const double *RC, int LP,
+                                         const double *KW) {
   const long ss = cc.C.ss;
   const bool old_cf = rk_step > 1;
+  const double2 *cfo = cc.cf[f];
   double2 *cff = cc.cf[f];
   const int nthr = blockDim.x;
 #pragma unroll 4
@@ -252,10 +254,12 @@ __device__ __forceinline__ void rhs_tile(const ColCase &cc, const FieldCoef &k, 
     if (m >= mt) continue;
     const long mg = m0 + m;
     const long o = (long)j * ss + mg;
+    const double2 old = old_cf ? cfo[o] : z2();
+    const double2 p0 = (FK < 2) ? cc.cp[o] : z2();
+    const double2 pm = (FK == 1) ? cc.cp[o - ss] : z2();
     double2 fv, rr;
     rhs_row<FK>(cc, k, f, j, o, mg == 0, KW[m], KW[MT + m], KW[2 * MT + m], RC, LP, CUt[i],
-                CUt[i - MT], CUt[i + MT], NLt[i], old_cf ? CFt[i] : z2(),
-                (FK < 2) ? CPt[i] : z2(), (FK == 1) ? CPt[i - MT] : z2(), fv, rr);
+                CUt[i - MT], CUt[i + MT], NLt[i], old, p0, pm, fv, rr);
     cff[o] = fv;
     NLt[i] = rr;
   }
@@ -264,29 +268,16 @@ __device__ __forceinline__ void rhs_tile(const ColCase &cc, const FieldCoef &k, 
 // Carry the per-segment values e(t) through the segments in order
 // t = t0, t0 + dt, ..., n steps: X(t) = e(t) + p(t) X(previous), storing the
 // carry into each segment (its value before the segment) in place of e(t).
-// The loads of a batch are issued before its chain.
 template <int MT>
 __device__ __forceinline__ void carry_chain(double2 *SV, const double *SP, int t0, int dt, int n,
                                             int m) {
   double2 X = z2();
-  constexpr int B = 8;
-  for (int b = 0; b < n; b += B) {
-    double2 e[B];
-    double p[B];
-#pragma unroll
-    for (int q = 0; q < B; q++) {
-      const int t = t0 + dt * (b + q < n ? b + q : n - 1);
-      e[q] = SV[t * MT + m];
-      p[q] = SP[t];
-    }
-#pragma unroll
-    for (int q = 0; q < B; q++) {
-      if (b + q < n) {
-        const int t = t0 + dt * (b + q);
-        SV[t * MT + m] = X;
-        X = make_double2(e[q].x + p[q] * X.x, e[q].y + p[q] * X.y);
-      }
-    }
+  for (int b = 0; b < n; b++) {
+    const int t = t0 + dt * b;
+    const double2 e = SV[t * MT + m];
+    const double p = SP[t];
+    SV[t * MT + m] = X;
+    X = make_double2(e.x + p * X.x, e.y + p * X.y);
   }
 }
 
@@ -300,10 +291,9 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   const int nseg = cc.nseg;
   const long ss = C.ss;
   const int mt = (int)((ss - m0) < MT ? (ss - m0) : MT);
-  const bool vel = f < 3, old_cf = rk_step > 1;
   double2 *CUt = reinterpret_cast<double2 *>(sbase);
-  double2 *NLt = CUt + P.tile, *CFt = NLt + P.tile, *CPt = CFt + P.tile;
-  double *TB = reinterpret_cast<double *>(CPt + P.tile);
+  double2 *NLt = CUt + P.tile;
+  double *TB = reinterpret_cast<double *>(NLt + P.tile);
   double *RC = TB + 5 * P.lp;  // the slots are sized for the largest case
   double2 *SV = reinterpret_cast<double2 *>(RC + 4 * P.lp);
   double *SP = reinterpret_cast<double *>(SV + P.nseg * MT);
@@ -319,14 +309,14 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
     KW[2 * MT + tid] = (C.beta == 1.0) ? k2 : pow(k2, C.beta);
   }
 
-  // ---- 0. the field's tiles by bulk tensor copies, the table and grid-
-  // factor rows by bulk copies, all in flight at once on one mbarrier
+  // ---- 0. the field's CU and NL tiles by bulk tensor copies, the table and
+  // grid-factor rows by bulk copies, all in flight at once on one mbarrier
   if (tid == 0) dg_mbar_init(bar, 1);
   __syncthreads();
   dg_pdl_wait();  // NL comes from the z-forward kernel
   if (tid == 0) {
     const int ctile = cc.nbox * cc.by * MT;
-    const unsigned ntiles = 2u + (old_cf ? 1u : 0u) + (vel ? 1u : 0u);
+    const unsigned ntiles = 2u;
     const int nrc = (f == 1) ? 4 : 2;  // grid-factor rows 2..5 (U2) or 0..1
     // extra_tx is 0 except in the wait test, where the barrier then never completes
     dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * ctile) * ntiles +
@@ -337,8 +327,6 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
       const int x = (int)(2 * m0), y = q * cc.by;
       dg_tma_load_2d(CUt + d, &cc.map_cu[f], x, y, bar);
       dg_tma_load_2d(NLt + d, &cc.map_nl[f], x, y, bar);
-      if (old_cf) dg_tma_load_2d(CFt + d, &cc.map_cf[f], x, y, bar);
-      if (vel) dg_tma_load_2d(CPt + d, &cc.map_cp, x, y, bar);
     }
     dg_bulk_load(TB, cc.tab + ((long)(rk_step - 1) * (3 + DG_MAX_TH) + f) * 5 * LP,
                  (unsigned)(sizeof(double) * 5 * LP), bar);
@@ -356,9 +344,9 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
 
   // ---- 1. explicit terms, CF and the right-hand side of rows lo..hi
   const FieldCoef k = field_coef(C, cc.dscal, rk_step, f);
-  if (f == 1) rhs_tile<MT, 1>(cc, k, rk_step, m0, f, mt, CUt, NLt, CFt, CPt, RC, LP, KW);
-  else if (f < 3) rhs_tile<MT, 0>(cc, k, rk_step, m0, f, mt, CUt, NLt, CFt, CPt, RC, LP, KW);
-  else rhs_tile<MT, 2>(cc, k, rk_step, m0, f, mt, CUt, NLt, CFt, CPt, RC, LP, KW);
+  if (f == 1) rhs_tile<MT, 1>(cc, k, rk_step, m0, f, mt, CUt, NLt, RC, LP, KW);
+  else if (f < 3) rhs_tile<MT, 0>(cc, k, rk_step, m0, f, mt, CUt, NLt, RC, LP, KW);
+  else rhs_tile<MT, 2>(cc, k, rk_step, m0, f, mt, CUt, NLt, RC, LP, KW);
   __syncthreads();
 
   // ---- 2. forward recurrence g(j) = r(j) + a(j) g(j-1) over each segment
@@ -562,7 +550,7 @@ static int col_threads(const dg_handle *h, int mt) {
 size_t dg_col_smem(const dg_handle *h, int mt) { return col_smem_l(col_sizes(h, mt), mt); }
 
 // The case description of handle h for `mt` modes per CTA (builds the
-// tensor maps of its CU, rhs and CF arrays and CP for that tile width).
+// tensor maps of its CU and rhs arrays for that tile width).
 static int fill_case(dg_handle *h, int mt, ColCase *cc) {
   const int L = h->NY + 2;
   int by = 0, nbox = 0, nseg = 0;
@@ -571,9 +559,8 @@ static int fill_case(dg_handle *h, int mt, ColCase *cc) {
   for (int f = 0; f < h->nf; f++) {
     DG_TRY(dg_tmap_planes(h->cu[f], h->ss, L, mt, by, &cc->map_cu[f]));
     DG_TRY(dg_tmap_planes(h->rhs[f], h->ss, L, mt, by, &cc->map_nl[f]));
-    DG_TRY(dg_tmap_planes(h->cf[f], h->ss, L, mt, by, &cc->map_cf[f]));
   }
-  DG_TRY(dg_tmap_planes(h->cp, h->ss, L, mt, by, &cc->map_cp));
+  cc->cp = h->cp;
   cc->C = make_col_const(h);
   cc->dscal = h->dscal;
   cc->tab = h->cn_tab;

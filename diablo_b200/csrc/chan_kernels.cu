@@ -1364,37 +1364,8 @@ size_t rd_smem(int L, int nseg, int mt) {
          sizeof(double) * ((size_t)nseg * mt + 3 * (size_t)L + 2 * (size_t)mt);
 }
 
-// Carry the per-(segment, mode) values e(t) through the segments in order
-// t = t0, t0 + dt, ..., n steps: X(t) = e(t) + p(t) X(previous), storing the
-// carry (the value before each segment) in place of e(t).  The loads of a
-// batch are issued before its chain.
 template <int MT>
-__device__ __forceinline__ void rd_carry(double2 *SV, const double *SP, int t0, int dt, int n,
-                                         int m) {
-  double2 X = make_double2(0.0, 0.0);
-  constexpr int B = 8;
-  for (int b = 0; b < n; b += B) {
-    double2 e[B];
-    double p[B];
-#pragma unroll
-    for (int q = 0; q < B; q++) {
-      const int t = t0 + dt * (b + q < n ? b + q : n - 1);
-      e[q] = SV[t * MT + m];
-      p[q] = SP[t * MT + m];
-    }
-#pragma unroll
-    for (int q = 0; q < B; q++) {
-      if (b + q < n) {
-        const int t = t0 + dt * (b + q);
-        SV[t * MT + m] = X;
-        X = make_double2(e[q].x + p[q] * X.x, e[q].y + p[q] * X.y);
-      }
-    }
-  }
-}
-
-template <int MT>
-__global__ void __launch_bounds__(RD_MAX_THR, 2) k_rd_col(RdArgs A) {
+__global__ void __launch_bounds__(RD_MAX_THR, 3) k_rd_col(RdArgs A) {
   extern __shared__ double2 rsm[];
   const int NY = A.NY, L = NY + 2, nseg = A.nseg;
   const long ss = A.ss;
@@ -1451,16 +1422,14 @@ __global__ void __launch_bounds__(RD_MAX_THR, 2) k_rd_col(RdArgs A) {
     rb[q] = (q < nr) ? A.rrb[o] : 0.0;
   }
   {
-    double2 r[RD_K];
-#pragma unroll
-    for (int q = 0; q < RD_K; q++) r[q] = PH[((q < nr) ? j0 + q : 1) * MT + m];
     double2 g = make_double2(0.0, 0.0);
     double pa = 1.0;
 #pragma unroll
     for (int q = 0; q < RD_K; q++) {
       if (q < nr) {
-        g.x = r[q].x + a[q] * g.x;
-        g.y = r[q].y + a[q] * g.y;
+        const double2 r = PH[(j0 + q) * MT + m];
+        g.x = r.x + a[q] * g.x;
+        g.y = r.y + a[q] * g.y;
         pa = a[q] * pa;
         PH[(j0 + q) * MT + m] = g;
       }
@@ -1471,38 +1440,45 @@ __global__ void __launch_bounds__(RD_MAX_THR, 2) k_rd_col(RdArgs A) {
     }
   }
   __syncthreads();
-  if (tid < MT) rd_carry<MT>(SV, SP, 0, 1, nseg, tid);
+  if (tid < MT) {
+    double2 G = make_double2(0.0, 0.0);
+    for (int t = 0; t < nseg; t++) {
+      const double2 e = SV[t * MT + tid];
+      const double p = SP[t * MT + tid];
+      SV[t * MT + tid] = G;
+      G = make_double2(e.x + p * G.x, e.y + p * G.y);
+    }
+  }
   __syncthreads();
   // ---- 3. g = local + product x carry, e = g / b; the backward recurrence
   // phi(j) = e(j) + f(j) phi(j+1), f = -c / b (row NY: f = 0; row 1: the
   // upper coefficient of APPLY_BC_REM_DIV_MPI, 0 for the mean mode, -1
   // otherwise)
   const bool mean = live && (m0 + m == 0);
-  double fr[RD_K];  // f = -c / b of the segment's rows
   {
     const double2 c = (nr > 0) ? SV[s * MT + m] : make_double2(0.0, 0.0);
+    double pi = 1.0;
     double2 e[RD_K];
 #pragma unroll
     for (int q = 0; q < RD_K; q++) {
-      const int j = (q < nr) ? j0 + q : 1;
-      e[q] = PH[j * MT + m];
-      const double up = (j == NY) ? 0.0 : (j == 1) ? (mean ? 0.0 : -1.0) : UU[j];
-      fr[q] = -up * rb[q];
-    }
-    double pi = 1.0;
-#pragma unroll
-    for (int q = 0; q < RD_K; q++) {
-      pi = a[q] * pi;
-      e[q] = make_double2((e[q].x + pi * c.x) * rb[q], (e[q].y + pi * c.y) * rb[q]);
+      e[q] = make_double2(0.0, 0.0);
+      if (q < nr) {
+        pi = a[q] * pi;
+        const double2 gv = PH[(j0 + q) * MT + m];
+        e[q] = make_double2((gv.x + pi * c.x) * rb[q], (gv.y + pi * c.y) * rb[q]);
+      }
     }
     double2 xl = make_double2(0.0, 0.0);
     double ps = 1.0;
 #pragma unroll
     for (int q = RD_K - 1; q >= 0; q--) {
       if (q < nr) {
-        xl = make_double2(e[q].x + fr[q] * xl.x, e[q].y + fr[q] * xl.y);
-        ps = fr[q] * ps;
-        PH[(j0 + q) * MT + m] = xl;
+        const int j = j0 + q;
+        const double up = (j == NY) ? 0.0 : (j == 1) ? (mean ? 0.0 : -1.0) : UU[j];
+        const double fj = -up * rb[q];
+        xl = make_double2(e[q].x + fj * xl.x, e[q].y + fj * xl.y);
+        ps = fj * ps;
+        PH[j * MT + m] = xl;
       }
     }
     if (nr > 0) {
@@ -1511,19 +1487,27 @@ __global__ void __launch_bounds__(RD_MAX_THR, 2) k_rd_col(RdArgs A) {
     }
   }
   __syncthreads();
-  if (tid < MT) rd_carry<MT>(SV, SP, nseg - 1, -1, nseg, tid);
+  if (tid < MT) {
+    double2 X = make_double2(0.0, 0.0);
+    for (int t = nseg - 1; t >= 0; t--) {
+      const double2 e = SV[t * MT + tid];
+      const double p = SP[t * MT + tid];
+      SV[t * MT + tid] = X;
+      X = make_double2(e.x + p * X.x, e.y + p * X.y);
+    }
+  }
   __syncthreads();
   if (nr > 0) {
     const double2 c = SV[s * MT + m];
-    double2 xl[RD_K];
-#pragma unroll
-    for (int q = 0; q < RD_K; q++) xl[q] = PH[((q < nr) ? j0 + q : 1) * MT + m];
     double p2 = 1.0;
 #pragma unroll
     for (int q = RD_K - 1; q >= 0; q--) {
       if (q < nr) {
-        p2 = fr[q] * p2;
-        PH[(j0 + q) * MT + m] = make_double2(xl[q].x + p2 * c.x, xl[q].y + p2 * c.y);
+        const int j = j0 + q;
+        const double up = (j == NY) ? 0.0 : (j == 1) ? (mean ? 0.0 : -1.0) : UU[j];
+        p2 = (-up * rb[q]) * p2;
+        const double2 xl = PH[j * MT + m];
+        PH[j * MT + m] = make_double2(xl.x + p2 * c.x, xl.y + p2 * c.y);
       }
     }
   }

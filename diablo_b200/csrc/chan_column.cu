@@ -26,12 +26,12 @@
 // of the same operations.  Segment boundaries depend only on NY, so a mode's
 // arithmetic does not depend on the tile width.
 //
-// One CTA per work item.  One thread fetches the field's CU tile and the NL
-// term the z-forward kernel left in the field's rhs array by bulk tensor
-// copies (TMA, no multicast), and the table and grid-factor rows by bulk
-// copies, all at once on one mbarrier with a bounded wait.  The right-hand
-// side is formed in a flat loop over (row, mode), CF_old and CP read there
-// directly, and replaces NL in shared memory,
+// One CTA per work item.  One thread fetches the item's inputs -- the
+// field's CU tile, the NL term the z-forward kernel left in the field's rhs
+// array, CF_old (substeps 2, 3), CP (velocity fields), by bulk tensor copies
+// (TMA, no multicast), and its table and grid-factor rows by bulk copies --
+// all at once on one mbarrier with a bounded wait.  The right-hand side is
+// formed in a flat loop over (row, mode) and replaces NL in shared memory,
 // the recurrences run there (each phase loads its rows before its chain),
 // and the post-CN field goes to the field's rhs array.  CU is read-only in
 // this kernel, so a field's right-hand side may read another field
@@ -66,10 +66,10 @@ struct ColConst {
 // Everything the column stage of one case needs, in device memory (tensor
 // maps first: 64-byte aligned).  Maps are 2-D over [plane][2 ss doubles].
 struct ColCase {
-  CUtensorMap map_cu[3 + DG_MAX_TH], map_nl[3 + DG_MAX_TH];
+  CUtensorMap map_cu[3 + DG_MAX_TH], map_nl[3 + DG_MAX_TH], map_cf[3 + DG_MAX_TH];
+  CUtensorMap map_cp;
   ColConst C;
   const double *dscal, *tab, *kxv, *kzv, *rowc;
-  const double2 *cp;
   const double2 *cu[3 + DG_MAX_TH];
   double2 *cf[3 + DG_MAX_TH], *out[3 + DG_MAX_TH];  // out: the rhs arrays
   int *err;
@@ -94,15 +94,25 @@ __device__ __forceinline__ double2 z2() { return make_double2(0.0, 0.0); }
 //   6 1/DYF(j)            7 REM_DIV upper diagonal
 
 // The field's coefficients that do not change along the column.
+// Everything the right-hand side of one field needs besides the tiles, read
+// from the case table once per CTA into registers (the loop that uses them
+// stores to global memory, after which the compiler would have to reload
+// anything it reads from the table).
 struct FieldCoef {
-  double T3, T4, T5, aaU, NU, nup, ipr, ddx, ddz, sgn, gr, time;
-  int lo, hi;
+  double T3, T4, T5, aaU, NU, nup, ipr, ddx, ddz, sgn, time;
+  double i_ro, px0, amp_omega0, omega0;
+  double w[DG_MAX_TH];              // coupling weight of each scalar (0: none)
+  const double2 *th[DG_MAX_TH];     // the scalars' CU
+  const double2 *uo;                // the other horizontal velocity (rotation)
+  const double2 *u1, *u3;           // U1, U3 (DRHODX/Z in a scalar's equation)
+  long ss;
+  int lo, hi, nth, f_type;
 };
 
-__device__ __forceinline__ FieldCoef field_coef(const ColConst &C, const double *dscal,
-                                                int rk_step, int f) {
+__device__ __forceinline__ FieldCoef field_coef(const ColCase &cc, int rk_step, int f) {
+  const ColConst &C = cc.C;
   FieldCoef k;
-  const double h = dscal[1 + rk_step];
+  const double h = cc.dscal[1 + rk_step];
   const double zeta = (rk_step == 2) ? -17.0 / 8.0 : (rk_step == 3) ? -5.0 / 4.0 : 0.0;
   const double bbar = (rk_step == 2) ? 25.0 / 8.0 : (rk_step == 3) ? 9.0 / 4.0 : 1.0;
   const double T1 = C.nu * h / 2.0;
@@ -111,14 +121,30 @@ __device__ __forceinline__ FieldCoef field_coef(const ColConst &C, const double 
   k.T5 = bbar * h;
   k.aaU = T1 * C.nuv;
   k.NU = C.nu;
-  k.time = dscal[0];
+  k.time = cc.dscal[0];
   const int n = f - 3;
   k.nup = (f >= 3) ? C.nu / pick(C.pr, n) : C.nu;
   k.ipr = (f >= 3) ? 1.0 / pick(C.pr, n) : 1.0;
   k.ddx = (f >= 3) ? pick(C.drhodx, n) : 0.0;
   k.ddz = (f >= 3) ? pick(C.drhodz, n) : 0.0;
   k.sgn = (f == 0) ? 1.0 : -1.0;
-  k.gr = (f == 0) ? C.grav_x : C.grav_z;
+  k.i_ro = C.i_ro;
+  k.px0 = C.px0;
+  k.amp_omega0 = C.amp_omega0;
+  k.omega0 = C.omega0;
+  k.f_type = C.f_type;
+  k.nth = C.nth;
+  k.ss = C.ss;
+  // U1, U3: RI GRAV_x/z TH; U2: RI GRAV_y times the GY interpolation
+  const double gr = (f == 0) ? C.grav_x : (f == 2) ? C.grav_z : C.grav_y;
+#pragma unroll
+  for (int q = 0; q < DG_MAX_TH; q++) {
+    k.w[q] = (q < C.nth && f < 3) ? C.ri[q] * gr : 0.0;
+    k.th[q] = cc.cu[3 + (q < C.nth ? q : 0)];
+  }
+  k.uo = cc.cu[(f == 0) ? 2 : 0];
+  k.u1 = cc.cu[0];
+  k.u3 = cc.cu[2];
   if (f == 0 || f == 2) { k.lo = C.JS; k.hi = C.JE; }
   else if (f == 1) { k.lo = 2; k.hi = C.NY; }
   else { k.lo = pick(C.JSt, n); k.hi = pick(C.JEt, n); }
@@ -126,29 +152,27 @@ __device__ __forceinline__ FieldCoef field_coef(const ColConst &C, const double 
 }
 
 // The explicit terms fv (the new CF) and the CN right-hand side r of field f
-// at row j, mode mg (offset o): u, um, up = CU at j, j-1, j+1; nlv = NL;
+// at row j, mode offset o: u, um, up = CU at j, j-1, j+1; nlv = NL;
 // old = CF_old; p0, pm = CP at j, j-1.  RC: the field's grid-factor rows in
 // shared memory, row stride ld: rows 0, 1 (U1, U3, TH) or 2, 3, 4, 5 (U2).
 template <int FK>
-__device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, int f, int j,
-                                        long o, bool mean, double KX, double KZ, double kk,
-                                        const double *RC, int ld, double2 u, double2 um, double2 up,
-                                        double2 nlv, double2 old, double2 p0, double2 pm,
-                                        double2 &fv, double2 &r) {
-  const ColConst &C = cc.C;
-  const int nth = C.nth;
-  const long ss = C.ss;
+__device__ __forceinline__ void rhs_row(const FieldCoef &k, int f, int j, long o, bool mean,
+                                        double KX, double KZ, double kk, const double *RC, int ld,
+                                        double2 u, double2 um, double2 up, double2 nlv,
+                                        double2 old, double2 p0, double2 pm, double2 &fv,
+                                        double2 &r) {
   if constexpr (FK == 0) {
     fv = make_double2(-k.NU * kk * u.x, -k.NU * kk * u.y);
-    if (C.i_ro != 0.0) {
-      const double2 uo = cc.cu[2 - f][o];
-      fv.x += k.sgn * C.i_ro * uo.x;
-      fv.y += k.sgn * C.i_ro * uo.y;
+    if (k.i_ro != 0.0) {
+      const double2 uo = k.uo[o];
+      fv.x += k.sgn * k.i_ro * uo.x;
+      fv.y += k.sgn * k.i_ro * uo.y;
     }
-    for (int q = 0; q < nth; q++) {
-      const double w = C.ri[q] * k.gr;
-      if (w == 0.0) continue;
-      const double2 t = cc.cu[3 + q][o];
+#pragma unroll
+    for (int q = 0; q < DG_MAX_TH; q++) {
+      const double w = k.w[q];
+      if (q >= k.nth || w == 0.0) continue;
+      const double2 t = k.th[q][o];
       fv.x += w * t.x;
       fv.y += w * t.y;
     }
@@ -161,8 +185,8 @@ __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, i
     r.x -= k.T4 * (-K * p0.y);
     r.y -= k.T4 * (K * p0.x);
     if (f == 0 && mean) {
-      if (C.f_type == 1) r.x -= k.T4 * C.px0;
-      else if (C.f_type == 2) r.x -= k.T4 * (C.px0 + C.amp_omega0 * cos(C.omega0 * k.time));
+      if (k.f_type == 1) r.x -= k.T4 * k.px0;
+      else if (k.f_type == 2) r.x -= k.T4 * (k.px0 + k.amp_omega0 * cos(k.omega0 * k.time));
     }
     r.x += k.T5 * fv.x;
     r.y += k.T5 * fv.y;
@@ -174,10 +198,11 @@ __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, i
     if (!mean) {
       const double dyfj = RC[3 * ld + j], dyfm = RC[3 * ld + j - 1];
       const double bw2 = 0.5 * RC[2 * ld + j];
-      for (int q = 0; q < nth; q++) {
-        if (C.ri[q] * C.grav_y == 0.0) continue;
-        const double w = C.ri[q] * C.grav_y * bw2;
-        const double2 t = cc.cu[3 + q][o], tm = cc.cu[3 + q][o - ss];
+#pragma unroll
+      for (int q = 0; q < DG_MAX_TH; q++) {
+        if (q >= k.nth || k.w[q] == 0.0) continue;
+        const double w = k.w[q] * bw2;
+        const double2 t = k.th[q][o], tm = k.th[q][o - k.ss];
         fv.x += w * (t.x * dyfm + tm.x * dyfj);
         fv.y += w * (t.y * dyfm + tm.y * dyfj);
       }
@@ -198,7 +223,7 @@ __device__ __forceinline__ void rhs_row(const ColCase &cc, const FieldCoef &k, i
   } else {
     fv = make_double2(-k.nup * kk * u.x, -k.nup * kk * u.y);
     if (k.ddx != 0.0 || k.ddz != 0.0) {
-      const double2 u1 = cc.cu[0][o], u3 = cc.cu[2][o];
+      const double2 u1 = k.u1[o], u3 = k.u3[o];
       fv.x = fv.x - u1.x * k.ddx - u3.x * k.ddz;
       fv.y = fv.y - u1.y * k.ddx - u3.y * k.ddz;
     }
@@ -223,43 +248,39 @@ struct ColLaunch {
   int nwork;  // work items (CTAs)
 };
 
-// Shared memory of one CTA (128-byte aligned): the tiles CU and NL (then R,
-// g, e and x of the recurrences) [tile] double2; the CN table
+// Shared memory of one CTA (128-byte aligned): the tiles CU, NL (then R, g,
+// e and x of the recurrences), CF_old and CP [tile] double2; the CN table
 // rows TB [5][lp] (a, 1/b, f = -c/b, kind, BC value); the field's grid
 // factors RC [4][lp]; per (segment, mode) values SV [nseg][MT] double2
 // (then carries); per segment products SP [nseg]; the modes' wavenumbers
 // and k^2 (to the power BETA) KW [3][MT]; the mbarrier.
 size_t col_smem_l(const ColLaunch &P, int mt) {
-  return sizeof(double2) * (2 * (size_t)P.tile + (size_t)P.nseg * mt) +
+  return sizeof(double2) * (4 * (size_t)P.tile + (size_t)P.nseg * mt) +
          sizeof(double) * (9 * (size_t)P.lp + (size_t)P.nseg + 3 * (size_t)mt) + 8 + 128;
 }
 
 // The right-hand side of field f (kind FK: 0 U1/U3, 1 U2, 2 scalar) for the
-// CTA's rows lo..hi: one element (row, mode) per step of a flat loop over
-// the CTA's threads, CU and NL from the staged tiles, CF_old and CP read
-// directly (each element once, coalesced); R replaces NL.
+// CTA's rows lo..hi, all from the staged tiles: one element (row, mode) per
+// step of a flat loop over the CTA's threads; R replaces NL.  The loop's
+// only global accesses are the CF stores and, with couplings, the other
+// fields' CU: everything else it reads is in registers or shared memory.
 template <int MT, int FK>
-__device__ __forceinline__ void rhs_tile(const ColCase &cc, const FieldCoef &k, int rk_step,
-                                         long m0, int f, int mt, const double2 *CUt,
-                                         double2 *NLt, const double *RC, int LP,
-                                         const double *KW) {
-  const long ss = cc.C.ss;
+__device__ __forceinline__ void rhs_tile(const FieldCoef &k, int rk_step, long m0, int f, int mt,
+                                         double2 *cff, const double2 *CUt, double2 *NLt,
+                                         const double2 *CFt, const double2 *CPt,
+                                         const double *RC, int LP, const double *KW) {
   const bool old_cf = rk_step > 1;
-  const double2 *cfo = cc.cf[f];
-  double2 *cff = cc.cf[f];
   const int nthr = blockDim.x;
 #pragma unroll 4
   for (int i = k.lo * MT + (int)threadIdx.x; i < (k.hi + 1) * MT; i += nthr) {
     const int j = i / MT, m = i - j * MT;
     if (m >= mt) continue;
     const long mg = m0 + m;
-    const long o = (long)j * ss + mg;
-    const double2 old = old_cf ? cfo[o] : z2();
-    const double2 p0 = (FK < 2) ? cc.cp[o] : z2();
-    const double2 pm = (FK == 1) ? cc.cp[o - ss] : z2();
+    const long o = (long)j * k.ss + mg;
     double2 fv, rr;
-    rhs_row<FK>(cc, k, f, j, o, mg == 0, KW[m], KW[MT + m], KW[2 * MT + m], RC, LP, CUt[i],
-                CUt[i - MT], CUt[i + MT], NLt[i], old, p0, pm, fv, rr);
+    rhs_row<FK>(k, f, j, o, mg == 0, KW[m], KW[MT + m], KW[2 * MT + m], RC, LP, CUt[i],
+                CUt[i - MT], CUt[i + MT], NLt[i], old_cf ? CFt[i] : z2(),
+                (FK < 2) ? CPt[i] : z2(), (FK == 1) ? CPt[i - MT] : z2(), fv, rr);
     cff[o] = fv;
     NLt[i] = rr;
   }
@@ -281,19 +302,26 @@ __device__ __forceinline__ void carry_chain(double2 *SV, const double *SP, int t
   }
 }
 
-// The column stage of field f for modes m0 .. m0+MT-1 of one case.
+// The column stage of field f for modes m0 .. m0+MT-1 of one case.  Every
+// value the CTA needs from the case table is read before its first global
+// store (after which the compiler would have to reload it).
 template <int MT>
 __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0, int f,
                                          const ColLaunch &P, long spin, unsigned extra_tx,
                                          unsigned char *sbase) {
-  const ColConst &C = cc.C;
-  const int NY = C.NY, L = NY + 2, LP = (L + 1) & ~1;  // the case's own row length
+  const int NY = cc.C.NY, L = NY + 2, LP = (L + 1) & ~1;  // the case's own row length
   const int nseg = cc.nseg;
-  const long ss = C.ss;
+  const long ss = cc.C.ss;
   const int mt = (int)((ss - m0) < MT ? (ss - m0) : MT);
+  const bool vel = f < 3, old_cf = rk_step > 1;
+  const int wlo = (f >= 3) ? pick(cc.C.JSt, f - 3) - 1 : 1;  // first row solved
+  double2 *const dst = cc.out[f];
+  double2 *const cff = cc.cf[f];
+  int *const err = cc.err;
+  const FieldCoef k = field_coef(cc, rk_step, f);
   double2 *CUt = reinterpret_cast<double2 *>(sbase);
-  double2 *NLt = CUt + P.tile;
-  double *TB = reinterpret_cast<double *>(NLt + P.tile);
+  double2 *NLt = CUt + P.tile, *CFt = NLt + P.tile, *CPt = CFt + P.tile;
+  double *TB = reinterpret_cast<double *>(CPt + P.tile);
   double *RC = TB + 5 * P.lp;  // the slots are sized for the largest case
   double2 *SV = reinterpret_cast<double2 *>(RC + 4 * P.lp);
   double *SP = reinterpret_cast<double *>(SV + P.nseg * MT);
@@ -302,21 +330,21 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   const int tid = threadIdx.x;
   if (tid < MT) {
     const long mg = (m0 + tid < ss) ? m0 + tid : 0;
-    const double KX = cc.kxv[mg % C.nkxp], KZ = cc.kzv[mg / C.nkxp];
+    const double KX = cc.kxv[mg % cc.C.nkxp], KZ = cc.kzv[mg / cc.C.nkxp];
     const double k2 = KX * KX + KZ * KZ;
     KW[tid] = KX;
     KW[MT + tid] = KZ;
-    KW[2 * MT + tid] = (C.beta == 1.0) ? k2 : pow(k2, C.beta);
+    KW[2 * MT + tid] = (cc.C.beta == 1.0) ? k2 : pow(k2, cc.C.beta);
   }
 
-  // ---- 0. the field's CU and NL tiles by bulk tensor copies, the table and
-  // grid-factor rows by bulk copies, all in flight at once on one mbarrier
+  // ---- 0. the field's tiles by bulk tensor copies, the table and grid-
+  // factor rows by bulk copies, all in flight at once on one mbarrier
   if (tid == 0) dg_mbar_init(bar, 1);
   __syncthreads();
   dg_pdl_wait();  // NL comes from the z-forward kernel
   if (tid == 0) {
     const int ctile = cc.nbox * cc.by * MT;
-    const unsigned ntiles = 2u;
+    const unsigned ntiles = 2u + (old_cf ? 1u : 0u) + (vel ? 1u : 0u);
     const int nrc = (f == 1) ? 4 : 2;  // grid-factor rows 2..5 (U2) or 0..1
     // extra_tx is 0 except in the wait test, where the barrier then never completes
     dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * ctile) * ntiles +
@@ -327,6 +355,8 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
       const int x = (int)(2 * m0), y = q * cc.by;
       dg_tma_load_2d(CUt + d, &cc.map_cu[f], x, y, bar);
       dg_tma_load_2d(NLt + d, &cc.map_nl[f], x, y, bar);
+      if (old_cf) dg_tma_load_2d(CFt + d, &cc.map_cf[f], x, y, bar);
+      if (vel) dg_tma_load_2d(CPt + d, &cc.map_cp, x, y, bar);
     }
     dg_bulk_load(TB, cc.tab + ((long)(rk_step - 1) * (3 + DG_MAX_TH) + f) * 5 * LP,
                  (unsigned)(sizeof(double) * 5 * LP), bar);
@@ -336,17 +366,16 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   const bool landed = dg_mbar_wait(bar, 0, spin);
   if (__syncthreads_or(!landed)) {
     if (tid == 0) {
-      atomicExch(cc.err + 1, 1);
+      atomicExch(err + 1, 1);
       dg_mbar_wait(bar, 0, spin);  // the copies in flight get one more bounded wait
     }
     return;
   }
 
   // ---- 1. explicit terms, CF and the right-hand side of rows lo..hi
-  const FieldCoef k = field_coef(C, cc.dscal, rk_step, f);
-  if (f == 1) rhs_tile<MT, 1>(cc, k, rk_step, m0, f, mt, CUt, NLt, RC, LP, KW);
-  else if (f < 3) rhs_tile<MT, 0>(cc, k, rk_step, m0, f, mt, CUt, NLt, RC, LP, KW);
-  else rhs_tile<MT, 2>(cc, k, rk_step, m0, f, mt, CUt, NLt, RC, LP, KW);
+  if (f == 1) rhs_tile<MT, 1>(k, rk_step, m0, f, mt, cff, CUt, NLt, CFt, CPt, RC, LP, KW);
+  else if (f < 3) rhs_tile<MT, 0>(k, rk_step, m0, f, mt, cff, CUt, NLt, CFt, CPt, RC, LP, KW);
+  else rhs_tile<MT, 2>(k, rk_step, m0, f, mt, cff, CUt, NLt, CFt, CPt, RC, LP, KW);
   __syncthreads();
 
   // ---- 2. forward recurrence g(j) = r(j) + a(j) g(j-1) over each segment
@@ -395,7 +424,6 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   __syncthreads();
   // ---- 4. g = local + product x carry, e = g / b; then the backward
   // recurrence x(j) = e(j) + f(j) x(j+1) over the segment (rows >= wlo)
-  const int wlo = (f >= 3) ? pick(C.JSt, f - 3) - 1 : 1;
   const int qb = wlo > j0 ? wlo - j0 : 0;  // first row of the segment to solve
   const bool solves = nr > 0 && qb < nr;
   double fc[SEG_K];
@@ -444,7 +472,6 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
     double2 xl[SEG_K];
 #pragma unroll
     for (int q = 0; q < SEG_K; q++) xl[q] = NLt[((q < nr) ? j0 + q : 0) * MT + m];
-    double2 *dst = cc.out[f];
     double p2 = 1.0;
 #pragma unroll
     for (int q = SEG_K - 1; q >= 0; q--) {
@@ -459,7 +486,7 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
 // The column kernel: CTA b takes work[b] = (case, mode tile, field) from
 // the case table (every case at substep rk_step with MT modes per CTA).
 template <int MT>
-__global__ void __launch_bounds__(COL_MAX_THR, 3) k_col_cn(const ColCase *__restrict__ cases,
+__global__ void __launch_bounds__(COL_MAX_THR, 2) k_col_cn(const ColCase *__restrict__ cases,
                                                        const int4 *__restrict__ work,
                                                        ColLaunch P, int rk_step, long spin,
                                                        unsigned extra_tx) {
@@ -550,7 +577,7 @@ static int col_threads(const dg_handle *h, int mt) {
 size_t dg_col_smem(const dg_handle *h, int mt) { return col_smem_l(col_sizes(h, mt), mt); }
 
 // The case description of handle h for `mt` modes per CTA (builds the
-// tensor maps of its CU and rhs arrays for that tile width).
+// tensor maps of its CU, rhs and CF arrays and CP for that tile width).
 static int fill_case(dg_handle *h, int mt, ColCase *cc) {
   const int L = h->NY + 2;
   int by = 0, nbox = 0, nseg = 0;
@@ -559,8 +586,9 @@ static int fill_case(dg_handle *h, int mt, ColCase *cc) {
   for (int f = 0; f < h->nf; f++) {
     DG_TRY(dg_tmap_planes(h->cu[f], h->ss, L, mt, by, &cc->map_cu[f]));
     DG_TRY(dg_tmap_planes(h->rhs[f], h->ss, L, mt, by, &cc->map_nl[f]));
+    DG_TRY(dg_tmap_planes(h->cf[f], h->ss, L, mt, by, &cc->map_cf[f]));
   }
-  cc->cp = h->cp;
+  DG_TRY(dg_tmap_planes(h->cp, h->ss, L, mt, by, &cc->map_cp));
   cc->C = make_col_const(h);
   cc->dscal = h->dscal;
   cc->tab = h->cn_tab;

@@ -26,12 +26,13 @@
 // of the same operations.  Segment boundaries depend only on NY, so a mode's
 // arithmetic does not depend on the tile width.
 //
-// One CTA per work item.  One thread fetches the item's inputs -- the
-// field's CU tile, the NL term the z-forward kernel left in the field's rhs
-// array, CF_old (substeps 2, 3), CP (velocity fields), by bulk tensor copies
-// (TMA, no multicast), and its table and grid-factor rows by bulk copies --
-// all at once on one mbarrier with a bounded wait.  The right-hand side is
-// formed in a flat loop over (row, mode) and replaces NL in shared memory,
+// One CTA per work item.  One thread fetches the field's CU tile and the NL
+// term the z-forward kernel left in the field's rhs array by bulk tensor
+// copies (TMA, no multicast), and the table and grid-factor rows by bulk
+// copies, all at once on one mbarrier with a bounded wait.  The right-hand
+// side is formed in a flat loop over (row, mode) -- CF_old and CP read there
+// in batches, each batch's loads issued before its stores -- and replaces
+// NL in shared memory,
 // the recurrences run there (each phase loads its rows before its chain),
 // and the post-CN field goes to the field's rhs array.  CU is read-only in
 // this kernel, so a field's right-hand side may read another field
@@ -66,10 +67,10 @@ struct ColConst {
 // Everything the column stage of one case needs, in device memory (tensor
 // maps first: 64-byte aligned).  Maps are 2-D over [plane][2 ss doubles].
 struct ColCase {
-  CUtensorMap map_cu[3 + DG_MAX_TH], map_nl[3 + DG_MAX_TH], map_cf[3 + DG_MAX_TH];
-  CUtensorMap map_cp;
+  CUtensorMap map_cu[3 + DG_MAX_TH], map_nl[3 + DG_MAX_TH];
   ColConst C;
   const double *dscal, *tab, *kxv, *kzv, *rowc;
+  const double2 *cp;
   const double2 *cu[3 + DG_MAX_TH];
   double2 *cf[3 + DG_MAX_TH], *out[3 + DG_MAX_TH];  // out: the rhs arrays
   int *err;
@@ -248,41 +249,59 @@ struct ColLaunch {
   int nwork;  // work items (CTAs)
 };
 
-// Shared memory of one CTA (128-byte aligned): the tiles CU, NL (then R, g,
-// e and x of the recurrences), CF_old and CP [tile] double2; the CN table
+// Shared memory of one CTA (128-byte aligned): the tiles CU and NL (then R,
+// g, e and x of the recurrences) [tile] double2; the CN table
 // rows TB [5][lp] (a, 1/b, f = -c/b, kind, BC value); the field's grid
 // factors RC [4][lp]; per (segment, mode) values SV [nseg][MT] double2
 // (then carries); per segment products SP [nseg]; the modes' wavenumbers
 // and k^2 (to the power BETA) KW [3][MT]; the mbarrier.
 size_t col_smem_l(const ColLaunch &P, int mt) {
-  return sizeof(double2) * (4 * (size_t)P.tile + (size_t)P.nseg * mt) +
+  return sizeof(double2) * (2 * (size_t)P.tile + (size_t)P.nseg * mt) +
          sizeof(double) * (9 * (size_t)P.lp + (size_t)P.nseg + 3 * (size_t)mt) + 8 + 128;
 }
 
 // The right-hand side of field f (kind FK: 0 U1/U3, 1 U2, 2 scalar) for the
-// CTA's rows lo..hi, all from the staged tiles: one element (row, mode) per
-// step of a flat loop over the CTA's threads; R replaces NL.  The loop's
-// only global accesses are the CF stores and, with couplings, the other
-// fields' CU: everything else it reads is in registers or shared memory.
+// CTA's rows lo..hi: a flat loop over (row, mode) elements in batches of
+// four per thread; CU and NL from the staged tiles, CF_old and CP read
+// directly (each element once, coalesced).  CF_old is the array the loop
+// writes CF into, so a batch's loads are all issued before its stores; CP
+// is read-only here and goes through the read-only data path.  R replaces
+// NL.  Everything else the loop reads is in registers or shared memory.
 template <int MT, int FK>
 __device__ __forceinline__ void rhs_tile(const FieldCoef &k, int rk_step, long m0, int f, int mt,
-                                         double2 *cff, const double2 *CUt, double2 *NLt,
-                                         const double2 *CFt, const double2 *CPt,
-                                         const double *RC, int LP, const double *KW) {
+                                         double2 *cff, const double2 *cpp, const double2 *CUt,
+                                         double2 *NLt, const double *RC, int LP,
+                                         const double *KW) {
   const bool old_cf = rk_step > 1;
   const int nthr = blockDim.x;
-#pragma unroll 4
-  for (int i = k.lo * MT + (int)threadIdx.x; i < (k.hi + 1) * MT; i += nthr) {
-    const int j = i / MT, m = i - j * MT;
-    if (m >= mt) continue;
-    const long mg = m0 + m;
-    const long o = (long)j * k.ss + mg;
-    double2 fv, rr;
-    rhs_row<FK>(k, f, j, o, mg == 0, KW[m], KW[MT + m], KW[2 * MT + m], RC, LP, CUt[i],
-                CUt[i - MT], CUt[i + MT], NLt[i], old_cf ? CFt[i] : z2(),
-                (FK < 2) ? CPt[i] : z2(), (FK == 1) ? CPt[i - MT] : z2(), fv, rr);
-    cff[o] = fv;
-    NLt[i] = rr;
+  const int i0 = k.lo * MT + (int)threadIdx.x, iend = (k.hi + 1) * MT;
+  constexpr int B = 4;
+  for (int base = i0; base < iend; base += B * nthr) {
+    double2 old[B], p0[B], pm[B];
+#pragma unroll
+    for (int u = 0; u < B; u++) {
+      const int i = base + u * nthr;
+      const int j = i / MT, m = i - j * MT;
+      const bool ok = i < iend && m < mt;
+      const long o = (long)j * k.ss + m0 + m;
+      old[u] = (ok && old_cf) ? cff[o] : z2();
+      p0[u] = (ok && FK < 2) ? __ldg(cpp + o) : z2();
+      pm[u] = (ok && FK == 1) ? __ldg(cpp + o - k.ss) : z2();
+    }
+#pragma unroll
+    for (int u = 0; u < B; u++) {
+      const int i = base + u * nthr;
+      const int j = i / MT, m = i - j * MT;
+      if (i < iend && m < mt) {
+        const long mg = m0 + m;
+        const long o = (long)j * k.ss + mg;
+        double2 fv, rr;
+        rhs_row<FK>(k, f, j, o, mg == 0, KW[m], KW[MT + m], KW[2 * MT + m], RC, LP, CUt[i],
+                    CUt[i - MT], CUt[i + MT], NLt[i], old[u], p0[u], pm[u], fv, rr);
+        cff[o] = fv;
+        NLt[i] = rr;
+      }
+    }
   }
 }
 
@@ -313,15 +332,15 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   const int nseg = cc.nseg;
   const long ss = cc.C.ss;
   const int mt = (int)((ss - m0) < MT ? (ss - m0) : MT);
-  const bool vel = f < 3, old_cf = rk_step > 1;
   const int wlo = (f >= 3) ? pick(cc.C.JSt, f - 3) - 1 : 1;  // first row solved
   double2 *const dst = cc.out[f];
   double2 *const cff = cc.cf[f];
   int *const err = cc.err;
   const FieldCoef k = field_coef(cc, rk_step, f);
   double2 *CUt = reinterpret_cast<double2 *>(sbase);
-  double2 *NLt = CUt + P.tile, *CFt = NLt + P.tile, *CPt = CFt + P.tile;
-  double *TB = reinterpret_cast<double *>(CPt + P.tile);
+  double2 *NLt = CUt + P.tile;
+  double *TB = reinterpret_cast<double *>(NLt + P.tile);
+  const double2 *const cpp = cc.cp;
   double *RC = TB + 5 * P.lp;  // the slots are sized for the largest case
   double2 *SV = reinterpret_cast<double2 *>(RC + 4 * P.lp);
   double *SP = reinterpret_cast<double *>(SV + P.nseg * MT);
@@ -344,7 +363,7 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   dg_pdl_wait();  // NL comes from the z-forward kernel
   if (tid == 0) {
     const int ctile = cc.nbox * cc.by * MT;
-    const unsigned ntiles = 2u + (old_cf ? 1u : 0u) + (vel ? 1u : 0u);
+    const unsigned ntiles = 2u;
     const int nrc = (f == 1) ? 4 : 2;  // grid-factor rows 2..5 (U2) or 0..1
     // extra_tx is 0 except in the wait test, where the barrier then never completes
     dg_mbar_expect_tx(bar, (unsigned)(sizeof(double2) * ctile) * ntiles +
@@ -355,8 +374,6 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
       const int x = (int)(2 * m0), y = q * cc.by;
       dg_tma_load_2d(CUt + d, &cc.map_cu[f], x, y, bar);
       dg_tma_load_2d(NLt + d, &cc.map_nl[f], x, y, bar);
-      if (old_cf) dg_tma_load_2d(CFt + d, &cc.map_cf[f], x, y, bar);
-      if (vel) dg_tma_load_2d(CPt + d, &cc.map_cp, x, y, bar);
     }
     dg_bulk_load(TB, cc.tab + ((long)(rk_step - 1) * (3 + DG_MAX_TH) + f) * 5 * LP,
                  (unsigned)(sizeof(double) * 5 * LP), bar);
@@ -373,9 +390,9 @@ __device__ __forceinline__ void col_body(const ColCase &cc, int rk_step, long m0
   }
 
   // ---- 1. explicit terms, CF and the right-hand side of rows lo..hi
-  if (f == 1) rhs_tile<MT, 1>(k, rk_step, m0, f, mt, cff, CUt, NLt, CFt, CPt, RC, LP, KW);
-  else if (f < 3) rhs_tile<MT, 0>(k, rk_step, m0, f, mt, cff, CUt, NLt, CFt, CPt, RC, LP, KW);
-  else rhs_tile<MT, 2>(k, rk_step, m0, f, mt, cff, CUt, NLt, CFt, CPt, RC, LP, KW);
+  if (f == 1) rhs_tile<MT, 1>(k, rk_step, m0, f, mt, cff, cpp, CUt, NLt, RC, LP, KW);
+  else if (f < 3) rhs_tile<MT, 0>(k, rk_step, m0, f, mt, cff, cpp, CUt, NLt, RC, LP, KW);
+  else rhs_tile<MT, 2>(k, rk_step, m0, f, mt, cff, cpp, CUt, NLt, RC, LP, KW);
   __syncthreads();
 
   // ---- 2. forward recurrence g(j) = r(j) + a(j) g(j-1) over each segment
@@ -577,7 +594,7 @@ static int col_threads(const dg_handle *h, int mt) {
 size_t dg_col_smem(const dg_handle *h, int mt) { return col_smem_l(col_sizes(h, mt), mt); }
 
 // The case description of handle h for `mt` modes per CTA (builds the
-// tensor maps of its CU, rhs and CF arrays and CP for that tile width).
+// tensor maps of its CU and rhs arrays for that tile width).
 static int fill_case(dg_handle *h, int mt, ColCase *cc) {
   const int L = h->NY + 2;
   int by = 0, nbox = 0, nseg = 0;
@@ -586,9 +603,8 @@ static int fill_case(dg_handle *h, int mt, ColCase *cc) {
   for (int f = 0; f < h->nf; f++) {
     DG_TRY(dg_tmap_planes(h->cu[f], h->ss, L, mt, by, &cc->map_cu[f]));
     DG_TRY(dg_tmap_planes(h->rhs[f], h->ss, L, mt, by, &cc->map_nl[f]));
-    DG_TRY(dg_tmap_planes(h->cf[f], h->ss, L, mt, by, &cc->map_cf[f]));
   }
-  DG_TRY(dg_tmap_planes(h->cp, h->ss, L, mt, by, &cc->map_cp));
+  cc->cp = h->cp;
   cc->C = make_col_const(h);
   cc->dscal = h->dscal;
   cc->tab = h->cn_tab;

@@ -791,7 +791,9 @@ auto xrow_kernel(int v) {
 // shared buffer, the row maxima reduced across the warp, and each warp's
 // min over the three components of CFL d / max|u| folded into the shared
 // minimum (division is correctly rounded and monotone, so only the largest
-// |u| of a row is divided).  Input: the z-inverse output H (kx = 0..NX/3).
+// |u| of a row is divided), the CTA's warps reduced in shared memory and
+// folded into the minimum once per CTA.  Input: the z-inverse output H
+// (kx = 0..NX/3).
 template <int NX, int PV>
 __global__ void __launch_bounds__(32 * XW_WARPS) k_cfl_w(const double2 *__restrict__ H, long Hfield,
                                                         int jmin, int NZ,
@@ -808,9 +810,11 @@ __global__ void __launch_bounds__(32 * XW_WARPS) k_cfl_w(const double2 *__restri
   for (int i = threadIdx.x; i < NX; i += blockDim.x) stw[i] = tw[i];
   dg_pdl_wait();
   __syncthreads();
-  const int z = blockIdx.x * XW_WARPS + warp;
+  __shared__ double wbest[XW_WARPS];
+  const int z0 = blockIdx.x * XW_WARPS + warp;
+  const bool zok = z0 < NZ;
+  const int z = zok ? z0 : NZ - 1;  // a spare warp repeats the last row
   const int j = jmin + blockIdx.y;
-  if (z >= NZ) return;
   const double2 *row = H + (long)j * NZ * NKXP + (long)z * NKXP;
 #pragma unroll
   for (int q = 0; q < 2; q++) {
@@ -849,10 +853,14 @@ __global__ void __launch_bounds__(32 * XW_WARPS) k_cfl_w(const double2 *__restri
     b2 = fmax(b2, __shfl_xor_sync(0xffffffffu, b2, o));
     b3 = fmax(b3, __shfl_xor_sync(0xffffffffu, b3, o));
   }
-  if (lane == 0) {
-    // +inf for an all-zero row, as the reference's division gives
-    const double best = fmin(fmin(cfl * dxv / b1, cfl * dy[j] / b2), cfl * dzv / b3);
-    atomicMin(out, (unsigned long long)__double_as_longlong(best));
+  // +inf for an all-zero row, as the reference's division gives
+  if (lane == 0) wbest[warp] = fmin(fmin(cfl * dxv / b1, cfl * dy[j] / b2), cfl * dzv / b3);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double best = wbest[0];
+#pragma unroll
+    for (int w = 1; w < XW_WARPS; w++) best = fmin(best, wbest[w]);
+    dg_fold_min(out, best);
   }
 }
 
@@ -1766,11 +1774,6 @@ __global__ void k_bc_vel(BcVel B, long ss, const double *__restrict__ dy,
 }
 
 // ------------------------------------------------------------- COURANT
-__device__ __forceinline__ void atomic_min_pos(unsigned long long *addr, double v) {
-  // v >= 0 or +inf: the IEEE bit patterns order like unsigned integers
-  atomicMin(addr, (unsigned long long)__double_as_longlong(v));
-}
-
 __global__ void k_cfl_min(const double *__restrict__ phys, long pfield, int NY, int NZ, int NX,
                           double cfl, double dxv, double dzv, const double *__restrict__ dy,
                           unsigned long long *__restrict__ out) {
@@ -1787,7 +1790,7 @@ __global__ void k_cfl_min(const double *__restrict__ phys, long pfield, int NY, 
     best = fmin(best, fmin(a, fmin(b, c)));
   }
   for (int off = 16; off > 0; off >>= 1) best = fmin(best, __shfl_down_sync(0xffffffffu, best, off));
-  if ((threadIdx.x & 31) == 0) atomic_min_pos(out, best);
+  if ((threadIdx.x & 31) == 0) dg_fold_min(out, best);
 }
 
 __global__ void k_dt_update(double *dscal, const unsigned long long *minbits, double dt0) {

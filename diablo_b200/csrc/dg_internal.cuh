@@ -316,6 +316,14 @@ __device__ __forceinline__ void dg_bulk_load(void *dst, const void *src, unsigne
 __device__ __forceinline__ void dg_fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
+// Folds v >= 0 (or +inf) into the running minimum at *out (the IEEE bit
+// patterns of non-negative doubles order like unsigned integers).  The atomic
+// runs only when v could lower the stored value: a reduction whose CTAs all
+// fold into one address would otherwise serialise on it.
+__device__ __forceinline__ void dg_fold_min(unsigned long long *out, double v) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  if (b < *reinterpret_cast<volatile unsigned long long *>(out)) atomicMin(out, b);
+}
 // true once phase `parity` of the barrier completed; false after `spin` polls
 __device__ __forceinline__ bool dg_mbar_wait(unsigned long long *bar, unsigned parity,
                                              long spin = DG_ASYNC_SPIN) {

@@ -274,9 +274,15 @@ __global__ void __launch_bounds__(NTHR) k_xc2r_cfl(const double2 *__restrict__ H
     if (zb < NZ) big = fmax(big, fabs(v.y));
   }
   for (int off = 16; off > 0; off >>= 1) big = fmax(big, __shfl_down_sync(0xffffffffu, big, off));
-  if ((tid & 31) == 0) {
-    const double best = cfl * d / big;  // +inf for an all-zero slab, as before
-    atomicMin(out, (unsigned long long)__double_as_longlong(best));
+  // the CTA's warps reduced in shared memory, folded into the minimum once
+  __shared__ double wbig[NTHR / 32];
+  if ((tid & 31) == 0) wbig[tid >> 5] = big;
+  __syncthreads();
+  if (tid == 0) {
+    double m = wbig[0];
+#pragma unroll
+    for (int w = 1; w < NTHR / 32; w++) m = fmax(m, wbig[w]);
+    dg_fold_min(out, cfl * d / m);  // +inf for an all-zero slab, as before
   }
 }
 

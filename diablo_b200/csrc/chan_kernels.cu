@@ -1476,7 +1476,7 @@ size_t rd_smem(int L, int nseg, int mt) {
 }
 
 template <int MT>
-__global__ void __launch_bounds__(RD_MAX_THR, 2) k_rd_col(RdArgs A) {
+__global__ void __launch_bounds__(RD_MAX_THR, 3) k_rd_col(RdArgs A) {
   extern __shared__ double2 rsm[];
   const int NY = A.NY, L = NY + 2, nseg = A.nseg;
   const long ss = A.ss;
@@ -1623,51 +1623,34 @@ __global__ void __launch_bounds__(RD_MAX_THR, 2) k_rd_col(RdArgs A) {
     }
   }
   __syncthreads();
-  // ---- 4. the projection, phi and CP += phi / H_BAR (rows 1..NY), in
-  // batches of four elements per thread: the velocity and CP arrays are read
-  // and written here (the same arrays when projecting in place), so each
-  // batch's loads are issued before its stores
+  // ---- 4. the projection, phi and CP += phi / H_BAR (rows 1..NY)
   const double ihh = (A.rk_step > 0) ? 1.0 / A.dscal[1 + A.rk_step] : 1.0;
-  constexpr int PB = 4;
-  for (int base = MT + tid; base < (NY + 1) * MT; base += PB * nthr) {
-    double2 a1[PB], a3[PB], b2[PB], pc[PB];
-#pragma unroll
-    for (int u = 0; u < PB; u++) {
-      const int i = base + u * nthr;
-      const int j = i / MT, mm = i - j * MT;
-      const bool ok = i < (NY + 1) * MT && mm < mt;
-      const long o = (long)j * ss + m0 + mm;
-      a1[u] = ok ? A.s1[o] : make_double2(0.0, 0.0);
-      a3[u] = ok ? A.s3[o] : make_double2(0.0, 0.0);
-      b2[u] = (ok && j >= 2) ? A.s2[o] : make_double2(0.0, 0.0);
-      pc[u] = (ok && A.rk_step > 0 && j >= A.JS && j <= A.JE) ? A.cp[o] : make_double2(0.0, 0.0);
+  for (int i = MT + tid; i < (NY + 1) * MT; i += nthr) {
+    const int j = i / MT, mm = i - j * MT;
+    if (mm >= mt) continue;
+    const long o = (long)j * ss + m0 + mm;
+    const double KX = KXS[mm], KZ = KZS[mm];
+    const double2 ph = PH[i];
+    double2 a1 = A.s1[o], a3 = A.s3[o];
+    // U1 -= i kx phi, U3 -= i kz phi
+    a1.x -= -KX * ph.y; a1.y -= KX * ph.x;
+    a3.x -= -KZ * ph.y; a3.y -= KZ * ph.x;
+    A.u1[o] = a1;
+    A.u3[o] = a3;
+    if (j >= 2) {
+      // U2(j) -= (phi(j) - phi(j-1)) / DY(j)
+      double2 b2 = A.s2[o];
+      const double2 pm = PH[i - MT];
+      b2.x -= (ph.x - pm.x) * IDY[j];
+      b2.y -= (ph.y - pm.y) * IDY[j];
+      A.u2[o] = b2;
     }
-#pragma unroll
-    for (int u = 0; u < PB; u++) {
-      const int i = base + u * nthr;
-      const int j = i / MT, mm = i - j * MT;
-      if (i >= (NY + 1) * MT || mm >= mt) continue;
-      const long o = (long)j * ss + m0 + mm;
-      const double KX = KXS[mm], KZ = KZS[mm];
-      const double2 ph = PH[i];
-      // U1 -= i kx phi, U3 -= i kz phi
-      a1[u].x -= -KX * ph.y; a1[u].y -= KX * ph.x;
-      a3[u].x -= -KZ * ph.y; a3[u].y -= KZ * ph.x;
-      A.u1[o] = a1[u];
-      A.u3[o] = a3[u];
-      if (j >= 2) {
-        // U2(j) -= (phi(j) - phi(j-1)) / DY(j)
-        const double2 pm = PH[i - MT];
-        b2[u].x -= (ph.x - pm.x) * IDY[j];
-        b2[u].y -= (ph.y - pm.y) * IDY[j];
-        A.u2[o] = b2[u];
-      }
-      A.phi[o] = ph;
-      if (A.rk_step > 0 && j >= A.JS && j <= A.JE) {
-        pc[u].x = pc[u].x + ph.x * ihh;
-        pc[u].y = pc[u].y + ph.y * ihh;
-        A.cp[o] = pc[u];
-      }
+    A.phi[o] = ph;
+    if (A.rk_step > 0 && j >= A.JS && j <= A.JE) {
+      double2 pc = A.cp[o];
+      pc.x = pc.x + ph.x * ihh;
+      pc.y = pc.y + ph.y * ihh;
+      A.cp[o] = pc;
     }
   }
   if (A.s1 == A.u1) return;

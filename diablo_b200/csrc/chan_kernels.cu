@@ -784,117 +784,6 @@ auto xrow_kernel(int v) {
   return k_xrow_w<NX, NTH, CX, 0>;
 }
 
-// ------------------------------------------------------- COURANT, warp rows
-// COURANT's maxima |U1|, |U2|, |U3| over physical planes jmin.. (for/
-// courant.f:35-60), one warp per z-row as in k_xrow_w's plane loads: U1 + i U2
-// and U3 packed into two complex transforms, the pruned x c2r in the warp's
-// shared buffer, the row maxima reduced across the warp, and each warp's
-// min over the three components of CFL d / max|u| folded into the shared
-// minimum (division is correctly rounded and monotone, so only the largest
-// |u| of a row is divided), the CTA's warps reduced in shared memory and
-// folded into the minimum once per CTA.  Input: the z-inverse output H
-// (kx = 0..NX/3).
-template <int NX, int PV>
-__global__ void __launch_bounds__(32 * XW_WARPS) k_cfl_w(const double2 *__restrict__ H, long Hfield,
-                                                        int jmin, int NZ,
-                                                        const double2 *__restrict__ tw, double cfl,
-                                                        double dxv, double dzv,
-                                                        const double *__restrict__ dy,
-                                                        unsigned long long *__restrict__ out) {
-  constexpr int NKXP = NX / 3 + 1;
-  constexpr int SSTR = padded_len(NX);
-  extern __shared__ double2 sm_raw[];
-  double2 *stw = sm_raw;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double2 *buf = stw + NX + warp * 2 * SSTR;
-  for (int i = threadIdx.x; i < NX; i += blockDim.x) stw[i] = tw[i];
-  dg_pdl_wait();
-  __syncthreads();
-  __shared__ double wbest[XW_WARPS];
-  const int z0 = blockIdx.x * XW_WARPS + warp;
-  const bool zok = z0 < NZ;
-  const int z = zok ? z0 : NZ - 1;  // a spare warp repeats the last row
-  const int j = jmin + blockIdx.y;
-  const double2 *row = H + (long)j * NZ * NKXP + (long)z * NKXP;
-#pragma unroll
-  for (int q = 0; q < 2; q++) {
-    const int fa = 2 * q, fb = 2 * q + 1;
-#pragma unroll
-    for (int i = 0; i < (NX + 31) / 32; i++) {
-      const int k = lane + 32 * i;
-      const int kk = (k <= NX / 2) ? k : NX - k;
-      // bins above NX/3 (the truncated band) are zero: the pruned first pass
-      // does not read them
-      if (k < NX && kk < NKXP && kk < NX / 2) {
-        double2 a = row[fa * Hfield + kk];
-        double2 bb = (fb < 3) ? row[fb * Hfield + kk] : make_double2(0.0, 0.0);
-        if (kk == 0) { a.y = 0.0; bb.y = 0.0; }
-        buf[q * SSTR + pad(k)] = (k == kk) ? make_double2(a.x - bb.y, a.y + bb.x)
-                                           : make_double2(a.x + bb.y, -a.y + bb.x);
-      }
-    }
-  }
-  __syncwarp();
-  wpasses_pz<NX, +1, PV>(buf, 2, SSTR, stw, lane);
-  double b1 = 0.0, b2 = 0.0, b3 = 0.0;
-#pragma unroll
-  for (int i = 0; i < (NX + 31) / 32; i++) {
-    const int x = lane + 32 * i;
-    if (x < NX) {
-      const double2 v0 = buf[pad(x)], v1 = buf[SSTR + pad(x)];
-      b1 = fmax(b1, fabs(v0.x));
-      b2 = fmax(b2, fabs(v0.y));
-      b3 = fmax(b3, fabs(v1.x));
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    b1 = fmax(b1, __shfl_xor_sync(0xffffffffu, b1, o));
-    b2 = fmax(b2, __shfl_xor_sync(0xffffffffu, b2, o));
-    b3 = fmax(b3, __shfl_xor_sync(0xffffffffu, b3, o));
-  }
-  // +inf for an all-zero row, as the reference's division gives
-  if (lane == 0) wbest[warp] = fmin(fmin(cfl * dxv / b1, cfl * dy[j] / b2), cfl * dzv / b3);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double best = wbest[0];
-#pragma unroll
-    for (int w = 1; w < XW_WARPS; w++) best = fmin(best, wbest[w]);
-    dg_fold_min(out, best);
-  }
-}
-
-template <int NX>
-auto cfl_kernel(int v) {
-  if constexpr (plan_has_variant(NX))
-    if (v) return k_cfl_w<NX, 1>;
-  return k_cfl_w<NX, 0>;
-}
-
-// COURANT's reduction over planes jmin..jmax of H: the warp-row kernel for
-// the warp x lengths, the CTA-row kernel otherwise
-static int cfl_planes(dg_handle *h, int jmin, int jmax) {
-  if (!xw_supported(h->NX)) return dg_xc2r_cfl(h, h->H, jmin, jmax, h->dmin_bits);
-  const long Hf = (long)h->nplanes * h->NZ * h->nkxp;
-  const double dxv = h->p.lx / h->NX, dzv = h->p.lz / h->NZ;
-  const size_t sm = sizeof(double2) * (h->NX + XW_WARPS * 2 * padded_len(h->NX));
-  dim3 grid(dg_cdiv(h->NZ, XW_WARPS), jmax - jmin + 1);
-  bool done = false;
-#define CFL_CASE(NXV)                                                                           \
-  if (!done && h->NX == NXV) {                                                                  \
-    auto kern = cfl_kernel<NXV>(h->fft_plan);                                                   \
-    dg_big_smem((const void *)kern);                                                            \
-    dg_kt_begin(h, "k_cfl_w", h->st);                                                           \
-    DG_CUDA(dg_launch(0, kern, grid, dim3(32 * XW_WARPS), sm, h->st, (const double2 *)h->H, Hf, \
-                      jmin, h->NZ, h->twx, h->p.cfl, dxv, dzv, h->dy, h->dmin_bits));           \
-    done = true;                                                                                \
-  }
-  CFL_CASE(16) CFL_CASE(32) CFL_CASE(48) CFL_CASE(64) CFL_CASE(96) CFL_CASE(128) CFL_CASE(256)
-#undef CFL_CASE
-  DG_LAUNCHED();
-  return DG_OK;
-}
-
 // ------------------------------------------------------------- zfwd + rhs
 constexpr int ZF_THR = 128;
 __host__ __device__ constexpr int zf_kxg(int nz) { return nz <= 128 ? 8 : (nz <= 256 ? 4 : 2); }
@@ -2047,7 +1936,7 @@ int dg_courant_dev(dg_handle *h, const double2 *const *u, bool side) {
   }
   auto reduce = [&]() -> int {
     DG_CUDA(cudaMemsetAsync(h->dmin_bits, 0x7f, sizeof(unsigned long long), h->st));
-    DG_TRY(cfl_planes(h, 1, h->NY));
+    DG_TRY(dg_xc2r_cfl(h, h->H, 1, h->NY, h->dmin_bits));
     dg_kt_begin(h, "k_dt_update", h->st);
     k_dt_update<<<1, 1, 0, h->st>>>(h->dscal, h->dmin_bits, courant_dt0(h));
     DG_LAUNCHED();

@@ -500,7 +500,7 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? (sizeof(CX) == 8 ? 4
   CX *buf = stw + NX + warp * MAXP * SSTR;
   // carried x-spectra: 0 fl1, 1 fl3, 2 ubar1 u2, 3 ubar3 u2, 4 g, 5+n flth
   CX *pvs = stw + NX + XW_WARPS * MAXP * SSTR + warp * (5 + NTH) * NKXP;
-  for (int i = threadIdx.x; i < NX; i += blockDim.x) stw[i] = tw[i];
+  stage_tw<NX, PV, tp_ok(NX)>(stw, tw, NX, threadIdx.x, blockDim.x);
   dg_pdl_wait();  // H comes from the z inverse
   __syncthreads();
   const int z = blockIdx.x * XW_WARPS + warp;
@@ -550,7 +550,7 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? (sizeof(CX) == 8 ? 4
     }
     __syncwarp();
     static_assert(NKXP - 1 == NX / 3, "the truncated band of the pruned pass is NX/3 + 1 ..");
-    wpasses_pz<NX, +1, PV>(buf, NPIN, SSTR, stw, lane);
+    wpasses_pz<NX, +1, PV, tp_ok(NX)>(buf, NPIN, SSTR, stw, lane);
 #pragma unroll
     for (int q = 0; q < NPIN; q++)
 #pragma unroll
@@ -666,7 +666,7 @@ __global__ void __launch_bounds__(32 * XW_WARPS, NTH == 0 ? (sizeof(CX) == 8 ? 4
     }
     }
     __syncwarp();
-    wpasses<NX, -1, 0, PV>(buf, NPP, SSTR, stw, lane);
+    wpasses<NX, -1, 0, PV, tp_ok(NX)>(buf, NPP, SSTR, stw, lane);
     const bool out = (j >= j0);
     const T d2 = (T)2 * dyf_j, dyj = dy[j];
     const T id2 = (T)1 / d2, idyj = (T)1 / dyj;  // per plane: multiply in the row loop
@@ -1004,7 +1004,7 @@ __global__ void __launch_bounds__(128, zw_minb(NZ, sizeof(CX))) k_zfwd_w(
   const int jlo = (f == 0 || f == 2) ? C.JS : (f == 1 ? 2 : sel(C.JSt, f - 3));
   const int jhi = (f == 0 || f == 2) ? C.JE : (f == 1 ? C.NY : sel(C.JEt, f - 3));
   if (j < jlo || j > jhi) return;
-  for (int i = threadIdx.x; i < NZ; i += blockDim.x) stw[i] = tw[i];
+  stage_tw<NZ, PV, tp_ok(NZ)>(stw, tw, NZ, threadIdx.x, blockDim.x);
   dg_pdl_wait();  // G comes from the x-row kernel
   const CX *GA = G + (2 * f) * Gfield + (long)j * NZ * nkxp;
   const CX *GB = G + (2 * f + 1) * Gfield + (long)j * NZ * nkxp;
@@ -1028,7 +1028,7 @@ __global__ void __launch_bounds__(128, zw_minb(NZ, sizeof(CX))) k_zfwd_w(
   }
   __syncthreads();
   CX *wb = buf + warp * 2 * KPW * SSTR;
-  wpasses_any<NZ, -1, 0, PV>(wb, 2 * KPW, SSTR, stw, lane);
+  wpasses_any<NZ, -1, 0, PV, tp_ok(NZ)>(wb, 2 * KPW, SSTR, stw, lane);
   __syncthreads();  // the epilogue below reads every warp's columns
 
   const double h = dscal[1 + rk_step];
@@ -1391,6 +1391,20 @@ __global__ void __launch_bounds__(RD_MAX_THR, 3) k_rd_col(RdArgs A) {
   }
   dg_pdl_wait();  // the velocity comes from the CN solve
   __syncthreads();
+  // The loops below read the velocity and CP and write the velocity, phi
+  // and CP, in place when projecting on its own.  Every store depends on the
+  // load of the same element in the same iteration, so the stores cannot move
+  // above those loads, and the loads of later elements may be issued early:
+  // the pointers are declared non-aliasing for that.
+  const double2 *__restrict__ s1 = A.s1;
+  const double2 *__restrict__ s2 = A.s2;
+  const double2 *__restrict__ s3 = A.s3;
+  double2 *__restrict__ u1 = A.u1;
+  double2 *__restrict__ u2 = A.u2;
+  double2 *__restrict__ u3 = A.u3;
+  const double2 *__restrict__ cpin = A.cp;
+  double2 *__restrict__ cpout = A.cp;
+  double2 *__restrict__ phio = A.phi;
   // ---- 1. the divergence (rows 2..NY-1; rows 1 and NY have a zero
   // right-hand side)
   for (int i = MT + tid; i < (NY + 1) * MT; i += nthr) {
@@ -1398,7 +1412,7 @@ __global__ void __launch_bounds__(RD_MAX_THR, 3) k_rd_col(RdArgs A) {
     double2 r = make_double2(0.0, 0.0);
     if (m < mt && j >= 2 && j < NY) {
       const long o = (long)j * ss + m0 + m;
-      const double2 a1 = A.s1[o], a3 = A.s3[o], b2 = A.s2[o], b2p = A.s2[o + ss];
+      const double2 a1 = s1[o], a3 = s3[o], b2 = s2[o], b2p = s2[o + ss];
       const double KX = KXS[m], KZ = KZS[m];
       const double id = IDYF[j];
       r.x = (-KX * a1.y) + (b2p.x - b2.x) * id + (-KZ * a3.y);
@@ -1514,32 +1528,35 @@ __global__ void __launch_bounds__(RD_MAX_THR, 3) k_rd_col(RdArgs A) {
   __syncthreads();
   // ---- 4. the projection, phi and CP += phi / H_BAR (rows 1..NY)
   const double ihh = (A.rk_step > 0) ? 1.0 / A.dscal[1 + A.rk_step] : 1.0;
+  const bool rkc = A.rk_step > 0;
+  const int JS = A.JS, JE = A.JE;
+#pragma unroll 4
   for (int i = MT + tid; i < (NY + 1) * MT; i += nthr) {
     const int j = i / MT, mm = i - j * MT;
     if (mm >= mt) continue;
     const long o = (long)j * ss + m0 + mm;
     const double KX = KXS[mm], KZ = KZS[mm];
     const double2 ph = PH[i];
-    double2 a1 = A.s1[o], a3 = A.s3[o];
+    double2 a1 = s1[o], a3 = s3[o];
     // U1 -= i kx phi, U3 -= i kz phi
     a1.x -= -KX * ph.y; a1.y -= KX * ph.x;
     a3.x -= -KZ * ph.y; a3.y -= KZ * ph.x;
-    A.u1[o] = a1;
-    A.u3[o] = a3;
+    u1[o] = a1;
+    u3[o] = a3;
     if (j >= 2) {
       // U2(j) -= (phi(j) - phi(j-1)) / DY(j)
-      double2 b2 = A.s2[o];
+      double2 b2 = s2[o];
       const double2 pm = PH[i - MT];
       b2.x -= (ph.x - pm.x) * IDY[j];
       b2.y -= (ph.y - pm.y) * IDY[j];
-      A.u2[o] = b2;
+      u2[o] = b2;
     }
-    A.phi[o] = ph;
-    if (A.rk_step > 0 && j >= A.JS && j <= A.JE) {
-      double2 pc = A.cp[o];
+    phio[o] = ph;
+    if (rkc && j >= JS && j <= JE) {
+      double2 pc = cpin[o];
       pc.x = pc.x + ph.x * ihh;
       pc.y = pc.y + ph.y * ihh;
-      A.cp[o] = pc;
+      cpout[o] = pc;
     }
   }
   if (A.s1 == A.u1) return;

@@ -377,7 +377,9 @@ __host__ __device__ constexpr bool warp_fft_ok(int n) {
   return n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 256;
 }
 
-template <int N, int R, int NS, int SIGN, typename C>
+// TP: tw is this pass's slice of the per-pass twiddle table (build_twp),
+// indexed r NS + k, instead of the plain table indexed r k N/(NS R).
+template <int N, int R, int NS, int SIGN, bool TP = false, typename C>
 __device__ __forceinline__ void wpass(C *__restrict__ buf, int nsig, int sstr,
                                       const C *__restrict__ tw, int lane) {
   constexpr int NB = N / R;
@@ -396,7 +398,7 @@ __device__ __forceinline__ void wpass(C *__restrict__ buf, int nsig, int sstr,
       for (int r = 0; r < R; r++) {
         C x = in[pad(b + r * NB)];
         if (NS > 1 && r > 0) {
-          C t = tw[r * k * TMUL];
+          C t = TP ? tw[r * NS + k] : tw[r * k * TMUL];
           if (SIGN > 0) t.y = -t.y;
           x = cmul(x, t);
         }
@@ -414,13 +416,54 @@ __device__ __forceinline__ void wpass(C *__restrict__ buf, int nsig, int sstr,
   }
 }
 
-template <int N, int SIGN, int P, int V = 0, typename C>
+// Per-pass twiddle table of a compile-time plan: for every pass p >= 1
+// (radix R_p, running span NS_p) the R_p x NS_p factors W^(r k N/(NS_p R_p)),
+// k fastest.  The lanes of a warp pass take consecutive k, so they read
+// consecutive entries; indexing the plain table by r k N/(NS R) strides it
+// and conflicts in the shared-memory banks.  Same values as the plain
+// table: results do not change.
+template <int N, int V>
+__host__ __device__ constexpr int twp_off(int p) {
+  int o = 0;
+  for (int q = 1; q < p; q++) o += plan_radix(N, q, V) * plan_ns(N, q, V);
+  return o;
+}
+template <int N, int V>
+__host__ __device__ constexpr int twp_len() { return twp_off<N, V>(plan_passes(N)); }
+// lengths whose warp passes take the per-pass table in the space of the plain one
+__host__ __device__ constexpr bool tp_ok(int N) {
+  return N == 16 || N == 32 || N == 48 || N == 64 || N == 128 || N == 256;
+}
+template <int N, int V = 0, typename C>
+__device__ __forceinline__ void build_twp(C *twp, const C *__restrict__ tw, int tid, int nthr) {
+  static_assert(twp_len<N, V>() <= N, "per-pass table longer than the plain one");
+  for (int i = tid; i < twp_len<N, V>(); i += nthr) {
+    int p = 1;
+    while (i >= twp_off<N, V>(p + 1)) p++;
+    const int R = plan_radix(N, p, V), NS = plan_ns(N, p, V);
+    const int e = i - twp_off<N, V>(p);
+    const int r = e / NS, k = e - r * NS;
+    twp[i] = tw[r * k * (N / (NS * R))];
+  }
+}
+// the twiddles a kernel stages: the per-pass table where its warp passes
+// take one (TP), the plain table otherwise
+template <int N, int V, bool TP, typename C>
+__device__ __forceinline__ void stage_tw(C *stw, const C *__restrict__ tw, int n, int tid,
+                                         int nthr) {
+  if constexpr (TP) build_twp<N, V>(stw, tw, tid, nthr);
+  else
+    for (int i = tid; i < n; i += nthr) stw[i] = tw[i];
+}
+
+template <int N, int SIGN, int P, int V = 0, bool TP = false, typename C>
 __device__ __forceinline__ void wpasses(C *buf, int nsig, int sstr, const C *tw,
                                         int lane) {
   constexpr int R = plan_radix(N, P, V);
   if constexpr (R != 0) {
-    wpass<N, R, plan_ns(N, P, V), SIGN>(buf, nsig, sstr, tw, lane);
-    wpasses<N, SIGN, P + 1, V>(buf, nsig, sstr, tw, lane);
+    wpass<N, R, plan_ns(N, P, V), SIGN, TP>(buf, nsig, sstr, TP ? tw + twp_off<N, V>(P) : tw,
+                                            lane);
+    wpasses<N, SIGN, P + 1, V, TP>(buf, nsig, sstr, tw, lane);
   }
 }
 
@@ -428,7 +471,7 @@ __device__ __forceinline__ void wpasses(C *buf, int nsig, int sstr, const C *tw,
 // butterflies l, l + 32, ... of one signal at a time, all loaded before the
 // __syncwarp and stored after it.  Same butterflies and twiddles as the CTA
 // passes, so the results are identical.
-template <int N, int R, int NS, int SIGN, typename C>
+template <int N, int R, int NS, int SIGN, bool TP = false, typename C>
 __device__ __forceinline__ void wpass_m(C *__restrict__ buf, int nsig, int sstr,
                                         const C *__restrict__ tw, int lane) {
   constexpr int NB = N / R;
@@ -446,7 +489,7 @@ __device__ __forceinline__ void wpass_m(C *__restrict__ buf, int nsig, int sstr,
         for (int r = 0; r < R; r++) {
           C x = in[pad(b + r * NB)];
           if (NS > 1 && r > 0) {
-            C t = tw[r * k * TMUL];
+            C t = TP ? tw[r * NS + k] : tw[r * k * TMUL];
             if (SIGN > 0) t.y = -t.y;
             x = cmul(x, t);
           }
@@ -473,13 +516,14 @@ __device__ __forceinline__ void wpass_m(C *__restrict__ buf, int nsig, int sstr,
 
 // warp passes for any compile-time length: signal-parallel where N/R <= 32,
 // butterfly-parallel above
-template <int N, int SIGN, int P, int V = 0, typename C>
+template <int N, int SIGN, int P, int V = 0, bool TP = false, typename C>
 __device__ __forceinline__ void wpasses_any(C *buf, int nsig, int sstr, const C *tw, int lane) {
   constexpr int R = plan_radix(N, P, V);
   if constexpr (R != 0) {
-    if constexpr (N / R <= 32) wpass<N, R, plan_ns(N, P, V), SIGN>(buf, nsig, sstr, tw, lane);
-    else wpass_m<N, R, plan_ns(N, P, V), SIGN>(buf, nsig, sstr, tw, lane);
-    wpasses_any<N, SIGN, P + 1, V>(buf, nsig, sstr, tw, lane);
+    const C *twp = TP ? tw + twp_off<N, V>(P) : tw;
+    if constexpr (N / R <= 32) wpass<N, R, plan_ns(N, P, V), SIGN, TP>(buf, nsig, sstr, twp, lane);
+    else wpass_m<N, R, plan_ns(N, P, V), SIGN, TP>(buf, nsig, sstr, twp, lane);
+    wpasses_any<N, SIGN, P + 1, V, TP>(buf, nsig, sstr, tw, lane);
   }
 }
 
@@ -521,14 +565,14 @@ __device__ __forceinline__ void wpass_first_pz(C *__restrict__ buf, int nsig, in
 
 // whole transform with the pruned first pass (lengths whose first pass has
 // at most 32 butterflies; others take wpasses_any)
-template <int N, int SIGN, int V = 0, typename C>
+template <int N, int SIGN, int V = 0, bool TP = false, typename C>
 __device__ __forceinline__ void wpasses_pz(C *buf, int nsig, int sstr, const C *tw, int lane) {
   constexpr int R0 = plan_radix(N, 0, V);
   if constexpr (N / R0 <= 32) {
     wpass_first_pz<N, R0, SIGN>(buf, nsig, sstr, lane);
-    wpasses_any<N, SIGN, 1, V>(buf, nsig, sstr, tw, lane);
+    wpasses_any<N, SIGN, 1, V, TP>(buf, nsig, sstr, tw, lane);
   } else {
-    wpasses_any<N, SIGN, 0, V>(buf, nsig, sstr, tw, lane);
+    wpasses_any<N, SIGN, 0, V, TP>(buf, nsig, sstr, tw, lane);
   }
 }
 
@@ -551,7 +595,7 @@ __device__ __forceinline__ C *fft(C *buf0, C *buf1, const FftPlan &pl, int nsig,
 // warps (no CTA barrier between passes), otherwise the CTA-wide passes run.
 // (For 192, 384 and 512 the CTA-wide passes measured faster here than
 // butterfly-parallel warp passes: fewer registers, more resident CTAs.)
-template <int N, int V = 0, typename C>
+template <int N, int V = 0, bool TP = false, typename C>
 __device__ __forceinline__ C *fft_cta(C *buf0, C *buf1, const FftPlan &pl,
                                             int nsig, int sig_stride, const C *tw,
                                             int sign) {
@@ -562,9 +606,9 @@ __device__ __forceinline__ C *fft_cta(C *buf0, C *buf1, const FftPlan &pl,
     const int ns = (nsig - s0) < per ? (nsig - s0) : per;
     if (ns > 0) {
       if (sign < 0)
-        wpasses_any<N, -1, 0, V>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
+        wpasses_any<N, -1, 0, V, TP>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
       else
-        wpasses_any<N, +1, 0, V>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
+        wpasses_any<N, +1, 0, V, TP>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
     }
     __syncthreads();
     return buf0;
@@ -575,14 +619,14 @@ __device__ __forceinline__ C *fft_cta(C *buf0, C *buf1, const FftPlan &pl,
 
 // CTA front end of an inverse transform with the truncated band unread
 // (wpass_first_pz); warp-capable lengths only
-template <int N, int V = 0, typename C>
+template <int N, int V = 0, bool TP = false, typename C>
 __device__ __forceinline__ C *fft_cta_inv_pz(C *buf0, int nsig, int sig_stride, const C *tw) {
   static_assert(N != 0 && warp_fft_ok(N), "pruned transforms need a warp-capable length");
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int per = (nsig + nw - 1) / nw;
   const int s0 = warp * per;
   const int ns = (nsig - s0) < per ? (nsig - s0) : per;
-  if (ns > 0) wpasses_pz<N, +1, V>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
+  if (ns > 0) wpasses_pz<N, +1, V, TP>(buf0 + (long)s0 * sig_stride, ns, sig_stride, tw, lane);
   __syncthreads();
   return buf0;
 }

@@ -1004,7 +1004,7 @@ __global__ void __launch_bounds__(128, zw_minb(NZ, sizeof(CX))) k_zfwd_w(
   const int jlo = (f == 0 || f == 2) ? C.JS : (f == 1 ? 2 : sel(C.JSt, f - 3));
   const int jhi = (f == 0 || f == 2) ? C.JE : (f == 1 ? C.NY : sel(C.JEt, f - 3));
   if (j < jlo || j > jhi) return;
-  stage_tw<NZ, PV, tp_ok(NZ)>(stw, tw, NZ, threadIdx.x, blockDim.x);
+  for (int i = threadIdx.x; i < NZ; i += blockDim.x) stw[i] = tw[i];
   dg_pdl_wait();  // G comes from the x-row kernel
   const CX *GA = G + (2 * f) * Gfield + (long)j * NZ * nkxp;
   const CX *GB = G + (2 * f + 1) * Gfield + (long)j * NZ * nkxp;
@@ -1028,7 +1028,7 @@ __global__ void __launch_bounds__(128, zw_minb(NZ, sizeof(CX))) k_zfwd_w(
   }
   __syncthreads();
   CX *wb = buf + warp * 2 * KPW * SSTR;
-  wpasses_any<NZ, -1, 0, PV, tp_ok(NZ)>(wb, 2 * KPW, SSTR, stw, lane);
+  wpasses_any<NZ, -1, 0, PV>(wb, 2 * KPW, SSTR, stw, lane);
   __syncthreads();  // the epilogue below reads every warp's columns
 
   const double h = dscal[1 + rk_step];

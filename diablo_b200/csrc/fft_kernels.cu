@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(NTHR) k_zinv(PA fields, int jmin, long ss, int
   const int f = blockIdx.z;
   const int tid = threadIdx.x, nthr = blockDim.x;
   const auto *in = fields(f) + (long)j * ss;
-  stage_tw<NT, PV, tp_ok(NT)>(stw, tw, NZ, tid, nthr);
+  for (int i = tid; i < NZ; i += nthr) stw[i] = tw[i];
   dg_pdl_wait();
   for (int base = 0; base < KXG * NZ; base += 8 * nthr) {
     using CI = typename std::remove_const<typename std::remove_pointer<decltype(in)>::type>::type;
@@ -84,10 +84,10 @@ __global__ void __launch_bounds__(NTHR) k_zinv(PA fields, int jmin, long ss, int
   __syncthreads();
   CX *res;
   if constexpr (NT != 0 && warp_fft_ok(NT)) {
-    if (NKZ == NZ / 3) res = fft_cta_inv_pz<NT, PV, tp_ok(NT)>(b0, KXG, sstr, stw);
-    else res = fft_cta<NT, PV, tp_ok(NT)>(b0, b1, pl, KXG, sstr, stw, +1);
+    if (NKZ == NZ / 3) res = fft_cta_inv_pz<NT, PV>(b0, KXG, sstr, stw);
+    else res = fft_cta<NT, PV>(b0, b1, pl, KXG, sstr, stw, +1);
   } else {
-    res = fft_cta<NT, PV, tp_ok(NT)>(b0, b1, pl, KXG, sstr, stw, +1);
+    res = fft_cta<NT, PV>(b0, b1, pl, KXG, sstr, stw, +1);
   }
   CX *out = H + f * Hfield + (long)j * NZ * nkxp;
   for (int idx = tid; idx < KXG * NZ; idx += nthr) {
@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(NTHR) k_xc2r_cfl(const double2 *__restrict__ H
   const int tid = threadIdx.x, nthr = blockDim.x;
   const double2 *in = H + f * Hfield + (long)j * NZ * nkxp;
   const int NKX = nkxp - 1;
-  stage_tw<NT, PV, tp_ok(NT)>(stw, tw, NX, tid, nthr);
+  for (int i = tid; i < NX; i += nthr) stw[i] = tw[i];
   dg_pdl_wait();
   // bin k of Z = A + iB with the Hermitian extension of A and B; the row-pair
   // loads are issued four bins at a time per thread
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(NTHR) k_xc2r_cfl(const double2 *__restrict__ H
     }
   }
   __syncthreads();
-  double2 *res = fft_cta<NT, PV, tp_ok(NT)>(b0, b1, pl, RPAIR, sstr, stw, +1);
+  double2 *res = fft_cta<NT, PV>(b0, b1, pl, RPAIR, sstr, stw, +1);
   const double d = (f == 0) ? dxv : (f == 1 ? dy[j] : dzv);
   // min over points of CFL d / |u| is CFL d / max |u| (division is correctly
   // rounded and monotone), so only the largest |u| of the CTA is divided

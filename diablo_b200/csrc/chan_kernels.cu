@@ -1935,23 +1935,21 @@ static double courant_dt0(const dg_handle *h) {
   return dt;
 }
 
-// With `side`, the x c2r and the reduction run on the side stream (they read
-// only H, dmin_bits and write the parked DELTA_T), so they overlap whatever
-// the main stream runs next; the caller joins ev_cfl1 before the commit.
+// With `side`, the caller joins ev_cfl1 before the commit.
 int dg_courant_dev(dg_handle *h, const double2 *const *u, bool side) {
-  // physical U1..U3 on planes 1..NY, reduced to COURANT's minimum on the fly
-  // (inside a substep the z inverse follows the CN solve kernel)
-  h->pdl_zinv = side ? h->pdl : 0;
-  const int zs = dg_zinv(h, u, 3, 1, h->NY, h->H, 0);
-  h->pdl_zinv = 0;
-  DG_TRY(zs);
+  // physical U1..U3 on planes 1..NY, reduced to COURANT's minimum on the fly.
+  // With `side`, all of it (the z inverse into H too) runs on the side
+  // stream: it reads only u and writes H, dmin_bits and the parked DELTA_T,
+  // so it overlaps REM_DIV on the main stream
   cudaStream_t keep = h->st;
   if (side) {
     DG_CUDA(cudaEventRecord(h->ev_cfl0, h->st));
     DG_CUDA(cudaStreamWaitEvent(h->st2, h->ev_cfl0, 0));
     h->st = h->st2;
   }
-  auto reduce = [&]() -> int {
+  auto run = [&]() -> int {
+    h->pdl_zinv = 0;
+    DG_TRY(dg_zinv(h, u, 3, 1, h->NY, h->H, 0));
     DG_CUDA(cudaMemsetAsync(h->dmin_bits, 0x7f, sizeof(unsigned long long), h->st));
     DG_TRY(dg_xc2r_cfl(h, h->H, 1, h->NY, h->dmin_bits));
     dg_kt_begin(h, "k_dt_update", h->st);
@@ -1959,7 +1957,7 @@ int dg_courant_dev(dg_handle *h, const double2 *const *u, bool side) {
     DG_LAUNCHED();
     return DG_OK;
   };
-  const int s = reduce();
+  const int s = run();
   h->st = keep;
   DG_TRY(s);
   if (side) DG_CUDA(cudaEventRecord(h->ev_cfl1, h->st2));
@@ -2311,10 +2309,10 @@ bool dg_chan_cfl(const dg_handle *h, int time_step, int rk_step) {
          (time_step % h->p.update_dt) == 0;
 }
 
-// After a column stage that stopped at the CN solves: COURANT on the post-CN
-// velocity (for/channel.f:1037-1040), REM_DIV_CHAN and CP += phi / H_BAR
-// while COURANT's reduction finishes on the side stream, then the new
-// DELTA_T is committed.
+// After the column stage of a substep that runs COURANT: COURANT on the
+// post-CN velocity (for/channel.f:1037-1040) on the side stream, REM_DIV_CHAN
+// and CP += phi / H_BAR on the main stream meanwhile, then the new DELTA_T
+// is committed.
 int dg_chan_cfl_tail(dg_handle *h, int rk_step) {
   // the column stage left the post-CN velocity in the rhs arrays
   const double2 *u[3] = {h->rhs[0], h->rhs[1], h->rhs[2]};
@@ -2329,9 +2327,9 @@ extern "C" int diablo_rk_chan_1(dg_handle *h, int time_step, int rk_step) {
   bool column = false;
   DG_TRY(dg_chan_nonlinear(h, time_step, rk_step, &column));
   if (!column) return DG_OK;
-  // 4. per-mode column stage: explicit terms and right-hand sides, CN solves,
-  //    REM_DIV_CHAN and CP += phi / H_BAR in one kernel; with COURANT the
-  //    kernel stops after the CN solves and the tail above follows
+  // 4. per-mode column stage: explicit terms, right-hand sides and CN solves
+  //    (k_col_cn), then REM_DIV_CHAN and CP += phi / H_BAR (k_rd_col); with
+  //    COURANT the tail above runs between them
   const bool cfl = dg_chan_cfl(h, time_step, rk_step);
   DG_TRY(dg_col_step_dev(h, rk_step, !cfl));
   if (cfl) DG_TRY(dg_chan_cfl_tail(h, rk_step));

@@ -77,6 +77,30 @@ template <> struct DFT<3> {
   }
 };
 
+// 5-point DFT: with W = exp(sign 2 pi i / 5), c_m = cos(2 pi m / 5) and
+// s_m = sin(2 pi m / 5), X_1,4 = x0 + c1 (x1 + x4) + c2 (x2 + x3)
+// +- sign i (s1 (x1 - x4) + s2 (x2 - x3)) and X_2,3 = x0 + c2 (x1 + x4)
+// + c1 (x2 + x3) +- sign i (s2 (x1 - x4) - s1 (x2 - x3)).
+template <> struct DFT<5> {
+  template <typename C> static __device__ __forceinline__ void run(C *v, int sign) {
+    using T = typename CT<C>::T;
+    const T c1 = (T)0.30901699437494742410, c2 = (T)-0.80901699437494742410;
+    const T s1 = (T)0.95105651629515357212, s2 = (T)0.58778525229247312917;
+    const C t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+    const C t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+    const C a1 = CT<C>::mk(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+    const C a2 = CT<C>::mk(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+    // b = s-weighted differences, then times sign * i
+    const C b1 = mul_si(CT<C>::mk(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y), sign);
+    const C b2 = mul_si(CT<C>::mk(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y), sign);
+    v[0] = cadd(v[0], cadd(t1, t2));
+    v[1] = cadd(a1, b1);
+    v[4] = csub(a1, b1);
+    v[2] = cadd(a2, b2);
+    v[3] = csub(a2, b2);
+  }
+};
+
 template <> struct DFT<4> {
   template <typename C> static __device__ __forceinline__ void run(C *v, int sign) {
     C s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
@@ -204,6 +228,7 @@ __device__ inline C *run(C *buf0, C *buf1, const FftPlan &pl, int nsig,
       case 8: pass<8>(src, dst, pl.n, Ns, nsig, sig_stride, tw, sign, tid, nthr); break;
       case 4: pass<4>(src, dst, pl.n, Ns, nsig, sig_stride, tw, sign, tid, nthr); break;
       case 3: pass<3>(src, dst, pl.n, Ns, nsig, sig_stride, tw, sign, tid, nthr); break;
+      case 5: pass<5>(src, dst, pl.n, Ns, nsig, sig_stride, tw, sign, tid, nthr); break;
       default: pass<2>(src, dst, pl.n, Ns, nsig, sig_stride, tw, sign, tid, nthr); break;
     }
     __syncthreads();

@@ -540,6 +540,7 @@ bool dg_make_plan(int n, FftPlan *pl) {
     else if (m % 4 == 0) r = 4;
     else if (m % 2 == 0) r = 2;
     else if (m % 3 == 0) r = 3;
+    else if (m % 5 == 0) r = 5;
     else return false;
     if (pl->np >= DG_MAX_PASSES) return false;
     pl->r[pl->np++] = r;

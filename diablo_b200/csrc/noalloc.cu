@@ -181,7 +181,7 @@ extern "C" int diablo_fft_xz_to_fourier_noalloc(const double *V, double *VV, int
   FftPlan plx, plz;
   if (nx < 8 || nz < 8 || (nx & 1) || (nz & 1) || nx > 4096 || nz > 4096 ||
       !dg_make_plan(nx, &plx) || !dg_make_plan(nz, &plz)) {
-    dg_set_error("NX and NZ must be even, 8..4096, and factor into 2 and 3");
+    dg_set_error("NX and NZ must be even, 8..4096, and factor into 2, 3 and 5");
     return DG_ERR_DIMS;
   }
   const int nkx = nx / 3, nkz = nz / 3;

@@ -129,7 +129,7 @@ static int validate(const dg_params *p, const double *gy) {
   }
   FftPlan t;
   if (!dg_make_plan(p->nx, &t) || !dg_make_plan(p->nz, &t)) {
-    dg_set_error("NX and NZ must factor into 2 and 3");
+    dg_set_error("NX and NZ must factor into 2, 3 and 5");
     return DG_ERR_DIMS;
   }
   if (p->num_per_dir == 2) {
@@ -185,7 +185,7 @@ static int validate(const dg_params *p, const double *gy) {
       return DG_ERR_DIMS;
     }
     if (!dg_make_plan(p->ny, &t) || p->ny < 8) {
-      dg_set_error("periodic NY must be >= 8 and factor into 2 and 3");
+      dg_set_error("periodic NY must be >= 8 and factor into 2, 3 and 5");
       return DG_ERR_DIMS;
     }
   }

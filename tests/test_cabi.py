@@ -36,7 +36,7 @@ def test_params_struct_layout_matches_header():
 def test_init_refuses_without_device_or_bad_args():
     L = _lib.load()
     p, gy = configs.kh_shear_layer(nx=32, ny=17, nz=16)
-    bad = p.replace(nx=30)  # 30 = 2*3*5 does not factor into 2 and 3
+    bad = p.replace(nx=28)  # 28 = 4*7: no radix-7 pass
     h = ctypes.c_void_p()
     code = L.diablo_gpu_init(ctypes.byref(bad.to_struct(DgParams)), None, None, ctypes.byref(h))
     assert code in (2,)  # DG_ERR_DIMS (also checked before any device call)

@@ -51,7 +51,7 @@ def fields(p):
 
 # ------------------------------------------------------------------ transforms
 @pytest.mark.parametrize("nx,nz,ny", [(32, 16, 9), (128, 32, 17), (48, 96, 7), (512, 384, 5),
-                                      (36, 18, 6)])
+                                      (36, 18, 6), (30, 20, 5), (80, 40, 7), (160, 120, 4)])
 def test_fft_xz_matches_oracle(nx, nz, ny):
     p = Params(nx=nx, ny=ny, nz=nz, lx=1.0, lz=1.0)
     gy = uniform_grid(ny, -1, 1)
@@ -250,6 +250,28 @@ def test_poisson_p_chan_matches_oracle(case):
     ch.close()
 
 
+@pytest.mark.parametrize("nx,nz", [(80, 40), (60, 30)])
+def test_channel_radix5_lengths_match_oracle(nx, nz):
+    """x and z lengths with a factor of 5 (FFTW takes any length; the runtime
+    plans add a radix-5 pass): a stratified KH layer and a no-slip channel
+    with COURANT, against the oracle."""
+    p, gy = configs.kh_shear_layer(nx=nx, ny=33, nz=nz)
+    ref, ch, _ = start_pair(p, gy, ics.kh_shear_layer, seed=21)
+    for s in range(1, 6):
+        ref.step(s)
+        ch.step(s)
+    compare(ref, ch, fields(p))
+    ch.close()
+    p, gy = configs.channel_re180(nx=nx, ny=33, nz=nz)
+    ref, ch, _ = start_pair(p, gy, ics.channel_laminar, seed=22)
+    for s in range(1, 6):
+        ref.step(s)
+        ch.step(s)
+    compare(ref, ch, fields(p))
+    assert abs(ch.get_time()[1] - ref.get_time()[1]) <= 1e-12 * ref.get_time()[1]
+    ch.close()
+
+
 @pytest.mark.parametrize("case", ["tall_ny257", "wide_512x384"])
 def test_channel_large_dims_short(case):
     """NY = 257 (the CN row templates of four fields exceed 48 KB) and the
@@ -284,7 +306,7 @@ def test_errors_are_reported_not_fatal():
     from diablo_b200.solver import DiabloError
     p, gy = configs.kh_shear_layer(nx=32, ny=17, nz=16)
     with pytest.raises(DiabloError):
-        channel(p.replace(nx=30), gy)
+        channel(p.replace(nx=28), gy)  # a factor of 7: no radix for it
     ch = channel(p, gy)
     with pytest.raises(DiabloError):
         ch.rk_chan_1(1, 4)

@@ -81,7 +81,7 @@ def test_budget_admission_and_errors():
     cs = cases()[:4]
     # room for the two largest cases at most
     budget = sorted(state_bytes(c[0]) for c in cs)[-1] * 2.05 / 1e9
-    bad = cs[0][0].replace(nx=30)               # NX that does not factor into 2 and 3
+    bad = cs[0][0].replace(nx=28)               # NX with a factor of 7: refused
     with Server(max_active=8, budget_gb=budget, autotune=False) as srv:
         ids = [srv.submit(p, gy, st, 5) for p, gy, st, _ in cs]
         bad_id = srv.submit(bad, cs[0][1], cs[0][2], 5)

@@ -1,7 +1,8 @@
 // Channel substep kernels (RK_CHAN_1, for/channel.f:62-1073) on the
 // retained-mode layout [j][kz][kx].
 //
-// One substep is four launches (five, plus COURANT's, when COURANT runs):
+// One substep is five launches (plus COURANT's on the side stream when it
+// runs):
 //   zinv        spectral U1..U3, TH -> half-physical H (z inverse per kx)
 //   k_xrow_w    per physical z-row, marching up in y: x c2r of every field,
 //               all products/fluxes of for/channel.f:409-571,665-720, x r2c,
@@ -16,14 +17,14 @@
 //               CF and the Crank-Nicolson right-hand side
 //               R = CU + zeta h CF_old - h grad P + beta h CF_new
 //                   + (nu h / 2) d2/dy2 CU,          for/channel.f:88-626)
-//   k_col_step  per mode tile (chan_column.cu): explicit terms, CF, the CN
-//               right-hand sides and solves of every field, REM_DIV_CHAN and
-//               CP += phi / h.  The reference solves the same x-z independent
-//               CN operator per physical column (for/channel.f:767-1029); it
-//               is linear and identical for every column, so it commutes with
-//               the x-z transform.  With COURANT the kernel stops after the
-//               CN solves and k_rd_col (below) projects after COURANT's
-//               transform (for/channel.f:1037-1065, 1103-1214).
+//   k_col_cn    per (mode tile, field) (chan_column.cu): explicit terms, CF,
+//               the CN right-hand side and solve.  The reference solves the
+//               same x-z independent CN operator per physical column
+//               (for/channel.f:767-1029); it is linear and identical for
+//               every column, so it commutes with the x-z transform.
+//   k_rd_col    per mode tile: REM_DIV_CHAN and CP += phi / h on the post-CN
+//               velocity (for/channel.f:1037-1065, 1103-1214); with COURANT,
+//               COURANT's transform and reduction run beside it.
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>

@@ -1205,12 +1205,17 @@ struct CnRows {
 
 // blockIdx.x = rk * nfld + field.  The CTA stages the field's row templates
 // into shared memory with coalesced loads and forms every row's (l, d, u) in
-// parallel; one thread then runs the elimination recurrence, whose critical
-// path per row is a multiply, a multiply-add and a reciprocal: the
-// multiplier is -l times the previous reciprocal pivot, the value the table
-// stores and the solves use (a division there would add a second long
-// operation to every row); the CTA writes the table back with coalesced
-// stores.
+// parallel.  The pivots b(j) = d(j) - l(j) u(j-1) / b(j-1) of the forward
+// elimination are ratios b(j) = p(j) / p(j-1) of the continuants
+//   p(j) = d(j) p(j-1) + w(j) p(j-2),   w(j) = -l(j) u(j-1),
+//   p(-1) = 1, p(-2) = 0,
+// so one thread runs that three-term recurrence, whose critical path per
+// row is a single multiply-add (a zero pivot restarts it the way the
+// elimination does: 1/b = 0, and the next row keeps its own diagonal), and
+// rescales the pair by a power of two every 4 rows (exact, so the ratios
+// are unchanged).  Every thread then forms its rows' reciprocal pivots
+// p(j-1) / p(j), multipliers -l(j) / b(j-1) and -u(j) / b(j), and the CTA
+// writes the table back with coalesced stores.
 constexpr int CT_THR = 128;
 
 __global__ void __launch_bounds__(CT_THR) k_cn_tables(CnRows P, const double *__restrict__ dscal,
@@ -1220,50 +1225,66 @@ __global__ void __launch_bounds__(CT_THR) k_cn_tables(CnRows P, const double *__
   extern __shared__ double ct_sm[];
   const int L = P.NY + 2;
   const int rk = blockIdx.x / P.nfld, f = blockIdx.x % P.nfld;
-  double *R = ct_sm;           // [8][L] templates
-  double *T = ct_sm + 8 * L;   // [5][L] the table
+  double *R = ct_sm;           // [8][L] templates, then the continuants [2][L]
+  double *T = ct_sm + 8 * L;   // [5][L]: w, 1/b, u, kind, bc value
   double *W = T + 5 * L;       // [2][L] l, d of every row
   const double *Rg = rows + (long)f * 8 * L;
   for (int i = threadIdx.x; i < 8 * L; i += CT_THR) R[i] = Rg[i];
   __syncthreads();
   const double h = dscal[2 + rk];
   const double s = (P.nu * h / 2.0) / P.pr[f] * P.nuv;
+  auto row_u = [&](int j) {
+    return (R[j] == (double)ROW_RHS) ? s * R[3 * L + j] : R[6 * L + j];
+  };
   for (int j = threadIdx.x; j < L; j += CT_THR) {
     const bool cn = R[j] == (double)ROW_RHS;
-    W[j] = cn ? s * R[1 * L + j] : R[4 * L + j];               // l
+    const double l = cn ? s * R[1 * L + j] : R[4 * L + j];
+    W[j] = l;
     W[L + j] = cn ? 1.0 + s * R[2 * L + j] : R[5 * L + j];     // d
-    T[2 * L + j] = cn ? s * R[3 * L + j] : R[6 * L + j];       // u
+    T[j] = (j > 0) ? -l * row_u(j - 1) : 0.0;                  // w
+    T[2 * L + j] = row_u(j);                                   // u
     T[3 * L + j] = R[j];                                       // kind
     T[4 * L + j] = R[7 * L + j];                               // bc value
   }
   __syncthreads();
+  double *Pc = R, *Qc = R + L;  // p(j) and p(j-1), one scale per row
   if (threadIdx.x == 0) {
     constexpr int B = 8;
-    const double *U = T + 2 * L;
-    double rbp = 0.0;  // reciprocal pivot of the previous row
+    double pm = 0.0, pc = 1.0;  // p(j-2), p(j-1)
     for (int j0 = 0; j0 < L; j0 += B) {
-      double l[B], d[B], c[B];
+      double d[B], w[B];
 #pragma unroll
       for (int q = 0; q < B; q++) {
         const int j = j0 + q < L ? j0 + q : L - 1;
-        l[q] = W[j];
         d[q] = W[L + j];
-        c[q] = j > 0 ? U[j - 1] : 0.0;
+        w[q] = T[j];
       }
 #pragma unroll
       for (int q = 0; q < B; q++) {
         const int j = j0 + q;
         if (j < L) {
-          const double a = (j > 0) ? -l[q] * rbp : 0.0;
-          const double b = (j > 0) ? d[q] + a * c[q] : d[q];
-          const double rb = (b != 0.0) ? 1.0 / b : 0.0;
-          T[j] = a;
-          T[L + j] = rb;
-          rbp = rb;
+          double pn = fma(d[q], pc, w[q] * pm);
+          const bool z = (pn == 0.0);
+          const double pq = z ? 0.0 : pc;
+          pn = z ? 1.0 : pn;
+          Pc[j] = pn;
+          Qc[j] = pq;
+          pm = pq;
+          pc = pn;
+          if ((q & 3) == 3) {
+            // 2^-e with e the exponent of p(j), clamped inside the normal range
+            const int e = ((__double2hiint(pc) >> 20) & 0x7ff) - 1023;
+            const int ec = e < -1000 ? -1000 : (e > 1000 ? 1000 : e);
+            const double sc = __hiloint2double((1023 - ec) << 20, 0);
+            pm *= sc;
+            pc *= sc;
+          }
         }
       }
     }
   }
+  __syncthreads();
+  for (int j = threadIdx.x; j < L; j += CT_THR) T[L + j] = Qc[j] / Pc[j];
   __syncthreads();
   // rows of LP = L rounded up to even doubles, so every row starts on a
   // 16-byte boundary (the column kernel fetches them by bulk copies)
@@ -1273,8 +1294,10 @@ __global__ void __launch_bounds__(CT_THR) k_cn_tables(CnRows P, const double *__
     const int r = i / LP, j = i - r * LP;
     double v = 0.0;
     if (j < L) {
-      // row 2: the backward recurrence's coefficient -c / b (0 on the last row)
-      if (r == 2) v = (j < L - 1) ? -T[2 * L + j] * T[L + j] : 0.0;
+      // row 0: the multiplier -l / b(j-1) (0 on the first row); row 2: the
+      // backward recurrence's coefficient -u / b (0 on the last row)
+      if (r == 0) v = (j > 0) ? -W[j] * T[L + j - 1] : 0.0;
+      else if (r == 2) v = (j < L - 1) ? -T[2 * L + j] * T[L + j] : 0.0;
       else v = T[r * L + j];
     }
     Tg[i] = v;

@@ -161,6 +161,8 @@ struct dg_handle {
                                 // column kernel assembles the right-hand sides)
   int wait_test;                // test only: poll limit of the next column-kernel launch,
                                 // whose barrier then expects 16 bytes more than it receives
+  int plane_xz;                 // LES transforms: one kernel per direction and plane where
+                                // the grid allows (1), or staged through les_H (0)
 
   // LES (dg_params.les): physical slots [nslots][NY+2][NZ][NX], spectral slots
   // [nslots][NY+2][ss], filter-width factors [2][NY+2] (DYF, DY), mean U1/U3
@@ -217,6 +219,15 @@ int dg_xr2c_planes(dg_handle *h, const double *phys, int nf, int jmin, int jmax,
                    long phys_plane_stride, long phys_row_stride, long field_stride, double2 *H);
 int dg_zfwd_planes(dg_handle *h, const double2 *H, int nf, int jmin, int jmax,
                    double2 *const *fields, double2 *raw_ref, long raw_ld);
+// whole-plane transforms (spectral planes <-> physical rows, one kernel per
+// direction, no staging array): DG_OK once launched, 1 when the grid does not
+// allow them (the caller then stages through a half-physical array)
+bool dg_plane_ok(const dg_handle *h);
+int dg_plane_c2r(dg_handle *h, const double2 *const *in, int nf, int jmin, int jmax, double *phys,
+                 long phys_plane_stride, long phys_row_stride, long field_stride);
+int dg_plane_r2c(dg_handle *h, const double *phys, int nf, int jmin, int jmax,
+                 long phys_plane_stride, long phys_row_stride, long field_stride,
+                 double2 *const *out);
 
 // channel / periodic internals
 int dg_chan_init(dg_handle *h);

@@ -329,6 +329,167 @@ __global__ void __launch_bounds__(NTHR) k_xr2c(const double *__restrict__ phys, 
   }
 }
 
+// ------------------------------------------- whole-plane transforms (x-z)
+// One CTA per (plane, field) moves a plane between the retained-mode layout
+// and physical rows without the half-physical staging array: the plane's
+// NKX+1 z columns (NZ bins each) stay in shared memory between the z and
+// the x transform.  Same passes, plans and twiddles as k_zinv + k_xc2r and
+// k_xr2c + k_zfwd (the plan variant 0), so the results are the same.
+// Requires NKX = NX/3 and NKZ = NZ/3 (the truncated bands the pruned first
+// passes skip).  Shared memory: the columns [NKX+1][SZ] (SZ odd, so the x
+// stage's reads across the columns hit distinct banks) and two row-pair
+// signals per warp.
+constexpr int PL_THR = 128;
+
+__host__ __device__ constexpr int pl_sz(int nz) { return padded_len(nz) | 1; }
+__host__ __device__ constexpr size_t pl_smem(int nx, int nz) {
+  return sizeof(double2) * ((size_t)(nx / 3 + 1) * pl_sz(nz) + (PL_THR / 32) * 2 * padded_len(nx));
+}
+
+template <int NXT, int NZT>
+__global__ void __launch_bounds__(PL_THR, 2) k_plane_c2r(CFieldPtrs fields, int jmin, long ss,
+                                                         const double2 *__restrict__ twz,
+                                                         const double2 *__restrict__ twx,
+                                                         double *__restrict__ phys, long pplane,
+                                                         long prow, long pfield) {
+  constexpr int NKXP = NXT / 3 + 1, NKZ = NZT / 3, NKZT = 2 * NKZ + 1;
+  constexpr int SZ = pl_sz(NZT), SX = padded_len(NXT);
+  extern __shared__ double2 sm[];
+  double2 *Hs = sm;                   // [NKXP][SZ]: the z bins of every kx column
+  double2 *xb = Hs + NKXP * SZ;       // [warp][2][SX]: row-pair signals
+  const int j = jmin + blockIdx.x, f = blockIdx.y;
+  const int tid = threadIdx.x;
+  const double2 *in = fields(f) + (long)j * ss;
+  // 1. retained modes into their z bins (the band stays unwritten: the
+  // pruned first pass does not read it); eight loads in flight per thread
+  for (int base = 0; base < NKZT * NKXP; base += 8 * PL_THR) {
+    double2 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int i = base + u * PL_THR + tid;
+      v[u] = (i < NKZT * NKXP) ? in[i] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int i = base + u * PL_THR + tid;
+      if (i < NKZT * NKXP) {
+        const int kp = i / NKXP, kx = i - kp * NKXP;
+        const int z = (kp <= NKZ) ? kp : kp + NZT - NKZT;
+        Hs[kx * SZ + pad(z)] = v[u];
+      }
+    }
+  }
+  __syncthreads();
+  // 2. z inverse of every column
+  fft_cta_inv_pz<NZT, 0>(Hs, NKXP, SZ, twz);
+  // 3. x c2r of row pairs (za, za + 1), two pairs per warp at a time: bin k
+  // of Z = A + iB with the Hermitian extension above NX/2 (as k_xc2r)
+  const int warp = tid >> 5, lane = tid & 31;
+  double2 *xw = xb + warp * 2 * SX;
+  double *out = phys + f * pfield + (long)j * pplane;
+  for (int p0 = 2 * warp; p0 < NZT / 2; p0 += 2 * (PL_THR / 32)) {
+    const int np = (NZT / 2 - p0) < 2 ? (NZT / 2 - p0) : 2;
+    for (int q = 0; q < np; q++) {
+      const int za = 2 * (p0 + q), zb = za + 1;
+#pragma unroll
+      for (int i = 0; i < (NXT + 31) / 32; i++) {
+        const int k = lane + 32 * i;
+        const int kk = (k <= NXT / 2) ? k : NXT - k;
+        if (k < NXT && kk < NKXP && kk < NXT / 2) {
+          double2 a = Hs[kk * SZ + pad(za)], b = Hs[kk * SZ + pad(zb)];
+          if (kk == 0) {
+            a.y = 0.0;
+            b.y = 0.0;
+          }
+          xw[q * SX + pad(k)] = (k == kk) ? make_double2(a.x - b.y, a.y + b.x)
+                                          : make_double2(a.x + b.y, -a.y + b.x);
+        }
+      }
+    }
+    __syncwarp();
+    wpasses_pz<NXT, +1, 0, false>(xw, np, SX, twx, lane);
+    for (int q = 0; q < np; q++) {
+      const int za = 2 * (p0 + q), zb = za + 1;
+#pragma unroll
+      for (int i = 0; i < (NXT + 31) / 32; i++) {
+        const int x = lane + 32 * i;
+        if (x < NXT) {
+          const double2 v = xw[q * SX + pad(x)];
+          out[(long)za * prow + x] = v.x;
+          out[(long)zb * prow + x] = v.y;
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+template <int NXT, int NZT>
+__global__ void __launch_bounds__(PL_THR, 2) k_plane_r2c(const double *__restrict__ phys,
+                                                         long pplane, long prow, long pfield,
+                                                         int jmin,
+                                                         const double2 *__restrict__ twx,
+                                                         const double2 *__restrict__ twz,
+                                                         FieldPtrs fields, long ss) {
+  constexpr int NKXP = NXT / 3 + 1, NKZ = NZT / 3, NKZT = 2 * NKZ + 1;
+  constexpr int SZ = pl_sz(NZT), SX = padded_len(NXT);
+  extern __shared__ double2 sm[];
+  double2 *Hs = sm;
+  double2 *xb = Hs + NKXP * SZ;
+  const int j = jmin + blockIdx.x, f = blockIdx.y;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  double2 *xw = xb + warp * 2 * SX;
+  const double *in = phys + f * pfield + (long)j * pplane;
+  const double rnx = (double)NXT;
+  // 1. x r2c of row pairs into the kx columns, kx = 0..NKX, / NX (as k_xr2c)
+  for (int p0 = 2 * warp; p0 < NZT / 2; p0 += 2 * (PL_THR / 32)) {
+    const int np = (NZT / 2 - p0) < 2 ? (NZT / 2 - p0) : 2;
+    for (int q = 0; q < np; q++) {
+      const int za = 2 * (p0 + q), zb = za + 1;
+      double a[(NXT + 31) / 32], b[(NXT + 31) / 32];
+#pragma unroll
+      for (int i = 0; i < (NXT + 31) / 32; i++) {
+        const int x = lane + 32 * i;
+        a[i] = (x < NXT) ? in[(long)za * prow + x] : 0.0;
+        b[i] = (x < NXT) ? in[(long)zb * prow + x] : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < (NXT + 31) / 32; i++) {
+        const int x = lane + 32 * i;
+        if (x < NXT) xw[q * SX + pad(x)] = make_double2(a[i], b[i]);
+      }
+    }
+    __syncwarp();
+    wpasses_any<NXT, -1, 0, 0, false>(xw, np, SX, twx, lane);
+    for (int q = 0; q < np; q++) {
+      const int za = 2 * (p0 + q), zb = za + 1;
+      for (int k = lane; k < NKXP; k += 32) {
+        const double2 zk = xw[q * SX + pad(k)];
+        const double2 zm = xw[q * SX + pad((NXT - k) % NXT)];
+        const double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+        const double2 B = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
+        Hs[k * SZ + pad(za)] = make_double2(A.x / rnx, A.y / rnx);
+        Hs[k * SZ + pad(zb)] = make_double2(B.x / rnx, B.y / rnx);
+      }
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  // 2. z forward of every column
+  FftPlan none{};
+  fft_cta<NZT>(Hs, Hs, none, NKXP, SZ, twz, -1);
+  // 3. retained modes out, / NZ (as k_zfwd)
+  double2 *out = fields(f) + (long)j * ss;
+  const double rnz = (double)NZT;
+  for (int i = tid; i < NKZT * NKXP; i += PL_THR) {
+    const int kp = i / NKXP, kx = i - kp * NKXP;
+    const int z = (kp <= NKZ) ? kp : kp + NZT - NKZT;
+    const double2 v = Hs[kx * SZ + pad(z)];
+    out[i] = make_double2(v.x / rnz, v.y / rnz);
+  }
+}
+
 size_t zsmem(int NZ, size_t esz = sizeof(double2)) {
   return esz * (NZ + fft_bufs(NZ) * batch_for(NZ) * padded_len(NZ));
 }
@@ -505,6 +666,110 @@ int dg_xr2c_planes(dg_handle *h, const double *phys, int nf, int jmin, int jmax,
 #undef KERNEL_BODY
   DG_LAUNCHED();
   return DG_OK;
+}
+
+// ------------------------------------------------- whole-plane transforms
+// Lengths of the whole-plane kernels: x and z lengths with a compile-time
+// warp plan up to 128 (the z columns of a plane then fit two CTAs per SM).
+#define DG_PLANE_NX(X) X(16) X(32) X(48) X(64) X(96) X(128)
+
+bool dg_plane_ok(const dg_handle *h) {
+  auto len_ok = [](int n) {
+    return n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128;
+  };
+  return h->plane_xz && !h->periodic && len_ok(h->NX) && len_ok(h->NZ) &&
+         h->nkxp == h->NX / 3 + 1 && h->NKZ == h->NZ / 3 &&
+         h->ss == (long)h->nkxp * (2 * h->NKZ + 1);
+}
+
+namespace {
+// the whole-plane kernels run two CTAs per SM at the largest sizes only with
+// the shared-memory carveout at its maximum
+void plane_attrs(const void *kern) {
+  static std::mutex mu;
+  static std::unordered_set<const void *> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.insert(kern).second) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+  }
+}
+
+template <int NXT, int NZT>
+int plane_c2r_t(dg_handle *h, const double2 *const *in, int nf, int jmin, int jmax, double *phys,
+                long pplane, long prow, long pfield) {
+  CFieldPtrs fp;
+  for (int f = 0; f < nf; f++) fp.p[f] = in[f];
+  auto kern = k_plane_c2r<NXT, NZT>;
+  plane_attrs((const void *)kern);
+  dg_kt_begin(h, "k_plane_c2r", h->st);
+  kern<<<dim3(jmax - jmin + 1, nf), PL_THR, pl_smem(NXT, NZT), h->st>>>(
+      fp, jmin, h->ss, h->twz, h->twx, phys, pplane, prow, pfield);
+  DG_LAUNCHED();
+  return DG_OK;
+}
+template <int NXT, int NZT>
+int plane_r2c_t(dg_handle *h, const double *phys, int nf, int jmin, int jmax, long pplane,
+                long prow, long pfield, double2 *const *out) {
+  FieldPtrs fp;
+  for (int f = 0; f < nf; f++) fp.p[f] = out[f];
+  auto kern = k_plane_r2c<NXT, NZT>;
+  plane_attrs((const void *)kern);
+  dg_kt_begin(h, "k_plane_r2c", h->st);
+  kern<<<dim3(jmax - jmin + 1, nf), PL_THR, pl_smem(NXT, NZT), h->st>>>(
+      phys, pplane, prow, pfield, jmin, h->twx, h->twz, fp, h->ss);
+  DG_LAUNCHED();
+  return DG_OK;
+}
+template <int NXT>
+int plane_c2r_z(dg_handle *h, const double2 *const *in, int nf, int jmin, int jmax, double *phys,
+                long pplane, long prow, long pfield) {
+#define KERNEL_BODY(NZT) return plane_c2r_t<NXT, NZT>(h, in, nf, jmin, jmax, phys, pplane, prow, pfield)
+  switch (h->NZ) {
+    DG_PLANE_NX(DG_CASE_N)
+    default: break;
+  }
+#undef KERNEL_BODY
+  return 1;
+}
+template <int NXT>
+int plane_r2c_z(dg_handle *h, const double *phys, int nf, int jmin, int jmax, long pplane,
+                long prow, long pfield, double2 *const *out) {
+#define KERNEL_BODY(NZT) return plane_r2c_t<NXT, NZT>(h, phys, nf, jmin, jmax, pplane, prow, pfield, out)
+  switch (h->NZ) {
+    DG_PLANE_NX(DG_CASE_N)
+    default: break;
+  }
+#undef KERNEL_BODY
+  return 1;
+}
+}  // namespace
+
+int dg_plane_c2r(dg_handle *h, const double2 *const *in, int nf, int jmin, int jmax, double *phys,
+                 long pplane, long prow, long pfield) {
+  if (!dg_plane_ok(h)) return 1;
+  if (jmax < jmin || nf <= 0) return DG_OK;
+#define KERNEL_BODY(NXT) return plane_c2r_z<NXT>(h, in, nf, jmin, jmax, phys, pplane, prow, pfield)
+  switch (h->NX) {
+    DG_PLANE_NX(DG_CASE_N)
+    default: break;
+  }
+#undef KERNEL_BODY
+  return 1;
+}
+
+int dg_plane_r2c(dg_handle *h, const double *phys, int nf, int jmin, int jmax, long pplane,
+                 long prow, long pfield, double2 *const *out) {
+  if (!dg_plane_ok(h)) return 1;
+  if (jmax < jmin || nf <= 0) return DG_OK;
+#define KERNEL_BODY(NXT) return plane_r2c_z<NXT>(h, phys, nf, jmin, jmax, pplane, prow, pfield, out)
+  switch (h->NX) {
+    DG_PLANE_NX(DG_CASE_N)
+    default: break;
+  }
+#undef KERNEL_BODY
+  return 1;
 }
 
 int dg_xc2r_cfl(dg_handle *h, const double2 *H, int jmin, int jmax, unsigned long long *out) {

@@ -628,6 +628,11 @@ int to_physical(dg_handle *h, const double2 *const *in, int n, int jmin, int jma
   const long pplane = (long)h->NZ * h->NX, pf = pfield_of(h);
   for (int b = 0; b < n; b += LES_HF) {
     const int k = (n - b < LES_HF) ? n - b : LES_HF;
+    const int r = dg_plane_c2r(h, in + b, k, jmin, jmax, out + (long)b * pf, pplane, h->NX, pf);
+    if (r != 1) {
+      DG_TRY(r);
+      continue;
+    }
     DG_TRY(dg_zinv(h, in + b, k, jmin, jmax, h->les_H, 0));
     DG_TRY(dg_xc2r_planes(h, h->les_H, k, jmin, jmax, out + (long)b * pf, pplane, h->NX, pf));
   }
@@ -638,6 +643,11 @@ int to_fourier(dg_handle *h, const double *in, int n, int jmin, int jmax, double
   const long pplane = (long)h->NZ * h->NX, pf = pfield_of(h);
   for (int b = 0; b < n; b += LES_HF) {
     const int k = (n - b < LES_HF) ? n - b : LES_HF;
+    const int r = dg_plane_r2c(h, in + (long)b * pf, k, jmin, jmax, pplane, h->NX, pf, out + b);
+    if (r != 1) {
+      DG_TRY(r);
+      continue;
+    }
     DG_TRY(dg_xr2c_planes(h, in + (long)b * pf, k, jmin, jmax, pplane, h->NX, pf, h->les_H));
     DG_TRY(dg_zfwd_planes(h, h->les_H, k, jmin, jmax, out + b, nullptr, 0));
   }

@@ -254,6 +254,7 @@ extern "C" int diablo_gpu_init(const dg_params *p, const double *gy, void *strea
   h->cn_mt = 4;
   h->zf_nlo = 1;
   h->pdl = 1;
+  h->plane_xz = 1;
   h->pi = 4.0 * atan(1.0);
   h->eps = (double)(float)0.000000001;  // default-real literal, for/fft.f:74
   // INIT_CHAN_MPI with NPROCY = 1 (for/mpi.f:1080-1100)

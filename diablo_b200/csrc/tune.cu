@@ -21,6 +21,12 @@
 //                       (128 = 8 x 16).  Same transform, different shared-
 //                       memory strides, twiddle reuse and registers; lengths
 //                       whose factors are all equal have one plan.
+//   DG_TUNE_PLANE_XZ    1 (default): the LES model's transforms between
+//                       spectral planes and physical rows run as one kernel
+//                       per direction where the grid allows (x and z lengths
+//                       16, 32, 48, 64, 96 or 128); 0: two launches each,
+//                       staged through a half-physical array.  Same passes,
+//                       same results.
 //   DG_TUNE_WAIT_TEST   test only, not a launch shape: value > 0 makes the
 //                       next column-kernel launch poll its bulk-copy barrier at
 //                       most `value` times and expect 16 bytes more than its
@@ -119,6 +125,10 @@ extern "C" int dg_tune_set(dg_handle *h, int key, int value) {
       if (value != 0 && value != 1) return DG_ERR_ARG;
       h->fft_plan = value;
       break;
+    case DG_TUNE_PLANE_XZ:
+      if (value != 0 && value != 1) return DG_ERR_ARG;
+      h->plane_xz = value;
+      break;
     default:
       return DG_ERR_ARG;
   }
@@ -136,6 +146,7 @@ extern "C" int dg_tune_get(dg_handle *h, int key, int *value) {
     case DG_TUNE_PDL: *value = h->pdl; return DG_OK;
     case DG_TUNE_WAIT_TEST: *value = h->wait_test; return DG_OK;
     case DG_TUNE_FFT_PLAN: *value = h->fft_plan; return DG_OK;
+    case DG_TUNE_PLANE_XZ: *value = h->plane_xz; return DG_OK;
     default: return DG_ERR_ARG;
   }
 }

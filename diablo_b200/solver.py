@@ -76,7 +76,8 @@ class _Solver:
     def _call(self, name, *args):
         _lib.check(name, getattr(self.L, name)(self.h, *args))
 
-    TUNE_KEYS = {"col_mt": 0, "xrow_chunk": 1, "ychunk": 2, "cn_mt": 3, "pdl": 4, "fft_plan": 6}
+    TUNE_KEYS = {"col_mt": 0, "xrow_chunk": 1, "ychunk": 2, "cn_mt": 3, "pdl": 4, "fft_plan": 6,
+                 "plane_xz": 7}
 
     def tune_set(self, **kw):
         """Launch-shape tunables (results do not depend on them)."""

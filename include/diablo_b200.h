@@ -229,7 +229,12 @@ int dg_timing_read(dg_handle *h, int i, char *name, int name_len, int64_t *launc
  * fastest and restores the state, TIME and DELTA_T; it allocates temporary
  * device copies of the state while it runs. */
 enum { DG_TUNE_COL_MT = 0, DG_TUNE_XROW_CHUNK = 1, DG_TUNE_YCHUNK = 2, DG_TUNE_CN_MT = 3,
-       DG_TUNE_PDL = 4, DG_TUNE_WAIT_TEST = 5, DG_TUNE_FFT_PLAN = 6 };
+       DG_TUNE_PDL = 4, DG_TUNE_WAIT_TEST = 5, DG_TUNE_FFT_PLAN = 6, DG_TUNE_PLANE_XZ = 7 };
+/* DG_TUNE_PLANE_XZ: 1 (default) moves the LES model's fields between
+ * spectral planes and physical rows with one kernel per direction and plane
+ * where the x and z lengths allow (16, 32, 48, 64, 96 or 128); 0 stages them
+ * through a half-physical array in two launches.  Same transforms, same
+ * results; the setting is not tuned. */
 /* DG_TUNE_FFT_PLAN: radix order of the x and z transform plans of the
  * substep (0: largest radix first, 128 = 16 x 8; 1: the reverse, 8 x 16).
  * The same transform either way; the autotuner times both per grid shape.

@@ -520,12 +520,13 @@ __device__ __forceinline__ void les_row(const LesCn &P, int f, int j, double T1,
 
 // One thread per physical column of one field: rows, THOMAS_FORWARD_REAL_MPI
 // and THOMAS_BACKWARD_REAL_MPI for the only rank (for/mpi.f:630-703,767-809),
-// the solution written back over the reference's ranges.  R (slot f) holds
-// the right-hand side and then the eliminated one, B (scratch) the reciprocal
-// pivots (0 for a zero pivot: the backward sweep then writes 0, as the
-// reference's guard does); the back substitution rebuilds each row's upper
-// diagonal from NU_T rather than storing it.  Both sweeps load CB rows at a
-// time before their recurrence so the loads overlap.
+// the solution written back over the reference's ranges.  The forward sweep
+// stores per row the two coefficients of the back substitution
+// x(j) = e(j) + f(j) x(j+1), e = g / b and f = -c / b (R's slot takes e,
+// the scratch slot B takes f; both 0 for a zero pivot, so the backward
+// sweep writes 0 there, as the reference's guard does); the backward sweep
+// then reads only those two.  Both sweeps load CB rows at a time before
+// their recurrence so the loads overlap.
 constexpr int CB = 8;
 
 __global__ void __launch_bounds__(128) k_les_cn(LesCn P, long np, long pfield,
@@ -551,9 +552,9 @@ __global__ void __launch_bounds__(128) k_les_cn(LesCn P, long np, long pfield,
   const double *nq = nut + q;
   double l, d, u, v;
   les_row(P, f, 0, T1, T2, tab, L, 0., 0., 0., 0., 0., 0., 0., l, d, u, v);
-  double rbprev = (d != 0.0) ? 1.0 / d : 0.0, cprev = u, gprev = v, bprev = d;
-  B[0] = rbprev;
-  R[0] = v;
+  double rbprev = (d != 0.0) ? 1.0 / d : 0.0, cprev = u, gprev = v;
+  B[0] = -u * rbprev;
+  R[0] = v * rbprev;
   for (int j0 = 1; j0 < L; j0 += CB) {
     double uu[CB + 2], nn[CB + 2], rr[CB];
 #pragma unroll
@@ -579,10 +580,9 @@ __global__ void __launch_bounds__(128) k_les_cn(LesCn P, long np, long pfield,
         const double g = v + a * gprev;
         const double rb = (b != 0.0) ? 1.0 / b : 0.0;
         const long o = (long)j * np;
-        B[o] = rb;
-        R[o] = g;
+        B[o] = -u * rb;
+        R[o] = g * rb;
         rbprev = rb;
-        bprev = b;
         cprev = u;
         gprev = g;
       }
@@ -594,28 +594,21 @@ __global__ void __launch_bounds__(128) k_les_cn(LesCn P, long np, long pfield,
   if (f == 1) { wlo = 1; whi = NY + 1; }
   else if (f >= 3) { wlo = P.jst[f - 3] - 1; whi = P.jet[f - 3] + 1; }
   else { wlo = P.JS - 1; whi = P.JE + 1; }
-  double x = gprev / bprev;
-  if (NY + 1 >= wlo && NY + 1 <= whi) U[(long)(NY + 1) * np] = x;
-  for (int j1 = NY; j1 >= 0; j1 -= CB) {
-    double bb[CB], gg[CB], nn[CB + 2];  // nn[k]: NU_T on plane j1 + 1 - k
-#pragma unroll
-    for (int k = 0; k < CB + 2; k++) {
-      const int j = j1 + 1 - k;
-      nn[k] = (j >= 0 && j < L) ? nq[(long)j * np] : 0.0;
-    }
+  double x = 0.0;
+  for (int j1 = NY + 1; j1 >= 0; j1 -= CB) {
+    double ff[CB], ee[CB];
 #pragma unroll
     for (int k = 0; k < CB; k++) {
       const int j = j1 - k;
       const long o = (long)(j >= 0 ? j : 0) * np;
-      bb[k] = B[o];
-      gg[k] = R[o];
+      ff[k] = B[o];
+      ee[k] = R[o];
     }
 #pragma unroll
     for (int k = 0; k < CB; k++) {
       const int j = j1 - k;
       if (j >= 0) {
-        les_row(P, f, j, T1, T2, tab, L, 0., 0., 0., nn[k + 2], nn[k + 1], nn[k], 0., l, d, u, v);
-        x = (gg[k] - u * x) * bb[k];
+        x = ee[k] + ff[k] * x;
         if (j >= wlo && j <= whi) U[(long)j * np] = x;
       }
     }

@@ -231,40 +231,45 @@ __global__ void k_les_bc_phys(LesBc B, int NY, long np, long pfield, const doubl
 // GY, S13, S23 at GY; raw where the reference leaves S_ij unscaled), NU_T at
 // GY (zero on planes 1, 2, NY, NY+1: GHOST_LES_MPI for one rank) and the
 // cross terms NU_T dU1/dy, NU_T dU3/dy on planes 2..NY.
-__global__ void k_les_model(int NY, long np, long pfield, int JS, int JE,
-                            const double *__restrict__ dy, const double *__restrict__ dyf,
-                            const double *__restrict__ dfac, const double *__restrict__ ubar,
-                            const double *__restrict__ S, double *__restrict__ P,
-                            double *__restrict__ X, const double *__restrict__ U,
-                            double *__restrict__ NUT) {
+__global__ void __launch_bounds__(256, 4)
+    k_les_model(int NY, long np, long pfield, int JS, int JE, const double *__restrict__ dy,
+                const double *__restrict__ dyf, const double *__restrict__ dfac,
+                const double *__restrict__ ubar, const double *__restrict__ S,
+                double *__restrict__ P, double *__restrict__ X, const double *__restrict__ U,
+                double *__restrict__ NUT) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long)(NY + 2) * np) return;
   const int j = (int)(t / np);
   const long o = t;
   const double *u1b = ubar, *u3b = ubar + NY + 2;
+  const double *U1 = U, *U3 = U + 2 * pfield;
+  // every load the point needs, issued together (the neighbouring planes
+  // clamped to the point's own where the branches below do not use them),
+  // so the thread waits on memory once
+  const long m = (j >= 1) ? o - np : o, pn = (j <= NY) ? o + np : o;
   const double r0 = S[o], r1 = S[pfield + o], r2 = S[2 * pfield + o], r3 = S[3 * pfield + o];
   const double r4 = S[4 * pfield + o], r5 = S[5 * pfield + o];
+  const double s0m = S[m], s1m = S[pfield + m], s2m = S[2 * pfield + m], s4m = S[4 * pfield + m];
+  const double n3 = S[3 * pfield + pn], n5 = S[5 * pfield + pn];
+  const double u1o = U1[o], u1m = U1[m], u3o = U3[o], u3m = U3[m];
   double p0 = r0, p2 = r2, p3 = r3, p4 = r4, p5 = r5;
   double tg = 0.0;  // |S| at GY
   if (j >= 2) {
-    const long m = o - np;
     const double w = 2.0 * dy[j];
-    const double b1 = (r0 * dyf[j - 1] + S[m] * dyf[j]) / w;
+    const double b1 = (r0 * dyf[j - 1] + s0m * dyf[j]) / w;
     const double b4 = r3 - 0.5 * (u1b[j] - u1b[j - 1]) / dy[j];
-    const double b5 = (r4 * dyf[j - 1] + S[4 * pfield + m] * dyf[j]) / w;
-    const double b2 = (r1 * dyf[j - 1] + S[pfield + m] * dyf[j]) / w;
+    const double b5 = (r4 * dyf[j - 1] + s4m * dyf[j]) / w;
+    const double b2 = (r1 * dyf[j - 1] + s1m * dyf[j]) / w;
     const double b6 = r5 - 0.5 * (u3b[j] - u3b[j - 1]) / dy[j];
-    const double b3 = (r2 * dyf[j - 1] + S[2 * pfield + m] * dyf[j]) / w;
+    const double b3 = (r2 * dyf[j - 1] + s2m * dyf[j]) / w;
     tg = sqrt(2.0 * (b1 * b1) + 4.0 * (b4 * b4) + 4.0 * (b5 * b5) + 2.0 * (b2 * b2) +
               4.0 * (b6 * b6) + 2.0 * (b3 * b3));
-    const double *U1 = U, *U3 = U + 2 * pfield;
-    const double du1 = 0.5 * (U1[o] - U1[m]) / dy[j];
-    const double du3 = 0.5 * (U3[o] - U3[m]) / dy[j];
+    const double du1 = 0.5 * (u1o - u1m) / dy[j];
+    const double du3 = 0.5 * (u3o - u3m) / dy[j];
     p3 = tg * (r3 - du1);
     p5 = tg * (r5 - du3);
   }
   if (j >= JS && j <= JE) {
-    const double n3 = S[3 * pfield + o + np], n5 = S[5 * pfield + o + np];
     const double a4 = 0.5 * (n3 + r3 - 0.5 * (u1b[j] - u1b[j - 1]) / dy[j] -
                              0.5 * (u1b[j + 1] - u1b[j]) / dy[j + 1]);
     const double a6 = 0.5 * (n5 + r5 - 0.5 * (u3b[j] - u3b[j - 1]) / dy[j] -
@@ -284,9 +289,8 @@ __global__ void k_les_model(int NY, long np, long pfield, int JS, int JE,
     const double nut = (j >= 3 && j <= NY - 1) ? -0.5 * dfac[NY + 2 + j] * tg : 0.0;
     NUT[o] = nut;
     if (j >= 2 && j <= NY) {
-      const double *U1 = U, *U3 = U + 2 * pfield;
-      X[o] = nut * (U1[o] - U1[o - np]) / dy[j];
-      X[pfield + o] = nut * (U3[o] - U3[o - np]) / dy[j];
+      X[o] = nut * (u1o - u1m) / dy[j];
+      X[pfield + o] = nut * (u3o - u3m) / dy[j];
     }
   }
 }

@@ -341,6 +341,16 @@ __global__ void __launch_bounds__(NTHR) k_xr2c(const double *__restrict__ phys, 
 // signals per warp.
 constexpr int PL_THR = 128;
 
+// 16-byte asynchronous copy global -> shared (both addresses 16-byte aligned)
+__device__ __forceinline__ void pl_cp16(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+// wait for every copy this thread issued
+__device__ __forceinline__ void pl_cp_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 __host__ __device__ constexpr int pl_sz(int nz) { return padded_len(nz) | 1; }
 __host__ __device__ constexpr size_t pl_smem(int nx, int nz) {
   return sizeof(double2) * ((size_t)(nx / 3 + 1) * pl_sz(nz) + (PL_THR / 32) * 2 * padded_len(nx));
@@ -362,23 +372,13 @@ __global__ void __launch_bounds__(PL_THR, 2) k_plane_c2r(CFieldPtrs fields, int 
   const double2 *in = fields(f) + (long)j * ss;
   // 1. retained modes into their z bins (the band stays unwritten: the
   // pruned first pass does not read it); eight loads in flight per thread
-  for (int base = 0; base < NKZT * NKXP; base += 8 * PL_THR) {
-    double2 v[8];
-#pragma unroll
-    for (int u = 0; u < 8; u++) {
-      const int i = base + u * PL_THR + tid;
-      v[u] = (i < NKZT * NKXP) ? in[i] : make_double2(0.0, 0.0);
-    }
-#pragma unroll
-    for (int u = 0; u < 8; u++) {
-      const int i = base + u * PL_THR + tid;
-      if (i < NKZT * NKXP) {
-        const int kp = i / NKXP, kx = i - kp * NKXP;
-        const int z = (kp <= NKZ) ? kp : kp + NZT - NKZT;
-        Hs[kx * SZ + pad(z)] = v[u];
-      }
-    }
+  // by asynchronous 16-byte copies, all of the plane's in flight at once
+  for (int i = tid; i < NKZT * NKXP; i += PL_THR) {
+    const int kp = i / NKXP, kx = i - kp * NKXP;
+    const int z = (kp <= NKZ) ? kp : kp + NZT - NKZT;
+    pl_cp16(Hs + kx * SZ + pad(z), in + i);
   }
+  pl_cp_wait_all();
   __syncthreads();
   // 2. z inverse of every column
   fft_cta_inv_pz<NZT, 0>(Hs, NKXP, SZ, twz);
@@ -442,25 +442,34 @@ __global__ void __launch_bounds__(PL_THR, 2) k_plane_r2c(const double *__restric
   double2 *xw = xb + warp * 2 * SX;
   const double *in = phys + f * pfield + (long)j * pplane;
   const double rnx = (double)NXT;
-  // 1. x r2c of row pairs into the kx columns, kx = 0..NKX, / NX (as k_xr2c)
-  for (int p0 = 2 * warp; p0 < NZT / 2; p0 += 2 * (PL_THR / 32)) {
+  // 1. x r2c of row pairs into the kx columns, kx = 0..NKX, / NX (as k_xr2c);
+  // a round's rows are loaded while the previous round transforms
+  constexpr int XPL = (NXT + 31) / 32;
+  constexpr int PSTEP = 2 * (PL_THR / 32);
+  double va[2][XPL], vb[2][XPL];
+  auto fetch = [&](int p) {
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+#pragma unroll
+      for (int i = 0; i < XPL; i++) {
+        const int x = lane + 32 * i, za = 2 * (p + q);
+        const bool ok = p + q < NZT / 2 && x < NXT;
+        va[q][i] = ok ? in[(long)za * prow + x] : 0.0;
+        vb[q][i] = ok ? in[(long)(za + 1) * prow + x] : 0.0;
+      }
+  };
+  if (2 * warp < NZT / 2) fetch(2 * warp);
+  for (int p0 = 2 * warp; p0 < NZT / 2; p0 += PSTEP) {
     const int np = (NZT / 2 - p0) < 2 ? (NZT / 2 - p0) : 2;
-    for (int q = 0; q < np; q++) {
-      const int za = 2 * (p0 + q), zb = za + 1;
-      double a[(NXT + 31) / 32], b[(NXT + 31) / 32];
 #pragma unroll
-      for (int i = 0; i < (NXT + 31) / 32; i++) {
-        const int x = lane + 32 * i;
-        a[i] = (x < NXT) ? in[(long)za * prow + x] : 0.0;
-        b[i] = (x < NXT) ? in[(long)zb * prow + x] : 0.0;
-      }
+    for (int q = 0; q < 2; q++)
 #pragma unroll
-      for (int i = 0; i < (NXT + 31) / 32; i++) {
+      for (int i = 0; i < XPL; i++) {
         const int x = lane + 32 * i;
-        if (x < NXT) xw[q * SX + pad(x)] = make_double2(a[i], b[i]);
+        if (q < np && x < NXT) xw[q * SX + pad(x)] = make_double2(va[q][i], vb[q][i]);
       }
-    }
     __syncwarp();
+    if (p0 + PSTEP < NZT / 2) fetch(p0 + PSTEP);
     wpasses_any<NXT, -1, 0, 0, false>(xw, np, SX, twx, lane);
     for (int q = 0; q < np; q++) {
       const int za = 2 * (p0 + q), zb = za + 1;

@@ -52,7 +52,10 @@
 
 namespace {
 
-constexpr int SEG_K = 8;         // rows per segment of the CN recurrences
+// rows per segment of the CN recurrences: 9 keeps a 129-plane column at 8
+// modes per CTA within four warps (15 segments), so that at the 128
+// registers a thread takes four CTAs share an SM (five warps fit three)
+constexpr int SEG_K = 9;
 constexpr int COL_MAX_THR = 256; // threads per CTA: MT x segments, rounded up to warps
 
 struct ColConst {

@@ -531,7 +531,7 @@ __device__ __forceinline__ void les_row(const LesCn &P, int f, int j, double T1,
 // sweep writes 0 there, as the reference's guard does); the backward sweep
 // then reads only those two.  Both sweeps load CB rows at a time before
 // their recurrence so the loads overlap.
-constexpr int CB = 8;
+constexpr int CB = 12;
 
 __global__ void __launch_bounds__(128) k_les_cn(LesCn P, long np, long pfield,
                                                 const double *__restrict__ dscal, int rk_step,
